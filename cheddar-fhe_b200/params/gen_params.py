@@ -1,0 +1,129 @@
+"""Generate CKKS parameter files in the reference's JSON schema.
+
+The schema (log_degree, log_default_scale, default_encryption_level,
+main_primes, terminal_primes, auxiliary_primes, level_config,
+additional_base, dense/sparse_hamming_weight, boot, num_cts_levels,
+num_stc_levels) is the one the reference's test bed parses
+(unittest/Testbed.h:95-221 of scale-snu/cheddar-fhe).  The primes are found
+here: NTT-friendly (p = 1 mod 2N for N = 2^16, hence for every smaller N)
+and below 2^31, as Parameter.cu:40-62 requires.
+
+Run:  python gen_params.py   (rewrites the *.json files beside this script)
+"""
+import json
+import os
+
+TWO_N = 1 << 17
+
+
+def is_prime(n):
+    if n < 2:
+        return False
+    for p in (2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37):
+        if n % p == 0:
+            return n == p
+    d, s = n - 1, 0
+    while d % 2 == 0:
+        d //= 2
+        s += 1
+    for a in (2, 3, 5, 7, 11, 13, 17):  # deterministic below 3.4e14
+        x = pow(a, d, n)
+        if x in (1, n - 1):
+            continue
+        for _ in range(s - 1):
+            x = x * x % n
+            if x == n - 1:
+                break
+        else:
+            return False
+    return True
+
+
+def primes_near(target, count, used, direction):
+    """`count` primes p = 1 mod 2^17 walking away from `target`."""
+    out = []
+    k = target // TWO_N
+    while len(out) < count:
+        p = k * TWO_N + 1
+        if p < (1 << 31) and p not in used and is_prime(p):
+            out.append(p)
+            used.add(p)
+        k += direction
+    return out
+
+
+def alternating(target, count, used):
+    """Primes alternately just above and just below `target` so that the
+    running product of rescaled primes stays close to target^k."""
+    up = primes_near(target, (count + 1) // 2, used, +1)
+    down = primes_near(target, count // 2, used, -1)
+    out = []
+    for i in range(count):
+        out.append(up[i // 2] if i % 2 == 0 else down[i // 2])
+    return out
+
+
+def keyswitch_params(num_main, num_aux, log_n=16, log_scale=30):
+    used = set()
+    aux = primes_near((1 << 31) - 1, num_aux, used, -1)
+    main = alternating(1 << log_scale, num_main, used)
+    levels = [[k, 0] for k in range(2, num_main + 1)]
+    return {
+        "log_degree": log_n,
+        "log_default_scale": log_scale,
+        "boot": False,
+        "dense_hamming_weight": 192,
+        "sparse_hamming_weight": 32,
+        "terminal_primes": [],
+        "main_primes": main,
+        "auxiliary_primes": aux,
+        "default_encryption_level": len(levels) - 1,
+        "level_config": levels,
+        "additional_base": [0, 0],
+    }
+
+
+def rational_params(log_n=16):
+    """A small parameter set with terminal primes and rational rescale
+    (levels that drop main primes while restoring terminal primes and vice
+    versa), for exercising the restore/padding constants of the merged
+    ModDown+Rescale."""
+    used = set()
+    aux = primes_near((1 << 31) - 1, 6, used, -1)
+    ter = primes_near(1 << 25, 4, used, +1)
+    main = alternating(1 << 30, 10, used)
+    levels = [[0, 2], [3, 0], [1, 4], [4, 2], [7, 0], [5, 4], [8, 2],
+              [10, 0], [10, 2], [10, 4]]
+    return {
+        "log_degree": log_n,
+        "log_default_scale": 30,
+        "boot": False,
+        "dense_hamming_weight": 192,
+        "sparse_hamming_weight": 32,
+        "terminal_primes": ter,
+        "main_primes": main,
+        "auxiliary_primes": aux,
+        "default_encryption_level": 7,
+        "level_config": levels,
+        "additional_base": [0, 0],
+    }
+
+
+def main():
+    here = os.path.dirname(os.path.abspath(__file__))
+    files = {
+        # L = 24 q primes + alpha = 8 aux primes: dnum = 3 at the top level
+        "keyswitch_l24_a8.json": keyswitch_params(24, 8),
+        # small: L = 8 + alpha = 3 (beta = 3, ragged last digit)
+        "keyswitch_l8_a3.json": keyswitch_params(8, 3),
+        "rational_t4_m10_a6.json": rational_params(),
+    }
+    for name, obj in files.items():
+        with open(os.path.join(here, name), "w") as f:
+            json.dump(obj, f, indent=1)
+            f.write("\n")
+        print("wrote", name)
+
+
+if __name__ == "__main__":
+    main()
