@@ -1,0 +1,384 @@
+"""Benchmark: homomorphic multiplication with relinearisation and rescale
+(HMult, the key-switching workload) at N = 2^16 on one B200.
+
+Workload (the key-switching configuration): 24 q primes (~30 bit) + 8
+auxiliary primes (31 bit), hybrid key switching with dnum = 3, top level.
+A step is one HMult+relin+rescale of each of `--batch` independent
+ciphertext pairs (all resident in HBM, inputs larger than L2).  Residues are
+synthetic: uniform in [0, q) from a seed (ciphertexts and the key alike; the
+arithmetic does not depend on their distribution).
+
+Reported (one JSON line on rank 0):
+  value      HMult/s with inputs resident in HBM, CUDA events, max over ranks
+  e2e        the same through the C ABI with host buffers: each step copies
+             the batch in from pinned host memory, runs, copies results out
+  roofline   the dominant kernel, timed alone on the launching stream
+  cpu_baseline  the CPU oracle's HMult on the host cores (bounded sample)
+`--impl reference` times the CPU implementation of the path (the oracle;
+the reference itself has no CPU path and cannot be built here) on the same
+configuration.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "cheddar-fhe_b200"))
+
+PARAM_FILE = "keyswitch_l24_a8.json"
+METRIC = "HMult+relin+rescale/s (keyswitch/s) at N=2^16, L=24, alpha=8, dnum=3"
+UNIT = "HMult/s"
+
+
+def env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(
+        os.environ.get("LOCAL_RANK", "0"))
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        import statistics
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4)
+                          if len(s) > 5 + i and s[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def cpu_baseline_run(max_seconds=20.0, reps=None):
+    """Times the CPU oracle's HMult on the same configuration."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import pyoracle as po
+    p = po.load_param_json(os.path.join(ROOT, "cheddar-fhe_b200", "params", PARAM_FILE))
+    o = po.Oracle(p)
+    lvl = o.max_level
+    a = [o.uniform(1, lvl), o.uniform(2, lvl)]
+    b = [o.uniform(3, lvl), o.uniform(4, lvl)]
+    kb = np.stack([o.uniform(10 + i, o.max_level, num_aux=o.alpha) for i in range(o.beta_max)])
+    ka = np.stack([o.uniform(20 + i, o.max_level, num_aux=o.alpha) for i in range(o.beta_max)])
+    o.hmult(lvl, a, b, (kb, ka), rescale=True)  # warm
+    n = 0
+    t0 = time.perf_counter()
+    while True:
+        o.hmult(lvl, a, b, (kb, ka), rescale=True)
+        n += 1
+        el = time.perf_counter() - t0
+        if (reps is not None and n >= reps) or (reps is None and el > max_seconds / 2) or el > max_seconds:
+            break
+    return n / el, n, el
+
+
+def run_reference(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return 0
+    cores = os.cpu_count()
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    times = []
+    for _ in range(args.warmup):
+        cpu_baseline_run(reps=1)
+    total_n, total_t = 0, 0.0
+    for _ in range(args.steps):
+        v, n, el = cpu_baseline_run(reps=1)
+        total_n += n
+        total_t += el
+        times.append(el)
+    value = total_n / total_t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total_t / max(1, args.steps),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic", "config": {"workload": "HMult+relin+rescale, N=2^16, L=24 q primes, "
+                                                    "alpha=8 aux primes, dnum=3, top level", "batch": 1},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{total_n} HMults of the CPU oracle (OpenMP over limbs)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference is GPU-only (no CPU implementation) and needs rmm/libtommath, which "
+                "cannot be built here; the CPU arm is the oracle port of its algorithm",
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import numpy as np
+    import torch
+    import cheddar_b200 as chd
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+
+    params = json.load(open(os.path.join(chd.PARAM_DIR, PARAM_FILE)))
+    ctx = chd.Context(json.dumps(params), device=local)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    lvl = ctx.max_level
+    nq = ctx.num_q(lvl)
+    n = ctx.n
+    beta = -(-ctx.L // ctx.alpha)
+    primes = torch.tensor(chd_primes(ctx), dtype=torch.int64, device="cuda")
+    gen = torch.Generator(device="cuda").manual_seed(1234 + rank)
+
+    def uniform(rows, gidx):
+        q = primes[gidx][:, None]
+        r = torch.randint(0, 2 ** 62, (rows, n), generator=gen, device="cuda", dtype=torch.int64)
+        return (r % q).to(torch.int32)
+
+    qg = torch.tensor(ctx.gidx(*ctx.level_np(lvl), 0), device="cuda", dtype=torch.int64)
+    kg = torch.tensor(ctx.gidx(*ctx.level_np(ctx.max_level), ctx.alpha), device="cuda", dtype=torch.int64)
+    kb = torch.stack([uniform(len(kg), kg) for _ in range(beta)]).contiguous()
+    ka = torch.stack([uniform(len(kg), kg) for _ in range(beta)]).contiguous()
+    key = chd.EvaluationKey(ctx, kb, ka, on_device=True)
+    B = args.batch
+    ins = [[uniform(nq, qg) for _ in range(4)] for _ in range(B)]
+    a_cts = [ctx.import_ct(lvl, [x[0], x[1]], on_device=True) for x in ins]
+    b_cts = [ctx.import_ct(lvl, [x[2], x[3]], on_device=True) for x in ins]
+    outs = [chd.Ciphertext(ctx) for _ in range(B)]
+    torch.cuda.synchronize()
+
+    def step():
+        ctx.HMultBatch(a_cts, b_cts, key, rescale=True, res_list=outs)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    # ---- timed region (device events on the launching stream) ----
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler = ClockSampler(torch.cuda.current_device())
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with sampler:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = world * B * args.steps / (ms / 1e3)
+
+    # ---- end to end through the C ABI with host buffers ----
+    e2e = e2e_run(ctx, chd, key, lvl, nq, n, B, args, stream, dist)
+
+    # ---- dominant kernel roofline ----
+    roof = roofline_probe(ctx, chd, lvl, nq, n, stream)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": "HMult+relin+rescale, N=2^16, L=24 q primes (30-bit), alpha=8 aux primes "
+                               "(31-bit), dnum=3, top level", "batch_per_gpu": B,
+                   "l2": "inputs larger than L2 (batch x 24 MB + 48 MB key)",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": e2e, "roofline": roof, "clocks": sampler.summary(),
+        "gpu_launches": launches_per_step(B) * args.steps,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            v, cnt, el = cpu_baseline_run(max_seconds=20.0)
+            line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                                    "sample": f"{cnt} HMults of the CPU oracle in {el:.1f} s "
+                                              "(OpenMP over limbs, all host threads)"}
+        except Exception as e:  # pragma: no cover
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                                    "sample": f"failed: {e}"}
+    if rank == 0:
+        print(json.dumps(line))
+    del outs, a_cts, b_cts, key
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def chd_primes(ctx):
+    import json as _j
+    p = _j.load(open(os.path.join(ROOT, "cheddar-fhe_b200", "params", PARAM_FILE)))
+    ter = list(reversed(p.get("terminal_primes", [])))
+    return ter + p["main_primes"] + p["auxiliary_primes"]
+
+
+def launches_per_step(batch):
+    # per HMult: tensor 1, ModUp (INTT 2 + BConv 1 + NTT 2), key MAC 1,
+    # merged ModDown+Rescale (INTT 2 + BConv 1 + NTT 2)
+    return batch * 12
+
+
+def e2e_run(ctx, chd, key, lvl, nq, n, B, args, stream, dist):
+    import torch
+    words = nq * n
+    host_in = [torch.randint(0, 1 << 29, (4, nq, n), dtype=torch.int32).pin_memory() for _ in range(B)]
+    host_out = [torch.empty((2, ctx.num_q(lvl - 1), n), dtype=torch.int32).pin_memory() for _ in range(B)]
+    dev_in = [torch.empty((4, nq, n), dtype=torch.int32, device="cuda") for _ in range(B)]
+    a_cts = [ctx.wrap_ct(lvl, [dev_in[i][0], dev_in[i][1]]) for i in range(B)]
+    b_cts = [ctx.wrap_ct(lvl, [dev_in[i][2], dev_in[i][3]]) for i in range(B)]
+    outs = [chd.Ciphertext(ctx) for _ in range(B)]
+
+    def step():
+        with torch.cuda.stream(stream):
+            for i in range(B):
+                dev_in[i].copy_(host_in[i], non_blocking=True)
+        ctx.HMultBatch(a_cts, b_cts, key, rescale=True, res_list=outs)
+        for i in range(B):
+            bx, ax, _ = ptrs(chd, outs[i])
+            hb = host_out[i]
+            nb = hb[0].numel() * 4
+            cuda_copy_d2h(hb[0].data_ptr(), bx, nb, stream)
+            cuda_copy_d2h(hb[1].data_ptr(), ax, nb, stream)
+
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    ev0.record(stream)
+    steps = max(3, args.steps // 2)
+    for _ in range(steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    world = 1
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        world = dist.get_world_size()
+    return {"value": world * B * steps / (ms / 1e3), "unit": UNIT,
+            "h2d_bytes_per_step": B * 4 * words * 4,
+            "d2h_bytes_per_step": B * 2 * ctx.num_q(lvl - 1) * n * 4}
+
+
+_cudart = None
+
+
+def cuda_copy_d2h(dst, src, nbytes, stream):
+    import ctypes
+    global _cudart
+    if _cudart is None:
+        import torch  # noqa: F401  (loads libcudart)
+        for name in ("libcudart.so.12", "libcudart.so"):
+            try:
+                _cudart = ctypes.CDLL(name)
+                break
+            except OSError:
+                continue
+        _cudart.cudaMemcpyAsync.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int,
+                                            ctypes.c_void_p]
+    rc = _cudart.cudaMemcpyAsync(ctypes.c_void_p(dst), ctypes.c_void_p(src), nbytes, 2,
+                                 ctypes.c_void_p(stream.cuda_stream))
+    if rc != 0:
+        raise RuntimeError(f"cudaMemcpyAsync failed: {rc}")
+
+
+def ptrs(chd, ct):
+    import ctypes
+    bx, ax, rx = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+    chd._check(chd.lib().chd_ct_device_ptrs(ct.ptr, ctypes.byref(bx), ctypes.byref(ax), ctypes.byref(rx)))
+    return bx.value, ax.value, rx.value
+
+
+def roofline_probe(ctx, chd, lvl, nq, n, stream):
+    """Times the forward NTT over the rows a batched ModUp transforms (the
+    kernel pair that dominates the launch list) on the launching stream.
+    Algorithmic bytes per launch: every limb read once and written once."""
+    import torch
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    m, t = ctx.level_np(lvl)
+    polys = 8
+    total = nq + ctx.alpha
+    buf = torch.randint(0, 1 << 29, (polys, total, n), dtype=torch.int32, device="cuda")
+    reps = 20
+    for _ in range(3):
+        ctx.ntt_raw(m, t, ctx.alpha, buf, mont=False, count=polys)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        ctx.ntt_raw(m, t, ctx.alpha, buf, mont=False, count=polys)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    algo_bytes = 2 * polys * total * n * 4  # one read + one write of every limb
+    achieved = algo_bytes / (ms / 1e3) / 1e9
+    return {"kernel": "forward NTT (column + row phase) over 8 x 32 limbs", "bound": "hbm",
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_source": peak_src, "traffic": None, "algorithmic_bytes_per_launch": algo_bytes,
+            "ms_per_launch": ms}
+
+
+if __name__ == "__main__":
+    sys.exit(main())

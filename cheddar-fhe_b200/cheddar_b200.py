@@ -1,0 +1,401 @@
+"""Python binding of the B200 CKKS evaluation core (libcheddar_b200.so).
+
+Mirrors the reference's server-side C++ API (scale-snu/cheddar-fhe,
+include/core/Context.h, include/core/Container.h): a Context created from
+the parameter JSON, device Ciphertexts, EvaluationKeys, and the evaluator
+calls HMult / HRot / HConj / Relinearize / Rescale / ... with the same
+argument meaning.  Everything runs in the CUDA library; this module only
+marshals arguments.  It raises if the library is missing — there is no CPU
+fallback.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcheddar_b200.so")
+PARAM_DIR = os.path.join(_HERE, "params")
+
+CHD_MODDOWN, CHD_RESCALE, CHD_MODDOWN_RESCALE = 0, 1, 2
+
+_lib = None
+
+
+class CheddarError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"cheddar error {code}: {msg}")
+        self.code = code
+
+
+def build():
+    """Compile the CUDA library in-tree (nvcc, sm_100a)."""
+    import subprocess
+    subprocess.run(["make", "-s", "-C", _HERE, "-j8"], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C {_HERE}`")
+    L = C.CDLL(LIB_PATH)
+    vp, i, d, u32p, i32p = C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_void_p
+    pp = C.POINTER(C.c_void_p)
+    sig = {
+        "chd_last_error": (C.c_char_p, []),
+        "chd_context_create_json": (i, [C.c_char_p, i, pp]),
+        "chd_context_create": (i, [i, d, i, i32p, i, u32p, i, u32p, i, u32p, i, i, i, i, pp]),
+        "chd_context_destroy": (None, [vp]),
+        "chd_context_set_stream": (i, [vp, vp]),
+        "chd_context_synchronize": (i, [vp]),
+        "chd_level_np": (i, [vp, i, C.POINTER(i), C.POINTER(i)]),
+        "chd_max_level": (i, [vp]),
+        "chd_degree": (i, [vp]),
+        "chd_alpha": (i, [vp]),
+        "chd_num_q_primes": (i, [vp]),
+        "chd_scale": (d, [vp, i]),
+        "chd_rescale_prime_prod": (d, [vp, i]),
+        "chd_prime_gidx": (i, [vp, i, i, i, i32p]),
+        "chd_ct_create": (i, [vp, pp]),
+        "chd_ct_destroy": (None, [vp]),
+        "chd_ct_wrap": (i, [vp, i, i, i, i, d, i, vp, vp, vp, C.c_size_t, pp]),
+        "chd_ct_import": (i, [vp, vp, i, i, i, i, d, i, vp, vp, vp, i]),
+        "chd_ct_export": (i, [vp, vp, vp, vp, vp, i]),
+        "chd_ct_info": (i, [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(i),
+                            C.POINTER(d), C.POINTER(i)]),
+        "chd_ct_device_ptrs": (i, [vp, pp, pp, pp]),
+        "chd_evk_create": (i, [vp, i, vp, vp, i, pp]),
+        "chd_evk_destroy": (None, [vp]),
+        "chd_add": (i, [vp, vp, vp, vp]),
+        "chd_sub": (i, [vp, vp, vp, vp]),
+        "chd_neg": (i, [vp, vp, vp]),
+        "chd_mult": (i, [vp, vp, vp, vp]),
+        "chd_mult_const": (i, [vp, vp, vp, u32p, d]),
+        "chd_add_const": (i, [vp, vp, vp, u32p]),
+        "chd_mult_plain": (i, [vp, vp, vp, vp, d]),
+        "chd_mult_imaginary_unit": (i, [vp, vp, vp]),
+        "chd_rescale": (i, [vp, vp, vp]),
+        "chd_relinearize": (i, [vp, vp, vp, vp]),
+        "chd_relinearize_rescale": (i, [vp, vp, vp, vp]),
+        "chd_mult_key": (i, [vp, vp, vp, vp]),
+        "chd_hmult": (i, [vp, vp, vp, vp, vp, i]),
+        "chd_hmult_batch": (i, [vp, i, pp, pp, pp, vp, i]),
+        "chd_hrot": (i, [vp, vp, vp, vp, i]),
+        "chd_hconj": (i, [vp, vp, vp, vp]),
+        "chd_hrot_add": (i, [vp, vp, vp, vp, vp, i]),
+        "chd_hoisted_rotate": (i, [vp, vp, i, i32p, pp, pp]),
+        "chd_moddown": (i, [vp, vp, vp]),
+        "chd_ntt": (i, [vp, i, i, i, vp, i, i]),
+        "chd_intt": (i, [vp, i, i, i, vp, i, i]),
+        "chd_modup_raw": (i, [vp, i, vp, vp]),
+        "chd_moddown_raw": (i, [vp, i, i, vp, vp, i]),
+        "chd_bconv_raw": (i, [vp, vp, i32p, i, i32p, i, vp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def _check(rc):
+    if rc != 0:
+        raise CheddarError(rc, lib().chd_last_error().decode())
+
+
+def _ptr(a):
+    """Device or host pointer of a numpy array or torch tensor."""
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return a
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    return a.ctypes.data
+
+
+def load_params(name_or_path):
+    path = name_or_path
+    if not os.path.exists(path):
+        path = os.path.join(PARAM_DIR, name_or_path)
+    with open(path) as f:
+        return f.read()
+
+
+class Context:
+    """Context<uint32_t>::Create(Parameter) (include/core/Context.h:70)."""
+
+    def __init__(self, json_text, device=0):
+        self.ptr = C.c_void_p()
+        _check(lib().chd_context_create_json(json_text.encode(), device, C.byref(self.ptr)))
+        L = lib()
+        self.max_level = L.chd_max_level(self.ptr)
+        self.n = L.chd_degree(self.ptr)
+        self.alpha = L.chd_alpha(self.ptr)
+        self.L = L.chd_num_q_primes(self.ptr)
+
+    @classmethod
+    def from_params(cls, name_or_path, device=0):
+        return cls(load_params(name_or_path), device)
+
+    def close(self):
+        if getattr(self, "ptr", None) and self.ptr.value:
+            lib().chd_context_destroy(self.ptr)
+            self.ptr = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_handle):
+        _check(lib().chd_context_set_stream(self.ptr, stream_handle))
+
+    def synchronize(self):
+        _check(lib().chd_context_synchronize(self.ptr))
+
+    def level_np(self, level):
+        m, t = C.c_int(), C.c_int()
+        _check(lib().chd_level_np(self.ptr, level, C.byref(m), C.byref(t)))
+        return m.value, t.value
+
+    def num_q(self, level):
+        m, t = self.level_np(level)
+        return m + t
+
+    def scale(self, level):
+        return lib().chd_scale(self.ptr, level)
+
+    def rescale_prime_prod(self, level):
+        return lib().chd_rescale_prime_prod(self.ptr, level)
+
+    def gidx(self, num_main, num_ter, num_aux):
+        out = np.zeros(256, dtype=np.int32)
+        k = lib().chd_prime_gidx(self.ptr, num_main, num_ter, num_aux, out.ctypes.data)
+        return out[:k].copy()
+
+    # ---- containers ----
+    def ciphertext(self):
+        return Ciphertext(self)
+
+    def import_ct(self, level, parts, scale=1.0, num_slots=None, num_aux=0, on_device=False):
+        ct = Ciphertext(self)
+        ct.load(level, parts, scale, num_slots, num_aux, on_device)
+        return ct
+
+    def wrap_ct(self, level, parts, scale=1.0, num_slots=None, num_aux=0):
+        """Ciphertext over caller-owned device buffers (torch tensors)."""
+        m, t = self.level_np(level)
+        rows = m + t + num_aux
+        words = min(int(p.numel()) for p in parts)
+        assert words >= rows * self.n
+        ct = Ciphertext.__new__(Ciphertext)
+        ct.ctx = self
+        ct.ptr = C.c_void_p()
+        ct._keep = parts
+        rx = _ptr(parts[2]) if len(parts) > 2 else None
+        _check(lib().chd_ct_wrap(self.ptr, m, t, num_aux, int(len(parts) > 2), scale,
+                                 num_slots or self.n // 2, _ptr(parts[0]), _ptr(parts[1]), rx,
+                                 words, C.byref(ct.ptr)))
+        return ct
+
+    def evk(self, bx, ax, on_device=False):
+        return EvaluationKey(self, bx, ax, on_device)
+
+    # ---- evaluator (Context.cpp of the reference) ----
+    def _new(self, res):
+        return res if res is not None else Ciphertext(self)
+
+    def Add(self, a, b, res=None):
+        res = self._new(res)
+        _check(lib().chd_add(self.ptr, res.ptr, a.ptr, b.ptr))
+        return res
+
+    def Sub(self, a, b, res=None):
+        res = self._new(res)
+        _check(lib().chd_sub(self.ptr, res.ptr, a.ptr, b.ptr))
+        return res
+
+    def Neg(self, a, res=None):
+        res = self._new(res)
+        _check(lib().chd_neg(self.ptr, res.ptr, a.ptr))
+        return res
+
+    def Mult(self, a, b, res=None):
+        res = self._new(res)
+        _check(lib().chd_mult(self.ptr, res.ptr, a.ptr, b.ptr))
+        return res
+
+    def MultConst(self, a, cx, const_scale, res=None):
+        res = self._new(res)
+        cx = np.ascontiguousarray(cx, dtype=np.uint32)
+        _check(lib().chd_mult_const(self.ptr, res.ptr, a.ptr, cx.ctypes.data, const_scale))
+        return res
+
+    def AddConst(self, a, cx, res=None):
+        res = self._new(res)
+        cx = np.ascontiguousarray(cx, dtype=np.uint32)
+        _check(lib().chd_add_const(self.ptr, res.ptr, a.ptr, cx.ctypes.data))
+        return res
+
+    def MultImaginaryUnit(self, a, res=None):
+        res = self._new(res)
+        _check(lib().chd_mult_imaginary_unit(self.ptr, res.ptr, a.ptr))
+        return res
+
+    def Rescale(self, a, res=None):
+        res = self._new(res)
+        _check(lib().chd_rescale(self.ptr, res.ptr, a.ptr))
+        return res
+
+    def Relinearize(self, a, key, res=None):
+        res = self._new(res)
+        _check(lib().chd_relinearize(self.ptr, res.ptr, a.ptr, key.ptr))
+        return res
+
+    def RelinearizeRescale(self, a, key, res=None):
+        res = self._new(res)
+        _check(lib().chd_relinearize_rescale(self.ptr, res.ptr, a.ptr, key.ptr))
+        return res
+
+    def MultKey(self, a, key, res=None):
+        res = self._new(res)
+        _check(lib().chd_mult_key(self.ptr, res.ptr, a.ptr, key.ptr))
+        return res
+
+    def HMult(self, a, b, mult_key, rescale=True, res=None):
+        res = self._new(res)
+        _check(lib().chd_hmult(self.ptr, res.ptr, a.ptr, b.ptr, mult_key.ptr, int(rescale)))
+        return res
+
+    def HMultBatch(self, a_list, b_list, mult_key, rescale=True, res_list=None):
+        n = len(a_list)
+        res_list = res_list or [Ciphertext(self) for _ in range(n)]
+        arr = lambda xs: (C.c_void_p * n)(*[x.ptr.value for x in xs])
+        _check(lib().chd_hmult_batch(self.ptr, n, arr(res_list), arr(a_list), arr(b_list),
+                                     mult_key.ptr, int(rescale)))
+        return res_list
+
+    def HRot(self, a, rot_key, rot_dist, res=None):
+        res = self._new(res)
+        _check(lib().chd_hrot(self.ptr, res.ptr, a.ptr, rot_key.ptr, rot_dist))
+        return res
+
+    def HConj(self, a, conj_key, res=None):
+        res = self._new(res)
+        _check(lib().chd_hconj(self.ptr, res.ptr, a.ptr, conj_key.ptr))
+        return res
+
+    def HRotAdd(self, a, b, rot_key, rot_dist, res=None):
+        res = self._new(res)
+        _check(lib().chd_hrot_add(self.ptr, res.ptr, a.ptr, b.ptr, rot_key.ptr, rot_dist))
+        return res
+
+    def HoistedRotate(self, a, rot_keys, rot_dists, outs=None):
+        n = len(rot_dists)
+        outs = outs or [Ciphertext(self) for _ in range(n)]
+        d = np.asarray(rot_dists, dtype=np.int32)
+        keys = (C.c_void_p * n)(*[k.ptr.value for k in rot_keys])
+        outp = (C.c_void_p * n)(*[o.ptr.value for o in outs])
+        _check(lib().chd_hoisted_rotate(self.ptr, a.ptr, n, d.ctypes.data, keys, outp))
+        return outs
+
+    def ModDown(self, a, res=None):
+        res = self._new(res)
+        _check(lib().chd_moddown(self.ptr, res.ptr, a.ptr))
+        return res
+
+    # ---- raw device-buffer kernels (parity entry points) ----
+    def ntt_raw(self, num_main, num_ter, num_aux, dev_ptr, mont=False, count=1):
+        _check(lib().chd_ntt(self.ptr, num_main, num_ter, num_aux, _ptr(dev_ptr), int(mont), count))
+
+    def intt_raw(self, num_main, num_ter, num_aux, dev_ptr, mont=True, count=1):
+        _check(lib().chd_intt(self.ptr, num_main, num_ter, num_aux, _ptr(dev_ptr), int(mont), count))
+
+    def modup_raw(self, level, src, dst):
+        _check(lib().chd_modup_raw(self.ptr, level, _ptr(src), _ptr(dst)))
+
+    def moddown_raw(self, level, kind, src, dst, npoly=1):
+        _check(lib().chd_moddown_raw(self.ptr, level, kind, _ptr(src), _ptr(dst), npoly))
+
+    def bconv_raw(self, xt, src_gidx, dst_gidx, out):
+        s = np.ascontiguousarray(src_gidx, dtype=np.int32)
+        d = np.ascontiguousarray(dst_gidx, dtype=np.int32)
+        _check(lib().chd_bconv_raw(self.ptr, _ptr(xt), s.ctypes.data, len(s), d.ctypes.data, len(d),
+                                   _ptr(out)))
+
+
+class Ciphertext:
+    """Ciphertext<uint32_t> on the device (include/core/Container.h:131-175)."""
+
+    def __init__(self, ctx):
+        self.ctx = ctx
+        self.ptr = C.c_void_p()
+        _check(lib().chd_ct_create(ctx.ptr, C.byref(self.ptr)))
+
+    def __del__(self):
+        try:
+            if self.ptr.value:
+                lib().chd_ct_destroy(self.ptr)
+                self.ptr = C.c_void_p()
+        except Exception:
+            pass
+
+    def load(self, level, parts, scale=1.0, num_slots=None, num_aux=0, on_device=False):
+        m, t = self.ctx.level_np(level)
+        num_slots = num_slots or self.ctx.n // 2
+        if on_device:
+            ps = [_ptr(p) for p in parts]
+        else:
+            self._host = [np.ascontiguousarray(p, dtype=np.uint32) for p in parts]
+            ps = [p.ctypes.data for p in self._host]
+        rx = ps[2] if len(ps) > 2 else None
+        _check(lib().chd_ct_import(self.ctx.ptr, self.ptr, m, t, num_aux, int(len(ps) > 2), scale,
+                                   num_slots, ps[0], ps[1], rx, int(on_device)))
+        self._host = None
+        return self
+
+    def info(self):
+        m, t, a, rx, ns = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        sc = C.c_double()
+        _check(lib().chd_ct_info(self.ptr, C.byref(m), C.byref(t), C.byref(a), C.byref(rx),
+                                 C.byref(sc), C.byref(ns)))
+        return dict(num_main=m.value, num_ter=t.value, num_aux=a.value, has_rx=bool(rx.value),
+                    scale=sc.value, num_slots=ns.value)
+
+    def numpy(self):
+        inf = self.info()
+        rows = inf["num_main"] + inf["num_ter"] + inf["num_aux"]
+        parts = [np.zeros((rows, self.ctx.n), dtype=np.uint32) for _ in range(3 if inf["has_rx"] else 2)]
+        _check(lib().chd_ct_export(self.ctx.ptr, self.ptr, parts[0].ctypes.data, parts[1].ctypes.data,
+                                   parts[2].ctypes.data if len(parts) > 2 else None, 0))
+        return parts
+
+
+class EvaluationKey:
+    """EvaluationKey<uint32_t>: beta pairs over the key basis [L + alpha][N]."""
+
+    def __init__(self, ctx, bx, ax, on_device=False):
+        self.ctx = ctx
+        self.ptr = C.c_void_p()
+        if on_device:
+            beta = bx.shape[0]
+            pb, pa = _ptr(bx), _ptr(ax)
+        else:
+            bx = np.ascontiguousarray(bx, dtype=np.uint32)
+            ax = np.ascontiguousarray(ax, dtype=np.uint32)
+            beta = bx.shape[0]
+            pb, pa = bx.ctypes.data, ax.ctypes.data
+        _check(lib().chd_evk_create(ctx.ptr, beta, pb, pa, int(on_device), C.byref(self.ptr)))
+
+    def __del__(self):
+        try:
+            if self.ptr.value:
+                lib().chd_evk_destroy(self.ptr)
+                self.ptr = C.c_void_p()
+        except Exception:
+            pass

@@ -1,0 +1,81 @@
+// Device modular arithmetic for 31-bit NTT-friendly primes.
+//
+// Residues are stored canonical in [0, q).  Products use signed Montgomery
+// reduction with R = 2^32 (the same number representation as the reference,
+// include/common/Basic.cuh:80-260 of scale-snu/cheddar-fhe: every evaluation-
+// domain residue x is held as x * R mod q).  The reduction below follows the
+// published signed-Montgomery method (G. Seiler, "Faster AVX2 optimized NTT
+// multiplication for Ring-LWE lattice cryptography", 2018): for |a| < q*2^31
+//   m = lo(a) * q^-1 mod 2^32 (signed),  r = hi(a) - hi(m * q)  in (-q, q),
+// and r = a * 2^-32 mod q.
+#pragma once
+
+#include <cstdint>
+
+namespace chd {
+
+struct Modulus {
+  uint32_t q;
+  int32_t qinv;  // q^-1 mod 2^32 as a signed word
+};
+
+__device__ __forceinline__ int32_t mont_reduce_lazy(int64_t a, uint32_t q, int32_t qinv) {
+  int32_t lo = static_cast<int32_t>(static_cast<uint32_t>(static_cast<uint64_t>(a)));
+  int32_t hi = static_cast<int32_t>(a >> 32);
+  int32_t m = lo * qinv;
+  return hi - __mulhi(m, static_cast<int32_t>(q));
+}
+
+// a * b * 2^-32 mod q in (-q, q) for |a * b| < q * 2^31
+__device__ __forceinline__ int32_t mont_mul_lazy(int32_t a, int32_t b, uint32_t q, int32_t qinv) {
+  int32_t lo = a * b;
+  int32_t hi = __mulhi(a, b);
+  int32_t m = lo * qinv;
+  return hi - __mulhi(m, static_cast<int32_t>(q));
+}
+
+__device__ __forceinline__ uint32_t canon(int32_t r, uint32_t q) {
+  return static_cast<uint32_t>(r < 0 ? r + static_cast<int32_t>(q) : r);
+}
+
+// canonical Montgomery product of canonical operands
+__device__ __forceinline__ uint32_t mont_mul(uint32_t a, uint32_t b, uint32_t q, int32_t qinv) {
+  return canon(mont_mul_lazy(static_cast<int32_t>(a), static_cast<int32_t>(b), q, qinv), q);
+}
+
+__device__ __forceinline__ uint32_t mont_reduce(int64_t a, uint32_t q, int32_t qinv) {
+  return canon(mont_reduce_lazy(a, q, qinv), q);
+}
+
+__device__ __forceinline__ uint32_t add_mod(uint32_t a, uint32_t b, uint32_t q) {
+  uint32_t r = a + b;
+  return r >= q ? r - q : r;
+}
+
+__device__ __forceinline__ uint32_t sub_mod(uint32_t a, uint32_t b, uint32_t q) {
+  int32_t r = static_cast<int32_t>(a) - static_cast<int32_t>(b);
+  return static_cast<uint32_t>(r < 0 ? r + static_cast<int32_t>(q) : r);
+}
+
+__device__ __forceinline__ uint32_t neg_mod(uint32_t a, uint32_t q) { return a ? q - a : 0u; }
+
+// centred representative in [-(q-1)/2, (q-1)/2] of a canonical residue
+__device__ __forceinline__ int32_t centre(uint32_t a, uint32_t q) {
+  return a > (q >> 1) ? static_cast<int32_t>(a) - static_cast<int32_t>(q) : static_cast<int32_t>(a);
+}
+
+// Cooley-Tukey butterfly on canonical values: (a, b) -> (a + w b, a - w b)
+__device__ __forceinline__ void ct_bfly(uint32_t &a, uint32_t &b, uint32_t w, uint32_t q, int32_t qinv) {
+  uint32_t t = mont_mul(b, w, q, qinv);
+  b = sub_mod(a, t, q);
+  a = add_mod(a, t, q);
+}
+
+// Gentleman-Sande butterfly on canonical values: (a, b) -> (a + b, (a - b) w)
+__device__ __forceinline__ void gs_bfly(uint32_t &a, uint32_t &b, uint32_t w, uint32_t q, int32_t qinv) {
+  uint32_t d = sub_mod(a, b, q);
+  a = add_mod(a, b, q);
+  b = mont_mul(d, w, q, qinv);
+}
+
+}  // namespace chd

@@ -1,0 +1,510 @@
+// C ABI over the host evaluator (include/cheddar_b200.h).
+#include <cstring>
+
+#include "../../include/cheddar_b200.h"
+#include "host.h"
+
+using namespace chd;
+
+struct chd_context {
+  std::unique_ptr<Context> c;
+};
+struct chd_ciphertext {
+  DeviceCt ct;
+};
+struct chd_evk {
+  DeviceEvk k;
+};
+
+namespace {
+int fail(int code, const std::string &msg) {
+  set_error(msg);
+  return code;
+}
+#define CHD_NOTNULL(p) \
+  if (!(p)) return fail(CHD_ERR_INVALID_ARG, std::string(__func__) + ": null argument " #p)
+}  // namespace
+
+extern "C" {
+
+const char *chd_last_error(void) { return last_error(); }
+
+int chd_context_create_json(const char *json_text, int device, chd_context **out) {
+  CHD_NOTNULL(json_text);
+  CHD_NOTNULL(out);
+  ParamSpec spec;
+  std::string err;
+  if (!parse_param_json(json_text, &spec, &err)) return fail(CHD_ERR_PARSE, err);
+  auto c = Context::create(spec, device, &err);
+  if (!c) return fail(CHD_ERR_INVALID_ARG, err);
+  *out = new chd_context{std::move(c)};
+  return CHD_OK;
+}
+
+int chd_context_create(int log_degree, double base_scale, int default_encryption_level, const int *level_config,
+                       int num_levels, const uint32_t *main_primes, int num_main, const uint32_t *aux_primes,
+                       int num_aux, const uint32_t *ter_primes, int num_ter, int additional_main,
+                       int additional_ter, int device, chd_context **out) {
+  CHD_NOTNULL(level_config);
+  CHD_NOTNULL(main_primes);
+  CHD_NOTNULL(aux_primes);
+  CHD_NOTNULL(out);
+  if (num_ter > 0 && !ter_primes) return fail(CHD_ERR_INVALID_ARG, "ter_primes is null");
+  ParamSpec s;
+  s.log_degree = log_degree;
+  s.base_scale = base_scale;
+  s.default_encryption_level = default_encryption_level;
+  for (int i = 0; i < num_levels; i++) s.level_config.emplace_back(level_config[2 * i], level_config[2 * i + 1]);
+  s.main_primes.assign(main_primes, main_primes + num_main);
+  s.aux_primes.assign(aux_primes, aux_primes + num_aux);
+  if (num_ter > 0) s.ter_primes.assign(ter_primes, ter_primes + num_ter);
+  s.additional_base = {additional_main, additional_ter};
+  std::string err;
+  auto c = Context::create(s, device, &err);
+  if (!c) return fail(CHD_ERR_INVALID_ARG, err);
+  *out = new chd_context{std::move(c)};
+  return CHD_OK;
+}
+
+void chd_context_destroy(chd_context *ctx) { delete ctx; }
+
+int chd_context_set_stream(chd_context *ctx, void *cuda_stream) {
+  CHD_NOTNULL(ctx);
+  Context &C = *ctx->c;
+  if (C.own_stream && C.stream) {
+    cudaStreamSynchronize(C.stream);
+  }
+  if (cuda_stream) {
+    if (C.own_stream && C.stream) cudaStreamDestroy(C.stream);
+    C.own_stream = false;
+    C.stream = static_cast<cudaStream_t>(cuda_stream);
+  } else if (!C.own_stream) {
+    cudaStreamCreateWithFlags(&C.stream, cudaStreamNonBlocking);
+    C.own_stream = true;
+  }
+  return CHD_OK;
+}
+
+int chd_context_synchronize(chd_context *ctx) {
+  CHD_NOTNULL(ctx);
+  cudaError_t e = cudaStreamSynchronize(ctx->c->stream);
+  if (e != cudaSuccess) return fail(CHD_ERR_CUDA, cudaGetErrorString(e));
+  return CHD_OK;
+}
+
+int chd_level_np(const chd_context *ctx, int level, int *num_main, int *num_ter) {
+  CHD_NOTNULL(ctx);
+  const Params &P = *ctx->c->P;
+  if (level < -1 || level > P.max_level) return fail(CHD_ERR_INVALID_LEVEL, "invalid level");
+  NP np = P.level_np(level, 0);
+  if (num_main) *num_main = np.main;
+  if (num_ter) *num_ter = np.ter;
+  return CHD_OK;
+}
+int chd_max_level(const chd_context *ctx) { return ctx ? ctx->c->P->max_level : -1; }
+int chd_degree(const chd_context *ctx) { return ctx ? ctx->c->P->n : -1; }
+int chd_alpha(const chd_context *ctx) { return ctx ? ctx->c->P->alpha : -1; }
+int chd_num_q_primes(const chd_context *ctx) { return ctx ? ctx->c->P->L : -1; }
+double chd_scale(const chd_context *ctx, int level) {
+  if (!ctx) return 0.0;
+  const Params &P = *ctx->c->P;
+  if (level == -1) level = 0;
+  if (level < 0 || level >= static_cast<int>(P.scale.size())) return 0.0;
+  return P.scale[level];
+}
+double chd_rescale_prime_prod(const chd_context *ctx, int level) {
+  if (!ctx) return 0.0;
+  const Params &P = *ctx->c->P;
+  if (level < 1 || level > P.max_level) return 0.0;
+  return P.rescale_prod[level];
+}
+int chd_prime_gidx(const chd_context *ctx, int num_main, int num_ter, int num_aux, int *out) {
+  if (!ctx || !out) return -1;
+  NP np{num_main, num_ter, num_aux};
+  ctx->c->P->gidx(np, out);
+  return np.total();
+}
+
+int chd_ct_create(chd_context *ctx, chd_ciphertext **out) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(out);
+  *out = new chd_ciphertext();
+  (*out)->ct.num_slots = ctx->c->P->n / 2;
+  return CHD_OK;
+}
+
+void chd_ct_destroy(chd_ciphertext *ct) { delete ct; }
+
+int chd_ct_wrap(chd_context *ctx, int num_main, int num_ter, int num_aux, int has_rx, double scale, int num_slots,
+                uint32_t *bx, uint32_t *ax, uint32_t *rx, size_t words_per_part, chd_ciphertext **out) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(out);
+  CHD_NOTNULL(bx);
+  CHD_NOTNULL(ax);
+  if (has_rx && !rx) return fail(CHD_ERR_INVALID_ARG, "chd_ct_wrap: rx is null");
+  NP np{num_main, num_ter, num_aux};
+  if (static_cast<size_t>(np.total()) * ctx->c->P->n > words_per_part)
+    return fail(CHD_ERR_SHAPE, "chd_ct_wrap: buffers smaller than the ciphertext");
+  auto *c = new chd_ciphertext();
+  c->ct.owned = false;
+  c->ct.np = np;
+  c->ct.has_rx = has_rx != 0;
+  c->ct.scale = scale;
+  c->ct.num_slots = num_slots;
+  c->ct.bx = bx;
+  c->ct.ax = ax;
+  c->ct.rx = has_rx ? rx : nullptr;
+  c->ct.cap_words = words_per_part;
+  *out = c;
+  return CHD_OK;
+}
+
+int chd_ct_import(chd_context *ctx, chd_ciphertext *ct, int num_main, int num_ter, int num_aux, int has_rx,
+                  double scale, int num_slots, const uint32_t *bx, const uint32_t *ax, const uint32_t *rx,
+                  int src_on_device) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(ct);
+  CHD_NOTNULL(bx);
+  CHD_NOTNULL(ax);
+  if (has_rx && !rx) return fail(CHD_ERR_INVALID_ARG, "chd_ct_import: rx is null");
+  Context &C = *ctx->c;
+  NP np{num_main, num_ter, num_aux};
+  if (C.P->np_to_level(NP{num_main, num_ter, 0}) < -1 || num_aux < 0 || num_aux > C.P->alpha)
+    return fail(CHD_ERR_INVALID_LEVEL, "chd_ct_import: (num_main, num_ter) is not a level");
+  int rc = ct->ct.reserve(np, has_rx != 0, C.P->n);
+  if (rc) return rc;
+  const size_t bytes = static_cast<size_t>(np.total()) * C.P->n * 4;
+  cudaMemcpyKind kind = src_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  cudaMemcpyAsync(ct->ct.bx, bx, bytes, kind, C.stream);
+  cudaMemcpyAsync(ct->ct.ax, ax, bytes, kind, C.stream);
+  if (has_rx) cudaMemcpyAsync(ct->ct.rx, rx, bytes, kind, C.stream);
+  ct->ct.scale = scale;
+  ct->ct.num_slots = num_slots;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(CHD_ERR_CUDA, cudaGetErrorString(e));
+  if (!src_on_device) cudaStreamSynchronize(C.stream);
+  return CHD_OK;
+}
+
+int chd_ct_export(chd_context *ctx, const chd_ciphertext *ct, uint32_t *bx, uint32_t *ax, uint32_t *rx,
+                  int dst_on_device) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(ct);
+  Context &C = *ctx->c;
+  const size_t bytes = static_cast<size_t>(ct->ct.np.total()) * C.P->n * 4;
+  cudaMemcpyKind kind = dst_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  if (bx) cudaMemcpyAsync(bx, ct->ct.bx, bytes, kind, C.stream);
+  if (ax) cudaMemcpyAsync(ax, ct->ct.ax, bytes, kind, C.stream);
+  if (rx && ct->ct.has_rx) cudaMemcpyAsync(rx, ct->ct.rx, bytes, kind, C.stream);
+  cudaError_t e = cudaStreamSynchronize(C.stream);
+  if (e != cudaSuccess) return fail(CHD_ERR_CUDA, cudaGetErrorString(e));
+  return CHD_OK;
+}
+
+int chd_ct_info(const chd_ciphertext *ct, int *num_main, int *num_ter, int *num_aux, int *has_rx, double *scale,
+                int *num_slots) {
+  CHD_NOTNULL(ct);
+  if (num_main) *num_main = ct->ct.np.main;
+  if (num_ter) *num_ter = ct->ct.np.ter;
+  if (num_aux) *num_aux = ct->ct.np.aux;
+  if (has_rx) *has_rx = ct->ct.has_rx;
+  if (scale) *scale = ct->ct.scale;
+  if (num_slots) *num_slots = ct->ct.num_slots;
+  return CHD_OK;
+}
+
+int chd_ct_device_ptrs(const chd_ciphertext *ct, uint32_t **bx, uint32_t **ax, uint32_t **rx) {
+  CHD_NOTNULL(ct);
+  if (bx) *bx = ct->ct.bx;
+  if (ax) *ax = ct->ct.ax;
+  if (rx) *rx = ct->ct.rx;
+  return CHD_OK;
+}
+
+int chd_evk_create(chd_context *ctx, int beta, const uint32_t *bx, const uint32_t *ax, int src_on_device,
+                   chd_evk **out) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(bx);
+  CHD_NOTNULL(ax);
+  CHD_NOTNULL(out);
+  Context &C = *ctx->c;
+  const int need = (C.P->L + C.P->alpha - 1) / C.P->alpha;
+  if (beta < need || beta > 8) return fail(CHD_ERR_KEY, "chd_evk_create: beta must cover all q primes (<= 8)");
+  auto *k = new chd_evk();
+  k->k.beta = beta;
+  k->k.np = NP{C.P->max_main, C.P->max_ter, C.P->alpha};
+  const size_t bytes = static_cast<size_t>(beta) * (C.P->L + C.P->alpha) * C.P->n * 4;
+  if (cudaMalloc(&k->k.bx, bytes) != cudaSuccess || cudaMalloc(&k->k.ax, bytes) != cudaSuccess) {
+    delete k;
+    return fail(CHD_ERR_ALLOC, "chd_evk_create: device allocation failed");
+  }
+  cudaMemcpyKind kind = src_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  cudaMemcpyAsync(k->k.bx, bx, bytes, kind, C.stream);
+  cudaMemcpyAsync(k->k.ax, ax, bytes, kind, C.stream);
+  cudaError_t e = cudaStreamSynchronize(C.stream);
+  if (e != cudaSuccess) {
+    delete k;
+    return fail(CHD_ERR_CUDA, cudaGetErrorString(e));
+  }
+  *out = k;
+  return CHD_OK;
+}
+
+void chd_evk_destroy(chd_evk *evk) { delete evk; }
+
+#define CTX_CT3(name, call)                                                                              \
+  int name(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_ciphertext *b) { \
+    CHD_NOTNULL(ctx);                                                                                  \
+    CHD_NOTNULL(res);                                                                                  \
+    CHD_NOTNULL(a);                                                                                    \
+    CHD_NOTNULL(b);                                                                                    \
+    return ctx->c->call(res->ct, a->ct, b->ct);                                                        \
+  }
+CTX_CT3(chd_add, add)
+CTX_CT3(chd_sub, sub)
+CTX_CT3(chd_mult, mult_tensor)
+#undef CTX_CT3
+
+int chd_neg(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  return ctx->c->neg(res->ct, a->ct);
+}
+
+int chd_mult_const(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *cx,
+                   double const_scale) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  CHD_NOTNULL(cx);
+  return ctx->c->mult_const(res->ct, a->ct, cx, const_scale);
+}
+
+int chd_add_const(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *cx) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  CHD_NOTNULL(cx);
+  return ctx->c->add_const(res->ct, a->ct, cx);
+}
+
+int chd_mult_plain(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *pt_dev,
+                   double pt_scale) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  CHD_NOTNULL(pt_dev);
+  return ctx->c->mult_plain(res->ct, a->ct, pt_dev, pt_scale);
+}
+
+int chd_mult_imaginary_unit(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  return ctx->c->mult_imag_unit(res->ct, a->ct);
+}
+
+int chd_rescale(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  return ctx->c->rescale(res->ct, a->ct);
+}
+
+int chd_relinearize(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *key) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  CHD_NOTNULL(key);
+  return ctx->c->relinearize(res->ct, a->ct, key->k, false);
+}
+
+int chd_relinearize_rescale(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *key) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  CHD_NOTNULL(key);
+  return ctx->c->relinearize(res->ct, a->ct, key->k, true);
+}
+
+int chd_mult_key(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *key) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  CHD_NOTNULL(key);
+  return ctx->c->mult_key(res->ct, a->ct, key->k);
+}
+
+int chd_hmult(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_ciphertext *b,
+              const chd_evk *mult_key, int rescale) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  CHD_NOTNULL(b);
+  CHD_NOTNULL(mult_key);
+  return ctx->c->hmult(res->ct, a->ct, b->ct, mult_key->k, rescale != 0);
+}
+
+int chd_hmult_batch(chd_context *ctx, int count, chd_ciphertext *const *res, const chd_ciphertext *const *a,
+                    const chd_ciphertext *const *b, const chd_evk *mult_key, int rescale) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  CHD_NOTNULL(b);
+  CHD_NOTNULL(mult_key);
+  if (count < 0) return fail(CHD_ERR_INVALID_ARG, "chd_hmult_batch: negative count");
+  std::vector<DeviceCt *> r(count);
+  std::vector<const DeviceCt *> x(count), y(count);
+  for (int i = 0; i < count; i++) {
+    if (!res[i] || !a[i] || !b[i]) return fail(CHD_ERR_INVALID_ARG, "chd_hmult_batch: null ciphertext");
+    r[i] = &res[i]->ct;
+    x[i] = &a[i]->ct;
+    y[i] = &b[i]->ct;
+  }
+  return ctx->c->hmult_batch(count, r.data(), x.data(), y.data(), mult_key->k, rescale != 0);
+}
+
+int chd_hrot(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *rot_key, int rot_dist) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  CHD_NOTNULL(rot_key);
+  return ctx->c->hrot(res->ct, a->ct, rot_key->k, rot_dist);
+}
+
+int chd_hconj(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *conj_key) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  CHD_NOTNULL(conj_key);
+  return ctx->c->hconj(res->ct, a->ct, conj_key->k);
+}
+
+int chd_hrot_add(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_ciphertext *b,
+                 const chd_evk *rot_key, int rot_dist) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  CHD_NOTNULL(b);
+  CHD_NOTNULL(rot_key);
+  return ctx->c->hrot_add(res->ct, a->ct, b->ct, rot_key->k, rot_dist);
+}
+
+int chd_hoisted_rotate(chd_context *ctx, const chd_ciphertext *a, int count, const int *rot_dists,
+                       const chd_evk *const *rot_keys, chd_ciphertext *const *out) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(a);
+  CHD_NOTNULL(rot_dists);
+  CHD_NOTNULL(rot_keys);
+  CHD_NOTNULL(out);
+  if (count <= 0) return fail(CHD_ERR_INVALID_ARG, "chd_hoisted_rotate: count must be positive");
+  std::vector<const DeviceEvk *> k(count);
+  std::vector<DeviceCt *> o(count);
+  for (int i = 0; i < count; i++) {
+    if (!rot_keys[i] || !out[i]) return fail(CHD_ERR_INVALID_ARG, "chd_hoisted_rotate: null key or output");
+    k[i] = &rot_keys[i]->k;
+    o[i] = &out[i]->ct;
+  }
+  return ctx->c->hoisted_rotate(a->ct, count, rot_dists, k.data(), o.data());
+}
+
+int chd_moddown(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  return ctx->c->moddown_ct(res->ct, a->ct);
+}
+
+int chd_ntt(chd_context *ctx, int num_main, int num_ter, int num_aux, uint32_t *data_dev, int mont, int count) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(data_dev);
+  NP np{num_main, num_ter, num_aux};
+  const Params &P = *ctx->c->P;
+  if (num_main < 0 || num_ter < 0 || num_aux < 0 || num_main > P.max_main || num_ter > P.max_ter ||
+      num_aux > P.alpha || count < 1)
+    return fail(CHD_ERR_INVALID_ARG, "chd_ntt: invalid prime counts");
+  return ctx->c->ntt(np, data_dev, mont != 0, count, static_cast<size_t>(np.total()) * P.n);
+}
+
+int chd_intt(chd_context *ctx, int num_main, int num_ter, int num_aux, uint32_t *data_dev, int mont, int count) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(data_dev);
+  NP np{num_main, num_ter, num_aux};
+  const Params &P = *ctx->c->P;
+  if (num_main < 0 || num_ter < 0 || num_aux < 0 || num_main > P.max_main || num_ter > P.max_ter ||
+      num_aux > P.alpha || count < 1)
+    return fail(CHD_ERR_INVALID_ARG, "chd_intt: invalid prime counts");
+  return ctx->c->intt(np, data_dev, mont != 0, count, static_cast<size_t>(np.total()) * P.n);
+}
+
+int chd_modup_raw(chd_context *ctx, int level, const uint32_t *src_dev, uint32_t *dst_dev) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(src_dev);
+  CHD_NOTNULL(dst_dev);
+  Context &C = *ctx->c;
+  if (level < -1 || level > C.P->max_level) return fail(CHD_ERR_INVALID_LEVEL, "chd_modup_raw: invalid level");
+  const LevelMS &m = C.lms(level);
+  const size_t stride = static_cast<size_t>(m.num_q + m.num_aux) * C.P->n;
+  std::vector<uint32_t *> d(m.beta);
+  for (int i = 0; i < m.beta; i++) d[i] = dst_dev + i * stride;
+  return C.modup(level, src_dev, d.data());
+}
+
+int chd_moddown_raw(chd_context *ctx, int level, int type, const uint32_t *src_dev, uint32_t *dst_dev, int npoly) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(src_dev);
+  CHD_NOTNULL(dst_dev);
+  Context &C = *ctx->c;
+  if (level < -1 || level > C.P->max_level) return fail(CHD_ERR_INVALID_LEVEL, "chd_moddown_raw: invalid level");
+  if (type < 0 || type > 2 || npoly < 1) return fail(CHD_ERR_INVALID_ARG, "chd_moddown_raw: bad type or npoly");
+  if (type != CHD_MODDOWN && level < 1) return fail(CHD_ERR_INVALID_LEVEL, "chd_moddown_raw: cannot rescale");
+  const LevelMS &m = C.lms(level);
+  const int nsa = type == CHD_RESCALE ? 0 : m.num_aux;
+  NP ns = C.P->level_np(level, nsa);
+  NP nd = C.P->level_np(type == CHD_MODDOWN ? level : level - 1, 0);
+  std::vector<const uint32_t *> s(npoly);
+  std::vector<uint32_t *> d(npoly);
+  for (int p = 0; p < npoly; p++) {
+    s[p] = src_dev + static_cast<size_t>(p) * ns.total() * C.P->n;
+    d[p] = dst_dev + static_cast<size_t>(p) * nd.total() * C.P->n;
+  }
+  Context::MDType t = type == CHD_MODDOWN ? Context::MDType::kModDown
+                      : type == CHD_RESCALE ? Context::MDType::kRescale : Context::MDType::kModDownRescale;
+  return C.moddown(level, t, s.data(), d.data(), npoly);
+}
+
+int chd_bconv_raw(chd_context *ctx, const int32_t *xt_dev, const int *src_gidx, int K, const int *dst_gidx, int M,
+                  uint32_t *out_dev) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(xt_dev);
+  CHD_NOTNULL(src_gidx);
+  CHD_NOTNULL(dst_gidx);
+  CHD_NOTNULL(out_dev);
+  Context &C = *ctx->c;
+  const int np_all = C.P->L + C.P->alpha;
+  if (K < 1 || K > 16 || M < 1 || M > 64) return fail(CHD_ERR_UNSUPPORTED, "chd_bconv_raw: K in [1,16], M in [1,64]");
+  for (int i = 0; i < K; i++)
+    if (src_gidx[i] < 0 || src_gidx[i] >= np_all) return fail(CHD_ERR_INVALID_ARG, "chd_bconv_raw: bad src index");
+  for (int i = 0; i < M; i++)
+    if (dst_gidx[i] < 0 || dst_gidx[i] >= np_all) return fail(CHD_ERR_INVALID_ARG, "chd_bconv_raw: bad dst index");
+  std::vector<int32_t> t(static_cast<size_t>(M) * K);
+  for (int m = 0; m < M; m++) {
+    uint32_t p = C.P->primes[dst_gidx[m]];
+    for (int k = 0; k < K; k++) {
+      uint32_t acc = 1;
+      for (int j = 0; j < K; j++)
+        if (j != k) acc = prime::mul_mod(acc, C.P->primes[src_gidx[j]], p);
+      t[m * K + k] = prime::centre(prime::to_mont(prime::to_mont(acc, p), p), p);
+    }
+  }
+  int32_t *dt = nullptr;
+  if (cudaMalloc(&dt, t.size() * 4) != cudaSuccess) return fail(CHD_ERR_ALLOC, "chd_bconv_raw: allocation failed");
+  cudaMemcpyAsync(dt, t.data(), t.size() * 4, cudaMemcpyHostToDevice, C.stream);
+  int rc = C.bconv(xt_dev, K, dt, dst_gidx, M, out_dev);
+  cudaStreamSynchronize(C.stream);
+  cudaFree(dt);
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,1549 @@
+// Host orchestration of the CKKS evaluation core.
+//
+// The level model, ModSwitch constants and evaluator compositions follow the
+// reference (scale-snu/cheddar-fhe): Parameter.cu:20-376, ModSwitch.cu:175-684,
+// Context.cpp:62-949.  Everything that touches residues runs in the CUDA
+// kernels of ntt.cu / elem.cu; this file only computes constants on the host
+// and builds launch descriptors.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+
+#include "host.h"
+
+namespace chd {
+
+// ---------------------------------------------------------------- errors
+namespace {
+thread_local std::string g_error;
+}
+void set_error(const std::string &msg) { g_error = msg; }
+const char *last_error() { return g_error.c_str(); }
+
+#define CHD_CHECK(cond, code, msg) \
+  do {                             \
+    if (!(cond)) {                 \
+      set_error(msg);              \
+      return code;                 \
+    }                              \
+  } while (0)
+#define CHD_TRY(expr)            \
+  do {                           \
+    Status _s = (expr);          \
+    if (_s != kOk) return _s;    \
+  } while (0)
+
+// ---------------------------------------------------------- prime utilities
+namespace prime {
+uint32_t mul_mod(uint32_t a, uint32_t b, uint32_t q) {
+  return static_cast<uint32_t>((static_cast<uint64_t>(a) * b) % q);
+}
+uint32_t inv_mod(uint32_t a, uint32_t q) {
+  int64_t t = 0, nt = 1, r = q, nr = a % q;
+  while (nr) {
+    int64_t k = r / nr;
+    int64_t tmp = t - k * nt;
+    t = nt;
+    nt = tmp;
+    tmp = r - k * nr;
+    r = nr;
+    nr = tmp;
+  }
+  if (t < 0) t += q;
+  return static_cast<uint32_t>(t);
+}
+uint32_t pow_mod(uint32_t a, int64_t e, uint32_t q) {
+  a %= q;
+  if (e < 0) {
+    a = inv_mod(a, q);
+    e = -e;
+  }
+  uint64_t r = 1, b = a;
+  while (e) {
+    if (e & 1) r = (r * b) % q;
+    b = (b * b) % q;
+    e >>= 1;
+  }
+  return static_cast<uint32_t>(r);
+}
+uint32_t smallest_generator(uint32_t q) {
+  // smallest r >= 2 whose order is q-1: r^((q-1)/f) != 1 for every prime
+  // factor f of q-1 (the choice of generator fixes psi, which fixes the
+  // evaluation order; it matches include/common/PrimeUtils.h:135-170)
+  uint32_t phi = q - 1, t = phi;
+  std::vector<uint32_t> f;
+  for (uint32_t i = 2; static_cast<uint64_t>(i) * i <= t; i++) {
+    if (t % i == 0) {
+      f.push_back(i);
+      while (t % i == 0) t /= i;
+    }
+  }
+  if (t > 1) f.push_back(t);
+  for (uint32_t r = 2; r < q; r++) {
+    bool ok = true;
+    for (uint32_t x : f)
+      if (pow_mod(r, phi / x, q) == 1) {
+        ok = false;
+        break;
+      }
+    if (ok) return r;
+  }
+  return 0;
+}
+uint32_t primitive_root(uint32_t m, uint32_t q) { return pow_mod(smallest_generator(q), (q - 1) / m, q); }
+int32_t inv_mod_word(uint32_t q) {
+  uint32_t x = q;
+  for (int i = 0; i < 5; i++) x *= 2u - q * x;
+  return static_cast<int32_t>(x);
+}
+uint32_t to_mont(uint32_t a, uint32_t q) { return static_cast<uint32_t>((static_cast<uint64_t>(a) << 32) % q); }
+int32_t centre(uint32_t a, uint32_t q) {
+  return a > (q >> 1) ? static_cast<int32_t>(a) - static_cast<int32_t>(q) : static_cast<int32_t>(a);
+}
+}  // namespace prime
+
+static unsigned brev_host(unsigned x, int bits) {
+  unsigned r = 0;
+  for (int i = 0; i < bits; i++) r |= ((x >> i) & 1u) << (bits - 1 - i);
+  return r;
+}
+
+// --------------------------------------------------------------- JSON
+namespace {
+struct JVal {
+  enum T { kNull, kBool, kNum, kStr, kArr, kObj } t = kNull;
+  double num = 0;
+  bool b = false;
+  std::string s;
+  std::vector<JVal> arr;
+  std::vector<std::pair<std::string, JVal>> obj;
+  const JVal *get(const std::string &k) const {
+    for (auto &kv : obj)
+      if (kv.first == k) return &kv.second;
+    return nullptr;
+  }
+};
+struct JParser {
+  const std::string &s;
+  size_t i = 0;
+  std::string err;
+  explicit JParser(const std::string &x) : s(x) {}
+  void ws() {
+    while (i < s.size() && (s[i] == ' ' || s[i] == '\n' || s[i] == '\t' || s[i] == '\r')) i++;
+  }
+  bool val(JVal &v) {
+    ws();
+    if (i >= s.size()) return fail("unexpected end");
+    char c = s[i];
+    if (c == '{') {
+      v.t = JVal::kObj;
+      i++;
+      ws();
+      if (i < s.size() && s[i] == '}') {
+        i++;
+        return true;
+      }
+      while (true) {
+        ws();
+        JVal k;
+        if (!str(k)) return false;
+        ws();
+        if (i >= s.size() || s[i] != ':') return fail("expected ':'");
+        i++;
+        JVal x;
+        if (!val(x)) return false;
+        v.obj.emplace_back(k.s, std::move(x));
+        ws();
+        if (i < s.size() && s[i] == ',') {
+          i++;
+          continue;
+        }
+        if (i < s.size() && s[i] == '}') {
+          i++;
+          return true;
+        }
+        return fail("expected ',' or '}'");
+      }
+    }
+    if (c == '[') {
+      v.t = JVal::kArr;
+      i++;
+      ws();
+      if (i < s.size() && s[i] == ']') {
+        i++;
+        return true;
+      }
+      while (true) {
+        JVal x;
+        if (!val(x)) return false;
+        v.arr.push_back(std::move(x));
+        ws();
+        if (i < s.size() && s[i] == ',') {
+          i++;
+          continue;
+        }
+        if (i < s.size() && s[i] == ']') {
+          i++;
+          return true;
+        }
+        return fail("expected ',' or ']'");
+      }
+    }
+    if (c == '"') return str(v);
+    if (s.compare(i, 4, "true") == 0) {
+      v.t = JVal::kBool;
+      v.b = true;
+      i += 4;
+      return true;
+    }
+    if (s.compare(i, 5, "false") == 0) {
+      v.t = JVal::kBool;
+      i += 5;
+      return true;
+    }
+    if (s.compare(i, 4, "null") == 0) {
+      i += 4;
+      return true;
+    }
+    size_t j = i;
+    while (j < s.size() && (isdigit(static_cast<unsigned char>(s[j])) || s[j] == '-' || s[j] == '+' ||
+                            s[j] == '.' || s[j] == 'e' || s[j] == 'E'))
+      j++;
+    if (j == i) return fail("unexpected character");
+    v.t = JVal::kNum;
+    v.num = std::strtod(s.substr(i, j - i).c_str(), nullptr);
+    i = j;
+    return true;
+  }
+  bool str(JVal &v) {
+    if (i >= s.size() || s[i] != '"') return fail("expected string");
+    i++;
+    v.t = JVal::kStr;
+    while (i < s.size() && s[i] != '"') {
+      if (s[i] == '\\' && i + 1 < s.size()) i++;
+      v.s.push_back(s[i++]);
+    }
+    if (i >= s.size()) return fail("unterminated string");
+    i++;
+    return true;
+  }
+  bool fail(const char *m) {
+    err = std::string(m) + " at offset " + std::to_string(i);
+    return false;
+  }
+};
+}  // namespace
+
+bool parse_param_json(const std::string &text, ParamSpec *out, std::string *err) {
+  // schema of unittest/Testbed.h:95-221 of the reference
+  JParser p(text);
+  JVal root;
+  if (!p.val(root) || root.t != JVal::kObj) {
+    *err = "JSON parse error: " + (p.err.empty() ? std::string("not an object") : p.err);
+    return false;
+  }
+  auto num = [&](const char *k, double *v, bool req) -> bool {
+    const JVal *x = root.get(k);
+    if (!x) {
+      if (req) *err = std::string("Missing ") + k + " in JSON";
+      return !req;
+    }
+    if (x->t != JVal::kNum) {
+      *err = std::string(k) + " should be a number";
+      return false;
+    }
+    *v = x->num;
+    return true;
+  };
+  auto primes = [&](const char *k, std::vector<uint32_t> *v, bool req) -> bool {
+    const JVal *x = root.get(k);
+    if (!x) {
+      if (req) *err = std::string("Missing ") + k + " in JSON";
+      return !req;
+    }
+    if (x->t != JVal::kArr) {
+      *err = std::string(k) + " should be an array";
+      return false;
+    }
+    for (auto &e : x->arr) {
+      if (e.t != JVal::kNum) {
+        *err = std::string(k) + " should be an array of integers";
+        return false;
+      }
+      v->push_back(static_cast<uint32_t>(e.num));
+    }
+    return true;
+  };
+  double d;
+  ParamSpec s;
+  if (!num("log_degree", &d, true)) return false;
+  s.log_degree = static_cast<int>(d);
+  if (!num("log_default_scale", &d, true)) return false;
+  s.base_scale = std::ldexp(1.0, static_cast<int>(d));
+  if (!num("default_encryption_level", &d, true)) return false;
+  s.default_encryption_level = static_cast<int>(d);
+  if (!primes("main_primes", &s.main_primes, true)) return false;
+  if (!primes("terminal_primes", &s.ter_primes, false)) return false;
+  if (!primes("auxiliary_primes", &s.aux_primes, true)) return false;
+  const JVal *lc = root.get("level_config");
+  if (!lc || lc->t != JVal::kArr) {
+    *err = "Missing level_config in JSON";
+    return false;
+  }
+  for (auto &e : lc->arr) {
+    if (e.t != JVal::kArr || e.arr.size() != 2) {
+      *err = "level_config should be an array of pairs";
+      return false;
+    }
+    s.level_config.emplace_back(static_cast<int>(e.arr[0].num), static_cast<int>(e.arr[1].num));
+  }
+  if (const JVal *ab = root.get("additional_base")) {
+    if (ab->t != JVal::kArr || ab->arr.size() != 2) {
+      *err = "additional_base should be an array of pairs";
+      return false;
+    }
+    s.additional_base = {static_cast<int>(ab->arr[0].num), static_cast<int>(ab->arr[1].num)};
+  }
+  if (num("dense_hamming_weight", &d, false) && root.get("dense_hamming_weight")) s.dense_hw = static_cast<int>(d);
+  if (num("sparse_hamming_weight", &d, false) && root.get("sparse_hamming_weight")) s.sparse_hw = static_cast<int>(d);
+  if (const JVal *b = root.get("boot")) s.boot = b->t == JVal::kBool && b->b;
+  if (num("num_cts_levels", &d, false) && root.get("num_cts_levels")) s.num_cts_levels = static_cast<int>(d);
+  if (num("num_stc_levels", &d, false) && root.get("num_stc_levels")) s.num_stc_levels = static_cast<int>(d);
+  *out = s;
+  return true;
+}
+
+// -------------------------------------------------------------- Params
+static bool np_less(std::pair<int, int> a, std::pair<int, int> b) {
+  // Parameter.cu:10-15
+  int at = a.first + a.second, bt = b.first + b.second;
+  return at < bt || (at == bt && a.first < b.first);
+}
+
+std::unique_ptr<Params> Params::create(const ParamSpec &spec, std::string *err) {
+  // validation of Parameter.cu:36-84
+  if (spec.log_degree < 12 || spec.log_degree > 16) {
+    *err = "log_degree must be in [12, 16]";
+    return nullptr;
+  }
+  if (spec.main_primes.empty() || spec.aux_primes.empty() || spec.level_config.empty()) {
+    *err = "main_primes, auxiliary_primes and level_config must be non-empty";
+    return nullptr;
+  }
+  const uint32_t two_n = 2u << spec.log_degree;
+  for (auto *lst : {&spec.main_primes, &spec.aux_primes, &spec.ter_primes})
+    for (uint32_t p : *lst) {
+      if (p >= (1u << 31)) {
+        *err = "Max prime is too large for the word size";
+        return nullptr;
+      }
+      if (p % two_n != 1) {
+        *err = "Prime is not NTT-friendly";
+        return nullptr;
+      }
+    }
+  const int nm = static_cast<int>(spec.main_primes.size()), nt = static_cast<int>(spec.ter_primes.size());
+  const int na = static_cast<int>(spec.aux_primes.size());
+  if (nm + nt + na > 250) {
+    *err = "too many primes";
+    return nullptr;
+  }
+  std::pair<int, int> prev{0, 0};
+  for (size_t i = 0; i + 1 < spec.level_config.size(); i++) {
+    auto c = spec.level_config[i];
+    if (c.first < 0 || c.first > nm || c.second < 0 || c.second > nt || !np_less(prev, c)) {
+      *err = "Invalid level configuration at level " + std::to_string(i);
+      return nullptr;
+    }
+    prev = c;
+  }
+  if (spec.level_config.back() != std::make_pair(nm, nt)) {
+    *err = "Invalid number of primes at the last level";
+    return nullptr;
+  }
+  if (spec.default_encryption_level < 0 ||
+      spec.default_encryption_level >= static_cast<int>(spec.level_config.size())) {
+    *err = "Invalid default encryption level";
+    return nullptr;
+  }
+  auto P = std::make_unique<Params>();
+  P->spec = spec;
+  P->log_n = spec.log_degree;
+  P->n = 1 << spec.log_degree;
+  P->max_ter = nt;
+  P->max_main = nm;
+  P->L = nm + nt;
+  P->alpha = na;
+  P->max_level = static_cast<int>(spec.level_config.size()) - 1;
+  P->short_np.main = spec.level_config[0].first - spec.additional_base.first;
+  P->short_np.ter = spec.level_config[0].second - spec.additional_base.second;
+  P->short_np.aux = P->short_np.main + P->short_np.ter;
+  if (P->short_np.main < 0 || P->short_np.ter < 0 || P->short_np.aux > na) {
+    *err = "Invalid additional base configuration";
+    return nullptr;
+  }
+  for (int i = nt - 1; i >= 0; i--) P->primes.push_back(spec.ter_primes[i]);
+  for (uint32_t p : spec.main_primes) P->primes.push_back(p);
+  for (uint32_t p : spec.aux_primes) P->primes.push_back(p);
+  for (uint32_t p : P->primes) P->qinv.push_back(prime::inv_mod_word(p));
+  P->galois.assign(P->n / 2 + 1, 1);
+  for (int i = 1; i < P->n / 2; i++) P->galois[i] = static_cast<int>((static_cast<int64_t>(P->galois[i - 1]) * 5) % (2 * P->n));
+  // scales, Parameter.cu:145-190
+  P->rescale_prod.assign(P->max_level + 1, 0.0);
+  P->scale.assign(spec.default_encryption_level + 1, 0.0);
+  P->scale[0] = spec.base_scale;
+  double ns = spec.base_scale;
+  for (int i = 1; i <= P->max_level; i++) {
+    NP up = P->level_np(i), lo = P->level_np(i - 1);
+    int td = up.ter - lo.ter, md = up.main - lo.main;
+    double num = 1.0, den = 1.0;
+    if (td >= 0)
+      for (int j = 0; j < td; j++) num *= spec.ter_primes[lo.ter + j];
+    else
+      for (int j = 0; j < -td; j++) den *= spec.ter_primes[up.ter + j];
+    if (md >= 0)
+      for (int j = 0; j < md; j++) num *= spec.main_primes[lo.main + j];
+    else
+      for (int j = 0; j < -md; j++) den *= spec.main_primes[up.main + j];
+    P->rescale_prod[i] = num / den;
+    if (i <= spec.default_encryption_level) {
+      ns = std::sqrt(ns * P->rescale_prod[i]);
+      P->scale[i] = ns;
+    }
+  }
+  return P;
+}
+
+NP Params::level_np(int level, int num_aux) const {
+  if (level == -1) return NP{short_np.main, short_np.ter, num_aux};
+  auto c = spec.level_config.at(level);
+  return NP{c.first, c.second, num_aux};
+}
+
+int Params::np_to_level(const NP &np) const {
+  for (int l = 0; l <= max_level; l++)
+    if (spec.level_config[l].first == np.main && spec.level_config[l].second == np.ter) return l;
+  if (np.main == short_np.main && np.ter == short_np.ter) return -1;
+  return -2;
+}
+
+void Params::gidx(const NP &np, int *out) const {
+  int k = 0;
+  for (int i = 0; i < np.q(); i++) out[k++] = max_ter - np.ter + i;
+  for (int a = 0; a < np.aux; a++) out[k++] = L + a;
+}
+
+int Params::sse_num_aux() const {
+  return spec.level_config[0].first + spec.level_config[0].second - spec.additional_base.first -
+         spec.additional_base.second;
+}
+
+uint32_t Params::galois_of(int amount) const {
+  if (amount == -1) return 2u * n - 1;
+  return static_cast<uint32_t>(galois.at(amount));
+}
+
+// -------------------------------------------------------------- devices
+DeviceCt::~DeviceCt() {
+  if (owned) {
+    cudaFree(bx);
+    cudaFree(ax);
+    cudaFree(rx);
+  }
+}
+
+Status DeviceCt::reserve(const NP &want, bool want_rx, int n) {
+  size_t words = static_cast<size_t>(want.total()) * n;
+  if (!owned) {
+    CHD_CHECK(words <= cap_words && (!want_rx || rx), kErrShape, "wrapped ciphertext buffer too small");
+  } else if (words > cap_words || (want_rx && !rx)) {
+    size_t cap = std::max(words, cap_words);
+    uint32_t *nb = nullptr, *na = nullptr, *nr = nullptr;
+    if (cudaMalloc(&nb, cap * 4) != cudaSuccess || cudaMalloc(&na, cap * 4) != cudaSuccess ||
+        (want_rx && cudaMalloc(&nr, cap * 4) != cudaSuccess)) {
+      cudaFree(nb);
+      cudaFree(na);
+      set_error("device allocation failed");
+      return kErrAlloc;
+    }
+    // reserve is only called before the result is written; old contents are
+    // not needed.  The buffers are freed after the stream drains.
+    cudaDeviceSynchronize();
+    cudaFree(bx);
+    cudaFree(ax);
+    cudaFree(rx);
+    bx = nb;
+    ax = na;
+    rx = nr;
+    cap_words = cap;
+  }
+  np = want;
+  has_rx = want_rx;
+  return kOk;
+}
+
+DeviceEvk::~DeviceEvk() {
+  if (owned) {
+    cudaFree(bx);
+    cudaFree(ax);
+  }
+}
+
+Arena::~Arena() {
+  for (auto &c : chunks_) cudaFree(c.p);
+}
+
+void *Arena::alloc(size_t bytes) {
+  bytes = (bytes + 255) & ~static_cast<size_t>(255);
+  // find the chunk holding top_
+  for (auto &c : chunks_) {
+    if (top_ >= c.start && top_ < c.start + c.size) {
+      if (top_ + bytes <= c.start + c.size) {
+        void *p = c.p + (top_ - c.start);
+        top_ += bytes;
+        return p;
+      }
+      break;
+    }
+  }
+  // next chunk that fits entirely, starting after top_
+  for (auto &c : chunks_) {
+    if (c.start >= top_ && c.size >= bytes) {
+      top_ = c.start + bytes;
+      return c.p;
+    }
+  }
+  size_t sz = std::max(bytes, total_ ? total_ : static_cast<size_t>(64) << 20);
+  char *p = nullptr;
+  if (cudaMalloc(&p, sz) != cudaSuccess) return nullptr;
+  chunks_.push_back(Chunk{p, sz, total_});
+  top_ = total_ + bytes;
+  total_ += sz;
+  return p;
+}
+
+void Arena::release(size_t m) { top_ = m; }
+
+struct ArenaScope {
+  Arena &a;
+  size_t m;
+  explicit ArenaScope(Arena &x) : a(x), m(x.mark()) {}
+  ~ArenaScope() { a.release(m); }
+};
+
+// -------------------------------------------------------------- Context
+std::unique_ptr<Context> Context::create(const ParamSpec &spec, int device, std::string *err) {
+  auto c = std::unique_ptr<Context>(new Context());
+  if (c->init(spec, device, err) != kOk) return nullptr;
+  return c;
+}
+
+Context::~Context() {
+  if (stream) cudaStreamSynchronize(stream);
+  for (auto &m : ms) {
+    for (auto *p : m.d_mod_up2) cudaFree(p);
+    cudaFree(m.d_mod_down2);
+    cudaFree(m.d_rs2);
+    cudaFree(m.d_mdr2);
+  }
+  cudaFree(d_primes);
+  cudaFree(d_qinv);
+  cudaFree(d_tw);
+  cudaFree(d_itw);
+  if (own_stream && stream) cudaStreamDestroy(stream);
+}
+
+Status Context::check_cuda(const char *where) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_error(std::string(where) + ": " + cudaGetErrorString(e));
+    return kErrCuda;
+  }
+  return kOk;
+}
+
+namespace {
+// ModSwitch constant tables, ModSwitch.cu:320-370
+void ms_consts(uint32_t n, const std::vector<uint32_t> &src, const std::vector<uint32_t> &dst, int rs, int re,
+               std::vector<uint32_t> *c1, std::vector<int32_t> *c2) {
+  const size_t sl = src.size(), dl = dst.size();
+  c1->assign(sl, 1);
+  c2->assign(sl * dl, 0);
+  for (size_t i = 0; i < sl; i++) {
+    uint32_t m = src[i], v = 1;
+    for (size_t j = 0; j < sl; j++)
+      if (j != i) v = prime::mul_mod(v, src[j], m);
+    v = prime::inv_mod(prime::mul_mod(v, n, m), m);
+    for (int j = rs; j < re; j++) v = prime::mul_mod(v, dst[j], m);
+    (*c1)[i] = v;  // plain form: INTT output is x*R, the Montgomery product drops R
+  }
+  for (size_t mi = 0; mi < dl; mi++) {
+    uint32_t p = dst[mi];
+    for (size_t i = 0; i < sl; i++) {
+      uint32_t acc = 1;
+      for (size_t j = 0; j < sl; j++)
+        if (j != i) acc = prime::mul_mod(acc, src[j], p);
+      acc = prime::to_mont(prime::to_mont(acc, p), p);
+      (*c2)[mi * sl + i] = prime::centre(acc, p);
+    }
+  }
+}
+// ModDown epilogue constants, ModSwitch.cu:372-411
+void epi_consts(const std::vector<uint32_t> &src, const std::vector<uint32_t> &dst, int rs, int re,
+                std::vector<uint32_t> *inv, std::vector<uint32_t> *pad) {
+  const size_t dl = dst.size();
+  inv->assign(dl, 0);
+  for (size_t i = 0; i < dl; i++) {
+    uint32_t p = dst[i], v = 1;
+    for (uint32_t s : src) v = prime::mul_mod(v, s, p);
+    (*inv)[i] = prime::to_mont(prime::inv_mod(v, p), p);
+  }
+  if (!pad) return;
+  const int rl = re - rs;
+  pad->assign(dl - rl, 0);
+  for (int i = 0; i < static_cast<int>(dl) - rl; i++) {
+    int pi = i >= rs ? i + rl : i;
+    uint32_t p = dst[pi], v = 1;
+    for (int j = rs; j < re; j++) v = prime::mul_mod(v, dst[j], p);
+    (*pad)[i] = prime::to_mont(v, p);
+  }
+}
+int32_t *upload_i32(const std::vector<int32_t> &v) {
+  int32_t *p = nullptr;
+  if (v.empty()) return nullptr;
+  if (cudaMalloc(&p, v.size() * 4) != cudaSuccess) return nullptr;
+  cudaMemcpy(p, v.data(), v.size() * 4, cudaMemcpyHostToDevice);
+  return p;
+}
+}  // namespace
+
+Status Context::init(const ParamSpec &spec, int dev, std::string *err) {
+  P = Params::create(spec, err);
+  if (!P) return kErrInvalidArg;
+  device = dev;
+  if (cudaSetDevice(dev) != cudaSuccess) {
+    *err = "cudaSetDevice failed";
+    return kErrCuda;
+  }
+  if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess) {
+    *err = "stream creation failed";
+    return kErrCuda;
+  }
+  own_stream = true;
+  const int n = P->n, np_all = P->L + P->alpha;
+  // twiddles, NTT.cu:1233-1299: psi_rev[j] = psi^brev(j) in Montgomery form
+  std::vector<uint32_t> tw(static_cast<size_t>(np_all) * n), itw(tw.size());
+  n_inv.resize(np_all);
+  n_inv_mont.resize(np_all);
+  mont_conv.resize(np_all);
+  imag_unit.resize(np_all);
+  std::vector<uint32_t> pw(n), pwi(n);
+  for (int g = 0; g < np_all; g++) {
+    uint32_t q = P->primes[g];
+    uint32_t psi = prime::primitive_root(2u * n, q), psi_inv = prime::inv_mod(psi, q);
+    n_inv[g] = prime::inv_mod(static_cast<uint32_t>(n), q);
+    n_inv_mont[g] = prime::to_mont(n_inv[g], q);
+    mont_conv[g] = prime::to_mont(prime::to_mont(1, q), q);
+    pw[0] = pwi[0] = 1;
+    for (int j = 1; j < n; j++) {
+      pw[j] = prime::mul_mod(pw[j - 1], psi, q);
+      pwi[j] = prime::mul_mod(pwi[j - 1], psi_inv, q);
+    }
+    for (int j = 0; j < n; j++) {
+      unsigned r = brev_host(j, P->log_n);
+      tw[static_cast<size_t>(g) * n + j] = prime::to_mont(pw[r], q);
+      itw[static_cast<size_t>(g) * n + j] = prime::to_mont(pwi[r], q);
+    }
+    imag_unit[g] = tw[static_cast<size_t>(g) * n + 1];  // psi^(N/2), Montgomery
+  }
+  if (cudaMalloc(&d_primes, np_all * 4) != cudaSuccess || cudaMalloc(&d_qinv, np_all * 4) != cudaSuccess ||
+      cudaMalloc(&d_tw, tw.size() * 4) != cudaSuccess || cudaMalloc(&d_itw, itw.size() * 4) != cudaSuccess) {
+    *err = "device allocation failed";
+    return kErrAlloc;
+  }
+  cudaMemcpy(d_primes, P->primes.data(), np_all * 4, cudaMemcpyHostToDevice);
+  cudaMemcpy(d_qinv, P->qinv.data(), np_all * 4, cudaMemcpyHostToDevice);
+  cudaMemcpy(d_tw, tw.data(), tw.size() * 4, cudaMemcpyHostToDevice);
+  cudaMemcpy(d_itw, itw.data(), itw.size() * 4, cudaMemcpyHostToDevice);
+  // P mod q_i (Montgomery), Context.cpp:78-90
+  p_prod.resize(P->L);
+  for (int i = 0; i < P->L; i++) {
+    uint32_t q = P->primes[i], v = 1;
+    for (int a = 0; a < P->alpha; a++) v = prime::mul_mod(v, P->primes[P->L + a], q);
+    p_prod[i] = prime::to_mont(v, q);
+  }
+  // per-level ModSwitch constants, ModSwitch.cu:175-318
+  ms.resize(P->max_level + 2);
+  for (int level = -1; level <= P->max_level; level++) {
+    LevelMS &m = ms[level + 1];
+    m.level = level;
+    m.num_aux = level == -1 ? P->sse_num_aux() : P->alpha;
+    NP np = P->level_np(level, m.num_aux);
+    const int nq = np.q(), tot = np.total();
+    m.num_q = nq;
+    m.beta = level == -1 ? 1 : (np.main + P->max_ter + m.num_aux - 1) / m.num_aux;
+    std::vector<int> g(tot);
+    P->gidx(np, g.data());
+    std::vector<uint32_t> lp(tot);
+    for (int i = 0; i < tot; i++) lp[i] = P->primes[g[i]];
+    const int padded = level == -1 ? nq : np.main + P->max_ter;
+    const int npad = padded - nq;
+    m.mod_up1.assign(nq, 0);
+    m.dig_s.assign(m.beta, 0);
+    m.dig_e.assign(m.beta, 0);
+    m.d_mod_up2.assign(m.beta, nullptr);
+    for (int i = 0; i < m.beta; i++) {
+      int s = i * m.num_aux, e = std::min((i + 1) * m.num_aux, padded);
+      if (e <= npad) continue;
+      s = std::max(0, s - npad);
+      e -= npad;
+      m.dig_s[i] = s;
+      m.dig_e[i] = e;
+      std::vector<uint32_t> src(lp.begin() + s, lp.begin() + e), dst(lp.begin(), lp.begin() + s);
+      dst.insert(dst.end(), lp.begin() + e, lp.end());
+      std::vector<uint32_t> c1;
+      std::vector<int32_t> c2;
+      ms_consts(n, src, dst, 0, 0, &c1, &c2);
+      std::copy(c1.begin(), c1.end(), m.mod_up1.begin() + s);
+      m.d_mod_up2[i] = upload_i32(c2);
+    }
+    std::vector<uint32_t> qp(lp.begin(), lp.begin() + nq), pp(lp.begin() + nq, lp.end());
+    std::vector<int32_t> c2;
+    ms_consts(n, pp, qp, 0, 0, &m.mod_down1, &c2);
+    m.d_mod_down2 = upload_i32(c2);
+    epi_consts(pp, qp, 0, 0, &m.inv_p_prod, nullptr);
+    if (level <= 0) continue;
+    NP nn = P->level_np(level - 1, m.num_aux);
+    std::vector<int> gn(nn.total());
+    P->gidx(nn, gn.data());
+    std::vector<uint32_t> next(nn.q());
+    for (int i = 0; i < nn.q(); i++) next[i] = P->primes[gn[i]];
+    const int nnq = nn.q();
+    const int md = np.main - nn.main, td = np.ter - nn.ter;
+    std::vector<uint32_t> rs_src;
+    if (td > 0) {
+      if (md > 0) continue;
+      rs_src.assign(lp.begin(), lp.begin() + td);
+      m.pad_start = 0;
+      m.pad_end = nq - td;
+      m.restore_start = nnq + md;
+      m.restore_end = nnq;
+    } else if (md > 0) {
+      if (td > 0) continue;
+      rs_src.assign(lp.begin() + nq - md, lp.begin() + nq);
+      m.pad_start = -td;
+      m.pad_end = nq - md - td;
+      m.restore_start = 0;
+      m.restore_end = -td;
+    } else {
+      continue;
+    }
+    m.has_rescale = true;
+    std::vector<uint32_t> mdr_src = rs_src;
+    mdr_src.insert(mdr_src.end(), pp.begin(), pp.end());
+    m.rs_src_len = static_cast<int>(rs_src.size());
+    m.mdr_src_len = static_cast<int>(mdr_src.size());
+    m.rs_dst_len = nnq;
+    ms_consts(n, rs_src, next, m.restore_start, m.restore_end, &m.rs1, &c2);
+    m.d_rs2 = upload_i32(c2);
+    epi_consts(rs_src, next, m.restore_start, m.restore_end, &m.rs_inv, &m.rs_pad);
+    ms_consts(n, mdr_src, next, m.restore_start, m.restore_end, &m.mdr1, &c2);
+    m.d_mdr2 = upload_i32(c2);
+    epi_consts(mdr_src, next, m.restore_start, m.restore_end, &m.mdr_inv, &m.mdr_pad);
+  }
+  if (cudaDeviceSynchronize() != cudaSuccess) {
+    *err = std::string("context setup: ") + cudaGetErrorString(cudaGetLastError());
+    return kErrCuda;
+  }
+  return kOk;
+}
+
+// ------------------------------------------------------- building blocks
+namespace {
+// Splits a long list of rows into RowBatch launches.
+template <typename F>
+void for_row_batches(const std::vector<RowDesc> &rows, F &&launch) {
+  RowBatch rb;
+  rb.count = 0;
+  for (const RowDesc &r : rows) {
+    rb.rows[rb.count++] = r;
+    if (rb.count == kMaxRows) {
+      launch(rb);
+      rb.count = 0;
+    }
+  }
+  if (rb.count) launch(rb);
+}
+}  // namespace
+
+Status Context::ntt(const NP &np, uint32_t *data, bool mont, int count, size_t stride) {
+  const int tot = np.total(), n = P->n;
+  std::vector<int> g(tot);
+  P->gidx(np, g.data());
+  std::vector<RowDesc> rows;
+  for (int c = 0; c < count; c++)
+    for (int i = 0; i < tot; i++) {
+      RowDesc r{};
+      r.src = r.dst = data + c * stride + static_cast<size_t>(i) * n;
+      r.tw = tw(g[i]);
+      r.q = P->primes[g[i]];
+      r.qinv = P->qinv[g[i]];
+      r.c0 = mont_conv[g[i]];
+      r.flags = mont ? kPreMult : 0u;
+      rows.push_back(r);
+    }
+  for_row_batches(rows, [&](const RowBatch &rb) { launch_ntt_fwd(rb, P->log_n, stream); });
+  return check_cuda("ntt");
+}
+
+Status Context::intt(const NP &np, uint32_t *data, bool mont, int count, size_t stride) {
+  const int tot = np.total(), n = P->n;
+  std::vector<int> g(tot);
+  P->gidx(np, g.data());
+  std::vector<RowDesc> rows;
+  for (int c = 0; c < count; c++)
+    for (int i = 0; i < tot; i++) {
+      RowDesc r{};
+      r.src = r.dst = data + c * stride + static_cast<size_t>(i) * n;
+      r.tw = itw(g[i]);
+      r.q = P->primes[g[i]];
+      r.qinv = P->qinv[g[i]];
+      r.c0 = mont ? n_inv[g[i]] : n_inv_mont[g[i]];
+      rows.push_back(r);
+    }
+  for_row_batches(rows, [&](const RowBatch &rb) { launch_ntt_inv(rb, P->log_n, stream); });
+  return check_cuda("intt");
+}
+
+Status Context::bconv(const int32_t *xt, int K, const int32_t *table, const int *dst_gidx, int M, uint32_t *out) {
+  CHD_CHECK(K >= 1 && K <= 16 && M >= 1 && M <= 64, kErrUnsupported, "bconv: K must be in [1,16], M in [1,64]");
+  BConvBatch b{};
+  b.count = 1;
+  b.primes = d_primes;
+  b.qinvs = d_qinv;
+  BConvJob &j = b.jobs[0];
+  j.xt = xt;
+  j.out = out;
+  j.table = table;
+  j.K = K;
+  j.M = M;
+  for (int m = 0; m < M; m++) {
+    j.out_row[m] = static_cast<uint8_t>(m);
+    j.out_gidx[m] = static_cast<uint8_t>(dst_gidx[m]);
+  }
+  launch_bconv(b, P->log_n, stream);
+  return check_cuda("bconv");
+}
+
+Status Context::modup(int level, const uint32_t *src, uint32_t *const *dst) {
+  // ModSwitch.cu:429-509
+  const LevelMS &m = lms(level);
+  const int n = P->n;
+  NP np = P->level_np(level, m.num_aux);
+  const int nq = np.q(), tot = np.total();
+  std::vector<int> g(tot);
+  P->gidx(np, g.data());
+  ArenaScope scope(arena);
+  int32_t *xt = static_cast<int32_t *>(arena.alloc(static_cast<size_t>(nq) * n * 4));
+  CHD_CHECK(xt, kErrAlloc, "modup: scratch allocation failed");
+  // 1. INTT * (N q-hat_i)^-1, centred (INTTAndMultConst with normalize)
+  std::vector<RowDesc> rows;
+  for (int r = 0; r < nq; r++) {
+    RowDesc d{};
+    d.src = src + static_cast<size_t>(r) * n;
+    d.dst = reinterpret_cast<uint32_t *>(xt) + static_cast<size_t>(r) * n;
+    d.tw = itw(g[r]);
+    d.q = P->primes[g[r]];
+    d.qinv = P->qinv[g[r]];
+    d.c0 = m.mod_up1[r];
+    d.flags = kCentre;
+    rows.push_back(d);
+  }
+  for_row_batches(rows, [&](const RowBatch &rb) { launch_ntt_inv(rb, P->log_n, stream); });
+  // 2. own primes copied, others base-converted
+  BConvBatch b{};
+  b.primes = d_primes;
+  b.qinvs = d_qinv;
+  for (int i = 0; i < m.beta; i++) {
+    const int s = m.dig_s[i], e = m.dig_e[i];
+    if (e <= 0) continue;
+    cudaMemcpyAsync(dst[i] + static_cast<size_t>(s) * n, src + static_cast<size_t>(s) * n,
+                    static_cast<size_t>(e - s) * n * 4, cudaMemcpyDeviceToDevice, stream);
+    BConvJob &j = b.jobs[b.count++];
+    j.xt = xt + static_cast<size_t>(s) * n;
+    j.out = dst[i];
+    j.table = m.d_mod_up2[i];
+    j.K = e - s;
+    j.M = tot - (e - s);
+    CHD_CHECK(j.K <= 16 && j.M <= 64, kErrUnsupported, "modup: digit too large");
+    int k = 0;
+    for (int r = 0; r < tot; r++) {
+      if (r >= s && r < e) continue;
+      j.out_row[k] = static_cast<uint8_t>(r);
+      j.out_gidx[k] = static_cast<uint8_t>(g[r]);
+      k++;
+    }
+    if (b.count == kMaxBConvJobs) {
+      launch_bconv(b, P->log_n, stream);
+      b.count = 0;
+    }
+  }
+  launch_bconv(b, P->log_n, stream);
+  // 3. NTT of the converted rows (NTTForModUp)
+  rows.clear();
+  for (int i = 0; i < m.beta; i++) {
+    const int s = m.dig_s[i], e = m.dig_e[i];
+    if (e <= 0) continue;
+    for (int r = 0; r < tot; r++) {
+      if (r >= s && r < e) continue;
+      RowDesc d{};
+      d.src = d.dst = dst[i] + static_cast<size_t>(r) * n;
+      d.tw = tw(g[r]);
+      d.q = P->primes[g[r]];
+      d.qinv = P->qinv[g[r]];
+      rows.push_back(d);
+    }
+  }
+  for_row_batches(rows, [&](const RowBatch &rb) { launch_ntt_fwd(rb, P->log_n, stream); });
+  return check_cuda("modup");
+}
+
+Status Context::moddown(int level, MDType type, const uint32_t *const *src, uint32_t *const *dst, int npoly) {
+  // ModSwitch.cu:566-684 with NTT.cu:973-1128 and the fused epilogue of
+  // NTT.cu:456-601
+  const LevelMS &m = lms(level);
+  const int n = P->n;
+  CHD_CHECK(type == MDType::kModDown || m.has_rescale, kErrInvalidLevel, "rescale not available at this level");
+  const int nsa = type == MDType::kRescale ? 0 : m.num_aux;
+  NP ns = P->level_np(level, nsa);
+  NP nd = P->level_np(type == MDType::kModDown ? level : level - 1, 0);
+  NP nn{std::min(ns.main, nd.main), std::min(ns.ter, nd.ter), 0};
+  const int src_len = ns.total() - nn.total(), dst_len = nd.total();
+  CHD_CHECK(src_len >= 1 && src_len <= 16, kErrUnsupported, "moddown: more than 16 dropped primes");
+  const uint32_t *c1 = type == MDType::kModDown ? m.mod_down1.data()
+                       : type == MDType::kRescale ? m.rs1.data() : m.mdr1.data();
+  const int32_t *table = type == MDType::kModDown ? m.d_mod_down2 : type == MDType::kRescale ? m.d_rs2 : m.d_mdr2;
+  const uint32_t *inv = type == MDType::kModDown ? m.inv_p_prod.data()
+                        : type == MDType::kRescale ? m.rs_inv.data() : m.mdr_inv.data();
+  const uint32_t *pad = type == MDType::kModDown ? nullptr
+                        : type == MDType::kRescale ? m.rs_pad.data() : m.mdr_pad.data();
+  std::vector<int> gs(ns.total()), gd(nd.total());
+  P->gidx(ns, gs.data());
+  P->gidx(nd, gd.data());
+  std::vector<int> srows;
+  const bool on_main = ns.main > nn.main, on_ter = ns.ter > nn.ter;
+  CHD_CHECK(!(on_main && on_ter), kErrInvalidArg, "moddown: invalid prime combination");
+  if (!on_ter)
+    for (int r = ns.ter + nn.main; r < ns.q(); r++) srows.push_back(r);
+  else
+    for (int r = 0; r < ns.ter - nn.ter; r++) srows.push_back(r);
+  for (int a = 0; a < nsa; a++) srows.push_back(ns.q() + a);
+  CHD_CHECK(static_cast<int>(srows.size()) == src_len, kErrInvalidArg, "moddown: internal row mismatch");
+  ArenaScope scope(arena);
+  int32_t *xt = static_cast<int32_t *>(arena.alloc(static_cast<size_t>(npoly) * src_len * n * 4));
+  CHD_CHECK(xt, kErrAlloc, "moddown: scratch allocation failed");
+  std::vector<RowDesc> rows;
+  for (int p = 0; p < npoly; p++)
+    for (int i = 0; i < src_len; i++) {
+      const int gg = gs[srows[i]];
+      RowDesc d{};
+      d.src = src[p] + static_cast<size_t>(srows[i]) * n;
+      d.dst = reinterpret_cast<uint32_t *>(xt) + (static_cast<size_t>(p) * src_len + i) * n;
+      d.tw = itw(gg);
+      d.q = P->primes[gg];
+      d.qinv = P->qinv[gg];
+      d.c0 = c1[i];
+      d.flags = kCentre;
+      rows.push_back(d);
+    }
+  for_row_batches(rows, [&](const RowBatch &rb) { launch_ntt_inv(rb, P->log_n, stream); });
+  BConvBatch b{};
+  b.primes = d_primes;
+  b.qinvs = d_qinv;
+  for (int p = 0; p < npoly; p++) {
+    BConvJob &j = b.jobs[b.count++];
+    j.xt = xt + static_cast<size_t>(p) * src_len * n;
+    j.out = dst[p];
+    j.table = table;
+    j.K = src_len;
+    j.M = dst_len;
+    for (int y = 0; y < dst_len; y++) {
+      j.out_row[y] = static_cast<uint8_t>(y);
+      j.out_gidx[y] = static_cast<uint8_t>(gd[y]);
+    }
+    if (b.count == kMaxBConvJobs) {
+      launch_bconv(b, P->log_n, stream);
+      b.count = 0;
+    }
+  }
+  launch_bconv(b, P->log_n, stream);
+  const int src2_start = nd.ter - nn.ter, src2_end = src2_start + nn.q();
+  const int src2_off = std::max(0, ns.ter - nd.ter);
+  rows.clear();
+  for (int p = 0; p < npoly; p++)
+    for (int y = 0; y < dst_len; y++) {
+      RowDesc d{};
+      d.src = d.dst = dst[p] + static_cast<size_t>(y) * n;
+      d.tw = tw(gd[y]);
+      d.q = P->primes[gd[y]];
+      d.qinv = P->qinv[gd[y]];
+      d.c2 = inv[y];
+      d.flags = kModDownEpi;
+      if (y >= src2_start && y < src2_end) {
+        d.flags |= kHasSrc2;
+        d.src2 = src[p] + static_cast<size_t>(src2_off + y - src2_start) * n;
+        if (pad) {
+          d.flags |= kPadSrc2;
+          d.c1 = pad[y - src2_start];
+        }
+      }
+      rows.push_back(d);
+    }
+  for_row_batches(rows, [&](const RowBatch &rb) { launch_ntt_fwd(rb, P->log_n, stream); });
+  return check_cuda("moddown");
+}
+
+// --------------------------------------------------------- evaluator
+Status Context::key_switch_core(int level, const uint32_t *d0, const uint32_t *d1, const uint32_t *d_in,
+                                const DeviceEvk &key, uint32_t *acc_b, uint32_t *acc_a) {
+  // Context.cpp:609-712 (MultKeyNoModDown with the CAccum of P * (d0, d1))
+  const LevelMS &m = lms(level);
+  const int n = P->n;
+  NP np = P->level_np(level, P->alpha);
+  const int nq = np.q(), tot = np.total();
+  CHD_CHECK(tot <= 64 && m.beta <= 8, kErrUnsupported, "key switch: more than 64 primes or 8 digits");
+  CHD_CHECK(key.np.aux == P->alpha && key.np.q() == P->L, kErrKey, "key switch: key basis mismatch");
+  const int prime_offset = P->max_ter - np.ter;
+  ArenaScope scope(arena);
+  std::vector<uint32_t *> mu(m.beta, nullptr);
+  for (int i = 0; i < m.beta; i++) {
+    mu[i] = static_cast<uint32_t *>(arena.alloc(static_cast<size_t>(tot) * n * 4));
+    CHD_CHECK(mu[i], kErrAlloc, "key switch: scratch allocation failed");
+  }
+  CHD_TRY(modup(level, d_in, mu.data()));
+  KeyMacDesc d{};
+  std::vector<int> g(tot);
+  P->gidx(np, g.data());
+  const size_t kstride = static_cast<size_t>(key.np.total()) * n;
+  int nb = 0;
+  for (int i = 0; i < m.beta; i++) {
+    if (m.dig_e[i] <= 0) continue;
+    CHD_CHECK(i < key.beta, kErrKey, "key switch: key has too few digits");
+    d.mu[nb] = mu[i];
+    d.kb[nb] = key.bx + i * kstride;
+    d.ka[nb] = key.ax + i * kstride;
+    nb++;
+  }
+  d.beta = nb;
+  d.d0 = d0;
+  d.d1 = d1;
+  d.acc_b = acc_b;
+  d.acc_a = acc_a;
+  d.rows = tot;
+  d.nq = nq;
+  for (int r = 0; r < tot; r++) {
+    d.q[r] = P->primes[g[r]];
+    d.qinv[r] = P->qinv[g[r]];
+    d.key_row[r] = static_cast<int16_t>(r < nq ? prime_offset + r : P->L + (r - nq));
+    d.p_prod[r] = r < nq ? p_prod[prime_offset + r] : 0;
+  }
+  launch_key_mac(d, P->log_n, stream);
+  return check_cuda("key switch");
+}
+
+static int level_of(const Params &P, const DeviceCt &a) { return P.np_to_level(NP{a.np.main, a.np.ter, 0}); }
+
+Status Context::hmult(DeviceCt &res, const DeviceCt &a, const DeviceCt &b, const DeviceEvk &key, bool rescale) {
+  // Context.cpp:862-871: Mult (tensor) then RelinearizeRescale (merged
+  // ModDown+Rescale) or Relinearize
+  CHD_CHECK(a.np == b.np && a.np.aux == 0, kErrShape, "HMult: operands must share a level and have no aux primes");
+  CHD_CHECK(!a.has_rx && !b.has_rx, kErrShape, "Relinearization required before Mult Ct x Ct");
+  const int level = level_of(*P, a);
+  CHD_CHECK(level >= 0, kErrInvalidLevel, "HMult: invalid level");
+  CHD_CHECK(!rescale || level >= 1, kErrInvalidLevel, "Not enough q primes to rescale");
+  const int n = P->n, nq = a.np.q(), tot = nq + P->alpha;
+  CHD_CHECK(tot <= 64, kErrUnsupported, "HMult: more than 64 primes in the extended basis");
+  ArenaScope scope(arena);
+  uint32_t *d = static_cast<uint32_t *>(arena.alloc(static_cast<size_t>(3) * nq * n * 4));
+  uint32_t *acc = static_cast<uint32_t *>(arena.alloc(static_cast<size_t>(2) * tot * n * 4));
+  CHD_CHECK(d && acc, kErrAlloc, "HMult: scratch allocation failed");
+  uint32_t *d0 = d, *d1 = d + static_cast<size_t>(nq) * n, *d2 = d + static_cast<size_t>(2) * nq * n;
+  std::vector<int> g(nq);
+  P->gidx(a.np, g.data());
+  TensorBatch tb{};
+  for (int r = 0; r < nq; r++) {
+    TensorRow &t = tb.rows[tb.count++];
+    const size_t o = static_cast<size_t>(r) * n;
+    t.b1 = a.bx + o;
+    t.a1 = a.ax + o;
+    t.b2 = b.bx + o;
+    t.a2 = b.ax + o;
+    t.d0 = d0 + o;
+    t.d1 = d1 + o;
+    t.d2 = d2 + o;
+    t.q = P->primes[g[r]];
+    t.qinv = P->qinv[g[r]];
+  }
+  launch_tensor(tb, P->log_n, stream);
+  uint32_t *acc_b = acc, *acc_a = acc + static_cast<size_t>(tot) * n;
+  CHD_TRY(key_switch_core(level, d0, d1, d2, key, acc_b, acc_a));
+  const double sa = a.scale, sb = b.scale;
+  const int slots = std::max(a.num_slots, b.num_slots);
+  NP out_np = P->level_np(rescale ? level - 1 : level, 0);
+  CHD_TRY(res.reserve(out_np, false, n));
+  const uint32_t *srcs[2] = {acc_b, acc_a};
+  uint32_t *dsts[2] = {res.bx, res.ax};
+  CHD_TRY(moddown(level, rescale ? MDType::kModDownRescale : MDType::kModDown, srcs, dsts, 2));
+  res.scale = rescale ? sa * sb / P->rescale_prod[level] : sa * sb;
+  res.num_slots = slots;
+  return kOk;
+}
+
+Status Context::hmult_batch(int count, DeviceCt *const *res, const DeviceCt *const *a, const DeviceCt *const *b,
+                            const DeviceEvk &key, bool rescale) {
+  for (int i = 0; i < count; i++) CHD_TRY(hmult(*res[i], *a[i], *b[i], key, rescale));
+  return kOk;
+}
+
+Status Context::relinearize(DeviceCt &res, const DeviceCt &a, const DeviceEvk &key, bool rescale) {
+  // Context.cpp:539-547 and :714-737
+  CHD_CHECK(a.has_rx && a.np.aux == 0, kErrShape, "Relinearize requires a ciphertext with rx");
+  const int level = level_of(*P, a);
+  CHD_CHECK(level >= 0, kErrInvalidLevel, "Relinearize: invalid level");
+  CHD_CHECK(!rescale || level >= 1, kErrInvalidLevel, "Not enough q primes to rescale");
+  const int n = P->n, tot = a.np.q() + P->alpha;
+  ArenaScope scope(arena);
+  uint32_t *acc = static_cast<uint32_t *>(arena.alloc(static_cast<size_t>(2) * tot * n * 4));
+  CHD_CHECK(acc, kErrAlloc, "Relinearize: scratch allocation failed");
+  uint32_t *acc_b = acc, *acc_a = acc + static_cast<size_t>(tot) * n;
+  CHD_TRY(key_switch_core(level, a.bx, a.ax, a.rx, key, acc_b, acc_a));
+  const double sc = a.scale;
+  const int slots = a.num_slots;
+  CHD_TRY(res.reserve(P->level_np(rescale ? level - 1 : level, 0), false, n));
+  const uint32_t *srcs[2] = {acc_b, acc_a};
+  uint32_t *dsts[2] = {res.bx, res.ax};
+  CHD_TRY(moddown(level, rescale ? MDType::kModDownRescale : MDType::kModDown, srcs, dsts, 2));
+  res.scale = rescale ? sc / P->rescale_prod[level] : sc;
+  res.num_slots = slots;
+  return kOk;
+}
+
+Status Context::mult_key(DeviceCt &res, const DeviceCt &a, const DeviceEvk &key) {
+  // Context.cpp:584-607
+  CHD_CHECK(!a.has_rx && a.np.aux == 0, kErrShape, "MultKey: ciphertext must be relinearised, no aux primes");
+  const int level = level_of(*P, a);
+  CHD_CHECK(level >= 0, kErrInvalidLevel, "MultKey: invalid level");
+  const int n = P->n, tot = a.np.q() + P->alpha;
+  ArenaScope scope(arena);
+  uint32_t *acc = static_cast<uint32_t *>(arena.alloc(static_cast<size_t>(2) * tot * n * 4));
+  CHD_CHECK(acc, kErrAlloc, "MultKey: scratch allocation failed");
+  uint32_t *acc_b = acc, *acc_a = acc + static_cast<size_t>(tot) * n;
+  CHD_TRY(key_switch_core(level, a.bx, nullptr, a.ax, key, acc_b, acc_a));
+  const double sc = a.scale;
+  const int slots = a.num_slots;
+  const NP np = a.np;
+  CHD_TRY(res.reserve(np, false, n));
+  const uint32_t *srcs[2] = {acc_b, acc_a};
+  uint32_t *dsts[2] = {res.bx, res.ax};
+  CHD_TRY(moddown(level, MDType::kModDown, srcs, dsts, 2));
+  res.scale = sc;
+  res.num_slots = slots;
+  return kOk;
+}
+
+Status Context::permute(DeviceCt &res, const DeviceCt &a, int amount) {
+  // Context.cpp:501-527 (ElementWise.cu:370-391)
+  CHD_CHECK(&res != &a, kErrInvalidArg, "Permute does not support in-place operation");
+  CHD_CHECK(amount == -1 || (amount >= 0 && amount <= P->n / 2), kErrInvalidArg, "Permute: invalid amount");
+  const int n = P->n, tot = a.np.total();
+  CHD_TRY(res.reserve(a.np, a.has_rx, n));
+  PermuteBatch pb{};
+  pb.galois = P->galois_of(amount);
+  std::vector<int> g(tot);
+  P->gidx(a.np, g.data());
+  const uint32_t *src[3] = {a.bx, a.ax, a.rx};
+  uint32_t *dst[3] = {res.bx, res.ax, res.rx};
+  const int parts = a.has_rx ? 3 : 2;
+  for (int p = 0; p < parts; p++)
+    for (int r = 0; r < tot; r++) {
+      if (pb.count == 64) {
+        launch_permute(pb, P->log_n, stream);
+        pb.count = 0;
+      }
+      PermuteRow &pr = pb.rows[pb.count++];
+      pr.src = src[p] + static_cast<size_t>(r) * n;
+      pr.dst = dst[p] + static_cast<size_t>(r) * n;
+      pr.add = nullptr;
+      pr.q = P->primes[g[r]];
+    }
+  launch_permute(pb, P->log_n, stream);
+  res.scale = a.scale;
+  res.num_slots = a.num_slots;
+  return check_cuda("permute");
+}
+
+// Temporary ciphertext carved from the arena (released with the enclosing
+// ArenaScope; stream order makes the reuse safe).
+static Status scratch_ct(Arena &arena, DeviceCt &t, const NP &np, bool rx, int n) {
+  const size_t words = static_cast<size_t>(np.total()) * n;
+  t.owned = false;
+  t.bx = static_cast<uint32_t *>(arena.alloc(words * 4));
+  t.ax = static_cast<uint32_t *>(arena.alloc(words * 4));
+  t.rx = rx ? static_cast<uint32_t *>(arena.alloc(words * 4)) : nullptr;
+  t.cap_words = words;
+  t.np = np;
+  t.has_rx = rx;
+  if (!t.bx || !t.ax || (rx && !t.rx)) {
+    set_error("scratch allocation failed");
+    return kErrAlloc;
+  }
+  return kOk;
+}
+
+Status Context::hrot(DeviceCt &res, const DeviceCt &a, const DeviceEvk &key, int dist) {
+  // Context.cpp:776-791: MultKey first, then the automorphism
+  int slots = a.num_slots > 0 ? a.num_slots : P->n / 2;
+  dist %= slots;
+  if (dist < 0) dist += slots;
+  if (dist == 0) {
+    if (&res == &a) return kOk;
+    const NP np = a.np;
+    const bool rx = a.has_rx;
+    CHD_TRY(res.reserve(np, rx, P->n));
+    const size_t bytes = static_cast<size_t>(np.total()) * P->n * 4;
+    cudaMemcpyAsync(res.bx, a.bx, bytes, cudaMemcpyDeviceToDevice, stream);
+    cudaMemcpyAsync(res.ax, a.ax, bytes, cudaMemcpyDeviceToDevice, stream);
+    if (rx) cudaMemcpyAsync(res.rx, a.rx, bytes, cudaMemcpyDeviceToDevice, stream);
+    res.scale = a.scale;
+    res.num_slots = a.num_slots;
+    return check_cuda("hrot copy");
+  }
+  ArenaScope scope(arena);
+  DeviceCt tmp;
+  CHD_TRY(scratch_ct(arena, tmp, a.np, false, P->n));
+  CHD_TRY(mult_key(tmp, a, key));
+  return permute(res, tmp, dist);
+}
+
+Status Context::hconj(DeviceCt &res, const DeviceCt &a, const DeviceEvk &key) {
+  ArenaScope scope(arena);
+  DeviceCt tmp;
+  CHD_TRY(scratch_ct(arena, tmp, a.np, false, P->n));
+  CHD_TRY(mult_key(tmp, a, key));
+  return permute(res, tmp, -1);
+}
+
+Status Context::hrot_add(DeviceCt &res, const DeviceCt &a, const DeviceCt &b, const DeviceEvk &key, int dist) {
+  // Context.cpp:800-830: res = Permute(MultKey(a)) + b
+  CHD_CHECK(a.np == b.np, kErrShape, "HRotAdd: level mismatch");
+  ArenaScope scope(arena);
+  DeviceCt tmp;
+  CHD_TRY(scratch_ct(arena, tmp, a.np, false, P->n));
+  CHD_TRY(hrot(tmp, a, key, dist));
+  return add(res, tmp, b);
+}
+
+Status Context::moddown_ct(DeviceCt &res, const DeviceCt &a) {
+  CHD_CHECK(a.np.aux == P->alpha, kErrShape, "ModDown: input must carry all aux primes");
+  const int level = P->np_to_level(NP{a.np.main, a.np.ter, 0});
+  CHD_CHECK(level >= 0, kErrInvalidLevel, "ModDown: invalid level");
+  NP out{a.np.main, a.np.ter, 0};
+  const double sc = a.scale;
+  const int slots = a.num_slots;
+  CHD_CHECK(&res != &a, kErrInvalidArg, "ModDown does not support in-place operation");
+  CHD_TRY(res.reserve(out, false, P->n));
+  const uint32_t *srcs[2] = {a.bx, a.ax};
+  uint32_t *dsts[2] = {res.bx, res.ax};
+  CHD_TRY(moddown(level, MDType::kModDown, srcs, dsts, 2));
+  res.scale = sc;
+  res.num_slots = slots;
+  return kOk;
+}
+
+Status Context::hoisted_rotate(const DeviceCt &a, int R, const int *dists, const DeviceEvk *const *keys,
+                               DeviceCt *const *out) {
+  // Hoist.cu:578-691 with the fused BS kernel of Hoist.cu:21-78: one ModUp,
+  // then every rotation in one launch, results left in Q u P
+  CHD_CHECK(!a.has_rx && a.np.aux == 0, kErrShape, "hoisted rotate: input must be relinearised");
+  const int level = level_of(*P, a);
+  CHD_CHECK(level >= 0, kErrInvalidLevel, "hoisted rotate: invalid level");
+  const LevelMS &m = lms(level);
+  const int n = P->n;
+  NP np = P->level_np(level, P->alpha);
+  const int nq = np.q(), tot = np.total();
+  CHD_CHECK(tot <= 64 && m.beta <= 8, kErrUnsupported, "hoisted rotate: too many primes");
+  const int prime_offset = P->max_ter - np.ter;
+  ArenaScope scope(arena);
+  std::vector<uint32_t *> mu(m.beta, nullptr);
+  for (int i = 0; i < m.beta; i++) {
+    mu[i] = static_cast<uint32_t *>(arena.alloc(static_cast<size_t>(tot) * n * 4));
+    CHD_CHECK(mu[i], kErrAlloc, "hoisted rotate: scratch allocation failed");
+  }
+  uint32_t *bxp = static_cast<uint32_t *>(arena.alloc(static_cast<size_t>(nq) * n * 4));
+  CHD_CHECK(bxp, kErrAlloc, "hoisted rotate: scratch allocation failed");
+  CHD_TRY(modup(level, a.ax, mu.data()));
+  std::vector<int> g(tot);
+  P->gidx(np, g.data());
+  {
+    ElemBatch eb{};
+    for (int r = 0; r < nq; r++) {
+      if (eb.count == kMaxElemRows) {
+        launch_elementwise(ElemOp::kMultConst, eb, P->log_n, stream);
+        eb.count = 0;
+      }
+      ElemRow &e = eb.rows[eb.count++];
+      e.a = a.bx + static_cast<size_t>(r) * n;
+      e.dst = bxp + static_cast<size_t>(r) * n;
+      e.q = P->primes[g[r]];
+      e.qinv = P->qinv[g[r]];
+      e.k = p_prod[prime_offset + r];
+    }
+    launch_elementwise(ElemOp::kMultConst, eb, P->log_n, stream);
+  }
+  for (int j = 0; j < R; j++) {
+    int slots = a.num_slots > 0 ? a.num_slots : n / 2;
+    int dd = dists[j] % slots;
+    if (dd < 0) dd += slots;
+    CHD_CHECK(dd > 0 && dd < n / 2, kErrInvalidArg, "hoisted rotate: invalid rotation");
+    CHD_TRY(out[j]->reserve(np, false, n));
+    out[j]->scale = a.scale;
+    out[j]->num_slots = a.num_slots;
+  }
+  const size_t kstride = static_cast<size_t>(P->L + P->alpha) * n;
+  for (int j0 = 0; j0 < R; j0 += kMaxHoist) {
+    HoistDesc d{};
+    int nb = 0;
+    for (int i = 0; i < m.beta; i++)
+      if (m.dig_e[i] > 0) d.mu[nb++] = mu[i];
+    d.beta = nb;
+    d.bxp = bxp;
+    d.rows = tot;
+    d.nq = nq;
+    d.R = std::min(kMaxHoist, R - j0);
+    for (int r = 0; r < tot; r++) {
+      d.q[r] = P->primes[g[r]];
+      d.qinv[r] = P->qinv[g[r]];
+      d.key_row[r] = static_cast<int16_t>(r < nq ? prime_offset + r : P->L + (r - nq));
+    }
+    for (int j = 0; j < d.R; j++) {
+      const DeviceEvk &k = *keys[j0 + j];
+      CHD_CHECK(k.np.aux == P->alpha && k.np.q() == P->L, kErrKey, "hoisted rotate: key basis mismatch");
+      int slots = a.num_slots > 0 ? a.num_slots : n / 2;
+      int dd = dists[j0 + j] % slots;
+      if (dd < 0) dd += slots;
+      int b = 0;
+      for (int i = 0; i < m.beta; i++) {
+        if (m.dig_e[i] <= 0) continue;
+        CHD_CHECK(i < k.beta, kErrKey, "hoisted rotate: key has too few digits");
+        d.kb[j][b] = k.bx + i * kstride;
+        d.ka[j][b] = k.ax + i * kstride;
+        b++;
+      }
+      d.out_b[j] = out[j0 + j]->bx;
+      d.out_a[j] = out[j0 + j]->ax;
+      d.galois_inv[j] = P->galois_of(n / 2 - dd);
+    }
+    launch_hoisted(d, P->log_n, stream);
+  }
+  return check_cuda("hoisted rotate");
+}
+
+// ------------------------------------------------------- element-wise ops
+namespace {
+Status elem_parts(Context &C, ElemOp op, const NP &np, int parts, uint32_t *const *dst, const uint32_t *const *a,
+                  const uint32_t *const *b, const uint32_t *k) {
+  const int n = C.P->n, tot = np.total();
+  std::vector<int> g(tot);
+  C.P->gidx(np, g.data());
+  ElemBatch eb{};
+  for (int p = 0; p < parts; p++)
+    for (int r = 0; r < tot; r++) {
+      if (eb.count == kMaxElemRows) {
+        launch_elementwise(op, eb, C.P->log_n, C.stream);
+        eb.count = 0;
+      }
+      ElemRow &e = eb.rows[eb.count++];
+      e.a = a[p] + static_cast<size_t>(r) * n;
+      e.b = b ? b[p] + static_cast<size_t>(r) * n : nullptr;
+      e.c = nullptr;
+      e.dst = dst[p] + static_cast<size_t>(r) * n;
+      e.q = C.P->primes[g[r]];
+      e.qinv = C.P->qinv[g[r]];
+      e.k = k ? k[r] : 0;
+    }
+  launch_elementwise(op, eb, C.P->log_n, C.stream);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_error(cudaGetErrorString(e));
+    return kErrCuda;
+  }
+  return kOk;
+}
+}  // namespace
+
+Status Context::add(DeviceCt &res, const DeviceCt &a, const DeviceCt &b) {
+  // Context.cpp:145-172
+  CHD_CHECK(a.np == b.np, kErrShape, "Add: level mismatch");
+  const bool both_rx = a.has_rx && b.has_rx;
+  const DeviceCt *rx_src = a.has_rx ? &a : (b.has_rx ? &b : nullptr);
+  const uint32_t *keep_rx = (!both_rx && rx_src) ? rx_src->rx : nullptr;
+  const bool out_rx = a.has_rx || b.has_rx;
+  const NP np = a.np;
+  const uint32_t *pa[3] = {a.bx, a.ax, a.rx}, *pb[3] = {b.bx, b.ax, b.rx};
+  const double sc = a.scale;
+  const int slots = std::max(a.num_slots, b.num_slots);
+  CHD_TRY(res.reserve(np, out_rx, P->n));
+  uint32_t *pd[3] = {res.bx, res.ax, res.rx};
+  CHD_TRY(elem_parts(*this, ElemOp::kAdd, np, both_rx ? 3 : 2, pd, pa, pb, nullptr));
+  if (keep_rx && keep_rx != res.rx)
+    cudaMemcpyAsync(res.rx, keep_rx, static_cast<size_t>(np.total()) * P->n * 4, cudaMemcpyDeviceToDevice, stream);
+  res.scale = sc;
+  res.num_slots = slots;
+  return kOk;
+}
+
+Status Context::sub(DeviceCt &res, const DeviceCt &a, const DeviceCt &b) {
+  CHD_CHECK(a.np == b.np, kErrShape, "Sub: level mismatch");
+  CHD_CHECK(a.has_rx == b.has_rx, kErrUnsupported, "Sub: mixed rx operands are not supported");
+  const NP np = a.np;
+  const uint32_t *pa[3] = {a.bx, a.ax, a.rx}, *pb[3] = {b.bx, b.ax, b.rx};
+  const double sc = a.scale;
+  const int slots = std::max(a.num_slots, b.num_slots);
+  const bool rx = a.has_rx;
+  CHD_TRY(res.reserve(np, rx, P->n));
+  uint32_t *pd[3] = {res.bx, res.ax, res.rx};
+  CHD_TRY(elem_parts(*this, ElemOp::kSub, np, rx ? 3 : 2, pd, pa, pb, nullptr));
+  res.scale = sc;
+  res.num_slots = slots;
+  return kOk;
+}
+
+Status Context::neg(DeviceCt &res, const DeviceCt &a) {
+  const NP np = a.np;
+  const uint32_t *pa[3] = {a.bx, a.ax, a.rx};
+  const bool rx = a.has_rx;
+  const double sc = a.scale;
+  const int slots = a.num_slots;
+  CHD_TRY(res.reserve(np, rx, P->n));
+  uint32_t *pd[3] = {res.bx, res.ax, res.rx};
+  CHD_TRY(elem_parts(*this, ElemOp::kNeg, np, rx ? 3 : 2, pd, pa, nullptr, nullptr));
+  res.scale = sc;
+  res.num_slots = slots;
+  return kOk;
+}
+
+Status Context::mult_tensor(DeviceCt &res, const DeviceCt &a, const DeviceCt &b) {
+  // Context.cpp:316-330
+  CHD_CHECK(a.np == b.np && a.np.aux == 0, kErrShape, "Mult: level mismatch");
+  CHD_CHECK(!a.has_rx && !b.has_rx, kErrShape, "Relinearization required before Mult Ct x Ct");
+  CHD_CHECK(&res != &a && &res != &b, kErrInvalidArg, "Mult: result must not alias an operand");
+  const int n = P->n, nq = a.np.q();
+  CHD_CHECK(nq <= 64, kErrUnsupported, "Mult: more than 64 primes");
+  CHD_TRY(res.reserve(a.np, true, n));
+  std::vector<int> g(nq);
+  P->gidx(a.np, g.data());
+  TensorBatch tb{};
+  for (int r = 0; r < nq; r++) {
+    TensorRow &t = tb.rows[tb.count++];
+    const size_t o = static_cast<size_t>(r) * n;
+    t.b1 = a.bx + o;
+    t.a1 = a.ax + o;
+    t.b2 = b.bx + o;
+    t.a2 = b.ax + o;
+    t.d0 = res.bx + o;
+    t.d1 = res.ax + o;
+    t.d2 = res.rx + o;
+    t.q = P->primes[g[r]];
+    t.qinv = P->qinv[g[r]];
+  }
+  launch_tensor(tb, P->log_n, stream);
+  res.scale = a.scale * b.scale;
+  res.num_slots = std::max(a.num_slots, b.num_slots);
+  return check_cuda("mult");
+}
+
+Status Context::mult_const(DeviceCt &res, const DeviceCt &a, const uint32_t *cx, double cscale) {
+  const NP np = a.np;
+  const uint32_t *pa[3] = {a.bx, a.ax, a.rx};
+  const bool rx = a.has_rx;
+  const double sc = a.scale * cscale;
+  const int slots = a.num_slots;
+  CHD_TRY(res.reserve(np, rx, P->n));
+  uint32_t *pd[3] = {res.bx, res.ax, res.rx};
+  CHD_TRY(elem_parts(*this, ElemOp::kMultConst, np, rx ? 3 : 2, pd, pa, nullptr, cx));
+  res.scale = sc;
+  res.num_slots = slots;
+  return kOk;
+}
+
+Status Context::add_const(DeviceCt &res, const DeviceCt &a, const uint32_t *cx) {
+  const NP np = a.np;
+  const bool rx = a.has_rx;
+  const double sc = a.scale;
+  const int slots = a.num_slots;
+  const uint32_t *pa[1] = {a.bx};
+  const uint32_t *keep[2] = {a.ax, a.rx};
+  CHD_TRY(res.reserve(np, rx, P->n));
+  uint32_t *pd[1] = {res.bx};
+  CHD_TRY(elem_parts(*this, ElemOp::kAddConst, np, 1, pd, pa, nullptr, cx));
+  const size_t bytes = static_cast<size_t>(np.total()) * P->n * 4;
+  if (keep[0] != res.ax) cudaMemcpyAsync(res.ax, keep[0], bytes, cudaMemcpyDeviceToDevice, stream);
+  if (rx && keep[1] != res.rx) cudaMemcpyAsync(res.rx, keep[1], bytes, cudaMemcpyDeviceToDevice, stream);
+  res.scale = sc;
+  res.num_slots = slots;
+  return kOk;
+}
+
+Status Context::mult_plain(DeviceCt &res, const DeviceCt &a, const uint32_t *pt, double pscale) {
+  const NP np = a.np;
+  const uint32_t *pa[3] = {a.bx, a.ax, a.rx};
+  const uint32_t *pp[3] = {pt, pt, pt};
+  const bool rx = a.has_rx;
+  const double sc = a.scale * pscale;
+  const int slots = a.num_slots;
+  CHD_TRY(res.reserve(np, rx, P->n));
+  uint32_t *pd[3] = {res.bx, res.ax, res.rx};
+  CHD_TRY(elem_parts(*this, ElemOp::kMult, np, rx ? 3 : 2, pd, pa, pp, nullptr));
+  res.scale = sc;
+  res.num_slots = slots;
+  return kOk;
+}
+
+Status Context::mult_imag_unit(DeviceCt &res, const DeviceCt &a) {
+  // ElementWise.cu:625-658: multiply by X^(N/2) = +-psi^(N/2) (psi_rev[1])
+  CHD_CHECK(a.np.aux == 0, kErrShape, "MultImaginaryUnit: no aux primes");
+  const NP np = a.np;
+  std::vector<int> g(np.total());
+  P->gidx(np, g.data());
+  std::vector<uint32_t> k(np.total());
+  for (int r = 0; r < np.total(); r++) k[r] = imag_unit[g[r]];
+  const uint32_t *pa[3] = {a.bx, a.ax, a.rx};
+  const bool rx = a.has_rx;
+  const double sc = a.scale;
+  const int slots = a.num_slots;
+  CHD_TRY(res.reserve(np, rx, P->n));
+  uint32_t *pd[3] = {res.bx, res.ax, res.rx};
+  CHD_TRY(elem_parts(*this, ElemOp::kMultImagUnit, np, rx ? 3 : 2, pd, pa, nullptr, k.data()));
+  res.scale = sc;
+  res.num_slots = slots;
+  return kOk;
+}
+
+Status Context::rescale(DeviceCt &res, const DeviceCt &a) {
+  // Context.cpp:739-774
+  CHD_CHECK(a.np.aux == 0, kErrShape, "Rescale is not supported for ciphertexts with p primes");
+  CHD_CHECK(&res != &a, kErrInvalidArg, "Rescale does not support in-place operation");
+  const int level = level_of(*P, a);
+  CHD_CHECK(level >= 1, kErrInvalidLevel, "Not enough q primes to rescale");
+  const bool rx = a.has_rx;
+  CHD_TRY(res.reserve(P->level_np(level - 1, 0), rx, P->n));
+  const uint32_t *srcs[3] = {a.bx, a.ax, a.rx};
+  uint32_t *dsts[3] = {res.bx, res.ax, res.rx};
+  CHD_TRY(moddown(level, MDType::kRescale, srcs, dsts, rx ? 3 : 2));
+  res.scale = a.scale / P->rescale_prod[level];
+  res.num_slots = a.num_slots;
+  return kOk;
+}
+
+}  // namespace chd

@@ -1,0 +1,277 @@
+// Base conversion, key-switching inner product, element-wise and
+// automorphism kernels.  All are HBM-streaming integer kernels: each thread
+// owns 4 consecutive coefficients (128-bit loads and stores), grid.y walks
+// the limbs (or jobs) of the batch.
+#include "arith.cuh"
+#include "kernels.h"
+
+namespace chd {
+namespace {
+
+__device__ __forceinline__ uint4 ld4(const uint32_t *p) { return __ldg(reinterpret_cast<const uint4 *>(p)); }
+__device__ __forceinline__ void st4(uint32_t *p, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+  *reinterpret_cast<uint4 *>(p) = make_uint4(a, b, c, d);
+}
+__device__ __forceinline__ void unpack(uint4 v, uint32_t *x) {
+  x[0] = v.x; x[1] = v.y; x[2] = v.z; x[3] = v.w;
+}
+
+// ------------------------------------------------------------------ BConv
+// out[m][n] = (sum_k xt[k][n] T[m][k]) * 2^-32 mod p_m, exact.  |xt| < 2^30
+// and |T| <= (p-1)/2 bound every product by p * 2^29, so a group of 4 terms
+// stays inside the (-p 2^31, p 2^31) input range of the Montgomery reduction;
+// group results are summed canonically.  (The reference kernel,
+// src/core/ModSwitch.cu:23-171, computes the same residue.)
+__global__ void __launch_bounds__(256) k_bconv(const __grid_constant__ BConvBatch b, int log_n) {
+  const BConvJob &jb = b.jobs[blockIdx.y];
+  const int n = 1 << log_n;
+  const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  if (i0 >= n) return;
+  const int K = jb.K;
+  int32_t x[16][4];
+#pragma unroll
+  for (int k = 0; k < 16; k++) {
+    if (k < K) {
+      int4 v = __ldg(reinterpret_cast<const int4 *>(jb.xt + static_cast<size_t>(k) * n + i0));
+      x[k][0] = v.x; x[k][1] = v.y; x[k][2] = v.z; x[k][3] = v.w;
+    }
+  }
+  for (int m = 0; m < jb.M; m++) {
+    const int g = jb.out_gidx[m];
+    const uint32_t p = __ldg(b.primes + g);
+    const int32_t pinv = __ldg(b.qinvs + g);
+    const int32_t *T = jb.table + m * K;
+    uint32_t s[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int k0 = 0; k0 < 16; k0 += 4) {
+      if (k0 < K) {
+        int64_t acc[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int k = k0; k < k0 + 4; k++) {
+          if (k < K) {
+            const int64_t t = __ldg(T + k);
+#pragma unroll
+            for (int l = 0; l < 4; l++) acc[l] += static_cast<int64_t>(x[k][l]) * t;
+          }
+        }
+#pragma unroll
+        for (int l = 0; l < 4; l++) s[l] = add_mod(s[l], mont_reduce(acc[l], p, pinv), p);
+      }
+    }
+    st4(jb.out + static_cast<size_t>(jb.out_row[m]) * n + i0, s[0], s[1], s[2], s[3]);
+  }
+}
+
+// ---------------------------------------------------------------- key MAC
+__global__ void __launch_bounds__(256) k_key_mac(const __grid_constant__ KeyMacDesc d, int log_n) {
+  const int n = 1 << log_n;
+  const int r = blockIdx.y;
+  const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  if (i0 >= n) return;
+  const uint32_t q = d.q[r];
+  const int32_t qi = d.qinv[r];
+  const size_t off = static_cast<size_t>(r) * n + i0;
+  const size_t koff = static_cast<size_t>(d.key_row[r]) * n + i0;
+  uint32_t sb[4] = {0, 0, 0, 0}, sa[4] = {0, 0, 0, 0};
+  for (int i = 0; i < d.beta; i++) {
+    uint32_t mu[4], kb[4], ka[4];
+    unpack(ld4(d.mu[i] + off), mu);
+    unpack(ld4(d.kb[i] + koff), kb);
+    unpack(ld4(d.ka[i] + koff), ka);
+#pragma unroll
+    for (int l = 0; l < 4; l++) {
+      sb[l] = add_mod(sb[l], mont_mul(mu[l], kb[l], q, qi), q);
+      sa[l] = add_mod(sa[l], mont_mul(mu[l], ka[l], q, qi), q);
+    }
+  }
+  if (r < d.nq) {
+    const uint32_t pp = d.p_prod[r];
+    if (d.d0) {
+      uint32_t v[4];
+      unpack(ld4(d.d0 + off), v);
+#pragma unroll
+      for (int l = 0; l < 4; l++) sb[l] = add_mod(sb[l], mont_mul(v[l], pp, q, qi), q);
+    }
+    if (d.d1) {
+      uint32_t v[4];
+      unpack(ld4(d.d1 + off), v);
+#pragma unroll
+      for (int l = 0; l < 4; l++) sa[l] = add_mod(sa[l], mont_mul(v[l], pp, q, qi), q);
+    }
+  }
+  st4(d.acc_b + off, sb[0], sb[1], sb[2], sb[3]);
+  st4(d.acc_a + off, sa[0], sa[1], sa[2], sa[3]);
+}
+
+// ----------------------------------------------------------- element-wise
+template <ElemOp OP>
+__global__ void __launch_bounds__(256) k_elem(const __grid_constant__ ElemBatch eb, int log_n) {
+  const int n = 1 << log_n;
+  const ElemRow &e = eb.rows[blockIdx.y];
+  const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  if (i0 >= n) return;
+  const uint32_t q = e.q;
+  const int32_t qi = e.qinv;
+  uint32_t a[4], b[4], c[4], o[4];
+  unpack(ld4(e.a + i0), a);
+  if (OP == ElemOp::kAdd || OP == ElemOp::kSub || OP == ElemOp::kMult || OP == ElemOp::kMultAdd)
+    unpack(ld4(e.b + i0), b);
+  if (OP == ElemOp::kMultAdd || OP == ElemOp::kMultConstAdd) unpack(ld4(e.c + i0), c);
+#pragma unroll
+  for (int l = 0; l < 4; l++) {
+    switch (OP) {
+      case ElemOp::kAdd: o[l] = add_mod(a[l], b[l], q); break;
+      case ElemOp::kSub: o[l] = sub_mod(a[l], b[l], q); break;
+      case ElemOp::kNeg: o[l] = neg_mod(a[l], q); break;
+      case ElemOp::kMult: o[l] = mont_mul(a[l], b[l], q, qi); break;
+      case ElemOp::kAddConst: o[l] = add_mod(a[l], e.k, q); break;
+      case ElemOp::kSubConst: o[l] = sub_mod(a[l], e.k, q); break;
+      case ElemOp::kSubOppConst: o[l] = sub_mod(e.k, a[l], q); break;
+      case ElemOp::kMultConst: o[l] = mont_mul(a[l], e.k, q, qi); break;
+      case ElemOp::kCopy: o[l] = a[l]; break;
+      case ElemOp::kMultImagUnit: {
+        // X^(N/2) in the bit-reversed evaluation domain: +-psi^(N/2)
+        const uint32_t u = ((i0 + l) & (n >> 1)) ? q - e.k : e.k;
+        o[l] = mont_mul(a[l], u, q, qi);
+        break;
+      }
+      case ElemOp::kMultAdd: o[l] = add_mod(c[l], mont_mul(a[l], b[l], q, qi), q); break;
+      case ElemOp::kMultConstAdd: o[l] = add_mod(c[l], mont_mul(a[l], e.k, q, qi), q); break;
+    }
+  }
+  st4(e.dst + i0, o[0], o[1], o[2], o[3]);
+}
+
+__global__ void __launch_bounds__(256) k_tensor(const __grid_constant__ TensorBatch tb, int log_n) {
+  const int n = 1 << log_n;
+  const TensorRow &t = tb.rows[blockIdx.y];
+  const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  if (i0 >= n) return;
+  const uint32_t q = t.q;
+  const int32_t qi = t.qinv;
+  uint32_t b1[4], a1[4], b2[4], a2[4], o0[4], o1[4], o2[4];
+  unpack(ld4(t.b1 + i0), b1);
+  unpack(ld4(t.a1 + i0), a1);
+  unpack(ld4(t.b2 + i0), b2);
+  unpack(ld4(t.a2 + i0), a2);
+#pragma unroll
+  for (int l = 0; l < 4; l++) {
+    o0[l] = mont_mul(b1[l], b2[l], q, qi);
+    o2[l] = mont_mul(a1[l], a2[l], q, qi);
+    o1[l] = add_mod(mont_mul(b1[l], a2[l], q, qi), mont_mul(a1[l], b2[l], q, qi), q);
+  }
+  st4(t.d0 + i0, o0[0], o0[1], o0[2], o0[3]);
+  st4(t.d1 + i0, o1[0], o1[1], o1[2], o1[3]);
+  st4(t.d2 + i0, o2[0], o2[1], o2[2], o2[3]);
+}
+
+__device__ __forceinline__ uint32_t brev_bits(uint32_t x, int bits) { return __brev(x) >> (32 - bits); }
+
+// source index of the automorphism gather for destination k
+__device__ __forceinline__ uint32_t galois_src(uint32_t k, uint32_t g, int log_n) {
+  const int lb = log_n + 1;
+  const uint32_t e = (brev_bits(k, lb) + 1u) * g - 1u;
+  return brev_bits(e & ((1u << lb) - 1u), lb);
+}
+
+__global__ void __launch_bounds__(256) k_permute(const __grid_constant__ PermuteBatch pb, int log_n) {
+  const int n = 1 << log_n;
+  const PermuteRow &p = pb.rows[blockIdx.y];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  uint32_t v = __ldg(p.src + galois_src(k, pb.galois, log_n));
+  if (p.add) v = add_mod(v, __ldg(p.add + k), p.q);
+  p.dst[k] = v;
+}
+
+// Hoisted rotations (one launch for all R rotations).  Each thread loads the
+// beta ModUp values of its coefficient once, then for every rotation forms
+// the key inner products and scatters them through the inverse automorphism.
+__global__ void __launch_bounds__(256) k_hoisted(const __grid_constant__ HoistDesc d, int log_n) {
+  const int n = 1 << log_n;
+  const int r = blockIdx.y;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const uint32_t q = d.q[r];
+  const int32_t qi = d.qinv[r];
+  const size_t off = static_cast<size_t>(r) * n + k;
+  const size_t koff = static_cast<size_t>(d.key_row[r]) * n + k;
+  uint32_t mu[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+    if (i < d.beta) mu[i] = __ldg(d.mu[i] + off);
+  const uint32_t bxp = (r < d.nq) ? __ldg(d.bxp + off) : 0u;
+  for (int j = 0; j < d.R; j++) {
+    uint32_t sb = bxp, sa = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      if (i < d.beta) {
+        const uint32_t kb = __ldg(d.kb[j][i] + koff);
+        const uint32_t ka = __ldg(d.ka[j][i] + koff);
+        sb = add_mod(sb, mont_mul(mu[i], kb, q, qi), q);
+        sa = add_mod(sa, mont_mul(mu[i], ka, q, qi), q);
+      }
+    }
+    const uint32_t dk = galois_src(k, d.galois_inv[j], log_n);
+    const size_t o = static_cast<size_t>(r) * n + dk;
+    d.out_b[j][o] = sb;
+    d.out_a[j][o] = sa;
+  }
+}
+
+}  // namespace
+
+void launch_bconv(const BConvBatch &b, int log_n, cudaStream_t s) {
+  if (b.count <= 0) return;
+  const int n = 1 << log_n;
+  k_bconv<<<dim3((n / 4 + 255) / 256, b.count), 256, 0, s>>>(b, log_n);
+}
+
+void launch_key_mac(const KeyMacDesc &d, int log_n, cudaStream_t s) {
+  if (d.rows <= 0) return;
+  const int n = 1 << log_n;
+  k_key_mac<<<dim3((n / 4 + 255) / 256, d.rows), 256, 0, s>>>(d, log_n);
+}
+
+void launch_elementwise(ElemOp op, const ElemBatch &b, int log_n, cudaStream_t s) {
+  if (b.count <= 0) return;
+  const int n = 1 << log_n;
+  dim3 grid((n / 4 + 255) / 256, b.count);
+  switch (op) {
+#define CHD_CASE(OP) \
+  case OP: k_elem<OP><<<grid, 256, 0, s>>>(b, log_n); break;
+    CHD_CASE(ElemOp::kAdd)
+    CHD_CASE(ElemOp::kSub)
+    CHD_CASE(ElemOp::kNeg)
+    CHD_CASE(ElemOp::kMult)
+    CHD_CASE(ElemOp::kAddConst)
+    CHD_CASE(ElemOp::kSubConst)
+    CHD_CASE(ElemOp::kSubOppConst)
+    CHD_CASE(ElemOp::kMultConst)
+    CHD_CASE(ElemOp::kCopy)
+    CHD_CASE(ElemOp::kMultImagUnit)
+    CHD_CASE(ElemOp::kMultAdd)
+    CHD_CASE(ElemOp::kMultConstAdd)
+#undef CHD_CASE
+  }
+}
+
+void launch_tensor(const TensorBatch &b, int log_n, cudaStream_t s) {
+  if (b.count <= 0) return;
+  const int n = 1 << log_n;
+  k_tensor<<<dim3((n / 4 + 255) / 256, b.count), 256, 0, s>>>(b, log_n);
+}
+
+void launch_permute(const PermuteBatch &b, int log_n, cudaStream_t s) {
+  if (b.count <= 0) return;
+  const int n = 1 << log_n;
+  k_permute<<<dim3((n + 255) / 256, b.count), 256, 0, s>>>(b, log_n);
+}
+
+void launch_hoisted(const HoistDesc &d, int log_n, cudaStream_t s) {
+  if (d.rows <= 0 || d.R <= 0) return;
+  const int n = 1 << log_n;
+  k_hoisted<<<dim3((n + 255) / 256, d.rows), 256, 0, s>>>(d, log_n);
+}
+
+}  // namespace chd

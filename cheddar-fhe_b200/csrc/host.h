@@ -1,0 +1,215 @@
+// Host-side model of the CKKS evaluation core: parameter / level model,
+// per-level ModSwitch constants, device tables, device ciphertexts and keys,
+// and the evaluator that composes the CUDA kernels.  The public C ABI
+// (include/cheddar_b200.h) is a thin layer over this.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "kernels.h"
+
+namespace chd {
+
+// ---- errors ----------------------------------------------------------------
+enum Status : int {
+  kOk = 0,
+  kErrInvalidArg = 1,
+  kErrInvalidLevel = 2,
+  kErrShape = 3,
+  kErrCuda = 4,
+  kErrAlloc = 5,
+  kErrUnsupported = 6,
+  kErrKey = 7,
+  kErrParse = 8,
+};
+void set_error(const std::string &msg);
+const char *last_error();
+
+struct Error {
+  Status code;
+  std::string msg;
+};
+
+// ---- prime utilities ---------------------------------------------------------
+namespace prime {
+uint32_t mul_mod(uint32_t a, uint32_t b, uint32_t q);
+uint32_t pow_mod(uint32_t a, int64_t e, uint32_t q);
+uint32_t inv_mod(uint32_t a, uint32_t q);
+uint32_t smallest_generator(uint32_t q);
+uint32_t primitive_root(uint32_t m, uint32_t q);
+int32_t inv_mod_word(uint32_t q);
+uint32_t to_mont(uint32_t a, uint32_t q);
+int32_t centre(uint32_t a, uint32_t q);
+}  // namespace prime
+
+// ---- level model -------------------------------------------------------------
+struct NP {
+  int main = 0, ter = 0, aux = 0;
+  int q() const { return main + ter; }
+  int total() const { return main + ter + aux; }
+  bool operator==(const NP &o) const { return main == o.main && ter == o.ter && aux == o.aux; }
+};
+
+struct ParamSpec {
+  int log_degree = 16;
+  double base_scale = 0;
+  int default_encryption_level = 0;
+  std::vector<std::pair<int, int>> level_config;
+  std::vector<uint32_t> main_primes, aux_primes, ter_primes;
+  std::pair<int, int> additional_base{0, 0};
+  int dense_hw = -1, sparse_hw = 32;
+  bool boot = false;
+  int num_cts_levels = 0, num_stc_levels = 0;
+};
+
+// Parses the reference's parameter JSON schema.
+bool parse_param_json(const std::string &text, ParamSpec *out, std::string *err);
+
+class Params {
+ public:
+  static std::unique_ptr<Params> create(const ParamSpec &spec, std::string *err);
+
+  ParamSpec spec;
+  int log_n = 0, n = 0, L = 0, alpha = 0, max_ter = 0, max_main = 0, max_level = 0;
+  NP short_np;                   // level -1 base
+  std::vector<uint32_t> primes;  // global order: ter reversed, main, aux
+  std::vector<int32_t> qinv;
+  std::vector<int> galois;       // 5^i mod 2N, i in [0, N/2]
+  std::vector<double> scale, rescale_prod;
+
+  NP level_np(int level, int num_aux = 0) const;
+  int np_to_level(const NP &np) const;  // -2 if not a level
+  void gidx(const NP &np, int *out) const;
+  int sse_num_aux() const;
+  uint32_t galois_of(int amount) const;  // amount in [0, N/2] or -1
+};
+
+// Per-level ModSwitch constants (host and device copies).
+struct LevelMS {
+  int level = 0, num_aux = 0, beta = 0, num_q = 0;
+  std::vector<uint32_t> mod_up1;
+  std::vector<int> dig_s, dig_e;
+  std::vector<int32_t *> d_mod_up2;  // device [dst][src] per digit
+  std::vector<uint32_t> mod_down1, inv_p_prod;
+  int32_t *d_mod_down2 = nullptr;
+  bool has_rescale = false;
+  int pad_start = 0, pad_end = 0, restore_start = 0, restore_end = 0;
+  int rs_src_len = 0, mdr_src_len = 0, rs_dst_len = 0;
+  std::vector<uint32_t> rs1, rs_inv, rs_pad, mdr1, mdr_inv, mdr_pad;
+  int32_t *d_rs2 = nullptr, *d_mdr2 = nullptr;
+};
+
+// ---- device objects ----------------------------------------------------------
+struct DeviceCt {
+  NP np;
+  bool has_rx = false;
+  double scale = 1.0;
+  int num_slots = 0;
+  uint32_t *bx = nullptr, *ax = nullptr, *rx = nullptr;
+  size_t cap_words = 0;  // allocated words per part
+  bool owned = true;
+  ~DeviceCt();
+  Status reserve(const NP &np, bool rx, int n);
+};
+
+struct DeviceEvk {
+  int beta = 0;
+  NP np;  // key basis (all q primes + alpha aux primes)
+  uint32_t *bx = nullptr, *ax = nullptr;  // [beta][np.total][N]
+  bool owned = true;
+  ~DeviceEvk();
+};
+
+// Stack arena over device memory: chunks are never moved, so pointers handed
+// out during an operation stay valid until the matching release.
+class Arena {
+ public:
+  ~Arena();
+  void *alloc(size_t bytes);
+  size_t mark() const { return top_; }
+  void release(size_t m);
+
+ private:
+  struct Chunk {
+    char *p;
+    size_t size;
+    size_t start;  // global offset of this chunk
+  };
+  std::vector<Chunk> chunks_;
+  size_t top_ = 0;   // global offset
+  size_t total_ = 0;
+};
+
+class Context {
+ public:
+  static std::unique_ptr<Context> create(const ParamSpec &spec, int device, std::string *err);
+  ~Context();
+
+  std::unique_ptr<Params> P;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  Arena arena;
+
+  // device tables
+  uint32_t *d_primes = nullptr;
+  int32_t *d_qinv = nullptr;
+  uint32_t *d_tw = nullptr, *d_itw = nullptr;  // [nprimes][N]
+  std::vector<uint32_t> n_inv, n_inv_mont, mont_conv, p_prod, imag_unit;
+  std::vector<LevelMS> ms;  // index level + 1
+
+  const LevelMS &lms(int level) const { return ms.at(level + 1); }
+  const uint32_t *tw(int g) const { return d_tw + (static_cast<size_t>(g) << P->log_n); }
+  const uint32_t *itw(int g) const { return d_itw + (static_cast<size_t>(g) << P->log_n); }
+
+  // ---- building blocks on raw device pointers ----
+  // NTT of the limbs of np stored contiguously at data (in place)
+  Status ntt(const NP &np, uint32_t *data, bool mont, int count = 1, size_t stride = 0);
+  Status intt(const NP &np, uint32_t *data, bool mont, int count = 1, size_t stride = 0);
+  // ModUp of src [num_q][N] at `level` into dst[beta] ([num_q + aux][N] each)
+  Status modup(int level, const uint32_t *src, uint32_t *const *dst);
+  enum class MDType { kModDown, kRescale, kModDownRescale };
+  // ModDown family on npoly polys
+  Status moddown(int level, MDType type, const uint32_t *const *src, uint32_t *const *dst, int npoly);
+  Status bconv(const int32_t *xt, int K, const int32_t *table, const int *dst_gidx, int M, uint32_t *out);
+
+  // ---- evaluator (Context.cpp of the reference) ----
+  Status add(DeviceCt &res, const DeviceCt &a, const DeviceCt &b);
+  Status sub(DeviceCt &res, const DeviceCt &a, const DeviceCt &b);
+  Status neg(DeviceCt &res, const DeviceCt &a);
+  Status mult_tensor(DeviceCt &res, const DeviceCt &a, const DeviceCt &b);
+  Status mult_const(DeviceCt &res, const DeviceCt &a, const uint32_t *cx, double cscale);
+  Status add_const(DeviceCt &res, const DeviceCt &a, const uint32_t *cx);
+  Status mult_plain(DeviceCt &res, const DeviceCt &a, const uint32_t *pt_dev, double pscale);
+  Status mult_imag_unit(DeviceCt &res, const DeviceCt &a);
+  Status rescale(DeviceCt &res, const DeviceCt &a);
+  Status relinearize(DeviceCt &res, const DeviceCt &a, const DeviceEvk &key, bool rescale);
+  Status hmult(DeviceCt &res, const DeviceCt &a, const DeviceCt &b, const DeviceEvk &key, bool rescale);
+  Status hmult_batch(int count, DeviceCt *const *res, const DeviceCt *const *a, const DeviceCt *const *b,
+                     const DeviceEvk &key, bool rescale);
+  Status mult_key(DeviceCt &res, const DeviceCt &a, const DeviceEvk &key);
+  Status permute(DeviceCt &res, const DeviceCt &a, int amount);
+  Status hrot(DeviceCt &res, const DeviceCt &a, const DeviceEvk &key, int dist);
+  Status hconj(DeviceCt &res, const DeviceCt &a, const DeviceEvk &key);
+  Status hrot_add(DeviceCt &res, const DeviceCt &a, const DeviceCt &b, const DeviceEvk &key, int dist);
+  // hoisted baby-step rotations, outputs stay in the Q u P basis
+  Status hoisted_rotate(const DeviceCt &a, int R, const int *dists, const DeviceEvk *const *keys,
+                        DeviceCt *const *out);
+  // ModDown of a Q u P ciphertext back to Q
+  Status moddown_ct(DeviceCt &res, const DeviceCt &a);
+
+ private:
+  Status init(const ParamSpec &spec, int dev, std::string *err);
+  Status check_cuda(const char *where);
+  // key-switch core: accum = sum_i ModUp(d_in)_i (.) key_i (+ P*(d0,d1))
+  Status key_switch_core(int level, const uint32_t *d0, const uint32_t *d1, const uint32_t *d_in,
+                         const DeviceEvk &key, uint32_t *acc_b, uint32_t *acc_a);
+};
+
+}  // namespace chd

@@ -1,0 +1,159 @@
+// Kernel launch interface shared by the host orchestration (context.cu) and
+// the CUDA translation units.  All launches are asynchronous on the given
+// stream; all row descriptors travel by value in the kernel parameters, so
+// launches need no host-to-device copies and can be captured in CUDA graphs.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace chd {
+
+// One limb (N residues of one prime) processed by a batched kernel.
+struct RowDesc {
+  const uint32_t *src;   // input limb
+  uint32_t *dst;         // output limb (may equal src for in-place phases)
+  const uint32_t *src2;  // second input (ModDown epilogue), or nullptr
+  const uint32_t *tw;    // twiddle table of this prime (N words)
+  uint32_t q;            // prime
+  int32_t qinv;          // q^-1 mod 2^32
+  uint32_t c0;           // pre-multiplier (forward NTT) / epilogue constant (INTT)
+  uint32_t c1;           // ModDown epilogue: src2 padding multiplier
+  uint32_t c2;           // ModDown epilogue: (prod src primes)^-1 (Montgomery)
+  uint32_t flags;        // see RowFlags
+};
+
+enum RowFlags : uint32_t {
+  kPreMult = 1u,       // forward NTT: multiply input by c0 (Montgomery) first
+  kCentre = 2u,        // inverse NTT: write the centred representative
+  kHasSrc2 = 4u,       // ModDown epilogue: src2 exists for this row
+  kPadSrc2 = 8u,       // ModDown epilogue: multiply src2 by c1 first
+  kModDownEpi = 16u,   // forward NTT row phase: apply (src2*c1 - x) * c2
+};
+
+constexpr int kMaxRows = 120;
+
+struct RowBatch {
+  int count;
+  RowDesc rows[kMaxRows];
+};
+
+// Forward negacyclic NTT (bit-reversed output) of `count` limbs.
+// Column phase then row phase for log_n = 16; a single-kernel shared-memory
+// transform for log_n <= 15.  In-place allowed (dst == src).
+void launch_ntt_fwd(const RowBatch &rb, int log_n, cudaStream_t s);
+// Row phase only / column phase only (used by fused pipelines and tests)
+void launch_ntt_fwd_cols(const RowBatch &rb, int log_n, cudaStream_t s);
+void launch_ntt_fwd_rows(const RowBatch &rb, int log_n, cudaStream_t s);
+// Inverse NTT (bit-reversed input); epilogue x * c0 (Montgomery), canonical
+// or centred (kCentre).  tw must point at the inverse twiddle table.
+void launch_ntt_inv(const RowBatch &rb, int log_n, cudaStream_t s);
+
+// Base conversion of one job: out[m][n] = (sum_k xt[k][n] * T[m][k]) * 2^-32
+// mod p_m.  xt holds K consecutive centred limbs; destination limb m is
+// row out_row[m] of `out` and uses the prime of global index out_gidx[m].
+struct BConvJob {
+  const int32_t *xt;
+  uint32_t *out;
+  const int32_t *table;  // device [M][K] centred constants
+  int K, M;
+  uint8_t out_row[64];
+  uint8_t out_gidx[64];
+};
+constexpr int kMaxBConvJobs = 24;
+struct BConvBatch {
+  int count;
+  const uint32_t *primes;  // device table of all primes (by global index)
+  const int32_t *qinvs;
+  BConvJob jobs[kMaxBConvJobs];
+};
+void launch_bconv(const BConvBatch &b, int log_n, cudaStream_t s);
+
+// Key-switching inner product with the P * (d0, d1) term folded in:
+//   acc_b[r] = sum_i mu_i[r] * kb_i[r] + (r < nq ? p_prod[r] * d0[r] : 0)
+//   acc_a[r] = sum_i mu_i[r] * ka_i[r] + (r < nq && d1 ? p_prod[r] * d1[r] : 0)
+struct KeyMacDesc {
+  const uint32_t *mu[8];     // beta ModUp outputs, each [rows][N]
+  const uint32_t *kb[8];     // key bx of digit i, row-0 pointer of the key basis
+  const uint32_t *ka[8];
+  const uint32_t *d0, *d1;   // [nq][N] or nullptr
+  uint32_t *acc_b, *acc_a;   // [rows][N]
+  uint32_t q[64];
+  int32_t qinv[64];
+  uint32_t p_prod[64];       // Montgomery P mod q, q rows only
+  int16_t key_row[64];       // key basis row of accumulator row r
+  int beta, rows, nq;
+};
+void launch_key_mac(const KeyMacDesc &d, int log_n, cudaStream_t s);
+
+// Element-wise kernels over a list of limbs (same op for every limb).
+enum class ElemOp : int {
+  kAdd, kSub, kNeg, kMult, kAddConst, kSubConst, kSubOppConst, kMultConst,
+  kCopy, kMultImagUnit, kMultAdd, kMultConstAdd
+};
+struct ElemRow {
+  const uint32_t *a, *b;  // inputs (b unused for unary)
+  const uint32_t *c;      // accumulator input for kMultAdd / kMultConstAdd
+  uint32_t *dst;
+  uint32_t q;
+  int32_t qinv;
+  uint32_t k;             // per-limb constant
+};
+constexpr int kMaxElemRows = 96;
+struct ElemBatch {
+  int count;
+  ElemRow rows[kMaxElemRows];
+};
+void launch_elementwise(ElemOp op, const ElemBatch &b, int log_n, cudaStream_t s);
+
+// Tensor product of (b1, a1) x (b2, a2) -> (d0, d1, d2) (Karatsuba form)
+struct TensorRow {
+  const uint32_t *b1, *a1, *b2, *a2;
+  uint32_t *d0, *d1, *d2;
+  uint32_t q;
+  int32_t qinv;
+};
+struct TensorBatch {
+  int count;
+  TensorRow rows[64];
+};
+void launch_tensor(const TensorBatch &b, int log_n, cudaStream_t s);
+
+// Automorphism X -> X^g in the bit-reversed evaluation domain (gather):
+// dst[k] = src[brev(((2 brev(k) + 1) g - 1) mod 2N)]
+struct PermuteRow {
+  const uint32_t *src;
+  uint32_t *dst;
+  const uint32_t *add;  // optional addend (PermuteAccum with src0)
+  uint32_t q;
+};
+struct PermuteBatch {
+  int count;
+  uint32_t galois;
+  PermuteRow rows[64];
+};
+void launch_permute(const PermuteBatch &b, int log_n, cudaStream_t s);
+
+// Hoisted rotations: one launch for up to kMaxHoist rotations of one ModUp'ed
+// input.  For every rotation j and row r of the extended basis Q u P:
+//   v = sum_i mu_i[r] (.) key_j,i[r]  (+ P * bx[r] on q rows for the b part)
+// scattered through the automorphism: out_j[galois_src(k, g_j)] = v[k] with
+// g_j the Galois factor of N/2 - r_j (the inverse of rotation r_j).
+constexpr int kMaxHoist = 32;
+struct HoistDesc {
+  const uint32_t *mu[8];
+  const uint32_t *bxp;                   // P * bx on q rows, [nq][N]
+  const uint32_t *kb[kMaxHoist][8];      // key row-0 pointers per rotation/digit
+  const uint32_t *ka[kMaxHoist][8];
+  uint32_t *out_b[kMaxHoist];            // outputs [rows][N]
+  uint32_t *out_a[kMaxHoist];
+  uint32_t galois_inv[kMaxHoist];
+  uint32_t q[64];
+  int32_t qinv[64];
+  int16_t key_row[64];
+  int beta, rows, nq, R;
+};
+void launch_hoisted(const HoistDesc &d, int log_n, cudaStream_t s);
+
+}  // namespace chd

@@ -1,0 +1,178 @@
+/*
+ * cheddar_b200.h — C ABI of the B200-native CKKS evaluation core.
+ *
+ * Each entry point replaces one call of the reference's server-side C++ API
+ * (scale-snu/cheddar-fhe); the reference interface is cited beside it.
+ * Plain pointers and sizes only.  Every function returns CHD_OK (0) or an
+ * error code; chd_last_error() describes the last failure of the calling
+ * thread.  (The reference terminates the process on any failed assertion,
+ * include/common/Assert.h:9-21; this ABI reports instead.)
+ *
+ * Data layout (reference include/core/Parameter.h:198-206): a polynomial is
+ * [num_primes][N] uint32 residues, prime order = terminal primes reversed,
+ * main primes, auxiliary primes; every residue canonical in [0, q), in the
+ * bit-reversed evaluation domain and in Montgomery form (x * 2^32 mod q).
+ * Evaluation keys are beta pairs (bx, ax), each over the key basis of all
+ * L = main + terminal primes followed by the alpha auxiliary primes.
+ *
+ * Threading: a context is not re-entrant; all its work is ordered on one CUDA
+ * stream (chd_context_set_stream).  Calls return before the GPU finishes;
+ * chd_ct_export and chd_context_synchronize wait.
+ */
+#ifndef CHEDDAR_B200_H_
+#define CHEDDAR_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CHD_OK 0
+#define CHD_ERR_INVALID_ARG 1
+#define CHD_ERR_INVALID_LEVEL 2
+#define CHD_ERR_SHAPE 3
+#define CHD_ERR_CUDA 4
+#define CHD_ERR_ALLOC 5
+#define CHD_ERR_UNSUPPORTED 6
+#define CHD_ERR_KEY 7
+#define CHD_ERR_PARSE 8
+
+/* ModDown family selector for chd_moddown_raw */
+#define CHD_MODDOWN 0
+#define CHD_RESCALE 1
+#define CHD_MODDOWN_RESCALE 2
+
+typedef struct chd_context chd_context;
+typedef struct chd_ciphertext chd_ciphertext;
+typedef struct chd_evk chd_evk;
+
+const char *chd_last_error(void);
+
+/* ---- context ------------------------------------------------------------ */
+/* Parameter JSON of the reference schema (unittest/Testbed.h:95-221) ->
+ * Parameter(...) (include/core/Parameter.h:42-47) + Context::Create
+ * (include/core/Context.h:70). */
+int chd_context_create_json(const char *json_text, int device, chd_context **out);
+/* Parameter(log_degree, base_scale, default_encryption_level, level_config,
+ * main_primes, aux_primes, ter_primes, additional_base) + Context::Create
+ * (include/core/Parameter.h:42-47, include/core/Context.h:70).
+ * level_config holds num_levels (num_main, num_ter) pairs. */
+int chd_context_create(int log_degree, double base_scale, int default_encryption_level,
+                       const int *level_config, int num_levels, const uint32_t *main_primes,
+                       int num_main, const uint32_t *aux_primes, int num_aux,
+                       const uint32_t *ter_primes, int num_ter, int additional_main,
+                       int additional_ter, int device, chd_context **out);
+void chd_context_destroy(chd_context *ctx);
+/* Orders all later work of ctx on the given cudaStream_t (NULL: the
+ * context's own non-blocking stream).  No reference counterpart: the
+ * reference uses the legacy default stream only (src/core/DeviceVector.cpp:68). */
+int chd_context_set_stream(chd_context *ctx, void *cuda_stream);
+int chd_context_synchronize(chd_context *ctx);
+/* Parameter::LevelToNP (include/core/Parameter.h:184) */
+int chd_level_np(const chd_context *ctx, int level, int *num_main, int *num_ter);
+/* Parameter::max_level_, degree_, alpha_, L_ (include/core/Parameter.h:56-64) */
+int chd_max_level(const chd_context *ctx);
+int chd_degree(const chd_context *ctx);
+int chd_alpha(const chd_context *ctx);
+int chd_num_q_primes(const chd_context *ctx);
+/* Parameter::GetScale / GetRescalePrimeProd (include/core/Parameter.h:86-100) */
+double chd_scale(const chd_context *ctx, int level);
+double chd_rescale_prime_prod(const chd_context *ctx, int level);
+/* global index (max-level order) of every prime of an np; returns the count */
+int chd_prime_gidx(const chd_context *ctx, int num_main, int num_ter, int num_aux, int *out);
+
+/* ---- ciphertexts (include/core/Container.h:131-218) ------------------------ */
+int chd_ct_create(chd_context *ctx, chd_ciphertext **out);
+void chd_ct_destroy(chd_ciphertext *ct);
+/* Wraps caller-owned device buffers (each words_per_part uint32 long). */
+int chd_ct_wrap(chd_context *ctx, int num_main, int num_ter, int num_aux, int has_rx, double scale,
+                int num_slots, uint32_t *bx, uint32_t *ax, uint32_t *rx, size_t words_per_part,
+                chd_ciphertext **out);
+/* Copies residues in ([num_q + num_aux][N] per part).  src_on_device: the
+ * pointers are device pointers (else host). */
+int chd_ct_import(chd_context *ctx, chd_ciphertext *ct, int num_main, int num_ter, int num_aux,
+                  int has_rx, double scale, int num_slots, const uint32_t *bx, const uint32_t *ax,
+                  const uint32_t *rx, int src_on_device);
+int chd_ct_export(chd_context *ctx, const chd_ciphertext *ct, uint32_t *bx, uint32_t *ax,
+                  uint32_t *rx, int dst_on_device);
+/* Ciphertext::GetNP / HasRx / GetScale / GetNumSlots */
+int chd_ct_info(const chd_ciphertext *ct, int *num_main, int *num_ter, int *num_aux, int *has_rx,
+                double *scale, int *num_slots);
+/* device pointers of the parts (valid until the ciphertext changes shape) */
+int chd_ct_device_ptrs(const chd_ciphertext *ct, uint32_t **bx, uint32_t **ax, uint32_t **rx);
+
+/* ---- evaluation keys (include/core/Container.h:283-344, EvkMap.h:23-26) --- */
+/* beta pairs over [L + alpha][N]: bx and ax each beta * (L+alpha) * N words */
+int chd_evk_create(chd_context *ctx, int beta, const uint32_t *bx, const uint32_t *ax,
+                   int src_on_device, chd_evk **out);
+void chd_evk_destroy(chd_evk *evk);
+
+/* ---- evaluator (include/core/Context.h:101-423) ----------------------------- */
+int chd_add(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_ciphertext *b);
+int chd_sub(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_ciphertext *b);
+int chd_neg(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a);
+/* Context::Mult(Ct, Ct, Ct): tensor product, result carries rx */
+int chd_mult(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_ciphertext *b);
+/* Context::Mult(Ct, Ct, Const) / Add(Ct, Ct, Const): cx = one Montgomery word
+ * per prime of a's np (host pointer) */
+int chd_mult_const(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a,
+                   const uint32_t *cx, double const_scale);
+int chd_add_const(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *cx);
+/* Context::Mult(Ct, Ct, Pt): pt_dev = [num_q][N] device residues */
+int chd_mult_plain(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a,
+                   const uint32_t *pt_dev, double pt_scale);
+int chd_mult_imaginary_unit(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a);
+int chd_rescale(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a);
+int chd_relinearize(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *key);
+int chd_relinearize_rescale(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a,
+                            const chd_evk *key);
+int chd_mult_key(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *key);
+/* Context::HMult(res, a, b, mult_key, rescale) (Context.cpp:862-871) */
+int chd_hmult(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a,
+              const chd_ciphertext *b, const chd_evk *mult_key, int rescale);
+/* Batched HMult over count independent pairs (no reference counterpart; the
+ * reference exposes one HMult per call) */
+int chd_hmult_batch(chd_context *ctx, int count, chd_ciphertext *const *res,
+                    const chd_ciphertext *const *a, const chd_ciphertext *const *b,
+                    const chd_evk *mult_key, int rescale);
+/* Context::HRot / HConj / HRotAdd (Context.cpp:776-830) */
+int chd_hrot(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *rot_key,
+             int rot_dist);
+int chd_hconj(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *conj_key);
+int chd_hrot_add(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a,
+                 const chd_ciphertext *b, const chd_evk *rot_key, int rot_dist);
+/* HoistHandler::EvaluateBabyStep with the fused key-mult
+ * (src/extension/Hoist.cu:578-691): count rotations of a in one launch,
+ * results left in the extended basis (num_aux = alpha). */
+int chd_hoisted_rotate(chd_context *ctx, const chd_ciphertext *a, int count, const int *rot_dists,
+                       const chd_evk *const *rot_keys, chd_ciphertext *const *out);
+/* ModSwitchHandler::ModDown of an extended-basis ciphertext (ModSwitch.cu:511-527) */
+int chd_moddown(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a);
+
+/* ---- raw kernels on device buffers (parity entry points) -------------------- */
+/* NTTHandler::NTT / INTT (include/core/NTT.h:55-62): count consecutive
+ * polynomials of np, in place. */
+int chd_ntt(chd_context *ctx, int num_main, int num_ter, int num_aux, uint32_t *data_dev, int mont,
+            int count);
+int chd_intt(chd_context *ctx, int num_main, int num_ter, int num_aux, uint32_t *data_dev, int mont,
+             int count);
+/* ModSwitchHandler::ModUp (ModSwitch.cu:429-509): src [num_q][N] ->
+ * dst [beta][num_q + alpha][N] */
+int chd_modup_raw(chd_context *ctx, int level, const uint32_t *src_dev, uint32_t *dst_dev);
+/* ModSwitchHandler::ModDown / Rescale / ModDownAndRescale (ModSwitch.cu:511-564)
+ * on npoly consecutive polynomials */
+int chd_moddown_raw(chd_context *ctx, int level, int type, const uint32_t *src_dev, uint32_t *dst_dev,
+                    int npoly);
+/* kernel::ModSwitchMatrixMult (ModSwitch.cu:23-171): K centred source limbs
+ * (global prime indices src_gidx) -> M limbs (dst_gidx), table
+ * T[m][k] = centre(prod_{j != k} src_j * 2^64 mod dst_m). */
+int chd_bconv_raw(chd_context *ctx, const int32_t *xt_dev, const int *src_gidx, int K,
+                  const int *dst_gidx, int M, uint32_t *out_dev);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CHEDDAR_B200_H_ */

@@ -1,0 +1,154 @@
+"""GPU evaluator (HMult, relinearise, rescale, key switching, rotations,
+conjugation, hoisted rotations, element-wise ops) against the oracle,
+bit-exact on identical injected residues; decoded precision checked with the
+reference's criterion (every slot within 1e-3, unittest/Testbed.h:93)."""
+import numpy as np
+import pytest
+
+from gpu_common import fresh_ct, mult_key, pair, rot_key, secret, uniform_parts
+
+pytestmark = pytest.mark.gpu
+KS = "keyswitch_l24_a8.json"
+
+
+def _eq(gpu_ct, ref_parts):
+    parts = gpu_ct.numpy()
+    assert len(parts) >= len(ref_parts)
+    for a, b in zip(parts, ref_parts):
+        assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("level,rescale", [(22, True), (22, False), (13, True), (1, True)])
+def test_hmult_bit_exact(cuda_ok, level, rescale):
+    o, g = pair(KS)
+    (kb, ka), key = mult_key(KS)
+    a = uniform_parts(KS, level, 100 + level)
+    b = uniform_parts(KS, level, 200 + level)
+    ga = g.import_ct(level, a)
+    gb = g.import_ct(level, b)
+    res = g.HMult(ga, gb, key, rescale=rescale)
+    _eq(res, o.hmult(level, a, b, (kb, ka), rescale=rescale))
+
+
+def test_hmult_inplace_and_batch(cuda_ok):
+    o, g = pair(KS)
+    (kb, ka), key = mult_key(KS)
+    lvl = 20
+    pairs = [(uniform_parts(KS, lvl, 300 + i), uniform_parts(KS, lvl, 400 + i)) for i in range(3)]
+    ga = [g.import_ct(lvl, a) for a, _ in pairs]
+    gb = [g.import_ct(lvl, b) for _, b in pairs]
+    outs = g.HMultBatch(ga, gb, key, rescale=True)
+    for (a, b), r in zip(pairs, outs):
+        _eq(r, o.hmult(lvl, a, b, (kb, ka), rescale=True))
+    # in place: res aliases the first operand
+    g.HMult(ga[0], gb[0], key, rescale=True, res=ga[0])
+    _eq(ga[0], o.hmult(lvl, pairs[0][0], pairs[0][1], (kb, ka), rescale=True))
+
+
+def test_hmult_decoded_precision(cuda_ok):
+    o, g = pair(KS)
+    (kb, ka), key = mult_key(KS)
+    s = secret(KS)
+    lvl = o.max_level
+    c1, sc, m1 = fresh_ct(KS, lvl, 1)
+    c2, _, m2 = fresh_ct(KS, lvl, 2)
+    r = g.HMult(g.import_ct(lvl, c1, sc), g.import_ct(lvl, c2, sc), key, rescale=True)
+    info = r.info()
+    assert info["num_main"] == o.level_np(lvl - 1)[0]
+    assert abs(info["scale"] - sc * sc / o.rescale_prime_prod(lvl)) < 1e-6 * info["scale"]
+    dec = o.decode(lvl - 1, info["scale"], o.decrypt(s, lvl - 1, r.numpy()), o.n // 2)
+    err = np.abs(dec - m1 * m2).max()
+    assert err < 1e-3, err
+
+
+@pytest.mark.parametrize("level", [22, 9])
+def test_relinearize_and_rescale(cuda_ok, level):
+    o, g = pair(KS)
+    (kb, ka), key = mult_key(KS)
+    a = uniform_parts(KS, level, 500 + level)
+    b = uniform_parts(KS, level, 600 + level)
+    t = g.Mult(g.import_ct(level, a), g.import_ct(level, b))
+    d0, d1, d2 = o.tensor(level, a[0], a[1], b[0], b[1])
+    _eq(t, [d0, d1, d2])
+    _eq(g.Relinearize(t, key), o.hmult(level, a, b, (kb, ka), rescale=False))
+    _eq(g.RelinearizeRescale(t, key), o.hmult(level, a, b, (kb, ka), rescale=True))
+    r = g.Rescale(g.import_ct(level, a))
+    _eq(r, list(o.rescale_ct(level, np.stack(a))))
+
+
+@pytest.mark.parametrize("rot", [1, 5, 1234, 16384, 32767])
+def test_hrot_bit_exact(cuda_ok, rot):
+    o, g = pair(KS)
+    (kb, ka), key = rot_key(KS, rot)
+    lvl = 21
+    a = uniform_parts(KS, lvl, 700)
+    _eq(g.HRot(g.import_ct(lvl, a), key, rot), o.hrot(lvl, a, (kb, ka), rot))
+
+
+def test_hconj_and_multkey(cuda_ok):
+    o, g = pair(KS)
+    (kb, ka), key = rot_key(KS, -1)
+    lvl = 22
+    a = uniform_parts(KS, lvl, 800)
+    ga = g.import_ct(lvl, a)
+    _eq(g.HConj(ga, key), o.hconj(lvl, a, (kb, ka)))
+    _eq(g.MultKey(ga, key), o.mult_key(lvl, a, (kb, ka)))
+
+
+def test_hrot_decoded(cuda_ok):
+    o, g = pair(KS)
+    s = secret(KS)
+    lvl = 22
+    c, sc, m = fresh_ct(KS, lvl, 3)
+    (kb, ka), key = rot_key(KS, 3)
+    r = g.HRot(g.import_ct(lvl, c, sc), key, 3)
+    dec = o.decode(lvl, sc, o.decrypt(s, lvl, r.numpy()), o.n // 2)
+    assert np.abs(dec - np.roll(m, -3)).max() < 1e-3
+    b, _, mb = fresh_ct(KS, lvl, 4)
+    r2 = g.HRotAdd(g.import_ct(lvl, c, sc), g.import_ct(lvl, b, sc), key, 3)
+    dec = o.decode(lvl, sc, o.decrypt(s, lvl, r2.numpy()), o.n // 2)
+    assert np.abs(dec - (np.roll(m, -3) + mb)).max() < 1e-3
+
+
+def test_hoisted_rotations(cuda_ok):
+    """30 distinct offsets: +-2^k (k < 15) and 1..4, in one hoisted launch;
+    equals the oracle's hoisted result and, after ModDown, per-offset HRot."""
+    o, g = pair(KS)
+    lvl = o.max_level
+    half = o.n // 2
+    offs = sorted({(s * (1 << k)) % half for k in range(15) for s in (1, -1)} | {1, 2, 3, 4})
+    offs = [r for r in offs if r != 0]
+    assert len(offs) == 30
+    a = uniform_parts(KS, lvl, 900)
+    keys = [rot_key(KS, r) for r in offs]
+    ga = g.import_ct(lvl, a)
+    outs = g.HoistedRotate(ga, [k[1] for k in keys], offs)
+    hb, ha = o.hoisted_rotate(lvl, a, [k[0] for k in keys], offs)
+    for i in range(len(offs)):
+        _eq(outs[i], [hb[i], ha[i]])
+    for i in (0, 7, 29):
+        md = g.ModDown(outs[i])
+        _eq(md, o.hrot(lvl, a, keys[i][0], offs[i]))
+
+
+def test_elementwise_ops(cuda_ok):
+    o, g = pair(KS)
+    lvl = 10
+    a = uniform_parts(KS, lvl, 1000)
+    b = uniform_parts(KS, lvl, 1001)
+    primes = o.primes(lvl).astype(np.uint64)[:, None]
+    ga, gb = g.import_ct(lvl, a), g.import_ct(lvl, b)
+    A = [x.astype(np.uint64) for x in a]
+    B = [x.astype(np.uint64) for x in b]
+    _eq(g.Add(ga, gb), [((x + y) % primes).astype(np.uint32) for x, y in zip(A, B)])
+    _eq(g.Sub(ga, gb), [((x + primes - y) % primes).astype(np.uint32) for x, y in zip(A, B)])
+    _eq(g.Neg(ga), [((primes - x) % primes).astype(np.uint32) for x in A])
+    _eq(g.MultImaginaryUnit(ga), [o.mult_imag_unit(lvl, x) for x in a])
+    cx = o.encode_const(lvl, 2.0 ** 20, 0.75)
+    r = g.MultConst(ga, cx, 2.0 ** 20)
+    Rinv = [pow(1 << 32, -1, int(p)) for p in primes[:, 0]]
+    ref = [np.stack([(x[i].astype(object) * int(cx[i]) * Rinv[i]) % int(primes[i, 0])
+                     for i in range(len(cx))]).astype(np.uint32) for x in A]
+    _eq(r, ref)
+    r = g.AddConst(ga, cx)
+    _eq(r, [((A[0] + cx.astype(np.uint64)[:, None]) % primes).astype(np.uint32), a[1]])
