@@ -507,4 +507,62 @@ int chd_bconv_raw(chd_context *ctx, const int32_t *xt_dev, const int *src_gidx, 
   return rc;
 }
 
+int chd_params_level_consts(const char *json_text, int level, int kind, int digit, uint32_t *c1, int32_t *table,
+                            uint32_t *inv, uint32_t *pad, int *dims) {
+  CHD_NOTNULL(json_text);
+  CHD_NOTNULL(dims);
+  ParamSpec spec;
+  std::string err;
+  if (!parse_param_json(json_text, &spec, &err)) return fail(CHD_ERR_PARSE, err);
+  auto P = Params::create(spec, &err);
+  if (!P) return fail(CHD_ERR_INVALID_ARG, err);
+  if (level < -1 || level > P->max_level) return fail(CHD_ERR_INVALID_LEVEL, "invalid level");
+  LevelMS m;
+  build_level_ms(*P, level, &m);
+  const std::vector<uint32_t> *v1 = nullptr, *vi = nullptr, *vp = nullptr;
+  const std::vector<int32_t> *vt = nullptr;
+  int K = 0, M = 0;
+  dims[3] = m.restore_start;
+  dims[4] = m.restore_end;
+  dims[5] = m.beta;
+  switch (kind) {
+    case 0: {  // ModUp digit
+      if (digit < 0 || digit >= m.beta) return fail(CHD_ERR_INVALID_ARG, "invalid digit");
+      K = m.dig_e[digit] - m.dig_s[digit];
+      if (K <= 0) {
+        dims[0] = dims[1] = dims[2] = 0;
+        return CHD_OK;
+      }
+      M = m.num_q + m.num_aux - K;
+      for (int i = 0; i < K; i++) c1[i] = m.mod_up1[m.dig_s[digit] + i];
+      vt = &m.mod_up2[digit];
+      break;
+    }
+    case 1:
+      v1 = &m.mod_down1, vt = &m.mod_down2, vi = &m.inv_p_prod;
+      K = m.num_aux, M = m.num_q;
+      break;
+    case 2:
+    case 3:
+      if (!m.has_rescale) return fail(CHD_ERR_INVALID_LEVEL, "no rescale at this level");
+      v1 = kind == 2 ? &m.rs1 : &m.mdr1;
+      vt = kind == 2 ? &m.rs2 : &m.mdr2;
+      vi = kind == 2 ? &m.rs_inv : &m.mdr_inv;
+      vp = kind == 2 ? &m.rs_pad : &m.mdr_pad;
+      K = kind == 2 ? m.rs_src_len : m.mdr_src_len;
+      M = m.rs_dst_len;
+      break;
+    default:
+      return fail(CHD_ERR_INVALID_ARG, "invalid kind");
+  }
+  dims[0] = K;
+  dims[1] = M;
+  dims[2] = vp ? static_cast<int>(vp->size()) : 0;
+  if (v1 && c1) std::copy(v1->begin(), v1->end(), c1);
+  if (vt && table) std::copy(vt->begin(), vt->end(), table);
+  if (vi && inv) std::copy(vi->begin(), vi->end(), inv);
+  if (vp && pad) std::copy(vp->begin(), vp->end(), pad);
+  return CHD_OK;
+}
+
 }  // extern "C"

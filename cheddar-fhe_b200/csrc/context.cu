@@ -618,6 +618,79 @@ int32_t *upload_i32(const std::vector<int32_t> &v) {
 }
 }  // namespace
 
+void build_level_ms(const Params &P, int level, LevelMS *out) {
+  // ModSwitch.cu:175-318 of the reference
+  LevelMS &m = *out;
+  const uint32_t n = static_cast<uint32_t>(P.n);
+  m.level = level;
+  m.num_aux = level == -1 ? P.sse_num_aux() : P.alpha;
+  NP np = P.level_np(level, m.num_aux);
+  const int nq = np.q(), tot = np.total();
+  m.num_q = nq;
+  m.beta = level == -1 ? 1 : (np.main + P.max_ter + m.num_aux - 1) / m.num_aux;
+  std::vector<int> g(tot);
+  P.gidx(np, g.data());
+  std::vector<uint32_t> lp(tot);
+  for (int i = 0; i < tot; i++) lp[i] = P.primes[g[i]];
+  const int padded = level == -1 ? nq : np.main + P.max_ter;
+  const int npad = padded - nq;
+  m.mod_up1.assign(nq, 0);
+  m.dig_s.assign(m.beta, 0);
+  m.dig_e.assign(m.beta, 0);
+  m.mod_up2.assign(m.beta, {});
+  for (int i = 0; i < m.beta; i++) {
+    int s = i * m.num_aux, e = std::min((i + 1) * m.num_aux, padded);
+    if (e <= npad) continue;
+    s = std::max(0, s - npad);
+    e -= npad;
+    m.dig_s[i] = s;
+    m.dig_e[i] = e;
+    std::vector<uint32_t> src(lp.begin() + s, lp.begin() + e), dst(lp.begin(), lp.begin() + s);
+    dst.insert(dst.end(), lp.begin() + e, lp.end());
+    std::vector<uint32_t> c1;
+    ms_consts(n, src, dst, 0, 0, &c1, &m.mod_up2[i]);
+    std::copy(c1.begin(), c1.end(), m.mod_up1.begin() + s);
+  }
+  std::vector<uint32_t> qp(lp.begin(), lp.begin() + nq), pp(lp.begin() + nq, lp.end());
+  ms_consts(n, pp, qp, 0, 0, &m.mod_down1, &m.mod_down2);
+  epi_consts(pp, qp, 0, 0, &m.inv_p_prod, nullptr);
+  if (level <= 0) return;
+  NP nn = P.level_np(level - 1, m.num_aux);
+  std::vector<int> gn(nn.total());
+  P.gidx(nn, gn.data());
+  std::vector<uint32_t> next(nn.q());
+  for (int i = 0; i < nn.q(); i++) next[i] = P.primes[gn[i]];
+  const int nnq = nn.q();
+  const int md = np.main - nn.main, td = np.ter - nn.ter;
+  std::vector<uint32_t> rs_src;
+  if (td > 0) {
+    if (md > 0) return;
+    rs_src.assign(lp.begin(), lp.begin() + td);
+    m.pad_start = 0;
+    m.pad_end = nq - td;
+    m.restore_start = nnq + md;
+    m.restore_end = nnq;
+  } else if (md > 0) {
+    rs_src.assign(lp.begin() + nq - md, lp.begin() + nq);
+    m.pad_start = -td;
+    m.pad_end = nq - md - td;
+    m.restore_start = 0;
+    m.restore_end = -td;
+  } else {
+    return;
+  }
+  m.has_rescale = true;
+  std::vector<uint32_t> mdr_src = rs_src;
+  mdr_src.insert(mdr_src.end(), pp.begin(), pp.end());
+  m.rs_src_len = static_cast<int>(rs_src.size());
+  m.mdr_src_len = static_cast<int>(mdr_src.size());
+  m.rs_dst_len = nnq;
+  ms_consts(n, rs_src, next, m.restore_start, m.restore_end, &m.rs1, &m.rs2);
+  epi_consts(rs_src, next, m.restore_start, m.restore_end, &m.rs_inv, &m.rs_pad);
+  ms_consts(n, mdr_src, next, m.restore_start, m.restore_end, &m.mdr1, &m.mdr2);
+  epi_consts(mdr_src, next, m.restore_start, m.restore_end, &m.mdr_inv, &m.mdr_pad);
+}
+
 Status Context::init(const ParamSpec &spec, int dev, std::string *err) {
   P = Params::create(spec, err);
   if (!P) return kErrInvalidArg;
@@ -677,80 +750,11 @@ Status Context::init(const ParamSpec &spec, int dev, std::string *err) {
   ms.resize(P->max_level + 2);
   for (int level = -1; level <= P->max_level; level++) {
     LevelMS &m = ms[level + 1];
-    m.level = level;
-    m.num_aux = level == -1 ? P->sse_num_aux() : P->alpha;
-    NP np = P->level_np(level, m.num_aux);
-    const int nq = np.q(), tot = np.total();
-    m.num_q = nq;
-    m.beta = level == -1 ? 1 : (np.main + P->max_ter + m.num_aux - 1) / m.num_aux;
-    std::vector<int> g(tot);
-    P->gidx(np, g.data());
-    std::vector<uint32_t> lp(tot);
-    for (int i = 0; i < tot; i++) lp[i] = P->primes[g[i]];
-    const int padded = level == -1 ? nq : np.main + P->max_ter;
-    const int npad = padded - nq;
-    m.mod_up1.assign(nq, 0);
-    m.dig_s.assign(m.beta, 0);
-    m.dig_e.assign(m.beta, 0);
-    m.d_mod_up2.assign(m.beta, nullptr);
-    for (int i = 0; i < m.beta; i++) {
-      int s = i * m.num_aux, e = std::min((i + 1) * m.num_aux, padded);
-      if (e <= npad) continue;
-      s = std::max(0, s - npad);
-      e -= npad;
-      m.dig_s[i] = s;
-      m.dig_e[i] = e;
-      std::vector<uint32_t> src(lp.begin() + s, lp.begin() + e), dst(lp.begin(), lp.begin() + s);
-      dst.insert(dst.end(), lp.begin() + e, lp.end());
-      std::vector<uint32_t> c1;
-      std::vector<int32_t> c2;
-      ms_consts(n, src, dst, 0, 0, &c1, &c2);
-      std::copy(c1.begin(), c1.end(), m.mod_up1.begin() + s);
-      m.d_mod_up2[i] = upload_i32(c2);
-    }
-    std::vector<uint32_t> qp(lp.begin(), lp.begin() + nq), pp(lp.begin() + nq, lp.end());
-    std::vector<int32_t> c2;
-    ms_consts(n, pp, qp, 0, 0, &m.mod_down1, &c2);
-    m.d_mod_down2 = upload_i32(c2);
-    epi_consts(pp, qp, 0, 0, &m.inv_p_prod, nullptr);
-    if (level <= 0) continue;
-    NP nn = P->level_np(level - 1, m.num_aux);
-    std::vector<int> gn(nn.total());
-    P->gidx(nn, gn.data());
-    std::vector<uint32_t> next(nn.q());
-    for (int i = 0; i < nn.q(); i++) next[i] = P->primes[gn[i]];
-    const int nnq = nn.q();
-    const int md = np.main - nn.main, td = np.ter - nn.ter;
-    std::vector<uint32_t> rs_src;
-    if (td > 0) {
-      if (md > 0) continue;
-      rs_src.assign(lp.begin(), lp.begin() + td);
-      m.pad_start = 0;
-      m.pad_end = nq - td;
-      m.restore_start = nnq + md;
-      m.restore_end = nnq;
-    } else if (md > 0) {
-      if (td > 0) continue;
-      rs_src.assign(lp.begin() + nq - md, lp.begin() + nq);
-      m.pad_start = -td;
-      m.pad_end = nq - md - td;
-      m.restore_start = 0;
-      m.restore_end = -td;
-    } else {
-      continue;
-    }
-    m.has_rescale = true;
-    std::vector<uint32_t> mdr_src = rs_src;
-    mdr_src.insert(mdr_src.end(), pp.begin(), pp.end());
-    m.rs_src_len = static_cast<int>(rs_src.size());
-    m.mdr_src_len = static_cast<int>(mdr_src.size());
-    m.rs_dst_len = nnq;
-    ms_consts(n, rs_src, next, m.restore_start, m.restore_end, &m.rs1, &c2);
-    m.d_rs2 = upload_i32(c2);
-    epi_consts(rs_src, next, m.restore_start, m.restore_end, &m.rs_inv, &m.rs_pad);
-    ms_consts(n, mdr_src, next, m.restore_start, m.restore_end, &m.mdr1, &c2);
-    m.d_mdr2 = upload_i32(c2);
-    epi_consts(mdr_src, next, m.restore_start, m.restore_end, &m.mdr_inv, &m.mdr_pad);
+    build_level_ms(*P, level, &m);
+    for (auto &t : m.mod_up2) m.d_mod_up2.push_back(t.empty() ? nullptr : upload_i32(t));
+    m.d_mod_down2 = upload_i32(m.mod_down2);
+    m.d_rs2 = upload_i32(m.rs2);
+    m.d_mdr2 = upload_i32(m.mdr2);
   }
   if (cudaDeviceSynchronize() != cudaSuccess) {
     *err = std::string("context setup: ") + cudaGetErrorString(cudaGetLastError());

@@ -95,15 +95,21 @@ struct LevelMS {
   int level = 0, num_aux = 0, beta = 0, num_q = 0;
   std::vector<uint32_t> mod_up1;
   std::vector<int> dig_s, dig_e;
-  std::vector<int32_t *> d_mod_up2;  // device [dst][src] per digit
+  std::vector<std::vector<int32_t>> mod_up2;  // host [dst][src] per digit
   std::vector<uint32_t> mod_down1, inv_p_prod;
-  int32_t *d_mod_down2 = nullptr;
+  std::vector<int32_t> mod_down2;
   bool has_rescale = false;
   int pad_start = 0, pad_end = 0, restore_start = 0, restore_end = 0;
   int rs_src_len = 0, mdr_src_len = 0, rs_dst_len = 0;
   std::vector<uint32_t> rs1, rs_inv, rs_pad, mdr1, mdr_inv, mdr_pad;
-  int32_t *d_rs2 = nullptr, *d_mdr2 = nullptr;
+  std::vector<int32_t> rs2, mdr2;
+  // device copies of the BConv tables
+  std::vector<int32_t *> d_mod_up2;
+  int32_t *d_mod_down2 = nullptr, *d_rs2 = nullptr, *d_mdr2 = nullptr;
 };
+
+// Host-only computation of the ModSwitch constants of one level (no GPU).
+void build_level_ms(const Params &P, int level, LevelMS *m);
 
 // ---- device objects ----------------------------------------------------------
 struct DeviceCt {

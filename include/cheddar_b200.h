@@ -171,6 +171,16 @@ int chd_moddown_raw(chd_context *ctx, int level, int type, const uint32_t *src_d
 int chd_bconv_raw(chd_context *ctx, const int32_t *xt_dev, const int *src_gidx, int K,
                   const int *dst_gidx, int M, uint32_t *out_dev);
 
+/* Host-side ModSwitch constants of one level, computed without a GPU
+ * (ModSwitchHandler ctor, src/core/ModSwitch.cu:175-411).  kind: 0 = ModUp
+ * digit `digit`, 1 = ModDown, 2 = Rescale, 3 = ModDownAndRescale.  Outputs:
+ * c1[K] (plain (N q-hat)^-1 x restore), table[M*K] (centred BConv table),
+ * inv[M] and pad[dims[2]] (Montgomery epilogue constants); dims = {K, M,
+ * pad_len, restore_start, restore_end, beta}.  Buffers: c1 >= 16,
+ * table >= 64*16, inv/pad >= 64 words. */
+int chd_params_level_consts(const char *json_text, int level, int kind, int digit, uint32_t *c1,
+                            int32_t *table, uint32_t *inv, uint32_t *pad, int *dims);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1638,3 +1638,56 @@ int orc_decode(const orc_ctx *c, int level, double scale, const uint32_t *pt,
   free(d);
   return 0;
 }
+
+/* Per-level ModSwitch constants (for comparison with the CUDA library's host
+ * code): kind 0 = ModUp digit, 1 = ModDown, 2 = Rescale, 3 = ModDown+Rescale;
+ * dims = {K, M, pad_len, restore_start, restore_end, beta}. */
+int orc_level_consts(const orc_ctx *c, int level, int kind, int digit,
+                     uint32_t *c1, int32_t *table, uint32_t *inv,
+                     uint32_t *pad, int *dims) {
+  if (level < -1 || level > c->max_level) return -1;
+  const msw_t *m = &c->msw[level + 1];
+  int K = 0, M = 0, pl = 0;
+  dims[3] = m->restore_start;
+  dims[4] = m->restore_end;
+  dims[5] = m->beta;
+  const uint32_t *v1 = NULL, *vi = NULL, *vp = NULL;
+  const int32_t *vt = NULL;
+  if (kind == 0) {
+    if (digit < 0 || digit >= m->beta) return -1;
+    K = m->dig_e[digit] - m->dig_s[digit];
+    if (m->dig_e[digit] <= 0) K = 0;
+    if (K <= 0) {
+      dims[0] = dims[1] = dims[2] = 0;
+      return 0;
+    }
+    M = m->num_q + m->num_aux - K;
+    v1 = m->mod_up1 + m->dig_s[digit];
+    vt = m->mod_up2[digit];
+  } else if (kind == 1) {
+    K = m->num_aux;
+    M = m->num_q;
+    v1 = m->mod_down1;
+    vt = m->mod_down2;
+    vi = m->inv_p_prod;
+  } else if (kind == 2 || kind == 3) {
+    if (!m->has_rescale) return -1;
+    K = kind == 2 ? m->rs_src_len : m->mdr_src_len;
+    M = m->rs_dst_len;
+    pl = M - (m->restore_end - m->restore_start);
+    v1 = kind == 2 ? m->rs1 : m->mdr1;
+    vt = kind == 2 ? m->rs2 : m->mdr2;
+    vi = kind == 2 ? m->rs_inv : m->mdr_inv;
+    vp = kind == 2 ? m->rs_pad : m->mdr_pad;
+  } else {
+    return -1;
+  }
+  dims[0] = K;
+  dims[1] = M;
+  dims[2] = pl;
+  if (v1 && c1) memcpy(c1, v1, sizeof(uint32_t) * K);
+  if (vt && table) memcpy(table, vt, sizeof(int32_t) * (size_t)K * M);
+  if (vi && inv) memcpy(inv, vi, sizeof(uint32_t) * M);
+  if (vp && pad) memcpy(pad, vp, sizeof(uint32_t) * pl);
+  return 0;
+}

@@ -110,6 +110,9 @@ int orc_bconv_table(const uint32_t *src, int K, const uint32_t *dst, int M,
                     int32_t *table);
 
 /* ---- ModSwitch (restating src/core/ModSwitch.cu) ---- */
+int orc_level_consts(const orc_ctx *c, int level, int kind, int digit,
+                     uint32_t *c1, int32_t *table, uint32_t *inv,
+                     uint32_t *pad, int *dims);
 /* src: [num_q][N] (eval, Montgomery); dst: beta x [num_q + num_aux][N] */
 int orc_modup(const orc_ctx *c, int level, const uint32_t *src, uint32_t *dst);
 /* src [num_q + alpha][N] -> dst [num_q][N] */

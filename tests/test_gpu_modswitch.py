@@ -17,6 +17,8 @@ def _dev(a):
 
 
 def _host(t):
+    # the library works on its own stream: wait for it before torch reads
+    torch.cuda.synchronize()
     return t.cpu().numpy().view(np.uint32)
 
 
@@ -30,6 +32,7 @@ def test_bconv_raw(cuda_ok, K, M):
     xt = np.stack([rng.integers(-(int(primes[s]) // 2), int(primes[s]) // 2 + 1, o.n) for s in src]).astype(np.int32)
     out = torch.zeros((M, o.n), dtype=torch.int32, device="cuda")
     g.bconv_raw(torch.from_numpy(xt).cuda(), src, dst, out)
+    g.synchronize()
     T = o.bconv_table(primes[src], primes[dst])
     assert np.array_equal(_host(out), o.bconv(xt, T, primes[dst]))
 
@@ -44,6 +47,7 @@ def test_modup(cuda_ok, level):
     beta = o.beta(level)
     out = torch.zeros((beta, o.num_q(level) + o.alpha, o.n), dtype=torch.int32, device="cuda")
     g.modup_raw(level, _dev(x), out)
+    g.synchronize()
     ref = o.modup(level, x)
     assert np.array_equal(_host(out).reshape(ref.shape), ref)
 
@@ -54,6 +58,7 @@ def test_moddown(cuda_ok, level):
     x = np.stack([o.uniform(40 + level + i, level, num_aux=o.alpha) for i in range(2)])
     out = torch.zeros((2, o.num_q(level), o.n), dtype=torch.int32, device="cuda")
     g.moddown_raw(level, chd.CHD_MODDOWN, _dev(x), out, npoly=2)
+    g.synchronize()
     for i in range(2):
         assert np.array_equal(_host(out[i]), o.moddown(level, x[i]))
 
@@ -64,9 +69,11 @@ def test_rescale_and_merged(cuda_ok, level):
     x = o.uniform(50 + level, level)
     out = torch.zeros((o.num_q(level - 1), o.n), dtype=torch.int32, device="cuda")
     g.moddown_raw(level, chd.CHD_RESCALE, _dev(x), out)
+    g.synchronize()
     assert np.array_equal(_host(out), o.rescale(level, x))
     xa = o.uniform(60 + level, level, num_aux=o.alpha)
     g.moddown_raw(level, chd.CHD_MODDOWN_RESCALE, _dev(xa), out)
+    g.synchronize()
     assert np.array_equal(_host(out), o.moddown_rescale(level, xa))
 
 
@@ -79,14 +86,18 @@ def test_rational_rescale_all_levels(cuda_ok, level):
     x = o.uniform(70 + level, level)
     out = torch.zeros((o.num_q(level - 1), o.n), dtype=torch.int32, device="cuda")
     g.moddown_raw(level, chd.CHD_RESCALE, _dev(x), out)
+    g.synchronize()
     assert np.array_equal(_host(out), o.rescale(level, x))
     xa = o.uniform(80 + level, level, num_aux=o.alpha)
     g.moddown_raw(level, chd.CHD_MODDOWN_RESCALE, _dev(xa), out)
+    g.synchronize()
     assert np.array_equal(_host(out), o.moddown_rescale(level, xa))
     out2 = torch.zeros((o.num_q(level), o.n), dtype=torch.int32, device="cuda")
     g.moddown_raw(level, chd.CHD_MODDOWN, _dev(xa), out2)
+    g.synchronize()
     assert np.array_equal(_host(out2), o.moddown(level, xa))
     mu = torch.zeros((o.beta(level), o.num_q(level) + o.alpha, o.n), dtype=torch.int32, device="cuda")
     g.modup_raw(level, _dev(x), mu)
+    g.synchronize()
     ref = o.modup(level, x)
     assert np.array_equal(_host(mu).reshape(ref.shape), ref)
