@@ -78,4 +78,30 @@ __device__ __forceinline__ void gs_bfly(uint32_t &a, uint32_t &b, uint32_t w, ui
   b = mont_mul(d, w, q, qinv);
 }
 
+// ---- Shoup multiplication with lazy [0, 2q) values (D. Harvey, "Faster
+// arithmetic for number-theoretic transforms", 2014): for any 32-bit b and a
+// constant w < q with companion ws = floor(w 2^32 / q),
+//   b w - floor(b ws / 2^32) q  lies in [0, 2q)  (q < 2^31 keeps 2q in a word).
+__device__ __forceinline__ uint32_t shoup_lazy(uint32_t b, uint32_t w, uint32_t ws, uint32_t q) {
+  return b * w - __umulhi(b, ws) * q;
+}
+// [0, 2q) -> [0, q): unsigned min(x, x - q)
+__device__ __forceinline__ uint32_t reduce2q(uint32_t x, uint32_t q) { return min(x, x - q); }
+
+// Cooley-Tukey butterfly, inputs and outputs in [0, 2q):
+// (a, b) -> (a + w b, a - w b)
+__device__ __forceinline__ void ct_lazy(uint32_t &a, uint32_t &b, uint2 w, uint32_t q) {
+  const uint32_t x = reduce2q(a, q);
+  const uint32_t t = reduce2q(shoup_lazy(b, w.x, w.y, q), q);
+  a = x + t;
+  b = x - t + q;
+}
+// Gentleman-Sande butterfly, inputs and outputs in [0, 2q):
+// (a, b) -> (a + b, (a - b) w)
+__device__ __forceinline__ void gs_lazy(uint32_t &a, uint32_t &b, uint2 w, uint32_t q) {
+  const uint32_t x = reduce2q(a, q), y = reduce2q(b, q);
+  a = x + y;
+  b = shoup_lazy(x - y + q, w.x, w.y, q);
+}
+
 }  // namespace chd

@@ -554,6 +554,12 @@ Context::~Context() {
   if (own_stream && stream) cudaStreamDestroy(stream);
 }
 
+void Context::mont_as_shoup(uint32_t c, int g, uint32_t *w, uint32_t *ws) const {
+  const uint32_t q = P->primes[g];
+  *w = prime::mul_mod(c, r_inv[g], q);
+  *ws = static_cast<uint32_t>((static_cast<uint64_t>(*w) << 32) / q);
+}
+
 Status Context::check_cuda(const char *where) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
@@ -705,19 +711,23 @@ Status Context::init(const ParamSpec &spec, int dev, std::string *err) {
   }
   own_stream = true;
   const int n = P->n, np_all = P->L + P->alpha;
-  // twiddles, NTT.cu:1233-1299: psi_rev[j] = psi^brev(j) in Montgomery form
-  std::vector<uint32_t> tw(static_cast<size_t>(np_all) * n), itw(tw.size());
+  // twiddles, NTT.cu:1233-1299: psi_rev[j] = psi^brev(j); stored plain with
+  // the Shoup companion floor(w 2^32 / q)
+  std::vector<uint2> tw(static_cast<size_t>(np_all) * n), itw(tw.size());
   n_inv.resize(np_all);
   n_inv_mont.resize(np_all);
   mont_conv.resize(np_all);
   imag_unit.resize(np_all);
+  r_inv.resize(np_all);
   std::vector<uint32_t> pw(n), pwi(n);
+  auto shoup = [](uint32_t w, uint32_t q) { return static_cast<uint32_t>((static_cast<uint64_t>(w) << 32) / q); };
   for (int g = 0; g < np_all; g++) {
     uint32_t q = P->primes[g];
     uint32_t psi = prime::primitive_root(2u * n, q), psi_inv = prime::inv_mod(psi, q);
     n_inv[g] = prime::inv_mod(static_cast<uint32_t>(n), q);
     n_inv_mont[g] = prime::to_mont(n_inv[g], q);
     mont_conv[g] = prime::to_mont(prime::to_mont(1, q), q);
+    r_inv[g] = prime::inv_mod(prime::to_mont(1, q), q);
     pw[0] = pwi[0] = 1;
     for (int j = 1; j < n; j++) {
       pw[j] = prime::mul_mod(pw[j - 1], psi, q);
@@ -725,20 +735,21 @@ Status Context::init(const ParamSpec &spec, int dev, std::string *err) {
     }
     for (int j = 0; j < n; j++) {
       unsigned r = brev_host(j, P->log_n);
-      tw[static_cast<size_t>(g) * n + j] = prime::to_mont(pw[r], q);
-      itw[static_cast<size_t>(g) * n + j] = prime::to_mont(pwi[r], q);
+      tw[static_cast<size_t>(g) * n + j] = make_uint2(pw[r], shoup(pw[r], q));
+      itw[static_cast<size_t>(g) * n + j] = make_uint2(pwi[r], shoup(pwi[r], q));
     }
-    imag_unit[g] = tw[static_cast<size_t>(g) * n + 1];  // psi^(N/2), Montgomery
+    imag_unit[g] = prime::to_mont(pw[brev_host(1, P->log_n)], q);  // psi^(N/2), Montgomery
   }
   if (cudaMalloc(&d_primes, np_all * 4) != cudaSuccess || cudaMalloc(&d_qinv, np_all * 4) != cudaSuccess ||
-      cudaMalloc(&d_tw, tw.size() * 4) != cudaSuccess || cudaMalloc(&d_itw, itw.size() * 4) != cudaSuccess) {
+      cudaMalloc(&d_tw, tw.size() * sizeof(uint2)) != cudaSuccess ||
+      cudaMalloc(&d_itw, itw.size() * sizeof(uint2)) != cudaSuccess) {
     *err = "device allocation failed";
     return kErrAlloc;
   }
   cudaMemcpy(d_primes, P->primes.data(), np_all * 4, cudaMemcpyHostToDevice);
   cudaMemcpy(d_qinv, P->qinv.data(), np_all * 4, cudaMemcpyHostToDevice);
-  cudaMemcpy(d_tw, tw.data(), tw.size() * 4, cudaMemcpyHostToDevice);
-  cudaMemcpy(d_itw, itw.data(), itw.size() * 4, cudaMemcpyHostToDevice);
+  cudaMemcpy(d_tw, tw.data(), tw.size() * sizeof(uint2), cudaMemcpyHostToDevice);
+  cudaMemcpy(d_itw, itw.data(), itw.size() * sizeof(uint2), cudaMemcpyHostToDevice);
   // P mod q_i (Montgomery), Context.cpp:78-90
   p_prod.resize(P->L);
   for (int i = 0; i < P->L; i++) {
@@ -792,8 +803,7 @@ Status Context::ntt(const NP &np, uint32_t *data, bool mont, int count, size_t s
       r.src = r.dst = data + c * stride + static_cast<size_t>(i) * n;
       r.tw = tw(g[i]);
       r.q = P->primes[g[i]];
-      r.qinv = P->qinv[g[i]];
-      r.c0 = mont_conv[g[i]];
+      mont_as_shoup(mont_conv[g[i]], g[i], &r.c0, &r.c0s);
       r.flags = mont ? kPreMult : 0u;
       rows.push_back(r);
     }
@@ -812,8 +822,7 @@ Status Context::intt(const NP &np, uint32_t *data, bool mont, int count, size_t 
       r.src = r.dst = data + c * stride + static_cast<size_t>(i) * n;
       r.tw = itw(g[i]);
       r.q = P->primes[g[i]];
-      r.qinv = P->qinv[g[i]];
-      r.c0 = mont ? n_inv[g[i]] : n_inv_mont[g[i]];
+      mont_as_shoup(mont ? n_inv[g[i]] : n_inv_mont[g[i]], g[i], &r.c0, &r.c0s);
       rows.push_back(r);
     }
   for_row_batches(rows, [&](const RowBatch &rb) { launch_ntt_inv(rb, P->log_n, stream); });
@@ -841,7 +850,13 @@ Status Context::bconv(const int32_t *xt, int K, const int32_t *table, const int 
 }
 
 Status Context::modup(int level, const uint32_t *src, uint32_t *const *dst) {
-  // ModSwitch.cu:429-509
+  const uint32_t *srcs[1] = {src};
+  uint32_t *const *dsts[1] = {dst};
+  return modup_many(level, 1, srcs, dsts);
+}
+
+Status Context::modup_many(int level, int count, const uint32_t *const *src, uint32_t *const *const *dst) {
+  // ModSwitch.cu:429-509, for `count` independent inputs at one level
   const LevelMS &m = lms(level);
   const int n = P->n;
   NP np = P->level_np(level, m.num_aux);
@@ -849,66 +864,67 @@ Status Context::modup(int level, const uint32_t *src, uint32_t *const *dst) {
   std::vector<int> g(tot);
   P->gidx(np, g.data());
   ArenaScope scope(arena);
-  int32_t *xt = static_cast<int32_t *>(arena.alloc(static_cast<size_t>(nq) * n * 4));
+  int32_t *xt = static_cast<int32_t *>(arena.alloc(static_cast<size_t>(count) * nq * n * 4));
   CHD_CHECK(xt, kErrAlloc, "modup: scratch allocation failed");
   // 1. INTT * (N q-hat_i)^-1, centred (INTTAndMultConst with normalize)
   std::vector<RowDesc> rows;
-  for (int r = 0; r < nq; r++) {
-    RowDesc d{};
-    d.src = src + static_cast<size_t>(r) * n;
-    d.dst = reinterpret_cast<uint32_t *>(xt) + static_cast<size_t>(r) * n;
-    d.tw = itw(g[r]);
-    d.q = P->primes[g[r]];
-    d.qinv = P->qinv[g[r]];
-    d.c0 = m.mod_up1[r];
-    d.flags = kCentre;
-    rows.push_back(d);
-  }
+  for (int c = 0; c < count; c++)
+    for (int r = 0; r < nq; r++) {
+      RowDesc d{};
+      d.src = src[c] + static_cast<size_t>(r) * n;
+      d.dst = reinterpret_cast<uint32_t *>(xt) + (static_cast<size_t>(c) * nq + r) * n;
+      d.tw = itw(g[r]);
+      d.q = P->primes[g[r]];
+      mont_as_shoup(m.mod_up1[r], g[r], &d.c0, &d.c0s);
+      d.flags = kCentre;
+      rows.push_back(d);
+    }
   for_row_batches(rows, [&](const RowBatch &rb) { launch_ntt_inv(rb, P->log_n, stream); });
   // 2. own primes copied, others base-converted
   BConvBatch b{};
   b.primes = d_primes;
   b.qinvs = d_qinv;
-  for (int i = 0; i < m.beta; i++) {
-    const int s = m.dig_s[i], e = m.dig_e[i];
-    if (e <= 0) continue;
-    cudaMemcpyAsync(dst[i] + static_cast<size_t>(s) * n, src + static_cast<size_t>(s) * n,
-                    static_cast<size_t>(e - s) * n * 4, cudaMemcpyDeviceToDevice, stream);
-    BConvJob &j = b.jobs[b.count++];
-    j.xt = xt + static_cast<size_t>(s) * n;
-    j.out = dst[i];
-    j.table = m.d_mod_up2[i];
-    j.K = e - s;
-    j.M = tot - (e - s);
-    CHD_CHECK(j.K <= 16 && j.M <= 64, kErrUnsupported, "modup: digit too large");
-    int k = 0;
-    for (int r = 0; r < tot; r++) {
-      if (r >= s && r < e) continue;
-      j.out_row[k] = static_cast<uint8_t>(r);
-      j.out_gidx[k] = static_cast<uint8_t>(g[r]);
-      k++;
+  for (int c = 0; c < count; c++)
+    for (int i = 0; i < m.beta; i++) {
+      const int s = m.dig_s[i], e = m.dig_e[i];
+      if (e <= 0) continue;
+      cudaMemcpyAsync(dst[c][i] + static_cast<size_t>(s) * n, src[c] + static_cast<size_t>(s) * n,
+                      static_cast<size_t>(e - s) * n * 4, cudaMemcpyDeviceToDevice, stream);
+      BConvJob &j = b.jobs[b.count++];
+      j.xt = xt + (static_cast<size_t>(c) * nq + s) * n;
+      j.out = dst[c][i];
+      j.table = m.d_mod_up2[i];
+      j.K = e - s;
+      j.M = tot - (e - s);
+      CHD_CHECK(j.K <= 16 && j.M <= 64, kErrUnsupported, "modup: digit too large");
+      int k = 0;
+      for (int r = 0; r < tot; r++) {
+        if (r >= s && r < e) continue;
+        j.out_row[k] = static_cast<uint8_t>(r);
+        j.out_gidx[k] = static_cast<uint8_t>(g[r]);
+        k++;
+      }
+      if (b.count == kMaxBConvJobs) {
+        launch_bconv(b, P->log_n, stream);
+        b.count = 0;
+      }
     }
-    if (b.count == kMaxBConvJobs) {
-      launch_bconv(b, P->log_n, stream);
-      b.count = 0;
-    }
-  }
   launch_bconv(b, P->log_n, stream);
   // 3. NTT of the converted rows (NTTForModUp)
   rows.clear();
-  for (int i = 0; i < m.beta; i++) {
-    const int s = m.dig_s[i], e = m.dig_e[i];
-    if (e <= 0) continue;
-    for (int r = 0; r < tot; r++) {
-      if (r >= s && r < e) continue;
-      RowDesc d{};
-      d.src = d.dst = dst[i] + static_cast<size_t>(r) * n;
-      d.tw = tw(g[r]);
-      d.q = P->primes[g[r]];
-      d.qinv = P->qinv[g[r]];
-      rows.push_back(d);
+  for (int c = 0; c < count; c++)
+    for (int i = 0; i < m.beta; i++) {
+      const int s = m.dig_s[i], e = m.dig_e[i];
+      if (e <= 0) continue;
+      for (int r = 0; r < tot; r++) {
+        if (r >= s && r < e) continue;
+        RowDesc d{};
+        d.src = d.dst = dst[c][i] + static_cast<size_t>(r) * n;
+        d.tw = tw(g[r]);
+        d.q = P->primes[g[r]];
+        rows.push_back(d);
+      }
     }
-  }
   for_row_batches(rows, [&](const RowBatch &rb) { launch_ntt_fwd(rb, P->log_n, stream); });
   return check_cuda("modup");
 }
@@ -956,8 +972,7 @@ Status Context::moddown(int level, MDType type, const uint32_t *const *src, uint
       d.dst = reinterpret_cast<uint32_t *>(xt) + (static_cast<size_t>(p) * src_len + i) * n;
       d.tw = itw(gg);
       d.q = P->primes[gg];
-      d.qinv = P->qinv[gg];
-      d.c0 = c1[i];
+      mont_as_shoup(c1[i], gg, &d.c0, &d.c0s);
       d.flags = kCentre;
       rows.push_back(d);
     }
@@ -991,15 +1006,14 @@ Status Context::moddown(int level, MDType type, const uint32_t *const *src, uint
       d.src = d.dst = dst[p] + static_cast<size_t>(y) * n;
       d.tw = tw(gd[y]);
       d.q = P->primes[gd[y]];
-      d.qinv = P->qinv[gd[y]];
-      d.c2 = inv[y];
+      mont_as_shoup(inv[y], gd[y], &d.c2, &d.c2s);
       d.flags = kModDownEpi;
       if (y >= src2_start && y < src2_end) {
         d.flags |= kHasSrc2;
         d.src2 = src[p] + static_cast<size_t>(src2_off + y - src2_start) * n;
         if (pad) {
           d.flags |= kPadSrc2;
-          d.c1 = pad[y - src2_start];
+          mont_as_shoup(pad[y - src2_start], gd[y], &d.c1, &d.c1s);
         }
       }
       rows.push_back(d);
@@ -1011,6 +1025,11 @@ Status Context::moddown(int level, MDType type, const uint32_t *const *src, uint
 // --------------------------------------------------------- evaluator
 Status Context::key_switch_core(int level, const uint32_t *d0, const uint32_t *d1, const uint32_t *d_in,
                                 const DeviceEvk &key, uint32_t *acc_b, uint32_t *acc_a) {
+  KSJob j{d0, d1, d_in, acc_b, acc_a};
+  return key_switch_many(level, 1, &j, key);
+}
+
+Status Context::key_switch_many(int level, int count, const KSJob *jobs, const DeviceEvk &key) {
   // Context.cpp:609-712 (MultKeyNoModDown with the CAccum of P * (d0, d1))
   const LevelMS &m = lms(level);
   const int n = P->n;
@@ -1020,30 +1039,33 @@ Status Context::key_switch_core(int level, const uint32_t *d0, const uint32_t *d
   CHD_CHECK(key.np.aux == P->alpha && key.np.q() == P->L, kErrKey, "key switch: key basis mismatch");
   const int prime_offset = P->max_ter - np.ter;
   ArenaScope scope(arena);
-  std::vector<uint32_t *> mu(m.beta, nullptr);
-  for (int i = 0; i < m.beta; i++) {
-    mu[i] = static_cast<uint32_t *>(arena.alloc(static_cast<size_t>(tot) * n * 4));
-    CHD_CHECK(mu[i], kErrAlloc, "key switch: scratch allocation failed");
+  const size_t mu_words = static_cast<size_t>(tot) * n;
+  uint32_t *mu_all = static_cast<uint32_t *>(arena.alloc(static_cast<size_t>(count) * m.beta * mu_words * 4));
+  CHD_CHECK(mu_all, kErrAlloc, "key switch: scratch allocation failed");
+  std::vector<uint32_t *> mu_ptrs(static_cast<size_t>(count) * m.beta);
+  std::vector<uint32_t *const *> dsts(count);
+  std::vector<const uint32_t *> srcs(count);
+  for (int c = 0; c < count; c++) {
+    for (int i = 0; i < m.beta; i++) mu_ptrs[c * m.beta + i] = mu_all + (static_cast<size_t>(c) * m.beta + i) * mu_words;
+    dsts[c] = mu_ptrs.data() + c * m.beta;
+    srcs[c] = jobs[c].d_in;
   }
-  CHD_TRY(modup(level, d_in, mu.data()));
+  CHD_TRY(modup_many(level, count, srcs.data(), dsts.data()));
   KeyMacDesc d{};
   std::vector<int> g(tot);
   P->gidx(np, g.data());
   const size_t kstride = static_cast<size_t>(key.np.total()) * n;
   int nb = 0;
+  std::vector<int> digits;
   for (int i = 0; i < m.beta; i++) {
     if (m.dig_e[i] <= 0) continue;
     CHD_CHECK(i < key.beta, kErrKey, "key switch: key has too few digits");
-    d.mu[nb] = mu[i];
     d.kb[nb] = key.bx + i * kstride;
     d.ka[nb] = key.ax + i * kstride;
+    digits.push_back(i);
     nb++;
   }
   d.beta = nb;
-  d.d0 = d0;
-  d.d1 = d1;
-  d.acc_b = acc_b;
-  d.acc_a = acc_a;
   d.rows = tot;
   d.nq = nq;
   for (int r = 0; r < tot; r++) {
@@ -1052,7 +1074,19 @@ Status Context::key_switch_core(int level, const uint32_t *d0, const uint32_t *d
     d.key_row[r] = static_cast<int16_t>(r < nq ? prime_offset + r : P->L + (r - nq));
     d.p_prod[r] = r < nq ? p_prod[prime_offset + r] : 0;
   }
-  launch_key_mac(d, P->log_n, stream);
+  for (int c0 = 0; c0 < count; c0 += kMaxKeyMacCts) {
+    d.count = std::min(kMaxKeyMacCts, count - c0);
+    for (int c = 0; c < d.count; c++) {
+      const KSJob &j = jobs[c0 + c];
+      KeyMacCt &k = d.ct[c];
+      for (int b = 0; b < nb; b++) k.mu[b] = mu_ptrs[(c0 + c) * m.beta + digits[b]];
+      k.d0 = j.d0;
+      k.d1 = j.d1;
+      k.acc_b = j.acc_b;
+      k.acc_a = j.acc_a;
+    }
+    launch_key_mac(d, P->log_n, stream);
+  }
   return check_cuda("key switch");
 }
 
@@ -1106,8 +1140,75 @@ Status Context::hmult(DeviceCt &res, const DeviceCt &a, const DeviceCt &b, const
 
 Status Context::hmult_batch(int count, DeviceCt *const *res, const DeviceCt *const *a, const DeviceCt *const *b,
                             const DeviceEvk &key, bool rescale) {
-  for (int i = 0; i < count; i++) CHD_TRY(hmult(*res[i], *a[i], *b[i], key, rescale));
-  return kOk;
+  // Batched Context::HMult: every stage (tensor, ModUp, key MAC, merged
+  // ModDown+Rescale) runs once for the whole batch.  Ciphertexts must share
+  // a level and must not alias each other's results.
+  if (count <= 0) return kOk;
+  bool uniform = true;
+  for (int i = 0; i < count; i++) {
+    CHD_CHECK(a[i]->np == b[i]->np && a[i]->np.aux == 0 && !a[i]->has_rx && !b[i]->has_rx, kErrShape,
+              "HMult batch: operands must share a level, no aux primes, no rx");
+    uniform = uniform && a[i]->np == a[0]->np;
+    for (int j = 0; j < count; j++)
+      if (res[i] == a[j] || res[i] == b[j]) uniform = false;  // aliasing: run one by one
+  }
+  if (!uniform) {
+    for (int i = 0; i < count; i++) CHD_TRY(hmult(*res[i], *a[i], *b[i], key, rescale));
+    return kOk;
+  }
+  const int level = level_of(*P, *a[0]);
+  CHD_CHECK(level >= 0, kErrInvalidLevel, "HMult: invalid level");
+  CHD_CHECK(!rescale || level >= 1, kErrInvalidLevel, "Not enough q primes to rescale");
+  const int n = P->n, nq = a[0]->np.q(), tot = nq + P->alpha;
+  CHD_CHECK(tot <= 64, kErrUnsupported, "HMult: more than 64 primes in the extended basis");
+  ArenaScope scope(arena);
+  const size_t qw = static_cast<size_t>(nq) * n, tw_ = static_cast<size_t>(tot) * n;
+  uint32_t *d = static_cast<uint32_t *>(arena.alloc(static_cast<size_t>(count) * 3 * qw * 4));
+  uint32_t *acc = static_cast<uint32_t *>(arena.alloc(static_cast<size_t>(count) * 2 * tw_ * 4));
+  CHD_CHECK(d && acc, kErrAlloc, "HMult: scratch allocation failed");
+  std::vector<int> g(nq);
+  P->gidx(a[0]->np, g.data());
+  TensorBatch tb{};
+  std::vector<KSJob> jobs(count);
+  for (int c = 0; c < count; c++) {
+    uint32_t *d0 = d + c * 3 * qw, *d1 = d0 + qw, *d2 = d1 + qw;
+    for (int r = 0; r < nq; r++) {
+      if (tb.count == 64) {
+        launch_tensor(tb, P->log_n, stream);
+        tb.count = 0;
+      }
+      TensorRow &t = tb.rows[tb.count++];
+      const size_t o = static_cast<size_t>(r) * n;
+      t.b1 = a[c]->bx + o;
+      t.a1 = a[c]->ax + o;
+      t.b2 = b[c]->bx + o;
+      t.a2 = b[c]->ax + o;
+      t.d0 = d0 + o;
+      t.d1 = d1 + o;
+      t.d2 = d2 + o;
+      t.q = P->primes[g[r]];
+      t.qinv = P->qinv[g[r]];
+    }
+    jobs[c] = KSJob{d0, d1, d2, acc + c * 2 * tw_, acc + c * 2 * tw_ + tw_};
+  }
+  launch_tensor(tb, P->log_n, stream);
+  CHD_TRY(key_switch_many(level, count, jobs.data(), key));
+  NP out_np = P->level_np(rescale ? level - 1 : level, 0);
+  std::vector<const uint32_t *> srcs(2 * count);
+  std::vector<uint32_t *> dsts(2 * count);
+  for (int c = 0; c < count; c++) {
+    const double sa = a[c]->scale, sb = b[c]->scale;
+    const int slots = std::max(a[c]->num_slots, b[c]->num_slots);
+    CHD_TRY(res[c]->reserve(out_np, false, n));
+    res[c]->scale = rescale ? sa * sb / P->rescale_prod[level] : sa * sb;
+    res[c]->num_slots = slots;
+    srcs[2 * c] = jobs[c].acc_b;
+    srcs[2 * c + 1] = jobs[c].acc_a;
+    dsts[2 * c] = res[c]->bx;
+    dsts[2 * c + 1] = res[c]->ax;
+  }
+  return moddown(level, rescale ? MDType::kModDownRescale : MDType::kModDown, srcs.data(), dsts.data(),
+                 2 * count);
 }
 
 Status Context::relinearize(DeviceCt &res, const DeviceCt &a, const DeviceEvk &key, bool rescale) {

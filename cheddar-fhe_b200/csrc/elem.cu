@@ -22,43 +22,50 @@ __device__ __forceinline__ void unpack(uint4 v, uint32_t *x) {
 // stays inside the (-p 2^31, p 2^31) input range of the Montgomery reduction;
 // group results are summed canonically.  (The reference kernel,
 // src/core/ModSwitch.cu:23-171, computes the same residue.)
+constexpr int kBConvTargetsPerCta = 8;
+
+template <int KMAX>
 __global__ void __launch_bounds__(256) k_bconv(const __grid_constant__ BConvBatch b, int log_n) {
   const BConvJob &jb = b.jobs[blockIdx.y];
+  const int m0 = blockIdx.z * kBConvTargetsPerCta;
+  if (m0 >= jb.M) return;
+  const int m1 = min(m0 + kBConvTargetsPerCta, jb.M);
   const int n = 1 << log_n;
-  const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * 2;
   if (i0 >= n) return;
   const int K = jb.K;
-  int32_t x[16][4];
+  int32_t x[KMAX][2];
 #pragma unroll
-  for (int k = 0; k < 16; k++) {
+  for (int k = 0; k < KMAX; k++) {
     if (k < K) {
-      int4 v = __ldg(reinterpret_cast<const int4 *>(jb.xt + static_cast<size_t>(k) * n + i0));
-      x[k][0] = v.x; x[k][1] = v.y; x[k][2] = v.z; x[k][3] = v.w;
+      int2 v = __ldg(reinterpret_cast<const int2 *>(jb.xt + static_cast<size_t>(k) * n + i0));
+      x[k][0] = v.x;
+      x[k][1] = v.y;
     }
   }
-  for (int m = 0; m < jb.M; m++) {
+  for (int m = m0; m < m1; m++) {
     const int g = jb.out_gidx[m];
     const uint32_t p = __ldg(b.primes + g);
     const int32_t pinv = __ldg(b.qinvs + g);
     const int32_t *T = jb.table + m * K;
-    uint32_t s[4] = {0, 0, 0, 0};
+    uint32_t s0 = 0, s1 = 0;
 #pragma unroll
-    for (int k0 = 0; k0 < 16; k0 += 4) {
+    for (int k0 = 0; k0 < KMAX; k0 += 4) {
       if (k0 < K) {
-        int64_t acc[4] = {0, 0, 0, 0};
+        int64_t a0 = 0, a1 = 0;
 #pragma unroll
         for (int k = k0; k < k0 + 4; k++) {
           if (k < K) {
             const int64_t t = __ldg(T + k);
-#pragma unroll
-            for (int l = 0; l < 4; l++) acc[l] += static_cast<int64_t>(x[k][l]) * t;
+            a0 += static_cast<int64_t>(x[k][0]) * t;
+            a1 += static_cast<int64_t>(x[k][1]) * t;
           }
         }
-#pragma unroll
-        for (int l = 0; l < 4; l++) s[l] = add_mod(s[l], mont_reduce(acc[l], p, pinv), p);
+        s0 = add_mod(s0, mont_reduce(a0, p, pinv), p);
+        s1 = add_mod(s1, mont_reduce(a1, p, pinv), p);
       }
     }
-    st4(jb.out + static_cast<size_t>(jb.out_row[m]) * n + i0, s[0], s[1], s[2], s[3]);
+    *reinterpret_cast<uint2 *>(jb.out + static_cast<size_t>(jb.out_row[m]) * n + i0) = make_uint2(s0, s1);
   }
 }
 
@@ -66,6 +73,7 @@ __global__ void __launch_bounds__(256) k_bconv(const __grid_constant__ BConvBatc
 __global__ void __launch_bounds__(256) k_key_mac(const __grid_constant__ KeyMacDesc d, int log_n) {
   const int n = 1 << log_n;
   const int r = blockIdx.y;
+  const KeyMacCt &c = d.ct[blockIdx.z];
   const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
   if (i0 >= n) return;
   const uint32_t q = d.q[r];
@@ -75,7 +83,7 @@ __global__ void __launch_bounds__(256) k_key_mac(const __grid_constant__ KeyMacD
   uint32_t sb[4] = {0, 0, 0, 0}, sa[4] = {0, 0, 0, 0};
   for (int i = 0; i < d.beta; i++) {
     uint32_t mu[4], kb[4], ka[4];
-    unpack(ld4(d.mu[i] + off), mu);
+    unpack(ld4(c.mu[i] + off), mu);
     unpack(ld4(d.kb[i] + koff), kb);
     unpack(ld4(d.ka[i] + koff), ka);
 #pragma unroll
@@ -86,21 +94,21 @@ __global__ void __launch_bounds__(256) k_key_mac(const __grid_constant__ KeyMacD
   }
   if (r < d.nq) {
     const uint32_t pp = d.p_prod[r];
-    if (d.d0) {
+    if (c.d0) {
       uint32_t v[4];
-      unpack(ld4(d.d0 + off), v);
+      unpack(ld4(c.d0 + off), v);
 #pragma unroll
       for (int l = 0; l < 4; l++) sb[l] = add_mod(sb[l], mont_mul(v[l], pp, q, qi), q);
     }
-    if (d.d1) {
+    if (c.d1) {
       uint32_t v[4];
-      unpack(ld4(d.d1 + off), v);
+      unpack(ld4(c.d1 + off), v);
 #pragma unroll
       for (int l = 0; l < 4; l++) sa[l] = add_mod(sa[l], mont_mul(v[l], pp, q, qi), q);
     }
   }
-  st4(d.acc_b + off, sb[0], sb[1], sb[2], sb[3]);
-  st4(d.acc_a + off, sa[0], sa[1], sa[2], sa[3]);
+  st4(c.acc_b + off, sb[0], sb[1], sb[2], sb[3]);
+  st4(c.acc_a + off, sa[0], sa[1], sa[2], sa[3]);
 }
 
 // ----------------------------------------------------------- element-wise
@@ -224,13 +232,26 @@ __global__ void __launch_bounds__(256) k_hoisted(const __grid_constant__ HoistDe
 void launch_bconv(const BConvBatch &b, int log_n, cudaStream_t s) {
   if (b.count <= 0) return;
   const int n = 1 << log_n;
-  k_bconv<<<dim3((n / 4 + 255) / 256, b.count), 256, 0, s>>>(b, log_n);
+  int max_m = 0;
+  for (int j = 0; j < b.count; j++) max_m = b.jobs[j].M > max_m ? b.jobs[j].M : max_m;
+  int max_k = 0;
+  for (int j = 0; j < b.count; j++) max_k = b.jobs[j].K > max_k ? b.jobs[j].K : max_k;
+  const int zs = (max_m + kBConvTargetsPerCta - 1) / kBConvTargetsPerCta;
+  const dim3 grid((n / 2 + 255) / 256, b.count, zs);
+  if (max_k <= 4)
+    k_bconv<4><<<grid, 256, 0, s>>>(b, log_n);
+  else if (max_k <= 8)
+    k_bconv<8><<<grid, 256, 0, s>>>(b, log_n);
+  else if (max_k <= 12)
+    k_bconv<12><<<grid, 256, 0, s>>>(b, log_n);
+  else
+    k_bconv<16><<<grid, 256, 0, s>>>(b, log_n);
 }
 
 void launch_key_mac(const KeyMacDesc &d, int log_n, cudaStream_t s) {
-  if (d.rows <= 0) return;
+  if (d.rows <= 0 || d.count <= 0) return;
   const int n = 1 << log_n;
-  k_key_mac<<<dim3((n / 4 + 255) / 256, d.rows), 256, 0, s>>>(d, log_n);
+  k_key_mac<<<dim3((n / 4 + 255) / 256, d.rows, d.count), 256, 0, s>>>(d, log_n);
 }
 
 void launch_elementwise(ElemOp op, const ElemBatch &b, int log_n, cudaStream_t s) {

@@ -166,13 +166,16 @@ class Context {
   // device tables
   uint32_t *d_primes = nullptr;
   int32_t *d_qinv = nullptr;
-  uint32_t *d_tw = nullptr, *d_itw = nullptr;  // [nprimes][N]
+  uint2 *d_tw = nullptr, *d_itw = nullptr;  // [nprimes][N] (psi_rev, Shoup companion)
   std::vector<uint32_t> n_inv, n_inv_mont, mont_conv, p_prod, imag_unit;
+  std::vector<uint32_t> r_inv;  // 2^-32 mod q per global prime
   std::vector<LevelMS> ms;  // index level + 1
 
   const LevelMS &lms(int level) const { return ms.at(level + 1); }
-  const uint32_t *tw(int g) const { return d_tw + (static_cast<size_t>(g) << P->log_n); }
-  const uint32_t *itw(int g) const { return d_itw + (static_cast<size_t>(g) << P->log_n); }
+  const uint2 *tw(int g) const { return d_tw + (static_cast<size_t>(g) << P->log_n); }
+  const uint2 *itw(int g) const { return d_itw + (static_cast<size_t>(g) << P->log_n); }
+  // (w, companion) that multiplies like a Montgomery product by c: c 2^-32 mod q
+  void mont_as_shoup(uint32_t c, int g, uint32_t *w, uint32_t *ws) const;
 
   // ---- building blocks on raw device pointers ----
   // NTT of the limbs of np stored contiguously at data (in place)
@@ -180,6 +183,7 @@ class Context {
   Status intt(const NP &np, uint32_t *data, bool mont, int count = 1, size_t stride = 0);
   // ModUp of src [num_q][N] at `level` into dst[beta] ([num_q + aux][N] each)
   Status modup(int level, const uint32_t *src, uint32_t *const *dst);
+  Status modup_many(int level, int count, const uint32_t *const *src, uint32_t *const *const *dst);
   enum class MDType { kModDown, kRescale, kModDownRescale };
   // ModDown family on npoly polys
   Status moddown(int level, MDType type, const uint32_t *const *src, uint32_t *const *dst, int npoly);
@@ -214,8 +218,13 @@ class Context {
   Status init(const ParamSpec &spec, int dev, std::string *err);
   Status check_cuda(const char *where);
   // key-switch core: accum = sum_i ModUp(d_in)_i (.) key_i (+ P*(d0,d1))
+  struct KSJob {
+    const uint32_t *d0, *d1, *d_in;
+    uint32_t *acc_b, *acc_a;
+  };
   Status key_switch_core(int level, const uint32_t *d0, const uint32_t *d1, const uint32_t *d_in,
                          const DeviceEvk &key, uint32_t *acc_b, uint32_t *acc_a);
+  Status key_switch_many(int level, int count, const KSJob *jobs, const DeviceEvk &key);
 };
 
 }  // namespace chd

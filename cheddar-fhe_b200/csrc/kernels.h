@@ -11,21 +11,22 @@
 namespace chd {
 
 // One limb (N residues of one prime) processed by a batched kernel.
+// Constants are plain residues w < q with their Shoup companions
+// floor(w 2^32 / q); twiddle tables hold (psi_rev[j], companion) pairs.
 struct RowDesc {
   const uint32_t *src;   // input limb
   uint32_t *dst;         // output limb (may equal src for in-place phases)
   const uint32_t *src2;  // second input (ModDown epilogue), or nullptr
-  const uint32_t *tw;    // twiddle table of this prime (N words)
+  const uint2 *tw;       // twiddle table of this prime (N pairs)
   uint32_t q;            // prime
-  int32_t qinv;          // q^-1 mod 2^32
-  uint32_t c0;           // pre-multiplier (forward NTT) / epilogue constant (INTT)
-  uint32_t c1;           // ModDown epilogue: src2 padding multiplier
-  uint32_t c2;           // ModDown epilogue: (prod src primes)^-1 (Montgomery)
   uint32_t flags;        // see RowFlags
+  uint32_t c0, c0s;      // pre-multiplier (forward) / output constant (inverse)
+  uint32_t c1, c1s;      // ModDown epilogue: src2 padding multiplier
+  uint32_t c2, c2s;      // ModDown epilogue: (prod of dropped primes)^-1
 };
 
 enum RowFlags : uint32_t {
-  kPreMult = 1u,       // forward NTT: multiply input by c0 (Montgomery) first
+  kPreMult = 1u,       // forward NTT: multiply input by c0 first
   kCentre = 2u,        // inverse NTT: write the centred representative
   kHasSrc2 = 4u,       // ModDown epilogue: src2 exists for this row
   kPadSrc2 = 8u,       // ModDown epilogue: multiply src2 by c1 first
@@ -46,8 +47,8 @@ void launch_ntt_fwd(const RowBatch &rb, int log_n, cudaStream_t s);
 // Row phase only / column phase only (used by fused pipelines and tests)
 void launch_ntt_fwd_cols(const RowBatch &rb, int log_n, cudaStream_t s);
 void launch_ntt_fwd_rows(const RowBatch &rb, int log_n, cudaStream_t s);
-// Inverse NTT (bit-reversed input); epilogue x * c0 (Montgomery), canonical
-// or centred (kCentre).  tw must point at the inverse twiddle table.
+// Inverse NTT (bit-reversed input); epilogue x * c0, canonical or centred
+// (kCentre).  tw must point at the inverse twiddle table.
 void launch_ntt_inv(const RowBatch &rb, int log_n, cudaStream_t s);
 
 // Base conversion of one job: out[m][n] = (sum_k xt[k][n] * T[m][k]) * 2^-32
@@ -73,17 +74,22 @@ void launch_bconv(const BConvBatch &b, int log_n, cudaStream_t s);
 // Key-switching inner product with the P * (d0, d1) term folded in:
 //   acc_b[r] = sum_i mu_i[r] * kb_i[r] + (r < nq ? p_prod[r] * d0[r] : 0)
 //   acc_a[r] = sum_i mu_i[r] * ka_i[r] + (r < nq && d1 ? p_prod[r] * d1[r] : 0)
-struct KeyMacDesc {
+// for up to kMaxKeyMacCts ciphertexts sharing one key (grid.z = ciphertext).
+constexpr int kMaxKeyMacCts = 16;
+struct KeyMacCt {
   const uint32_t *mu[8];     // beta ModUp outputs, each [rows][N]
-  const uint32_t *kb[8];     // key bx of digit i, row-0 pointer of the key basis
-  const uint32_t *ka[8];
   const uint32_t *d0, *d1;   // [nq][N] or nullptr
   uint32_t *acc_b, *acc_a;   // [rows][N]
+};
+struct KeyMacDesc {
+  const uint32_t *kb[8];     // key bx of digit i, row-0 pointer of the key basis
+  const uint32_t *ka[8];
   uint32_t q[64];
   int32_t qinv[64];
   uint32_t p_prod[64];       // Montgomery P mod q, q rows only
   int16_t key_row[64];       // key basis row of accumulator row r
-  int beta, rows, nq;
+  int beta, rows, nq, count;
+  KeyMacCt ct[kMaxKeyMacCts];
 };
 void launch_key_mac(const KeyMacDesc &d, int log_n, cudaStream_t s);
 

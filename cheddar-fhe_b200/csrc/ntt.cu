@@ -4,20 +4,22 @@
 // forward transform of a limb a (natural order) is
 //     A[k] = sum_i a_i * psi^((2 brev(k) + 1) i)  mod q,
 // stored bit-reversed, with psi the primitive 2N-th root derived from the
-// smallest generator of Z_q^* and twiddles psi_rev[j] = psi^brev(j) held in
-// Montgomery form (src/core/NTT.cu:1233-1299 and include/common/
-// PrimeUtils.h:135-196 of the reference).  Stage m of the Cooley-Tukey network
-// pairs index j with j + N/(2m) using twiddle psi_rev[m + floor(j m / N)].
+// smallest generator of Z_q^* and twiddles psi_rev[j] = psi^brev(j)
+// (src/core/NTT.cu:1233-1299 and include/common/PrimeUtils.h:135-196 of the
+// reference).  Stage m of the Cooley-Tukey network pairs index j with
+// j + N/(2m) using twiddle psi_rev[m + floor(j m / N)]; the inverse runs the
+// Gentleman-Sande network with psi^-1.  All arithmetic is exact mod q: values
+// travel lazily in [0, 2q) between stages (Shoup products, arith.cuh) and are
+// reduced to [0, q) on output, so every output word is the canonical residue.
 //
 // Layout for N = 2^16: the limb is a 128 x 512 row-major matrix.  Stages
 // m = 1..64 only pair elements of the same column (128-point column
-// transforms, one CTA per 32-column tile); stages m = 128..32768 stay inside
-// one 512-element row (one CTA per 4 rows, radix-8 rounds exchanged through
-// shared memory).  The inverse runs the Gentleman-Sande network in the
-// opposite order (rows first, then columns) and fuses the per-limb output
-// constant (N^-1, the BConv q-hat^-1, ...) and the optional centring into the
-// column phase.  For N <= 2^15 the whole limb fits in shared memory and a
-// single kernel runs every stage.
+// transforms, one CTA per 32-column tile, shared twiddles); stages
+// m = 128..32768 stay inside one 512-element row (one CTA per 4 rows, three
+// radix-8 rounds exchanged through shared memory).  The inverse runs rows
+// first, then columns, and fuses the per-limb output constant and the
+// optional centring into the column phase.  For N <= 2^15 the whole limb
+// fits in shared memory and one kernel runs every stage.
 #include "arith.cuh"
 #include "kernels.h"
 
@@ -26,13 +28,49 @@ namespace {
 
 constexpr int kColTile = 32;
 
+// Radix-8 forward network on x[0..7] (three CT stages: distances 4, 2, 1 in
+// register index) with twiddles tw[b0], tw[b1 + g], tw[b2 + g].
+__device__ __forceinline__ void radix8_fwd(uint32_t *x, const uint2 *tw, int b0, int b1, int b2, uint32_t q) {
+  const uint2 w0 = __ldg(tw + b0);
+#pragma unroll
+  for (int k = 0; k < 4; k++) ct_lazy(x[k], x[k + 4], w0, q);
+#pragma unroll
+  for (int g = 0; g < 2; g++) {
+    const uint2 w1 = __ldg(tw + b1 + g);
+    ct_lazy(x[4 * g], x[4 * g + 2], w1, q);
+    ct_lazy(x[4 * g + 1], x[4 * g + 3], w1, q);
+  }
+#pragma unroll
+  for (int g = 0; g < 4; g++) {
+    const uint2 w2 = __ldg(tw + b2 + g);
+    ct_lazy(x[2 * g], x[2 * g + 1], w2, q);
+  }
+}
+
+// Radix-8 inverse network (GS stages at distances 1, 2, 4), mirror of the above.
+__device__ __forceinline__ void radix8_inv(uint32_t *x, const uint2 *tw, int b0, int b1, int b2, uint32_t q) {
+#pragma unroll
+  for (int g = 0; g < 4; g++) {
+    const uint2 w2 = __ldg(tw + b2 + g);
+    gs_lazy(x[2 * g], x[2 * g + 1], w2, q);
+  }
+#pragma unroll
+  for (int g = 0; g < 2; g++) {
+    const uint2 w1 = __ldg(tw + b1 + g);
+    gs_lazy(x[4 * g], x[4 * g + 2], w1, q);
+    gs_lazy(x[4 * g + 1], x[4 * g + 3], w1, q);
+  }
+  const uint2 w0 = __ldg(tw + b0);
+#pragma unroll
+  for (int k = 0; k < 4; k++) gs_lazy(x[k], x[k + 4], w0, q);
+}
+
 // ---------------------------------------------------------------- N = 2^16
 __global__ void __launch_bounds__(256) k_fwd_cols16(const __grid_constant__ RowBatch rb) {
   __shared__ uint32_t sm[128 * kColTile];
   const RowDesc &rd = rb.rows[blockIdx.y];
   const uint32_t q = rd.q;
-  const int32_t qi = rd.qinv;
-  const uint32_t *tw = rd.tw;
+  const uint2 *tw = rd.tw;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int c = blockIdx.x * kColTile + lane;
   uint32_t x[16];
@@ -40,7 +78,7 @@ __global__ void __launch_bounds__(256) k_fwd_cols16(const __grid_constant__ RowB
   for (int k = 0; k < 16; k++) x[k] = __ldg(rd.src + (w + 8 * k) * 512 + c);
   if (rd.flags & kPreMult) {
 #pragma unroll
-    for (int k = 0; k < 16; k++) x[k] = mont_mul(x[k], rd.c0, q, qi);
+    for (int k = 0; k < 16; k++) x[k] = shoup_lazy(x[k], rd.c0, rd.c0s, q);
   }
   // stages m = 1, 2, 4, 8 on rows w + 8k: pair (k, k + 8/m), group k / (16/m)
 #pragma unroll
@@ -48,9 +86,9 @@ __global__ void __launch_bounds__(256) k_fwd_cols16(const __grid_constant__ RowB
     const int m = 1 << s, h = 8 >> s;
 #pragma unroll
     for (int g = 0; g < m; g++) {
-      const uint32_t wv = __ldg(tw + m + g);
+      const uint2 wv = __ldg(tw + m + g);
 #pragma unroll
-      for (int j = 0; j < h; j++) ct_bfly(x[g * 2 * h + j], x[g * 2 * h + j + h], wv, q, qi);
+      for (int j = 0; j < h; j++) ct_lazy(x[g * 2 * h + j], x[g * 2 * h + j + h], wv, q);
     }
   }
 #pragma unroll
@@ -63,35 +101,19 @@ __global__ void __launch_bounds__(256) k_fwd_cols16(const __grid_constant__ RowB
     uint32_t y[8];
 #pragma unroll
     for (int u = 0; u < 8; u++) y[u] = sm[(8 * j + u) * kColTile + lane];
-    {
-      const uint32_t wv = __ldg(tw + 16 + j);
+    radix8_fwd(y, tw, 16 + j, 32 + 2 * j, 64 + 4 * j, q);
 #pragma unroll
-      for (int u = 0; u < 4; u++) ct_bfly(y[u], y[u + 4], wv, q, qi);
-    }
-#pragma unroll
-    for (int g = 0; g < 2; g++) {
-      const uint32_t wv = __ldg(tw + 32 + 2 * j + g);
-      ct_bfly(y[4 * g], y[4 * g + 2], wv, q, qi);
-      ct_bfly(y[4 * g + 1], y[4 * g + 3], wv, q, qi);
-    }
-#pragma unroll
-    for (int g = 0; g < 4; g++) {
-      const uint32_t wv = __ldg(tw + 64 + 4 * j + g);
-      ct_bfly(y[2 * g], y[2 * g + 1], wv, q, qi);
-    }
-#pragma unroll
-    for (int u = 0; u < 8; u++) rd.dst[(8 * j + u) * 512 + c] = y[u];
+    for (int u = 0; u < 8; u++) rd.dst[(8 * j + u) * 512 + c] = y[u];  // lazy [0, 2q)
   }
 }
 
-// Row phase of the forward transform, with the optional ModDown epilogue
-// (src2 * c1 - x) * c2.
+// Row phase of the forward transform (input lazy from the column phase),
+// canonical output, with the optional ModDown epilogue (src2 * c1 - x) * c2.
 __global__ void __launch_bounds__(256) k_fwd_rows16(const __grid_constant__ RowBatch rb) {
   __shared__ uint32_t sm[4][512];
   const RowDesc &rd = rb.rows[blockIdx.y];
   const uint32_t q = rd.q;
-  const int32_t qi = rd.qinv;
-  const uint32_t *tw = rd.tw;
+  const uint2 *tw = rd.tw;
   const int t = threadIdx.x & 63, rl = threadIdx.x >> 6;
   const int r = blockIdx.x * 4 + rl;
   uint32_t *srow = sm[rl];
@@ -99,69 +121,23 @@ __global__ void __launch_bounds__(256) k_fwd_rows16(const __grid_constant__ RowB
   uint32_t x[8];
 #pragma unroll
   for (int k = 0; k < 8; k++) x[k] = src[t + 64 * k];
-  // round 1: stages s = 0, 1, 2 on c = t + 64k
-  {
-    const uint32_t w0 = __ldg(tw + 128 + r);
-#pragma unroll
-    for (int k = 0; k < 4; k++) ct_bfly(x[k], x[k + 4], w0, q, qi);
-#pragma unroll
-    for (int g = 0; g < 2; g++) {
-      const uint32_t w1 = __ldg(tw + 256 + 2 * r + g);
-      ct_bfly(x[4 * g], x[4 * g + 2], w1, q, qi);
-      ct_bfly(x[4 * g + 1], x[4 * g + 3], w1, q, qi);
-    }
-#pragma unroll
-    for (int g = 0; g < 4; g++) {
-      const uint32_t w2 = __ldg(tw + 512 + 4 * r + g);
-      ct_bfly(x[2 * g], x[2 * g + 1], w2, q, qi);
-    }
-  }
+  radix8_fwd(x, tw, 128 + r, 256 + 2 * r, 512 + 4 * r, q);
 #pragma unroll
   for (int k = 0; k < 8; k++) srow[t + 64 * k] = x[k];
   __syncthreads();
-  // round 2: stages s = 3, 4, 5 on c = 64b + u0 + 8k
   const int b = t >> 3, u0 = t & 7;
 #pragma unroll
   for (int k = 0; k < 8; k++) x[k] = srow[64 * b + u0 + 8 * k];
-  {
-    const uint32_t w0 = __ldg(tw + 1024 + 8 * r + b);
-#pragma unroll
-    for (int k = 0; k < 4; k++) ct_bfly(x[k], x[k + 4], w0, q, qi);
-#pragma unroll
-    for (int g = 0; g < 2; g++) {
-      const uint32_t w1 = __ldg(tw + 2048 + 16 * r + 2 * b + g);
-      ct_bfly(x[4 * g], x[4 * g + 2], w1, q, qi);
-      ct_bfly(x[4 * g + 1], x[4 * g + 3], w1, q, qi);
-    }
-#pragma unroll
-    for (int g = 0; g < 4; g++) {
-      const uint32_t w2 = __ldg(tw + 4096 + 32 * r + 4 * b + g);
-      ct_bfly(x[2 * g], x[2 * g + 1], w2, q, qi);
-    }
-  }
+  radix8_fwd(x, tw, 1024 + 8 * r + b, 2048 + 16 * r + 2 * b, 4096 + 32 * r + 4 * b, q);
   __syncthreads();
 #pragma unroll
   for (int k = 0; k < 8; k++) srow[64 * b + u0 + 8 * k] = x[k];
   __syncthreads();
-  // round 3: stages s = 6, 7, 8 on c = 8t + k
 #pragma unroll
   for (int k = 0; k < 8; k++) x[k] = srow[8 * t + k];
-  {
-    const uint32_t w0 = __ldg(tw + 8192 + 64 * r + t);
+  radix8_fwd(x, tw, 8192 + 64 * r + t, 16384 + 128 * r + 2 * t, 32768 + 256 * r + 4 * t, q);
 #pragma unroll
-    for (int k = 0; k < 4; k++) ct_bfly(x[k], x[k + 4], w0, q, qi);
-#pragma unroll
-    for (int g = 0; g < 2; g++) {
-      const uint32_t w1 = __ldg(tw + 16384 + 128 * r + 2 * t + g);
-      ct_bfly(x[4 * g], x[4 * g + 2], w1, q, qi);
-      ct_bfly(x[4 * g + 1], x[4 * g + 3], w1, q, qi);
-    }
-#pragma unroll
-    for (int g = 0; g < 4; g++) {
-      const uint32_t w2 = __ldg(tw + 32768 + 256 * r + 4 * t + g);
-      ct_bfly(x[2 * g], x[2 * g + 1], w2, q, qi);
-    }
-  }
+  for (int k = 0; k < 8; k++) x[k] = reduce2q(x[k], q);
   const int base = r * 512 + 8 * t;
   if (rd.flags & kModDownEpi) {
     uint32_t v[8];
@@ -172,27 +148,26 @@ __global__ void __launch_bounds__(256) k_fwd_rows16(const __grid_constant__ RowB
       v[4] = a1.x; v[5] = a1.y; v[6] = a1.z; v[7] = a1.w;
       if (rd.flags & kPadSrc2) {
 #pragma unroll
-        for (int k = 0; k < 8; k++) v[k] = mont_mul(v[k], rd.c1, q, qi);
+        for (int k = 0; k < 8; k++) v[k] = reduce2q(shoup_lazy(v[k], rd.c1, rd.c1s, q), q);
       }
     } else {
 #pragma unroll
       for (int k = 0; k < 8; k++) v[k] = 0;
     }
 #pragma unroll
-    for (int k = 0; k < 8; k++) x[k] = mont_mul(sub_mod(v[k], x[k], q), rd.c2, q, qi);
+    for (int k = 0; k < 8; k++) x[k] = reduce2q(shoup_lazy(v[k] - x[k] + q, rd.c2, rd.c2s, q), q);
   }
   uint4 *o = reinterpret_cast<uint4 *>(rd.dst + base);
   o[0] = make_uint4(x[0], x[1], x[2], x[3]);
   o[1] = make_uint4(x[4], x[5], x[6], x[7]);
 }
 
-// Inverse, row phase: Gentleman-Sande stages m = 32768 .. 128.
+// Inverse, row phase: Gentleman-Sande stages m = 32768 .. 128 (lazy output).
 __global__ void __launch_bounds__(256) k_inv_rows16(const __grid_constant__ RowBatch rb) {
   __shared__ uint32_t sm[4][512];
   const RowDesc &rd = rb.rows[blockIdx.y];
   const uint32_t q = rd.q;
-  const int32_t qi = rd.qinv;
-  const uint32_t *tw = rd.tw;
+  const uint2 *tw = rd.tw;
   const int t = threadIdx.x & 63, rl = threadIdx.x >> 6;
   const int r = blockIdx.x * 4 + rl;
   uint32_t *srow = sm[rl];
@@ -204,80 +179,32 @@ __global__ void __launch_bounds__(256) k_inv_rows16(const __grid_constant__ RowB
     x[0] = a0.x; x[1] = a0.y; x[2] = a0.z; x[3] = a0.w;
     x[4] = a1.x; x[5] = a1.y; x[6] = a1.z; x[7] = a1.w;
   }
-  // stages s = 8, 7, 6 on c = 8t + k
-#pragma unroll
-  for (int g = 0; g < 4; g++) {
-    const uint32_t w2 = __ldg(tw + 32768 + 256 * r + 4 * t + g);
-    gs_bfly(x[2 * g], x[2 * g + 1], w2, q, qi);
-  }
-#pragma unroll
-  for (int g = 0; g < 2; g++) {
-    const uint32_t w1 = __ldg(tw + 16384 + 128 * r + 2 * t + g);
-    gs_bfly(x[4 * g], x[4 * g + 2], w1, q, qi);
-    gs_bfly(x[4 * g + 1], x[4 * g + 3], w1, q, qi);
-  }
-  {
-    const uint32_t w0 = __ldg(tw + 8192 + 64 * r + t);
-#pragma unroll
-    for (int k = 0; k < 4; k++) gs_bfly(x[k], x[k + 4], w0, q, qi);
-  }
+  radix8_inv(x, tw, 8192 + 64 * r + t, 16384 + 128 * r + 2 * t, 32768 + 256 * r + 4 * t, q);
 #pragma unroll
   for (int k = 0; k < 8; k++) srow[8 * t + k] = x[k];
   __syncthreads();
   const int b = t >> 3, u0 = t & 7;
 #pragma unroll
   for (int k = 0; k < 8; k++) x[k] = srow[64 * b + u0 + 8 * k];
-#pragma unroll
-  for (int g = 0; g < 4; g++) {
-    const uint32_t w2 = __ldg(tw + 4096 + 32 * r + 4 * b + g);
-    gs_bfly(x[2 * g], x[2 * g + 1], w2, q, qi);
-  }
-#pragma unroll
-  for (int g = 0; g < 2; g++) {
-    const uint32_t w1 = __ldg(tw + 2048 + 16 * r + 2 * b + g);
-    gs_bfly(x[4 * g], x[4 * g + 2], w1, q, qi);
-    gs_bfly(x[4 * g + 1], x[4 * g + 3], w1, q, qi);
-  }
-  {
-    const uint32_t w0 = __ldg(tw + 1024 + 8 * r + b);
-#pragma unroll
-    for (int k = 0; k < 4; k++) gs_bfly(x[k], x[k + 4], w0, q, qi);
-  }
+  radix8_inv(x, tw, 1024 + 8 * r + b, 2048 + 16 * r + 2 * b, 4096 + 32 * r + 4 * b, q);
   __syncthreads();
 #pragma unroll
   for (int k = 0; k < 8; k++) srow[64 * b + u0 + 8 * k] = x[k];
   __syncthreads();
 #pragma unroll
   for (int k = 0; k < 8; k++) x[k] = srow[t + 64 * k];
-#pragma unroll
-  for (int g = 0; g < 4; g++) {
-    const uint32_t w2 = __ldg(tw + 512 + 4 * r + g);
-    gs_bfly(x[2 * g], x[2 * g + 1], w2, q, qi);
-  }
-#pragma unroll
-  for (int g = 0; g < 2; g++) {
-    const uint32_t w1 = __ldg(tw + 256 + 2 * r + g);
-    gs_bfly(x[4 * g], x[4 * g + 2], w1, q, qi);
-    gs_bfly(x[4 * g + 1], x[4 * g + 3], w1, q, qi);
-  }
-  {
-    const uint32_t w0 = __ldg(tw + 128 + r);
-#pragma unroll
-    for (int k = 0; k < 4; k++) gs_bfly(x[k], x[k + 4], w0, q, qi);
-  }
+  radix8_inv(x, tw, 128 + r, 256 + 2 * r, 512 + 4 * r, q);
   uint32_t *dst = rd.dst + r * 512;
 #pragma unroll
   for (int k = 0; k < 8; k++) dst[t + 64 * k] = x[k];
 }
 
-// Inverse, column phase: stages m = 64 .. 1, then x * c0 (Montgomery),
-// canonical or centred.
+// Inverse, column phase: stages m = 64 .. 1, then x * c0, canonical or centred.
 __global__ void __launch_bounds__(256) k_inv_cols16(const __grid_constant__ RowBatch rb) {
   __shared__ uint32_t sm[128 * kColTile];
   const RowDesc &rd = rb.rows[blockIdx.y];
   const uint32_t q = rd.q;
-  const int32_t qi = rd.qinv;
-  const uint32_t *tw = rd.tw;
+  const uint2 *tw = rd.tw;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int c = blockIdx.x * kColTile + lane;
   const uint32_t *src = rd.dst;  // the row phase wrote dst
@@ -287,22 +214,7 @@ __global__ void __launch_bounds__(256) k_inv_cols16(const __grid_constant__ RowB
     uint32_t y[8];
 #pragma unroll
     for (int u = 0; u < 8; u++) y[u] = src[(8 * j + u) * 512 + c];
-#pragma unroll
-    for (int g = 0; g < 4; g++) {
-      const uint32_t wv = __ldg(tw + 64 + 4 * j + g);
-      gs_bfly(y[2 * g], y[2 * g + 1], wv, q, qi);
-    }
-#pragma unroll
-    for (int g = 0; g < 2; g++) {
-      const uint32_t wv = __ldg(tw + 32 + 2 * j + g);
-      gs_bfly(y[4 * g], y[4 * g + 2], wv, q, qi);
-      gs_bfly(y[4 * g + 1], y[4 * g + 3], wv, q, qi);
-    }
-    {
-      const uint32_t wv = __ldg(tw + 16 + j);
-#pragma unroll
-      for (int u = 0; u < 4; u++) gs_bfly(y[u], y[u + 4], wv, q, qi);
-    }
+    radix8_inv(y, tw, 16 + j, 32 + 2 * j, 64 + 4 * j, q);
 #pragma unroll
     for (int u = 0; u < 8; u++) sm[(8 * j + u) * kColTile + lane] = y[u];
   }
@@ -316,15 +228,15 @@ __global__ void __launch_bounds__(256) k_inv_cols16(const __grid_constant__ RowB
     const int m = 1 << s, h = 8 >> s;
 #pragma unroll
     for (int g = 0; g < m; g++) {
-      const uint32_t wv = __ldg(tw + m + g);
+      const uint2 wv = __ldg(tw + m + g);
 #pragma unroll
-      for (int j = 0; j < h; j++) gs_bfly(x[g * 2 * h + j], x[g * 2 * h + j + h], wv, q, qi);
+      for (int j = 0; j < h; j++) gs_lazy(x[g * 2 * h + j], x[g * 2 * h + j + h], wv, q);
     }
   }
   const bool centre_out = (rd.flags & kCentre) != 0;
 #pragma unroll
   for (int k = 0; k < 16; k++) {
-    uint32_t v = mont_mul(x[k], rd.c0, q, qi);
+    uint32_t v = reduce2q(shoup_lazy(x[k], rd.c0, rd.c0s, q), q);
     if (centre_out) v = static_cast<uint32_t>(centre(v, q));
     rd.dst[(w + 8 * k) * 512 + c] = v;
   }
@@ -337,12 +249,11 @@ __global__ void __launch_bounds__(1024) k_small(const __grid_constant__ RowBatch
   extern __shared__ uint32_t sa[];
   const RowDesc &rd = rb.rows[blockIdx.x];
   const uint32_t q = rd.q;
-  const int32_t qi = rd.qinv;
-  const uint32_t *tw = rd.tw;
+  const uint2 *tw = rd.tw;
   const int n = 1 << log_n, half = n >> 1;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     uint32_t v = rd.src[i];
-    if (kFwd && (rd.flags & kPreMult)) v = mont_mul(v, rd.c0, q, qi);
+    if (kFwd && (rd.flags & kPreMult)) v = shoup_lazy(v, rd.c0, rd.c0s, q);
     sa[i] = v;
   }
   __syncthreads();
@@ -351,7 +262,7 @@ __global__ void __launch_bounds__(1024) k_small(const __grid_constant__ RowBatch
       const int t = 1 << lt;
       for (int b = threadIdx.x; b < half; b += blockDim.x) {
         const int i = b >> lt, j = 2 * i * t + (b & (t - 1));
-        ct_bfly(sa[j], sa[j + t], __ldg(tw + m + i), q, qi);
+        ct_lazy(sa[j], sa[j + t], __ldg(tw + m + i), q);
       }
       __syncthreads();
     }
@@ -360,24 +271,24 @@ __global__ void __launch_bounds__(1024) k_small(const __grid_constant__ RowBatch
       const int t = 1 << lt;
       for (int b = threadIdx.x; b < half; b += blockDim.x) {
         const int i = b >> lt, j = 2 * i * t + (b & (t - 1));
-        gs_bfly(sa[j], sa[j + t], __ldg(tw + m + i), q, qi);
+        gs_lazy(sa[j], sa[j + t], __ldg(tw + m + i), q);
       }
       __syncthreads();
     }
   }
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    uint32_t x = sa[i];
+    uint32_t x = reduce2q(sa[i], q);
     if (kFwd) {
       if (rd.flags & kModDownEpi) {
         uint32_t v = 0;
         if (rd.flags & kHasSrc2) {
           v = rd.src2[i];
-          if (rd.flags & kPadSrc2) v = mont_mul(v, rd.c1, q, qi);
+          if (rd.flags & kPadSrc2) v = reduce2q(shoup_lazy(v, rd.c1, rd.c1s, q), q);
         }
-        x = mont_mul(sub_mod(v, x, q), rd.c2, q, qi);
+        x = reduce2q(shoup_lazy(v - x + q, rd.c2, rd.c2s, q), q);
       }
     } else {
-      x = mont_mul(x, rd.c0, q, qi);
+      x = reduce2q(shoup_lazy(x, rd.c0, rd.c0s, q), q);
       if (rd.flags & kCentre) x = static_cast<uint32_t>(centre(x, q));
     }
     rd.dst[i] = x;
