@@ -866,6 +866,7 @@ Status Context::modup_many(int level, int count, const uint32_t *const *src, uin
   ArenaScope scope(arena);
   int32_t *xt = static_cast<int32_t *>(arena.alloc(static_cast<size_t>(count) * nq * n * 4));
   CHD_CHECK(xt, kErrAlloc, "modup: scratch allocation failed");
+  if (P->log_n == 16) return modup_fused(level, count, src, dst, reinterpret_cast<uint32_t *>(xt));
   // 1. INTT * (N q-hat_i)^-1, centred (INTTAndMultConst with normalize)
   std::vector<RowDesc> rows;
   for (int c = 0; c < count; c++)
@@ -929,6 +930,81 @@ Status Context::modup_many(int level, int count, const uint32_t *const *src, uin
   return check_cuda("modup");
 }
 
+// N = 2^16: INTT row phase -> fused column pass (INTT columns, centred
+// constant, BConv, NTT columns) -> NTT row phase.
+Status Context::modup_fused(int level, int count, const uint32_t *const *src, uint32_t *const *const *dst,
+                            uint32_t *rows_out) {
+  const LevelMS &m = lms(level);
+  const int n = P->n;
+  NP np = P->level_np(level, m.num_aux);
+  const int nq = np.q(), tot = np.total();
+  std::vector<int> g(tot);
+  P->gidx(np, g.data());
+  std::vector<RowDesc> rows;
+  for (int c = 0; c < count; c++)
+    for (int r = 0; r < nq; r++) {
+      RowDesc d{};
+      d.src = src[c] + static_cast<size_t>(r) * n;
+      d.dst = rows_out + (static_cast<size_t>(c) * nq + r) * n;
+      d.tw = itw(g[r]);
+      d.q = P->primes[g[r]];
+      rows.push_back(d);
+    }
+  for_row_batches(rows, [&](const RowBatch &rb) { launch_ntt_inv_rows(rb, P->log_n, stream); });
+  MSColBatch b{};
+  b.tw = d_tw;
+  b.itw = d_itw;
+  b.primes = d_primes;
+  b.qinvs = d_qinv;
+  for (int c = 0; c < count; c++)
+    for (int i = 0; i < m.beta; i++) {
+      const int s = m.dig_s[i], e = m.dig_e[i];
+      if (e <= 0) continue;
+      cudaMemcpyAsync(dst[c][i] + static_cast<size_t>(s) * n, src[c] + static_cast<size_t>(s) * n,
+                      static_cast<size_t>(e - s) * n * 4, cudaMemcpyDeviceToDevice, stream);
+      MSColJob &j = b.jobs[b.count++];
+      j.src = rows_out + static_cast<size_t>(c) * nq * n;
+      j.dst = dst[c][i];
+      j.table = m.d_mod_up2[i];
+      j.K = e - s;
+      j.M = tot - (e - s);
+      CHD_CHECK(j.K <= 16 && j.M <= 64, kErrUnsupported, "modup: digit too large");
+      for (int k = 0; k < j.K; k++) {
+        j.src_row[k] = static_cast<uint8_t>(s + k);
+        j.src_gidx[k] = static_cast<uint8_t>(g[s + k]);
+        mont_as_shoup(m.mod_up1[s + k], g[s + k], &j.c0[k], &j.c0s[k]);
+      }
+      int k = 0;
+      for (int r = 0; r < tot; r++) {
+        if (r >= s && r < e) continue;
+        j.dst_row[k] = static_cast<uint8_t>(r);
+        j.dst_gidx[k] = static_cast<uint8_t>(g[r]);
+        k++;
+      }
+      if (b.count == kMaxMSColJobs) {
+        launch_modswitch_cols(b, P->log_n, stream);
+        b.count = 0;
+      }
+    }
+  launch_modswitch_cols(b, P->log_n, stream);
+  rows.clear();
+  for (int c = 0; c < count; c++)
+    for (int i = 0; i < m.beta; i++) {
+      const int s = m.dig_s[i], e = m.dig_e[i];
+      if (e <= 0) continue;
+      for (int r = 0; r < tot; r++) {
+        if (r >= s && r < e) continue;
+        RowDesc d{};
+        d.src = d.dst = dst[c][i] + static_cast<size_t>(r) * n;
+        d.tw = tw(g[r]);
+        d.q = P->primes[g[r]];
+        rows.push_back(d);
+      }
+    }
+  for_row_batches(rows, [&](const RowBatch &rb) { launch_ntt_fwd_rows(rb, P->log_n, stream); });
+  return check_cuda("modup");
+}
+
 Status Context::moddown(int level, MDType type, const uint32_t *const *src, uint32_t *const *dst, int npoly) {
   // ModSwitch.cu:566-684 with NTT.cu:973-1128 and the fused epilogue of
   // NTT.cu:456-601
@@ -964,6 +1040,7 @@ Status Context::moddown(int level, MDType type, const uint32_t *const *src, uint
   int32_t *xt = static_cast<int32_t *>(arena.alloc(static_cast<size_t>(npoly) * src_len * n * 4));
   CHD_CHECK(xt, kErrAlloc, "moddown: scratch allocation failed");
   std::vector<RowDesc> rows;
+  const bool fused = P->log_n == 16;
   for (int p = 0; p < npoly; p++)
     for (int i = 0; i < src_len; i++) {
       const int gg = gs[srows[i]];
@@ -976,27 +1053,59 @@ Status Context::moddown(int level, MDType type, const uint32_t *const *src, uint
       d.flags = kCentre;
       rows.push_back(d);
     }
-  for_row_batches(rows, [&](const RowBatch &rb) { launch_ntt_inv(rb, P->log_n, stream); });
-  BConvBatch b{};
-  b.primes = d_primes;
-  b.qinvs = d_qinv;
-  for (int p = 0; p < npoly; p++) {
-    BConvJob &j = b.jobs[b.count++];
-    j.xt = xt + static_cast<size_t>(p) * src_len * n;
-    j.out = dst[p];
-    j.table = table;
-    j.K = src_len;
-    j.M = dst_len;
-    for (int y = 0; y < dst_len; y++) {
-      j.out_row[y] = static_cast<uint8_t>(y);
-      j.out_gidx[y] = static_cast<uint8_t>(gd[y]);
+  if (fused) {
+    for_row_batches(rows, [&](const RowBatch &rb) { launch_ntt_inv_rows(rb, P->log_n, stream); });
+    MSColBatch b{};
+    b.tw = d_tw;
+    b.itw = d_itw;
+    b.primes = d_primes;
+    b.qinvs = d_qinv;
+    for (int p = 0; p < npoly; p++) {
+      MSColJob &j = b.jobs[b.count++];
+      j.src = reinterpret_cast<uint32_t *>(xt) + static_cast<size_t>(p) * src_len * n;
+      j.dst = dst[p];
+      j.table = table;
+      j.K = src_len;
+      j.M = dst_len;
+      for (int i = 0; i < src_len; i++) {
+        const int gg = gs[srows[i]];
+        j.src_row[i] = static_cast<uint8_t>(i);
+        j.src_gidx[i] = static_cast<uint8_t>(gg);
+        mont_as_shoup(c1[i], gg, &j.c0[i], &j.c0s[i]);
+      }
+      for (int y = 0; y < dst_len; y++) {
+        j.dst_row[y] = static_cast<uint8_t>(y);
+        j.dst_gidx[y] = static_cast<uint8_t>(gd[y]);
+      }
+      if (b.count == kMaxMSColJobs) {
+        launch_modswitch_cols(b, P->log_n, stream);
+        b.count = 0;
+      }
     }
-    if (b.count == kMaxBConvJobs) {
-      launch_bconv(b, P->log_n, stream);
-      b.count = 0;
+    launch_modswitch_cols(b, P->log_n, stream);
+  } else {
+    for_row_batches(rows, [&](const RowBatch &rb) { launch_ntt_inv(rb, P->log_n, stream); });
+    BConvBatch b{};
+    b.primes = d_primes;
+    b.qinvs = d_qinv;
+    for (int p = 0; p < npoly; p++) {
+      BConvJob &j = b.jobs[b.count++];
+      j.xt = xt + static_cast<size_t>(p) * src_len * n;
+      j.out = dst[p];
+      j.table = table;
+      j.K = src_len;
+      j.M = dst_len;
+      for (int y = 0; y < dst_len; y++) {
+        j.out_row[y] = static_cast<uint8_t>(y);
+        j.out_gidx[y] = static_cast<uint8_t>(gd[y]);
+      }
+      if (b.count == kMaxBConvJobs) {
+        launch_bconv(b, P->log_n, stream);
+        b.count = 0;
+      }
     }
+    launch_bconv(b, P->log_n, stream);
   }
-  launch_bconv(b, P->log_n, stream);
   const int src2_start = nd.ter - nn.ter, src2_end = src2_start + nn.q();
   const int src2_off = std::max(0, ns.ter - nd.ter);
   rows.clear();
@@ -1018,7 +1127,10 @@ Status Context::moddown(int level, MDType type, const uint32_t *const *src, uint
       }
       rows.push_back(d);
     }
-  for_row_batches(rows, [&](const RowBatch &rb) { launch_ntt_fwd(rb, P->log_n, stream); });
+  if (fused)
+    for_row_batches(rows, [&](const RowBatch &rb) { launch_ntt_fwd_rows(rb, P->log_n, stream); });
+  else
+    for_row_batches(rows, [&](const RowBatch &rb) { launch_ntt_fwd(rb, P->log_n, stream); });
   return check_cuda("moddown");
 }
 

@@ -184,6 +184,8 @@ class Context {
   // ModUp of src [num_q][N] at `level` into dst[beta] ([num_q + aux][N] each)
   Status modup(int level, const uint32_t *src, uint32_t *const *dst);
   Status modup_many(int level, int count, const uint32_t *const *src, uint32_t *const *const *dst);
+  Status modup_fused(int level, int count, const uint32_t *const *src, uint32_t *const *const *dst,
+                     uint32_t *rows_out);
   enum class MDType { kModDown, kRescale, kModDownRescale };
   // ModDown family on npoly polys
   Status moddown(int level, MDType type, const uint32_t *const *src, uint32_t *const *dst, int npoly);

@@ -71,6 +71,32 @@ struct BConvBatch {
 };
 void launch_bconv(const BConvBatch &b, int log_n, cudaStream_t s);
 
+// Fused ModSwitch column pass (N = 2^16 only): per 16-column tile
+//   x~_k  = centre(INTT column phase(src_k) * c0_k)        (K <= 16 sources)
+//   y_m   = (sum_k x~_k T[m][k]) * 2^-32 mod p_m           (exact BConv)
+//   dst_m = NTT column phase(y_m)                          (lazy [0, 2q))
+// src_k = src + src_row[k] * N holds the INTT row-phase output; dst_m =
+// dst + dst_row[m] * N is finished by launch_ntt_fwd_rows.
+struct MSColJob {
+  const uint32_t *src;
+  uint32_t *dst;
+  const int32_t *table;  // device [M][K]
+  int K, M;
+  uint8_t src_row[16], src_gidx[16];
+  uint8_t dst_row[64], dst_gidx[64];
+  uint32_t c0[16], c0s[16];
+};
+constexpr int kMaxMSColJobs = 24;
+struct MSColBatch {
+  int count;
+  const uint2 *tw, *itw;  // twiddle tables [nprimes][N]
+  const uint32_t *primes;
+  const int32_t *qinvs;
+  MSColJob jobs[kMaxMSColJobs];
+};
+void launch_modswitch_cols(const MSColBatch &b, int log_n, cudaStream_t s);
+void launch_ntt_inv_rows(const RowBatch &rb, int log_n, cudaStream_t s);
+
 // Key-switching inner product with the P * (d0, d1) term folded in:
 //   acc_b[r] = sum_i mu_i[r] * kb_i[r] + (r < nq ? p_prod[r] * d0[r] : 0)
 //   acc_a[r] = sum_i mu_i[r] * ka_i[r] + (r < nq && d1 ? p_prod[r] * d1[r] : 0)

@@ -1,0 +1,195 @@
+// Fused ModSwitch column kernel for N = 2^16.
+//
+// ModUp and ModDown (src/core/ModSwitch.cu:429-684 of the reference) are
+//   INTT(sources) * (N q-hat_k)^-1 (centred)  ->  BConv  ->  NTT(targets).
+// With the 128 x 512 limb layout used by ntt.cu, the INTT's last phase, the
+// base conversion and the NTT's first phase all act on the same columns, so
+// one CTA can take a 16-column tile through all three without touching HBM
+// in between: the K centred sources of the tile stay in shared memory
+// (K x 8 KB) and every target is converted, transformed and written once.
+// The row phases before (INTT) and after (NTT, with the ModDown epilogue)
+// stay in ntt.cu.
+//
+// Per tile and thread: 16 elements of one column.  The column transforms use
+// the same stage schedule as ntt.cu (radix-16 on rows rg + 8k in registers,
+// radix-8 on rows 8j + u after one shared-memory exchange).
+#include "arith.cuh"
+#include "kernels.h"
+
+namespace chd {
+namespace {
+
+constexpr int kTC = 16;          // columns per tile
+constexpr int kExRows = 136;     // 128 rows + one padding row per 16 rows
+
+// exchange-buffer index: a 16-word gap every 16 rows keeps both access
+// patterns (rows rg + 8k and rows 8j + u) free of bank conflicts
+__device__ __forceinline__ int exi(int row, int col) { return (row + (row >> 4)) * kTC + col; }
+
+__device__ __forceinline__ void radix8_fwd_c(uint32_t *x, const uint2 *tw, int b0, int b1, int b2, uint32_t q) {
+  const uint2 w0 = __ldg(tw + b0);
+#pragma unroll
+  for (int k = 0; k < 4; k++) ct_lazy(x[k], x[k + 4], w0, q);
+#pragma unroll
+  for (int g = 0; g < 2; g++) {
+    const uint2 w1 = __ldg(tw + b1 + g);
+    ct_lazy(x[4 * g], x[4 * g + 2], w1, q);
+    ct_lazy(x[4 * g + 1], x[4 * g + 3], w1, q);
+  }
+#pragma unroll
+  for (int g = 0; g < 4; g++) {
+    const uint2 w2 = __ldg(tw + b2 + g);
+    ct_lazy(x[2 * g], x[2 * g + 1], w2, q);
+  }
+}
+
+__device__ __forceinline__ void radix8_inv_c(uint32_t *x, const uint2 *tw, int b0, int b1, int b2, uint32_t q) {
+#pragma unroll
+  for (int g = 0; g < 4; g++) {
+    const uint2 w2 = __ldg(tw + b2 + g);
+    gs_lazy(x[2 * g], x[2 * g + 1], w2, q);
+  }
+#pragma unroll
+  for (int g = 0; g < 2; g++) {
+    const uint2 w1 = __ldg(tw + b1 + g);
+    gs_lazy(x[4 * g], x[4 * g + 2], w1, q);
+    gs_lazy(x[4 * g + 1], x[4 * g + 3], w1, q);
+  }
+  const uint2 w0 = __ldg(tw + b0);
+#pragma unroll
+  for (int k = 0; k < 4; k++) gs_lazy(x[k], x[k + 4], w0, q);
+}
+
+template <int KMAX>
+__global__ void __launch_bounds__(128) k_modswitch_cols(const __grid_constant__ MSColBatch b) {
+  extern __shared__ uint32_t smem[];
+  const MSColJob &jb = b.jobs[blockIdx.y];
+  uint32_t *ex = smem;
+  int32_t *xs = reinterpret_cast<int32_t *>(smem + kExRows * kTC);  // [K][128][kTC]
+  const int t = threadIdx.x, w = t >> 5, lane = t & 31;
+  const int cl = lane & 15, rg = 2 * w + (lane >> 4);
+  const int col = blockIdx.x * kTC + cl;
+  const int K = jb.K;
+
+  // ---- phase A: INTT column stages, output constant, centring -> xs
+  for (int k = 0; k < K; k++) {
+    const int g = jb.src_gidx[k];
+    const uint32_t q = __ldg(b.primes + g);
+    const uint2 *itw = b.itw + (static_cast<size_t>(g) << 16);
+    const uint32_t *src = jb.src + (static_cast<size_t>(jb.src_row[k]) << 16);
+#pragma unroll
+    for (int hh = 0; hh < 2; hh++) {
+      const int j = 2 * rg + hh;
+      uint32_t y[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) y[u] = __ldg(src + (8 * j + u) * 512 + col);
+      radix8_inv_c(y, itw, 16 + j, 32 + 2 * j, 64 + 4 * j, q);
+#pragma unroll
+      for (int u = 0; u < 8; u++) ex[exi(8 * j + u, cl)] = y[u];
+    }
+    __syncthreads();
+    uint32_t x[16];
+#pragma unroll
+    for (int e = 0; e < 16; e++) x[e] = ex[exi(rg + 8 * e, cl)];
+#pragma unroll
+    for (int s = 3; s >= 0; s--) {
+      const int m = 1 << s, h = 8 >> s;
+#pragma unroll
+      for (int gg = 0; gg < m; gg++) {
+        const uint2 wv = __ldg(itw + m + gg);
+#pragma unroll
+        for (int i = 0; i < h; i++) gs_lazy(x[gg * 2 * h + i], x[gg * 2 * h + i + h], wv, q);
+      }
+    }
+    const uint32_t c0 = jb.c0[k], c0s = jb.c0s[k];
+#pragma unroll
+    for (int e = 0; e < 16; e++) {
+      const uint32_t v = reduce2q(shoup_lazy(x[e], c0, c0s, q), q);
+      xs[(k * 128 + rg + 8 * e) * kTC + cl] = centre(v, q);
+    }
+    __syncthreads();
+  }
+
+  // ---- phase B: exact BConv per target, then NTT column stages
+  for (int m = 0; m < jb.M; m++) {
+    const int g = jb.dst_gidx[m];
+    const uint32_t p = __ldg(b.primes + g);
+    const int32_t pinv = __ldg(b.qinvs + g);
+    const uint2 *tw = b.tw + (static_cast<size_t>(g) << 16);
+    const int32_t *T = jb.table + m * K;
+    uint32_t v[16];
+#pragma unroll
+    for (int e = 0; e < 16; e++) v[e] = 0;
+#pragma unroll
+    for (int k0 = 0; k0 < KMAX; k0 += 4) {
+      if (k0 < K) {
+        int64_t a[16];
+#pragma unroll
+        for (int e = 0; e < 16; e++) a[e] = 0;
+#pragma unroll
+        for (int k = k0; k < k0 + 4; k++) {
+          if (k < K) {
+            const int64_t tk = __ldg(T + k);
+            const int32_t *xk = xs + (k * 128 + rg) * kTC + cl;
+#pragma unroll
+            for (int e = 0; e < 16; e++) a[e] += static_cast<int64_t>(xk[8 * e * kTC]) * tk;
+          }
+        }
+#pragma unroll
+        for (int e = 0; e < 16; e++) v[e] = add_mod(v[e], mont_reduce(a[e], p, pinv), p);
+      }
+    }
+    // forward stages m = 1, 2, 4, 8 on rows rg + 8e
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+      const int mm = 1 << s, h = 8 >> s;
+#pragma unroll
+      for (int gg = 0; gg < mm; gg++) {
+        const uint2 wv = __ldg(tw + mm + gg);
+#pragma unroll
+        for (int i = 0; i < h; i++) ct_lazy(v[gg * 2 * h + i], v[gg * 2 * h + i + h], wv, p);
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < 16; e++) ex[exi(rg + 8 * e, cl)] = v[e];
+    __syncthreads();
+    uint32_t *dst = jb.dst + (static_cast<size_t>(jb.dst_row[m]) << 16);
+#pragma unroll
+    for (int hh = 0; hh < 2; hh++) {
+      const int j = 2 * rg + hh;
+      uint32_t y[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) y[u] = ex[exi(8 * j + u, cl)];
+      radix8_fwd_c(y, tw, 16 + j, 32 + 2 * j, 64 + 4 * j, p);
+#pragma unroll
+      for (int u = 0; u < 8; u++) dst[(8 * j + u) * 512 + col] = y[u];
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+size_t modswitch_cols_smem(int kmax) { return (static_cast<size_t>(kExRows) * kTC + static_cast<size_t>(kmax) * 128 * kTC) * 4; }
+
+void launch_modswitch_cols(const MSColBatch &b, int log_n, cudaStream_t s) {
+  if (b.count <= 0 || log_n != 16) return;
+  int max_k = 0;
+  for (int j = 0; j < b.count; j++) max_k = b.jobs[j].K > max_k ? b.jobs[j].K : max_k;
+  const dim3 grid(512 / kTC, b.count);
+  if (max_k <= 8) {
+    const size_t sm = modswitch_cols_smem(8);
+    cudaFuncSetAttribute(k_modswitch_cols<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm));
+    k_modswitch_cols<8><<<grid, 128, sm, s>>>(b);
+  } else if (max_k <= 12) {
+    const size_t sm = modswitch_cols_smem(12);
+    cudaFuncSetAttribute(k_modswitch_cols<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm));
+    k_modswitch_cols<12><<<grid, 128, sm, s>>>(b);
+  } else {
+    const size_t sm = modswitch_cols_smem(16);
+    cudaFuncSetAttribute(k_modswitch_cols<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm));
+    k_modswitch_cols<16><<<grid, 128, sm, s>>>(b);
+  }
+}
+
+}  // namespace chd

@@ -319,6 +319,11 @@ void launch_ntt_fwd(const RowBatch &rb, int log_n, cudaStream_t s) {
   }
 }
 
+void launch_ntt_inv_rows(const RowBatch &rb, int log_n, cudaStream_t s) {
+  if (rb.count <= 0) return;
+  k_inv_rows16<<<dim3(128 / 4, rb.count), 256, 0, s>>>(rb);
+}
+
 void launch_ntt_inv(const RowBatch &rb, int log_n, cudaStream_t s) {
   if (rb.count <= 0) return;
   if (log_n == 16) {
