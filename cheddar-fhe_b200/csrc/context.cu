@@ -1005,6 +1005,228 @@ Status Context::modup_fused(int level, int count, const uint32_t *const *src, ui
   return check_cuda("modup");
 }
 
+Status Context::moddown_plan(int level, MDType type, MDPlan *pl) const {
+  const LevelMS &m = lms(level);
+  CHD_CHECK(type == MDType::kModDown || m.has_rescale, kErrInvalidLevel, "rescale not available at this level");
+  const int nsa = type == MDType::kRescale ? 0 : m.num_aux;
+  pl->ns = P->level_np(level, nsa);
+  pl->nd = P->level_np(type == MDType::kModDown ? level : level - 1, 0);
+  pl->nn = NP{std::min(pl->ns.main, pl->nd.main), std::min(pl->ns.ter, pl->nd.ter), 0};
+  pl->src_len = pl->ns.total() - pl->nn.total();
+  pl->dst_len = pl->nd.total();
+  CHD_CHECK(pl->src_len >= 1 && pl->src_len <= 16, kErrUnsupported, "moddown: more than 16 dropped primes");
+  pl->c1 = type == MDType::kModDown ? m.mod_down1.data() : type == MDType::kRescale ? m.rs1.data() : m.mdr1.data();
+  pl->table = type == MDType::kModDown ? m.d_mod_down2 : type == MDType::kRescale ? m.d_rs2 : m.d_mdr2;
+  pl->inv = type == MDType::kModDown ? m.inv_p_prod.data() : type == MDType::kRescale ? m.rs_inv.data() : m.mdr_inv.data();
+  pl->pad = type == MDType::kModDown ? nullptr : type == MDType::kRescale ? m.rs_pad.data() : m.mdr_pad.data();
+  pl->gs.assign(pl->ns.total(), 0);
+  pl->gd.assign(pl->nd.total(), 0);
+  P->gidx(pl->ns, pl->gs.data());
+  P->gidx(pl->nd, pl->gd.data());
+  pl->srows.clear();
+  const bool on_main = pl->ns.main > pl->nn.main, on_ter = pl->ns.ter > pl->nn.ter;
+  CHD_CHECK(!(on_main && on_ter), kErrInvalidArg, "moddown: invalid prime combination");
+  if (!on_ter)
+    for (int r = pl->ns.ter + pl->nn.main; r < pl->ns.q(); r++) pl->srows.push_back(r);
+  else
+    for (int r = 0; r < pl->ns.ter - pl->nn.ter; r++) pl->srows.push_back(r);
+  for (int a = 0; a < nsa; a++) pl->srows.push_back(pl->ns.q() + a);
+  CHD_CHECK(static_cast<int>(pl->srows.size()) == pl->src_len, kErrInvalidArg, "moddown: internal row mismatch");
+  pl->src2_start = pl->nd.ter - pl->nn.ter;
+  pl->src2_end = pl->src2_start + pl->nn.q();
+  pl->src2_off = std::max(0, pl->ns.ter - pl->nd.ter);
+  return kOk;
+}
+
+Status Context::key_switch_fused(int level, int count, const KSIn *in, const DeviceEvk &key, MDType type) {
+  CHD_CHECK(P->log_n == 16, kErrUnsupported, "fused key switch needs N = 2^16");
+  CHD_CHECK(type != MDType::kRescale, kErrInvalidArg, "fused key switch ends in ModDown or ModDownAndRescale");
+  const LevelMS &m = lms(level);
+  const int n = P->n;
+  NP np = P->level_np(level, P->alpha);
+  const int nq = np.q(), tot = np.total();
+  CHD_CHECK(tot <= 64 && m.beta <= 8, kErrUnsupported, "key switch: more than 64 primes or 8 digits");
+  CHD_CHECK(key.np.aux == P->alpha && key.np.q() == P->L, kErrKey, "key switch: key basis mismatch");
+  MDPlan pl;
+  CHD_TRY(moddown_plan(level, type, &pl));
+  const int prime_offset = P->max_ter - np.ter;
+  std::vector<int> g(tot);
+  P->gidx(np, g.data());
+  std::vector<int> digits;
+  for (int i = 0; i < m.beta; i++)
+    if (m.dig_e[i] > 0) {
+      CHD_CHECK(i < key.beta, kErrKey, "key switch: key has too few digits");
+      digits.push_back(i);
+    }
+  const int nb = static_cast<int>(digits.size());
+  ArenaScope scope(arena);
+  const size_t N = static_cast<size_t>(n);
+  uint32_t *t1 = static_cast<uint32_t *>(arena.alloc(count * nq * N * 4));
+  uint32_t *mu = static_cast<uint32_t *>(arena.alloc(count * nb * tot * N * 4));
+  uint32_t *acc = static_cast<uint32_t *>(arena.alloc(count * 2 * tot * N * 4));
+  uint32_t *drop = static_cast<uint32_t *>(arena.alloc(count * 2 * pl.src_len * N * 4));
+  CHD_CHECK(t1 && mu && acc && drop, kErrAlloc, "key switch: scratch allocation failed");
+  auto MU = [&](int c, int b) { return mu + (static_cast<size_t>(c) * nb + b) * tot * N; };
+  // 1. ModUp INTT row phase of the key-switched input (a1 a2 / ax / rx)
+  std::vector<RowDesc> rows;
+  for (int c = 0; c < count; c++)
+    for (int r = 0; r < nq; r++) {
+      RowDesc d{};
+      const size_t o = static_cast<size_t>(r) * N;
+      d.src = (in[c].mode == 2 ? in[c].a2 : in[c].a1) + o;
+      if (in[c].mode == 0) {
+        d.src2 = in[c].a2 + o;
+        d.flags = kMulSrc2;
+        d.qinv = P->qinv[g[r]];
+      }
+      d.dst = t1 + (static_cast<size_t>(c) * nq + r) * N;
+      d.tw = itw(g[r]);
+      d.q = P->primes[g[r]];
+      rows.push_back(d);
+    }
+  for_row_batches(rows, [&](const RowBatch &rb) { launch_ntt_inv_rows(rb, P->log_n, stream); });
+  // 2. ModUp column pass per (ciphertext, digit)
+  {
+    MSColBatch b{};
+    b.tw = d_tw;
+    b.itw = d_itw;
+    b.primes = d_primes;
+    b.qinvs = d_qinv;
+    for (int c = 0; c < count; c++)
+      for (int bi = 0; bi < nb; bi++) {
+        const int i = digits[bi], s = m.dig_s[i], e = m.dig_e[i];
+        MSColJob &j = b.jobs[b.count++];
+        j.src = t1 + static_cast<size_t>(c) * nq * N;
+        j.dst = MU(c, bi);
+        j.table = m.d_mod_up2[i];
+        j.K = e - s;
+        j.M = tot - (e - s);
+        CHD_CHECK(j.K <= 16 && j.M <= 64, kErrUnsupported, "modup: digit too large");
+        for (int k = 0; k < j.K; k++) {
+          j.src_row[k] = static_cast<uint8_t>(s + k);
+          j.src_gidx[k] = static_cast<uint8_t>(g[s + k]);
+          mont_as_shoup(m.mod_up1[s + k], g[s + k], &j.c0[k], &j.c0s[k]);
+        }
+        int k = 0;
+        for (int r = 0; r < tot; r++) {
+          if (r >= s && r < e) continue;
+          j.dst_row[k] = static_cast<uint8_t>(r);
+          j.dst_gidx[k] = static_cast<uint8_t>(g[r]);
+          k++;
+        }
+        if (b.count == kMaxMSColJobs) {
+          launch_modswitch_cols(b, P->log_n, stream);
+          b.count = 0;
+        }
+      }
+    launch_modswitch_cols(b, P->log_n, stream);
+  }
+  // 3. row pass: ModUp NTT rows, key inner product, P (d0, d1), INTT rows of
+  //    the dropped primes
+  {
+    KSRowsDesc d{};
+    const size_t kstride = static_cast<size_t>(key.np.total()) * N;
+    for (int bi = 0; bi < nb; bi++) {
+      d.kb[bi] = key.bx + digits[bi] * kstride;
+      d.ka[bi] = key.ax + digits[bi] * kstride;
+    }
+    d.tw = d_tw;
+    d.itw = d_itw;
+    d.beta = nb;
+    d.rows = tot;
+    d.nq = nq;
+    d.mode = in[0].mode;
+    for (int r = 0; r < tot; r++) {
+      d.q[r] = P->primes[g[r]];
+      d.qinv[r] = P->qinv[g[r]];
+      d.p_prod[r] = r < nq ? p_prod[prime_offset + r] : 0;
+      d.key_row[r] = static_cast<int16_t>(r < nq ? prime_offset + r : P->L + (r - nq));
+      d.gidx[r] = static_cast<uint8_t>(g[r]);
+      d.own_digit[r] = -1;
+      d.drop_idx[r] = -1;
+      for (int bi = 0; bi < nb; bi++)
+        if (r >= m.dig_s[digits[bi]] && r < m.dig_e[digits[bi]]) d.own_digit[r] = static_cast<int8_t>(bi);
+    }
+    for (int i = 0; i < pl.src_len; i++) d.drop_idx[pl.srows[i]] = static_cast<int8_t>(i);
+    for (int c0 = 0; c0 < count; c0 += kMaxKSRowsCts) {
+      d.count = std::min(kMaxKSRowsCts, count - c0);
+      for (int c = 0; c < d.count; c++) {
+        const KSIn &x = in[c0 + c];
+        CHD_CHECK(x.mode == d.mode, kErrInvalidArg, "key switch: mixed modes in one batch");
+        KSRowsCt &k = d.ct[c];
+        for (int bi = 0; bi < nb; bi++) k.mu[bi] = MU(c0 + c, bi);
+        k.b1 = x.b1;
+        k.a1 = x.a1;
+        k.b2 = x.b2;
+        k.a2 = x.a2;
+        k.acc_b = acc + static_cast<size_t>(c0 + c) * 2 * tot * N;
+        k.acc_a = k.acc_b + static_cast<size_t>(tot) * N;
+        k.drop_b = drop + static_cast<size_t>(c0 + c) * 2 * pl.src_len * N;
+        k.drop_a = k.drop_b + static_cast<size_t>(pl.src_len) * N;
+      }
+      launch_ks_rows(d, P->log_n, stream);
+    }
+  }
+  // 4. ModDown column pass per (ciphertext, part)
+  {
+    MSColBatch b{};
+    b.tw = d_tw;
+    b.itw = d_itw;
+    b.primes = d_primes;
+    b.qinvs = d_qinv;
+    for (int c = 0; c < count; c++)
+      for (int p = 0; p < 2; p++) {
+        MSColJob &j = b.jobs[b.count++];
+        j.src = drop + (static_cast<size_t>(c) * 2 + p) * pl.src_len * N;
+        j.dst = p == 0 ? in[c].out_b : in[c].out_a;
+        j.table = pl.table;
+        j.K = pl.src_len;
+        j.M = pl.dst_len;
+        for (int i = 0; i < pl.src_len; i++) {
+          const int gg = pl.gs[pl.srows[i]];
+          j.src_row[i] = static_cast<uint8_t>(i);
+          j.src_gidx[i] = static_cast<uint8_t>(gg);
+          mont_as_shoup(pl.c1[i], gg, &j.c0[i], &j.c0s[i]);
+        }
+        for (int y = 0; y < pl.dst_len; y++) {
+          j.dst_row[y] = static_cast<uint8_t>(y);
+          j.dst_gidx[y] = static_cast<uint8_t>(pl.gd[y]);
+        }
+        if (b.count == kMaxMSColJobs) {
+          launch_modswitch_cols(b, P->log_n, stream);
+          b.count = 0;
+        }
+      }
+    launch_modswitch_cols(b, P->log_n, stream);
+  }
+  // 5. NTT row phase with the ModDown epilogue (src2 = kept accumulators)
+  rows.clear();
+  for (int c = 0; c < count; c++)
+    for (int p = 0; p < 2; p++) {
+      const uint32_t *src = acc + (static_cast<size_t>(c) * 2 + p) * tot * N;
+      uint32_t *dst = p == 0 ? in[c].out_b : in[c].out_a;
+      for (int y = 0; y < pl.dst_len; y++) {
+        RowDesc d{};
+        d.src = d.dst = dst + static_cast<size_t>(y) * N;
+        d.tw = tw(pl.gd[y]);
+        d.q = P->primes[pl.gd[y]];
+        mont_as_shoup(pl.inv[y], pl.gd[y], &d.c2, &d.c2s);
+        d.flags = kModDownEpi;
+        if (y >= pl.src2_start && y < pl.src2_end) {
+          d.flags |= kHasSrc2;
+          d.src2 = src + static_cast<size_t>(pl.src2_off + y - pl.src2_start) * N;
+          if (pl.pad) {
+            d.flags |= kPadSrc2;
+            mont_as_shoup(pl.pad[y - pl.src2_start], pl.gd[y], &d.c1, &d.c1s);
+          }
+        }
+        rows.push_back(d);
+      }
+    }
+  for_row_batches(rows, [&](const RowBatch &rb) { launch_ntt_fwd_rows(rb, P->log_n, stream); });
+  return check_cuda("key switch");
+}
+
 Status Context::moddown(int level, MDType type, const uint32_t *const *src, uint32_t *const *dst, int npoly) {
   // ModSwitch.cu:566-684 with NTT.cu:973-1128 and the fused epilogue of
   // NTT.cu:456-601
@@ -1214,6 +1436,29 @@ Status Context::hmult(DeviceCt &res, const DeviceCt &a, const DeviceCt &b, const
   CHD_CHECK(!rescale || level >= 1, kErrInvalidLevel, "Not enough q primes to rescale");
   const int n = P->n, nq = a.np.q(), tot = nq + P->alpha;
   CHD_CHECK(tot <= 64, kErrUnsupported, "HMult: more than 64 primes in the extended basis");
+  if (n == 65536) {
+    // fused pipeline; an aliased result is written through a scratch copy
+    if (&res != &a && &res != &b) {
+      DeviceCt *r[1] = {&res};
+      const DeviceCt *x[1] = {&a}, *y[1] = {&b};
+      return hmult_batch(1, r, x, y, key, rescale);
+    }
+    ArenaScope scope(arena);
+    NP out_np = P->level_np(rescale ? level - 1 : level, 0);
+    const size_t words = static_cast<size_t>(out_np.total()) * n;
+    uint32_t *tb = static_cast<uint32_t *>(arena.alloc(words * 4)), *ta = static_cast<uint32_t *>(arena.alloc(words * 4));
+    CHD_CHECK(tb && ta, kErrAlloc, "HMult: scratch allocation failed");
+    KSIn in{0, a.bx, a.ax, b.bx, b.ax, tb, ta};
+    const double sc = rescale ? a.scale * b.scale / P->rescale_prod[level] : a.scale * b.scale;
+    const int slots = std::max(a.num_slots, b.num_slots);
+    CHD_TRY(key_switch_fused(level, 1, &in, key, rescale ? MDType::kModDownRescale : MDType::kModDown));
+    CHD_TRY(res.reserve(out_np, false, n));
+    cudaMemcpyAsync(res.bx, tb, words * 4, cudaMemcpyDeviceToDevice, stream);
+    cudaMemcpyAsync(res.ax, ta, words * 4, cudaMemcpyDeviceToDevice, stream);
+    res.scale = sc;
+    res.num_slots = slots;
+    return check_cuda("hmult");
+  }
   ArenaScope scope(arena);
   uint32_t *d = static_cast<uint32_t *>(arena.alloc(static_cast<size_t>(3) * nq * n * 4));
   uint32_t *acc = static_cast<uint32_t *>(arena.alloc(static_cast<size_t>(2) * tot * n * 4));
@@ -1273,6 +1518,21 @@ Status Context::hmult_batch(int count, DeviceCt *const *res, const DeviceCt *con
   CHD_CHECK(!rescale || level >= 1, kErrInvalidLevel, "Not enough q primes to rescale");
   const int n = P->n, nq = a[0]->np.q(), tot = nq + P->alpha;
   CHD_CHECK(tot <= 64, kErrUnsupported, "HMult: more than 64 primes in the extended basis");
+  if (P->log_n == 16) {
+    std::vector<KSIn> in(count);
+    NP out_np = P->level_np(rescale ? level - 1 : level, 0);
+    for (int c = 0; c < count; c++) {
+      const double sa = a[c]->scale, sb = b[c]->scale;
+      const int slots = std::max(a[c]->num_slots, b[c]->num_slots);
+      in[c] = KSIn{0, a[c]->bx, a[c]->ax, b[c]->bx, b[c]->ax, nullptr, nullptr};
+      CHD_TRY(res[c]->reserve(out_np, false, n));
+      res[c]->scale = rescale ? sa * sb / P->rescale_prod[level] : sa * sb;
+      res[c]->num_slots = slots;
+      in[c].out_b = res[c]->bx;
+      in[c].out_a = res[c]->ax;
+    }
+    return key_switch_fused(level, count, in.data(), key, rescale ? MDType::kModDownRescale : MDType::kModDown);
+  }
   ArenaScope scope(arena);
   const size_t qw = static_cast<size_t>(nq) * n, tw_ = static_cast<size_t>(tot) * n;
   uint32_t *d = static_cast<uint32_t *>(arena.alloc(static_cast<size_t>(count) * 3 * qw * 4));
@@ -1330,6 +1590,23 @@ Status Context::relinearize(DeviceCt &res, const DeviceCt &a, const DeviceEvk &k
   CHD_CHECK(level >= 0, kErrInvalidLevel, "Relinearize: invalid level");
   CHD_CHECK(!rescale || level >= 1, kErrInvalidLevel, "Not enough q primes to rescale");
   const int n = P->n, tot = a.np.q() + P->alpha;
+  if (n == 65536) {
+    ArenaScope scope(arena);
+    NP out_np = P->level_np(rescale ? level - 1 : level, 0);
+    const size_t words = static_cast<size_t>(out_np.total()) * n;
+    uint32_t *tb = static_cast<uint32_t *>(arena.alloc(words * 4)), *ta = static_cast<uint32_t *>(arena.alloc(words * 4));
+    CHD_CHECK(tb && ta, kErrAlloc, "Relinearize: scratch allocation failed");
+    KSIn in{2, a.bx, a.ax, nullptr, a.rx, tb, ta};
+    const double sc = rescale ? a.scale / P->rescale_prod[level] : a.scale;
+    const int slots = a.num_slots;
+    CHD_TRY(key_switch_fused(level, 1, &in, key, rescale ? MDType::kModDownRescale : MDType::kModDown));
+    CHD_TRY(res.reserve(out_np, false, n));
+    cudaMemcpyAsync(res.bx, tb, words * 4, cudaMemcpyDeviceToDevice, stream);
+    cudaMemcpyAsync(res.ax, ta, words * 4, cudaMemcpyDeviceToDevice, stream);
+    res.scale = sc;
+    res.num_slots = slots;
+    return check_cuda("relinearize");
+  }
   ArenaScope scope(arena);
   uint32_t *acc = static_cast<uint32_t *>(arena.alloc(static_cast<size_t>(2) * tot * n * 4));
   CHD_CHECK(acc, kErrAlloc, "Relinearize: scratch allocation failed");
@@ -1352,6 +1629,23 @@ Status Context::mult_key(DeviceCt &res, const DeviceCt &a, const DeviceEvk &key)
   const int level = level_of(*P, a);
   CHD_CHECK(level >= 0, kErrInvalidLevel, "MultKey: invalid level");
   const int n = P->n, tot = a.np.q() + P->alpha;
+  if (n == 65536) {
+    ArenaScope scope(arena);
+    const size_t words = static_cast<size_t>(a.np.total()) * n;
+    uint32_t *tb = static_cast<uint32_t *>(arena.alloc(words * 4)), *ta = static_cast<uint32_t *>(arena.alloc(words * 4));
+    CHD_CHECK(tb && ta, kErrAlloc, "MultKey: scratch allocation failed");
+    KSIn in{1, a.bx, a.ax, nullptr, nullptr, tb, ta};
+    const double sc = a.scale;
+    const int slots = a.num_slots;
+    const NP np = a.np;
+    CHD_TRY(key_switch_fused(level, 1, &in, key, MDType::kModDown));
+    CHD_TRY(res.reserve(np, false, n));
+    cudaMemcpyAsync(res.bx, tb, words * 4, cudaMemcpyDeviceToDevice, stream);
+    cudaMemcpyAsync(res.ax, ta, words * 4, cudaMemcpyDeviceToDevice, stream);
+    res.scale = sc;
+    res.num_slots = slots;
+    return check_cuda("mult key");
+  }
   ArenaScope scope(arena);
   uint32_t *acc = static_cast<uint32_t *>(arena.alloc(static_cast<size_t>(2) * tot * n * 4));
   CHD_CHECK(acc, kErrAlloc, "MultKey: scratch allocation failed");

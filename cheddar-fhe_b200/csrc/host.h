@@ -187,6 +187,24 @@ class Context {
   Status modup_fused(int level, int count, const uint32_t *const *src, uint32_t *const *const *dst,
                      uint32_t *rows_out);
   enum class MDType { kModDown, kRescale, kModDownRescale };
+  // Which rows a ModDown / Rescale / ModDownAndRescale drops and the
+  // constants of its BConv and epilogue (ModSwitch.cu:566-684).
+  struct MDPlan {
+    NP ns, nd, nn;
+    int src_len = 0, dst_len = 0, src2_start = 0, src2_end = 0, src2_off = 0;
+    std::vector<int> srows, gs, gd;
+    const uint32_t *c1 = nullptr, *inv = nullptr, *pad = nullptr;
+    const int32_t *table = nullptr;
+  };
+  Status moddown_plan(int level, MDType type, MDPlan *plan) const;
+  // Fused N = 2^16 key switch (see keyswitch.cu): count inputs at one level,
+  // results written to out_b / out_a after ModDown (or ModDownAndRescale).
+  struct KSIn {
+    int mode;  // 0 HMult (b1,a1,b2,a2), 1 MultKey (b1=bx, a1=ax), 2 Relinearize (b1=bx, a1=ax, a2=rx)
+    const uint32_t *b1, *a1, *b2, *a2;
+    uint32_t *out_b, *out_a;
+  };
+  Status key_switch_fused(int level, int count, const KSIn *in, const DeviceEvk &key, MDType type);
   // ModDown family on npoly polys
   Status moddown(int level, MDType type, const uint32_t *const *src, uint32_t *const *dst, int npoly);
   Status bconv(const int32_t *xt, int K, const int32_t *table, const int *dst_gidx, int M, uint32_t *out);

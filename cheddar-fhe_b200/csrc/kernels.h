@@ -20,6 +20,8 @@ struct RowDesc {
   const uint2 *tw;       // twiddle table of this prime (N pairs)
   uint32_t q;            // prime
   uint32_t flags;        // see RowFlags
+  int32_t qinv;          // q^-1 mod 2^32 (Montgomery product of kMulSrc2)
+  uint32_t pad_;
   uint32_t c0, c0s;      // pre-multiplier (forward) / output constant (inverse)
   uint32_t c1, c1s;      // ModDown epilogue: src2 padding multiplier
   uint32_t c2, c2s;      // ModDown epilogue: (prod of dropped primes)^-1
@@ -31,6 +33,7 @@ enum RowFlags : uint32_t {
   kHasSrc2 = 4u,       // ModDown epilogue: src2 exists for this row
   kPadSrc2 = 8u,       // ModDown epilogue: multiply src2 by c1 first
   kModDownEpi = 16u,   // forward NTT row phase: apply (src2*c1 - x) * c2
+  kMulSrc2 = 32u,      // inverse NTT row phase: input is src (.) src2 (Montgomery)
 };
 
 constexpr int kMaxRows = 120;
@@ -96,6 +99,32 @@ struct MSColBatch {
 };
 void launch_modswitch_cols(const MSColBatch &b, int log_n, cudaStream_t s);
 void launch_ntt_inv_rows(const RowBatch &rb, int log_n, cudaStream_t s);
+
+// Fused key-switching row pass (N = 2^16), see keyswitch.cu.  Modes:
+//   0 HMult:       own ModUp value a1 a2, d0 = b1 b2, d1 = b1 a2 + a1 b2
+//   1 MultKey:     own ModUp value a1 (= ax), d0 = b1 (= bx)
+//   2 Relinearize: own ModUp value a2 (= rx), d0 = b1 (= bx), d1 = a1 (= ax)
+struct KSRowsCt {
+  const uint32_t *mu[8];             // ModUp column-pass outputs [tot][N] per digit
+  const uint32_t *b1, *a1, *b2, *a2; // inputs [nq][N]
+  uint32_t *acc_b, *acc_a;           // kept primes: evaluation-domain accumulators [tot][N]
+  uint32_t *drop_b, *drop_a;         // dropped primes: INTT row-phase output [ndrop][N]
+};
+constexpr int kMaxKSRowsCts = 16;
+struct KSRowsDesc {
+  const uint32_t *kb[8], *ka[8];     // key digit pointers (row 0 of the key basis)
+  const uint2 *tw, *itw;
+  int beta, rows, nq, count, mode;
+  uint32_t q[64];
+  int32_t qinv[64];
+  uint32_t p_prod[64];
+  int16_t key_row[64];
+  uint8_t gidx[64];
+  int8_t own_digit[64];              // digit owning row j (q primes), else -1
+  int8_t drop_idx[64];               // row of j in the drop buffers, else -1
+  KSRowsCt ct[kMaxKSRowsCts];
+};
+void launch_ks_rows(const KSRowsDesc &d, int log_n, cudaStream_t s);
 
 // Key-switching inner product with the P * (d0, d1) term folded in:
 //   acc_b[r] = sum_i mu_i[r] * kb_i[r] + (r < nq ? p_prod[r] * d0[r] : 0)

@@ -1,0 +1,195 @@
+// Fused key-switching row kernel for N = 2^16.
+//
+// Between the two fused column passes of a key switch (modswitch.cu) every
+// remaining step is row-local in the 128 x 512 limb layout:
+//   * the ModUp NTT row phase of every digit (src/core/NTT.cu NTTForModUp),
+//   * the key inner product sum_i ModUp(d)_i (.) key_i (Context.cpp:609-647),
+//   * the P * (d0, d1) term (Context.cpp:687-699) with the tensor product
+//     d0 = b1 b2, d1 = b1 a2 + a1 b2 recomputed from the inputs
+//     (ElementWise.cu:504-575), and the own-digit ModUp value d2 = a1 a2,
+//   * and, for the primes that ModDown drops, the INTT row phase
+//     (NTT.cu:973-1128, INTTForModDown).
+// One CTA owns 4 rows of one prime of the extended basis Q u P for one
+// ciphertext; it reads each input row once and writes either the
+// evaluation-domain accumulator (kept primes, consumed by the ModDown
+// epilogue) or the INTT row-phase output (dropped primes, consumed by the
+// ModDown column pass).
+#include "arith.cuh"
+#include "kernels.h"
+
+namespace chd {
+namespace {
+
+__device__ __forceinline__ void r8_fwd(uint32_t *x, const uint2 *tw, int b0, int b1, int b2, uint32_t q) {
+  const uint2 w0 = __ldg(tw + b0);
+#pragma unroll
+  for (int k = 0; k < 4; k++) ct_lazy(x[k], x[k + 4], w0, q);
+#pragma unroll
+  for (int g = 0; g < 2; g++) {
+    const uint2 w1 = __ldg(tw + b1 + g);
+    ct_lazy(x[4 * g], x[4 * g + 2], w1, q);
+    ct_lazy(x[4 * g + 1], x[4 * g + 3], w1, q);
+  }
+#pragma unroll
+  for (int g = 0; g < 4; g++) {
+    const uint2 w2 = __ldg(tw + b2 + g);
+    ct_lazy(x[2 * g], x[2 * g + 1], w2, q);
+  }
+}
+
+__device__ __forceinline__ void r8_inv(uint32_t *x, const uint2 *tw, int b0, int b1, int b2, uint32_t q) {
+#pragma unroll
+  for (int g = 0; g < 4; g++) {
+    const uint2 w2 = __ldg(tw + b2 + g);
+    gs_lazy(x[2 * g], x[2 * g + 1], w2, q);
+  }
+#pragma unroll
+  for (int g = 0; g < 2; g++) {
+    const uint2 w1 = __ldg(tw + b1 + g);
+    gs_lazy(x[4 * g], x[4 * g + 2], w1, q);
+    gs_lazy(x[4 * g + 1], x[4 * g + 3], w1, q);
+  }
+  const uint2 w0 = __ldg(tw + b0);
+#pragma unroll
+  for (int k = 0; k < 4; k++) gs_lazy(x[k], x[k + 4], w0, q);
+}
+
+__device__ __forceinline__ void ld8(const uint32_t *p, uint32_t *x) {
+  const uint4 *v = reinterpret_cast<const uint4 *>(p);
+  const uint4 a = __ldg(v), b = __ldg(v + 1);
+  x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
+  x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
+}
+__device__ __forceinline__ void st8(uint32_t *p, const uint32_t *x) {
+  uint4 *v = reinterpret_cast<uint4 *>(p);
+  v[0] = make_uint4(x[0], x[1], x[2], x[3]);
+  v[1] = make_uint4(x[4], x[5], x[6], x[7]);
+}
+
+__global__ void __launch_bounds__(256) k_ks_rows(const __grid_constant__ KSRowsDesc d) {
+  __shared__ uint32_t sm[4][512];
+  const int j = blockIdx.y;
+  const KSRowsCt &c = d.ct[blockIdx.z];
+  const uint32_t q = d.q[j];
+  const int32_t qi = d.qinv[j];
+  const int g = d.gidx[j];
+  const uint2 *tw = d.tw + (static_cast<size_t>(g) << 16);
+  const int t = threadIdx.x & 63, rl = threadIdx.x >> 6;
+  const int r = blockIdx.x * 4 + rl;
+  uint32_t *srow = sm[rl];
+  const int b = t >> 3, u0 = t & 7;
+  const size_t off = static_cast<size_t>(j) * 65536 + r * 512 + 8 * t;       // accumulator-row offset
+  const size_t koff = static_cast<size_t>(d.key_row[j]) * 65536 + r * 512 + 8 * t;
+  const size_t qoff = off;  // input rows share the accumulator row index for q primes
+  const bool is_q = j < d.nq;
+  const int mode = d.mode;
+  uint32_t a1[8], a2[8];
+  if (is_q) {
+    ld8(c.a1 + qoff, a1);
+    if (mode != 1) ld8(c.a2 + qoff, a2);
+  }
+  uint32_t sb[8], sa[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) sb[k] = sa[k] = 0;
+  for (int i = 0; i < d.beta; i++) {
+    uint32_t v[8];
+    if (d.own_digit[j] == i) {
+      // own primes of the digit: the ModUp value is the key-switched input
+#pragma unroll
+      for (int k = 0; k < 8; k++) v[k] = mode == 0 ? mont_mul(a1[k], a2[k], q, qi) : (mode == 1 ? a1[k] : a2[k]);
+    } else {
+      const uint32_t *src = c.mu[i] + static_cast<size_t>(j) * 65536 + r * 512;
+#pragma unroll
+      for (int k = 0; k < 8; k++) v[k] = src[t + 64 * k];
+      r8_fwd(v, tw, 128 + r, 256 + 2 * r, 512 + 4 * r, q);
+#pragma unroll
+      for (int k = 0; k < 8; k++) srow[t + 64 * k] = v[k];
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < 8; k++) v[k] = srow[64 * b + u0 + 8 * k];
+      r8_fwd(v, tw, 1024 + 8 * r + b, 2048 + 16 * r + 2 * b, 4096 + 32 * r + 4 * b, q);
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < 8; k++) srow[64 * b + u0 + 8 * k] = v[k];
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < 8; k++) v[k] = srow[8 * t + k];
+      r8_fwd(v, tw, 8192 + 64 * r + t, 16384 + 128 * r + 2 * t, 32768 + 256 * r + 4 * t, q);
+#pragma unroll
+      for (int k = 0; k < 8; k++) v[k] = reduce2q(v[k], q);
+      __syncthreads();
+    }
+    uint32_t kb[8], ka[8];
+    ld8(d.kb[i] + koff, kb);
+    ld8(d.ka[i] + koff, ka);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      sb[k] = add_mod(sb[k], mont_mul(v[k], kb[k], q, qi), q);
+      sa[k] = add_mod(sa[k], mont_mul(v[k], ka[k], q, qi), q);
+    }
+  }
+  if (is_q) {
+    // P * (d0, d1): HMult d0 = b1 b2, d1 = b1 a2 + a1 b2; MultKey d0 = bx;
+    // Relinearize d0 = bx, d1 = ax
+    const uint32_t pp = d.p_prod[j];
+    uint32_t b1[8];
+    ld8(c.b1 + qoff, b1);
+    if (mode == 0) {
+      uint32_t b2[8];
+      ld8(c.b2 + qoff, b2);
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        const uint32_t d0 = mont_mul(b1[k], b2[k], q, qi);
+        const uint32_t d1 = add_mod(mont_mul(b1[k], a2[k], q, qi), mont_mul(a1[k], b2[k], q, qi), q);
+        sb[k] = add_mod(sb[k], mont_mul(d0, pp, q, qi), q);
+        sa[k] = add_mod(sa[k], mont_mul(d1, pp, q, qi), q);
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        sb[k] = add_mod(sb[k], mont_mul(b1[k], pp, q, qi), q);
+        if (mode == 2) sa[k] = add_mod(sa[k], mont_mul(a1[k], pp, q, qi), q);
+      }
+    }
+  }
+  const int di = d.drop_idx[j];
+  if (di < 0) {
+    st8(c.acc_b + off, sb);
+    st8(c.acc_a + off, sa);
+    return;
+  }
+  // dropped prime: INTT row phase of both accumulators (ModDown's first step)
+  const uint2 *itw = d.itw + (static_cast<size_t>(g) << 16);
+  uint32_t *outs[2] = {c.drop_b + static_cast<size_t>(di) * 65536 + r * 512,
+                       c.drop_a + static_cast<size_t>(di) * 65536 + r * 512};
+#pragma unroll
+  for (int p = 0; p < 2; p++) {
+    uint32_t *x = p == 0 ? sb : sa;
+    r8_inv(x, itw, 8192 + 64 * r + t, 16384 + 128 * r + 2 * t, 32768 + 256 * r + 4 * t, q);
+#pragma unroll
+    for (int k = 0; k < 8; k++) srow[8 * t + k] = x[k];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 8; k++) x[k] = srow[64 * b + u0 + 8 * k];
+    r8_inv(x, itw, 1024 + 8 * r + b, 2048 + 16 * r + 2 * b, 4096 + 32 * r + 4 * b, q);
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 8; k++) srow[64 * b + u0 + 8 * k] = x[k];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 8; k++) x[k] = srow[t + 64 * k];
+    r8_inv(x, itw, 128 + r, 256 + 2 * r, 512 + 4 * r, q);
+#pragma unroll
+    for (int k = 0; k < 8; k++) outs[p][t + 64 * k] = x[k];
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+void launch_ks_rows(const KSRowsDesc &d, int log_n, cudaStream_t s) {
+  if (d.count <= 0 || d.rows <= 0 || log_n != 16) return;
+  k_ks_rows<<<dim3(32, d.rows, d.count), 256, 0, s>>>(d);
+}
+
+}  // namespace chd

@@ -179,6 +179,13 @@ __global__ void __launch_bounds__(256) k_inv_rows16(const __grid_constant__ RowB
     x[0] = a0.x; x[1] = a0.y; x[2] = a0.z; x[3] = a0.w;
     x[4] = a1.x; x[5] = a1.y; x[6] = a1.z; x[7] = a1.w;
   }
+  if (rd.flags & kMulSrc2) {
+    const uint4 *p = reinterpret_cast<const uint4 *>(rd.src2 + base);
+    uint4 a0 = __ldg(p), a1 = __ldg(p + 1);
+    const uint32_t y[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+#pragma unroll
+    for (int k = 0; k < 8; k++) x[k] = mont_mul(x[k], y[k], q, rd.qinv);
+  }
   radix8_inv(x, tw, 8192 + 64 * r + t, 16384 + 128 * r + 2 * t, 32768 + 256 * r + 4 * t, q);
 #pragma unroll
   for (int k = 0; k < 8; k++) srow[8 * t + k] = x[k];
