@@ -16,57 +16,12 @@
 // ModDown column pass).
 #include "arith.cuh"
 #include "kernels.h"
+#include "ntt_common.cuh"
 
 namespace chd {
 namespace {
 
-__device__ __forceinline__ void r8_fwd(uint32_t *x, const uint2 *tw, int b0, int b1, int b2, uint32_t q) {
-  const uint2 w0 = __ldg(tw + b0);
-#pragma unroll
-  for (int k = 0; k < 4; k++) ct_lazy(x[k], x[k + 4], w0, q);
-#pragma unroll
-  for (int g = 0; g < 2; g++) {
-    const uint2 w1 = __ldg(tw + b1 + g);
-    ct_lazy(x[4 * g], x[4 * g + 2], w1, q);
-    ct_lazy(x[4 * g + 1], x[4 * g + 3], w1, q);
-  }
-#pragma unroll
-  for (int g = 0; g < 4; g++) {
-    const uint2 w2 = __ldg(tw + b2 + g);
-    ct_lazy(x[2 * g], x[2 * g + 1], w2, q);
-  }
-}
-
-__device__ __forceinline__ void r8_inv(uint32_t *x, const uint2 *tw, int b0, int b1, int b2, uint32_t q) {
-#pragma unroll
-  for (int g = 0; g < 4; g++) {
-    const uint2 w2 = __ldg(tw + b2 + g);
-    gs_lazy(x[2 * g], x[2 * g + 1], w2, q);
-  }
-#pragma unroll
-  for (int g = 0; g < 2; g++) {
-    const uint2 w1 = __ldg(tw + b1 + g);
-    gs_lazy(x[4 * g], x[4 * g + 2], w1, q);
-    gs_lazy(x[4 * g + 1], x[4 * g + 3], w1, q);
-  }
-  const uint2 w0 = __ldg(tw + b0);
-#pragma unroll
-  for (int k = 0; k < 4; k++) gs_lazy(x[k], x[k + 4], w0, q);
-}
-
-__device__ __forceinline__ void ld8(const uint32_t *p, uint32_t *x) {
-  const uint4 *v = reinterpret_cast<const uint4 *>(p);
-  const uint4 a = __ldg(v), b = __ldg(v + 1);
-  x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
-  x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
-}
-__device__ __forceinline__ void st8(uint32_t *p, const uint32_t *x) {
-  uint4 *v = reinterpret_cast<uint4 *>(p);
-  v[0] = make_uint4(x[0], x[1], x[2], x[3]);
-  v[1] = make_uint4(x[4], x[5], x[6], x[7]);
-}
-
-__global__ void __launch_bounds__(256) k_ks_rows(const __grid_constant__ KSRowsDesc d) {
+__global__ void __launch_bounds__(256, 3) k_ks_rows(const __grid_constant__ KSRowsDesc d) {
   __shared__ uint32_t sm[4][512];
   const int j = blockIdx.y;
   const KSRowsCt &c = d.ct[blockIdx.z];
@@ -77,7 +32,6 @@ __global__ void __launch_bounds__(256) k_ks_rows(const __grid_constant__ KSRowsD
   const int t = threadIdx.x & 63, rl = threadIdx.x >> 6;
   const int r = blockIdx.x * 4 + rl;
   uint32_t *srow = sm[rl];
-  const int b = t >> 3, u0 = t & 7;
   const size_t off = static_cast<size_t>(j) * 65536 + r * 512 + 8 * t;       // accumulator-row offset
   const size_t koff = static_cast<size_t>(d.key_row[j]) * 65536 + r * 512 + 8 * t;
   const size_t qoff = off;  // input rows share the accumulator row index for q primes
@@ -101,20 +55,7 @@ __global__ void __launch_bounds__(256) k_ks_rows(const __grid_constant__ KSRowsD
       const uint32_t *src = c.mu[i] + static_cast<size_t>(j) * 65536 + r * 512;
 #pragma unroll
       for (int k = 0; k < 8; k++) v[k] = src[t + 64 * k];
-      r8_fwd(v, tw, 128 + r, 256 + 2 * r, 512 + 4 * r, q);
-#pragma unroll
-      for (int k = 0; k < 8; k++) srow[t + 64 * k] = v[k];
-      __syncthreads();
-#pragma unroll
-      for (int k = 0; k < 8; k++) v[k] = srow[64 * b + u0 + 8 * k];
-      r8_fwd(v, tw, 1024 + 8 * r + b, 2048 + 16 * r + 2 * b, 4096 + 32 * r + 4 * b, q);
-      __syncthreads();
-#pragma unroll
-      for (int k = 0; k < 8; k++) srow[64 * b + u0 + 8 * k] = v[k];
-      __syncthreads();
-#pragma unroll
-      for (int k = 0; k < 8; k++) v[k] = srow[8 * t + k];
-      r8_fwd(v, tw, 8192 + 64 * r + t, 16384 + 128 * r + 2 * t, 32768 + 256 * r + 4 * t, q);
+      row_fwd(v, srow, tw, r, t, q);
 #pragma unroll
       for (int k = 0; k < 8; k++) v[k] = reduce2q(v[k], q);
       __syncthreads();
@@ -165,20 +106,7 @@ __global__ void __launch_bounds__(256) k_ks_rows(const __grid_constant__ KSRowsD
 #pragma unroll
   for (int p = 0; p < 2; p++) {
     uint32_t *x = p == 0 ? sb : sa;
-    r8_inv(x, itw, 8192 + 64 * r + t, 16384 + 128 * r + 2 * t, 32768 + 256 * r + 4 * t, q);
-#pragma unroll
-    for (int k = 0; k < 8; k++) srow[8 * t + k] = x[k];
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < 8; k++) x[k] = srow[64 * b + u0 + 8 * k];
-    r8_inv(x, itw, 1024 + 8 * r + b, 2048 + 16 * r + 2 * b, 4096 + 32 * r + 4 * b, q);
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < 8; k++) srow[64 * b + u0 + 8 * k] = x[k];
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < 8; k++) x[k] = srow[t + 64 * k];
-    r8_inv(x, itw, 128 + r, 256 + 2 * r, 512 + 4 * r, q);
+    row_inv(x, srow, itw, r, t, q);
 #pragma unroll
     for (int k = 0; k < 8; k++) outs[p][t + 64 * k] = x[k];
     __syncthreads();

@@ -15,6 +15,7 @@
 // radix-8 on rows 8j + u after one shared-memory exchange).
 #include "arith.cuh"
 #include "kernels.h"
+#include "ntt_common.cuh"
 
 namespace chd {
 namespace {
@@ -26,46 +27,14 @@ constexpr int kExRows = 136;     // 128 rows + one padding row per 16 rows
 // patterns (rows rg + 8k and rows 8j + u) free of bank conflicts
 __device__ __forceinline__ int exi(int row, int col) { return (row + (row >> 4)) * kTC + col; }
 
-__device__ __forceinline__ void radix8_fwd_c(uint32_t *x, const uint2 *tw, int b0, int b1, int b2, uint32_t q) {
-  const uint2 w0 = __ldg(tw + b0);
-#pragma unroll
-  for (int k = 0; k < 4; k++) ct_lazy(x[k], x[k + 4], w0, q);
-#pragma unroll
-  for (int g = 0; g < 2; g++) {
-    const uint2 w1 = __ldg(tw + b1 + g);
-    ct_lazy(x[4 * g], x[4 * g + 2], w1, q);
-    ct_lazy(x[4 * g + 1], x[4 * g + 3], w1, q);
-  }
-#pragma unroll
-  for (int g = 0; g < 4; g++) {
-    const uint2 w2 = __ldg(tw + b2 + g);
-    ct_lazy(x[2 * g], x[2 * g + 1], w2, q);
-  }
-}
-
-__device__ __forceinline__ void radix8_inv_c(uint32_t *x, const uint2 *tw, int b0, int b1, int b2, uint32_t q) {
-#pragma unroll
-  for (int g = 0; g < 4; g++) {
-    const uint2 w2 = __ldg(tw + b2 + g);
-    gs_lazy(x[2 * g], x[2 * g + 1], w2, q);
-  }
-#pragma unroll
-  for (int g = 0; g < 2; g++) {
-    const uint2 w1 = __ldg(tw + b1 + g);
-    gs_lazy(x[4 * g], x[4 * g + 2], w1, q);
-    gs_lazy(x[4 * g + 1], x[4 * g + 3], w1, q);
-  }
-  const uint2 w0 = __ldg(tw + b0);
-#pragma unroll
-  for (int k = 0; k < 4; k++) gs_lazy(x[k], x[k + 4], w0, q);
-}
-
 template <int KMAX>
 __global__ void __launch_bounds__(128) k_modswitch_cols(const __grid_constant__ MSColBatch b) {
   extern __shared__ uint32_t smem[];
   const MSColJob &jb = b.jobs[blockIdx.y];
   uint32_t *ex = smem;
-  int32_t *xs = reinterpret_cast<int32_t *>(smem + kExRows * kTC);  // [K][128][kTC]
+  // centred sources, private to the thread that produced them:
+  // xs4[(k * 4 + e / 4) * 128 + thread] holds elements 4(e/4) .. 4(e/4)+3
+  int4 *xs4 = reinterpret_cast<int4 *>(smem + kExRows * kTC);
   const int t = threadIdx.x, w = t >> 5, lane = t & 31;
   const int cl = lane & 15, rg = 2 * w + (lane >> 4);
   const int col = blockIdx.x * kTC + cl;
@@ -83,7 +52,7 @@ __global__ void __launch_bounds__(128) k_modswitch_cols(const __grid_constant__ 
       uint32_t y[8];
 #pragma unroll
       for (int u = 0; u < 8; u++) y[u] = __ldg(src + (8 * j + u) * 512 + col);
-      radix8_inv_c(y, itw, 16 + j, 32 + 2 * j, 64 + 4 * j, q);
+      radix8_inv(y, itw, 16 + j, 32 + 2 * j, 64 + 4 * j, q);
 #pragma unroll
       for (int u = 0; u < 8; u++) ex[exi(8 * j + u, cl)] = y[u];
     }
@@ -91,22 +60,14 @@ __global__ void __launch_bounds__(128) k_modswitch_cols(const __grid_constant__ 
     uint32_t x[16];
 #pragma unroll
     for (int e = 0; e < 16; e++) x[e] = ex[exi(rg + 8 * e, cl)];
-#pragma unroll
-    for (int s = 3; s >= 0; s--) {
-      const int m = 1 << s, h = 8 >> s;
-#pragma unroll
-      for (int gg = 0; gg < m; gg++) {
-        const uint2 wv = __ldg(itw + m + gg);
-#pragma unroll
-        for (int i = 0; i < h; i++) gs_lazy(x[gg * 2 * h + i], x[gg * 2 * h + i + h], wv, q);
-      }
-    }
+    radix16_cols_inv(x, itw, q);
     const uint32_t c0 = jb.c0[k], c0s = jb.c0s[k];
+    int32_t v[16];
 #pragma unroll
-    for (int e = 0; e < 16; e++) {
-      const uint32_t v = reduce2q(shoup_lazy(x[e], c0, c0s, q), q);
-      xs[(k * 128 + rg + 8 * e) * kTC + cl] = centre(v, q);
-    }
+    for (int e = 0; e < 16; e++) v[e] = centre(reduce2q(shoup_lazy(x[e], c0, c0s, q), q), q);
+#pragma unroll
+    for (int e4 = 0; e4 < 4; e4++)
+      xs4[(k * 4 + e4) * 128 + t] = make_int4(v[4 * e4], v[4 * e4 + 1], v[4 * e4 + 2], v[4 * e4 + 3]);
     __syncthreads();
   }
 
@@ -130,26 +91,21 @@ __global__ void __launch_bounds__(128) k_modswitch_cols(const __grid_constant__ 
         for (int k = k0; k < k0 + 4; k++) {
           if (k < K) {
             const int64_t tk = __ldg(T + k);
-            const int32_t *xk = xs + (k * 128 + rg) * kTC + cl;
 #pragma unroll
-            for (int e = 0; e < 16; e++) a[e] += static_cast<int64_t>(xk[8 * e * kTC]) * tk;
+            for (int e4 = 0; e4 < 4; e4++) {
+              const int4 xv = xs4[(k * 4 + e4) * 128 + t];
+              a[4 * e4] += static_cast<int64_t>(xv.x) * tk;
+              a[4 * e4 + 1] += static_cast<int64_t>(xv.y) * tk;
+              a[4 * e4 + 2] += static_cast<int64_t>(xv.z) * tk;
+              a[4 * e4 + 3] += static_cast<int64_t>(xv.w) * tk;
+            }
           }
         }
 #pragma unroll
         for (int e = 0; e < 16; e++) v[e] = add_mod(v[e], mont_reduce(a[e], p, pinv), p);
       }
     }
-    // forward stages m = 1, 2, 4, 8 on rows rg + 8e
-#pragma unroll
-    for (int s = 0; s < 4; s++) {
-      const int mm = 1 << s, h = 8 >> s;
-#pragma unroll
-      for (int gg = 0; gg < mm; gg++) {
-        const uint2 wv = __ldg(tw + mm + gg);
-#pragma unroll
-        for (int i = 0; i < h; i++) ct_lazy(v[gg * 2 * h + i], v[gg * 2 * h + i + h], wv, p);
-      }
-    }
+    radix16_cols_fwd(v, tw, p);  // stages m = 1, 2, 4, 8 on rows rg + 8e
 #pragma unroll
     for (int e = 0; e < 16; e++) ex[exi(rg + 8 * e, cl)] = v[e];
     __syncthreads();
@@ -160,7 +116,7 @@ __global__ void __launch_bounds__(128) k_modswitch_cols(const __grid_constant__ 
       uint32_t y[8];
 #pragma unroll
       for (int u = 0; u < 8; u++) y[u] = ex[exi(8 * j + u, cl)];
-      radix8_fwd_c(y, tw, 16 + j, 32 + 2 * j, 64 + 4 * j, p);
+      radix8_fwd(y, tw, 16 + j, 32 + 2 * j, 64 + 4 * j, p);
 #pragma unroll
       for (int u = 0; u < 8; u++) dst[(8 * j + u) * 512 + col] = y[u];
     }

@@ -22,48 +22,12 @@
 // fits in shared memory and one kernel runs every stage.
 #include "arith.cuh"
 #include "kernels.h"
+#include "ntt_common.cuh"
 
 namespace chd {
 namespace {
 
 constexpr int kColTile = 32;
-
-// Radix-8 forward network on x[0..7] (three CT stages: distances 4, 2, 1 in
-// register index) with twiddles tw[b0], tw[b1 + g], tw[b2 + g].
-__device__ __forceinline__ void radix8_fwd(uint32_t *x, const uint2 *tw, int b0, int b1, int b2, uint32_t q) {
-  const uint2 w0 = __ldg(tw + b0);
-#pragma unroll
-  for (int k = 0; k < 4; k++) ct_lazy(x[k], x[k + 4], w0, q);
-#pragma unroll
-  for (int g = 0; g < 2; g++) {
-    const uint2 w1 = __ldg(tw + b1 + g);
-    ct_lazy(x[4 * g], x[4 * g + 2], w1, q);
-    ct_lazy(x[4 * g + 1], x[4 * g + 3], w1, q);
-  }
-#pragma unroll
-  for (int g = 0; g < 4; g++) {
-    const uint2 w2 = __ldg(tw + b2 + g);
-    ct_lazy(x[2 * g], x[2 * g + 1], w2, q);
-  }
-}
-
-// Radix-8 inverse network (GS stages at distances 1, 2, 4), mirror of the above.
-__device__ __forceinline__ void radix8_inv(uint32_t *x, const uint2 *tw, int b0, int b1, int b2, uint32_t q) {
-#pragma unroll
-  for (int g = 0; g < 4; g++) {
-    const uint2 w2 = __ldg(tw + b2 + g);
-    gs_lazy(x[2 * g], x[2 * g + 1], w2, q);
-  }
-#pragma unroll
-  for (int g = 0; g < 2; g++) {
-    const uint2 w1 = __ldg(tw + b1 + g);
-    gs_lazy(x[4 * g], x[4 * g + 2], w1, q);
-    gs_lazy(x[4 * g + 1], x[4 * g + 3], w1, q);
-  }
-  const uint2 w0 = __ldg(tw + b0);
-#pragma unroll
-  for (int k = 0; k < 4; k++) gs_lazy(x[k], x[k + 4], w0, q);
-}
 
 // ---------------------------------------------------------------- N = 2^16
 __global__ void __launch_bounds__(256) k_fwd_cols16(const __grid_constant__ RowBatch rb) {
@@ -80,17 +44,7 @@ __global__ void __launch_bounds__(256) k_fwd_cols16(const __grid_constant__ RowB
 #pragma unroll
     for (int k = 0; k < 16; k++) x[k] = shoup_lazy(x[k], rd.c0, rd.c0s, q);
   }
-  // stages m = 1, 2, 4, 8 on rows w + 8k: pair (k, k + 8/m), group k / (16/m)
-#pragma unroll
-  for (int s = 0; s < 4; s++) {
-    const int m = 1 << s, h = 8 >> s;
-#pragma unroll
-    for (int g = 0; g < m; g++) {
-      const uint2 wv = __ldg(tw + m + g);
-#pragma unroll
-      for (int j = 0; j < h; j++) ct_lazy(x[g * 2 * h + j], x[g * 2 * h + j + h], wv, q);
-    }
-  }
+  radix16_cols_fwd(x, tw, q);  // stages m = 1, 2, 4, 8 on rows w + 8k
 #pragma unroll
   for (int k = 0; k < 16; k++) sm[(w + 8 * k) * kColTile + lane] = x[k];
   __syncthreads();
@@ -121,21 +75,7 @@ __global__ void __launch_bounds__(256) k_fwd_rows16(const __grid_constant__ RowB
   uint32_t x[8];
 #pragma unroll
   for (int k = 0; k < 8; k++) x[k] = src[t + 64 * k];
-  radix8_fwd(x, tw, 128 + r, 256 + 2 * r, 512 + 4 * r, q);
-#pragma unroll
-  for (int k = 0; k < 8; k++) srow[t + 64 * k] = x[k];
-  __syncthreads();
-  const int b = t >> 3, u0 = t & 7;
-#pragma unroll
-  for (int k = 0; k < 8; k++) x[k] = srow[64 * b + u0 + 8 * k];
-  radix8_fwd(x, tw, 1024 + 8 * r + b, 2048 + 16 * r + 2 * b, 4096 + 32 * r + 4 * b, q);
-  __syncthreads();
-#pragma unroll
-  for (int k = 0; k < 8; k++) srow[64 * b + u0 + 8 * k] = x[k];
-  __syncthreads();
-#pragma unroll
-  for (int k = 0; k < 8; k++) x[k] = srow[8 * t + k];
-  radix8_fwd(x, tw, 8192 + 64 * r + t, 16384 + 128 * r + 2 * t, 32768 + 256 * r + 4 * t, q);
+  row_fwd(x, srow, tw, r, t, q);
 #pragma unroll
   for (int k = 0; k < 8; k++) x[k] = reduce2q(x[k], q);
   const int base = r * 512 + 8 * t;
@@ -186,21 +126,7 @@ __global__ void __launch_bounds__(256) k_inv_rows16(const __grid_constant__ RowB
 #pragma unroll
     for (int k = 0; k < 8; k++) x[k] = mont_mul(x[k], y[k], q, rd.qinv);
   }
-  radix8_inv(x, tw, 8192 + 64 * r + t, 16384 + 128 * r + 2 * t, 32768 + 256 * r + 4 * t, q);
-#pragma unroll
-  for (int k = 0; k < 8; k++) srow[8 * t + k] = x[k];
-  __syncthreads();
-  const int b = t >> 3, u0 = t & 7;
-#pragma unroll
-  for (int k = 0; k < 8; k++) x[k] = srow[64 * b + u0 + 8 * k];
-  radix8_inv(x, tw, 1024 + 8 * r + b, 2048 + 16 * r + 2 * b, 4096 + 32 * r + 4 * b, q);
-  __syncthreads();
-#pragma unroll
-  for (int k = 0; k < 8; k++) srow[64 * b + u0 + 8 * k] = x[k];
-  __syncthreads();
-#pragma unroll
-  for (int k = 0; k < 8; k++) x[k] = srow[t + 64 * k];
-  radix8_inv(x, tw, 128 + r, 256 + 2 * r, 512 + 4 * r, q);
+  row_inv(x, srow, tw, r, t, q);
   uint32_t *dst = rd.dst + r * 512;
 #pragma unroll
   for (int k = 0; k < 8; k++) dst[t + 64 * k] = x[k];
@@ -229,17 +155,7 @@ __global__ void __launch_bounds__(256) k_inv_cols16(const __grid_constant__ RowB
   uint32_t x[16];
 #pragma unroll
   for (int k = 0; k < 16; k++) x[k] = sm[(w + 8 * k) * kColTile + lane];
-  // stages m = 8, 4, 2, 1 on rows w + 8k: pair (k, k + 8/m)
-#pragma unroll
-  for (int s = 3; s >= 0; s--) {
-    const int m = 1 << s, h = 8 >> s;
-#pragma unroll
-    for (int g = 0; g < m; g++) {
-      const uint2 wv = __ldg(tw + m + g);
-#pragma unroll
-      for (int j = 0; j < h; j++) gs_lazy(x[g * 2 * h + j], x[g * 2 * h + j + h], wv, q);
-    }
-  }
+  radix16_cols_inv(x, tw, q);  // stages m = 8, 4, 2, 1 on rows w + 8k
   const bool centre_out = (rd.flags & kCentre) != 0;
 #pragma unroll
   for (int k = 0; k < 16; k++) {

@@ -1,0 +1,183 @@
+// cheddar_b200.hpp — header-only C++ mirror of the reference's server-side
+// API (scale-snu/cheddar-fhe include/core/Context.h, Container.h) over the C
+// ABI of include/cheddar_b200.h.  Method names, argument order and meaning
+// follow the reference: results are written into a caller-owned `res`
+// (Context.h:101-423).  On failure the reference terminates the process
+// (include/common/Assert.h:9-21); this shim throws cheddar_b200::Error
+// instead (define CHEDDAR_B200_ABORT_ON_ERROR to print and std::exit like
+// the reference).
+#pragma once
+
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "cheddar_b200.h"
+
+namespace cheddar_b200 {
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+inline void check(int rc) {
+  if (rc == CHD_OK) return;
+#ifdef CHEDDAR_B200_ABORT_ON_ERROR
+  std::fprintf(stderr, "ERROR: %s\n", chd_last_error());
+  std::exit(EXIT_FAILURE);
+#else
+  throw Error(rc, chd_last_error());
+#endif
+}
+
+class Context;
+
+// Ciphertext<uint32_t> (Container.h:131-175): device residues [np][N] per part.
+class Ciphertext {
+ public:
+  explicit Ciphertext(Context &ctx);
+  ~Ciphertext() { chd_ct_destroy(ct_); }
+  Ciphertext(const Ciphertext &) = delete;
+  Ciphertext &operator=(const Ciphertext &) = delete;
+  Ciphertext(Ciphertext &&o) noexcept : ct_(o.ct_) { o.ct_ = nullptr; }
+
+  // Ciphertext::GetNP / HasRx / GetScale / GetNumSlots
+  int NumMain() const { return info().num_main; }
+  int NumTer() const { return info().num_ter; }
+  int NumAux() const { return info().num_aux; }
+  bool HasRx() const { return info().has_rx; }
+  double GetScale() const { return info().scale; }
+  int GetNumSlots() const { return info().num_slots; }
+
+  chd_ciphertext *raw() const { return ct_; }
+
+ private:
+  struct Info {
+    int num_main, num_ter, num_aux, has_rx;
+    double scale;
+    int num_slots;
+  };
+  Info info() const {
+    Info i{};
+    check(chd_ct_info(ct_, &i.num_main, &i.num_ter, &i.num_aux, &i.has_rx, &i.scale, &i.num_slots));
+    return i;
+  }
+  chd_ciphertext *ct_ = nullptr;
+};
+
+// EvaluationKey<uint32_t> (Container.h:283-344): beta pairs over [L + alpha][N].
+class EvaluationKey {
+ public:
+  EvaluationKey(Context &ctx, int beta, const uint32_t *bx, const uint32_t *ax, bool on_device);
+  ~EvaluationKey() { chd_evk_destroy(k_); }
+  EvaluationKey(const EvaluationKey &) = delete;
+  EvaluationKey &operator=(const EvaluationKey &) = delete;
+  chd_evk *raw() const { return k_; }
+
+ private:
+  chd_evk *k_ = nullptr;
+};
+
+// Context<uint32_t> (Context.h:17-424)
+class Context {
+ public:
+  using Ct = Ciphertext;
+  using Evk = EvaluationKey;
+
+  // Parameter JSON (unittest/Testbed.h schema) -> Parameter + Context::Create
+  static std::shared_ptr<Context> Create(const std::string &param_json, int device = 0) {
+    chd_context *c = nullptr;
+    check(chd_context_create_json(param_json.c_str(), device, &c));
+    return std::shared_ptr<Context>(new Context(c));
+  }
+  // Parameter(log_degree, base_scale, default_encryption_level, level_config,
+  //           main_primes, aux_primes, ter_primes, additional_base)
+  static std::shared_ptr<Context> Create(int log_degree, double base_scale, int default_encryption_level,
+                                         const std::vector<std::pair<int, int>> &level_config,
+                                         const std::vector<uint32_t> &main_primes,
+                                         const std::vector<uint32_t> &aux_primes,
+                                         const std::vector<uint32_t> &ter_primes = {},
+                                         std::pair<int, int> additional_base = {0, 0}, int device = 0) {
+    std::vector<int> lc;
+    for (auto &p : level_config) {
+      lc.push_back(p.first);
+      lc.push_back(p.second);
+    }
+    chd_context *c = nullptr;
+    check(chd_context_create(log_degree, base_scale, default_encryption_level, lc.data(),
+                             static_cast<int>(level_config.size()), main_primes.data(),
+                             static_cast<int>(main_primes.size()), aux_primes.data(),
+                             static_cast<int>(aux_primes.size()), ter_primes.empty() ? nullptr : ter_primes.data(),
+                             static_cast<int>(ter_primes.size()), additional_base.first, additional_base.second,
+                             device, &c));
+    return std::shared_ptr<Context>(new Context(c));
+  }
+  ~Context() { chd_context_destroy(c_); }
+  Context(const Context &) = delete;
+  Context &operator=(const Context &) = delete;
+
+  chd_context *raw() const { return c_; }
+  int MaxLevel() const { return chd_max_level(c_); }
+  int Degree() const { return chd_degree(c_); }
+  double GetScale(int level) const { return chd_scale(c_, level); }
+  double GetRescalePrimeProd(int level) const { return chd_rescale_prime_prod(c_, level); }
+  void SetStream(void *cuda_stream) { check(chd_context_set_stream(c_, cuda_stream)); }
+  void Synchronize() { check(chd_context_synchronize(c_)); }
+
+  // residue import / export ([np][N] per part), host or device pointers
+  void Import(Ct &ct, int level, int num_aux, double scale, int num_slots, const uint32_t *bx,
+              const uint32_t *ax, const uint32_t *rx = nullptr, bool on_device = false) {
+    int m = 0, t = 0;
+    check(chd_level_np(c_, level, &m, &t));
+    check(chd_ct_import(c_, ct.raw(), m, t, num_aux, rx != nullptr, scale, num_slots, bx, ax, rx, on_device));
+  }
+  void Export(const Ct &ct, uint32_t *bx, uint32_t *ax, uint32_t *rx = nullptr, bool on_device = false) {
+    check(chd_ct_export(c_, ct.raw(), bx, ax, rx, on_device));
+  }
+
+  // ---- evaluator (same signatures as the reference) ----
+  void Add(Ct &res, const Ct &a, const Ct &b) const { check(chd_add(c_, res.raw(), a.raw(), b.raw())); }
+  void Sub(Ct &res, const Ct &a, const Ct &b) const { check(chd_sub(c_, res.raw(), a.raw(), b.raw())); }
+  void Neg(Ct &res, const Ct &a) const { check(chd_neg(c_, res.raw(), a.raw())); }
+  void Mult(Ct &res, const Ct &a, const Ct &b) const { check(chd_mult(c_, res.raw(), a.raw(), b.raw())); }
+  void MultImaginaryUnit(Ct &res, const Ct &a) const { check(chd_mult_imaginary_unit(c_, res.raw(), a.raw())); }
+  void Rescale(Ct &res, const Ct &a) const { check(chd_rescale(c_, res.raw(), a.raw())); }
+  void Relinearize(Ct &res, const Ct &a, const Evk &key) const {
+    check(chd_relinearize(c_, res.raw(), a.raw(), key.raw()));
+  }
+  void RelinearizeRescale(Ct &res, const Ct &a, const Evk &key) const {
+    check(chd_relinearize_rescale(c_, res.raw(), a.raw(), key.raw()));
+  }
+  void MultKey(Ct &res, const Ct &a, const Evk &key) const { check(chd_mult_key(c_, res.raw(), a.raw(), key.raw())); }
+  void HMult(Ct &res, const Ct &a, const Ct &b, const Evk &mult_key, bool rescale = true) const {
+    check(chd_hmult(c_, res.raw(), a.raw(), b.raw(), mult_key.raw(), rescale ? 1 : 0));
+  }
+  void HRot(Ct &res, const Ct &a, const Evk &rot_key, int rot_dist) const {
+    check(chd_hrot(c_, res.raw(), a.raw(), rot_key.raw(), rot_dist));
+  }
+  void HConj(Ct &res, const Ct &a, const Evk &conj_key) const {
+    check(chd_hconj(c_, res.raw(), a.raw(), conj_key.raw()));
+  }
+  void HRotAdd(Ct &res, const Ct &a, const Ct &b, const Evk &rot_key, int rot_dist) const {
+    check(chd_hrot_add(c_, res.raw(), a.raw(), b.raw(), rot_key.raw(), rot_dist));
+  }
+
+ private:
+  explicit Context(chd_context *c) : c_(c) {}
+  chd_context *c_ = nullptr;
+};
+
+inline Ciphertext::Ciphertext(Context &ctx) { check(chd_ct_create(ctx.raw(), &ct_)); }
+
+inline EvaluationKey::EvaluationKey(Context &ctx, int beta, const uint32_t *bx, const uint32_t *ax,
+                                    bool on_device) {
+  check(chd_evk_create(ctx.raw(), beta, bx, ax, on_device ? 1 : 0, &k_));
+}
+
+}  // namespace cheddar_b200

@@ -1,0 +1,39 @@
+"""The header-only C++ mirror (include/cheddar_b200.hpp) compiles and links
+against the C ABI library, and reports a parameter error by exception (no
+GPU needed: the JSON is rejected before any device call)."""
+import os
+import subprocess
+import tempfile
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+SRC = r'''
+#include "cheddar_b200.hpp"
+#include <cstdio>
+int main() {
+  try {
+    auto ctx = cheddar_b200::Context::Create("{\"log_degree\": 16}");
+    (void)ctx;
+    return 2;
+  } catch (const cheddar_b200::Error &e) {
+    std::printf("%d %s\n", e.code, e.what());
+    return e.code == CHD_ERR_PARSE ? 0 : 3;
+  }
+}
+'''
+
+
+def test_cpp_shim_compiles_and_reports_errors():
+    lib_dir = os.path.join(ROOT, "cheddar-fhe_b200")
+    if not os.path.exists(os.path.join(lib_dir, "libcheddar_b200.so")):
+        pytest.skip("library not built")
+    with tempfile.TemporaryDirectory() as d:
+        src = os.path.join(d, "t.cpp")
+        exe = os.path.join(d, "t")
+        open(src, "w").write(SRC)
+        subprocess.run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), src, "-o", exe,
+                        "-L", lib_dir, "-lcheddar_b200", f"-Wl,-rpath,{lib_dir}"], check=True)
+        out = subprocess.run([exe], capture_output=True, text=True)
+        assert out.returncode == 0, out.stdout + out.stderr
+        assert "Missing" in out.stdout
