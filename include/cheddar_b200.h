@@ -171,6 +171,17 @@ int chd_moddown_raw(chd_context *ctx, int level, int type, const uint32_t *src_d
 int chd_bconv_raw(chd_context *ctx, const int32_t *xt_dev, const int *src_gidx, int K,
                   const int *dst_gidx, int M, uint32_t *out_dev);
 
+/* ModUp like chd_modup_raw, but allocating no device memory: for callers
+ * that must not allocate once running (latency-critical servers, where a
+ * cudaMalloc can synchronise the device; hosts whose device memory belongs
+ * to another allocator or a fixed budget).  No counterpart in the reference.
+ * Its scratch is one static device array of 2^21 words (8 MiB) per GPU,
+ * held until the process exits: num_q(level) * N must fit (32 q primes at
+ * N = 2^16), else CHD_ERR_UNSUPPORTED.  All calls share that array, so calls
+ * whose GPU work overlaps race.  The first call on a device looks up the
+ * array's address; make it before any stream capture. */
+int chd_modup_raw_noalloc(chd_context *ctx, int level, const uint32_t *src_dev, uint32_t *dst_dev);
+
 /* Host-side ModSwitch constants of one level, computed without a GPU
  * (ModSwitchHandler ctor, src/core/ModSwitch.cu:175-411).  kind: 0 = ModUp
  * digit `digit`, 1 = ModDown, 2 = Rescale, 3 = ModDownAndRescale.  Outputs:
