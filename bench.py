@@ -12,7 +12,9 @@ Reported (one JSON line on rank 0):
   value      HMult/s with inputs resident in HBM, CUDA events, max over ranks
   e2e        the same through the C ABI with host buffers: each step copies
              the batch in from pinned host memory, runs, copies results out
-  roofline   the dominant kernel, timed alone on the launching stream
+  roofline   the kernel with the largest device time in the step, timed by
+             CUDA events on the context stream around its launches (a
+             second pass of the same steps), algorithmic bytes per launch
   cpu_baseline  the CPU oracle's HMult on the host cores (bounded sample)
 `--impl reference` times the CPU implementation of the path (the oracle;
 the reference itself has no CPU path and cannot be built here) on the same
@@ -224,8 +226,14 @@ def main():
     # ---- end to end through the C ABI with host buffers ----
     e2e = e2e_run(ctx, chd, key, lvl, nq, n, B, args, stream, dist)
 
-    # ---- dominant kernel roofline ----
-    roof = roofline_probe(ctx, chd, lvl, nq, n, stream)
+    # ---- per-stage device timing of the same step: dominant kernel, launches ----
+    ctx.stage_timing(True)
+    for _ in range(args.steps):
+        step()
+    stages = ctx.stage_times()
+    ctx.stage_timing(False)
+    roof = roofline_from_stages(ctx, lvl, B, stages, args.steps)
+    launches = sum(nl for _, nl in stages.values())
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -236,7 +244,7 @@ def main():
                    "l2": "inputs larger than L2 (batch x 24 MB + 48 MB key)",
                    "parallelism": f"replicas x{world}"},
         "e2e": e2e, "roofline": roof, "clocks": sampler.summary(),
-        "gpu_launches": launches_per_step(B) * args.steps,
+        "gpu_launches": launches,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -262,12 +270,6 @@ def chd_primes(ctx):
     p = _j.load(open(os.path.join(ROOT, "cheddar-fhe_b200", "params", PARAM_FILE)))
     ter = list(reversed(p.get("terminal_primes", [])))
     return ter + p["main_primes"] + p["auxiliary_primes"]
-
-
-def launches_per_step(batch):
-    # per HMult: tensor 1, ModUp (INTT 2 + BConv 1 + NTT 2), key MAC 1,
-    # merged ModDown+Rescale (INTT 2 + BConv 1 + NTT 2)
-    return batch * 12
 
 
 def e2e_run(ctx, chd, key, lvl, nq, n, B, args, stream, dist):
@@ -345,11 +347,31 @@ def ptrs(chd, ct):
     return bx.value, ax.value, rx.value
 
 
-def roofline_probe(ctx, chd, lvl, nq, n, stream):
-    """Times the forward NTT over the rows a batched ModUp transforms (the
-    kernel pair that dominates the launch list) on the launching stream.
-    Algorithmic bytes per launch: every limb read once and written once."""
-    import torch
+def stage_limbs(ctx, lvl, batch):
+    """Algorithmic limbs (N x u32 = 256 KiB each) one bench step moves per
+    fused key-switch stage: every operand read once, every result written
+    once; twiddles and tables excluded.  Returns {stage: (per-ciphertext
+    limbs, per-launch limbs)}: the key is read once per key-switch row
+    launch whatever the batch."""
+    nq = ctx.num_q(lvl)
+    tot = nq + ctx.alpha
+    beta = -(-nq // ctx.alpha)          # digits at the top level (no terminal primes)
+    dst = ctx.num_q(lvl - 1)            # ModDownAndRescale keeps the next level's primes
+    drop = tot - dst
+    return {
+        "modup_inv_rows": (2 * nq + nq, 0),                  # a1, a2 in; a1*a2 rows out
+        "modup_cols": (nq + beta * tot - nq, 0),             # digit sources in; other primes out
+        "ks_rows": ((beta * tot - nq) + 4 * nq + 2 * tot,    # ModUp outputs, b1 a1 b2 a2, accumulators
+                    2 * beta * tot),                         # key (bx, ax) per launch
+        "moddown_cols": (2 * drop + 2 * dst, 0),             # dropped rows in; BConv+NTT out
+        "fwd_rows_epilogue": (2 * dst + 2 * dst + 2 * dst, 0),  # BConv rows, kept accumulators in; out
+    }
+
+
+def roofline_from_stages(ctx, lvl, batch, stages, steps):
+    """Roofline of the stage with the largest device time: algorithmic bytes
+    per launch / average launch duration (CUDA events on the context stream,
+    around each stage's launches inside the bench step)."""
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -357,27 +379,42 @@ def roofline_probe(ctx, chd, lvl, nq, n, stream):
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    m, t = ctx.level_np(lvl)
-    polys = 8
-    total = nq + ctx.alpha
-    buf = torch.randint(0, 1 << 29, (polys, total, n), dtype=torch.int32, device="cuda")
-    reps = 20
-    for _ in range(3):
-        ctx.ntt_raw(m, t, ctx.alpha, buf, mont=False, count=polys)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(reps):
-        ctx.ntt_raw(m, t, ctx.alpha, buf, mont=False, count=polys)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / reps
-    algo_bytes = 2 * polys * total * n * 4  # one read + one write of every limb
-    achieved = algo_bytes / (ms / 1e3) / 1e9
-    return {"kernel": "forward NTT (column + row phase) over 8 x 32 limbs", "bound": "hbm",
-            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "peak_source": peak_src, "traffic": None, "algorithmic_bytes_per_launch": algo_bytes,
-            "ms_per_launch": ms}
+    limbs = stage_limbs(ctx, lvl, batch)
+    limb_bytes = ctx.n * 4
+    name = max(stages, key=lambda k: stages[k][0])
+    ms_total, nl = stages[name]
+    per_ct, per_launch = limbs[name]
+    launches_per_step = nl / steps
+    algo = (per_ct * batch / launches_per_step + per_launch) * limb_bytes
+    ms = ms_total / nl
+    achieved = algo / (ms / 1e3) / 1e9
+    traffic = ncu_traffic(name, batch)
+    return {"kernel": KERNEL_OF_STAGE[name], "bound": "hbm", "achieved": achieved, "peak": peak,
+            "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
+            "algorithmic_bytes_per_launch": algo, "ms_per_launch": ms,
+            "stage_ms_per_step": {k: v[0] / steps for k, v in stages.items()},
+            "stage_launches_per_step": {k: v[1] / steps for k, v in stages.items()}}
+
+
+KERNEL_OF_STAGE = {
+    "modup_inv_rows": "k_inv_rows16", "modup_cols": "k_modswitch_cols (ModUp)", "ks_rows": "k_ks_rows",
+    "moddown_cols": "k_modswitch_cols (ModDown)", "fwd_rows_epilogue": "k_fwd_rows16",
+}
+
+
+def ncu_traffic(stage, batch):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of
+    the stage's kernel at this batch, from the committed ncu summary
+    profiles/traffic_hmult_l24.md (a line `traffic <stage> <batch> <bytes>`);
+    None when that capture has not been made."""
+    try:
+        for ln in open(os.path.join(ROOT, "profiles", "traffic_hmult_l24.md")):
+            f = ln.strip().strip("`").split()
+            if len(f) == 4 and f[0] == "traffic" and f[1] == stage and int(f[2]) == batch:
+                return float(f[3])
+    except (OSError, ValueError):
+        pass
+    return None
 
 
 if __name__ == "__main__":

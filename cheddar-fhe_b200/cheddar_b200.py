@@ -19,6 +19,10 @@ PARAM_DIR = os.path.join(_HERE, "params")
 
 CHD_MODDOWN, CHD_RESCALE, CHD_MODDOWN_RESCALE = 0, 1, 2
 
+# stages of the fused N = 2^16 key switch (chd_stage_times), in launch order
+KS_STAGE_NAMES = ("modup_inv_rows", "modup_cols", "ks_rows", "moddown_cols", "fwd_rows_epilogue")
+KS_STAGES = len(KS_STAGE_NAMES)
+
 _lib = None
 
 
@@ -50,6 +54,8 @@ def lib():
         "chd_context_destroy": (None, [vp]),
         "chd_context_set_stream": (i, [vp, vp]),
         "chd_context_synchronize": (i, [vp]),
+        "chd_stage_timing": (i, [vp, i]),
+        "chd_stage_times": (i, [vp, vp, vp]),
         "chd_level_np": (i, [vp, i, C.POINTER(i), C.POINTER(i)]),
         "chd_max_level": (i, [vp]),
         "chd_degree": (i, [vp]),
@@ -157,6 +163,18 @@ class Context:
 
     def synchronize(self):
         _check(lib().chd_context_synchronize(self.ptr))
+
+    def stage_timing(self, enable):
+        """Start (clearing earlier records) or stop device timing of the fused
+        key-switch stages."""
+        _check(lib().chd_stage_timing(self.ptr, 1 if enable else 0))
+
+    def stage_times(self):
+        """{stage: (device ms, launches)} summed since stage_timing(True)."""
+        ms = (C.c_double * KS_STAGES)()
+        nl = (C.c_int * KS_STAGES)()
+        _check(lib().chd_stage_times(self.ptr, ms, nl))
+        return {name: (ms[i], nl[i]) for i, name in enumerate(KS_STAGE_NAMES)}
 
     def level_np(self, level):
         m, t = C.c_int(), C.c_int()

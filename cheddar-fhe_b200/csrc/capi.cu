@@ -85,6 +85,23 @@ int chd_context_set_stream(chd_context *ctx, void *cuda_stream) {
   return CHD_OK;
 }
 
+int chd_stage_timing(chd_context *ctx, int enable) {
+  CHD_NOTNULL(ctx);
+  Context &C = *ctx->c;
+  if (enable) {
+    C.timer.used = 0;
+    C.timer.spans.clear();
+  }
+  C.timer.on = enable != 0;
+  return CHD_OK;
+}
+
+int chd_stage_times(chd_context *ctx, double *ms, int *launches) {
+  CHD_NOTNULL(ctx);
+  if (!ms || !launches) return fail(CHD_ERR_INVALID_ARG, "chd_stage_times: null output");
+  return ctx->c->timer_read(ms, launches);
+}
+
 int chd_context_synchronize(chd_context *ctx) {
   CHD_NOTNULL(ctx);
   cudaError_t e = cudaStreamSynchronize(ctx->c->stream);

@@ -551,7 +551,41 @@ Context::~Context() {
   cudaFree(d_qinv);
   cudaFree(d_tw);
   cudaFree(d_itw);
+  for (cudaEvent_t e : timer.ev) cudaEventDestroy(e);
   if (own_stream && stream) cudaStreamDestroy(stream);
+}
+
+int Context::timer_mark() {
+  if (!timer.on) return -1;
+  if (timer.used == static_cast<int>(timer.ev.size())) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return -1;
+    timer.ev.push_back(e);
+  }
+  cudaEventRecord(timer.ev[timer.used], stream);
+  return timer.used++;
+}
+
+void Context::timer_span(int stage, int e0, int launches) {
+  if (e0 < 0) return;
+  const int e1 = timer_mark();
+  if (e1 >= 0) timer.spans.push_back({stage, e0, e1, launches});
+}
+
+Status Context::timer_read(double *ms, int *launches) {
+  for (int s = 0; s < kKsStages; s++) {
+    ms[s] = 0;
+    launches[s] = 0;
+  }
+  for (const auto &sp : timer.spans) {
+    CHD_CHECK(cudaEventSynchronize(timer.ev[sp.e1]) == cudaSuccess, kErrCuda, "stage timer: event wait failed");
+    float t = 0;
+    CHD_CHECK(cudaEventElapsedTime(&t, timer.ev[sp.e0], timer.ev[sp.e1]) == cudaSuccess, kErrCuda,
+              "stage timer: elapsed time failed");
+    ms[sp.stage] += t;
+    launches[sp.stage] += sp.launches;
+  }
+  return kOk;
 }
 
 void Context::mont_as_shoup(uint32_t c, int g, uint32_t *w, uint32_t *ws) const {
@@ -1084,9 +1118,16 @@ Status Context::key_switch_fused(int level, int count, const KSIn *in, const Dev
       d.q = P->primes[g[r]];
       rows.push_back(d);
     }
-  for_row_batches(rows, [&](const RowBatch &rb) { launch_ntt_inv_rows(rb, P->log_n, stream); });
+  int nl = 0, t0 = timer_mark();
+  for_row_batches(rows, [&](const RowBatch &rb) {
+    launch_ntt_inv_rows(rb, P->log_n, stream);
+    nl++;
+  });
+  timer_span(kKsInvRows, t0, nl);
   // 2. ModUp column pass per (ciphertext, digit)
   {
+    nl = 0;
+    t0 = timer_mark();
     MSColBatch b{};
     b.tw = d_tw;
     b.itw = d_itw;
@@ -1116,10 +1157,12 @@ Status Context::key_switch_fused(int level, int count, const KSIn *in, const Dev
         }
         if (b.count == kMaxMSColJobs) {
           launch_modswitch_cols(b, P->log_n, stream);
+          nl++;
           b.count = 0;
         }
       }
     launch_modswitch_cols(b, P->log_n, stream);
+    timer_span(kKsModUpCols, t0, nl + (b.count > 0));
   }
   // 3. row pass: ModUp NTT rows, key inner product, P (d0, d1), INTT rows of
   //    the dropped primes
@@ -1148,6 +1191,8 @@ Status Context::key_switch_fused(int level, int count, const KSIn *in, const Dev
         if (r >= m.dig_s[digits[bi]] && r < m.dig_e[digits[bi]]) d.own_digit[r] = static_cast<int8_t>(bi);
     }
     for (int i = 0; i < pl.src_len; i++) d.drop_idx[pl.srows[i]] = static_cast<int8_t>(i);
+    nl = 0;
+    t0 = timer_mark();
     for (int c0 = 0; c0 < count; c0 += kMaxKSRowsCts) {
       d.count = std::min(kMaxKSRowsCts, count - c0);
       for (int c = 0; c < d.count; c++) {
@@ -1165,7 +1210,9 @@ Status Context::key_switch_fused(int level, int count, const KSIn *in, const Dev
         k.drop_a = k.drop_b + static_cast<size_t>(pl.src_len) * N;
       }
       launch_ks_rows(d, P->log_n, stream);
+      nl++;
     }
+    timer_span(kKsRows, t0, nl);
   }
   // 4. ModDown column pass per (ciphertext, part)
   {
@@ -1174,6 +1221,8 @@ Status Context::key_switch_fused(int level, int count, const KSIn *in, const Dev
     b.itw = d_itw;
     b.primes = d_primes;
     b.qinvs = d_qinv;
+    nl = 0;
+    t0 = timer_mark();
     for (int c = 0; c < count; c++)
       for (int p = 0; p < 2; p++) {
         MSColJob &j = b.jobs[b.count++];
@@ -1194,10 +1243,12 @@ Status Context::key_switch_fused(int level, int count, const KSIn *in, const Dev
         }
         if (b.count == kMaxMSColJobs) {
           launch_modswitch_cols(b, P->log_n, stream);
+          nl++;
           b.count = 0;
         }
       }
     launch_modswitch_cols(b, P->log_n, stream);
+    timer_span(kKsModDownCols, t0, nl + (b.count > 0));
   }
   // 5. NTT row phase with the ModDown epilogue (src2 = kept accumulators)
   rows.clear();
@@ -1223,7 +1274,13 @@ Status Context::key_switch_fused(int level, int count, const KSIn *in, const Dev
         rows.push_back(d);
       }
     }
-  for_row_batches(rows, [&](const RowBatch &rb) { launch_ntt_fwd_rows(rb, P->log_n, stream); });
+  nl = 0;
+  t0 = timer_mark();
+  for_row_batches(rows, [&](const RowBatch &rb) {
+    launch_ntt_fwd_rows(rb, P->log_n, stream);
+    nl++;
+  });
+  timer_span(kKsFwdRows, t0, nl);
   return check_cuda("key switch");
 }
 

@@ -234,6 +234,22 @@ class Context {
   // ModDown of a Q u P ciphertext back to Q
   Status moddown_ct(DeviceCt &res, const DeviceCt &a);
 
+  // ---- optional device timing of the fused key-switch stages ----
+  // Events recorded on the context stream around each stage's launches.
+  enum KsStage { kKsInvRows, kKsModUpCols, kKsRows, kKsModDownCols, kKsFwdRows, kKsStages };
+  struct StageTimer {
+    bool on = false;
+    std::vector<cudaEvent_t> ev;  // pool, reused across sessions
+    int used = 0;
+    struct Span {
+      int stage, e0, e1, launches;
+    };
+    std::vector<Span> spans;
+  } timer;
+  int timer_mark();                                   // records an event; -1 when off
+  void timer_span(int stage, int e0, int launches);   // closes a span opened by timer_mark
+  Status timer_read(double *ms, int *launches);       // sums per stage (waits for the stream)
+
  private:
   Status init(const ParamSpec &spec, int dev, std::string *err);
   Status check_cuda(const char *where);

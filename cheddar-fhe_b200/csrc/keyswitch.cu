@@ -23,14 +23,16 @@ namespace {
 
 __global__ void __launch_bounds__(256, 3) k_ks_rows(const __grid_constant__ KSRowsDesc d) {
   __shared__ uint32_t sm[4][512];
-  const int j = blockIdx.y;
-  const KSRowsCt &c = d.ct[blockIdx.z];
+  // grid (count, 32, rows): the ciphertexts sharing one key row are
+  // neighbours in launch order, so the key row comes from HBM once
+  const int j = blockIdx.z;
+  const KSRowsCt &c = d.ct[blockIdx.x];
   const uint32_t q = d.q[j];
   const int32_t qi = d.qinv[j];
   const int g = d.gidx[j];
   const uint2 *tw = d.tw + (static_cast<size_t>(g) << 16);
   const int t = threadIdx.x & 63, rl = threadIdx.x >> 6;
-  const int r = blockIdx.x * 4 + rl;
+  const int r = blockIdx.y * 4 + rl;
   uint32_t *srow = sm[rl];
   const size_t off = static_cast<size_t>(j) * 65536 + r * 512 + 8 * t;       // accumulator-row offset
   const size_t koff = static_cast<size_t>(d.key_row[j]) * 65536 + r * 512 + 8 * t;
@@ -117,7 +119,7 @@ __global__ void __launch_bounds__(256, 3) k_ks_rows(const __grid_constant__ KSRo
 
 void launch_ks_rows(const KSRowsDesc &d, int log_n, cudaStream_t s) {
   if (d.count <= 0 || d.rows <= 0 || log_n != 16) return;
-  k_ks_rows<<<dim3(32, d.rows, d.count), 256, 0, s>>>(d);
+  k_ks_rows<<<dim3(d.count, 32, d.rows), 256, 0, s>>>(d);
 }
 
 }  // namespace chd

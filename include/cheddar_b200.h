@@ -182,6 +182,18 @@ int chd_bconv_raw(chd_context *ctx, const int32_t *xt_dev, const int *src_gidx, 
  * array's address; make it before any stream capture. */
 int chd_modup_raw_noalloc(chd_context *ctx, int level, const uint32_t *src_dev, uint32_t *dst_dev);
 
+/* Device timing of the fused key-switch stages (no reference counterpart;
+ * the reference's unit tests time whole operations, unittest/Testbed.h:24-47).
+ * enable != 0 clears earlier records and starts recording CUDA events on the
+ * context stream around every stage; 0 stops.  chd_stage_times waits for the
+ * recorded work and returns, per stage, the summed device milliseconds and
+ * the number of kernel launches:
+ *   0 ModUp INTT row phase, 1 ModUp column pass, 2 key-switch row pass,
+ *   3 ModDown column pass, 4 NTT row phase with the ModDown epilogue. */
+#define CHD_KS_STAGES 5
+int chd_stage_timing(chd_context *ctx, int enable);
+int chd_stage_times(chd_context *ctx, double *ms, int *launches);
+
 /* Host-side ModSwitch constants of one level, computed without a GPU
  * (ModSwitchHandler ctor, src/core/ModSwitch.cu:175-411).  kind: 0 = ModUp
  * digit `digit`, 1 = ModDown, 2 = Rescale, 3 = ModDownAndRescale.  Outputs:

@@ -45,6 +45,29 @@ def test_hmult_inplace_and_batch(cuda_ok):
     _eq(ga[0], o.hmult(lvl, pairs[0][0], pairs[0][1], (kb, ka), rescale=True))
 
 
+def test_stage_timing(cuda_ok):
+    # per-stage device timing of the fused key switch: every stage is timed,
+    # launches are counted, results are unchanged, and stopping freezes it
+    import cheddar_b200 as chd
+    o, g = pair(KS)
+    (kb, ka), key = mult_key(KS)
+    lvl = 18
+    pairs = [(uniform_parts(KS, lvl, 700 + i), uniform_parts(KS, lvl, 800 + i)) for i in range(2)]
+    ga = [g.import_ct(lvl, a) for a, _ in pairs]
+    gb = [g.import_ct(lvl, b) for _, b in pairs]
+    g.stage_timing(True)
+    outs = g.HMultBatch(ga, gb, key, rescale=True)
+    t1 = g.stage_times()
+    g.stage_timing(False)
+    assert tuple(t1) == chd.KS_STAGE_NAMES
+    for name, (ms, nl) in t1.items():
+        assert ms > 0 and nl >= 1, (name, ms, nl)
+    for (a, b), r in zip(pairs, outs):
+        _eq(r, o.hmult(lvl, a, b, (kb, ka), rescale=True))
+    g.HMultBatch(ga, gb, key, rescale=True)
+    assert g.stage_times() == t1
+
+
 def test_hmult_decoded_precision(cuda_ok):
     o, g = pair(KS)
     (kb, ka), key = mult_key(KS)
