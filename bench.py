@@ -235,6 +235,9 @@ def main():
     roof = roofline_from_stages(ctx, lvl, B, stages, args.steps)
     launches = sum(nl for _, nl in stages.values())
 
+    # ---- base conversion as a dense contraction: CUDA cores vs tensor cores ----
+    bconv_cmp = bconv_engines(ctx, chd, stream)
+
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -243,7 +246,7 @@ def main():
                                "(31-bit), dnum=3, top level", "batch_per_gpu": B,
                    "l2": "inputs larger than L2 (batch x 24 MB + 48 MB key)",
                    "parallelism": f"replicas x{world}"},
-        "e2e": e2e, "roofline": roof, "clocks": sampler.summary(),
+        "e2e": e2e, "roofline": roof, "clocks": sampler.summary(), "bconv_engines": bconv_cmp,
         "gpu_launches": launches,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -394,6 +397,60 @@ def roofline_from_stages(ctx, lvl, batch, stages, steps):
             "algorithmic_bytes_per_launch": algo, "ms_per_launch": ms,
             "stage_ms_per_step": {k: v[0] / steps for k, v in stages.items()},
             "stage_launches_per_step": {k: v[1] / steps for k, v in stages.items()}}
+
+
+def bconv_engines(ctx, chd, stream, npoly=64, reps=10):
+    """Base conversion of 64 polynomials at N = 2^16, ModUp 12 -> 4 (12 q
+    primes extended by 4 auxiliary primes) and ModDown 4 -> 12, on the CUDA
+    cores (int64 multiply-adds) and on the tcgen05 tensor cores (INT8 4-limb
+    GEMM, int32 accumulation); outputs compared for equality.  Inputs are
+    centred uniform residues, larger than L2 (64 x 16 limbs = 268 MB per
+    direction).  Algorithmic bytes: every source limb read once, every
+    target limb written once."""
+    import torch
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    n = ctx.n
+    main = list(range(12))
+    aux = list(range(ctx.L, ctx.L + 4))
+    gen = torch.Generator(device="cuda").manual_seed(99)
+    res = {"workload": "BConv, 64 polys, N=2^16, ModUp 12->4 and ModDown 4->12", "engines_equal": True}
+    for name, src, dst in (("modup_12_to_4", main, aux), ("moddown_4_to_12", aux, main)):
+        K, M = len(src), len(dst)
+        xt = torch.randint(-(1 << 29), 1 << 29, (npoly, K, n), generator=gen, device="cuda", dtype=torch.int32)
+        outs = {}
+        row = {}
+        for eng_name, eng in (("cuda_core", chd.BCONV_CUDA_CORE), ("tensor_core", chd.BCONV_TENSOR_CORE)):
+            out = torch.zeros((npoly, M, n), dtype=torch.int32, device="cuda")
+            torch.cuda.synchronize()
+            for _ in range(3):
+                ctx.bconv_batch(xt, src, dst, out, engine=eng, npoly=npoly)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                ctx.bconv_batch(xt, src, dst, out, engine=eng, npoly=npoly)
+            e1.record(stream)
+            ctx.synchronize()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            algo = npoly * (K + M) * n * 4
+            entry = {"ms": ms, "GB/s": algo / (ms / 1e3) / 1e9, "hbm_frac": algo / (ms / 1e3) / 1e9 / hbm}
+            if eng == chd.BCONV_TENSOR_CORE:
+                ks = (4 * K + 31) // 32
+                nb = max(16, (4 * M + 15) // 16 * 16)
+                ops = 2 * npoly * n * ks * 32 * nb  # int8 multiply-adds issued, x2
+                entry["int8_tops"] = ops / (ms / 1e3) / 1e12
+                entry["int8_frac_of_nominal_4500"] = ops / (ms / 1e3) / 1e12 / 4500.0
+            row[eng_name] = entry
+            outs[eng_name] = out
+        res["engines_equal"] = res["engines_equal"] and bool(torch.equal(outs["cuda_core"], outs["tensor_core"]))
+        row["speedup_tensor_vs_cuda_core"] = row["cuda_core"]["ms"] / row["tensor_core"]["ms"]
+        res[name] = row
+    return res
 
 
 KERNEL_OF_STAGE = {

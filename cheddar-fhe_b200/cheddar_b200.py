@@ -18,6 +18,7 @@ LIB_PATH = os.path.join(_HERE, "libcheddar_b200.so")
 PARAM_DIR = os.path.join(_HERE, "params")
 
 CHD_MODDOWN, CHD_RESCALE, CHD_MODDOWN_RESCALE = 0, 1, 2
+BCONV_CUDA_CORE, BCONV_TENSOR_CORE = 0, 1   # chd_bconv_batch engines
 
 # stages of the fused N = 2^16 key switch (chd_stage_times), in launch order
 KS_STAGE_NAMES = ("modup_inv_rows", "modup_cols", "ks_rows", "moddown_cols", "fwd_rows_epilogue")
@@ -98,6 +99,7 @@ def lib():
         "chd_modup_raw": (i, [vp, i, vp, vp]),
         "chd_moddown_raw": (i, [vp, i, i, vp, vp, i]),
         "chd_bconv_raw": (i, [vp, vp, i32p, i, i32p, i, vp]),
+        "chd_bconv_batch": (i, [vp, i, i, vp, i32p, i, i32p, i, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -345,6 +347,16 @@ class Context:
         d = np.ascontiguousarray(dst_gidx, dtype=np.int32)
         _check(lib().chd_bconv_raw(self.ptr, _ptr(xt), s.ctypes.data, len(s), d.ctypes.data, len(d),
                                    _ptr(out)))
+
+    def bconv_batch(self, xt, src_gidx, dst_gidx, out, engine=BCONV_CUDA_CORE, npoly=1):
+        """Batched BConv of npoly polynomials ([npoly][K][N] int32 centred ->
+        [npoly][M][N]); engine BCONV_CUDA_CORE or BCONV_TENSOR_CORE (tcgen05
+        INT8 limb split), identical results.  Asynchronous on the context
+        stream."""
+        s = np.ascontiguousarray(src_gidx, dtype=np.int32)
+        d = np.ascontiguousarray(dst_gidx, dtype=np.int32)
+        _check(lib().chd_bconv_batch(self.ptr, engine, npoly, _ptr(xt), s.ctypes.data, len(s), d.ctypes.data,
+                                     len(d), _ptr(out)))
 
 
 class Ciphertext:

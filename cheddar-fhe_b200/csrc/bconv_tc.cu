@@ -1,0 +1,236 @@
+// Base conversion on the tcgen05 tensor cores (INT8 limb split, exact).
+//
+// BConv (kernel::ModSwitchMatrixMult, src/core/ModSwitch.cu:23-171 of the
+// reference) computes, per coefficient n and target prime p_m,
+//   out[m][n] = (sum_k x_k[n] * T[m][k]) * 2^-32 mod p_m
+// with centred sources |x_k| < 2^30 and the centred table T (k_bconv in
+// elem.cu does it with int64 multiply-adds).  Here the contraction runs as an
+// int8 GEMM with int32 accumulation:
+//   * each source is split into four balanced signed bytes,
+//     x = sum_j 2^(8j) s_j, s_j in [-128, 127]   (A operand, s8, [coeff][4K]);
+//   * each constant c[m][k][j] = 2^(8j) T[m][k] mod p_m (canonical, < 2^31) is
+//     split into four unsigned bytes u[m][k][j][i]  (B operand, u8, [4M][4K]);
+//   * D[n][4m+i] = sum_(k,j) s_j(x_k[n]) u[m][k][j][i]  (|D| < 2^21 for K <= 16)
+//     is exact in int32, and V = sum_i 2^(8i) D[n][4m+i] (|V| < 2^46) is
+//     congruent to sum_k x_k T[m][k] mod p_m.
+// The Montgomery reduction of V therefore yields the same canonical residue
+// as the int64 path: the output is bit-identical.
+//
+// One CTA (4 warps, thread t <-> coefficient row t of a 128-row tile) loops
+// over tiles: sources -> balanced bytes -> shared memory in the canonical
+// K-major no-swizzle layout -> one thread issues the MMAs (M = 128,
+// N = 4M padded to 16, K = 32 bytes per instruction) into TMEM and commits
+// them to an mbarrier -> every warp reads its 32 TMEM lanes back and
+// recombines.  The B operand is prepared once per call on the host in the
+// same layout and copied linearly into shared memory.
+#include <cstdio>
+
+#include "arith.cuh"
+#include "kernels.h"
+
+namespace chd {
+namespace {
+
+constexpr int kRows = 128;          // coefficients per tile (MMA M)
+constexpr int kATileBytes = kRows * 32;  // one K-step of A: 128 rows x 32 bytes
+constexpr uint32_t kWaitLimit = 1u << 22;  // mbarrier polls before giving up
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// K-major, no-swizzle shared-memory matrix descriptor: 8-row x 16-byte core
+// matrices; lbo = byte distance between the two 16-byte K halves of a
+// 32-byte K step, sbo = byte distance between consecutive 8-row groups.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= static_cast<uint64_t>((addr >> 4) & 0x3FFF);
+  d |= static_cast<uint64_t>((lbo >> 4) & 0x3FFF) << 16;
+  d |= static_cast<uint64_t>((sbo >> 4) & 0x3FFF) << 32;
+  d |= 1ull << 46;  // descriptor version for tcgen05
+  return d;         // base offset 0, layout type 0 (no swizzle)
+}
+
+// balanced base-256 digits of a centred residue, packed little-endian
+__device__ __forceinline__ uint32_t split_s8(int32_t x) {
+  const int32_t s0 = static_cast<int8_t>(x & 0xff);
+  x = (x - s0) >> 8;
+  const int32_t s1 = static_cast<int8_t>(x & 0xff);
+  x = (x - s1) >> 8;
+  const int32_t s2 = static_cast<int8_t>(x & 0xff);
+  x = (x - s2) >> 8;  // |x| <= 65 for |input| < 2^30
+  return (static_cast<uint32_t>(s0) & 0xff) | ((static_cast<uint32_t>(s1) & 0xff) << 8) |
+         ((static_cast<uint32_t>(s2) & 0xff) << 16) | (static_cast<uint32_t>(x) << 24);
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// bounded wait; false when the limit ran out
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (uint32_t i = 0; i < kWaitLimit; i++)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+        "=r"(r[15])
+      : "r"(taddr));
+}
+
+__global__ void __launch_bounds__(128) k_bconv_tc(const __grid_constant__ BConvTcDesc d) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tmem_slot;
+  const int t = threadIdx.x, w = t >> 5;
+  const int KS = d.ksteps, NB = d.nb;
+  uint8_t *sa = smem;                                 // KS x 4096 bytes
+  uint8_t *sb = smem + KS * kATileBytes;              // KS x NB x 32 bytes
+  const uint32_t sa_u = smem_u32(sa), sb_u = smem_u32(sb), bar = smem_u32(&mbar);
+
+  // B operand: already in the canonical layout, copy linearly
+  {
+    const uint4 *src = reinterpret_cast<const uint4 *>(d.bmat);
+    uint4 *dst = reinterpret_cast<uint4 *>(sb);
+    for (int i = t; i < KS * NB * 2; i += 128) dst[i] = src[i];
+  }
+  if (t == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+  }
+  if (w == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                 "r"(d.tmem_cols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_slot;
+  const uint32_t lane_base = static_cast<uint32_t>(32 * (w & 3)) << 16;
+
+  const int tiles_per_poly = d.n / kRows;
+  const int ntiles = d.npoly * tiles_per_poly;
+  const size_t n = static_cast<size_t>(d.n);
+  uint32_t phase = 0;
+  bool ok = true;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int poly = tile / tiles_per_poly;
+    const size_t col = static_cast<size_t>(tile % tiles_per_poly) * kRows + t;
+    const int32_t *x = d.xt + static_cast<size_t>(poly) * d.K * n + col;
+    // A operand: row t, chunk c (sources 4c..4c+3) at
+    //   kstep (c / 2) * 4096 + (t / 8) * 256 + (c % 2) * 128 + (t % 8) * 16
+    for (int c = 0; c < 2 * KS; c++) {
+      uint32_t v[4];
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const int k = 4 * c + e;
+        v[e] = k < d.K ? split_s8(__ldg(x + static_cast<size_t>(k) * n)) : 0u;
+      }
+      const int off = (c >> 1) * kATileBytes + (t >> 3) * 256 + (c & 1) * 128 + (t & 7) * 16;
+      *reinterpret_cast<uint4 *>(sa + off) = make_uint4(v[0], v[1], v[2], v[3]);
+    }
+    // make the generic-proxy stores visible to the tensor core
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (t == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      for (int s = 0; s < KS; s++) {
+        const uint64_t ad = smem_desc(sa_u + s * kATileBytes, 128, 256);
+        const uint64_t bd = smem_desc(sb_u + s * NB * 32, 128, 256);
+        const uint32_t acc = s > 0 ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+            ::"r"(tmem), "l"(ad), "l"(bd), "r"(d.idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+            : "memory");
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                   : "memory");
+    }
+    // every thread polls with a limit; the CTA leaves together if any gave up
+    if (!__syncthreads_and(mbar_wait(bar, phase) ? 1 : 0)) {
+      ok = false;
+      break;
+    }
+    phase ^= 1u;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // epilogue: 4 targets (16 TMEM columns) per load
+    uint32_t *o = d.out + static_cast<size_t>(poly) * d.M * n + col;
+    for (int m0 = 0; m0 < d.M; m0 += 4) {
+      uint32_t r[16];
+      tmem_ld16(tmem + lane_base + static_cast<uint32_t>(4 * m0), r);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const int m = m0 + e;
+        if (m < d.M) {
+          const int64_t v = static_cast<int64_t>(static_cast<int32_t>(r[4 * e])) +
+                            (static_cast<int64_t>(static_cast<int32_t>(r[4 * e + 1])) << 8) +
+                            (static_cast<int64_t>(static_cast<int32_t>(r[4 * e + 2])) << 16) +
+                            (static_cast<int64_t>(static_cast<int32_t>(r[4 * e + 3])) << 24);
+          o[static_cast<size_t>(m) * n] = mont_reduce(v, d.p[m], d.pinv[m]);
+        }
+      }
+    }
+    // TMEM reads and shared-memory reads of this tile finish before the
+    // next tile's stores and MMAs
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+  }
+  if (!ok) {
+    if (t == 0 && d.err) atomicExch(d.err, 1);
+    // give the MMA in flight a second bounded chance to land before TMEM is freed
+    mbar_wait(bar, phase);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (w == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(d.tmem_cols) : "memory");
+  }
+}
+
+}  // namespace
+
+size_t bconv_tc_smem(int ksteps, int nb) { return static_cast<size_t>(ksteps) * (kATileBytes + nb * 32); }
+
+int launch_bconv_tc(const BConvTcDesc &d, int num_sms, cudaStream_t s) {
+  if (d.npoly <= 0) return 0;
+  if (d.n % kRows != 0 || d.K < 1 || d.K > 16 || d.M < 1 || d.M > 64) return -1;
+  // CTAs per SM limited so that their TMEM columns fit in the SM's 512
+  const int cap = 512 / d.tmem_cols;
+  size_t sm = bconv_tc_smem(d.ksteps, d.nb);
+  const size_t per_sm = 233472;  // shared memory per SM (228 KiB)
+  const size_t floor_sm = per_sm / (cap + 1) - 1024 + 16;
+  if (sm < floor_sm) sm = floor_sm;
+  if (cudaFuncSetAttribute(k_bconv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)) !=
+      cudaSuccess)
+    return -2;
+  int per = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bconv_tc, 128, sm) != cudaSuccess || per < 1) return -2;
+  if (per > cap) per = cap;
+  const int ntiles = d.npoly * (d.n / kRows);
+  int grid = num_sms * per;
+  if (grid > ntiles) grid = ntiles;
+  k_bconv_tc<<<grid, 128, sm, s>>>(d);
+  return 0;
+}
+
+}  // namespace chd

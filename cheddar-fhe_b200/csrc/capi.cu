@@ -104,8 +104,17 @@ int chd_stage_times(chd_context *ctx, double *ms, int *launches) {
 
 int chd_context_synchronize(chd_context *ctx) {
   CHD_NOTNULL(ctx);
-  cudaError_t e = cudaStreamSynchronize(ctx->c->stream);
+  Context &C = *ctx->c;
+  cudaError_t e = cudaStreamSynchronize(C.stream);
   if (e != cudaSuccess) return fail(CHD_ERR_CUDA, cudaGetErrorString(e));
+  // a kernel whose bounded wait ran out leaves 1 in the device error word
+  int flag = 0;
+  e = cudaMemcpy(&flag, C.d_err, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return fail(CHD_ERR_CUDA, cudaGetErrorString(e));
+  if (flag) {
+    cudaMemset(C.d_err, 0, sizeof(int));
+    return fail(CHD_ERR_CUDA, "a kernel gave up waiting for its tensor-core work (bounded wait ran out)");
+  }
   return CHD_OK;
 }
 
@@ -491,6 +500,31 @@ int chd_moddown_raw(chd_context *ctx, int level, int type, const uint32_t *src_d
   return C.moddown(level, t, s.data(), d.data(), npoly);
 }
 
+namespace {
+// BConv table of ModSwitchMatrixMult (ModSwitch.cu:320-411): T[m][k] =
+// centre(prod_{j != k} src_j * R^2 mod dst_m), validated indices
+int bconv_table(const Context &C, const int *src_gidx, int K, const int *dst_gidx, int M, std::vector<int32_t> *t,
+                const char *who) {
+  const int np_all = C.P->L + C.P->alpha;
+  if (K < 1 || K > 16 || M < 1 || M > 64) return fail(CHD_ERR_UNSUPPORTED, std::string(who) + ": K in [1,16], M in [1,64]");
+  for (int i = 0; i < K; i++)
+    if (src_gidx[i] < 0 || src_gidx[i] >= np_all) return fail(CHD_ERR_INVALID_ARG, std::string(who) + ": bad src index");
+  for (int i = 0; i < M; i++)
+    if (dst_gidx[i] < 0 || dst_gidx[i] >= np_all) return fail(CHD_ERR_INVALID_ARG, std::string(who) + ": bad dst index");
+  t->assign(static_cast<size_t>(M) * K, 0);
+  for (int m = 0; m < M; m++) {
+    uint32_t p = C.P->primes[dst_gidx[m]];
+    for (int k = 0; k < K; k++) {
+      uint32_t acc = 1;
+      for (int j = 0; j < K; j++)
+        if (j != k) acc = prime::mul_mod(acc, C.P->primes[src_gidx[j]], p);
+      (*t)[m * K + k] = prime::centre(prime::to_mont(prime::to_mont(acc, p), p), p);
+    }
+  }
+  return CHD_OK;
+}
+}  // namespace
+
 int chd_bconv_raw(chd_context *ctx, const int32_t *xt_dev, const int *src_gidx, int K, const int *dst_gidx, int M,
                   uint32_t *out_dev) {
   CHD_NOTNULL(ctx);
@@ -499,29 +533,32 @@ int chd_bconv_raw(chd_context *ctx, const int32_t *xt_dev, const int *src_gidx, 
   CHD_NOTNULL(dst_gidx);
   CHD_NOTNULL(out_dev);
   Context &C = *ctx->c;
-  const int np_all = C.P->L + C.P->alpha;
-  if (K < 1 || K > 16 || M < 1 || M > 64) return fail(CHD_ERR_UNSUPPORTED, "chd_bconv_raw: K in [1,16], M in [1,64]");
-  for (int i = 0; i < K; i++)
-    if (src_gidx[i] < 0 || src_gidx[i] >= np_all) return fail(CHD_ERR_INVALID_ARG, "chd_bconv_raw: bad src index");
-  for (int i = 0; i < M; i++)
-    if (dst_gidx[i] < 0 || dst_gidx[i] >= np_all) return fail(CHD_ERR_INVALID_ARG, "chd_bconv_raw: bad dst index");
-  std::vector<int32_t> t(static_cast<size_t>(M) * K);
-  for (int m = 0; m < M; m++) {
-    uint32_t p = C.P->primes[dst_gidx[m]];
-    for (int k = 0; k < K; k++) {
-      uint32_t acc = 1;
-      for (int j = 0; j < K; j++)
-        if (j != k) acc = prime::mul_mod(acc, C.P->primes[src_gidx[j]], p);
-      t[m * K + k] = prime::centre(prime::to_mont(prime::to_mont(acc, p), p), p);
-    }
-  }
+  std::vector<int32_t> t;
+  int rc = bconv_table(C, src_gidx, K, dst_gidx, M, &t, "chd_bconv_raw");
+  if (rc != CHD_OK) return rc;
   int32_t *dt = nullptr;
   if (cudaMalloc(&dt, t.size() * 4) != cudaSuccess) return fail(CHD_ERR_ALLOC, "chd_bconv_raw: allocation failed");
   cudaMemcpyAsync(dt, t.data(), t.size() * 4, cudaMemcpyHostToDevice, C.stream);
-  int rc = C.bconv(xt_dev, K, dt, dst_gidx, M, out_dev);
+  rc = C.bconv(xt_dev, K, dt, dst_gidx, M, out_dev);
   cudaStreamSynchronize(C.stream);
   cudaFree(dt);
   return rc;
+}
+
+int chd_bconv_batch(chd_context *ctx, int engine, int npoly, const int32_t *xt_dev, const int *src_gidx, int K,
+                    const int *dst_gidx, int M, uint32_t *out_dev) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(src_gidx);
+  CHD_NOTNULL(dst_gidx);
+  if (npoly < 0) return fail(CHD_ERR_INVALID_ARG, "chd_bconv_batch: negative npoly");
+  if (npoly > 0 && (!xt_dev || !out_dev)) return fail(CHD_ERR_INVALID_ARG, "chd_bconv_batch: null buffer");
+  if (engine != CHD_BCONV_CUDA_CORE && engine != CHD_BCONV_TENSOR_CORE)
+    return fail(CHD_ERR_INVALID_ARG, "chd_bconv_batch: unknown engine");
+  Context &C = *ctx->c;
+  std::vector<int32_t> t;
+  int rc = bconv_table(C, src_gidx, K, dst_gidx, M, &t, "chd_bconv_batch");
+  if (rc != CHD_OK) return rc;
+  return C.bconv_many(engine, npoly, xt_dev, K, t, dst_gidx, M, out_dev);
 }
 
 int chd_params_level_consts(const char *json_text, int level, int kind, int digit, uint32_t *c1, int32_t *table,

@@ -549,6 +549,7 @@ Context::~Context() {
   }
   cudaFree(d_primes);
   cudaFree(d_qinv);
+  cudaFree(d_err);
   cudaFree(d_tw);
   cudaFree(d_itw);
   for (cudaEvent_t e : timer.ev) cudaEventDestroy(e);
@@ -780,6 +781,11 @@ Status Context::init(const ParamSpec &spec, int dev, std::string *err) {
     *err = "device allocation failed";
     return kErrAlloc;
   }
+  if (cudaMalloc(&d_err, sizeof(int)) != cudaSuccess || cudaMemset(d_err, 0, sizeof(int)) != cudaSuccess) {
+    *err = "device allocation failed";
+    return kErrAlloc;
+  }
+  cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
   cudaMemcpy(d_primes, P->primes.data(), np_all * 4, cudaMemcpyHostToDevice);
   cudaMemcpy(d_qinv, P->qinv.data(), np_all * 4, cudaMemcpyHostToDevice);
   cudaMemcpy(d_tw, tw.data(), tw.size() * sizeof(uint2), cudaMemcpyHostToDevice);
@@ -881,6 +887,86 @@ Status Context::bconv(const int32_t *xt, int K, const int32_t *table, const int 
   }
   launch_bconv(b, P->log_n, stream);
   return check_cuda("bconv");
+}
+
+Status Context::bconv_many(int engine, int npoly, const int32_t *xt, int K, const std::vector<int32_t> &table,
+                           const int *dst_gidx, int M, uint32_t *out) {
+  CHD_CHECK(K >= 1 && K <= 16 && M >= 1 && M <= 64, kErrUnsupported, "bconv: K must be in [1,16], M in [1,64]");
+  CHD_CHECK(static_cast<int>(table.size()) == M * K, kErrInvalidArg, "bconv: table size mismatch");
+  if (npoly <= 0) return kOk;
+  const size_t n = static_cast<size_t>(P->n);
+  ArenaScope scope(arena);
+  if (engine == 0) {
+    int32_t *dt = static_cast<int32_t *>(arena.alloc(table.size() * 4));
+    CHD_CHECK(dt, kErrAlloc, "bconv: scratch allocation failed");
+    cudaMemcpyAsync(dt, table.data(), table.size() * 4, cudaMemcpyHostToDevice, stream);
+    BConvBatch b{};
+    b.primes = d_primes;
+    b.qinvs = d_qinv;
+    for (int i = 0; i < npoly; i++) {
+      BConvJob &j = b.jobs[b.count++];
+      j.xt = xt + static_cast<size_t>(i) * K * n;
+      j.out = out + static_cast<size_t>(i) * M * n;
+      j.table = dt;
+      j.K = K;
+      j.M = M;
+      for (int m = 0; m < M; m++) {
+        j.out_row[m] = static_cast<uint8_t>(m);
+        j.out_gidx[m] = static_cast<uint8_t>(dst_gidx[m]);
+      }
+      if (b.count == kMaxBConvJobs) {
+        launch_bconv(b, P->log_n, stream);
+        b.count = 0;
+      }
+    }
+    launch_bconv(b, P->log_n, stream);
+    return check_cuda("bconv");
+  }
+  CHD_CHECK(engine == 1, kErrInvalidArg, "bconv: engine must be 0 (CUDA cores) or 1 (tensor cores)");
+  CHD_CHECK(P->n % 128 == 0, kErrUnsupported, "bconv: tensor-core engine needs N >= 128");
+  BConvTcDesc d{};
+  d.K = K;
+  d.M = M;
+  d.n = P->n;
+  d.npoly = npoly;
+  d.ksteps = (4 * K + 31) / 32;
+  d.nb = std::max(16, (4 * M + 15) / 16 * 16);
+  d.tmem_cols = 32;
+  while (d.tmem_cols < d.nb) d.tmem_cols *= 2;
+  // kind::i8: D s32 (bits 4-5 = 2), A s8 (bits 7-9 = 1), B u8 (bits 10-12 = 0),
+  // both K-major, N >> 3 at bit 17, M >> 4 at bit 24
+  d.idesc = (2u << 4) | (1u << 7) | (0u << 10) | (static_cast<uint32_t>(d.nb >> 3) << 17) | ((128u >> 4) << 24);
+  // B operand image: row r = 4m + i (byte i of the constant), K byte kb = 4k + j
+  std::vector<uint8_t> img(static_cast<size_t>(d.ksteps) * d.nb * 32, 0);
+  for (int m = 0; m < M; m++) {
+    const uint32_t p = P->primes[dst_gidx[m]];
+    d.p[m] = p;
+    d.pinv[m] = P->qinv[dst_gidx[m]];
+    for (int k = 0; k < K; k++) {
+      const int32_t tc = table[static_cast<size_t>(m) * K + k];
+      const uint64_t t = tc < 0 ? static_cast<uint64_t>(static_cast<int64_t>(tc) + p) : static_cast<uint64_t>(tc);
+      for (int j = 0; j < 4; j++) {
+        const uint32_t c = static_cast<uint32_t>((t << (8 * j)) % p);
+        const int kb = 4 * k + j;
+        for (int i = 0; i < 4; i++) {
+          const int r = 4 * m + i;
+          const size_t off = static_cast<size_t>(kb / 32) * d.nb * 32 + (r / 8) * 256 + ((kb % 32) / 16) * 128 +
+                             (r % 8) * 16 + (kb % 16);
+          img[off] = static_cast<uint8_t>(c >> (8 * i));
+        }
+      }
+    }
+  }
+  uint8_t *dimg = static_cast<uint8_t *>(arena.alloc(img.size()));
+  CHD_CHECK(dimg, kErrAlloc, "bconv: scratch allocation failed");
+  cudaMemcpyAsync(dimg, img.data(), img.size(), cudaMemcpyHostToDevice, stream);
+  d.xt = xt;
+  d.out = out;
+  d.bmat = dimg;
+  d.err = d_err;
+  const int rc = launch_bconv_tc(d, num_sms, stream);
+  CHD_CHECK(rc == 0, kErrCuda, "bconv: tensor-core launch configuration failed");
+  return check_cuda("bconv (tensor cores)");
 }
 
 Status Context::modup(int level, const uint32_t *src, uint32_t *const *dst) {

@@ -166,6 +166,8 @@ class Context {
   // device tables
   uint32_t *d_primes = nullptr;
   int32_t *d_qinv = nullptr;
+  int *d_err = nullptr;   // set by kernels whose bounded waits ran out
+  int num_sms = 0;
   uint2 *d_tw = nullptr, *d_itw = nullptr;  // [nprimes][N] (psi_rev, Shoup companion)
   std::vector<uint32_t> n_inv, n_inv_mont, mont_conv, p_prod, imag_unit;
   std::vector<uint32_t> r_inv;  // 2^-32 mod q per global prime
@@ -208,6 +210,12 @@ class Context {
   // ModDown family on npoly polys
   Status moddown(int level, MDType type, const uint32_t *const *src, uint32_t *const *dst, int npoly);
   Status bconv(const int32_t *xt, int K, const int32_t *table, const int *dst_gidx, int M, uint32_t *out);
+  // BConv of npoly polynomials ([npoly][K][N] -> [npoly][M][N]) with the
+  // host table T[m][k] (centred, Montgomery q-hat R^2): engine 0 on the CUDA
+  // cores (int64 multiply-adds), engine 1 on the tcgen05 tensor cores (INT8
+  // limb split); identical results.
+  Status bconv_many(int engine, int npoly, const int32_t *xt, int K, const std::vector<int32_t> &table,
+                    const int *dst_gidx, int M, uint32_t *out);
 
   // ---- evaluator (Context.cpp of the reference) ----
   Status add(DeviceCt &res, const DeviceCt &a, const DeviceCt &b);

@@ -74,6 +74,27 @@ struct BConvBatch {
 };
 void launch_bconv(const BConvBatch &b, int log_n, cudaStream_t s);
 
+// BConv of npoly polynomials on the tcgen05 tensor cores (bconv_tc.cu):
+// xt [npoly][K][n] centred sources, out [npoly][M][n]; bmat is the B operand
+// (bytes of 2^(8j) T[m][k] mod p_m) in the canonical K-major shared-memory
+// image, ksteps x nb x 32 bytes.  err is set to 1 when an MMA completion wait
+// runs out (the kernel then returns without finishing).
+struct BConvTcDesc {
+  const int32_t *xt;
+  uint32_t *out;
+  const uint8_t *bmat;
+  int *err;
+  int K, M, n, npoly;
+  int ksteps;      // ceil(4K / 32)
+  int nb;          // 4M rounded up to a multiple of 16 (MMA N)
+  int tmem_cols;   // power of two >= max(32, nb)
+  uint32_t idesc;  // tcgen05 instruction descriptor (kind::i8, s8 x u8 -> s32, M = 128, N = nb)
+  uint32_t p[64];
+  int32_t pinv[64];
+};
+size_t bconv_tc_smem(int ksteps, int nb);
+int launch_bconv_tc(const BConvTcDesc &d, int num_sms, cudaStream_t s);
+
 // Fused ModSwitch column pass (N = 2^16 only): per 16-column tile
 //   x~_k  = centre(INTT column phase(src_k) * c0_k)        (K <= 16 sources)
 //   y_m   = (sum_k x~_k T[m][k]) * 2^-32 mod p_m           (exact BConv)

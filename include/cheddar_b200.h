@@ -171,6 +171,18 @@ int chd_moddown_raw(chd_context *ctx, int level, int type, const uint32_t *src_d
 int chd_bconv_raw(chd_context *ctx, const int32_t *xt_dev, const int *src_gidx, int K,
                   const int *dst_gidx, int M, uint32_t *out_dev);
 
+/* Batched kernel::ModSwitchMatrixMult: npoly polynomials, each K centred
+ * source limbs [K][N] (xt_dev + i*K*N) -> M limbs [M][N] (out_dev + i*M*N),
+ * same table and result as chd_bconv_raw.  engine CHD_BCONV_CUDA_CORE runs
+ * int64 multiply-adds; CHD_BCONV_TENSOR_CORE runs the contraction as an INT8
+ * 4-limb GEMM on the tcgen05 tensor cores with int32 accumulation (exact,
+ * bit-identical output).  Asynchronous; chd_context_synchronize reports a
+ * tensor-core wait that ran out. */
+#define CHD_BCONV_CUDA_CORE 0
+#define CHD_BCONV_TENSOR_CORE 1
+int chd_bconv_batch(chd_context *ctx, int engine, int npoly, const int32_t *xt_dev, const int *src_gidx, int K,
+                    const int *dst_gidx, int M, uint32_t *out_dev);
+
 /* ModUp like chd_modup_raw, but allocating no device memory: for callers
  * that must not allocate once running (latency-critical servers, where a
  * cudaMalloc can synchronise the device; hosts whose device memory belongs
