@@ -23,7 +23,7 @@
 // them to an mbarrier -> every warp reads its 32 TMEM lanes back and
 // recombines.  The B operand is prepared once per call on the host in the
 // same layout and copied linearly into shared memory.
-#include <cstdio>
+#include <algorithm>
 
 #include "arith.cuh"
 #include "kernels.h"
@@ -92,15 +92,23 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
       : "r"(taddr));
 }
 
+// Software pipeline over iterations (TPI tiles each), two buffers for the A
+// tiles and the TMEM accumulators:
+//   split + store A(i) -> MMA(i) -> loads of i+1 in flight -> epilogue(i-1)
+// so the HBM loads of one iteration overlap the MMAs of the current one and
+// the TMEM read-back and stores of the previous one.
+template <int TPI>
 __global__ void __launch_bounds__(128) k_bconv_tc(const __grid_constant__ BConvTcDesc d) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  __shared__ __align__(8) uint64_t mbar;
+  __shared__ __align__(8) uint64_t mbar[2];
   __shared__ uint32_t tmem_slot;
   const int t = threadIdx.x, w = t >> 5;
-  const int KS = d.ksteps, NB = d.nb;
-  uint8_t *sa = smem;                                 // KS x 4096 bytes
-  uint8_t *sb = smem + KS * kATileBytes;              // KS x NB x 32 bytes
-  const uint32_t sa_u = smem_u32(sa), sb_u = smem_u32(sb), bar = smem_u32(&mbar);
+  const int KS = d.ksteps, NB = d.nb, K = d.K, M = d.M;
+  const int abuf = TPI * KS * kATileBytes;            // one A buffer
+  uint8_t *sa = smem;                                 // 2 x TPI x KS x 4096 bytes
+  uint8_t *sb = smem + 2 * abuf;                      // KS x NB x 32 bytes
+  const uint32_t sa_u = smem_u32(sa), sb_u = smem_u32(sb);
+  const uint32_t bar0 = smem_u32(&mbar[0]), bar1 = smem_u32(&mbar[1]);
 
   // B operand: already in the canonical layout, copy linearly
   {
@@ -109,7 +117,8 @@ __global__ void __launch_bounds__(128) k_bconv_tc(const __grid_constant__ BConvT
     for (int i = t; i < KS * NB * 2; i += 128) dst[i] = src[i];
   }
   if (t == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar1) : "memory");
   }
   if (w == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
@@ -122,82 +131,131 @@ __global__ void __launch_bounds__(128) k_bconv_tc(const __grid_constant__ BConvT
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_slot;
   const uint32_t lane_base = static_cast<uint32_t>(32 * (w & 3)) << 16;
+  const uint32_t tbuf = static_cast<uint32_t>(TPI * NB);  // TMEM columns of one accumulator buffer
 
+  // an iteration takes TPI consecutive 128-row tiles of one polynomial
+  // (TPI divides the tiles per polynomial)
   const int tiles_per_poly = d.n / kRows;
-  const int ntiles = d.npoly * tiles_per_poly;
+  const int nits = d.npoly * tiles_per_poly / TPI;
   const size_t n = static_cast<size_t>(d.n);
-  uint32_t phase = 0;
-  bool ok = true;
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int poly = tile / tiles_per_poly;
-    const size_t col = static_cast<size_t>(tile % tiles_per_poly) * kRows + t;
-    const int32_t *x = d.xt + static_cast<size_t>(poly) * d.K * n + col;
-    // A operand: row t, chunk c (sources 4c..4c+3) at
-    //   kstep (c / 2) * 4096 + (t / 8) * 256 + (c % 2) * 128 + (t % 8) * 16
-    for (int c = 0; c < 2 * KS; c++) {
-      uint32_t v[4];
+  auto src_of = [&](int it) {
+    const int tile0 = it * TPI;
+    return d.xt + static_cast<size_t>(tile0 / tiles_per_poly) * K * n +
+           static_cast<size_t>(tile0 % tiles_per_poly) * kRows + t;
+  };
+  auto dst_of = [&](int it) {
+    const int tile0 = it * TPI;
+    return d.out + static_cast<size_t>(tile0 / tiles_per_poly) * M * n +
+           static_cast<size_t>(tile0 % tiles_per_poly) * kRows + t;
+  };
+  int32_t v[TPI][16];
+  auto load = [&](int it) {
+    const int32_t *x = src_of(it);
 #pragma unroll
-      for (int e = 0; e < 4; e++) {
-        const int k = 4 * c + e;
-        v[e] = k < d.K ? split_s8(__ldg(x + static_cast<size_t>(k) * n)) : 0u;
+    for (int u = 0; u < TPI; u++)
+#pragma unroll
+      for (int k = 0; k < 16; k++) v[u][k] = k < K ? __ldg(x + static_cast<size_t>(k) * n + u * kRows) : 0;
+  };
+  auto epilogue = [&](int it, int b) {
+    uint32_t *o = dst_of(it);
+#pragma unroll
+    for (int u = 0; u < TPI; u++)
+      for (int m0 = 0; m0 < M; m0 += 4) {
+        uint32_t r[16];
+        tmem_ld16(tmem + lane_base + b * tbuf + static_cast<uint32_t>(u * NB + 4 * m0), r);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          const int m = m0 + e;
+          if (m < M) {
+            const int64_t val = static_cast<int64_t>(static_cast<int32_t>(r[4 * e])) +
+                                (static_cast<int64_t>(static_cast<int32_t>(r[4 * e + 1])) << 8) +
+                                (static_cast<int64_t>(static_cast<int32_t>(r[4 * e + 2])) << 16) +
+                                (static_cast<int64_t>(static_cast<int32_t>(r[4 * e + 3])) << 24);
+            o[static_cast<size_t>(m) * n + u * kRows] = mont_reduce(val, d.p[m], d.pinv[m]);
+          }
+        }
       }
-      const int off = (c >> 1) * kATileBytes + (t >> 3) * 256 + (c & 1) * 128 + (t & 7) * 16;
-      *reinterpret_cast<uint4 *>(sa + off) = make_uint4(v[0], v[1], v[2], v[3]);
-    }
+  };
+
+  // phase parity of each accumulator buffer's mbarrier (bit b), kept in a
+  // register
+  uint32_t parity = 0u;
+  bool ok = true;
+  int prev = -1;  // iteration whose accumulators wait for their epilogue
+  int it = blockIdx.x;
+  if (it < nits) load(it);
+  for (int i = 0; it < nits; i++, it += gridDim.x) {
+    const int b = i & 1;
+    // A operand of tile u: row t, chunk c (sources 4c..4c+3) at
+    //   b * abuf + (u * KS + c / 2) * 4096 + (t / 8) * 256 + (c % 2) * 128 + (t % 8) * 16
+#pragma unroll
+    for (int u = 0; u < TPI; u++)
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        if (c < 2 * KS) {
+          const int off = b * abuf + (u * KS + (c >> 1)) * kATileBytes + (t >> 3) * 256 + (c & 1) * 128 + (t & 7) * 16;
+          *reinterpret_cast<uint4 *>(sa + off) = make_uint4(split_s8(v[u][4 * c]), split_s8(v[u][4 * c + 1]),
+                                                            split_s8(v[u][4 * c + 2]), split_s8(v[u][4 * c + 3]));
+        }
+      }
     // make the generic-proxy stores visible to the tensor core
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (t == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      for (int s = 0; s < KS; s++) {
-        const uint64_t ad = smem_desc(sa_u + s * kATileBytes, 128, 256);
-        const uint64_t bd = smem_desc(sb_u + s * NB * 32, 128, 256);
-        const uint32_t acc = s > 0 ? 1u : 0u;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "setp.ne.b32 p, %4, 0;\n\t"
-            "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-            ::"r"(tmem), "l"(ad), "l"(bd), "r"(d.idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
-            : "memory");
-      }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+      for (int u = 0; u < TPI; u++)
+        for (int s = 0; s < KS; s++) {
+          const uint64_t ad = smem_desc(sa_u + b * abuf + (u * KS + s) * kATileBytes, 128, 256);
+          const uint64_t bd = smem_desc(sb_u + s * NB * 32, 128, 256);
+          const uint32_t acc = s > 0 ? 1u : 0u;
+          asm volatile(
+              "{\n\t.reg .pred p;\n\t"
+              "setp.ne.b32 p, %4, 0;\n\t"
+              "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+              ::"r"(tmem + b * tbuf + static_cast<uint32_t>(u * NB)), "l"(ad), "l"(bd), "r"(d.idesc), "r"(acc),
+              "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+              : "memory");
+        }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(b ? bar1
+                                                                                                          : bar0)
                    : "memory");
     }
-    // every thread polls with a limit; the CTA leaves together if any gave up
-    if (!__syncthreads_and(mbar_wait(bar, phase) ? 1 : 0)) {
-      ok = false;
-      break;
-    }
-    phase ^= 1u;
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    // epilogue: 4 targets (16 TMEM columns) per load
-    uint32_t *o = d.out + static_cast<size_t>(poly) * d.M * n + col;
-    for (int m0 = 0; m0 < d.M; m0 += 4) {
-      uint32_t r[16];
-      tmem_ld16(tmem + lane_base + static_cast<uint32_t>(4 * m0), r);
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-      for (int e = 0; e < 4; e++) {
-        const int m = m0 + e;
-        if (m < d.M) {
-          const int64_t v = static_cast<int64_t>(static_cast<int32_t>(r[4 * e])) +
-                            (static_cast<int64_t>(static_cast<int32_t>(r[4 * e + 1])) << 8) +
-                            (static_cast<int64_t>(static_cast<int32_t>(r[4 * e + 2])) << 16) +
-                            (static_cast<int64_t>(static_cast<int32_t>(r[4 * e + 3])) << 24);
-          o[static_cast<size_t>(m) * n] = mont_reduce(v, d.p[m], d.pinv[m]);
-        }
+    // next iteration's loads go out while the MMAs run
+    if (it + static_cast<int>(gridDim.x) < nits) load(it + gridDim.x);
+    if (prev >= 0) {
+      const int pb = b ^ 1;
+      // every thread polls with a limit; the CTA leaves together if any gave up
+      if (!__syncthreads_and(mbar_wait(pb ? bar1 : bar0, (parity >> pb) & 1u) ? 1 : 0)) {
+        ok = false;
+        break;
       }
+      parity ^= 1u << pb;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      epilogue(prev, pb);
+      // TMEM reads of buffer pb finish before MMAs overwrite it
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     }
-    // TMEM reads and shared-memory reads of this tile finish before the
-    // next tile's stores and MMAs
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
+    prev = it;
+  }
+  if (ok && prev >= 0) {
+    // the last iteration's accumulators sit in buffer ((iterations - 1) & 1)
+    const int nmine = (nits - 1 - static_cast<int>(blockIdx.x)) / static_cast<int>(gridDim.x) + 1;
+    const int pb = (nmine - 1) & 1;
+    if (__syncthreads_and(mbar_wait(pb ? bar1 : bar0, (parity >> pb) & 1u) ? 1 : 0)) {
+      parity ^= 1u << pb;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      epilogue(prev, pb);
+    } else {
+      ok = false;
+    }
   }
   if (!ok) {
     if (t == 0 && d.err) atomicExch(d.err, 1);
-    // give the MMA in flight a second bounded chance to land before TMEM is freed
-    mbar_wait(bar, phase);
+    // give the MMAs in flight a second bounded chance to land before TMEM is freed
+    mbar_wait(bar0, parity & 1u);
+    mbar_wait(bar1, (parity >> 1) & 1u);
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -209,28 +267,52 @@ __global__ void __launch_bounds__(128) k_bconv_tc(const __grid_constant__ BConvT
 
 }  // namespace
 
-size_t bconv_tc_smem(int ksteps, int nb) { return static_cast<size_t>(ksteps) * (kATileBytes + nb * 32); }
+size_t bconv_tc_smem(int tpi, int ksteps, int nb) {
+  return static_cast<size_t>(ksteps) * (2 * static_cast<size_t>(tpi) * kATileBytes + nb * 32);
+}
+
+namespace {
+template <int TPI>
+int launch_tpi(const BConvTcDesc &d, int num_sms, cudaStream_t s) {
+  // CTAs per SM: TMEM (512 columns), registers, shared memory (228 KiB per
+  // SM, 1 KiB reserved per CTA), 16 CTAs of 128 threads; the dynamic shared
+  // memory is padded so that no more CTAs than the TMEM allows are resident
+  const int cap = 512 / d.tmem_cols;
+  size_t sm = bconv_tc_smem(TPI, d.ksteps, d.nb);
+  cudaFuncAttributes fa{};
+  if (cudaFuncGetAttributes(&fa, k_bconv_tc<TPI>) != cudaSuccess) return -2;
+  const size_t per_sm = 233472, reserved = 1024 + fa.sharedSizeBytes;
+  const size_t floor_sm = per_sm / (cap + 1) + 16 > reserved ? per_sm / (cap + 1) + 16 - reserved : 0;
+  if (sm < floor_sm) sm = floor_sm;
+  if (cudaFuncSetAttribute(k_bconv_tc<TPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)) !=
+      cudaSuccess)
+    return -2;
+  int per = cap;
+  const int regs = fa.numRegs > 0 ? fa.numRegs : 64;
+  per = std::min(per, 65536 / (regs * 128));
+  per = std::min(per, static_cast<int>(per_sm / (sm + reserved)));
+  per = std::min(per, 16);
+  if (per < 1) return -2;
+  const int nits = d.npoly * (d.n / kRows) / TPI;
+  int grid = num_sms * per;
+  if (grid > nits) grid = nits;
+  k_bconv_tc<TPI><<<grid, 128, sm, s>>>(d);
+  return 0;
+}
+}  // namespace
 
 int launch_bconv_tc(const BConvTcDesc &d, int num_sms, cudaStream_t s) {
   if (d.npoly <= 0) return 0;
-  if (d.n % kRows != 0 || d.K < 1 || d.K > 16 || d.M < 1 || d.M > 64) return -1;
-  // CTAs per SM limited so that their TMEM columns fit in the SM's 512
-  const int cap = 512 / d.tmem_cols;
-  size_t sm = bconv_tc_smem(d.ksteps, d.nb);
-  const size_t per_sm = 233472;  // shared memory per SM (228 KiB)
-  const size_t floor_sm = per_sm / (cap + 1) - 1024 + 16;
-  if (sm < floor_sm) sm = floor_sm;
-  if (cudaFuncSetAttribute(k_bconv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)) !=
-      cudaSuccess)
-    return -2;
-  int per = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bconv_tc, 128, sm) != cudaSuccess || per < 1) return -2;
-  if (per > cap) per = cap;
-  const int ntiles = d.npoly * (d.n / kRows);
-  int grid = num_sms * per;
-  if (grid > ntiles) grid = ntiles;
-  k_bconv_tc<<<grid, 128, sm, s>>>(d);
-  return 0;
+  if (d.n % kRows != 0 || d.K < 1 || d.K > 16 || d.M < 1 || d.M > 64 || 2 * d.tpi * d.nb > d.tmem_cols ||
+      d.tmem_cols > 512)
+    return -1;
+  if ((d.n / kRows) % d.tpi != 0) return -1;
+  switch (d.tpi) {
+    case 1: return launch_tpi<1>(d, num_sms, s);
+    case 2: return launch_tpi<2>(d, num_sms, s);
+    case 4: return launch_tpi<4>(d, num_sms, s);
+    default: return -1;
+  }
 }
 
 }  // namespace chd

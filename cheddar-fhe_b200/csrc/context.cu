@@ -931,8 +931,12 @@ Status Context::bconv_many(int engine, int npoly, const int32_t *xt, int K, cons
   d.npoly = npoly;
   d.ksteps = (4 * K + 31) / 32;
   d.nb = std::max(16, (4 * M + 15) / 16 * 16);
+  // tiles per iteration: 4 while the two accumulator buffers leave room for
+  // two CTAs per SM in TMEM
+  d.tpi = 8 * d.nb <= 256 ? 4 : (4 * d.nb <= 256 ? 2 : 1);
+  while ((P->n / 128) % d.tpi != 0) d.tpi /= 2;
   d.tmem_cols = 32;
-  while (d.tmem_cols < d.nb) d.tmem_cols *= 2;
+  while (d.tmem_cols < 2 * d.tpi * d.nb) d.tmem_cols *= 2;
   // kind::i8: D s32 (bits 4-5 = 2), A s8 (bits 7-9 = 1), B u8 (bits 10-12 = 0),
   // both K-major, N >> 3 at bit 17, M >> 4 at bit 24
   d.idesc = (2u << 4) | (1u << 7) | (0u << 10) | (static_cast<uint32_t>(d.nb >> 3) << 17) | ((128u >> 4) << 24);

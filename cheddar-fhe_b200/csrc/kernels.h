@@ -87,12 +87,13 @@ struct BConvTcDesc {
   int K, M, n, npoly;
   int ksteps;      // ceil(4K / 32)
   int nb;          // 4M rounded up to a multiple of 16 (MMA N)
-  int tmem_cols;   // power of two >= max(32, nb)
+  int tpi;         // 128-row tiles per CTA iteration (1, 2 or 4), each with nb TMEM columns
+  int tmem_cols;   // power of two >= max(32, 2 * tpi * nb) (two accumulator buffers), <= 512
   uint32_t idesc;  // tcgen05 instruction descriptor (kind::i8, s8 x u8 -> s32, M = 128, N = nb)
   uint32_t p[64];
   int32_t pinv[64];
 };
-size_t bconv_tc_smem(int ksteps, int nb);
+size_t bconv_tc_smem(int tpi, int ksteps, int nb);
 int launch_bconv_tc(const BConvTcDesc &d, int num_sms, cudaStream_t s);
 
 // Fused ModSwitch column pass (N = 2^16 only): per 16-column tile
