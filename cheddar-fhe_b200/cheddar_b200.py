@@ -100,6 +100,9 @@ def lib():
         "chd_moddown_raw": (i, [vp, i, i, vp, vp, i]),
         "chd_bconv_raw": (i, [vp, vp, i32p, i, i32p, i, vp]),
         "chd_bconv_batch": (i, [vp, i, i, vp, i32p, i, i32p, i, vp]),
+        "chd_encode": (i, [vp, i, d, vp, vp, i, i, vp, C.POINTER(i)]),
+        "chd_encode_const": (i, [vp, i, d, d, i, vp]),
+        "chd_modup_to_max": (i, [vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -347,6 +350,32 @@ class Context:
         d = np.ascontiguousarray(dst_gidx, dtype=np.int32)
         _check(lib().chd_bconv_raw(self.ptr, _ptr(xt), s.ctypes.data, len(s), d.ctypes.data, len(d),
                                    _ptr(out)))
+
+    def encode(self, level, scale, msg, num_aux=0, out=None):
+        """Encoder::Encode: complex slots -> device plaintext (torch int32
+        [num_q(level) + num_aux][N], evaluation domain, Montgomery form)."""
+        import torch
+        msg = np.asarray(msg, dtype=np.complex128)
+        re = np.ascontiguousarray(msg.real)
+        im = np.ascontiguousarray(msg.imag)
+        if out is None:
+            out = torch.empty((self.num_q(level) + num_aux, self.n), dtype=torch.int32, device="cuda")
+        ns = C.c_int()
+        _check(lib().chd_encode(self.ptr, level, scale, re.ctypes.data, im.ctypes.data, len(msg), num_aux,
+                                _ptr(out), C.byref(ns)))
+        return out
+
+    def encode_const(self, level, scale, value, num_aux=0):
+        """Encoder::EncodeConstant: Montgomery residues per prime (host)."""
+        out = np.zeros(self.num_q(level) + num_aux, dtype=np.uint32)
+        _check(lib().chd_encode_const(self.ptr, level, scale, value, num_aux, out.ctypes.data))
+        return out
+
+    def ModUpToMax(self, a, res=None):
+        """BootContext::ModUpToMax (no sparse-secret encapsulation)."""
+        res = res if res is not None else Ciphertext(self)
+        _check(lib().chd_modup_to_max(self.ptr, res.ptr, a.ptr))
+        return res
 
     def bconv_batch(self, xt, src_gidx, dst_gidx, out, engine=BCONV_CUDA_CORE, npoly=1):
         """Batched BConv of npoly polynomials ([npoly][K][N] int32 centred ->

@@ -1,0 +1,221 @@
+// Host side of the bootstrapping path: the encoder (plaintexts and
+// constants for the linear transforms and EvalMod) and ModUpToMax.
+//
+// Encoder (src/core/Encode.cpp of the reference): slots -> special IFFT in
+// FP64 with the twiddle table e^(2 pi i k / 2N) -> value * scale truncated
+// toward zero to an integer (BigInt(double), include/core/BigInt.h:24) ->
+// residues -> NTT with Montgomery conversion on the device.  The FP64 steps
+// follow the reference's operation order exactly, so the residues are
+// bit-identical wherever the reference's host build evaluates the same
+// IEEE expressions (no fused multiply-add; this file is built with
+// -ffp-contract=off).
+#include <cmath>
+#include <complex>
+
+#include "host.h"
+#include "kernels.h"
+
+namespace chd {
+namespace {
+
+using cd = std::complex<double>;
+
+unsigned brev_bits(unsigned x, int bits) {
+  unsigned r = 0;
+  for (int i = 0; i < bits; i++) r |= ((x >> i) & 1u) << (bits - 1 - i);
+  return r;
+}
+
+// round-toward-zero integer of v, reduced to [0, p): exact for every finite
+// double (|v| >= 2^53 is already an integer m * 2^e)
+uint32_t trunc_mod(double v, uint32_t p) {
+  if (v == 0.0) return 0;
+  const bool neg = v < 0;
+  const double a = std::fabs(v);
+  uint64_t r;
+  if (a < 18446744073709551616.0) {
+    r = static_cast<uint64_t>(a) % p;
+  } else {
+    int e;
+    const double m = std::frexp(a, &e);  // a = m 2^e, m in [0.5, 1)
+    const uint64_t mi = static_cast<uint64_t>(std::ldexp(m, 53));
+    uint64_t pw = 1 % p, b = 2;
+    for (int sh = e - 53; sh; sh >>= 1) {
+      if (sh & 1) pw = pw * b % p;
+      b = b * b % p;
+    }
+    r = (mi % p) * pw % p;
+  }
+  if (neg && r) r = p - r;
+  return static_cast<uint32_t>(r);
+}
+
+}  // namespace
+
+const std::vector<std::complex<double>> &Context::enc_twiddles() {
+  if (enc_tw.empty()) {
+    const int M = 2 * P->n;
+    enc_tw.resize(M);
+    for (int i = 0; i < M; i++) enc_tw[i] = std::polar(1.0, 2.0 * M_PI * i / M);
+  }
+  return enc_tw;
+}
+
+void Context::special_ifft(std::vector<std::complex<double>> &d) {
+  // Encoder::SpecialIFFT, Encode.cpp:84-107
+  const auto &tw = enc_twiddles();
+  const int ns = static_cast<int>(d.size()), M = 2 * P->n;
+  for (int stride = ns / 2; stride >= 1; stride /= 2) {
+    const int sg = stride * 2, st8 = stride << 3, gap = M / st8;
+    for (int i = 0; i < ns; i += sg)
+      for (int j = 0; j < stride; j++) {
+        const int ti = (st8 - static_cast<int>(P->galois[j] % st8)) * gap;
+        cd x = d[i + j] + d[i + j + stride];
+        cd y = d[i + j] - d[i + j + stride];
+        y *= tw[ti];
+        d[i + j] = x;
+        d[i + j + stride] = y;
+      }
+  }
+  int lb = 0;
+  while ((1 << lb) < ns) lb++;
+  for (int i = 0; i < ns; i++) {
+    const int j = static_cast<int>(brev_bits(static_cast<unsigned>(i), lb));
+    if (i < j) std::swap(d[i], d[j]);
+  }
+  for (int i = 0; i < ns; i++) d[i] /= static_cast<double>(ns);
+}
+
+void Context::special_fft(std::vector<std::complex<double>> &d) {
+  // Encoder::SpecialFFT, Encode.cpp:109-133
+  const auto &tw = enc_twiddles();
+  const int ns = static_cast<int>(d.size()), M = 2 * P->n;
+  int lb = 0;
+  while ((1 << lb) < ns) lb++;
+  for (int i = 0; i < ns; i++) {
+    const int j = static_cast<int>(brev_bits(static_cast<unsigned>(i), lb));
+    if (i < j) std::swap(d[i], d[j]);
+  }
+  for (int stride = 1; stride < ns; stride *= 2) {
+    const int sg = stride * 2, st8 = stride << 3, gap = M / st8;
+    for (int i = 0; i < ns; i += sg)
+      for (int j = 0; j < stride; j++) {
+        const int ti = static_cast<int>(P->galois[j] % st8) * gap;
+        cd x = d[i + j];
+        cd y = d[i + j + stride];
+        y *= tw[ti];
+        d[i + j] = x + y;
+        d[i + j + stride] = x - y;
+      }
+  }
+}
+
+Status Context::encode(int level, double scale, const std::complex<double> *msg, int msg_len, int num_aux,
+                       uint32_t *pt_dev, int *num_slots_out) {
+  // Encoder::Encode / EncodeWorker / ComplexVectorToPlaintext,
+  // Encode.cpp:23-41, 135-190
+  CHD_CHECK(msg_len >= 1 && msg_len <= P->n / 2, kErrInvalidArg, "Encode: 1 <= message length <= N/2");
+  CHD_CHECK(num_aux >= 0 && num_aux <= P->alpha, kErrInvalidArg, "Encode: invalid number of aux primes");
+  CHD_CHECK(level >= -1 && level <= P->max_level, kErrInvalidLevel, "Encode: invalid level");
+  int ns = 1;
+  while (ns < msg_len) ns *= 2;
+  std::vector<cd> d(ns, cd(0.0, 0.0));
+  for (int i = 0; i < msg_len; i++) d[i] = msg[i];
+  special_ifft(d);
+  const NP np = P->level_np(level, num_aux);
+  const int tot = np.total(), n = P->n, half = n / 2, gap = half / ns;
+  std::vector<int> g(tot);
+  P->gidx(np, g.data());
+  std::vector<uint32_t> mx(static_cast<size_t>(tot) * n, 0);
+  for (int i = 0; i < ns; i++) {
+    const cd v = d[i] * scale;
+    const double re = v.real(), im = v.imag();
+    for (int k = 0; k < tot; k++) {
+      const uint32_t p = P->primes[g[k]];
+      mx[static_cast<size_t>(k) * n + i * gap] = trunc_mod(re, p);
+      mx[static_cast<size_t>(k) * n + i * gap + half] = trunc_mod(im, p);
+    }
+  }
+  cudaMemcpyAsync(pt_dev, mx.data(), mx.size() * 4, cudaMemcpyHostToDevice, stream);
+  if (num_slots_out) *num_slots_out = ns;
+  // NTT(..., true): to the evaluation domain, Montgomery form
+  CHD_TRY(ntt(np, pt_dev, true));
+  // the host buffer must outlive the copy
+  return cudaStreamSynchronize(stream) == cudaSuccess ? kOk : check_cuda("encode");
+}
+
+void Context::encode_const(int level, double scale, double value, int num_aux, std::vector<uint32_t> *cx) const {
+  // Encoder::EncodeConstant, Encode.cpp:250-275
+  const NP np = P->level_np(level, num_aux);
+  const int tot = np.total();
+  std::vector<int> g(tot);
+  P->gidx(np, g.data());
+  cx->resize(tot);
+  const double v = value * scale;
+  for (int k = 0; k < tot; k++) {
+    const uint32_t p = P->primes[g[k]];
+    (*cx)[k] = prime::to_mont(trunc_mod(v, p), p);
+  }
+}
+
+Status Context::modup_to_max(DeviceCt &res, const DeviceCt &a) {
+  // BootContext::ModUpToMax without sparse-secret encapsulation
+  // (BootContext.cpp:186-270): per part, INTTAndMultConst with
+  // (prod_{j != i} q_j * N)^-1 (BootContext.cpp:93-107), the CRT lift
+  // (ElementWise.cu:575-623, 1646-1670), NTT to the top level.
+  const NP np = P->level_np(-1);
+  CHD_CHECK(a.np == np, kErrShape, "ModUpToMax: input must be at level -1 without aux primes");
+  CHD_CHECK(!a.has_rx, kErrShape, "ModUpToMax: input has Rx");
+  const int nb = np.q();
+  CHD_CHECK(nb == 1 || nb == 2, kErrUnsupported, "ModUpToMax: level -1 must have one or two primes");
+  const int n = P->n;
+  int g[2];
+  P->gidx(np, g);
+  ArenaScope scope(arena);
+  uint32_t *t = static_cast<uint32_t *>(arena.alloc(static_cast<size_t>(2) * nb * n * 4));
+  CHD_CHECK(t, kErrAlloc, "ModUpToMax: scratch allocation failed");
+  RowBatch rb;
+  rb.count = 0;
+  for (int part = 0; part < 2; part++)
+    for (int i = 0; i < nb; i++) {
+      const uint32_t q = P->primes[g[i]];
+      uint32_t c = static_cast<uint32_t>(n % q);
+      for (int j = 0; j < nb; j++)
+        if (j != i) c = prime::mul_mod(c, P->primes[g[j]], q);
+      c = prime::inv_mod(c, q);  // plain, applied like a Montgomery constant
+      RowDesc &d = rb.rows[rb.count++];
+      d = RowDesc{};
+      d.src = (part == 0 ? a.bx : a.ax) + static_cast<size_t>(i) * n;
+      d.dst = t + (static_cast<size_t>(part) * nb + i) * n;
+      d.tw = itw(g[i]);
+      d.q = q;
+      mont_as_shoup(c, g[i], &d.c0, &d.c0s);
+    }
+  launch_ntt_inv(rb, P->log_n, stream);
+  const NP maxnp = P->level_np(P->max_level);
+  const double scale = a.scale;
+  const int slots = a.num_slots;
+  CHD_TRY(res.reserve(maxnp, false, n));
+  ModUpToMaxDesc d{};
+  d.src[0] = t;
+  d.src[1] = t + static_cast<size_t>(nb) * n;
+  d.dst[0] = res.bx;
+  d.dst[1] = res.ax;
+  std::vector<int> gm(maxnp.total());
+  P->gidx(maxnp, gm.data());
+  for (int r = 0; r < maxnp.total(); r++) d.p[r] = P->primes[gm[r]];
+  d.q0 = P->primes[g[0]];
+  d.q1 = nb == 2 ? P->primes[g[1]] : 0;
+  d.nbase = nb;
+  d.rows = maxnp.total();
+  d.parts = 2;
+  d.n = n;
+  launch_modup_to_max(d, stream);
+  CHD_TRY(ntt(maxnp, res.bx, true));
+  CHD_TRY(ntt(maxnp, res.ax, true));
+  res.scale = scale;
+  res.num_slots = slots;
+  return check_cuda("ModUpToMax");
+}
+
+}  // namespace chd

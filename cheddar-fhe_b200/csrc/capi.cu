@@ -1,6 +1,8 @@
 // C ABI over the host evaluator (include/cheddar_b200.h).
 #include <cstring>
 
+#include <complex>
+
 #include "../../include/cheddar_b200.h"
 #include "host.h"
 
@@ -336,6 +338,37 @@ int chd_rescale(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) 
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   return ctx->c->rescale(res->ct, a->ct);
+}
+
+int chd_encode(chd_context *ctx, int level, double scale, const double *re, const double *im, int msg_len,
+               int num_aux, uint32_t *pt_dev, int *num_slots) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(re);
+  CHD_NOTNULL(im);
+  CHD_NOTNULL(pt_dev);
+  if (msg_len < 1) return fail(CHD_ERR_INVALID_ARG, "chd_encode: empty message");
+  std::vector<std::complex<double>> msg(msg_len);
+  for (int i = 0; i < msg_len; i++) msg[i] = std::complex<double>(re[i], im[i]);
+  return ctx->c->encode(level, scale, msg.data(), msg_len, num_aux, pt_dev, num_slots);
+}
+
+int chd_encode_const(chd_context *ctx, int level, double scale, double value, int num_aux, uint32_t *cx) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(cx);
+  const Params &P = *ctx->c->P;
+  if (level < -1 || level > P.max_level) return fail(CHD_ERR_INVALID_LEVEL, "chd_encode_const: invalid level");
+  if (num_aux < 0 || num_aux > P.alpha) return fail(CHD_ERR_INVALID_ARG, "chd_encode_const: invalid aux count");
+  std::vector<uint32_t> v;
+  ctx->c->encode_const(level, scale, value, num_aux, &v);
+  std::copy(v.begin(), v.end(), cx);
+  return CHD_OK;
+}
+
+int chd_modup_to_max(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  return ctx->c->modup_to_max(res->ct, a->ct);
 }
 
 int chd_relinearize(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *key) {

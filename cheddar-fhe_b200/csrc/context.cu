@@ -21,19 +21,6 @@ thread_local std::string g_error;
 void set_error(const std::string &msg) { g_error = msg; }
 const char *last_error() { return g_error.c_str(); }
 
-#define CHD_CHECK(cond, code, msg) \
-  do {                             \
-    if (!(cond)) {                 \
-      set_error(msg);              \
-      return code;                 \
-    }                              \
-  } while (0)
-#define CHD_TRY(expr)            \
-  do {                           \
-    Status _s = (expr);          \
-    if (_s != kOk) return _s;    \
-  } while (0)
-
 // ---------------------------------------------------------- prime utilities
 namespace prime {
 uint32_t mul_mod(uint32_t a, uint32_t b, uint32_t q) {
@@ -525,12 +512,6 @@ void *Arena::alloc(size_t bytes) {
 
 void Arena::release(size_t m) { top_ = m; }
 
-struct ArenaScope {
-  Arena &a;
-  size_t m;
-  explicit ArenaScope(Arena &x) : a(x), m(x.mark()) {}
-  ~ArenaScope() { a.release(m); }
-};
 
 // -------------------------------------------------------------- Context
 std::unique_ptr<Context> Context::create(const ParamSpec &spec, int device, std::string *err) {

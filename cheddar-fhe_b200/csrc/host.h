@@ -10,6 +10,7 @@
 #include <memory>
 #include <string>
 #include <utility>
+#include <complex>
 #include <vector>
 
 #include "kernels.h"
@@ -152,6 +153,28 @@ class Arena {
   size_t total_ = 0;
 };
 
+// Error helpers of the host code: record the message, return the status.
+#define CHD_CHECK(cond, code, msg) \
+  do {                             \
+    if (!(cond)) {                 \
+      set_error(msg);              \
+      return code;                 \
+    }                              \
+  } while (0)
+#define CHD_TRY(expr)            \
+  do {                           \
+    Status _s = (expr);          \
+    if (_s != kOk) return _s;    \
+  } while (0)
+
+// Releases everything allocated from the arena inside a scope.
+struct ArenaScope {
+  Arena &a;
+  size_t m;
+  explicit ArenaScope(Arena &x) : a(x), m(x.mark()) {}
+  ~ArenaScope() { a.release(m); }
+};
+
 class Context {
  public:
   static std::unique_ptr<Context> create(const ParamSpec &spec, int device, std::string *err);
@@ -172,6 +195,8 @@ class Context {
   std::vector<uint32_t> n_inv, n_inv_mont, mont_conv, p_prod, imag_unit;
   std::vector<uint32_t> r_inv;  // 2^-32 mod q per global prime
   std::vector<LevelMS> ms;  // index level + 1
+  std::vector<std::complex<double>> enc_tw;  // e^(2 pi i k / 2N), built on first use
+  const std::vector<std::complex<double>> &enc_twiddles();
 
   const LevelMS &lms(int level) const { return ms.at(level + 1); }
   const uint2 *tw(int g) const { return d_tw + (static_cast<size_t>(g) << P->log_n); }
@@ -241,6 +266,20 @@ class Context {
                         DeviceCt *const *out);
   // ModDown of a Q u P ciphertext back to Q
   Status moddown_ct(DeviceCt &res, const DeviceCt &a);
+
+  // ---- bootstrapping building blocks (boot.cu) ----
+  // Encoder::Encode (Encode.cpp:23-41, 84-107, 135-190): msg_len complex
+  // slots (padded to a power of two) -> plaintext [level_np(level, num_aux)]
+  // in the NTT Montgomery domain at pt_dev; waits for the upload.
+  Status encode(int level, double scale, const std::complex<double> *msg, int msg_len, int num_aux,
+                uint32_t *pt_dev, int *num_slots_out);
+  // Encoder::EncodeConstant (Encode.cpp:250-275): Montgomery residues
+  void encode_const(int level, double scale, double value, int num_aux, std::vector<uint32_t> *cx) const;
+  void special_ifft(std::vector<std::complex<double>> &d);
+  void special_fft(std::vector<std::complex<double>> &d);
+  // BootContext::ModUpToMax without sparse-secret encapsulation
+  // (BootContext.cpp:186-270): level -1 -> top level
+  Status modup_to_max(DeviceCt &res, const DeviceCt &a);
 
   // ---- optional device timing of the fused key-switch stages ----
   // Events recorded on the context stream around each stage's launches.

@@ -96,6 +96,50 @@ struct BConvTcDesc {
 size_t bconv_tc_smem(int tpi, int ksteps, int nb);
 int launch_bconv_tc(const BConvTcDesc &d, int num_sms, cudaStream_t s);
 
+// ---- bootstrapping kernels (boot_kernels.cu) ----
+// Lift of a level -1 polynomial (coefficient domain, nbase = 1 or 2 base
+// limbs per part) to the rows primes p[] (kernel::ModUpToMax1/2).
+struct ModUpToMaxDesc {
+  const uint32_t *src[2];  // per part: [nbase][n]
+  uint32_t *dst[2];        // per part: [rows][n]
+  uint32_t p[64];
+  uint32_t q0, q1;
+  int nbase, rows, parts, n;
+};
+void launch_modup_to_max(const ModUpToMaxDesc &d, cudaStream_t s);
+
+// out[o].(b, a)[r] = sum_t pt[o][t][r] (.) in_(b, a)[term[o][t]][r]
+constexpr int kMaxPtAccumIn = 64;
+constexpr int kMaxPtAccumTerms = 32;
+constexpr int kMaxPtAccumOuts = 16;
+struct PtAccumOut {
+  uint32_t *b, *a;
+  int terms;
+  int16_t term[kMaxPtAccumTerms];
+  const uint32_t *pt[kMaxPtAccumTerms];
+};
+struct PtAccumDesc {
+  const uint32_t *in_b[kMaxPtAccumIn], *in_a[kMaxPtAccumIn];
+  uint32_t q[64];
+  int32_t qinv[64];
+  int rows, outs, n;
+  PtAccumOut out[kMaxPtAccumOuts];
+};
+void launch_pt_accum(const PtAccumDesc &d, cudaStream_t s);
+
+// dst[part][r] = sum_t c[t][r] * src[t][part][src_row0[t] + r]
+constexpr int kMaxConstAccumTerms = 16;
+struct ConstAccumDesc {
+  const uint32_t *src[kMaxConstAccumTerms][3];
+  int src_row0[kMaxConstAccumTerms];
+  uint32_t c[kMaxConstAccumTerms][64];
+  uint32_t *dst[3];
+  uint32_t q[64];
+  int32_t qinv[64];
+  int terms, rows, parts, n;
+};
+void launch_const_accum(const ConstAccumDesc &d, cudaStream_t s);
+
 // Fused ModSwitch column pass (N = 2^16 only): per 16-column tile
 //   x~_k  = centre(INTT column phase(src_k) * c0_k)        (K <= 16 sources)
 //   y_m   = (sum_k x~_k T[m][k]) * 2^-32 mod p_m           (exact BConv)

@@ -171,6 +171,22 @@ int chd_moddown_raw(chd_context *ctx, int level, int type, const uint32_t *src_d
 int chd_bconv_raw(chd_context *ctx, const int32_t *xt_dev, const int *src_gidx, int K,
                   const int *dst_gidx, int M, uint32_t *out_dev);
 
+/* ---- bootstrapping building blocks ---- */
+/* Encoder::Encode (src/core/Encode.cpp:23-41, 84-107, 135-190): msg_len
+ * complex slots (re, im; padded to a power of two, written to *num_slots)
+ * at `scale` -> plaintext [num_q(level) + num_aux][N] at pt_dev, evaluation
+ * domain, Montgomery form (prime order: terminal reversed, main, aux).
+ * FP64 special IFFT on the host, truncation toward zero, device NTT;
+ * returns after the upload. */
+int chd_encode(chd_context *ctx, int level, double scale, const double *re, const double *im, int msg_len,
+               int num_aux, uint32_t *pt_dev, int *num_slots);
+/* Encoder::EncodeConstant (Encode.cpp:250-275): cx[num_q(level) + num_aux]
+ * Montgomery residues of trunc(value * scale), host memory. */
+int chd_encode_const(chd_context *ctx, int level, double scale, double value, int num_aux, uint32_t *cx);
+/* BootContext::ModUpToMax (src/extension/BootContext.cpp:186-270) without
+ * sparse-secret encapsulation: a at level -1 -> res at the top level. */
+int chd_modup_to_max(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a);
+
 /* Batched kernel::ModSwitchMatrixMult: npoly polynomials, each K centred
  * source limbs [K][N] (xt_dev + i*K*N) -> M limbs [M][N] (out_dev + i*M*N),
  * same table and result as chd_bconv_raw.  engine CHD_BCONV_CUDA_CORE runs

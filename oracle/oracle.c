@@ -1455,6 +1455,59 @@ int orc_decrypt(const orc_ctx *c, const uint32_t *s, int level,
   return 0;
 }
 
+
+/* ========================================================================
+ * ModUpToMax without sparse-secret encapsulation — BootContext.cpp:186-270
+ * (INTTAndMultConst with mod_max_intt_const_, BootContext.cpp:93-107;
+ * ModUpToMax1/2, ElementWise.cu:575-623; NTT(..., true) at the top level)
+ * ====================================================================== */
+int orc_modup_to_max(const orc_ctx *c, const uint32_t *bx, const uint32_t *ax,
+                     uint32_t *res_bx, uint32_t *res_ax) {
+  np_t b = level_np(c, -1, 0), mx = level_np(c, c->max_level, 0);
+  int nb = np_q(b), N = c->n, tot = np_total(mx);
+  if (nb < 1 || nb > 2) return -1;
+  int gb[2], gm[256];
+  np_gidx(c, b, gb);
+  np_gidx(c, mx, gm);
+  const uint32_t *src[2] = {bx, ax};
+  uint32_t *dst[2] = {res_bx, res_ax};
+  int32_t *t = malloc(sizeof(int32_t) * (size_t)nb * N);
+  for (int part = 0; part < 2; part++) {
+    for (int i = 0; i < nb; i++) {
+      uint32_t q = c->primes[gb[i]];
+      uint32_t k = (uint32_t)(N % q);
+      for (int j = 0; j < nb; j++)
+        if (j != i) k = mul_mod(k, c->primes[gb[j]], q);
+      k = orc_inv_mod(k, q);
+      int32_t *a = t + (size_t)i * N;
+      memcpy(a, src[part] + (size_t)i * N, sizeof(int32_t) * N);
+      intt_core(c, gb[i], a);
+      for (int j = 0; j < N; j++) a[j] = ep_mult(a[j], k, q, c->qinv[gb[i]]);
+    }
+#pragma omp parallel for schedule(static)
+    for (int r = 0; r < tot; r++) {
+      int64_t p = c->primes[gm[r]];
+      uint32_t *o = dst[part] + (size_t)r * N;
+      for (int j = 0; j < N; j++) {
+        if (nb == 1) {
+          o[j] = (uint32_t)((uint32_t)t[j] % (uint32_t)p);
+        } else {
+          int64_t q0 = c->primes[gb[0]], q1 = c->primes[gb[1]], qp = q0 * q1;
+          int64_t v = (int64_t)(uint32_t)t[j] * q1 + (int64_t)(uint32_t)t[N + j] * q0;
+          if (v >= qp) v -= qp;
+          if (v > (qp >> 1)) v -= qp;
+          int64_t m = v % p;
+          if (m < 0) m += p;
+          o[j] = (uint32_t)m;
+        }
+      }
+      orc_ntt_limb(c, gm[r], o, 1);
+    }
+  }
+  free(t);
+  return 0;
+}
+
 /* ---- encoding — Encode.cpp:10-21, 84-133, 135-190, 250-275 ---- */
 typedef struct {
   double re, im;

@@ -190,6 +190,10 @@ int orc_encode(const orc_ctx *c, int level, double scale, const double *re,
                const double *im, int num_slots, int num_aux, uint32_t *pt);
 int orc_decode(const orc_ctx *c, int level, double scale, const uint32_t *pt,
                int num_slots, double *re, double *im);
+/* BootContext::ModUpToMax without sparse-secret encapsulation: level -1
+ * (bx, ax) -> top level (res_bx, res_ax) */
+int orc_modup_to_max(const orc_ctx *c, const uint32_t *bx, const uint32_t *ax,
+                     uint32_t *res_bx, uint32_t *res_ax);
 /* EncodeConstant: one Montgomery word per prime */
 int orc_encode_const(const orc_ctx *c, int level, double scale, double value,
                      int num_aux, uint32_t *cx);

@@ -83,6 +83,7 @@ def lib():
             "orc_encode": (C.c_int, [vp, C.c_int, C.c_double, f64p, f64p, C.c_int, C.c_int, u32p]),
             "orc_decode": (C.c_int, [vp, C.c_int, C.c_double, u32p, C.c_int, f64p, f64p]),
             "orc_encode_const": (C.c_int, [vp, C.c_int, C.c_double, C.c_double, C.c_int, u32p]),
+            "orc_modup_to_max": (C.c_int, [vp, u32p, u32p, u32p, u32p]),
             "orc_uniform": (C.c_int, [vp, C.c_uint64, C.c_int, C.c_int, C.c_int, u32p]),
             "orc_mont_reduce_lazy": (C.c_int32, [C.c_int64, C.c_uint32, C.c_int32]),
             "orc_mont_mult_lazy": (C.c_int32, [C.c_int32, C.c_int32, C.c_uint32, C.c_int32]),
@@ -394,6 +395,16 @@ class Oracle:
         out = np.zeros(self.num_q(level) + num_aux, dtype=np.uint32)
         lib().orc_encode_const(self.ptr, level, scale, value, num_aux, out)
         return out
+
+    def modup_to_max(self, bx, ax):
+        """BootContext::ModUpToMax without sparse-secret encapsulation
+        (BootContext.cpp:186-270): level -1 (bx, ax) -> top level."""
+        nq = self.num_q(self.max_level)
+        rb = np.zeros((nq, self.n), dtype=np.uint32)
+        ra = np.zeros((nq, self.n), dtype=np.uint32)
+        _check(lib().orc_modup_to_max(self.ptr, np.ascontiguousarray(bx, dtype=np.uint32),
+                                      np.ascontiguousarray(ax, dtype=np.uint32), rb, ra), "modup_to_max")
+        return rb, ra
 
     def uniform(self, seed, level, num_aux=0):
         m, t = self.level_np(level)
