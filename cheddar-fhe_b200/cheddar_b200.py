@@ -103,6 +103,17 @@ def lib():
         "chd_encode": (i, [vp, i, d, vp, vp, i, i, vp, C.POINTER(i)]),
         "chd_encode_const": (i, [vp, i, d, d, i, vp]),
         "chd_modup_to_max": (i, [vp, vp, vp]),
+        "chd_evk_map_create": (i, [vp, pp]),
+        "chd_evk_map_destroy": (None, [vp]),
+        "chd_evk_map_set_rotation": (i, [vp, i, vp]),
+        "chd_evk_map_set_conjugation": (i, [vp, vp]),
+        "chd_evk_map_set_mult": (i, [vp, vp]),
+        "chd_lintrans_create": (i, [vp, i, i, vp, vp, vp, i, d, i, i, i, i, pp]),
+        "chd_lintrans_destroy": (None, [vp]),
+        "chd_lintrans_rotations": (i, [vp, vp, i, C.POINTER(i)]),
+        "chd_lintrans_num_pts": (i, [vp, C.POINTER(i)]),
+        "chd_lintrans_pt": (i, [vp, i, C.POINTER(i), C.POINTER(i), vp, vp]),
+        "chd_lintrans_evaluate": (i, [vp, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -386,6 +397,89 @@ class Context:
         d = np.ascontiguousarray(dst_gidx, dtype=np.int32)
         _check(lib().chd_bconv_batch(self.ptr, engine, npoly, _ptr(xt), s.ctypes.data, len(s), d.ctypes.data,
                                      len(d), _ptr(out)))
+
+
+class EvkMap:
+    """EvkMap (include/core/EvkMap.h): keys by rotation index plus the
+    conjugation and multiplication keys; holds references to the keys."""
+
+    def __init__(self, ctx):
+        self.ctx = ctx
+        self.ptr = C.c_void_p()
+        self._keep = []
+        _check(lib().chd_evk_map_create(ctx.ptr, C.byref(self.ptr)))
+
+    def __del__(self):
+        try:
+            if self.ptr.value:
+                lib().chd_evk_map_destroy(self.ptr)
+                self.ptr = C.c_void_p()
+        except Exception:
+            pass
+
+    def set_rotation(self, r, key):
+        self._keep.append(key)
+        _check(lib().chd_evk_map_set_rotation(self.ptr, r, key.ptr))
+
+    def set_conjugation(self, key):
+        self._keep.append(key)
+        _check(lib().chd_evk_map_set_conjugation(self.ptr, key.ptr))
+
+    def set_mult(self, key):
+        self._keep.append(key)
+        _check(lib().chd_evk_map_set_mult(self.ptr, key.ptr))
+
+
+class LinearTransform:
+    """LinearTransform + HoistHandler (src/extension/LinearTransform.cpp,
+    Hoist.cu): diagonals {index: complex[width]} encoded at pt_level."""
+
+    def __init__(self, ctx, diags, pt_level, pt_scale, bs, gs=1, pre_rotation=0, additional_pt_rot=0):
+        self.ctx = ctx
+        idx = sorted(diags)
+        width = len(diags[idx[0]])
+        vals = np.stack([np.asarray(diags[i], dtype=np.complex128) for i in idx])
+        re = np.ascontiguousarray(vals.real)
+        im = np.ascontiguousarray(vals.imag)
+        ia = np.ascontiguousarray(idx, dtype=np.int32)
+        self.width = width
+        self.ptr = C.c_void_p()
+        _check(lib().chd_lintrans_create(ctx.ptr, width, len(idx), ia.ctypes.data, re.ctypes.data, im.ctypes.data,
+                                         pt_level, pt_scale, bs, gs, pre_rotation, additional_pt_rot,
+                                         C.byref(self.ptr)))
+
+    def __del__(self):
+        try:
+            if self.ptr.value:
+                lib().chd_lintrans_destroy(self.ptr)
+                self.ptr = C.c_void_p()
+        except Exception:
+            pass
+
+    def rotations(self):
+        cnt = C.c_int()
+        _check(lib().chd_lintrans_rotations(self.ptr, None, 0, C.byref(cnt)))
+        out = (C.c_int * max(1, cnt.value))()
+        _check(lib().chd_lintrans_rotations(self.ptr, out, cnt.value, C.byref(cnt)))
+        return [out[i] for i in range(cnt.value)]
+
+    def plaintexts(self):
+        """[(giant step, baby step, message)] as compiled (after the swap)."""
+        cnt = C.c_int()
+        _check(lib().chd_lintrans_num_pts(self.ptr, C.byref(cnt)))
+        res = []
+        for i in range(cnt.value):
+            g, b = C.c_int(), C.c_int()
+            re = np.zeros(self.width)
+            im = np.zeros(self.width)
+            _check(lib().chd_lintrans_pt(self.ptr, i, C.byref(g), C.byref(b), re.ctypes.data, im.ctypes.data))
+            res.append((g.value, b.value, re + 1j * im))
+        return res
+
+    def evaluate(self, ct, keys, res=None):
+        res = res if res is not None else Ciphertext(self.ctx)
+        _check(lib().chd_lintrans_evaluate(self.ctx.ptr, self.ptr, res.ptr, ct.ptr, keys.ptr))
+        return res
 
 
 class Ciphertext:

@@ -1,6 +1,7 @@
 // C ABI over the host evaluator (include/cheddar_b200.h).
 #include <cstring>
 
+#include <algorithm>
 #include <complex>
 
 #include "../../include/cheddar_b200.h"
@@ -16,6 +17,13 @@ struct chd_ciphertext {
 };
 struct chd_evk {
   DeviceEvk k;
+};
+struct chd_evk_map {
+  RotKeys rot;
+  const DeviceEvk *conj = nullptr, *mult = nullptr;
+};
+struct chd_lintrans {
+  LTPlan plan;
 };
 
 namespace {
@@ -369,6 +377,128 @@ int chd_modup_to_max(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   return ctx->c->modup_to_max(res->ct, a->ct);
+}
+
+int chd_evk_map_create(chd_context *ctx, chd_evk_map **out) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(out);
+  *out = new chd_evk_map();
+  return CHD_OK;
+}
+
+void chd_evk_map_destroy(chd_evk_map *m) { delete m; }
+
+int chd_evk_map_set_rotation(chd_evk_map *m, int rot_idx, const chd_evk *key) {
+  CHD_NOTNULL(m);
+  CHD_NOTNULL(key);
+  if (rot_idx <= 0) return fail(CHD_ERR_INVALID_ARG, "chd_evk_map_set_rotation: rotation index must be positive");
+  m->rot[rot_idx] = &key->k;
+  return CHD_OK;
+}
+
+int chd_evk_map_set_conjugation(chd_evk_map *m, const chd_evk *key) {
+  CHD_NOTNULL(m);
+  CHD_NOTNULL(key);
+  m->conj = &key->k;
+  return CHD_OK;
+}
+
+int chd_evk_map_set_mult(chd_evk_map *m, const chd_evk *key) {
+  CHD_NOTNULL(m);
+  CHD_NOTNULL(key);
+  m->mult = &key->k;
+  return CHD_OK;
+}
+
+int chd_lintrans_create(chd_context *ctx, int width, int n_diag, const int *diag_idx, const double *re,
+                        const double *im, int pt_level, double pt_scale, int bs, int gs, int pre_rotation,
+                        int additional_pt_rot, chd_lintrans **out) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(diag_idx);
+  CHD_NOTNULL(re);
+  CHD_NOTNULL(im);
+  CHD_NOTNULL(out);
+  if (width <= 0 || n_diag <= 0 || bs <= 0 || gs <= 0) return fail(CHD_ERR_INVALID_ARG, "chd_lintrans_create: bad shape");
+  SMat m;
+  m.h = m.w = width;
+  for (int i = 0; i < n_diag; i++) {
+    if (diag_idx[i] < 0 || diag_idx[i] >= width) return fail(CHD_ERR_INVALID_ARG, "chd_lintrans_create: bad diagonal");
+    std::vector<std::complex<double>> v(width);
+    for (int k = 0; k < width; k++)
+      v[k] = std::complex<double>(re[static_cast<size_t>(i) * width + k], im[static_cast<size_t>(i) * width + k]);
+    m.d[diag_idx[i]] = std::move(v);
+  }
+  auto *lt = new chd_lintrans();
+  int rc = ctx->c->lt_build(m, pt_level, pt_scale, bs, gs, pre_rotation, additional_pt_rot, false, &lt->plan);
+  if (rc != CHD_OK) {
+    delete lt;
+    return rc;
+  }
+  *out = lt;
+  return CHD_OK;
+}
+
+void chd_lintrans_destroy(chd_lintrans *lt) { delete lt; }
+
+int chd_lintrans_rotations(const chd_lintrans *lt, int *out, int cap, int *count) {
+  CHD_NOTNULL(lt);
+  CHD_NOTNULL(count);
+  std::vector<int> r;
+  for (int b : lt->plan.bs_idx)
+    if (b) r.push_back(b);
+  for (int g : lt->plan.gs_idx)
+    if (g) r.push_back(g);
+  std::sort(r.begin(), r.end());
+  r.erase(std::unique(r.begin(), r.end()), r.end());
+  *count = static_cast<int>(r.size());
+  if (out)
+    for (int i = 0; i < std::min(cap, *count); i++) out[i] = r[i];
+  return CHD_OK;
+}
+
+int chd_lintrans_num_pts(const chd_lintrans *lt, int *count) {
+  CHD_NOTNULL(lt);
+  CHD_NOTNULL(count);
+  *count = static_cast<int>(lt->plan.pts.size());
+  return CHD_OK;
+}
+
+int chd_lintrans_pt(const chd_lintrans *lt, int i, int *gs, int *bs, double *re, double *im) {
+  CHD_NOTNULL(lt);
+  if (i < 0 || i >= static_cast<int>(lt->plan.pts.size())) return fail(CHD_ERR_INVALID_ARG, "chd_lintrans_pt: index");
+  const LTPlan::Pt &p = lt->plan.pts[i];
+  if (gs) *gs = p.gs;
+  if (bs) *bs = p.bs;
+  for (size_t k = 0; k < p.msg.size(); k++) {
+    if (re) re[k] = p.msg[k].real();
+    if (im) im[k] = p.msg[k].imag();
+  }
+  return CHD_OK;
+}
+
+int chd_lintrans_evaluate(chd_context *ctx, const chd_lintrans *lt, chd_ciphertext *res, const chd_ciphertext *in,
+                          const chd_evk_map *keys) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(lt);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(in);
+  CHD_NOTNULL(keys);
+  if (res == in) {
+    DeviceCt tmp;
+    int rc = ctx->c->lt_evaluate(tmp, in->ct, lt->plan, keys->rot);
+    if (rc != CHD_OK) return rc;
+    std::swap(res->ct.bx, tmp.bx);
+    std::swap(res->ct.ax, tmp.ax);
+    std::swap(res->ct.rx, tmp.rx);
+    std::swap(res->ct.cap_words, tmp.cap_words);
+    std::swap(res->ct.owned, tmp.owned);
+    res->ct.np = tmp.np;
+    res->ct.has_rx = tmp.has_rx;
+    res->ct.scale = tmp.scale;
+    res->ct.num_slots = tmp.num_slots;
+    return CHD_OK;
+  }
+  return ctx->c->lt_evaluate(res->ct, in->ct, lt->plan, keys->rot);
 }
 
 int chd_relinearize(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *key) {

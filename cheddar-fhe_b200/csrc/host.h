@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <map>
 #include <memory>
 #include <string>
 #include <utility>
@@ -167,6 +168,38 @@ class Arena {
     if (_s != kOk) return _s;    \
   } while (0)
 
+// Square complex matrix stored by diagonals: d[i][k] = M[k][(k + i) mod w]
+// (StripedMatrix, include/extension/StripedMatrix.h).
+struct SMat {
+  int h = 0, w = 0;
+  std::map<int, std::vector<std::complex<double>>> d;
+};
+SMat smat_mult(const SMat &a, const SMat &b);
+SMat smat_scale(const SMat &a, std::complex<double> b);
+
+// A compiled linear transform (LinearTransform + HoistHandler): encoded
+// diagonals keyed by (giant step, baby step), device plaintexts over the
+// Q u P basis of pt_level.
+struct LTPlan {
+  struct Pt {
+    int gs = 0, bs = 0;
+    std::vector<std::complex<double>> msg;
+    uint32_t *dev = nullptr;
+  };
+  int pt_level = 0, width = 0, pt_slots = 0;
+  double pt_scale = 0;
+  std::vector<int> bs_idx, gs_idx;  // sorted
+  std::vector<Pt> pts;              // giant step major, baby step minor
+  LTPlan() = default;
+  LTPlan(const LTPlan &) = delete;
+  LTPlan &operator=(const LTPlan &) = delete;
+  LTPlan(LTPlan &&) = default;
+  LTPlan &operator=(LTPlan &&) = default;
+  ~LTPlan();
+};
+struct DeviceEvk;
+using RotKeys = std::map<int, const DeviceEvk *>;
+
 // Releases everything allocated from the arena inside a scope.
 struct ArenaScope {
   Arena &a;
@@ -280,6 +313,13 @@ class Context {
   // BootContext::ModUpToMax without sparse-secret encapsulation
   // (BootContext.cpp:186-270): level -1 -> top level
   Status modup_to_max(DeviceCt &res, const DeviceCt &a);
+
+  // Linear transform planning and evaluation (lintrans.cu): LinearTransform
+  // ctor + HoistHandler ctor (LinearTransform.cpp:8-75, Hoist.cu:120-167)
+  Status lt_build(const SMat &m, int pt_level, double pt_scale, int bs, int gs, int pre_rotation,
+                  int additional_pt_rot, bool suppress_swap, LTPlan *out);
+  // HoistHandler::Evaluate (Hoist.cu:554-975): res at pt_level - 1
+  Status lt_evaluate(DeviceCt &res, const DeviceCt &in, const LTPlan &pl, const RotKeys &keys);
 
   // ---- optional device timing of the fused key-switch stages ----
   // Events recorded on the context stream around each stage's launches.

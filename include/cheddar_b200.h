@@ -187,6 +187,35 @@ int chd_encode_const(chd_context *ctx, int level, double scale, double value, in
  * sparse-secret encapsulation: a at level -1 -> res at the top level. */
 int chd_modup_to_max(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a);
 
+/* EvkMap (include/core/EvkMap.h): rotation / conjugation / multiplication
+ * keys by index.  The map borrows the keys; they must outlive it. */
+typedef struct chd_evk_map chd_evk_map;
+int chd_evk_map_create(chd_context *ctx, chd_evk_map **out);
+void chd_evk_map_destroy(chd_evk_map *m);
+int chd_evk_map_set_rotation(chd_evk_map *m, int rot_idx, const chd_evk *key);
+int chd_evk_map_set_conjugation(chd_evk_map *m, const chd_evk *key);
+int chd_evk_map_set_mult(chd_evk_map *m, const chd_evk *key);
+
+/* LinearTransform (src/extension/LinearTransform.cpp:77-124) with the
+ * HoistHandler's double-hoisted baby-step / giant-step evaluation
+ * (src/extension/Hoist.cu).  The matrix has `width` slots and n_diag
+ * diagonals diag_idx[i] with values re/im [n_diag][width]
+ * (d[k] = M[k][(k + i) mod width]); diagonals are encoded at pt_level /
+ * pt_scale with the alpha auxiliary primes.  Evaluation: res (level
+ * pt_level - 1, scale pt_scale * in.scale / rescale prime product) = M in. */
+typedef struct chd_lintrans chd_lintrans;
+int chd_lintrans_create(chd_context *ctx, int width, int n_diag, const int *diag_idx, const double *re,
+                        const double *im, int pt_level, double pt_scale, int bs, int gs, int pre_rotation,
+                        int additional_pt_rot, chd_lintrans **out);
+void chd_lintrans_destroy(chd_lintrans *lt);
+/* HoistHandler::AddRequiredRotations: the rotation keys the transform uses */
+int chd_lintrans_rotations(const chd_lintrans *lt, int *out, int cap, int *count);
+/* the compiled plaintext map (giant step, baby step, message [width]) */
+int chd_lintrans_num_pts(const chd_lintrans *lt, int *count);
+int chd_lintrans_pt(const chd_lintrans *lt, int i, int *gs, int *bs, double *re, double *im);
+int chd_lintrans_evaluate(chd_context *ctx, const chd_lintrans *lt, chd_ciphertext *res, const chd_ciphertext *in,
+                          const chd_evk_map *keys);
+
 /* Batched kernel::ModSwitchMatrixMult: npoly polynomials, each K centred
  * source limbs [K][N] (xt_dev + i*K*N) -> M limbs [M][N] (out_dev + i*M*N),
  * same table and result as chd_bconv_raw.  engine CHD_BCONV_CUDA_CORE runs
