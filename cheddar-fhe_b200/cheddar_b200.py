@@ -114,6 +114,12 @@ def lib():
         "chd_lintrans_num_pts": (i, [vp, C.POINTER(i)]),
         "chd_lintrans_pt": (i, [vp, i, C.POINTER(i), C.POINTER(i), vp, vp]),
         "chd_lintrans_evaluate": (i, [vp, vp, vp, vp, vp]),
+        "chd_poly_create": (i, [vp, vp, i, i, d, d, i, pp]),
+        "chd_evalmod_create": (i, [vp, i, vp, i, i, i, pp, C.POINTER(d), C.POINTER(d)]),
+        "chd_program_destroy": (None, [vp]),
+        "chd_program_json": (i, [vp, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+        "chd_program_run": (i, [vp, vp, vp, vp, vp]),
+        "chd_boot_mod_coefficients": (i, [vp, i]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -479,6 +485,62 @@ class LinearTransform:
     def evaluate(self, ct, keys, res=None):
         res = res if res is not None else Ciphertext(self.ctx)
         _check(lib().chd_lintrans_evaluate(self.ctx.ptr, self.ptr, res.ptr, ct.ptr, keys.ptr))
+        return res
+
+
+def boot_mod_coefficients():
+    """BootParameter's EvalMod Chebyshev coefficients."""
+    n = lib().chd_boot_mod_coefficients(None, 0)
+    out = np.zeros(n)
+    lib().chd_boot_mod_coefficients(out.ctypes.data, n)
+    return out
+
+
+class Program:
+    """A compiled ciphertext program (EvalPoly / EvalMod)."""
+
+    def __init__(self, ctx, ptr, start_scale=None, end_scale=None):
+        self.ctx = ctx
+        self.ptr = ptr
+        self.start_scale = start_scale
+        self.end_scale = end_scale
+
+    @classmethod
+    def poly(cls, ctx, coeffs, input_level, input_scale, target_scale, chebyshev=True):
+        c = np.ascontiguousarray(coeffs, dtype=np.float64)
+        p = C.c_void_p()
+        _check(lib().chd_poly_create(ctx.ptr, c.ctypes.data, len(c), input_level, input_scale, target_scale,
+                                     int(chebyshev), C.byref(p)))
+        return cls(ctx, p, input_scale, target_scale)
+
+    @classmethod
+    def evalmod(cls, ctx, start_level, coeffs, num_double_angle=3, initial_K=2):
+        c = np.ascontiguousarray(coeffs, dtype=np.float64)
+        p = C.c_void_p()
+        s0, s1 = C.c_double(), C.c_double()
+        _check(lib().chd_evalmod_create(ctx.ptr, start_level, c.ctypes.data, len(c), num_double_angle, initial_K,
+                                        C.byref(p), C.byref(s0), C.byref(s1)))
+        return cls(ctx, p, s0.value, s1.value)
+
+    def __del__(self):
+        try:
+            if self.ptr.value:
+                lib().chd_program_destroy(self.ptr)
+                self.ptr = C.c_void_p()
+        except Exception:
+            pass
+
+    def json(self):
+        import json
+        n = C.c_size_t()
+        _check(lib().chd_program_json(self.ptr, None, 0, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        _check(lib().chd_program_json(self.ptr, buf, n.value, C.byref(n)))
+        return json.loads(buf.value.decode())
+
+    def run(self, ct, keys, res=None):
+        res = res if res is not None else Ciphertext(self.ctx)
+        _check(lib().chd_program_run(self.ctx.ptr, self.ptr, res.ptr, ct.ptr, keys.ptr))
         return res
 
 

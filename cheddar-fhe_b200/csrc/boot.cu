@@ -52,6 +52,24 @@ uint32_t trunc_mod(double v, uint32_t p) {
 
 }  // namespace
 
+// BootParameter's EvalMod polynomial (src/extension/BootParameter.cpp:13-23):
+// Chebyshev coefficients of the cosine approximation, to be used with
+// initial K = 2 and three double-angle steps.  The values are the
+// reference's, digit for digit, because the encoded constants (and hence
+// every residue of a bootstrap) depend on them.
+const std::vector<double> &boot_mod_coefficients() {
+  static const std::vector<double> c{
+      0.12517186708929745802,    0.0, 0.2894364973331168731,      0.0,
+      0.36272381596524499154,    0.0, 0.3011054704600794278,      0.0,
+      -0.10550875667295944105,   0.0, -0.43588877795190139706,    0.0,
+      0.37482647434055190702,    0.0, -0.14821069913569220404,    0.0,
+      0.03665437786710548091,    0.0, -0.0063882548960017121343,  0.0,
+      0.00083684232451067872756, 0.0, -8.6443599931576702305e-05, 0.0,
+      7.0966437900548814324e-06, 0.0, -5.228015817181348194e-07,  0.0,
+      2.2714690137973883081e-08, 0.0, -2.3761936068138980797e-09};
+  return c;
+}
+
 const std::vector<std::complex<double>> &Context::enc_twiddles() {
   if (enc_tw.empty()) {
     const int M = 2 * P->n;

@@ -25,6 +25,11 @@ struct chd_evk_map {
 struct chd_lintrans {
   LTPlan plan;
 };
+struct chd_program {
+  Program prog;
+  double start_scale = 0, end_scale = 0;
+  int out_level = 0;
+};
 
 namespace {
 int fail(int code, const std::string &msg) {
@@ -499,6 +504,121 @@ int chd_lintrans_evaluate(chd_context *ctx, const chd_lintrans *lt, chd_cipherte
     return CHD_OK;
   }
   return ctx->c->lt_evaluate(res->ct, in->ct, lt->plan, keys->rot);
+}
+
+int chd_poly_create(chd_context *ctx, const double *coeffs, int n, int input_level, double input_scale,
+                    double target_scale, int chebyshev, chd_program **out) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(coeffs);
+  CHD_NOTNULL(out);
+  if (n < 1) return fail(CHD_ERR_INVALID_ARG, "chd_poly_create: no coefficients");
+  auto *pg = new chd_program();
+  pg->prog.input = pg->prog.reg();
+  int reg = -1;
+  int rc = ctx->c->compile_poly(pg->prog, pg->prog.input, std::vector<double>(coeffs, coeffs + n), input_level,
+                                input_scale, target_scale, chebyshev != 0, &reg, &pg->out_level);
+  if (rc != CHD_OK) {
+    delete pg;
+    return rc;
+  }
+  pg->prog.output = reg;
+  pg->start_scale = input_scale;
+  pg->end_scale = target_scale;
+  *out = pg;
+  return CHD_OK;
+}
+
+int chd_evalmod_create(chd_context *ctx, int start_level, const double *coeffs, int n, int num_double_angle,
+                       int initial_K, chd_program **out, double *start_scale, double *end_scale) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(coeffs);
+  CHD_NOTNULL(out);
+  auto *pg = new chd_program();
+  pg->prog.input = pg->prog.reg();
+  int reg = -1;
+  int rc = ctx->c->compile_evalmod(pg->prog, pg->prog.input, start_level, std::vector<double>(coeffs, coeffs + n),
+                                   num_double_angle, initial_K, &reg, &pg->out_level, &pg->start_scale,
+                                   &pg->end_scale);
+  if (rc != CHD_OK) {
+    delete pg;
+    return rc;
+  }
+  pg->prog.output = reg;
+  if (start_scale) *start_scale = pg->start_scale;
+  if (end_scale) *end_scale = pg->end_scale;
+  *out = pg;
+  return CHD_OK;
+}
+
+void chd_program_destroy(chd_program *p) { delete p; }
+
+int chd_boot_mod_coefficients(double *out, int cap) {
+  const auto &c = boot_mod_coefficients();
+  if (out)
+    for (int i = 0; i < std::min(cap, static_cast<int>(c.size())); i++) out[i] = c[i];
+  return static_cast<int>(c.size());
+}
+
+int chd_program_json(const chd_program *p, char *buf, size_t cap, size_t *len) {
+  CHD_NOTNULL(p);
+  CHD_NOTNULL(len);
+  const Program &g = p->prog;
+  std::string s;
+  char tmp[512];
+  snprintf(tmp, sizeof tmp, "{\"nregs\":%d,\"input\":%d,\"output\":%d,\"out_level\":%d,\"consts\":[", g.nregs,
+           g.input, g.output, p->out_level);
+  s += tmp;
+  for (size_t i = 0; i < g.consts.size(); i++) {
+    snprintf(tmp, sizeof tmp, "%s[%d,%.17g,%.17g]", i ? "," : "", g.consts[i].level, g.consts[i].scale,
+             g.consts[i].value);
+    s += tmp;
+  }
+  s += "],\"ops\":[";
+  for (size_t i = 0; i < g.ops.size(); i++) {
+    const ProgOp &o = g.ops[i];
+    snprintf(tmp, sizeof tmp, "%s{\"k\":%d,\"d\":%d,\"a\":%d,\"b\":%d,\"l\":%d,\"c\":%d,\"p\":%d,\"r\":%d,\"sc\":%.17g,\"s\":[",
+             i ? "," : "", static_cast<int>(o.kind), o.dst, o.a, o.b, o.level, o.c, o.plain, o.rot, o.scale);
+    s += tmp;
+    for (size_t j = 0; j < o.srcs.size(); j++) s += (j ? "," : "") + std::to_string(o.srcs[j]);
+    s += "],\"cs\":[";
+    for (size_t j = 0; j < o.cs.size(); j++) s += (j ? "," : "") + std::to_string(o.cs[j]);
+    s += "]}";
+  }
+  s += "]}";
+  *len = s.size() + 1;
+  if (buf && cap >= s.size() + 1) memcpy(buf, s.c_str(), s.size() + 1);
+  return CHD_OK;
+}
+
+namespace {
+Status copy_ct(Context &C, DeviceCt &dst, const DeviceCt &src) {
+  CHD_TRY(dst.reserve(src.np, src.has_rx, C.P->n));
+  const size_t bytes = static_cast<size_t>(src.np.total()) * C.P->n * 4;
+  cudaMemcpyAsync(dst.bx, src.bx, bytes, cudaMemcpyDeviceToDevice, C.stream);
+  cudaMemcpyAsync(dst.ax, src.ax, bytes, cudaMemcpyDeviceToDevice, C.stream);
+  if (src.has_rx) cudaMemcpyAsync(dst.rx, src.rx, bytes, cudaMemcpyDeviceToDevice, C.stream);
+  dst.scale = src.scale;
+  dst.num_slots = src.num_slots;
+  return kOk;
+}
+}  // namespace
+
+int chd_program_run(chd_context *ctx, const chd_program *p, chd_ciphertext *res, const chd_ciphertext *in,
+                    const chd_evk_map *keys) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(p);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(in);
+  Context &C = *ctx->c;
+  std::vector<DeviceCt> regs(p->prog.nregs);
+  int rc = copy_ct(C, regs[p->prog.input], in->ct);
+  if (rc != CHD_OK) return rc;
+  rc = C.run_program(p->prog, regs, keys ? keys->mult : nullptr, keys ? keys->conj : nullptr,
+                     keys ? &keys->rot : nullptr, nullptr);
+  if (rc != CHD_OK) return rc;
+  rc = copy_ct(C, res->ct, regs[p->prog.output]);
+  if (rc != CHD_OK) return rc;
+  return cudaStreamSynchronize(C.stream) == cudaSuccess ? CHD_OK : fail(CHD_ERR_CUDA, "chd_program_run: CUDA error");
 }
 
 int chd_relinearize(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *key) {

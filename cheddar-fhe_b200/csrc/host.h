@@ -200,6 +200,56 @@ struct LTPlan {
 struct DeviceEvk;
 using RotKeys = std::map<int, const DeviceEvk *>;
 
+// A straight-line program of ciphertext operations over registers, the
+// compiled form of EvalPoly / EvalMod / Boot (planning on the host, every
+// op a call of the device evaluator).  Constants are (level, scale, value)
+// triples encoded with Encoder::EncodeConstant.
+struct ProgConst {
+  int level = 0;
+  double scale = 1.0, value = 0.0;
+};
+enum class OpKind : int {
+  kConstMult = 0,   // dst = a (.) c at `level`               (Context::MultUnsafe Ct x Const)
+  kTensor = 1,      // dst = a x b at `level`, three parts       (Context::MultUnsafe Ct x Ct)
+  kConstAccum = 2,  // dst = sum_i src_i (.) c_i (+ plain) at `level` (ElementWiseHandler::CAccum)
+  kAddConst = 3,    // dst = a + c (b part)                      (Context::Add Ct + Const)
+  kAdd = 4,         // dst = a + b                               (Context::Add Ct + Ct)
+  kRelinRescale = 5,// dst = RelinearizeRescale(a)
+  kRescale = 6,     // dst = Rescale(a)
+  kLevelDown = 7,   // dst = Rescale(a (.) c), c = 1 at the rescale prime product (AddLowerLevelsUntil)
+  kCopy = 8,
+  kSetScale = 9,    // metadata only
+  kSub = 10,        // dst = a - b
+  kHConj = 11,      // dst = HConj(a)
+  kMultImag = 12,   // dst = i * a
+  kModUpToMax = 13, // dst = ModUpToMax(a)
+  kHRotAdd = 14,    // dst = HRot(a, r) + b
+  kLinTrans = 15,   // dst = lin_trans[lt](a)
+};
+struct ProgOp {
+  OpKind kind = OpKind::kCopy;
+  int dst = -1, a = -1, b = -1;
+  int level = 0;
+  int c = -1;                   // constant index
+  std::vector<int> srcs, cs;    // kConstAccum terms
+  int plain = -1;               // kConstAccum plain addend (may be dst itself)
+  int rot = 0;                  // kHRotAdd rotation, kLinTrans transform index
+  double scale = 0.0;           // kSetScale
+};
+struct Program {
+  int nregs = 0, input = 0, output = 0;
+  std::vector<ProgConst> consts;
+  std::vector<ProgOp> ops;
+  int add_const(int level, double scale, double value) {
+    consts.push_back(ProgConst{level, scale, value});
+    return static_cast<int>(consts.size()) - 1;
+  }
+  int reg() { return nregs++; }
+};
+
+// EvalMod cosine polynomial of the reference's BootParameter
+const std::vector<double> &boot_mod_coefficients();
+
 // Releases everything allocated from the arena inside a scope.
 struct ArenaScope {
   Arena &a;
@@ -320,6 +370,21 @@ class Context {
                   int additional_pt_rot, bool suppress_swap, LTPlan *out);
   // HoistHandler::Evaluate (Hoist.cu:554-975): res at pt_level - 1
   Status lt_evaluate(DeviceCt &res, const DeviceCt &in, const LTPlan &pl, const RotKeys &keys);
+
+  // EvalPoly::Compile (EvalPoly.cpp:750-830) of a polynomial in the
+  // Chebyshev (or power) basis for an input at (input_level, input_scale):
+  // appends the evaluation to `prog` reading register `in`, returns the
+  // result register (scale target_scale, level input_level - ceil(log2(deg+1))).
+  Status compile_poly(Program &prog, int in, const std::vector<double> &coeffs, int input_level, double input_scale,
+                      double target_scale, bool chebyshev, int *out_reg, int *out_level);
+  // EvalMod (EvalMod.cpp:9-61): x -> mod-reduction approximation, appended to prog
+  Status compile_evalmod(Program &prog, int in, int start_level, const std::vector<double> &mod_coeffs,
+                         int num_double_angle, int initial_K, int *out_reg, int *out_level, double *start_scale,
+                         double *end_scale);
+  // Runs a program (program.cu): regs[input] holds the input
+  Status run_program(const Program &prog, std::vector<DeviceCt> &regs, const DeviceEvk *mult_key,
+                     const DeviceEvk *conj_key, const RotKeys *rot_keys, const std::vector<const LTPlan *> *lts);
+  bool mult_unsafe_compatible(int l1, int l2) const;
 
   // ---- optional device timing of the fused key-switch stages ----
   // Events recorded on the context stream around each stage's launches.

@@ -1,0 +1,270 @@
+// Device interpreter of op programs (compiled EvalPoly / EvalMod / Boot).
+//
+// Every op writes a spare ciphertext, which is then swapped into the
+// destination register, so outputs may alias inputs freely.  The op
+// semantics are the reference Context's (src/core/Context.cpp):
+// MultUnsafe Ct x Const / Ct x Ct at a target level reading the inputs'
+// limbs past their extra terminal primes ("front ignore"), CAccum,
+// Add / Sub with mixed Rx, RelinearizeRescale, Rescale, LevelDown through
+// the level-down constant, HConj, MultImaginaryUnit, ModUpToMax, HRotAdd
+// and linear transforms.
+#include <algorithm>
+
+#include "host.h"
+#include "kernels.h"
+
+namespace chd {
+namespace {
+
+void swap_ct(DeviceCt &x, DeviceCt &y) {
+  std::swap(x.np, y.np);
+  std::swap(x.has_rx, y.has_rx);
+  std::swap(x.scale, y.scale);
+  std::swap(x.num_slots, y.num_slots);
+  std::swap(x.bx, y.bx);
+  std::swap(x.ax, y.ax);
+  std::swap(x.rx, y.rx);
+  std::swap(x.cap_words, y.cap_words);
+  std::swap(x.owned, y.owned);
+}
+
+uint32_t *part_of(DeviceCt &c, int p) { return p == 0 ? c.bx : (p == 1 ? c.ax : c.rx); }
+const uint32_t *part_of(const DeviceCt &c, int p) { return p == 0 ? c.bx : (p == 1 ? c.ax : c.rx); }
+
+}  // namespace
+
+Status Context::run_program(const Program &prog, std::vector<DeviceCt> &regs, const DeviceEvk *mult_key,
+                            const DeviceEvk *conj_key, const RotKeys *rot_keys,
+                            const std::vector<const LTPlan *> *lts) {
+  CHD_CHECK(static_cast<int>(regs.size()) >= prog.nregs, kErrInvalidArg, "program: too few registers");
+  const int n = P->n;
+  // constants: Montgomery residues over their own level's q primes
+  std::vector<std::vector<uint32_t>> cx(prog.consts.size());
+  std::vector<NP> cnp(prog.consts.size());
+  for (size_t i = 0; i < prog.consts.size(); i++) {
+    const ProgConst &c = prog.consts[i];
+    encode_const(c.level, c.scale, c.value, 0, &cx[i]);
+    cnp[i] = P->level_np(c.level);
+  }
+  DeviceCt spare, spare2;
+  // dst (parts) = sum over terms of src_t (.) c_t, at np, each term reading
+  // its source from row `front_t`
+  struct Term {
+    const DeviceCt *src;
+    int front;
+    const uint32_t *c;  // per dst row constant (Montgomery), already offset
+  };
+  auto const_accum = [&](DeviceCt &dst, const NP &np, int parts, const std::vector<Term> &terms) -> Status {
+    const int nq = np.q();
+    std::vector<int> g(nq);
+    P->gidx(np, g.data());
+    for (int p = 0; p < parts; p++) {
+      ConstAccumDesc d{};
+      for (const Term &t : terms) {
+        if (p == 2 && !t.src->has_rx) continue;
+        CHD_CHECK(d.terms < kMaxConstAccumTerms, kErrUnsupported, "program: too many accumulation terms");
+        d.src[d.terms][0] = part_of(*t.src, p);
+        d.src_row0[d.terms] = t.front;
+        for (int r = 0; r < nq; r++) d.c[d.terms][r] = t.c[r];
+        d.terms++;
+      }
+      d.dst[0] = part_of(dst, p);
+      for (int r = 0; r < nq; r++) {
+        d.q[r] = P->primes[g[r]];
+        d.qinv[r] = P->qinv[g[r]];
+      }
+      d.rows = nq;
+      d.parts = 1;
+      d.n = n;
+      if (d.terms == 0) {
+        cudaMemsetAsync(d.dst[0], 0, static_cast<size_t>(nq) * n * 4, stream);
+      } else {
+        launch_const_accum(d, stream);
+      }
+    }
+    return kOk;
+  };
+  auto front_of = [&](const NP &src, const NP &dst) -> int { return src.ter - dst.ter; };
+  auto check_subset = [&](const NP &sub, const NP &sup) -> Status {
+    CHD_CHECK(sub.main <= sup.main && sub.ter <= sup.ter, kErrShape, "program: incompatible levels");
+    return kOk;
+  };
+  std::vector<std::vector<uint32_t>> ones;  // Montgomery 1 per level, by q count
+  auto mont_one = [&](const NP &np) -> const uint32_t * {
+    ones.emplace_back(np.q());
+    std::vector<int> g(np.q());
+    P->gidx(np, g.data());
+    for (int r = 0; r < np.q(); r++) ones.back()[r] = prime::to_mont(1, P->primes[g[r]]);
+    return ones.back().data();
+  };
+
+  for (const ProgOp &op : prog.ops) {
+    DeviceCt &t = spare;
+    switch (op.kind) {
+      case OpKind::kConstMult:
+      case OpKind::kLevelDown: {
+        const DeviceCt &a = regs.at(op.a);
+        const int level = op.kind == OpKind::kLevelDown ? P->np_to_level(NP{a.np.main, a.np.ter, 0}) : op.level;
+        const NP np = P->level_np(level);
+        CHD_TRY(check_subset(np, a.np));
+        CHD_TRY(check_subset(np, cnp.at(op.c)));
+        DeviceCt &m = op.kind == OpKind::kLevelDown ? spare2 : t;
+        CHD_TRY(m.reserve(np, a.has_rx, n));
+        const uint32_t *c = cx[op.c].data() + front_of(cnp[op.c], np);
+        CHD_TRY(const_accum(m, np, a.has_rx ? 3 : 2, {{&a, front_of(a.np, np), c}}));
+        m.scale = a.scale * prog.consts[op.c].scale;
+        m.num_slots = a.num_slots;
+        if (op.kind == OpKind::kLevelDown) {
+          CHD_TRY(rescale(t, m));
+        }
+        break;
+      }
+      case OpKind::kTensor: {
+        const DeviceCt &a = regs.at(op.a), &b = regs.at(op.b);
+        CHD_CHECK(!a.has_rx && !b.has_rx, kErrShape, "Relinearization required before MultUnsafe Ct x Ct");
+        const NP np = P->level_np(op.level);
+        CHD_TRY(check_subset(np, a.np));
+        CHD_TRY(check_subset(np, b.np));
+        CHD_TRY(t.reserve(np, true, n));
+        const int fa = front_of(a.np, np), fb = front_of(b.np, np), nq = np.q();
+        std::vector<int> g(nq);
+        P->gidx(np, g.data());
+        TensorBatch tb{};
+        for (int r = 0; r < nq; r++) {
+          if (tb.count == 64) {
+            launch_tensor(tb, P->log_n, stream);
+            tb.count = 0;
+          }
+          TensorRow &row = tb.rows[tb.count++];
+          const size_t oa = static_cast<size_t>(fa + r) * n, ob = static_cast<size_t>(fb + r) * n;
+          row.b1 = a.bx + oa;
+          row.a1 = a.ax + oa;
+          row.b2 = b.bx + ob;
+          row.a2 = b.ax + ob;
+          row.d0 = t.bx + static_cast<size_t>(r) * n;
+          row.d1 = t.ax + static_cast<size_t>(r) * n;
+          row.d2 = t.rx + static_cast<size_t>(r) * n;
+          row.q = P->primes[g[r]];
+          row.qinv = P->qinv[g[r]];
+        }
+        launch_tensor(tb, P->log_n, stream);
+        t.scale = a.scale * b.scale;
+        t.num_slots = std::max(a.num_slots, b.num_slots);
+        break;
+      }
+      case OpKind::kConstAccum: {
+        const NP np = P->level_np(op.level);
+        std::vector<Term> terms;
+        double scale = 0;
+        int slots = 0;
+        for (size_t i = 0; i < op.srcs.size(); i++) {
+          const DeviceCt &s = regs.at(op.srcs[i]);
+          CHD_TRY(check_subset(np, s.np));
+          CHD_TRY(check_subset(np, cnp.at(op.cs[i])));
+          terms.push_back({&s, front_of(s.np, np), cx[op.cs[i]].data() + front_of(cnp[op.cs[i]], np)});
+          if (scale == 0) scale = s.scale * prog.consts[op.cs[i]].scale;
+          slots = std::max(slots, s.num_slots);
+        }
+        bool rx = false;
+        if (op.plain >= 0) {
+          const DeviceCt &pl = regs.at(op.plain);
+          CHD_CHECK(pl.np == np, kErrShape, "program: accumulator level mismatch");
+          terms.push_back({&pl, 0, mont_one(np)});
+          rx = pl.has_rx;
+          if (scale == 0) scale = pl.scale;
+          slots = std::max(slots, pl.num_slots);
+        }
+        CHD_TRY(t.reserve(np, rx, n));
+        CHD_TRY(const_accum(t, np, rx ? 3 : 2, terms));
+        t.scale = scale;
+        t.num_slots = slots;
+        break;
+      }
+      case OpKind::kAddConst: {
+        const DeviceCt &a = regs.at(op.a);
+        const NP np{a.np.main, a.np.ter, 0};
+        CHD_CHECK(a.np.aux == 0, kErrShape, "program: AddConst on aux primes");
+        CHD_TRY(check_subset(np, cnp.at(op.c)));
+        CHD_TRY(t.reserve(np, a.has_rx, n));
+        const uint32_t *c = cx[op.c].data() + front_of(cnp[op.c], np);
+        // b part: a.b + c; a / r parts copied
+        const int nq = np.q();
+        std::vector<int> g(nq);
+        P->gidx(np, g.data());
+        ElemBatch eb{};
+        for (int r = 0; r < nq; r++) {
+          if (eb.count == kMaxElemRows) {
+            launch_elementwise(ElemOp::kAddConst, eb, P->log_n, stream);
+            eb.count = 0;
+          }
+          ElemRow &e = eb.rows[eb.count++];
+          e.a = a.bx + static_cast<size_t>(r) * n;
+          e.dst = t.bx + static_cast<size_t>(r) * n;
+          e.q = P->primes[g[r]];
+          e.qinv = P->qinv[g[r]];
+          e.k = c[r];
+        }
+        launch_elementwise(ElemOp::kAddConst, eb, P->log_n, stream);
+        const size_t bytes = static_cast<size_t>(nq) * n * 4;
+        cudaMemcpyAsync(t.ax, a.ax, bytes, cudaMemcpyDeviceToDevice, stream);
+        if (a.has_rx) cudaMemcpyAsync(t.rx, a.rx, bytes, cudaMemcpyDeviceToDevice, stream);
+        t.scale = a.scale;
+        t.num_slots = a.num_slots;
+        break;
+      }
+      case OpKind::kAdd:
+        CHD_TRY(add(t, regs.at(op.a), regs.at(op.b)));
+        break;
+      case OpKind::kSub:
+        CHD_TRY(sub(t, regs.at(op.a), regs.at(op.b)));
+        break;
+      case OpKind::kRelinRescale:
+        CHD_CHECK(mult_key, kErrKey, "program: multiplication key missing");
+        CHD_TRY(relinearize(t, regs.at(op.a), *mult_key, true));
+        break;
+      case OpKind::kRescale:
+        CHD_TRY(rescale(t, regs.at(op.a)));
+        break;
+      case OpKind::kCopy: {
+        const DeviceCt &a = regs.at(op.a);
+        CHD_TRY(t.reserve(a.np, a.has_rx, n));
+        const size_t bytes = static_cast<size_t>(a.np.total()) * n * 4;
+        for (int p = 0; p < (a.has_rx ? 3 : 2); p++)
+          cudaMemcpyAsync(part_of(t, p), part_of(a, p), bytes, cudaMemcpyDeviceToDevice, stream);
+        t.scale = a.scale;
+        t.num_slots = a.num_slots;
+        break;
+      }
+      case OpKind::kSetScale:
+        regs.at(op.dst).scale = op.scale;
+        continue;
+      case OpKind::kHConj:
+        CHD_CHECK(conj_key, kErrKey, "program: conjugation key missing");
+        CHD_TRY(hconj(t, regs.at(op.a), *conj_key));
+        break;
+      case OpKind::kMultImag:
+        CHD_TRY(mult_imag_unit(t, regs.at(op.a)));
+        break;
+      case OpKind::kModUpToMax:
+        CHD_TRY(modup_to_max(t, regs.at(op.a)));
+        break;
+      case OpKind::kHRotAdd: {
+        CHD_CHECK(rot_keys, kErrKey, "program: rotation keys missing");
+        auto it = rot_keys->find(op.rot);
+        CHD_CHECK(it != rot_keys->end() && it->second, kErrKey,
+                  "program: missing rotation key " + std::to_string(op.rot));
+        CHD_TRY(hrot_add(t, regs.at(op.a), regs.at(op.b), *it->second, op.rot));
+        break;
+      }
+      case OpKind::kLinTrans:
+        CHD_CHECK(lts && op.rot >= 0 && op.rot < static_cast<int>(lts->size()) && rot_keys, kErrInvalidArg,
+                  "program: linear transform missing");
+        CHD_TRY(lt_evaluate(t, regs.at(op.a), *(*lts)[op.rot], *rot_keys));
+        break;
+    }
+    swap_ct(regs.at(op.dst), t);
+  }
+  return check_cuda("program");
+}
+
+}  // namespace chd

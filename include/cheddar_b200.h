@@ -216,6 +216,28 @@ int chd_lintrans_pt(const chd_lintrans *lt, int i, int *gs, int *bs, double *re,
 int chd_lintrans_evaluate(chd_context *ctx, const chd_lintrans *lt, chd_ciphertext *res, const chd_ciphertext *in,
                           const chd_evk_map *keys);
 
+/* Compiled ciphertext programs: EvalPoly (src/extension/EvalPoly.cpp) of
+ * a polynomial given by its coefficients (Chebyshev basis when chebyshev
+ * != 0) for an input at (input_level, input_scale), result at
+ * target_scale; and EvalMod (src/extension/EvalMod.cpp: x - 1/(4K), the
+ * Chebyshev cosine of coeffs, num_double_angle double-angle steps) for an
+ * input at start_level.  Running a program needs the multiplication key in
+ * the key map.  chd_program_json writes the compiled op list (ops,
+ * registers, constants as (level, scale, value)) for inspection and
+ * testing; *len receives the size including the terminating zero. */
+typedef struct chd_program chd_program;
+int chd_poly_create(chd_context *ctx, const double *coeffs, int n, int input_level, double input_scale,
+                    double target_scale, int chebyshev, chd_program **out);
+int chd_evalmod_create(chd_context *ctx, int start_level, const double *coeffs, int n, int num_double_angle,
+                       int initial_K, chd_program **out, double *start_scale, double *end_scale);
+void chd_program_destroy(chd_program *p);
+/* BootParameter's EvalMod Chebyshev coefficients (BootParameter.cpp:13-23);
+ * returns their number, copies up to cap of them */
+int chd_boot_mod_coefficients(double *out, int cap);
+int chd_program_json(const chd_program *p, char *buf, size_t cap, size_t *len);
+int chd_program_run(chd_context *ctx, const chd_program *p, chd_ciphertext *res, const chd_ciphertext *in,
+                    const chd_evk_map *keys);
+
 /* Batched kernel::ModSwitchMatrixMult: npoly polynomials, each K centred
  * source limbs [K][N] (xt_dev + i*K*N) -> M limbs [M][N] (out_dev + i*M*N),
  * same table and result as chd_bconv_raw.  engine CHD_BCONV_CUDA_CORE runs

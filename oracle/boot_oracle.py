@@ -157,3 +157,190 @@ def lt_evaluate(o, level, ct, ct_scale, pts, pt_scale, keys):
     rb = o.moddown_rescale(level, final[0])
     ra = o.moddown_rescale(level, final[1])
     return (rb, ra), pt_scale * ct_scale / o.rescale_prime_prod(level)
+
+
+# ---------------------------------------------------------------------------
+# Op programs (compiled EvalPoly / EvalMod / Boot): each op restated on the
+# oracle's primitives with the semantics of the reference Context
+# (src/core/Context.cpp): MultUnsafe Ct x Const / Ct x Ct at a target level
+# reading past extra terminal primes, CAccum, Add / Sub with mixed Rx,
+# RelinearizeRescale, Rescale, LevelDown, HConj, MultImaginaryUnit,
+# ModUpToMax, HRotAdd, linear transforms.
+# ---------------------------------------------------------------------------
+
+K_CONST_MULT, K_TENSOR, K_CACCUM, K_ADD_CONST, K_ADD, K_RELIN_RESCALE, K_RESCALE, K_LEVEL_DOWN, \
+    K_COPY, K_SET_SCALE, K_SUB, K_HCONJ, K_MULT_IMAG, K_MODUP_TO_MAX, K_HROT_ADD, K_LIN_TRANS = range(16)
+
+
+class Ct:
+    def __init__(self, level, parts, scale):
+        self.level = level
+        self.parts = [np.asarray(p, dtype=np.uint32) for p in parts]
+        self.scale = scale
+
+
+def _ter(o, level):
+    return o.level_np(level)[1]
+
+
+def _qprimes(o, level):
+    return [int(p) for p in o.primes(level)]
+
+
+def _cmul_rows(o, level, x, front, c, cfront):
+    qs = _qprimes(o, level)
+    out = np.zeros((len(qs), o.n), dtype=np.uint32)
+    for r, q in enumerate(qs):
+        out[r] = mont_mul(x[front + r], c[cfront + r], q)
+    return out
+
+
+def run_program(o, prog, inp, mult_key=None, conj_key=None, rot_keys=None, lts=None):
+    """Runs a compiled program (the dict of chd_program_json) on `inp`
+    (a Ct); returns the output Ct."""
+    consts = []
+    for level, scale, value in prog["consts"]:
+        consts.append((level, scale, o.encode_const(level, scale, value)))
+    regs = {prog["input"]: inp}
+
+    def acc_part(level, terms, p):
+        qs = _qprimes(o, level)
+        out = np.zeros((len(qs), o.n), dtype=np.uint32)
+        for ct, front, c, cfront in terms:
+            if p >= len(ct.parts):
+                continue
+            for r, q in enumerate(qs):
+                v = ct.parts[p][front + r] if c is None else mont_mul(ct.parts[p][front + r], c[cfront + r], q)
+                out[r] = add_mod(out[r], v, q)
+        return out
+
+    for op in prog["ops"]:
+        k, d, a, b, lvl = op["k"], op["d"], op["a"], op["b"], op["l"]
+        if k in (K_CONST_MULT, K_LEVEL_DOWN):
+            x = regs[a]
+            level = x.level if k == K_LEVEL_DOWN else lvl
+            cl, cs, cx = consts[op["c"]]
+            parts = [_cmul_rows(o, level, p, _ter(o, x.level) - _ter(o, level), cx, _ter(o, cl) - _ter(o, level))
+                     for p in x.parts]
+            y = Ct(level, parts, x.scale * cs)
+            if k == K_LEVEL_DOWN:
+                y = Ct(level - 1, o.rescale_ct(level, np.stack(y.parts)), y.scale / o.rescale_prime_prod(level))
+            regs[d] = y
+        elif k == K_TENSOR:
+            x, y = regs[a], regs[b]
+            nq = o.num_q(lvl)
+            fx, fy = _ter(o, x.level) - _ter(o, lvl), _ter(o, y.level) - _ter(o, lvl)
+            d0, d1, d2 = o.tensor(lvl, x.parts[0][fx:fx + nq], x.parts[1][fx:fx + nq],
+                                  y.parts[0][fy:fy + nq], y.parts[1][fy:fy + nq])
+            regs[d] = Ct(lvl, [d0, d1, d2], x.scale * y.scale)
+        elif k == K_CACCUM:
+            terms = []
+            scale = 0.0
+            for s, c in zip(op["s"], op["cs"]):
+                x = regs[s]
+                cl, cs, cx = consts[c]
+                terms.append((x, _ter(o, x.level) - _ter(o, lvl), cx, _ter(o, cl) - _ter(o, lvl)))
+                if scale == 0:
+                    scale = x.scale * cs
+            nparts = 2
+            if op["p"] >= 0:
+                pl = regs[op["p"]]
+                terms.append((pl, 0, None, 0))
+                nparts = len(pl.parts)
+                if scale == 0:
+                    scale = pl.scale
+            regs[d] = Ct(lvl, [acc_part(lvl, terms, p) for p in range(nparts)], scale)
+        elif k == K_ADD_CONST:
+            x = regs[a]
+            cl, cs, cx = consts[op["c"]]
+            qs = _qprimes(o, x.level)
+            f = _ter(o, cl) - _ter(o, x.level)
+            bx = np.stack([add_mod(x.parts[0][r], cx[f + r], q) for r, q in enumerate(qs)])
+            regs[d] = Ct(x.level, [bx] + list(x.parts[1:]), x.scale)
+        elif k in (K_ADD, K_SUB):
+            x, y = regs[a], regs[b]
+            qs = _qprimes(o, x.level)
+            both = min(len(x.parts), len(y.parts))
+            parts = []
+            for p in range(both):
+                if k == K_ADD:
+                    parts.append(np.stack([add_mod(x.parts[p][r], y.parts[p][r], q) for r, q in enumerate(qs)]))
+                else:
+                    parts.append(np.stack([((x.parts[p][r].astype(np.int64) - y.parts[p][r]) % q).astype(np.uint32)
+                                           for r, q in enumerate(qs)]))
+            if len(x.parts) == 3 and both == 2:
+                parts.append(x.parts[2])
+            elif len(y.parts) == 3 and both == 2:
+                parts.append(y.parts[2])
+            regs[d] = Ct(x.level, parts, x.scale)
+        elif k == K_RELIN_RESCALE:
+            x = regs[a]
+            rb, ra = o.relinearize(x.level, x.parts, mult_key, rescale=True)
+            regs[d] = Ct(x.level - 1, [rb, ra], x.scale / o.rescale_prime_prod(x.level))
+        elif k == K_RESCALE:
+            x = regs[a]
+            regs[d] = Ct(x.level - 1, list(o.rescale_ct(x.level, np.stack(x.parts))),
+                         x.scale / o.rescale_prime_prod(x.level))
+        elif k == K_COPY:
+            x = regs[a]
+            regs[d] = Ct(x.level, [p.copy() for p in x.parts], x.scale)
+        elif k == K_SET_SCALE:
+            regs[d].scale = op["sc"]
+        elif k == K_HCONJ:
+            x = regs[a]
+            rb, ra = o.hconj(x.level, x.parts, conj_key)
+            regs[d] = Ct(x.level, [rb, ra], x.scale)
+        elif k == K_MULT_IMAG:
+            x = regs[a]
+            regs[d] = Ct(x.level, [o.mult_imag_unit(x.level, p) for p in x.parts], x.scale)
+        elif k == K_MODUP_TO_MAX:
+            x = regs[a]
+            rb, ra = o.modup_to_max(x.parts[0], x.parts[1])
+            regs[d] = Ct(o.max_level, [rb, ra], x.scale)
+        elif k == K_HROT_ADD:
+            x, y = regs[a], regs[b]
+            rb, ra = o.hrot(x.level, x.parts, rot_keys[op["r"]], op["r"])
+            qs = _qprimes(o, x.level)
+            regs[d] = Ct(x.level, [np.stack([add_mod(rb[r], y.parts[0][r], q) for r, q in enumerate(qs)]),
+                                   np.stack([add_mod(ra[r], y.parts[1][r], q) for r, q in enumerate(qs)])], x.scale)
+        elif k == K_LIN_TRANS:
+            x = regs[a]
+            plan = lts[op["r"]]
+            (rb, ra), sc = lt_evaluate(o, plan["level"], x.parts, x.scale, plan["pts"], plan["scale"], rot_keys)
+            regs[d] = Ct(plan["level"] - 1, [rb, ra], sc)
+        else:
+            raise ValueError(f"unknown op {k}")
+    return regs[prog["output"]]
+
+
+def plain_program(prog, x):
+    """Evaluates a program on plain values (constants by their value; scales,
+    rescaling and key switching are identities on the message), which is the
+    polynomial the compiled program computes (cf. EvalPoly::PlainEvaluate,
+    EvalPoly.cpp:845-854)."""
+    regs = {prog["input"]: np.asarray(x, dtype=np.float64)}
+    vals = [c[2] for c in prog["consts"]]
+    for op in prog["ops"]:
+        k, d, a, b = op["k"], op["d"], op["a"], op["b"]
+        if k == K_CONST_MULT:
+            regs[d] = regs[a] * vals[op["c"]]
+        elif k == K_TENSOR:
+            regs[d] = regs[a] * regs[b]
+        elif k == K_CACCUM:
+            v = sum(regs[s] * vals[c] for s, c in zip(op["s"], op["cs"]))
+            if op["p"] >= 0:
+                v = v + regs[op["p"]]
+            regs[d] = v
+        elif k == K_ADD_CONST:
+            regs[d] = regs[a] + vals[op["c"]]
+        elif k == K_ADD:
+            regs[d] = regs[a] + regs[b]
+        elif k == K_SUB:
+            regs[d] = regs[a] - regs[b]
+        elif k in (K_RELIN_RESCALE, K_RESCALE, K_LEVEL_DOWN, K_COPY):
+            regs[d] = regs[a]
+        elif k == K_SET_SCALE:
+            pass
+        else:
+            raise ValueError(f"plain evaluation does not cover op {k}")
+    return regs[prog["output"]]

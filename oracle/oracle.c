@@ -1119,6 +1119,28 @@ int orc_hmult(const orc_ctx *c, int level, const uint32_t *b1,
   return rc;
 }
 
+/* Context::Relinearize / RelinearizeRescale (Context.cpp:539-547, 714-737)
+ * of a three-part ciphertext (d0, d1, d2) */
+int orc_relinearize(const orc_ctx *c, int level, const uint32_t *d0,
+                    const uint32_t *d1, const uint32_t *d2,
+                    const uint32_t *key_bx, const uint32_t *key_ax, int rescale,
+                    uint32_t *out_bx, uint32_t *out_ax) {
+  if (level < 0 || level > c->max_level || (rescale && level < 1)) {
+    set_err("invalid level");
+    return -1;
+  }
+  np_t n = level_np(c, level, 0);
+  int N = c->n, tot = np_q(n) + c->alpha;
+  uint32_t *acc = malloc(2 * (size_t)tot * N * sizeof(uint32_t));
+  uint32_t *ab = acc, *aa = acc + (size_t)tot * N;
+  int rc = mult_key_no_moddown(c, level, d0, d1, d2, key_bx, key_ax, ab, aa);
+  int md = rescale ? MD_MDR : MD_MODDOWN;
+  if (!rc) rc = moddown_worker(c, level, md, ab, out_bx);
+  if (!rc) rc = moddown_worker(c, level, md, aa, out_ax);
+  free(acc);
+  return rc;
+}
+
 int orc_mult_key(const orc_ctx *c, int level, const uint32_t *bx,
                  const uint32_t *ax, const uint32_t *key_bx,
                  const uint32_t *key_ax, uint32_t *out_bx, uint32_t *out_ax) {

@@ -144,6 +144,10 @@ int orc_hmult(const orc_ctx *c, int level, const uint32_t *b1,
               const uint32_t *key_bx, const uint32_t *key_ax, int rescale,
               uint32_t *out_bx, uint32_t *out_ax);
 /* MultKey then ModDown (key switch of a 2-part ciphertext) */
+int orc_relinearize(const orc_ctx *c, int level, const uint32_t *d0,
+                    const uint32_t *d1, const uint32_t *d2,
+                    const uint32_t *key_bx, const uint32_t *key_ax, int rescale,
+                    uint32_t *out_bx, uint32_t *out_ax);
 int orc_mult_key(const orc_ctx *c, int level, const uint32_t *bx,
                  const uint32_t *ax, const uint32_t *key_bx,
                  const uint32_t *key_ax, uint32_t *out_bx, uint32_t *out_ax);

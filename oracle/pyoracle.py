@@ -84,6 +84,7 @@ def lib():
             "orc_decode": (C.c_int, [vp, C.c_int, C.c_double, u32p, C.c_int, f64p, f64p]),
             "orc_encode_const": (C.c_int, [vp, C.c_int, C.c_double, C.c_double, C.c_int, u32p]),
             "orc_modup_to_max": (C.c_int, [vp, u32p, u32p, u32p, u32p]),
+            "orc_relinearize": (C.c_int, [vp, C.c_int, u32p, u32p, u32p, u32p, u32p, C.c_int, u32p, u32p]),
             "orc_uniform": (C.c_int, [vp, C.c_uint64, C.c_int, C.c_int, C.c_int, u32p]),
             "orc_mont_reduce_lazy": (C.c_int32, [C.c_int64, C.c_uint32, C.c_int32]),
             "orc_mont_mult_lazy": (C.c_int32, [C.c_int32, C.c_int32, C.c_uint32, C.c_int32]),
@@ -287,6 +288,16 @@ class Oracle:
         c = lambda x: np.ascontiguousarray(x, dtype=np.uint32)
         _check(lib().orc_hmult(self.ptr, level, c(a[0]), c(a[1]), c(b[0]), c(b[1]),
                                c(key[0]), c(key[1]), int(rescale), ob, oa), "hmult")
+        return ob, oa
+
+    def relinearize(self, level, d, key, rescale=True):
+        """Context::Relinearize(Rescale) of three parts d = (d0, d1, d2)."""
+        nq = self.num_q(level - 1 if rescale else level)
+        ob = np.zeros((nq, self.n), dtype=np.uint32)
+        oa = np.zeros_like(ob)
+        c = lambda x: np.ascontiguousarray(x, dtype=np.uint32)
+        _check(lib().orc_relinearize(self.ptr, level, c(d[0]), c(d[1]), c(d[2]), c(key[0]), c(key[1]),
+                                     int(rescale), ob, oa), "relinearize")
         return ob, oa
 
     def mult_key(self, level, a, key):
