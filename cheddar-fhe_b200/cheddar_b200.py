@@ -120,6 +120,14 @@ def lib():
         "chd_program_json": (i, [vp, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
         "chd_program_run": (i, [vp, vp, vp, vp, vp]),
         "chd_boot_mod_coefficients": (i, [vp, i]),
+        "chd_boot_create": (i, [vp, i, i, i, i, pp]),
+        "chd_boot_destroy": (None, [vp]),
+        "chd_boot_rotations": (i, [vp, vp, i, C.POINTER(i)]),
+        "chd_boot_levels": (i, [vp, vp, vp]),
+        "chd_boot_json": (i, [vp, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+        "chd_boot_lt_info": (i, [vp, i, C.POINTER(i), C.POINTER(d), C.POINTER(i), C.POINTER(i)]),
+        "chd_boot_lt_pt": (i, [vp, i, i, C.POINTER(i), C.POINTER(i), vp, vp]),
+        "chd_boot_run": (i, [vp, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -541,6 +549,70 @@ class Program:
     def run(self, ct, keys, res=None):
         res = res if res is not None else Ciphertext(self.ctx)
         _check(lib().chd_program_run(self.ctx.ptr, self.ptr, res.ptr, ct.ptr, keys.ptr))
+        return res
+
+
+class BootContext:
+    """BootContext prepared for `num_slots` (full slots): CoeffToSlot,
+    EvalMod, SlotToCoeff (src/extension/BootContext.cpp)."""
+
+    def __init__(self, ctx, num_slots=None, num_cts_levels=4, num_stc_levels=3, log_message_ratio=5):
+        self.ctx = ctx
+        self.ptr = C.c_void_p()
+        ns = num_slots if num_slots is not None else ctx.n // 2
+        _check(lib().chd_boot_create(ctx.ptr, ns, num_cts_levels, num_stc_levels, log_message_ratio,
+                                     C.byref(self.ptr)))
+        lv = (C.c_int * 5)()
+        sc = (C.c_double * 5)()
+        _check(lib().chd_boot_levels(self.ptr, lv, sc))
+        self.cts_start, self.eval_mod_start, self.stc_start, self.end_level, self.log_scaleup = list(lv)
+        self.cts_const, self.stc_const, self.eval_mod_start_scale, self.eval_mod_end_scale, self.final_scale = list(sc)
+
+    def __del__(self):
+        try:
+            if self.ptr.value:
+                lib().chd_boot_destroy(self.ptr)
+                self.ptr = C.c_void_p()
+        except Exception:
+            pass
+
+    def rotations(self):
+        cnt = C.c_int()
+        _check(lib().chd_boot_rotations(self.ptr, None, 0, C.byref(cnt)))
+        out = (C.c_int * max(1, cnt.value))()
+        _check(lib().chd_boot_rotations(self.ptr, out, cnt.value, C.byref(cnt)))
+        return [out[i] for i in range(cnt.value)]
+
+    def json(self):
+        import json
+        n = C.c_size_t()
+        _check(lib().chd_boot_json(self.ptr, None, 0, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        _check(lib().chd_boot_json(self.ptr, buf, n.value, C.byref(n)))
+        return json.loads(buf.value.decode())
+
+    def transforms(self):
+        """[{level, scale, pts: [(gs, bs, message)]}] for CtS then StC."""
+        res = []
+        i = 0
+        while True:
+            lvl, sc, npts, w = C.c_int(), C.c_double(), C.c_int(), C.c_int()
+            if lib().chd_boot_lt_info(self.ptr, i, C.byref(lvl), C.byref(sc), C.byref(npts), C.byref(w)) != 0:
+                break
+            pts = []
+            for j in range(npts.value):
+                g, b = C.c_int(), C.c_int()
+                re = np.zeros(w.value)
+                im = np.zeros(w.value)
+                _check(lib().chd_boot_lt_pt(self.ptr, i, j, C.byref(g), C.byref(b), re.ctypes.data, im.ctypes.data))
+                pts.append((g.value, b.value, re + 1j * im))
+            res.append({"level": lvl.value, "scale": sc.value, "pts": pts})
+            i += 1
+        return res
+
+    def Boot(self, ct, keys, res=None):
+        res = res if res is not None else Ciphertext(self.ctx)
+        _check(lib().chd_boot_run(self.ctx.ptr, self.ptr, res.ptr, ct.ptr, keys.ptr))
         return res
 
 

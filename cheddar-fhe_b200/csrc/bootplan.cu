@@ -1,0 +1,323 @@
+// Bootstrapping plan: constants, CoeffToSlot / SlotToCoeff linear
+// transforms and the Boot op program.
+//
+// Follows the reference:
+//   BootContext ctor (src/extension/BootContext.cpp:38-92): scale-up
+//     exponent, CtS / StC constants, EvalMod;
+//   EvalSpecialFFT::PopulatePlainMatrices / PreparePlaintexts / BSGSSplit
+//     (src/extension/EvalSpecialFFT.cpp:30-300): the special FFT as
+//     striped butterfly stages, grouped into num_cts (num_stc) phases, each
+//     a LinearTransform at its level with the min-KS pre-rotations;
+//   BootContext::Boot (BootContext.cpp:296-370): scale-up at level -1,
+//     ModUpToMax, CoeffToSlot, real / imaginary split, EvalMod on each,
+//     recombination, SlotToCoeff.
+// Full-slot bootstrapping (N/2 slots) without sparse-secret encapsulation.
+#include <algorithm>
+#include <cmath>
+
+#include "host.h"
+
+namespace chd {
+namespace {
+
+using cd = std::complex<double>;
+
+int log2_ceil(int a) {
+  int r = 0;
+  while ((1 << r) < a) r++;
+  return r;
+}
+bool is_pow2(int a) { return a > 0 && (a & (a - 1)) == 0; }
+
+std::pair<int, int> bsgs_split(int num_diag) {
+  // EvalSpecialFFT::BSGSSplit, EvalSpecialFFT.cpp:33-62
+  if (num_diag <= 4) return {num_diag, 1};
+  int bs;
+  switch (num_diag) {
+    case 7:
+    case 8:
+    case 15:
+    case 16:
+      bs = 4;
+      break;
+    case 31:
+    case 32:
+    case 63:
+    case 64:
+      bs = 8;
+      break;
+    default:
+      bs = 1 << ((log2_ceil(num_diag) + 1) / 2);
+      break;
+  }
+  return {bs, (num_diag + bs - 1) / bs};
+}
+
+}  // namespace
+
+Status Context::boot_build(int num_slots, int num_cts, int num_stc, int log_msg_ratio, BootPlan *out) {
+  const int half = P->n / 2;
+  CHD_CHECK(num_slots == half, kErrUnsupported, "Boot: only full-slot bootstrapping (N/2 slots) is supported");
+  CHD_CHECK(num_slots >= 256 && is_pow2(num_slots), kErrInvalidArg, "Boot: power-of-two slots >= 256");
+  CHD_CHECK(num_cts >= 2 && num_stc >= 2, kErrInvalidArg, "Boot: use at least 2 levels for CtS and StC");
+  CHD_CHECK(P->spec.dense_hw <= 0 || P->spec.dense_hw <= P->spec.sparse_hw, kErrUnsupported,
+            "Boot: sparse-secret encapsulation is not supported (dense Hamming weight > sparse)");
+  BootPlan &bp = *out;
+  bp = BootPlan{};
+  bp.num_slots = num_slots;
+  // BootParameter levels, BootParameter.cpp:25-41
+  const auto &mod_co = boot_mod_coefficients();
+  const int num_da = 3, initial_K = 2;
+  const int em_levels = log2_ceil(static_cast<int>(mod_co.size())) + num_da;
+  bp.max_level = P->max_level;
+  bp.cts_start = bp.max_level;
+  bp.em_start = bp.max_level - num_cts;
+  bp.stc_start = bp.em_start - em_levels;
+  bp.end_level = bp.stc_start - num_stc;
+  CHD_CHECK(bp.end_level >= 0, kErrInvalidLevel, "Boot: not enough levels");
+  CHD_CHECK(P->spec.default_encryption_level == bp.stc_start, kErrInvalidArg,
+            "Parameter mismatch for BootContext (default encryption level must be the StC start level)");
+  // BootContext ctor, BootContext.cpp:44-92
+  auto log2_scale = [](double s) { return static_cast<int>(std::log2(s) + 0.5); };
+  double level_zero_scale = P->spec.base_scale;
+  const int log_lzs = log2_scale(level_zero_scale);
+  const NP b = P->level_np(-1);
+  std::vector<int> gb(b.q());
+  P->gidx(b, gb.data());
+  double q0_prod = 1.0;
+  for (int g : gb) q0_prod *= P->primes[g];
+  const int log_q0 = log2_scale(q0_prod);
+  bp.log_scaleup = (log_q0 - log_lzs) - log_msg_ratio;
+  CHD_CHECK(bp.log_scaleup >= 0, kErrInvalidArg, "Invalid level zero scaleup");
+  level_zero_scale *= (1 << bp.log_scaleup);
+  CHD_CHECK(log_q0 <= 62 && log_lzs <= 62, kErrInvalidArg, "Invalid q0_prod or level zero scale");
+  const int log_em_start = log2_scale(P->rescale_prod.at(bp.em_start));
+  const int actual_K = (1 << num_da) * initial_K;
+  double em_end = static_cast<double>(uint64_t{1} << log_em_start);
+  for (int i = 0; i < em_levels; i++) em_end = em_end * em_end / P->rescale_prod.at(bp.em_start - i);
+  bp.cts_const = static_cast<double>(uint64_t{1} << (log_em_start - P->log_n)) / (q0_prod * actual_K);
+  bp.stc_const = (q0_prod * P->scale.at(bp.end_level)) / (em_end * level_zero_scale);
+
+  // ---- special FFT stages (EvalSpecialFFT::PopulatePlainMatrices) ----
+  const int ns = num_slots, M = 2 * P->n, stages = log2_ceil(ns);
+  const auto &tw = enc_twiddles();
+  std::vector<SMat> fft(stages), ifft(stages);
+  for (int i = 0; i < stages; i++) {
+    const int stride = 1 << i, sg = stride * 2, st8 = stride << 3, gap = M / st8;
+    SMat &ft = fft[i];
+    SMat &it = ifft[stages - i - 1];
+    ft.h = ft.w = it.h = it.w = ns;
+    ft.d.emplace(0, std::vector<cd>(ns, cd(0)));
+    ft.d.emplace(stride, std::vector<cd>(ns, cd(0)));
+    if (i != stages - 1) ft.d.emplace(ns - stride, std::vector<cd>(ns, cd(0)));
+    it.d.emplace(0, std::vector<cd>(ns, cd(0)));
+    it.d.emplace(stride, std::vector<cd>(ns, cd(0)));
+    if (i != stages - 1) it.d.emplace(ns - stride, std::vector<cd>(ns, cd(0)));
+    // at the last stage ns - stride == stride: the "minus" diagonal is the
+    // "plus" one, as in the reference's map
+    std::vector<cd> &f0 = ft.d[0], &fp = ft.d[stride], &fm = ft.d[ns - stride];
+    std::vector<cd> &i0 = it.d[0], &ip = it.d[stride], &im = it.d[ns - stride];
+    for (int j = 0; j < stride; j++) {
+      const int fti = static_cast<int>(P->galois[j] % st8) * gap;
+      const int iti = (st8 - static_cast<int>(P->galois[j] % st8)) * gap;
+      const cd ftw = tw[fti], itw = tw[iti];
+      f0[j] = 1;
+      fp[j] = ftw;
+      fm[j + stride] = 1;
+      f0[j + stride] = -ftw;
+      i0[j] = 1;
+      ip[j] = 1;
+      im[j + stride] = itw;
+      i0[j + stride] = -itw;
+    }
+    const int num_double = log2_ceil(ns / sg);
+    for (int r = 0; r < num_double; r++) {
+      const int len = sg * (1 << r);
+      auto dup = [&](std::vector<cd> &v) { std::copy(v.begin(), v.begin() + len, v.begin() + len); };
+      dup(f0);
+      dup(fp);
+      if (i != stages - 1) dup(fm);
+      dup(i0);
+      dup(ip);
+      if (i != stages - 1) dup(im);
+    }
+  }
+
+  // ---- phases (EvalSpecialFFT::PreparePlaintexts) ----
+  const double cts_div = std::pow(bp.cts_const, 1.0 / num_cts);
+  const double stc_div = std::pow(bp.stc_const, 1.0 / num_stc);
+  bp.lts.resize(num_cts + num_stc);
+  int left = stages, cumul = 0;
+  for (int i = 0; i < num_cts; i++) {
+    const int st = i == 0 ? (left + num_cts - 1) / num_cts : left / (num_cts - i);
+    left -= st;
+    SMat ph = ifft[cumul];
+    for (int j = cumul + 1; j < cumul + st; j++) ph = smat_mult(ifft[j], ph);
+    ph = smat_scale(ph, cd(cts_div));
+    int eff = static_cast<int>(ph.d.size());
+    if (i == num_cts - 1) eff += 1;
+    auto [bs, gs] = bsgs_split(eff);
+    int pre, add = -(1 << left);
+    if (i == 0) {
+      pre = 1 << left;
+    } else if (i == num_cts - 1) {
+      pre = -(1 << st);
+      add = 0;
+    } else {
+      pre = -((1 << st) - 1) * (1 << left);
+    }
+    const int lvl = bp.cts_start - i;
+    CHD_TRY(lt_build(ph, lvl, P->rescale_prod.at(lvl), bs, gs, pre, add, false, &bp.lts[i]));
+    cumul += st;
+  }
+  left = stages;
+  cumul = 0;
+  for (int i = 0; i < num_stc; i++) {
+    const int st = left / (num_stc - i);
+    left -= st;
+    SMat ph = fft[cumul];
+    for (int j = cumul + 1; j < cumul + st; j++) ph = smat_mult(fft[j], ph);
+    ph = smat_scale(ph, cd(stc_div));
+    int eff = static_cast<int>(ph.d.size());
+    if (i == 0) eff += 1;
+    auto [bs, gs] = bsgs_split(eff);
+    int pre, add;
+    if (i == 0) {
+      pre = -(1 << st);
+      add = 1 << st;
+    } else if (i == num_stc - 1) {
+      pre = 1 << cumul;
+      add = 0;
+    } else {
+      pre = -((1 << st) - 1) * (1 << cumul);
+      add = 1 << (st + cumul);
+    }
+    const int lvl = bp.stc_start - i;
+    CHD_TRY(lt_build(ph, lvl, P->rescale_prod.at(lvl), bs, gs, pre, add, false, &bp.lts[num_cts + i]));
+    cumul += st;
+  }
+  for (auto &l : bp.lts) bp.lt_ptrs.push_back(&l);
+  {
+    std::vector<int> r;
+    for (const auto &l : bp.lts) {
+      for (int x : l.bs_idx)
+        if (x) r.push_back(x);
+      for (int x : l.gs_idx)
+        if (x) r.push_back(x);
+    }
+    std::sort(r.begin(), r.end());
+    r.erase(std::unique(r.begin(), r.end()), r.end());
+    bp.rotations = r;
+  }
+
+  // ---- the Boot program (BootContext::Boot, full slots, kNormal) ----
+  Program &pg = bp.prog;
+  pg.input = pg.reg();
+  auto op = [&](OpKind k, int a, int b = -1) {
+    ProgOp o;
+    o.kind = k;
+    o.dst = pg.reg();
+    o.a = a;
+    o.b = b;
+    pg.ops.push_back(o);
+    return o.dst;
+  };
+  // 0. scale up: MultUnsafe(input, scaleup constant, level -1)
+  const int su = pg.add_const(-1, 1.0, static_cast<double>(1 << bp.log_scaleup));
+  {
+    ProgOp o;
+    o.kind = OpKind::kConstMult;
+    o.dst = pg.reg();
+    o.a = pg.input;
+    o.c = su;
+    o.level = -1;
+    pg.ops.push_back(o);
+    // 1. ModUpToMax (no sparse-secret encapsulation); full slots: no trace
+    int x = op(OpKind::kModUpToMax, o.dst);
+    // 2. CoeffToSlot
+    for (int i = 0; i < num_cts; i++) {
+      ProgOp l;
+      l.kind = OpKind::kLinTrans;
+      l.dst = pg.reg();
+      l.a = x;
+      l.rot = i;
+      pg.ops.push_back(l);
+      x = l.dst;
+    }
+    // 3. real / imaginary parts, EvalMod on each
+    int em_reg = -1, em_level = 0;
+    double s0 = 0, s1 = 0;
+    {
+      // the EvalMod start scale is fixed by the parameters; set it first
+      Program probe;
+      probe.input = probe.reg();
+      CHD_TRY(compile_evalmod(probe, probe.input, bp.em_start, mod_co, num_da, initial_K, &em_reg, &em_level, &s0,
+                              &s1));
+    }
+    bp.em_start_scale = s0;
+    bp.em_end_scale = s1;
+    ProgOp ss;
+    ss.kind = OpKind::kSetScale;
+    ss.dst = x;
+    ss.a = x;
+    ss.scale = s0;
+    pg.ops.push_back(ss);
+    const int conj = op(OpKind::kHConj, x);
+    int re = op(OpKind::kAdd, x, conj);
+    int im = op(OpKind::kSub, conj, x);
+    im = op(OpKind::kMultImag, im);
+    int re_out = -1, im_out = -1;
+    CHD_TRY(compile_evalmod(pg, re, bp.em_start, mod_co, num_da, initial_K, &re_out, &em_level, &s0, &s1));
+    CHD_TRY(compile_evalmod(pg, im, bp.em_start, mod_co, num_da, initial_K, &im_out, &em_level, &s0, &s1));
+    CHD_CHECK(em_level == bp.stc_start, kErrInvalidLevel, "Boot: EvalMod level bookkeeping mismatch");
+    im_out = op(OpKind::kMultImag, im_out);
+    x = op(OpKind::kAdd, re_out, im_out);
+    // 4. SlotToCoeff
+    for (int i = 0; i < num_stc; i++) {
+      ProgOp l;
+      l.kind = OpKind::kLinTrans;
+      l.dst = pg.reg();
+      l.a = x;
+      l.rot = num_cts + i;
+      pg.ops.push_back(l);
+      x = l.dst;
+    }
+    bp.final_scale = P->scale.at(bp.end_level);
+    ProgOp fs;
+    fs.kind = OpKind::kSetScale;
+    fs.dst = x;
+    fs.a = x;
+    fs.scale = bp.final_scale;
+    pg.ops.push_back(fs);
+    pg.output = x;
+  }
+  return kOk;
+}
+
+Status Context::boot_run(const BootPlan &bp, DeviceCt &res, const DeviceCt &in, const DeviceEvk &mult_key,
+                         const DeviceEvk &conj_key, const RotKeys &rot_keys, std::vector<DeviceCt> *regs_io) {
+  // BootContext::Boot: the input must sit at level 0 (LevelDown needs the
+  // sparse-secret constants)
+  CHD_CHECK(in.np == P->level_np(0) && !in.has_rx, kErrShape, "Boot: input must be at level 0 without Rx");
+  std::vector<DeviceCt> local;
+  std::vector<DeviceCt> &regs = regs_io ? *regs_io : local;
+  if (static_cast<int>(regs.size()) < bp.prog.nregs) regs.resize(bp.prog.nregs);
+  DeviceCt &r0 = regs[bp.prog.input];
+  CHD_TRY(r0.reserve(in.np, false, P->n));
+  const size_t bytes = static_cast<size_t>(in.np.total()) * P->n * 4;
+  cudaMemcpyAsync(r0.bx, in.bx, bytes, cudaMemcpyDeviceToDevice, stream);
+  cudaMemcpyAsync(r0.ax, in.ax, bytes, cudaMemcpyDeviceToDevice, stream);
+  r0.scale = in.scale;
+  r0.num_slots = in.num_slots;
+  CHD_TRY(run_program(bp.prog, regs, &mult_key, &conj_key, &rot_keys, &bp.lt_ptrs));
+  const DeviceCt &o = regs[bp.prog.output];
+  CHD_TRY(res.reserve(o.np, false, P->n));
+  const size_t ob = static_cast<size_t>(o.np.total()) * P->n * 4;
+  cudaMemcpyAsync(res.bx, o.bx, ob, cudaMemcpyDeviceToDevice, stream);
+  cudaMemcpyAsync(res.ax, o.ax, ob, cudaMemcpyDeviceToDevice, stream);
+  res.scale = bp.final_scale;
+  res.num_slots = in.num_slots;
+  return check_cuda("boot");
+}
+
+}  // namespace chd

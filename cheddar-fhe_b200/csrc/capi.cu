@@ -25,6 +25,10 @@ struct chd_evk_map {
 struct chd_lintrans {
   LTPlan plan;
 };
+struct chd_boot {
+  BootPlan plan;
+  std::vector<DeviceCt> regs;  // program registers kept across calls
+};
 struct chd_program {
   Program prog;
   double start_scale = 0, end_scale = 0;
@@ -619,6 +623,110 @@ int chd_program_run(chd_context *ctx, const chd_program *p, chd_ciphertext *res,
   rc = copy_ct(C, res->ct, regs[p->prog.output]);
   if (rc != CHD_OK) return rc;
   return cudaStreamSynchronize(C.stream) == cudaSuccess ? CHD_OK : fail(CHD_ERR_CUDA, "chd_program_run: CUDA error");
+}
+
+int chd_boot_create(chd_context *ctx, int num_slots, int num_cts_levels, int num_stc_levels, int log_message_ratio,
+                    chd_boot **out) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(out);
+  auto *b = new chd_boot();
+  int rc = ctx->c->boot_build(num_slots, num_cts_levels, num_stc_levels, log_message_ratio, &b->plan);
+  if (rc != CHD_OK) {
+    delete b;
+    return rc;
+  }
+  *out = b;
+  return CHD_OK;
+}
+
+void chd_boot_destroy(chd_boot *b) { delete b; }
+
+int chd_boot_rotations(const chd_boot *b, int *out, int cap, int *count) {
+  CHD_NOTNULL(b);
+  CHD_NOTNULL(count);
+  *count = static_cast<int>(b->plan.rotations.size());
+  if (out)
+    for (int i = 0; i < std::min(cap, *count); i++) out[i] = b->plan.rotations[i];
+  return CHD_OK;
+}
+
+int chd_boot_levels(const chd_boot *b, int *levels, double *scales) {
+  CHD_NOTNULL(b);
+  const BootPlan &p = b->plan;
+  if (levels) {
+    levels[0] = p.cts_start;
+    levels[1] = p.em_start;
+    levels[2] = p.stc_start;
+    levels[3] = p.end_level;
+    levels[4] = p.log_scaleup;
+  }
+  if (scales) {
+    scales[0] = p.cts_const;
+    scales[1] = p.stc_const;
+    scales[2] = p.em_start_scale;
+    scales[3] = p.em_end_scale;
+    scales[4] = p.final_scale;
+  }
+  return CHD_OK;
+}
+
+int chd_boot_json(const chd_boot *b, char *buf, size_t cap, size_t *len) {
+  CHD_NOTNULL(b);
+  chd_program tmp;
+  tmp.prog = b->plan.prog;
+  tmp.out_level = b->plan.end_level;
+  return chd_program_json(&tmp, buf, cap, len);
+}
+
+int chd_boot_lt_info(const chd_boot *b, int i, int *level, double *scale, int *npts, int *width) {
+  CHD_NOTNULL(b);
+  if (i < 0 || i >= static_cast<int>(b->plan.lts.size())) return fail(CHD_ERR_INVALID_ARG, "chd_boot_lt_info: index");
+  const LTPlan &l = b->plan.lts[i];
+  if (level) *level = l.pt_level;
+  if (scale) *scale = l.pt_scale;
+  if (npts) *npts = static_cast<int>(l.pts.size());
+  if (width) *width = l.width;
+  return CHD_OK;
+}
+
+int chd_boot_lt_pt(const chd_boot *b, int i, int j, int *gs, int *bs, double *re, double *im) {
+  CHD_NOTNULL(b);
+  if (i < 0 || i >= static_cast<int>(b->plan.lts.size())) return fail(CHD_ERR_INVALID_ARG, "chd_boot_lt_pt: index");
+  const LTPlan &l = b->plan.lts[i];
+  if (j < 0 || j >= static_cast<int>(l.pts.size())) return fail(CHD_ERR_INVALID_ARG, "chd_boot_lt_pt: index");
+  const LTPlan::Pt &p = l.pts[j];
+  if (gs) *gs = p.gs;
+  if (bs) *bs = p.bs;
+  for (size_t k = 0; k < p.msg.size(); k++) {
+    if (re) re[k] = p.msg[k].real();
+    if (im) im[k] = p.msg[k].imag();
+  }
+  return CHD_OK;
+}
+
+int chd_boot_run(chd_context *ctx, chd_boot *b, chd_ciphertext *res, const chd_ciphertext *in, const chd_evk_map *keys) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(b);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(in);
+  CHD_NOTNULL(keys);
+  if (!keys->mult || !keys->conj) return fail(CHD_ERR_KEY, "chd_boot_run: multiplication and conjugation keys required");
+  if (res == in) {
+    DeviceCt tmp;
+    int rc = ctx->c->boot_run(b->plan, tmp, in->ct, *keys->mult, *keys->conj, keys->rot, &b->regs);
+    if (rc != CHD_OK) return rc;
+    std::swap(res->ct.bx, tmp.bx);
+    std::swap(res->ct.ax, tmp.ax);
+    std::swap(res->ct.rx, tmp.rx);
+    std::swap(res->ct.cap_words, tmp.cap_words);
+    std::swap(res->ct.owned, tmp.owned);
+    res->ct.np = tmp.np;
+    res->ct.has_rx = false;
+    res->ct.scale = tmp.scale;
+    res->ct.num_slots = tmp.num_slots;
+    return CHD_OK;
+  }
+  return ctx->c->boot_run(b->plan, res->ct, in->ct, *keys->mult, *keys->conj, keys->rot, &b->regs);
 }
 
 int chd_relinearize(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *key) {

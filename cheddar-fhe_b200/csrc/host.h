@@ -247,6 +247,17 @@ struct Program {
   int reg() { return nregs++; }
 };
 
+// A prepared bootstrapping (BootContext + EvalSpecialFFT + EvalMod for one
+// slot count): the CtS then StC linear transforms and the Boot program.
+struct BootPlan {
+  int num_slots = 0, max_level = 0, cts_start = 0, em_start = 0, stc_start = 0, end_level = 0, log_scaleup = 0;
+  double cts_const = 0, stc_const = 0, em_start_scale = 0, em_end_scale = 0, final_scale = 0;
+  std::vector<LTPlan> lts;
+  std::vector<const LTPlan *> lt_ptrs;
+  Program prog;
+  std::vector<int> rotations;  // rotation keys the transforms use
+};
+
 // EvalMod cosine polynomial of the reference's BootParameter
 const std::vector<double> &boot_mod_coefficients();
 
@@ -385,6 +396,13 @@ class Context {
   Status run_program(const Program &prog, std::vector<DeviceCt> &regs, const DeviceEvk *mult_key,
                      const DeviceEvk *conj_key, const RotKeys *rot_keys, const std::vector<const LTPlan *> *lts);
   bool mult_unsafe_compatible(int l1, int l2) const;
+  // BootContext (bootplan.cu): prepare full-slot bootstrapping with
+  // num_cts / num_stc levels for CoeffToSlot / SlotToCoeff
+  Status boot_build(int num_slots, int num_cts, int num_stc, int log_msg_ratio, BootPlan *out);
+  // BootContext::Boot: in at level 0 -> res at the end level.  regs_io,
+  // when given, keeps the program registers allocated across calls.
+  Status boot_run(const BootPlan &bp, DeviceCt &res, const DeviceCt &in, const DeviceEvk &mult_key,
+                  const DeviceEvk &conj_key, const RotKeys &rot_keys, std::vector<DeviceCt> *regs_io);
 
   // ---- optional device timing of the fused key-switch stages ----
   // Events recorded on the context stream around each stage's launches.

@@ -109,6 +109,36 @@ def rational_params(log_n=16):
     }
 
 
+def boot_params(log_n=16):
+    """The shape of the reference's bootparam_30.json: two ~20-bit base
+    primes (level 0 and the level -1 base), 22 primes near 2^30 (one per
+    level), then 12 levels of two primes near 2^29 each (the CoeffToSlot
+    and EvalMod levels), 12 auxiliary primes; 4 CtS and 3 StC levels.  The
+    secret is sparse (Hamming weight 32) and sparse-secret encapsulation is
+    off (dense = sparse weight)."""
+    used = set()
+    aux = primes_near((1 << 31) - 1, 12, used, -1)
+    base = primes_near(1 << 20, 2, used, +1)
+    mid = alternating(1 << 30, 22, used)
+    top = alternating(1 << 29, 24, used)
+    levels = [[k, 0] for k in range(2, 25)] + [[k, 0] for k in range(26, 49, 2)]
+    return {
+        "log_degree": log_n,
+        "log_default_scale": 30,
+        "boot": True,
+        "dense_hamming_weight": 32,
+        "sparse_hamming_weight": 32,
+        "num_cts_levels": 4,
+        "num_stc_levels": 3,
+        "terminal_primes": [],
+        "main_primes": base + mid + top,
+        "auxiliary_primes": aux,
+        "default_encryption_level": 22,
+        "level_config": levels,
+        "additional_base": [0, 0],
+    }
+
+
 def main():
     here = os.path.dirname(os.path.abspath(__file__))
     files = {
@@ -117,6 +147,8 @@ def main():
         # small: L = 8 + alpha = 3 (beta = 3, ragged last digit)
         "keyswitch_l8_a3.json": keyswitch_params(8, 3),
         "rational_t4_m10_a6.json": rational_params(),
+        # bootstrapping: 48 q primes (max level 34) + alpha = 12 aux primes
+        "boot_l34_a12.json": boot_params(),
     }
     for name, obj in files.items():
         with open(os.path.join(here, name), "w") as f:

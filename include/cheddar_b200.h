@@ -238,6 +238,28 @@ int chd_program_json(const chd_program *p, char *buf, size_t cap, size_t *len);
 int chd_program_run(chd_context *ctx, const chd_program *p, chd_ciphertext *res, const chd_ciphertext *in,
                     const chd_evk_map *keys);
 
+/* BootContext (src/extension/BootContext.cpp) for one slot count:
+ * PrepareEvalMod + PrepareEvalSpecialFFT (EvalSpecialFFT.cpp) with
+ * num_cts_levels / num_stc_levels (BootParameter; log_message_ratio 5 in
+ * the reference), then Boot (full slots, BootVariant::kNormal, no
+ * sparse-secret encapsulation): in at level 0 -> res at the end level
+ * (StC start - num_stc_levels).  Keys: the multiplication and conjugation
+ * keys and every rotation chd_boot_rotations lists, at the top level.
+ * chd_boot_levels: {CtS start, EvalMod start, StC start, end level,
+ * log2 scale-up} and {CtS constant, StC constant, EvalMod start scale,
+ * EvalMod end scale, final scale}.  chd_boot_json / _lt_info / _lt_pt
+ * export the compiled program and the transforms' plaintext maps. */
+typedef struct chd_boot chd_boot;
+int chd_boot_create(chd_context *ctx, int num_slots, int num_cts_levels, int num_stc_levels, int log_message_ratio,
+                    chd_boot **out);
+void chd_boot_destroy(chd_boot *b);
+int chd_boot_rotations(const chd_boot *b, int *out, int cap, int *count);
+int chd_boot_levels(const chd_boot *b, int *levels, double *scales);
+int chd_boot_json(const chd_boot *b, char *buf, size_t cap, size_t *len);
+int chd_boot_lt_info(const chd_boot *b, int i, int *level, double *scale, int *npts, int *width);
+int chd_boot_lt_pt(const chd_boot *b, int i, int j, int *gs, int *bs, double *re, double *im);
+int chd_boot_run(chd_context *ctx, chd_boot *b, chd_ciphertext *res, const chd_ciphertext *in, const chd_evk_map *keys);
+
 /* Batched kernel::ModSwitchMatrixMult: npoly polynomials, each K centred
  * source limbs [K][N] (xt_dev + i*K*N) -> M limbs [M][N] (out_dev + i*M*N),
  * same table and result as chd_bconv_raw.  engine CHD_BCONV_CUDA_CORE runs

@@ -1,0 +1,63 @@
+"""Full-slot bootstrapping (BootContext::Boot, src/extension/BootContext.cpp:
+scale-up, ModUpToMax, CoeffToSlot, EvalMod on the real and imaginary parts,
+SlotToCoeff) on the bootstrapping parameter set at N = 2^12 (2048 slots):
+the GPU result equals the oracle running the same compiled program on its
+own primitives, bit for bit, and decrypts to the input message (slots
+uniform in [-1, 1] x [-1, 1]; precision reported in bits)."""
+import functools
+
+import numpy as np
+import pytest
+
+import cheddar_b200 as chd
+from boot_oracle import Ct, run_program
+from gpu_common import pair
+
+pytestmark = pytest.mark.gpu
+BOOT = "boot_l34_a12.json"
+LOGN = 12
+
+
+@functools.lru_cache(maxsize=None)
+def _setup():
+    o, g = pair(BOOT, LOGN)
+    bc = chd.BootContext(g)
+    s = o.gen_secret(99, 32)
+    mk = o.gen_mult_key(77, s)
+    ck = o.gen_conj_key(78, s)
+    rks = {r: o.gen_rot_key(1000 + r, s, r) for r in bc.rotations()}
+    keys = chd.EvkMap(g)
+    keys.set_mult(g.evk(*mk))
+    keys.set_conjugation(g.evk(*ck))
+    for r, k in rks.items():
+        keys.set_rotation(r, g.evk(*k))
+    return o, g, bc, s, mk, ck, rks, keys
+
+
+def test_boot_levels(cuda_ok):
+    o, g, bc, *_ = _setup()
+    assert bc.cts_start == o.max_level == 34
+    assert (bc.eval_mod_start, bc.stc_start, bc.end_level) == (30, 22, 19)
+    assert bc.log_scaleup >= 0
+
+
+def test_boot_bit_exact_and_precision(cuda_ok):
+    o, g, bc, s, mk, ck, rks, keys = _setup()
+    rng = np.random.default_rng(2024)
+    half = o.n // 2
+    msg = (rng.random(half) * 2 - 1) + 1j * (rng.random(half) * 2 - 1)
+    sc0 = o.scale(0)
+    bx, ax = o.encrypt(5, s, 0, o.encode(0, sc0, msg))
+    res = bc.Boot(g.import_ct(0, [bx, ax], sc0), keys)
+    parts = res.numpy()
+    ref = run_program(o, bc.json(), Ct(0, [bx, ax], sc0), mult_key=mk, conj_key=ck, rot_keys=rks,
+                      lts=bc.transforms())
+    assert ref.level == bc.end_level
+    assert np.array_equal(parts[0], ref.parts[0]) and np.array_equal(parts[1], ref.parts[1])
+    info = res.info()
+    assert abs(info["scale"] - bc.final_scale) <= 1e-9 * bc.final_scale
+    dec = o.decode(bc.end_level, bc.final_scale, o.decrypt(s, bc.end_level, parts), half)
+    err = np.abs(dec - msg).max()
+    bits = -np.log2(err)
+    print(f"bootstrapping precision: {bits:.2f} bits (max error {err:.3e})")
+    assert bits > 10, bits
