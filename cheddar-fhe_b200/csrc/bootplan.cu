@@ -301,7 +301,7 @@ Status Context::boot_run(const BootPlan &bp, DeviceCt &res, const DeviceCt &in, 
   CHD_CHECK(in.np == P->level_np(0) && !in.has_rx, kErrShape, "Boot: input must be at level 0 without Rx");
   std::vector<DeviceCt> local;
   std::vector<DeviceCt> &regs = regs_io ? *regs_io : local;
-  if (static_cast<int>(regs.size()) < bp.prog.nregs) regs.resize(bp.prog.nregs);
+  CHD_TRY(program_regs(bp.prog, regs));
   DeviceCt &r0 = regs[bp.prog.input];
   CHD_TRY(r0.reserve(in.np, false, P->n));
   const size_t bytes = static_cast<size_t>(in.np.total()) * P->n * 4;

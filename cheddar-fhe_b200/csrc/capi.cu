@@ -614,8 +614,10 @@ int chd_program_run(chd_context *ctx, const chd_program *p, chd_ciphertext *res,
   CHD_NOTNULL(res);
   CHD_NOTNULL(in);
   Context &C = *ctx->c;
-  std::vector<DeviceCt> regs(p->prog.nregs);
-  int rc = copy_ct(C, regs[p->prog.input], in->ct);
+  std::vector<DeviceCt> regs;
+  int rc = C.program_regs(p->prog, regs);
+  if (rc != CHD_OK) return rc;
+  rc = copy_ct(C, regs[p->prog.input], in->ct);
   if (rc != CHD_OK) return rc;
   rc = C.run_program(p->prog, regs, keys ? keys->mult : nullptr, keys ? keys->conj : nullptr,
                      keys ? &keys->rot : nullptr, nullptr);

@@ -440,6 +440,18 @@ DeviceCt::~DeviceCt() {
   }
 }
 
+DeviceCt &DeviceCt::operator=(DeviceCt &&o) noexcept {
+  if (this != &o) {
+    if (owned) {
+      cudaFree(bx);
+      cudaFree(ax);
+      cudaFree(rx);
+    }
+    take(o);
+  }
+  return *this;
+}
+
 Status DeviceCt::reserve(const NP &want, bool want_rx, int n) {
   size_t words = static_cast<size_t>(want.total()) * n;
   if (!owned) {
@@ -1824,7 +1836,7 @@ Status Context::permute(DeviceCt &res, const DeviceCt &a, int amount) {
 
 // Temporary ciphertext carved from the arena (released with the enclosing
 // ArenaScope; stream order makes the reuse safe).
-static Status scratch_ct(Arena &arena, DeviceCt &t, const NP &np, bool rx, int n) {
+Status scratch_ct(Arena &arena, DeviceCt &t, const NP &np, bool rx, int n) {
   const size_t words = static_cast<size_t>(np.total()) * n;
   t.owned = false;
   t.bx = static_cast<uint32_t *>(arena.alloc(words * 4));

@@ -122,8 +122,29 @@ struct DeviceCt {
   uint32_t *bx = nullptr, *ax = nullptr, *rx = nullptr;
   size_t cap_words = 0;  // allocated words per part
   bool owned = true;
+  DeviceCt() = default;
+  DeviceCt(const DeviceCt &) = delete;
+  DeviceCt &operator=(const DeviceCt &) = delete;
+  // moves transfer the buffers (containers of ciphertexts may reallocate)
+  DeviceCt(DeviceCt &&o) noexcept { take(o); }
+  DeviceCt &operator=(DeviceCt &&o) noexcept;
   ~DeviceCt();
   Status reserve(const NP &np, bool rx, int n);
+
+ private:
+  void take(DeviceCt &o) noexcept {
+    np = o.np;
+    has_rx = o.has_rx;
+    scale = o.scale;
+    num_slots = o.num_slots;
+    bx = o.bx;
+    ax = o.ax;
+    rx = o.rx;
+    cap_words = o.cap_words;
+    owned = o.owned;
+    o.bx = o.ax = o.rx = nullptr;
+    o.cap_words = 0;
+  }
 };
 
 struct DeviceEvk {
@@ -261,6 +282,10 @@ struct BootPlan {
 // EvalMod cosine polynomial of the reference's BootParameter
 const std::vector<double> &boot_mod_coefficients();
 
+// A ciphertext whose buffers come from the arena (not owned; released with
+// the enclosing ArenaScope)
+Status scratch_ct(Arena &arena, DeviceCt &t, const NP &np, bool rx, int n);
+
 // Releases everything allocated from the arena inside a scope.
 struct ArenaScope {
   Arena &a;
@@ -396,6 +421,8 @@ class Context {
   Status run_program(const Program &prog, std::vector<DeviceCt> &regs, const DeviceEvk *mult_key,
                      const DeviceEvk *conj_key, const RotKeys *rot_keys, const std::vector<const LTPlan *> *lts);
   bool mult_unsafe_compatible(int l1, int l2) const;
+  // sizes the registers of a program (plus two spares) at top-level capacity
+  Status program_regs(const Program &prog, std::vector<DeviceCt> &regs);
   // BootContext (bootplan.cu): prepare full-slot bootstrapping with
   // num_cts / num_stc levels for CoeffToSlot / SlotToCoeff
   Status boot_build(int num_slots, int num_cts, int num_stc, int log_msg_ratio, BootPlan *out);

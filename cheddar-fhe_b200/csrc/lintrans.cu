@@ -337,6 +337,8 @@ Status Context::lt_evaluate(DeviceCt &res, const DeviceCt &in, const LTPlan &pl,
   } else {
     // baby steps (Hoist.cu:578-691)
     std::vector<DeviceCt> bs(pl.bs_idx.size());
+    for (size_t i = 0; i < pl.bs_idx.size(); i++)
+      if (pl.bs_idx[i] != 0) CHD_TRY(scratch_ct(arena, bs[i], qp, false, n));
     std::vector<int> rot_d;
     std::vector<const DeviceEvk *> rot_k;
     std::vector<DeviceCt *> rot_o;

@@ -33,10 +33,28 @@ const uint32_t *part_of(const DeviceCt &c, int p) { return p == 0 ? c.bx : (p ==
 
 }  // namespace
 
+Status Context::program_regs(const Program &prog, std::vector<DeviceCt> &regs) {
+  // registers plus two spares, all at top-level capacity with an Rx part,
+  // so that no op reallocates (a reallocation synchronises the device).
+  // Registers that already have the capacity keep their contents.
+  if (static_cast<int>(regs.size()) < prog.nregs + 2) regs.resize(prog.nregs + 2);
+  const NP top = P->level_np(P->max_level);
+  const size_t words = static_cast<size_t>(top.total()) * P->n;
+  for (auto &r : regs) {
+    if (r.cap_words < words || !r.rx) {
+      CHD_CHECK(r.cap_words == 0, kErrInvalidArg, "program: register would lose its contents");
+      CHD_TRY(r.reserve(top, true, P->n));
+      r.np = NP{};
+      r.has_rx = false;
+    }
+  }
+  return kOk;
+}
+
 Status Context::run_program(const Program &prog, std::vector<DeviceCt> &regs, const DeviceEvk *mult_key,
                             const DeviceEvk *conj_key, const RotKeys *rot_keys,
                             const std::vector<const LTPlan *> *lts) {
-  CHD_CHECK(static_cast<int>(regs.size()) >= prog.nregs, kErrInvalidArg, "program: too few registers");
+  CHD_TRY(program_regs(prog, regs));
   const int n = P->n;
   // constants: Montgomery residues over their own level's q primes
   std::vector<std::vector<uint32_t>> cx(prog.consts.size());
@@ -46,7 +64,7 @@ Status Context::run_program(const Program &prog, std::vector<DeviceCt> &regs, co
     encode_const(c.level, c.scale, c.value, 0, &cx[i]);
     cnp[i] = P->level_np(c.level);
   }
-  DeviceCt spare, spare2;
+  DeviceCt &spare = regs[prog.nregs], &spare2 = regs[prog.nregs + 1];
   // dst (parts) = sum over terms of src_t (.) c_t, at np, each term reading
   // its source from row `front_t`
   struct Term {
