@@ -16,6 +16,9 @@ Reported (one JSON line on rank 0):
              CUDA events on the context stream around its launches (a
              second pass of the same steps), algorithmic bytes per launch
   cpu_baseline  the CPU oracle's HMult on the host cores (bounded sample)
+  bootstrap  full-slot bootstrapping throughput at N = 2^16 (bootstraps/s;
+             --boot-precision adds a real-key run with decoded precision)
+  bconv_engines  base conversion on CUDA cores vs tcgen05 tensor cores
 `--impl reference` times the CPU implementation of the path (the oracle;
 the reference itself has no CPU path and cannot be built here) on the same
 configuration.
@@ -151,6 +154,11 @@ def main():
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-boot", action="store_true", help="skip the bootstrapping measurement")
+    ap.add_argument("--boot-batch", type=int, default=8)
+    ap.add_argument("--boot-precision", action="store_true",
+                    help="also bootstrap one ciphertext with real keys (oracle key generation, slow) "
+                         "and report decoded precision in bits")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -238,6 +246,9 @@ def main():
     # ---- base conversion as a dense contraction: CUDA cores vs tensor cores ----
     bconv_cmp = bconv_engines(ctx, chd, stream)
 
+    # ---- full-slot bootstrapping at N = 2^16 ----
+    boot = None if args.no_boot else boot_bench(chd, args, stream, dist)
+
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -247,6 +258,7 @@ def main():
                    "l2": "inputs larger than L2 (batch x 24 MB + 48 MB key)",
                    "parallelism": f"replicas x{world}"},
         "e2e": e2e, "roofline": roof, "clocks": sampler.summary(), "bconv_engines": bconv_cmp,
+        "bootstrap": boot,
         "gpu_launches": launches,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -451,6 +463,123 @@ def bconv_engines(ctx, chd, stream, npoly=64, reps=10):
         row["speedup_tensor_vs_cuda_core"] = row["cuda_core"]["ms"] / row["tensor_core"]["ms"]
         res[name] = row
     return res
+
+
+BOOT_PARAM_FILE = "boot_l34_a12.json"
+
+
+def boot_bench(chd, args, stream, dist):
+    """Full-slot bootstrapping (N = 2^16, 2^15 slots; 48 q primes with the
+    reference's bootparam_30 level shape, alpha = 12, 4 CoeffToSlot and 3
+    SlotToCoeff levels, EvalMod with the reference's cosine polynomial and 3
+    double angles).  A step bootstraps a batch of level-0 ciphertexts one
+    after the other; CUDA events on the context stream, inputs resident.
+    The evaluation keys are uniform random residues (the work is that of
+    real keys; decoded precision is measured with real keys by the tests
+    and by --boot-precision)."""
+    import torch
+    params = json.load(open(os.path.join(chd.PARAM_DIR, BOOT_PARAM_FILE)))
+    ctx = chd.Context(json.dumps(params), device=torch.cuda.current_device())
+    ctx.set_stream(stream.cuda_stream)
+    t0 = time.time()
+    bc = chd.BootContext(ctx)
+    plan_s = time.time() - t0
+    rots = bc.rotations()
+    n, L, a = ctx.n, ctx.L, ctx.alpha
+    beta = -(-L // a)
+    allp = torch.tensor(list(reversed(params.get("terminal_primes", []))) + params["main_primes"] +
+                        params["auxiliary_primes"], dtype=torch.int64, device="cuda")
+    gen = torch.Generator(device="cuda").manual_seed(4321)
+
+    def uniform(rows_gidx):
+        q = allp[torch.tensor(rows_gidx, device="cuda", dtype=torch.int64)][:, None]
+        r = torch.randint(0, 2 ** 62, (len(rows_gidx), n), generator=gen, device="cuda", dtype=torch.int64)
+        return (r % q).to(torch.int32)
+
+    kg = list(ctx.gidx(*ctx.level_np(ctx.max_level), a))
+    keys = chd.EvkMap(ctx)
+    held = []
+
+    def ukey():
+        kb = torch.stack([uniform(kg) for _ in range(beta)]).contiguous()
+        ka = torch.stack([uniform(kg) for _ in range(beta)]).contiguous()
+        k = chd.EvaluationKey(ctx, kb, ka, on_device=True)
+        held.append(k)
+        return k
+
+    keys.set_mult(ukey())
+    keys.set_conjugation(ukey())
+    for r in rots:
+        keys.set_rotation(r, ukey())
+    g0 = list(ctx.gidx(*ctx.level_np(0), 0))
+    B = args.boot_batch
+    ins = [ctx.import_ct(0, [uniform(g0), uniform(g0)], on_device=True, scale=ctx.scale(0)) for _ in range(B)]
+    outs = [chd.Ciphertext(ctx) for _ in range(B)]
+    torch.cuda.synchronize()
+
+    def step():
+        for i in range(B):
+            bc.Boot(ins[i], keys, res=outs[i])
+
+    for _ in range(2):
+        step()
+    ctx.synchronize()
+    steps = max(1, min(args.steps, 5))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    world = 1
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        world = dist.get_world_size()
+    res = {"metric": "bootstraps/s (full slots, N=2^16)", "value": world * B * steps / (ms / 1e3),
+           "unit": "bootstraps/s", "ms_per_boot": ms / (B * steps), "batch_per_gpu": B, "steps": steps,
+           "warmup": 2, "params": "48 q primes (bootparam_30 level shape), alpha=12, 4 CtS + 3 StC levels, "
+                                  "EvalMod deg-30 Chebyshev cosine + 3 double angles",
+           "rotation_keys": len(rots), "plan_seconds": plan_s,
+           "keys": "uniform random residues (same work as real keys)",
+           "levels": {"cts_start": bc.cts_start, "eval_mod_start": bc.eval_mod_start,
+                      "stc_start": bc.stc_start, "end": bc.end_level}}
+    if args.boot_precision:
+        res["precision"] = boot_precision(chd, ctx, bc, params)
+    del ins, outs, keys, held
+    ctx.close()
+    return res
+
+
+def boot_precision(chd, ctx, bc, params):
+    """One bootstrap with real keys (oracle key generation): decoded
+    precision in bits against the input slots (uniform in [-1, 1]^2)."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    o = po.Oracle(params)
+    s = o.gen_secret(99, 32)
+    keys = chd.EvkMap(ctx)
+    held = [ctx.evk(*o.gen_mult_key(77, s)), ctx.evk(*o.gen_conj_key(78, s))]
+    keys.set_mult(held[0])
+    keys.set_conjugation(held[1])
+    for r in bc.rotations():
+        k = ctx.evk(*o.gen_rot_key(1000 + r, s, r))
+        held.append(k)
+        keys.set_rotation(r, k)
+    rng = np.random.default_rng(2024)
+    msg = (rng.random(o.n // 2) * 2 - 1) + 1j * (rng.random(o.n // 2) * 2 - 1)
+    bx, ax = o.encrypt(5, s, 0, o.encode(0, o.scale(0), msg))
+    r = bc.Boot(ctx.import_ct(0, [bx, ax], o.scale(0)), keys)
+    dec = o.decode(bc.end_level, bc.final_scale, o.decrypt(s, bc.end_level, r.numpy()), o.n // 2)
+    err = float(np.abs(dec - msg).max())
+    return {"bits": -float(np.log2(err)), "max_abs_error": err, "slots": o.n // 2}
 
 
 KERNEL_OF_STAGE = {
