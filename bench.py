@@ -246,6 +246,9 @@ def main():
     # ---- base conversion as a dense contraction: CUDA cores vs tensor cores ----
     bconv_cmp = bconv_engines(ctx, chd, stream)
 
+    # ---- hoisted rotations and a mixed-level batch ----
+    hoist_mixed = hoist_mixed_bench(ctx, chd, key, uniform, stream)
+
     # ---- full-slot bootstrapping at N = 2^16 ----
     boot = None if args.no_boot else boot_bench(chd, args, stream, dist)
 
@@ -258,7 +261,7 @@ def main():
                    "l2": "inputs larger than L2 (batch x 24 MB + 48 MB key)",
                    "parallelism": f"replicas x{world}"},
         "e2e": e2e, "roofline": roof, "clocks": sampler.summary(), "bconv_engines": bconv_cmp,
-        "bootstrap": boot,
+        "bootstrap": boot, "hoisted_and_mixed": hoist_mixed,
         "gpu_launches": launches,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -462,6 +465,98 @@ def bconv_engines(ctx, chd, stream, npoly=64, reps=10):
         res["engines_equal"] = res["engines_equal"] and bool(torch.equal(outs["cuda_core"], outs["tensor_core"]))
         row["speedup_tensor_vs_cuda_core"] = row["cuda_core"]["ms"] / row["tensor_core"]["ms"]
         res[name] = row
+    return res
+
+
+def hoist_mixed_bench(ctx, chd, key, uniform, stream, reps=5):
+    """(i) One ciphertext at the top level rotated by the 30 distinct offsets
+    {+-2^k, k < 15} u {1..4} mod 2^15: all rotations of one ModUp in one
+    launch (HoistedRotate, results in Q u P, then ModDown) against 30
+    separate HRot calls.  (ii) 16 HMult+relin+rescale pairs at levels drawn
+    uniformly from 5..22 (seed 0; 22 is this set's top level): one HMult
+    call per pair, the batched call (one fused pipeline per level), and the
+    batched call captured once in a CUDA graph and replayed.  Keys are
+    uniform random residues; CUDA events on the context stream."""
+    import numpy as np
+    import torch
+    n, L, a = ctx.n, ctx.L, ctx.alpha
+    beta = -(-L // a)
+    lvl = ctx.max_level
+    kg = torch.tensor(ctx.gidx(*ctx.level_np(lvl), a), device="cuda", dtype=torch.int64)
+    offsets = sorted({(1 << k) % (n // 2) for k in range(15)} | {(-(1 << k)) % (n // 2) for k in range(15)} |
+                     {1, 2, 3, 4})
+    keys = []
+    for _ in offsets:
+        kb = torch.stack([uniform(len(kg), kg) for _ in range(beta)]).contiguous()
+        ka = torch.stack([uniform(len(kg), kg) for _ in range(beta)]).contiguous()
+        keys.append(chd.EvaluationKey(ctx, kb, ka, on_device=True))
+    qg = torch.tensor(ctx.gidx(*ctx.level_np(lvl), 0), device="cuda", dtype=torch.int64)
+    ct = ctx.import_ct(lvl, [uniform(len(qg), qg), uniform(len(qg), qg)], on_device=True)
+    qp_outs = [chd.Ciphertext(ctx) for _ in offsets]
+    outs = [chd.Ciphertext(ctx) for _ in offsets]
+
+    def timed(fn):
+        for _ in range(2):
+            fn()
+        ctx.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        ctx.synchronize()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    def hoisted():
+        ctx.HoistedRotate(ct, keys, offsets, outs=qp_outs)
+        for q, o in zip(qp_outs, outs):
+            ctx.ModDown(q, res=o)
+
+    def separate():
+        for k, r, o in zip(keys, offsets, outs):
+            ctx.HRot(ct, k, r, res=o)
+
+    ms_h = timed(hoisted)
+    ms_s = timed(separate)
+    R = len(offsets)
+    res = {"hoisted_rotations": {
+        "workload": f"{R} rotations of one ciphertext at level {lvl} (N=2^16, L=24, alpha=8)",
+        "offsets": R, "hoisted_ms": ms_h, "separate_ms": ms_s,
+        "hoisted_rotations_per_s": R / (ms_h / 1e3), "separate_rotations_per_s": R / (ms_s / 1e3),
+        "speedup": ms_s / ms_h}}
+    del keys, qp_outs, outs
+    # (ii) mixed-level batch
+    levels = [int(x) for x in np.random.default_rng(0).integers(5, 23, 16)]
+
+    def ct_at(level):
+        g = torch.tensor(ctx.gidx(*ctx.level_np(level), 0), device="cuda", dtype=torch.int64)
+        return ctx.import_ct(level, [uniform(len(g), g), uniform(len(g), g)], on_device=True)
+
+    A = [ct_at(x) for x in levels]
+    Bc = [ct_at(x) for x in levels]
+    outs = [chd.Ciphertext(ctx) for _ in levels]
+
+    def one_by_one():
+        for x, y, o in zip(A, Bc, outs):
+            ctx.HMult(x, y, key, rescale=True, res=o)
+
+    def batched():
+        ctx.HMultBatch(A, Bc, key, rescale=True, res_list=outs)
+
+    ms_1 = timed(one_by_one)
+    ms_b = timed(batched)
+    ctx.synchronize()
+    ctx.graph_begin()
+    batched()
+    graph = ctx.graph_end()
+    ms_g = timed(graph.launch)
+    del graph
+    res["mixed_level_batch"] = {
+        "workload": "16 HMult+relin+rescale pairs, levels U(5..22) seed 0, N=2^16, alpha=8",
+        "levels": levels, "one_by_one_ms": ms_1, "batched_ms": ms_b, "graph_ms": ms_g,
+        "hmult_per_s": {"one_by_one": 16 / (ms_1 / 1e3), "batched": 16 / (ms_b / 1e3),
+                        "graph": 16 / (ms_g / 1e3)}}
     return res
 
 

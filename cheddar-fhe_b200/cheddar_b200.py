@@ -128,6 +128,10 @@ def lib():
         "chd_boot_lt_info": (i, [vp, i, C.POINTER(i), C.POINTER(d), C.POINTER(i), C.POINTER(i)]),
         "chd_boot_lt_pt": (i, [vp, i, i, C.POINTER(i), C.POINTER(i), vp, vp]),
         "chd_boot_run": (i, [vp, vp, vp, vp, vp]),
+        "chd_graph_begin": (i, [vp]),
+        "chd_graph_end": (i, [vp, pp]),
+        "chd_graph_launch": (i, [vp, vp]),
+        "chd_graph_destroy": (None, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -193,6 +197,15 @@ class Context:
 
     def synchronize(self):
         _check(lib().chd_context_synchronize(self.ptr))
+
+    def graph_begin(self):
+        """Start capturing the GPU work of the following calls (see Graph)."""
+        _check(lib().chd_graph_begin(self.ptr))
+
+    def graph_end(self):
+        g = C.c_void_p()
+        _check(lib().chd_graph_end(self.ptr, C.byref(g)))
+        return Graph(self, g)
 
     def stage_timing(self, enable):
         """Start (clearing earlier records) or stop device timing of the fused
@@ -411,6 +424,26 @@ class Context:
         d = np.ascontiguousarray(dst_gidx, dtype=np.int32)
         _check(lib().chd_bconv_batch(self.ptr, engine, npoly, _ptr(xt), s.ctypes.data, len(s), d.ctypes.data,
                                      len(d), _ptr(out)))
+
+
+class Graph:
+    """A captured CUDA graph of library calls; launch() replays it on the
+    context stream over the same buffers."""
+
+    def __init__(self, ctx, ptr):
+        self.ctx = ctx
+        self.ptr = ptr
+
+    def launch(self):
+        _check(lib().chd_graph_launch(self.ctx.ptr, self.ptr))
+
+    def __del__(self):
+        try:
+            if self.ptr.value:
+                lib().chd_graph_destroy(self.ptr)
+                self.ptr = C.c_void_p()
+        except Exception:
+            pass
 
 
 class EvkMap:

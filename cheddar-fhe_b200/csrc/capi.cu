@@ -29,6 +29,14 @@ struct chd_boot {
   BootPlan plan;
   std::vector<DeviceCt> regs;  // program registers kept across calls
 };
+struct chd_graph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  ~chd_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+  }
+};
 struct chd_program {
   Program prog;
   double start_scale = 0, end_scale = 0;
@@ -730,6 +738,41 @@ int chd_boot_run(chd_context *ctx, chd_boot *b, chd_ciphertext *res, const chd_c
   }
   return ctx->c->boot_run(b->plan, res->ct, in->ct, *keys->mult, *keys->conj, keys->rot, &b->regs);
 }
+
+int chd_graph_begin(chd_context *ctx) {
+  CHD_NOTNULL(ctx);
+  Context &C = *ctx->c;
+  if (!C.stream) return fail(CHD_ERR_INVALID_ARG, "chd_graph_begin: capture needs a non-default context stream");
+  cudaError_t e = cudaStreamBeginCapture(C.stream, cudaStreamCaptureModeRelaxed);
+  if (e != cudaSuccess) return fail(CHD_ERR_CUDA, std::string("chd_graph_begin: ") + cudaGetErrorString(e));
+  return CHD_OK;
+}
+
+int chd_graph_end(chd_context *ctx, chd_graph **out) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(out);
+  Context &C = *ctx->c;
+  auto *g = new chd_graph();
+  cudaError_t e = cudaStreamEndCapture(C.stream, &g->graph);
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+  if (e != cudaSuccess) {
+    delete g;
+    cudaGetLastError();
+    return fail(CHD_ERR_CUDA, std::string("chd_graph_end: ") + cudaGetErrorString(e));
+  }
+  *out = g;
+  return CHD_OK;
+}
+
+int chd_graph_launch(chd_context *ctx, const chd_graph *g) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(g);
+  cudaError_t e = cudaGraphLaunch(g->exec, ctx->c->stream);
+  if (e != cudaSuccess) return fail(CHD_ERR_CUDA, std::string("chd_graph_launch: ") + cudaGetErrorString(e));
+  return CHD_OK;
+}
+
+void chd_graph_destroy(chd_graph *g) { delete g; }
 
 int chd_relinearize(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *key) {
   CHD_NOTNULL(ctx);

@@ -1641,16 +1641,32 @@ Status Context::hmult_batch(int count, DeviceCt *const *res, const DeviceCt *con
   // ModDown+Rescale) runs once for the whole batch.  Ciphertexts must share
   // a level and must not alias each other's results.
   if (count <= 0) return kOk;
-  bool uniform = true;
+  bool uniform = true, aliased = false;
   for (int i = 0; i < count; i++) {
     CHD_CHECK(a[i]->np == b[i]->np && a[i]->np.aux == 0 && !a[i]->has_rx && !b[i]->has_rx, kErrShape,
-              "HMult batch: operands must share a level, no aux primes, no rx");
+              "HMult batch: each pair must share a level, no aux primes, no rx");
     uniform = uniform && a[i]->np == a[0]->np;
     for (int j = 0; j < count; j++)
-      if (res[i] == a[j] || res[i] == b[j]) uniform = false;  // aliasing: run one by one
+      if (res[i] == a[j] || res[i] == b[j]) aliased = true;
+  }
+  if (aliased) {  // results overwrite operands of other pairs: one by one
+    for (int i = 0; i < count; i++) CHD_TRY(hmult(*res[i], *a[i], *b[i], key, rescale));
+    return kOk;
   }
   if (!uniform) {
-    for (int i = 0; i < count; i++) CHD_TRY(hmult(*res[i], *a[i], *b[i], key, rescale));
+    // mixed levels: one batched pipeline per level, in level order
+    std::map<int, std::vector<int>> by_level;
+    for (int i = 0; i < count; i++) by_level[-level_of(*P, *a[i])].push_back(i);
+    for (const auto &e : by_level) {
+      std::vector<DeviceCt *> r;
+      std::vector<const DeviceCt *> x, y;
+      for (int i : e.second) {
+        r.push_back(res[i]);
+        x.push_back(a[i]);
+        y.push_back(b[i]);
+      }
+      CHD_TRY(hmult_batch(static_cast<int>(r.size()), r.data(), x.data(), y.data(), key, rescale));
+    }
     return kOk;
   }
   const int level = level_of(*P, *a[0]);

@@ -133,7 +133,8 @@ int chd_mult_key(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a,
 int chd_hmult(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a,
               const chd_ciphertext *b, const chd_evk *mult_key, int rescale);
 /* Batched HMult over count independent pairs (no reference counterpart; the
- * reference exposes one HMult per call) */
+ * reference exposes one HMult per call).  Pairs at different levels run as
+ * one batched pipeline per level. */
 int chd_hmult_batch(chd_context *ctx, int count, chd_ciphertext *const *res,
                     const chd_ciphertext *const *a, const chd_ciphertext *const *b,
                     const chd_evk *mult_key, int rescale);
@@ -259,6 +260,19 @@ int chd_boot_json(const chd_boot *b, char *buf, size_t cap, size_t *len);
 int chd_boot_lt_info(const chd_boot *b, int i, int *level, double *scale, int *npts, int *width);
 int chd_boot_lt_pt(const chd_boot *b, int i, int j, int *gs, int *bs, double *re, double *im);
 int chd_boot_run(chd_context *ctx, chd_boot *b, chd_ciphertext *res, const chd_ciphertext *in, const chd_evk_map *keys);
+
+/* CUDA graphs of library calls (no reference counterpart; the reference
+ * issues every kernel from the host).  chd_graph_begin starts capturing the
+ * GPU work of the following calls on the context stream; chd_graph_end
+ * instantiates it; chd_graph_launch replays it on the context stream,
+ * reading and writing the same buffers.  Calls made while capturing must
+ * not allocate or wait: run the same calls once before capturing so that
+ * results and scratch are already sized. */
+typedef struct chd_graph chd_graph;
+int chd_graph_begin(chd_context *ctx);
+int chd_graph_end(chd_context *ctx, chd_graph **out);
+int chd_graph_launch(chd_context *ctx, const chd_graph *g);
+void chd_graph_destroy(chd_graph *g);
 
 /* Batched kernel::ModSwitchMatrixMult: npoly polynomials, each K centred
  * source limbs [K][N] (xt_dev + i*K*N) -> M limbs [M][N] (out_dev + i*M*N),
