@@ -128,8 +128,9 @@ __global__ void __launch_bounds__(128) k_modswitch_cols(const __grid_constant__ 
 
 size_t modswitch_cols_smem(int kmax) { return (static_cast<size_t>(kExRows) * kTC + static_cast<size_t>(kmax) * 128 * kTC) * 4; }
 
-void launch_modswitch_cols(const MSColBatch &b, int log_n, cudaStream_t s) {
-  if (b.count <= 0 || log_n != 16) return;
+namespace {
+
+void launch_batch(const MSColBatch &b, cudaStream_t s) {
   int max_k = 0;
   for (int j = 0; j < b.count; j++) max_k = b.jobs[j].K > max_k ? b.jobs[j].K : max_k;
   const dim3 grid(512 / kTC, b.count);
@@ -146,6 +147,61 @@ void launch_modswitch_cols(const MSColBatch &b, int log_n, cudaStream_t s) {
     cudaFuncSetAttribute(k_modswitch_cols<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm));
     k_modswitch_cols<16><<<grid, 128, sm, s>>>(b);
   }
+}
+
+int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
+}  // namespace
+
+void launch_modswitch_cols(const MSColBatch &b, int log_n, cudaStream_t s) {
+  if (b.count <= 0 || log_n != 16) return;
+  // A small batch (one ciphertext: a few jobs x 32 column tiles) leaves
+  // most SMs idle.  Spread each job's targets over `groups` sub-jobs (each
+  // repeats the job's INTT column stages for its own subset of targets) so
+  // that the grid covers about two CTAs per SM; at least 4 targets each.
+  const int tiles = 512 / kTC;
+  const int want = 2 * sm_count();
+  int max_m = 0;
+  for (int j = 0; j < b.count; j++) max_m = b.jobs[j].M > max_m ? b.jobs[j].M : max_m;
+  int groups = (want + tiles * b.count - 1) / (tiles * b.count);
+  groups = groups < 1 ? 1 : groups;
+  const int by_m = max_m / 4 > 1 ? max_m / 4 : 1;
+  groups = groups > by_m ? by_m : groups;
+  if (groups == 1) {
+    launch_batch(b, s);
+    return;
+  }
+  MSColBatch e = b;
+  e.count = 0;
+  for (int j = 0; j < b.count; j++) {
+    const MSColJob &src = b.jobs[j];
+    for (int g = 0; g < groups; g++) {
+      const int m0 = src.M * g / groups, m1 = src.M * (g + 1) / groups;
+      if (m1 <= m0) continue;
+      MSColJob &d = e.jobs[e.count++];
+      d = src;
+      d.M = m1 - m0;
+      d.table = src.table + static_cast<size_t>(m0) * src.K;
+      for (int m = 0; m < d.M; m++) {
+        d.dst_row[m] = src.dst_row[m0 + m];
+        d.dst_gidx[m] = src.dst_gidx[m0 + m];
+      }
+      if (e.count == kMaxMSColJobs) {
+        launch_batch(e, s);
+        e.count = 0;
+      }
+    }
+  }
+  if (e.count) launch_batch(e, s);
 }
 
 }  // namespace chd
