@@ -41,25 +41,29 @@ __global__ void k_modup_to_max(const __grid_constant__ ModUpToMaxDesc d) {
 }
 
 // out[o][r] = sum_t pt[o][t][r] (.) in[t][r]  (Montgomery products, canonical)
+// One thread owns one coefficient of one row for every output, so the
+// baby-step values it reads for the first giant step are L1 hits for the
+// others.
 __global__ void k_pt_accum(const __grid_constant__ PtAccumDesc d) {
   const int r = blockIdx.y;
-  const int o = blockIdx.z;
   const uint32_t q = d.q[r];
   const int32_t qi = d.qinv[r];
   const size_t n = static_cast<size_t>(d.n);
   const size_t off = static_cast<size_t>(r) * n;
-  const PtAccumOut &out = d.out[o];
   for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-    uint32_t sb = 0, sa = 0;
-    for (int t = 0; t < out.terms; t++) {
-      const int ti = out.term[t];
-      const uint32_t m = out.pt[t][off + i];
-      sb = add_mod(sb, mont_mul(d.in_b[ti][off + i], m, q, qi), q);
-      sa = add_mod(sa, mont_mul(d.in_a[ti][off + i], m, q, qi), q);
+    for (int o = 0; o < d.outs; o++) {
+      const PtAccumOut &out = d.out[o];
+      uint32_t sb = 0, sa = 0;
+      for (int t = 0; t < out.terms; t++) {
+        const int ti = out.term[t];
+        const uint32_t m = out.pt[t][off + i];
+        sb = add_mod(sb, mont_mul(d.in_b[ti][off + i], m, q, qi), q);
+        sa = add_mod(sa, mont_mul(d.in_a[ti][off + i], m, q, qi), q);
+      }
+      out.b[off + i] = sb;
+      out.a[off + i] = sa;
     }
-    out.b[off + i] = sb;
-    out.a[off + i] = sa;
   }
 }
 
@@ -90,7 +94,7 @@ void launch_modup_to_max(const ModUpToMaxDesc &d, cudaStream_t s) {
 
 void launch_pt_accum(const PtAccumDesc &d, cudaStream_t s) {
   if (d.rows <= 0 || d.outs <= 0) return;
-  k_pt_accum<<<dim3(64, d.rows, d.outs), 256, 0, s>>>(d);
+  k_pt_accum<<<dim3(64, d.rows), 256, 0, s>>>(d);
 }
 
 void launch_const_accum(const ConstAccumDesc &d, cudaStream_t s) {

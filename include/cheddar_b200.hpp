@@ -167,10 +167,102 @@ class Context {
   void HRotAdd(Ct &res, const Ct &a, const Ct &b, const Evk &rot_key, int rot_dist) const {
     check(chd_hrot_add(c_, res.raw(), a.raw(), b.raw(), rot_key.raw(), rot_dist));
   }
+  // batched HMult over independent pairs (one fused pipeline per level)
+  void HMultBatch(const std::vector<Ct *> &res, const std::vector<const Ct *> &a,
+                  const std::vector<const Ct *> &b, const Evk &mult_key, bool rescale = true) const {
+    std::vector<chd_ciphertext *> r;
+    std::vector<const chd_ciphertext *> x, y;
+    for (size_t i = 0; i < res.size(); i++) {
+      r.push_back(res[i]->raw());
+      x.push_back(a[i]->raw());
+      y.push_back(b[i]->raw());
+    }
+    check(chd_hmult_batch(c_, static_cast<int>(r.size()), r.data(), x.data(), y.data(), mult_key.raw(),
+                          rescale ? 1 : 0));
+  }
+
+  // ---- encoder (Encoder::Encode / EncodeConstant) ----
+  // plaintext [num_q(level) + num_aux][N] at pt_dev (evaluation domain, Montgomery)
+  int Encode(uint32_t *pt_dev, int level, double scale, const std::vector<double> &re,
+             const std::vector<double> &im, int num_aux = 0) const {
+    int slots = 0;
+    check(chd_encode(c_, level, scale, re.data(), im.data(), static_cast<int>(re.size()), num_aux, pt_dev, &slots));
+    return slots;
+  }
+  std::vector<uint32_t> EncodeConstant(int level, double scale, double value, int num_aux = 0) const {
+    int m = 0, t = 0;
+    check(chd_level_np(c_, level, &m, &t));
+    std::vector<uint32_t> cx(m + t + num_aux);
+    check(chd_encode_const(c_, level, scale, value, num_aux, cx.data()));
+    return cx;
+  }
+
+  // ---- CUDA graphs of library calls ----
+  void BeginGraph() { check(chd_graph_begin(c_)); }
+  chd_graph *EndGraph() {
+    chd_graph *g = nullptr;
+    check(chd_graph_end(c_, &g));
+    return g;
+  }
+  void LaunchGraph(const chd_graph *g) { check(chd_graph_launch(c_, g)); }
 
  private:
   explicit Context(chd_context *c) : c_(c) {}
   chd_context *c_ = nullptr;
+};
+
+// EvkMap (include/core/EvkMap.h): keys by rotation index plus the
+// conjugation and multiplication keys (borrowed; they must outlive the map)
+class EvkMap {
+ public:
+  explicit EvkMap(Context &ctx) { check(chd_evk_map_create(ctx.raw(), &m_)); }
+  ~EvkMap() { chd_evk_map_destroy(m_); }
+  EvkMap(const EvkMap &) = delete;
+  EvkMap &operator=(const EvkMap &) = delete;
+  void AddRotationKey(int rot_idx, const EvaluationKey &k) { check(chd_evk_map_set_rotation(m_, rot_idx, k.raw())); }
+  void SetConjugationKey(const EvaluationKey &k) { check(chd_evk_map_set_conjugation(m_, k.raw())); }
+  void SetMultiplicationKey(const EvaluationKey &k) { check(chd_evk_map_set_mult(m_, k.raw())); }
+  chd_evk_map *raw() const { return m_; }
+
+ private:
+  chd_evk_map *m_ = nullptr;
+};
+
+// BootContext (include/extension/BootContext.h) for one slot count:
+// PrepareEvalMod + PrepareEvalSpecialFFT at construction, then Boot.
+class BootContext {
+ public:
+  BootContext(Context &ctx, int num_slots, int num_cts_levels = 4, int num_stc_levels = 3,
+              int log_message_ratio = 5)
+      : ctx_(ctx) {
+    check(chd_boot_create(ctx.raw(), num_slots, num_cts_levels, num_stc_levels, log_message_ratio, &b_));
+  }
+  ~BootContext() { chd_boot_destroy(b_); }
+  BootContext(const BootContext &) = delete;
+  BootContext &operator=(const BootContext &) = delete;
+  // AddRequiredRotations: the rotation keys the client must provide
+  std::vector<int> RequiredRotations() const {
+    int n = 0;
+    check(chd_boot_rotations(b_, nullptr, 0, &n));
+    std::vector<int> r(n);
+    check(chd_boot_rotations(b_, r.data(), n, &n));
+    return r;
+  }
+  int GetEndLevel() const {
+    int lv[5];
+    check(chd_boot_levels(b_, lv, nullptr));
+    return lv[3];
+  }
+  void ModUpToMax(Ciphertext &res, const Ciphertext &in) const {
+    check(chd_modup_to_max(ctx_.raw(), res.raw(), in.raw()));
+  }
+  void Boot(Ciphertext &res, const Ciphertext &in, const EvkMap &evk_map) {
+    check(chd_boot_run(ctx_.raw(), b_, res.raw(), in.raw(), evk_map.raw()));
+  }
+
+ private:
+  Context &ctx_;
+  chd_boot *b_ = nullptr;
 };
 
 inline Ciphertext::Ciphertext(Context &ctx) { check(chd_ct_create(ctx.raw(), &ct_)); }

@@ -1,4 +1,5 @@
-"""The header-only C++ mirror (include/cheddar_b200.hpp) compiles and links
+"""The header-only C++ mirror (include/cheddar_b200.hpp), including its
+bootstrapping classes, compiles and links
 against the C ABI library, and reports a parameter error by exception (no
 GPU needed: the JSON is rejected before any device call)."""
 import os
@@ -11,6 +12,26 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 SRC = r'''
 #include "cheddar_b200.hpp"
 #include <cstdio>
+// compiled, not run: the bootstrapping-side classes of the shim
+void unused_paths(cheddar_b200::Context &ctx, const cheddar_b200::EvaluationKey &k) {
+  cheddar_b200::EvkMap m(ctx);
+  m.SetMultiplicationKey(k);
+  m.SetConjugationKey(k);
+  m.AddRotationKey(1, k);
+  cheddar_b200::BootContext bc(ctx, 1 << 15);
+  std::vector<int> r = bc.RequiredRotations();
+  cheddar_b200::Ciphertext a(ctx), b(ctx);
+  bc.ModUpToMax(b, a);
+  bc.Boot(b, a, m);
+  std::vector<uint32_t> cx = ctx.EncodeConstant(0, 1.0, 0.5);
+  ctx.HMultBatch({&b}, {&a}, {&a}, k, true);
+  ctx.BeginGraph();
+  chd_graph *g = ctx.EndGraph();
+  ctx.LaunchGraph(g);
+  chd_graph_destroy(g);
+  (void)r;
+  (void)cx;
+}
 int main() {
   try {
     auto ctx = cheddar_b200::Context::Create("{\"log_degree\": 16}");
