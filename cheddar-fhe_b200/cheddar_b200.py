@@ -102,12 +102,15 @@ def lib():
         "chd_bconv_batch": (i, [vp, i, i, vp, i32p, i, i32p, i, vp]),
         "chd_encode": (i, [vp, i, d, vp, vp, i, i, vp, C.POINTER(i)]),
         "chd_encode_const": (i, [vp, i, d, d, i, vp]),
-        "chd_modup_to_max": (i, [vp, vp, vp]),
+        "chd_modup_to_max": (i, [vp, vp, vp, vp]),
         "chd_evk_map_create": (i, [vp, pp]),
         "chd_evk_map_destroy": (None, [vp]),
         "chd_evk_map_set_rotation": (i, [vp, i, vp]),
         "chd_evk_map_set_conjugation": (i, [vp, vp]),
         "chd_evk_map_set_mult": (i, [vp, vp]),
+        "chd_evk_map_set_dense_to_sparse": (i, [vp, vp]),
+        "chd_evk_map_set_sparse_to_dense": (i, [vp, vp]),
+        "chd_evk_create_np": (i, [vp, i, i, i, i, vp, vp, i, pp]),
         "chd_lintrans_create": (i, [vp, i, i, vp, vp, vp, i, d, i, i, i, i, pp]),
         "chd_lintrans_destroy": (None, [vp]),
         "chd_lintrans_rotations": (i, [vp, vp, i, C.POINTER(i)]),
@@ -409,10 +412,11 @@ class Context:
         _check(lib().chd_encode_const(self.ptr, level, scale, value, num_aux, out.ctypes.data))
         return out
 
-    def ModUpToMax(self, a, res=None):
-        """BootContext::ModUpToMax (no sparse-secret encapsulation)."""
+    def ModUpToMax(self, a, res=None, keys=None):
+        """BootContext::ModUpToMax; keys (EvkMap) with the dense-to-sparse and
+        sparse-to-dense keys under sparse-secret encapsulation."""
         res = res if res is not None else Ciphertext(self)
-        _check(lib().chd_modup_to_max(self.ptr, res.ptr, a.ptr))
+        _check(lib().chd_modup_to_max(self.ptr, res.ptr, a.ptr, keys.ptr if keys is not None else None))
         return res
 
     def bconv_batch(self, xt, src_gidx, dst_gidx, out, engine=BCONV_CUDA_CORE, npoly=1):
@@ -475,6 +479,14 @@ class EvkMap:
     def set_mult(self, key):
         self._keep.append(key)
         _check(lib().chd_evk_map_set_mult(self.ptr, key.ptr))
+
+    def set_dense_to_sparse(self, key):
+        self._keep.append(key)
+        _check(lib().chd_evk_map_set_dense_to_sparse(self.ptr, key.ptr))
+
+    def set_sparse_to_dense(self, key):
+        self._keep.append(key)
+        _check(lib().chd_evk_map_set_sparse_to_dense(self.ptr, key.ptr))
 
 
 class LinearTransform:
@@ -699,7 +711,10 @@ class Ciphertext:
 class EvaluationKey:
     """EvaluationKey<uint32_t>: beta pairs over the key basis [L + alpha][N]."""
 
-    def __init__(self, ctx, bx, ax, on_device=False):
+    def __init__(self, ctx, bx, ax, on_device=False, basis=None):
+        """basis = (num_main, num_ter, num_aux) for a key over another basis
+        than [L + alpha] (the dense-to-sparse key of sparse-secret
+        encapsulation)."""
         self.ctx = ctx
         self.ptr = C.c_void_p()
         if on_device:
@@ -710,7 +725,11 @@ class EvaluationKey:
             ax = np.ascontiguousarray(ax, dtype=np.uint32)
             beta = bx.shape[0]
             pb, pa = bx.ctypes.data, ax.ctypes.data
-        _check(lib().chd_evk_create(ctx.ptr, beta, pb, pa, int(on_device), C.byref(self.ptr)))
+        if basis is None:
+            _check(lib().chd_evk_create(ctx.ptr, beta, pb, pa, int(on_device), C.byref(self.ptr)))
+        else:
+            _check(lib().chd_evk_create_np(ctx.ptr, basis[0], basis[1], basis[2], beta, pb, pa, int(on_device),
+                                           C.byref(self.ptr)))
 
     def __del__(self):
         try:

@@ -60,8 +60,6 @@ Status Context::boot_build(int num_slots, int num_cts, int num_stc, int log_msg_
   CHD_CHECK(num_slots == half, kErrUnsupported, "Boot: only full-slot bootstrapping (N/2 slots) is supported");
   CHD_CHECK(num_slots >= 256 && is_pow2(num_slots), kErrInvalidArg, "Boot: power-of-two slots >= 256");
   CHD_CHECK(num_cts >= 2 && num_stc >= 2, kErrInvalidArg, "Boot: use at least 2 levels for CtS and StC");
-  CHD_CHECK(P->spec.dense_hw <= 0 || P->spec.dense_hw <= P->spec.sparse_hw, kErrUnsupported,
-            "Boot: sparse-secret encapsulation is not supported (dense Hamming weight > sparse)");
   BootPlan &bp = *out;
   bp = BootPlan{};
   bp.num_slots = num_slots;
@@ -294,11 +292,16 @@ Status Context::boot_build(int num_slots, int num_cts, int num_stc, int log_msg_
   return kOk;
 }
 
-Status Context::boot_run(const BootPlan &bp, DeviceCt &res, const DeviceCt &in, const DeviceEvk &mult_key,
-                         const DeviceEvk &conj_key, const RotKeys &rot_keys, std::vector<DeviceCt> *regs_io) {
-  // BootContext::Boot: the input must sit at level 0 (LevelDown needs the
-  // sparse-secret constants)
-  CHD_CHECK(in.np == P->level_np(0) && !in.has_rx, kErrShape, "Boot: input must be at level 0 without Rx");
+Status Context::boot_run(const BootPlan &bp, DeviceCt &res, const DeviceCt &in, const ProgKeys &keys,
+                         std::vector<DeviceCt> *regs_io) {
+  // BootContext::Boot (BootContext.cpp:296-370); an input above level 0 is
+  // first brought down with Context::LevelDown (Context.cpp:917-929): per
+  // level, times the constant 1 at that level's scale, then Rescale
+  CHD_CHECK(in.np.aux == 0 && !in.has_rx, kErrShape, "Boot: input must be relinearised without aux primes");
+  const int in_level = P->np_to_level(in.np);
+  CHD_CHECK(in_level >= 0 && in_level <= P->spec.default_encryption_level, kErrInvalidLevel,
+            "Boot: input level must be in [0, default encryption level]");
+  CHD_CHECK(keys.mult && keys.conj && keys.rot, kErrKey, "Boot: multiplication, conjugation and rotation keys needed");
   std::vector<DeviceCt> local;
   std::vector<DeviceCt> &regs = regs_io ? *regs_io : local;
   CHD_TRY(program_regs(bp.prog, regs));
@@ -309,7 +312,33 @@ Status Context::boot_run(const BootPlan &bp, DeviceCt &res, const DeviceCt &in, 
   cudaMemcpyAsync(r0.ax, in.ax, bytes, cudaMemcpyDeviceToDevice, stream);
   r0.scale = in.scale;
   r0.num_slots = in.num_slots;
-  CHD_TRY(run_program(bp.prog, regs, &mult_key, &conj_key, &rot_keys, &bp.lt_ptrs));
+  if (in_level > 0) {
+    Program ld;
+    ld.input = ld.reg();
+    int x = ld.input;
+    for (int i = in_level; i > 0; i--) {
+      ProgOp m;
+      m.kind = OpKind::kConstMult;
+      m.dst = ld.reg();
+      m.a = x;
+      m.c = ld.add_const(i, P->scale.at(i), 1.0);
+      m.level = i;
+      ld.ops.push_back(m);
+      ProgOp r;
+      r.kind = OpKind::kRescale;
+      r.dst = ld.reg();
+      r.a = m.dst;
+      ld.ops.push_back(r);
+      x = r.dst;
+    }
+    ld.output = x;
+    std::vector<DeviceCt> lregs;
+    CHD_TRY(program_regs(ld, lregs));
+    swap_regs(lregs[ld.input], r0);
+    CHD_TRY(run_program(ld, lregs, keys, nullptr));
+    swap_regs(lregs[ld.output], r0);
+  }
+  CHD_TRY(run_program(bp.prog, regs, keys, &bp.lt_ptrs));
   const DeviceCt &o = regs[bp.prog.output];
   CHD_TRY(res.reserve(o.np, false, P->n));
   const size_t ob = static_cast<size_t>(o.np.total()) * P->n * 4;

@@ -20,7 +20,16 @@ struct chd_evk {
 };
 struct chd_evk_map {
   RotKeys rot;
-  const DeviceEvk *conj = nullptr, *mult = nullptr;
+  const DeviceEvk *conj = nullptr, *mult = nullptr, *dts = nullptr, *std_key = nullptr;
+  ProgKeys keys() const {
+    ProgKeys k;
+    k.mult = mult;
+    k.conj = conj;
+    k.dts = dts;
+    k.std_key = std_key;
+    k.rot = &rot;
+    return k;
+  }
 };
 struct chd_lintrans {
   LTPlan plan;
@@ -389,11 +398,24 @@ int chd_encode_const(chd_context *ctx, int level, double scale, double value, in
   return CHD_OK;
 }
 
-int chd_modup_to_max(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) {
+int chd_modup_to_max(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk_map *keys) {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
-  return ctx->c->modup_to_max(res->ct, a->ct);
+  Context &C = *ctx->c;
+  if (C.uses_sse()) {
+    if (!keys || !keys->dts || !keys->std_key)
+      return fail(CHD_ERR_KEY, "chd_modup_to_max: dense-to-sparse and sparse-to-dense keys required");
+    if (res == a) {
+      DeviceCt tmp;
+      int rc = C.modup_to_max_sse(tmp, a->ct, *keys->dts, *keys->std_key);
+      if (rc != CHD_OK) return rc;
+      swap_regs(res->ct, tmp);
+      return CHD_OK;
+    }
+    return C.modup_to_max_sse(res->ct, a->ct, *keys->dts, *keys->std_key);
+  }
+  return C.modup_to_max(res->ct, a->ct);
 }
 
 int chd_evk_map_create(chd_context *ctx, chd_evk_map **out) {
@@ -424,6 +446,50 @@ int chd_evk_map_set_mult(chd_evk_map *m, const chd_evk *key) {
   CHD_NOTNULL(m);
   CHD_NOTNULL(key);
   m->mult = &key->k;
+  return CHD_OK;
+}
+
+int chd_evk_map_set_dense_to_sparse(chd_evk_map *m, const chd_evk *key) {
+  CHD_NOTNULL(m);
+  CHD_NOTNULL(key);
+  m->dts = &key->k;
+  return CHD_OK;
+}
+
+int chd_evk_map_set_sparse_to_dense(chd_evk_map *m, const chd_evk *key) {
+  CHD_NOTNULL(m);
+  CHD_NOTNULL(key);
+  m->std_key = &key->k;
+  return CHD_OK;
+}
+
+int chd_evk_create_np(chd_context *ctx, int num_main, int num_ter, int num_aux, int beta, const uint32_t *bx,
+                      const uint32_t *ax, int src_on_device, chd_evk **out) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(bx);
+  CHD_NOTNULL(ax);
+  CHD_NOTNULL(out);
+  Context &C = *ctx->c;
+  if (num_main < 0 || num_ter < 0 || num_aux < 1 || num_main > C.P->max_main || num_ter > C.P->max_ter ||
+      num_aux > C.P->alpha || beta < 1 || beta > 8)
+    return fail(CHD_ERR_KEY, "chd_evk_create_np: invalid key basis");
+  auto *k = new chd_evk();
+  k->k.beta = beta;
+  k->k.np = NP{num_main, num_ter, num_aux};
+  const size_t bytes = static_cast<size_t>(beta) * (num_main + num_ter + num_aux) * C.P->n * 4;
+  if (cudaMalloc(&k->k.bx, bytes) != cudaSuccess || cudaMalloc(&k->k.ax, bytes) != cudaSuccess) {
+    delete k;
+    return fail(CHD_ERR_ALLOC, "chd_evk_create_np: device allocation failed");
+  }
+  cudaMemcpyKind kind = src_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  cudaMemcpyAsync(k->k.bx, bx, bytes, kind, C.stream);
+  cudaMemcpyAsync(k->k.ax, ax, bytes, kind, C.stream);
+  cudaError_t e = cudaStreamSynchronize(C.stream);
+  if (e != cudaSuccess) {
+    delete k;
+    return fail(CHD_ERR_CUDA, cudaGetErrorString(e));
+  }
+  *out = k;
   return CHD_OK;
 }
 
@@ -627,8 +693,7 @@ int chd_program_run(chd_context *ctx, const chd_program *p, chd_ciphertext *res,
   if (rc != CHD_OK) return rc;
   rc = copy_ct(C, regs[p->prog.input], in->ct);
   if (rc != CHD_OK) return rc;
-  rc = C.run_program(p->prog, regs, keys ? keys->mult : nullptr, keys ? keys->conj : nullptr,
-                     keys ? &keys->rot : nullptr, nullptr);
+  rc = C.run_program(p->prog, regs, keys ? keys->keys() : ProgKeys{}, nullptr);
   if (rc != CHD_OK) return rc;
   rc = copy_ct(C, res->ct, regs[p->prog.output]);
   if (rc != CHD_OK) return rc;
@@ -721,9 +786,10 @@ int chd_boot_run(chd_context *ctx, chd_boot *b, chd_ciphertext *res, const chd_c
   CHD_NOTNULL(in);
   CHD_NOTNULL(keys);
   if (!keys->mult || !keys->conj) return fail(CHD_ERR_KEY, "chd_boot_run: multiplication and conjugation keys required");
+  const ProgKeys pk = keys->keys();
   if (res == in) {
     DeviceCt tmp;
-    int rc = ctx->c->boot_run(b->plan, tmp, in->ct, *keys->mult, *keys->conj, keys->rot, &b->regs);
+    int rc = ctx->c->boot_run(b->plan, tmp, in->ct, pk, &b->regs);
     if (rc != CHD_OK) return rc;
     std::swap(res->ct.bx, tmp.bx);
     std::swap(res->ct.ax, tmp.ax);
@@ -736,7 +802,7 @@ int chd_boot_run(chd_context *ctx, chd_boot *b, chd_ciphertext *res, const chd_c
     res->ct.num_slots = tmp.num_slots;
     return CHD_OK;
   }
-  return ctx->c->boot_run(b->plan, res->ct, in->ct, *keys->mult, *keys->conj, keys->rot, &b->regs);
+  return ctx->c->boot_run(b->plan, res->ct, in->ct, pk, &b->regs);
 }
 
 int chd_graph_begin(chd_context *ctx) {

@@ -220,6 +220,13 @@ struct LTPlan {
 };
 struct DeviceEvk;
 using RotKeys = std::map<int, const DeviceEvk *>;
+// The keys a program may use (EvkMap: multiplication, conjugation,
+// rotations, and the dense-to-sparse / sparse-to-dense keys of
+// sparse-secret encapsulation)
+struct ProgKeys {
+  const DeviceEvk *mult = nullptr, *conj = nullptr, *dts = nullptr, *std_key = nullptr;
+  const RotKeys *rot = nullptr;
+};
 
 // A straight-line program of ciphertext operations over registers, the
 // compiled form of EvalPoly / EvalMod / Boot (planning on the host, every
@@ -281,6 +288,9 @@ struct BootPlan {
 
 // EvalMod cosine polynomial of the reference's BootParameter
 const std::vector<double> &boot_mod_coefficients();
+
+// Exchanges two ciphertexts' buffers and metadata
+void swap_regs(DeviceCt &x, DeviceCt &y);
 
 // A ciphertext whose buffers come from the arena (not owned; released with
 // the enclosing ArenaScope)
@@ -399,6 +409,10 @@ class Context {
   // BootContext::ModUpToMax without sparse-secret encapsulation
   // (BootContext.cpp:186-270): level -1 -> top level
   Status modup_to_max(DeviceCt &res, const DeviceCt &a);
+  // ... with sparse-secret encapsulation: dense-to-sparse key switch at level
+  // -1, lift, single-digit sparse-to-dense key switch, ModDown
+  Status modup_to_max_sse(DeviceCt &res, const DeviceCt &a, const DeviceEvk &dts, const DeviceEvk &std_key);
+  bool uses_sse() const { return P->spec.dense_hw > 0 && P->spec.dense_hw > P->spec.sparse_hw; }
 
   // Linear transform planning and evaluation (lintrans.cu): LinearTransform
   // ctor + HoistHandler ctor (LinearTransform.cpp:8-75, Hoist.cu:120-167)
@@ -418,8 +432,8 @@ class Context {
                          int num_double_angle, int initial_K, int *out_reg, int *out_level, double *start_scale,
                          double *end_scale);
   // Runs a program (program.cu): regs[input] holds the input
-  Status run_program(const Program &prog, std::vector<DeviceCt> &regs, const DeviceEvk *mult_key,
-                     const DeviceEvk *conj_key, const RotKeys *rot_keys, const std::vector<const LTPlan *> *lts);
+  Status run_program(const Program &prog, std::vector<DeviceCt> &regs, const ProgKeys &keys,
+                     const std::vector<const LTPlan *> *lts);
   bool mult_unsafe_compatible(int l1, int l2) const;
   // sizes the registers of a program (plus two spares) at top-level capacity
   Status program_regs(const Program &prog, std::vector<DeviceCt> &regs);
@@ -428,8 +442,8 @@ class Context {
   Status boot_build(int num_slots, int num_cts, int num_stc, int log_msg_ratio, BootPlan *out);
   // BootContext::Boot: in at level 0 -> res at the end level.  regs_io,
   // when given, keeps the program registers allocated across calls.
-  Status boot_run(const BootPlan &bp, DeviceCt &res, const DeviceCt &in, const DeviceEvk &mult_key,
-                  const DeviceEvk &conj_key, const RotKeys &rot_keys, std::vector<DeviceCt> *regs_io);
+  Status boot_run(const BootPlan &bp, DeviceCt &res, const DeviceCt &in, const ProgKeys &keys,
+                  std::vector<DeviceCt> *regs_io);
 
   // ---- optional device timing of the fused key-switch stages ----
   // Events recorded on the context stream around each stage's launches.

@@ -16,7 +16,9 @@
 namespace chd {
 namespace {
 
-void swap_ct(DeviceCt &x, DeviceCt &y) {
+}  // namespace
+
+void swap_regs(DeviceCt &x, DeviceCt &y) {
   std::swap(x.np, y.np);
   std::swap(x.has_rx, y.has_rx);
   std::swap(x.scale, y.scale);
@@ -27,6 +29,8 @@ void swap_ct(DeviceCt &x, DeviceCt &y) {
   std::swap(x.cap_words, y.cap_words);
   std::swap(x.owned, y.owned);
 }
+
+namespace {
 
 uint32_t *part_of(DeviceCt &c, int p) { return p == 0 ? c.bx : (p == 1 ? c.ax : c.rx); }
 const uint32_t *part_of(const DeviceCt &c, int p) { return p == 0 ? c.bx : (p == 1 ? c.ax : c.rx); }
@@ -51,9 +55,10 @@ Status Context::program_regs(const Program &prog, std::vector<DeviceCt> &regs) {
   return kOk;
 }
 
-Status Context::run_program(const Program &prog, std::vector<DeviceCt> &regs, const DeviceEvk *mult_key,
-                            const DeviceEvk *conj_key, const RotKeys *rot_keys,
+Status Context::run_program(const Program &prog, std::vector<DeviceCt> &regs, const ProgKeys &keys,
                             const std::vector<const LTPlan *> *lts) {
+  const DeviceEvk *mult_key = keys.mult, *conj_key = keys.conj;
+  const RotKeys *rot_keys = keys.rot;
   CHD_TRY(program_regs(prog, regs));
   const int n = P->n;
   // constants: Montgomery residues over their own level's q primes
@@ -264,7 +269,13 @@ Status Context::run_program(const Program &prog, std::vector<DeviceCt> &regs, co
         CHD_TRY(mult_imag_unit(t, regs.at(op.a)));
         break;
       case OpKind::kModUpToMax:
-        CHD_TRY(modup_to_max(t, regs.at(op.a)));
+        if (uses_sse()) {
+          CHD_CHECK(keys.dts && keys.std_key, kErrKey,
+                    "program: dense-to-sparse and sparse-to-dense keys required (sparse-secret encapsulation)");
+          CHD_TRY(modup_to_max_sse(t, regs.at(op.a), *keys.dts, *keys.std_key));
+        } else {
+          CHD_TRY(modup_to_max(t, regs.at(op.a)));
+        }
         break;
       case OpKind::kHRotAdd: {
         CHD_CHECK(rot_keys, kErrKey, "program: rotation keys missing");
@@ -280,7 +291,7 @@ Status Context::run_program(const Program &prog, std::vector<DeviceCt> &regs, co
         CHD_TRY(lt_evaluate(t, regs.at(op.a), *(*lts)[op.rot], *rot_keys));
         break;
     }
-    swap_ct(regs.at(op.dst), t);
+    swap_regs(regs.at(op.dst), t);
   }
   return check_cuda("program");
 }

@@ -149,6 +149,9 @@ def main():
         "rational_t4_m10_a6.json": rational_params(),
         # bootstrapping: 48 q primes (max level 34) + alpha = 12 aux primes
         "boot_l34_a12.json": boot_params(),
+        # the same with sparse-secret encapsulation (dense Hamming weight
+        # 32768 > sparse 32), as the reference's bootparam_*.json files
+        "boot_l34_a12_sse.json": dict(boot_params(), dense_hamming_weight=32768),
     }
     for name, obj in files.items():
         with open(os.path.join(here, name), "w") as f:

@@ -47,6 +47,7 @@ extern "C" {
 typedef struct chd_context chd_context;
 typedef struct chd_ciphertext chd_ciphertext;
 typedef struct chd_evk chd_evk;
+typedef struct chd_evk_map chd_evk_map;
 
 const char *chd_last_error(void);
 
@@ -184,18 +185,30 @@ int chd_encode(chd_context *ctx, int level, double scale, const double *re, cons
 /* Encoder::EncodeConstant (Encode.cpp:250-275): cx[num_q(level) + num_aux]
  * Montgomery residues of trunc(value * scale), host memory. */
 int chd_encode_const(chd_context *ctx, int level, double scale, double value, int num_aux, uint32_t *cx);
-/* BootContext::ModUpToMax (src/extension/BootContext.cpp:186-270) without
- * sparse-secret encapsulation: a at level -1 -> res at the top level. */
-int chd_modup_to_max(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a);
+/* BootContext::ModUpToMax (src/extension/BootContext.cpp:186-270): a at
+ * level -1 -> res at the top level.  With sparse-secret encapsulation (the
+ * parameters' dense Hamming weight above the sparse one) the key map must
+ * hold the dense-to-sparse and sparse-to-dense keys; otherwise keys may be
+ * NULL. */
+int chd_modup_to_max(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk_map *keys);
 
 /* EvkMap (include/core/EvkMap.h): rotation / conjugation / multiplication
  * keys by index.  The map borrows the keys; they must outlive it. */
-typedef struct chd_evk_map chd_evk_map;
 int chd_evk_map_create(chd_context *ctx, chd_evk_map **out);
 void chd_evk_map_destroy(chd_evk_map *m);
 int chd_evk_map_set_rotation(chd_evk_map *m, int rot_idx, const chd_evk *key);
 int chd_evk_map_set_conjugation(chd_evk_map *m, const chd_evk *key);
 int chd_evk_map_set_mult(chd_evk_map *m, const chd_evk *key);
+/* EvkMap::GetDenseToSparseKey / GetSparseToDenseKey (sparse-secret
+ * encapsulation, UserInterface.cu:342-356): the dense-to-sparse key over the
+ * level -1 primes and as many aux primes (one digit, chd_evk_create_np), the
+ * sparse-to-dense key over the full key basis (its digit 0 is used). */
+int chd_evk_map_set_dense_to_sparse(chd_evk_map *m, const chd_evk *key);
+int chd_evk_map_set_sparse_to_dense(chd_evk_map *m, const chd_evk *key);
+/* An evaluation key over an explicit basis (num_main, num_ter, num_aux):
+ * beta digits of [num_main + num_ter + num_aux][N] per part. */
+int chd_evk_create_np(chd_context *ctx, int num_main, int num_ter, int num_aux, int beta, const uint32_t *bx,
+                      const uint32_t *ax, int src_on_device, chd_evk **out);
 
 /* LinearTransform (src/extension/LinearTransform.cpp:77-124) with the
  * HoistHandler's double-hoisted baby-step / giant-step evaluation
@@ -242,10 +255,13 @@ int chd_program_run(chd_context *ctx, const chd_program *p, chd_ciphertext *res,
 /* BootContext (src/extension/BootContext.cpp) for one slot count:
  * PrepareEvalMod + PrepareEvalSpecialFFT (EvalSpecialFFT.cpp) with
  * num_cts_levels / num_stc_levels (BootParameter; log_message_ratio 5 in
- * the reference), then Boot (full slots, BootVariant::kNormal, no
- * sparse-secret encapsulation): in at level 0 -> res at the end level
- * (StC start - num_stc_levels).  Keys: the multiplication and conjugation
- * keys and every rotation chd_boot_rotations lists, at the top level.
+ * the reference), then Boot (full slots, BootVariant::kNormal, with
+ * sparse-secret encapsulation when the parameters' dense Hamming weight
+ * exceeds the sparse one): in at a level in [0, default encryption level]
+ * (brought to level 0 by LevelDown) -> res at the end level (StC start -
+ * num_stc_levels).  Keys: the multiplication and conjugation keys, every
+ * rotation chd_boot_rotations lists, and with encapsulation the
+ * dense-to-sparse and sparse-to-dense keys.
  * chd_boot_levels: {CtS start, EvalMod start, StC start, end level,
  * log2 scale-up} and {CtS constant, StC constant, EvalMod start scale,
  * EvalMod end scale, final scale}.  chd_boot_json / _lt_info / _lt_pt

@@ -222,6 +222,8 @@ class EvkMap {
   void AddRotationKey(int rot_idx, const EvaluationKey &k) { check(chd_evk_map_set_rotation(m_, rot_idx, k.raw())); }
   void SetConjugationKey(const EvaluationKey &k) { check(chd_evk_map_set_conjugation(m_, k.raw())); }
   void SetMultiplicationKey(const EvaluationKey &k) { check(chd_evk_map_set_mult(m_, k.raw())); }
+  void SetDenseToSparseKey(const EvaluationKey &k) { check(chd_evk_map_set_dense_to_sparse(m_, k.raw())); }
+  void SetSparseToDenseKey(const EvaluationKey &k) { check(chd_evk_map_set_sparse_to_dense(m_, k.raw())); }
   chd_evk_map *raw() const { return m_; }
 
  private:
@@ -253,8 +255,8 @@ class BootContext {
     check(chd_boot_levels(b_, lv, nullptr));
     return lv[3];
   }
-  void ModUpToMax(Ciphertext &res, const Ciphertext &in) const {
-    check(chd_modup_to_max(ctx_.raw(), res.raw(), in.raw()));
+  void ModUpToMax(Ciphertext &res, const Ciphertext &in, const EvkMap &evk_map) const {
+    check(chd_modup_to_max(ctx_.raw(), res.raw(), in.raw(), evk_map.raw()));
   }
   void Boot(Ciphertext &res, const Ciphertext &in, const EvkMap &evk_map) {
     check(chd_boot_run(ctx_.raw(), b_, res.raw(), in.raw(), evk_map.raw()));

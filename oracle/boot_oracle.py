@@ -195,9 +195,10 @@ def _cmul_rows(o, level, x, front, c, cfront):
     return out
 
 
-def run_program(o, prog, inp, mult_key=None, conj_key=None, rot_keys=None, lts=None):
+def run_program(o, prog, inp, mult_key=None, conj_key=None, rot_keys=None, lts=None, sse_keys=None):
     """Runs a compiled program (the dict of chd_program_json) on `inp`
-    (a Ct); returns the output Ct."""
+    (a Ct); returns the output Ct.  sse_keys = (dts, std) selects
+    ModUpToMax with sparse-secret encapsulation."""
     consts = []
     for level, scale, value in prog["consts"]:
         consts.append((level, scale, o.encode_const(level, scale, value)))
@@ -295,7 +296,10 @@ def run_program(o, prog, inp, mult_key=None, conj_key=None, rot_keys=None, lts=N
             regs[d] = Ct(x.level, [o.mult_imag_unit(x.level, p) for p in x.parts], x.scale)
         elif k == K_MODUP_TO_MAX:
             x = regs[a]
-            rb, ra = o.modup_to_max(x.parts[0], x.parts[1])
+            if sse_keys is not None:
+                rb, ra = o.modup_to_max_sse(x.parts[0], x.parts[1], sse_keys[0], sse_keys[1])
+            else:
+                rb, ra = o.modup_to_max(x.parts[0], x.parts[1])
             regs[d] = Ct(o.max_level, [rb, ra], x.scale)
         elif k == K_HROT_ADD:
             x, y = regs[a], regs[b]
@@ -344,3 +348,62 @@ def plain_program(prog, x):
         else:
             raise ValueError(f"plain evaluation does not cover op {k}")
     return regs[prog["output"]]
+
+
+# ---------------------------------------------------------------------------
+# Test-only key generation for sparse-secret encapsulation (the reference's
+# UserInterface::PrepareBasicEvks, UserInterface.cu:342-356 with PrepareEvk,
+# :366-458): b = e - a s_enc + P s_target on the q primes of the digit, a
+# uniform, e a rounded Gaussian (sigma 3.2) in the evaluation domain.
+# ---------------------------------------------------------------------------
+
+def _error_row(o, g, e):
+    q = int(o.all_primes()[g])
+    limb = np.where(e < 0, q + e, e).astype(np.uint32)
+    return o.ntt_limb(g, limb, mont=True)
+
+
+def gen_evk_rows(o, seed, gidx, nq, enc_s, tgt_s, p_mont):
+    """One-digit key over the rows `gidx` (q rows first): target term on the
+    first nq rows with the Montgomery constants p_mont[r]."""
+    rng = np.random.default_rng(seed)
+    primes = o.all_primes()
+    kb = np.zeros((1, len(gidx), o.n), dtype=np.uint32)
+    ka = np.zeros_like(kb)
+    e = np.rint(rng.normal(0, 3.2, o.n)).astype(np.int64)
+    for r, g in enumerate(gidx):
+        q = int(primes[g])
+        a = rng.integers(0, q, o.n, dtype=np.int64).astype(np.uint32)
+        b = _error_row(o, g, e)
+        b = ((b.astype(np.int64) - mont_mul(a, enc_s[g], q)) % q).astype(np.uint32)
+        if r < nq:
+            b = add_mod(b, mont_mul(tgt_s[g], p_mont[r], q), q)
+        kb[0, r] = b
+        ka[0, r] = a
+    return kb, ka
+
+
+def gen_sse_keys(o, seed, dense_s, sparse_s):
+    """(dense-to-sparse key over [num_q(-1) + sse aux], sparse-to-dense key
+    over [L + alpha] as one digit)."""
+    primes = [int(p) for p in o.all_primes()]
+    m, t = o.level_np(-1)
+    nb = m + t
+    L, alpha = o.L, o.alpha
+    g_dts = list(range(o.max_ter - t, o.max_ter + m)) + [L + j for j in range(nb)]
+    p_dts = []
+    for g in g_dts[:nb]:
+        v = 1
+        for j in range(nb):
+            v = v * primes[L + j] % primes[g]
+        p_dts.append(v * 2 ** 32 % primes[g])
+    dts = gen_evk_rows(o, seed, g_dts, nb, sparse_s, dense_s, p_dts)
+    g_std = list(range(L + alpha))
+    p_std = []
+    for g in g_std[:L]:
+        v = 1
+        for j in range(alpha):
+            v = v * primes[L + j] % primes[g]
+        p_std.append(v * 2 ** 32 % primes[g])
+    std = gen_evk_rows(o, seed + 1, g_std, L, dense_s, sparse_s, p_std)
+    return dts, std

@@ -1530,6 +1530,118 @@ int orc_modup_to_max(const orc_ctx *c, const uint32_t *bx, const uint32_t *ax,
   return 0;
 }
 
+/* ModUpToMax with sparse-secret encapsulation — BootContext.cpp:186-270:
+ * dense-to-sparse MultKey at level -1 (Context.cpp:584-607, DtS mod switcher,
+ * p_prod_dts of Context.cpp:108-123), exact lift of bx to the top-level q
+ * primes and of ax to the top-level q and alpha aux primes, PMult with the
+ * digit-0 sparse-to-dense key plus P * bx on the q primes (PseudoModUp,
+ * CAccum), ModDown with the top level's mod switcher.  Key layouts: dts
+ * [num_q(-1) + sse aux][N] (one digit), std [L + alpha][N] (digit 0). */
+int orc_modup_to_max_sse(const orc_ctx *c, const uint32_t *bx, const uint32_t *ax,
+                         const uint32_t *dts_bx, const uint32_t *dts_ax,
+                         const uint32_t *std_bx, const uint32_t *std_ax,
+                         uint32_t *res_bx, uint32_t *res_ax) {
+  const msw_t *m = &c->msw[0];
+  np_t b = level_np(c, -1, 0), db = level_np(c, -1, m->num_aux);
+  int nb = np_q(b), dt = np_total(db), N = c->n;
+  if (nb < 1 || nb > 2 || m->beta != 1) return -1;
+  int gd[256];
+  np_gidx(c, db, gd);
+  /* 1. DtS key switch */
+  uint32_t *mu = malloc(sizeof(uint32_t) * (size_t)dt * N);
+  uint32_t *acc = malloc(sizeof(uint32_t) * 2 * (size_t)dt * N);
+  uint32_t *sw = malloc(sizeof(uint32_t) * 2 * (size_t)nb * N);
+  modup_impl(c, m, b, ax, mu);
+  for (int r = 0; r < dt; r++) {
+    uint32_t q = c->primes[gd[r]];
+    int32_t qi = c->qinv[gd[r]];
+    uint32_t pp = 1;
+    for (int j = 0; j < m->num_aux; j++) pp = mul_mod(pp, c->primes[gd[nb + j]], q);
+    pp = orc_to_mont(pp, q);
+    for (int j = 0; j < N; j++) {
+      size_t k = (size_t)r * N + j;
+      uint32_t vb = orc_mont_mult(mu[k], dts_bx[k], q, qi);
+      uint32_t va = orc_mont_mult(mu[k], dts_ax[k], q, qi);
+      if (r < nb) vb = add_mod(vb, orc_mont_mult(bx[k], pp, q, qi), q);
+      acc[k] = vb;
+      acc[(size_t)dt * N + k] = va;
+    }
+  }
+  moddown_worker(c, -1, MD_MODDOWN, acc, sw);
+  moddown_worker(c, -1, MD_MODDOWN, acc + (size_t)dt * N, sw + (size_t)nb * N);
+  /* 2. lift */
+  np_t top = level_np(c, c->max_level, 0), tqp = level_np(c, c->max_level, c->alpha);
+  int nq = np_q(top), qt = np_total(tqp);
+  int gb[2], gm[256];
+  np_gidx(c, b, gb);
+  np_gidx(c, tqp, gm);
+  int32_t *t = malloc(sizeof(int32_t) * 2 * (size_t)nb * N);
+  for (int part = 0; part < 2; part++)
+    for (int i = 0; i < nb; i++) {
+      uint32_t q = c->primes[gb[i]];
+      uint32_t k = (uint32_t)(N % q);
+      for (int j = 0; j < nb; j++)
+        if (j != i) k = mul_mod(k, c->primes[gb[j]], q);
+      k = orc_inv_mod(k, q);
+      int32_t *a = t + ((size_t)part * nb + i) * N;
+      memcpy(a, sw + ((size_t)part * nb + i) * N, sizeof(int32_t) * N);
+      intt_core(c, gb[i], a);
+      for (int j = 0; j < N; j++) a[j] = ep_mult(a[j], k, q, c->qinv[gb[i]]);
+    }
+  uint32_t *lb = malloc(sizeof(uint32_t) * (size_t)nq * N);
+  uint32_t *la = malloc(sizeof(uint32_t) * (size_t)qt * N);
+  for (int part = 0; part < 2; part++) {
+    int rows = part == 0 ? nq : qt;
+    uint32_t *o = part == 0 ? lb : la;
+    const int32_t *src = t + (size_t)part * nb * N;
+#pragma omp parallel for schedule(static)
+    for (int r = 0; r < rows; r++) {
+      int64_t p = c->primes[gm[r]];
+      uint32_t *row = o + (size_t)r * N;
+      for (int j = 0; j < N; j++) {
+        if (nb == 1) {
+          row[j] = (uint32_t)((uint32_t)src[j] % (uint32_t)p);
+        } else {
+          int64_t q0 = c->primes[gb[0]], q1 = c->primes[gb[1]], qp = q0 * q1;
+          int64_t v = (int64_t)(uint32_t)src[j] * q1 + (int64_t)(uint32_t)src[N + j] * q0;
+          if (v >= qp) v -= qp;
+          if (v > (qp >> 1)) v -= qp;
+          int64_t mm = v % p;
+          if (mm < 0) mm += p;
+          row[j] = (uint32_t)mm;
+        }
+      }
+      orc_ntt_limb(c, gm[r], row, 1);
+    }
+  }
+  /* 3. StD: key digit 0 (.) a_lift + P * b_lift on q primes; ModDown */
+  int po = c->max_ter - top.num_ter;
+  uint32_t *acc2 = malloc(sizeof(uint32_t) * 2 * (size_t)qt * N);
+  for (int r = 0; r < qt; r++) {
+    uint32_t q = c->primes[gm[r]];
+    int32_t qi = c->qinv[gm[r]];
+    int kr = r < nq ? po + r : c->L + (r - nq);
+    for (int j = 0; j < N; j++) {
+      size_t k = (size_t)r * N + j, kk = (size_t)kr * N + j;
+      uint32_t vb = orc_mont_mult(la[k], std_bx[kk], q, qi);
+      uint32_t va = orc_mont_mult(la[k], std_ax[kk], q, qi);
+      if (r < nq) vb = add_mod(vb, orc_mont_mult(lb[k], c->p_prod[po + r], q, qi), q);
+      acc2[k] = vb;
+      acc2[(size_t)qt * N + k] = va;
+    }
+  }
+  moddown_worker(c, c->max_level, MD_MODDOWN, acc2, res_bx);
+  moddown_worker(c, c->max_level, MD_MODDOWN, acc2 + (size_t)qt * N, res_ax);
+  free(mu);
+  free(acc);
+  free(sw);
+  free(t);
+  free(lb);
+  free(la);
+  free(acc2);
+  return 0;
+}
+
 /* ---- encoding — Encode.cpp:10-21, 84-133, 135-190, 250-275 ---- */
 typedef struct {
   double re, im;

@@ -198,6 +198,11 @@ int orc_decode(const orc_ctx *c, int level, double scale, const uint32_t *pt,
  * (bx, ax) -> top level (res_bx, res_ax) */
 int orc_modup_to_max(const orc_ctx *c, const uint32_t *bx, const uint32_t *ax,
                      uint32_t *res_bx, uint32_t *res_ax);
+/* ... with sparse-secret encapsulation (DtS key at level -1, StD digit-0 key) */
+int orc_modup_to_max_sse(const orc_ctx *c, const uint32_t *bx, const uint32_t *ax,
+                         const uint32_t *dts_bx, const uint32_t *dts_ax,
+                         const uint32_t *std_bx, const uint32_t *std_ax,
+                         uint32_t *res_bx, uint32_t *res_ax);
 /* EncodeConstant: one Montgomery word per prime */
 int orc_encode_const(const orc_ctx *c, int level, double scale, double value,
                      int num_aux, uint32_t *cx);

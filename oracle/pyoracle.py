@@ -84,6 +84,7 @@ def lib():
             "orc_decode": (C.c_int, [vp, C.c_int, C.c_double, u32p, C.c_int, f64p, f64p]),
             "orc_encode_const": (C.c_int, [vp, C.c_int, C.c_double, C.c_double, C.c_int, u32p]),
             "orc_modup_to_max": (C.c_int, [vp, u32p, u32p, u32p, u32p]),
+            "orc_modup_to_max_sse": (C.c_int, [vp, u32p, u32p, u32p, u32p, u32p, u32p, u32p, u32p]),
             "orc_relinearize": (C.c_int, [vp, C.c_int, u32p, u32p, u32p, u32p, u32p, C.c_int, u32p, u32p]),
             "orc_uniform": (C.c_int, [vp, C.c_uint64, C.c_int, C.c_int, C.c_int, u32p]),
             "orc_mont_reduce_lazy": (C.c_int32, [C.c_int64, C.c_uint32, C.c_int32]),
@@ -415,6 +416,18 @@ class Oracle:
         ra = np.zeros((nq, self.n), dtype=np.uint32)
         _check(lib().orc_modup_to_max(self.ptr, np.ascontiguousarray(bx, dtype=np.uint32),
                                       np.ascontiguousarray(ax, dtype=np.uint32), rb, ra), "modup_to_max")
+        return rb, ra
+
+    def modup_to_max_sse(self, bx, ax, dts, std):
+        """ModUpToMax with sparse-secret encapsulation (BootContext.cpp:
+        186-270); dts = (kb, ka) [1][num_q(-1) + sse aux][N], std = (kb, ka)
+        with digit 0 over [L + alpha][N]."""
+        nq = self.num_q(self.max_level)
+        rb = np.zeros((nq, self.n), dtype=np.uint32)
+        ra = np.zeros((nq, self.n), dtype=np.uint32)
+        c = lambda x: np.ascontiguousarray(x, dtype=np.uint32)
+        _check(lib().orc_modup_to_max_sse(self.ptr, c(bx), c(ax), c(dts[0]), c(dts[1]), c(std[0][0]), c(std[1][0]),
+                                          rb, ra), "modup_to_max_sse")
         return rb, ra
 
     def uniform(self, seed, level, num_aux=0):

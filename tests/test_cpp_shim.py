@@ -21,7 +21,9 @@ void unused_paths(cheddar_b200::Context &ctx, const cheddar_b200::EvaluationKey 
   cheddar_b200::BootContext bc(ctx, 1 << 15);
   std::vector<int> r = bc.RequiredRotations();
   cheddar_b200::Ciphertext a(ctx), b(ctx);
-  bc.ModUpToMax(b, a);
+  bc.ModUpToMax(b, a, m);
+  m.SetDenseToSparseKey(k);
+  m.SetSparseToDenseKey(k);
   bc.Boot(b, a, m);
   std::vector<uint32_t> cx = ctx.EncodeConstant(0, 1.0, 0.5);
   ctx.HMultBatch({&b}, {&a}, {&a}, k, true);

@@ -44,9 +44,14 @@ def test_encode_const_bit_exact(cuda_ok, value, log_scale):
                               o.encode_const(level, 2.0 ** log_scale, value, num_aux))
 
 
+# ModUpToMax without sparse-secret encapsulation needs a parameter set whose
+# dense and sparse Hamming weights agree (the key-switching set has 192 > 32)
+PLAIN = "boot_l34_a12.json"
+
+
 def test_modup_to_max_bit_exact(cuda_ok):
-    o, g = pair(KS)
-    bx, ax = uniform_parts(KS, -1, 4242)
+    o, g = pair(PLAIN, 12)
+    bx, ax = uniform_parts(PLAIN, -1, 4242, log_n=12)
     ref_b, ref_a = o.modup_to_max(bx, ax)
     r = g.ModUpToMax(g.import_ct(-1, [bx, ax]))
     parts = r.numpy()
@@ -61,8 +66,8 @@ def test_modup_to_max_bit_exact(cuda_ok):
 def test_modup_to_max_keeps_base_limbs(cuda_ok):
     # the lift is congruent to the input modulo the base primes, which are the
     # first primes of the top level: those limbs come back unchanged
-    o, g = pair(KS)
-    bx, ax = uniform_parts(KS, -1, 777)
+    o, g = pair(PLAIN, 12)
+    bx, ax = uniform_parts(PLAIN, -1, 777, log_n=12)
     r = g.ModUpToMax(g.import_ct(-1, [bx, ax])).numpy()
     nb = o.num_q(-1)
     assert np.array_equal(r[0][:nb], bx) and np.array_equal(r[1][:nb], ax)
