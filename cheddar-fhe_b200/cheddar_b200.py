@@ -113,10 +113,10 @@ def lib():
         "chd_evk_create_np": (i, [vp, i, i, i, i, vp, vp, i, pp]),
         "chd_lintrans_create": (i, [vp, i, i, vp, vp, vp, i, d, i, i, i, i, pp]),
         "chd_lintrans_destroy": (None, [vp]),
-        "chd_lintrans_rotations": (i, [vp, vp, i, C.POINTER(i)]),
+        "chd_lintrans_rotations": (i, [vp, i, vp, i, C.POINTER(i)]),
         "chd_lintrans_num_pts": (i, [vp, C.POINTER(i)]),
         "chd_lintrans_pt": (i, [vp, i, C.POINTER(i), C.POINTER(i), vp, vp]),
-        "chd_lintrans_evaluate": (i, [vp, vp, vp, vp, vp]),
+        "chd_lintrans_evaluate": (i, [vp, vp, vp, vp, vp, i]),
         "chd_poly_create": (i, [vp, vp, i, i, d, d, i, pp]),
         "chd_evalmod_create": (i, [vp, i, vp, i, i, i, pp, C.POINTER(d), C.POINTER(d)]),
         "chd_program_destroy": (None, [vp]),
@@ -125,12 +125,12 @@ def lib():
         "chd_boot_mod_coefficients": (i, [vp, i]),
         "chd_boot_create": (i, [vp, i, i, i, i, pp]),
         "chd_boot_destroy": (None, [vp]),
-        "chd_boot_rotations": (i, [vp, vp, i, C.POINTER(i)]),
+        "chd_boot_rotations": (i, [vp, i, vp, i, C.POINTER(i)]),
         "chd_boot_levels": (i, [vp, vp, vp]),
         "chd_boot_json": (i, [vp, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
         "chd_boot_lt_info": (i, [vp, i, C.POINTER(i), C.POINTER(d), C.POINTER(i), C.POINTER(i)]),
         "chd_boot_lt_pt": (i, [vp, i, i, C.POINTER(i), C.POINTER(i), vp, vp]),
-        "chd_boot_run": (i, [vp, vp, vp, vp, vp]),
+        "chd_boot_run": (i, [vp, vp, vp, vp, vp, i]),
         "chd_graph_begin": (i, [vp]),
         "chd_graph_end": (i, [vp, pp]),
         "chd_graph_launch": (i, [vp, vp]),
@@ -515,11 +515,11 @@ class LinearTransform:
         except Exception:
             pass
 
-    def rotations(self):
+    def rotations(self, min_ks=False):
         cnt = C.c_int()
-        _check(lib().chd_lintrans_rotations(self.ptr, None, 0, C.byref(cnt)))
+        _check(lib().chd_lintrans_rotations(self.ptr, int(min_ks), None, 0, C.byref(cnt)))
         out = (C.c_int * max(1, cnt.value))()
-        _check(lib().chd_lintrans_rotations(self.ptr, out, cnt.value, C.byref(cnt)))
+        _check(lib().chd_lintrans_rotations(self.ptr, int(min_ks), out, cnt.value, C.byref(cnt)))
         return [out[i] for i in range(cnt.value)]
 
     def plaintexts(self):
@@ -535,9 +535,9 @@ class LinearTransform:
             res.append((g.value, b.value, re + 1j * im))
         return res
 
-    def evaluate(self, ct, keys, res=None):
+    def evaluate(self, ct, keys, res=None, min_ks=False):
         res = res if res is not None else Ciphertext(self.ctx)
-        _check(lib().chd_lintrans_evaluate(self.ctx.ptr, self.ptr, res.ptr, ct.ptr, keys.ptr))
+        _check(lib().chd_lintrans_evaluate(self.ctx.ptr, self.ptr, res.ptr, ct.ptr, keys.ptr, int(min_ks)))
         return res
 
 
@@ -621,11 +621,11 @@ class BootContext:
         except Exception:
             pass
 
-    def rotations(self):
+    def rotations(self, min_ks=False):
         cnt = C.c_int()
-        _check(lib().chd_boot_rotations(self.ptr, None, 0, C.byref(cnt)))
+        _check(lib().chd_boot_rotations(self.ptr, int(min_ks), None, 0, C.byref(cnt)))
         out = (C.c_int * max(1, cnt.value))()
-        _check(lib().chd_boot_rotations(self.ptr, out, cnt.value, C.byref(cnt)))
+        _check(lib().chd_boot_rotations(self.ptr, int(min_ks), out, cnt.value, C.byref(cnt)))
         return [out[i] for i in range(cnt.value)]
 
     def json(self):
@@ -655,9 +655,9 @@ class BootContext:
             i += 1
         return res
 
-    def Boot(self, ct, keys, res=None):
+    def Boot(self, ct, keys, res=None, min_ks=False):
         res = res if res is not None else Ciphertext(self.ctx)
-        _check(lib().chd_boot_run(self.ctx.ptr, self.ptr, res.ptr, ct.ptr, keys.ptr))
+        _check(lib().chd_boot_run(self.ctx.ptr, self.ptr, res.ptr, ct.ptr, keys.ptr, int(min_ks)))
         return res
 
 

@@ -523,14 +523,31 @@ int chd_lintrans_create(chd_context *ctx, int width, int n_diag, const int *diag
 
 void chd_lintrans_destroy(chd_lintrans *lt) { delete lt; }
 
-int chd_lintrans_rotations(const chd_lintrans *lt, int *out, int cap, int *count) {
+namespace {
+// HoistHandler::AddRequiredRotations (Hoist.cu:977-1003)
+int plan_rotations(const LTPlan &p, bool min_ks, std::vector<int> *r) {
+  if (min_ks) {
+    int bs = 0, gs = 0;
+    const int rc = lt_min_ks_strides(p, &bs, &gs);
+    if (rc != CHD_OK) return rc;
+    if (bs) r->push_back(bs);
+    if (gs) r->push_back(gs);
+    return CHD_OK;
+  }
+  for (int b : p.bs_idx)
+    if (b) r->push_back(b);
+  for (int g : p.gs_idx)
+    if (g) r->push_back(g);
+  return CHD_OK;
+}
+}  // namespace
+
+int chd_lintrans_rotations(const chd_lintrans *lt, int min_ks, int *out, int cap, int *count) {
   CHD_NOTNULL(lt);
   CHD_NOTNULL(count);
   std::vector<int> r;
-  for (int b : lt->plan.bs_idx)
-    if (b) r.push_back(b);
-  for (int g : lt->plan.gs_idx)
-    if (g) r.push_back(g);
+  int rc = plan_rotations(lt->plan, min_ks != 0, &r);
+  if (rc != CHD_OK) return rc;
   std::sort(r.begin(), r.end());
   r.erase(std::unique(r.begin(), r.end()), r.end());
   *count = static_cast<int>(r.size());
@@ -560,12 +577,22 @@ int chd_lintrans_pt(const chd_lintrans *lt, int i, int *gs, int *bs, double *re,
 }
 
 int chd_lintrans_evaluate(chd_context *ctx, const chd_lintrans *lt, chd_ciphertext *res, const chd_ciphertext *in,
-                          const chd_evk_map *keys) {
+                          const chd_evk_map *keys, int min_ks) {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(lt);
   CHD_NOTNULL(res);
   CHD_NOTNULL(in);
   CHD_NOTNULL(keys);
+  if (min_ks) {
+    if (res == in) {
+      DeviceCt tmp;
+      int rc = ctx->c->lt_evaluate_min_ks(tmp, in->ct, lt->plan, keys->rot);
+      if (rc != CHD_OK) return rc;
+      swap_regs(res->ct, tmp);
+      return CHD_OK;
+    }
+    return ctx->c->lt_evaluate_min_ks(res->ct, in->ct, lt->plan, keys->rot);
+  }
   if (res == in) {
     DeviceCt tmp;
     int rc = ctx->c->lt_evaluate(tmp, in->ct, lt->plan, keys->rot);
@@ -716,12 +743,19 @@ int chd_boot_create(chd_context *ctx, int num_slots, int num_cts_levels, int num
 
 void chd_boot_destroy(chd_boot *b) { delete b; }
 
-int chd_boot_rotations(const chd_boot *b, int *out, int cap, int *count) {
+int chd_boot_rotations(const chd_boot *b, int min_ks, int *out, int cap, int *count) {
   CHD_NOTNULL(b);
   CHD_NOTNULL(count);
-  *count = static_cast<int>(b->plan.rotations.size());
+  std::vector<int> r;
+  for (const auto &l : b->plan.lts) {
+    int rc = plan_rotations(l, min_ks != 0, &r);
+    if (rc != CHD_OK) return rc;
+  }
+  std::sort(r.begin(), r.end());
+  r.erase(std::unique(r.begin(), r.end()), r.end());
+  *count = static_cast<int>(r.size());
   if (out)
-    for (int i = 0; i < std::min(cap, *count); i++) out[i] = b->plan.rotations[i];
+    for (int i = 0; i < std::min(cap, *count); i++) out[i] = r[i];
   return CHD_OK;
 }
 
@@ -779,14 +813,16 @@ int chd_boot_lt_pt(const chd_boot *b, int i, int j, int *gs, int *bs, double *re
   return CHD_OK;
 }
 
-int chd_boot_run(chd_context *ctx, chd_boot *b, chd_ciphertext *res, const chd_ciphertext *in, const chd_evk_map *keys) {
+int chd_boot_run(chd_context *ctx, chd_boot *b, chd_ciphertext *res, const chd_ciphertext *in, const chd_evk_map *keys,
+                 int min_ks) {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(b);
   CHD_NOTNULL(res);
   CHD_NOTNULL(in);
   CHD_NOTNULL(keys);
   if (!keys->mult || !keys->conj) return fail(CHD_ERR_KEY, "chd_boot_run: multiplication and conjugation keys required");
-  const ProgKeys pk = keys->keys();
+  ProgKeys pk = keys->keys();
+  pk.min_ks = min_ks != 0;
   if (res == in) {
     DeviceCt tmp;
     int rc = ctx->c->boot_run(b->plan, tmp, in->ct, pk, &b->regs);

@@ -226,6 +226,7 @@ using RotKeys = std::map<int, const DeviceEvk *>;
 struct ProgKeys {
   const DeviceEvk *mult = nullptr, *conj = nullptr, *dts = nullptr, *std_key = nullptr;
   const RotKeys *rot = nullptr;
+  bool min_ks = false;  // linear transforms in the min-KS form
 };
 
 // A straight-line program of ciphertext operations over registers, the
@@ -288,6 +289,9 @@ struct BootPlan {
 
 // EvalMod cosine polynomial of the reference's BootParameter
 const std::vector<double> &boot_mod_coefficients();
+
+// HoistHandler::CheckStrideMinKS: the baby / giant strides of a plan
+Status lt_min_ks_strides(const LTPlan &pl, int *bs_stride, int *gs_stride);
 
 // Exchanges two ciphertexts' buffers and metadata
 void swap_regs(DeviceCt &x, DeviceCt &y);
@@ -420,6 +424,8 @@ class Context {
                   int additional_pt_rot, bool suppress_swap, LTPlan *out);
   // HoistHandler::Evaluate (Hoist.cu:554-975): res at pt_level - 1
   Status lt_evaluate(DeviceCt &res, const DeviceCt &in, const LTPlan &pl, const RotKeys &keys);
+  // the min-KS evaluation (Hoist.cu:490-552): two rotation keys per transform
+  Status lt_evaluate_min_ks(DeviceCt &res, const DeviceCt &in, const LTPlan &pl, const RotKeys &keys);
 
   // EvalPoly::Compile (EvalPoly.cpp:750-830) of a polynomial in the
   // Chebyshev (or power) basis for an input at (input_level, input_scale):

@@ -158,6 +158,142 @@ LTPlan::~LTPlan() {
   for (auto &p : pts) cudaFree(p.dev);
 }
 
+Status lt_min_ks_strides(const LTPlan &pl, int *bs_stride, int *gs_stride) {
+  // HoistHandler::CheckStrideMinKS, Hoist.cu:169-205: non-zero baby (giant)
+  // steps must be 1..k times their gcd
+  auto stride = [](const std::vector<int> &idx, int *out) -> bool {
+    int g = 0, cnt = 0, mx = 0;
+    for (int x : idx) {
+      if (x == 0) continue;
+      int a = g, b = x;
+      while (b) {
+        const int t = a % b;
+        a = b;
+        b = t;
+      }
+      g = a;
+      cnt++;
+      mx = std::max(mx, x);
+    }
+    *out = g;
+    return cnt * g == mx;
+  };
+  CHD_CHECK(stride(pl.bs_idx, bs_stride), kErrInvalidArg, "MinKS does not apply to the given hoist map baby-step sequence");
+  CHD_CHECK(stride(pl.gs_idx, gs_stride), kErrInvalidArg, "MinKS does not apply to the given hoist map giant-step sequence");
+  return kOk;
+}
+
+Status Context::lt_evaluate_min_ks(DeviceCt &res, const DeviceCt &in, const LTPlan &pl, const RotKeys &keys) {
+  // HoistHandler::EvaluateMinKSBabyStep / EvaluateMinKSGiantStep
+  // (Hoist.cu:490-552): baby steps by repeated HRot with the baby stride,
+  // giant steps in reverse order, accumulate, HRot by the giant stride,
+  // then Rescale.  Works in the Q basis of pt_level.
+  const int level = pl.pt_level;
+  const int n = P->n;
+  CHD_CHECK(!in.has_rx && in.np.aux == 0, kErrShape, "Hoist: input should be relinearized and mod-down");
+  CHD_CHECK(in.np == P->level_np(level), kErrShape, "Hoist: input level mismatch");
+  CHD_CHECK(!(pl.bs_idx.size() == 1 && pl.bs_idx[0] == 0), kErrInvalidArg,
+            "Hoist: min_ks should be false for bs == 1 case");
+  int bs_stride = 0, gs_stride = 0;
+  CHD_TRY(lt_min_ks_strides(pl, &bs_stride, &gs_stride));
+  auto key_of = [&](int r) -> const DeviceEvk * {
+    auto it = keys.find(r);
+    return it == keys.end() ? nullptr : it->second;
+  };
+  const NP np = P->level_np(level);
+  const int nq = np.q();
+  std::vector<int> g(nq);
+  P->gidx(np, g.data());
+  ArenaScope scope(arena);
+  // baby steps in the Q basis
+  std::vector<DeviceCt> bs(pl.bs_idx.size());
+  std::map<int, int> slot_of;
+  for (size_t i = 0; i < pl.bs_idx.size(); i++) {
+    CHD_TRY(scratch_ct(arena, bs[i], np, false, n));
+    slot_of[pl.bs_idx[i]] = static_cast<int>(i);
+  }
+  const DeviceEvk *kb = key_of(bs_stride);
+  for (size_t i = 0; i < pl.bs_idx.size(); i++) {
+    const int r = pl.bs_idx[i];
+    if (r == 0) {
+      const size_t bytes = static_cast<size_t>(nq) * n * 4;
+      cudaMemcpyAsync(bs[i].bx, in.bx, bytes, cudaMemcpyDeviceToDevice, stream);
+      cudaMemcpyAsync(bs[i].ax, in.ax, bytes, cudaMemcpyDeviceToDevice, stream);
+      bs[i].scale = in.scale;
+      bs[i].num_slots = in.num_slots;
+    } else {
+      CHD_CHECK(kb, kErrKey, "Hoist: missing rotation key " + std::to_string(bs_stride));
+      auto it = slot_of.find(r - bs_stride);
+      CHD_CHECK(it != slot_of.end(), kErrInvalidArg, "Hoist: MinKS baby-step sequence is not complete");
+      CHD_TRY(hrot(bs[i], bs[it->second], *kb, bs_stride));
+    }
+  }
+  // giant steps, reversed
+  DeviceCt acc, tmp;
+  CHD_TRY(scratch_ct(arena, acc, np, false, n));
+  CHD_TRY(scratch_ct(arena, tmp, np, false, n));
+  const DeviceEvk *kg = key_of(gs_stride);
+  bool first = true;
+  int prev = 0;
+  for (auto git = pl.gs_idx.rbegin(); git != pl.gs_idx.rend(); ++git) {
+    const int gsi = *git;
+    PtAccumDesc d{};
+    int nin = 0;
+    std::map<int, int> in_of;
+    PtAccumOut &po = d.out[0];
+    for (const auto &pt : pl.pts) {
+      if (pt.gs != gsi) continue;
+      auto f = in_of.find(pt.bs);
+      if (f == in_of.end()) {
+        CHD_CHECK(nin < kMaxPtAccumIn, kErrUnsupported, "Hoist: too many baby steps");
+        const DeviceCt &b = bs[slot_of.at(pt.bs)];
+        d.in_b[nin] = b.bx;
+        d.in_a[nin] = b.ax;
+        f = in_of.emplace(pt.bs, nin++).first;
+      }
+      CHD_CHECK(po.terms < kMaxPtAccumTerms, kErrUnsupported, "Hoist: too many terms");
+      po.term[po.terms] = static_cast<int16_t>(f->second);
+      po.pt[po.terms] = pt.dev;  // the first nq rows are the q primes
+      po.terms++;
+    }
+    for (int r = 0; r < nq; r++) {
+      d.q[r] = P->primes[g[r]];
+      d.qinv[r] = P->qinv[g[r]];
+    }
+    d.rows = nq;
+    d.n = n;
+    d.outs = 1;
+    if (first) {
+      po.b = acc.bx;
+      po.a = acc.ax;
+      launch_pt_accum(d, stream);
+    } else {
+      CHD_CHECK(prev == gsi + gs_stride, kErrInvalidArg, "Hoist: MinKS giant-step sequence is not complete");
+      po.b = tmp.bx;
+      po.a = tmp.ax;
+      launch_pt_accum(d, stream);
+      CHD_TRY(add(acc, acc, tmp));
+    }
+    acc.scale = in.scale * pl.pt_scale;
+    acc.num_slots = std::max(in.num_slots, pl.pt_slots);
+    if (gsi != 0) {
+      CHD_CHECK(kg, kErrKey, "Hoist: missing rotation key " + std::to_string(gs_stride));
+      CHD_TRY(hrot(tmp, acc, *kg, gs_stride));
+      const size_t bytes = static_cast<size_t>(nq) * n * 4;
+      cudaMemcpyAsync(acc.bx, tmp.bx, bytes, cudaMemcpyDeviceToDevice, stream);
+      cudaMemcpyAsync(acc.ax, tmp.ax, bytes, cudaMemcpyDeviceToDevice, stream);
+    } else {
+      CHD_CHECK(first || prev == gs_stride, kErrInvalidArg, "Hoist: MinKS giant-step sequence is not complete");
+    }
+    first = false;
+    prev = gsi;
+  }
+  const double sc = acc.scale;
+  CHD_TRY(rescale(res, acc));
+  res.scale = sc / P->rescale_prod[level];
+  return check_cuda("linear transform (min-KS)");
+}
+
 Status Context::lt_evaluate(DeviceCt &res, const DeviceCt &in, const LTPlan &pl, const RotKeys &keys) {
   // HoistHandler::Evaluate, Hoist.cu:554-975 (non-min-KS, fused kernels)
   const int level = pl.pt_level;

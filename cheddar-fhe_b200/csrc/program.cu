@@ -288,7 +288,11 @@ Status Context::run_program(const Program &prog, std::vector<DeviceCt> &regs, co
       case OpKind::kLinTrans:
         CHD_CHECK(lts && op.rot >= 0 && op.rot < static_cast<int>(lts->size()) && rot_keys, kErrInvalidArg,
                   "program: linear transform missing");
-        CHD_TRY(lt_evaluate(t, regs.at(op.a), *(*lts)[op.rot], *rot_keys));
+        if (keys.min_ks) {
+          CHD_TRY(lt_evaluate_min_ks(t, regs.at(op.a), *(*lts)[op.rot], *rot_keys));
+        } else {
+          CHD_TRY(lt_evaluate(t, regs.at(op.a), *(*lts)[op.rot], *rot_keys));
+        }
         break;
     }
     swap_regs(regs.at(op.dst), t);

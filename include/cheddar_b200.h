@@ -222,13 +222,16 @@ int chd_lintrans_create(chd_context *ctx, int width, int n_diag, const int *diag
                         const double *im, int pt_level, double pt_scale, int bs, int gs, int pre_rotation,
                         int additional_pt_rot, chd_lintrans **out);
 void chd_lintrans_destroy(chd_lintrans *lt);
-/* HoistHandler::AddRequiredRotations: the rotation keys the transform uses */
-int chd_lintrans_rotations(const chd_lintrans *lt, int *out, int cap, int *count);
+/* HoistHandler::AddRequiredRotations: the rotation keys the transform uses
+ * (min_ks != 0: only the baby and giant strides) */
+int chd_lintrans_rotations(const chd_lintrans *lt, int min_ks, int *out, int cap, int *count);
 /* the compiled plaintext map (giant step, baby step, message [width]) */
 int chd_lintrans_num_pts(const chd_lintrans *lt, int *count);
 int chd_lintrans_pt(const chd_lintrans *lt, int i, int *gs, int *bs, double *re, double *im);
+/* min_ks != 0: the min-KS evaluation (HoistHandler::EvaluateMinKS*,
+ * Hoist.cu:490-552): repeated rotations by the strides, in the Q basis */
 int chd_lintrans_evaluate(chd_context *ctx, const chd_lintrans *lt, chd_ciphertext *res, const chd_ciphertext *in,
-                          const chd_evk_map *keys);
+                          const chd_evk_map *keys, int min_ks);
 
 /* Compiled ciphertext programs: EvalPoly (src/extension/EvalPoly.cpp) of
  * a polynomial given by its coefficients (Chebyshev basis when chebyshev
@@ -270,12 +273,14 @@ typedef struct chd_boot chd_boot;
 int chd_boot_create(chd_context *ctx, int num_slots, int num_cts_levels, int num_stc_levels, int log_message_ratio,
                     chd_boot **out);
 void chd_boot_destroy(chd_boot *b);
-int chd_boot_rotations(const chd_boot *b, int *out, int cap, int *count);
+int chd_boot_rotations(const chd_boot *b, int min_ks, int *out, int cap, int *count);
 int chd_boot_levels(const chd_boot *b, int *levels, double *scales);
 int chd_boot_json(const chd_boot *b, char *buf, size_t cap, size_t *len);
 int chd_boot_lt_info(const chd_boot *b, int i, int *level, double *scale, int *npts, int *width);
 int chd_boot_lt_pt(const chd_boot *b, int i, int j, int *gs, int *bs, double *re, double *im);
-int chd_boot_run(chd_context *ctx, chd_boot *b, chd_ciphertext *res, const chd_ciphertext *in, const chd_evk_map *keys);
+/* Boot(res, input, evk_map, min_ks) (BootContext.h:139-140) */
+int chd_boot_run(chd_context *ctx, chd_boot *b, chd_ciphertext *res, const chd_ciphertext *in, const chd_evk_map *keys,
+                 int min_ks);
 
 /* CUDA graphs of library calls (no reference counterpart; the reference
  * issues every kernel from the host).  chd_graph_begin starts capturing the

@@ -243,11 +243,11 @@ class BootContext {
   BootContext(const BootContext &) = delete;
   BootContext &operator=(const BootContext &) = delete;
   // AddRequiredRotations: the rotation keys the client must provide
-  std::vector<int> RequiredRotations() const {
+  std::vector<int> RequiredRotations(bool min_ks = false) const {
     int n = 0;
-    check(chd_boot_rotations(b_, nullptr, 0, &n));
+    check(chd_boot_rotations(b_, min_ks ? 1 : 0, nullptr, 0, &n));
     std::vector<int> r(n);
-    check(chd_boot_rotations(b_, r.data(), n, &n));
+    check(chd_boot_rotations(b_, min_ks ? 1 : 0, r.data(), n, &n));
     return r;
   }
   int GetEndLevel() const {
@@ -258,8 +258,8 @@ class BootContext {
   void ModUpToMax(Ciphertext &res, const Ciphertext &in, const EvkMap &evk_map) const {
     check(chd_modup_to_max(ctx_.raw(), res.raw(), in.raw(), evk_map.raw()));
   }
-  void Boot(Ciphertext &res, const Ciphertext &in, const EvkMap &evk_map) {
-    check(chd_boot_run(ctx_.raw(), b_, res.raw(), in.raw(), evk_map.raw()));
+  void Boot(Ciphertext &res, const Ciphertext &in, const EvkMap &evk_map, bool min_ks = false) {
+    check(chd_boot_run(ctx_.raw(), b_, res.raw(), in.raw(), evk_map.raw(), min_ks ? 1 : 0));
   }
 
  private:

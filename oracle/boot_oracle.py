@@ -99,7 +99,20 @@ class HoistOracle:
         return self.o.permute(self.level, amount, x, num_aux=self.alpha)
 
 
-def lt_evaluate(o, level, ct, ct_scale, pts, pt_scale, keys):
+def _stride(idx):
+    """HoistHandler::CheckStrideMinKS (Hoist.cu:169-205)."""
+    import math
+    g, cnt, mx = 0, 0, 0
+    for x in idx:
+        if x:
+            g = math.gcd(g, x)
+            cnt += 1
+            mx = max(mx, x)
+    assert cnt * g == mx, "MinKS does not apply to the given sequence"
+    return g
+
+
+def lt_evaluate(o, level, ct, ct_scale, pts, pt_scale, keys, min_ks=False):
     """HoistHandler::Evaluate for the compiled map `pts` = [(gs, bs, msg)];
     keys = {rotation: (kb, ka)}.  Returns ((bx, ax) at level - 1, scale)."""
     h = HoistOracle(o, level)
@@ -107,6 +120,38 @@ def lt_evaluate(o, level, ct, ct_scale, pts, pt_scale, keys):
     enc = {(g, b): o.encode(level, pt_scale, m, num_aux=h.alpha) for g, b, m in pts}
     bs_set = sorted({b for _, b, _ in pts})
     gs_set = sorted({g for g, _, _ in pts})
+    if min_ks:
+        # EvaluateMinKSBabyStep / EvaluateMinKSGiantStep (Hoist.cu:490-552)
+        nq = h.nq
+        bstr, gstr = _stride(bs_set), _stride(gs_set)
+        bs = {}
+        for b in bs_set:
+            if b == 0:
+                bs[0] = (np.asarray(bx), np.asarray(ax))
+            else:
+                bs[b] = o.hrot(level, bs[b - bstr], keys[bstr], bstr)
+        acc = None
+        for g in reversed(gs_set):
+            sb = np.zeros((nq, o.n), dtype=np.uint32)
+            sa = np.zeros_like(sb)
+            for b in bs_set:
+                if (g, b) not in enc:
+                    continue
+                pt = enc[(g, b)]
+                for r in range(nq):
+                    q = h.primes[r]
+                    sb[r] = add_mod(sb[r], mont_mul(bs[b][0][r], pt[r], q), q)
+                    sa[r] = add_mod(sa[r], mont_mul(bs[b][1][r], pt[r], q), q)
+            if acc is not None:
+                for r in range(nq):
+                    q = h.primes[r]
+                    sb[r] = add_mod(sb[r], acc[0][r], q)
+                    sa[r] = add_mod(sa[r], acc[1][r], q)
+            acc = (sb, sa)
+            if g != 0:
+                acc = o.hrot(level, acc, keys[gstr], gstr)
+        rb, ra = o.rescale_ct(level, np.stack(acc))
+        return (rb, ra), pt_scale * ct_scale / o.rescale_prime_prod(level)
     if bs_set == [0]:
         # Hoist.cu:706-808 (single baby step 0 after the swap)
         mu = o.modup(level, ax)
@@ -195,7 +240,8 @@ def _cmul_rows(o, level, x, front, c, cfront):
     return out
 
 
-def run_program(o, prog, inp, mult_key=None, conj_key=None, rot_keys=None, lts=None, sse_keys=None):
+def run_program(o, prog, inp, mult_key=None, conj_key=None, rot_keys=None, lts=None, sse_keys=None,
+                min_ks=False):
     """Runs a compiled program (the dict of chd_program_json) on `inp`
     (a Ct); returns the output Ct.  sse_keys = (dts, std) selects
     ModUpToMax with sparse-secret encapsulation."""
@@ -310,7 +356,8 @@ def run_program(o, prog, inp, mult_key=None, conj_key=None, rot_keys=None, lts=N
         elif k == K_LIN_TRANS:
             x = regs[a]
             plan = lts[op["r"]]
-            (rb, ra), sc = lt_evaluate(o, plan["level"], x.parts, x.scale, plan["pts"], plan["scale"], rot_keys)
+            (rb, ra), sc = lt_evaluate(o, plan["level"], x.parts, x.scale, plan["pts"], plan["scale"], rot_keys,
+                                       min_ks=min_ks)
             regs[d] = Ct(plan["level"] - 1, [rb, ra], sc)
         else:
             raise ValueError(f"unknown op {k}")

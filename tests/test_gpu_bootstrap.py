@@ -25,7 +25,7 @@ def _setup():
     s = o.gen_secret(99, 32)
     mk = o.gen_mult_key(77, s)
     ck = o.gen_conj_key(78, s)
-    rks = {r: o.gen_rot_key(1000 + r, s, r) for r in bc.rotations()}
+    rks = {r: o.gen_rot_key(1000 + r, s, r) for r in sorted(set(bc.rotations()) | set(bc.rotations(min_ks=True)))}
     keys = chd.EvkMap(g)
     keys.set_mult(g.evk(*mk))
     keys.set_conjugation(g.evk(*ck))
@@ -61,3 +61,24 @@ def test_boot_bit_exact_and_precision(cuda_ok):
     bits = -np.log2(err)
     print(f"bootstrapping precision: {bits:.2f} bits (max error {err:.3e})")
     assert bits > 10, bits
+
+
+def test_boot_min_ks_bit_exact_and_precision(cuda_ok):
+    # Boot(res, input, evk_map, min_ks = true): the reference's Boot-MinKS
+    # test (unittest/Bootstrapping.cpp:34-36); two keys per transform
+    o, g, bc, s, mk, ck, rks, keys = _setup()
+    assert len(bc.rotations(min_ks=True)) < len(bc.rotations())
+    rng = np.random.default_rng(4048)
+    half = o.n // 2
+    msg = (rng.random(half) * 2 - 1) + 1j * (rng.random(half) * 2 - 1)
+    sc0 = o.scale(0)
+    bx, ax = o.encrypt(8, s, 0, o.encode(0, sc0, msg))
+    res = bc.Boot(g.import_ct(0, [bx, ax], sc0), keys, min_ks=True)
+    parts = res.numpy()
+    ref = run_program(o, bc.json(), Ct(0, [bx, ax], sc0), mult_key=mk, conj_key=ck, rot_keys=rks,
+                      lts=bc.transforms(), min_ks=True)
+    assert np.array_equal(parts[0], ref.parts[0]) and np.array_equal(parts[1], ref.parts[1])
+    dec = o.decode(bc.end_level, bc.final_scale, o.decrypt(s, bc.end_level, parts), half)
+    err = np.abs(dec - msg).max()
+    print(f"min-KS bootstrapping precision: {-np.log2(err):.2f} bits")
+    assert -np.log2(err) > 10

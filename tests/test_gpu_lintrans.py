@@ -53,3 +53,27 @@ def test_lintrans_bit_exact(cuda_ok, idx, bs, gs):
     assert abs(info["scale"] - rscale) <= 1e-9 * rscale
     dec = o.decode(LEVEL - 1, rscale, o.decrypt(secret(KS), LEVEL - 1, parts), width)
     assert np.abs(dec - _matvec(diags, msg)).max() < 1e-3
+
+
+def test_lintrans_min_ks_bit_exact(cuda_ok):
+    # the min-KS evaluation (two rotation keys: the baby and giant strides)
+    o, g = pair(KS)
+    width = o.n // 2
+    diags = _diags(list(range(16)), width, seed=99)
+    pt_scale = o.rescale_prime_prod(LEVEL)
+    lt = chd.LinearTransform(g, diags, LEVEL, pt_scale, 4, 4)
+    rots = lt.rotations(min_ks=True)
+    assert rots == [1, 4]
+    keys = chd.EvkMap(g)
+    host_keys = {}
+    for r in rots:
+        (kb, ka), k = rot_key(KS, r)
+        keys.set_rotation(r, k)
+        host_keys[r] = (kb, ka)
+    (bx, ax), sc, msg = fresh_ct(KS, LEVEL, 41)
+    res = lt.evaluate(g.import_ct(LEVEL, [bx, ax], sc), keys, min_ks=True)
+    (rb, ra), rscale = lt_evaluate(o, LEVEL, (bx, ax), sc, lt.plaintexts(), pt_scale, host_keys, min_ks=True)
+    parts = res.numpy()
+    assert np.array_equal(parts[0], rb) and np.array_equal(parts[1], ra)
+    dec = o.decode(LEVEL - 1, rscale, o.decrypt(secret(KS), LEVEL - 1, parts), width)
+    assert np.abs(dec - _matvec(diags, msg)).max() < 1e-3
