@@ -71,14 +71,17 @@ __global__ void __launch_bounds__(128) k_modswitch_cols(const __grid_constant__ 
     __syncthreads();
   }
 
-  // ---- phase B: exact BConv per target, then NTT column stages
-  for (int m = 0; m < jb.M; m++) {
+  // ---- phase B: exact BConv per target, then NTT column stages.  Targets
+  // go in pairs: the two BConv accumulations share the source loads from
+  // shared memory, and the two radix-16 column stages are independent
+  // instruction streams (the kernel is latency-bound at 2-3 warps per
+  // scheduler); the radix-8 stages then pass through the exchange buffer
+  // one target after the other.
+  auto bconv = [&](int m, uint32_t (&v)[16]) {
     const int g = jb.dst_gidx[m];
     const uint32_t p = __ldg(b.primes + g);
     const int32_t pinv = __ldg(b.qinvs + g);
-    const uint2 *tw = b.tw + (static_cast<size_t>(g) << 16);
     const int32_t *T = jb.table + m * K;
-    uint32_t v[16];
 #pragma unroll
     for (int e = 0; e < 16; e++) v[e] = 0;
 #pragma unroll
@@ -105,7 +108,51 @@ __global__ void __launch_bounds__(128) k_modswitch_cols(const __grid_constant__ 
         for (int e = 0; e < 16; e++) v[e] = add_mod(v[e], mont_reduce(a[e], p, pinv), p);
       }
     }
-    radix16_cols_fwd(v, tw, p);  // stages m = 1, 2, 4, 8 on rows rg + 8e
+  };
+  auto bconv2 = [&](int m0, int m1, uint32_t (&v0)[16], uint32_t (&v1)[16]) {
+    const int g0 = jb.dst_gidx[m0], g1 = jb.dst_gidx[m1];
+    const uint32_t p0 = __ldg(b.primes + g0), p1 = __ldg(b.primes + g1);
+    const int32_t pi0 = __ldg(b.qinvs + g0), pi1 = __ldg(b.qinvs + g1);
+    const int32_t *T0 = jb.table + m0 * K, *T1 = jb.table + m1 * K;
+#pragma unroll
+    for (int e = 0; e < 16; e++) v0[e] = v1[e] = 0;
+#pragma unroll
+    for (int k0 = 0; k0 < KMAX; k0 += 4) {
+      if (k0 < K) {
+        int64_t a0[16], a1[16];
+#pragma unroll
+        for (int e = 0; e < 16; e++) a0[e] = a1[e] = 0;
+#pragma unroll
+        for (int k = k0; k < k0 + 4; k++) {
+          if (k < K) {
+            const int64_t t0 = __ldg(T0 + k), t1 = __ldg(T1 + k);
+#pragma unroll
+            for (int e4 = 0; e4 < 4; e4++) {
+              const int4 xv = xs4[(k * 4 + e4) * 128 + t];
+              a0[4 * e4] += static_cast<int64_t>(xv.x) * t0;
+              a1[4 * e4] += static_cast<int64_t>(xv.x) * t1;
+              a0[4 * e4 + 1] += static_cast<int64_t>(xv.y) * t0;
+              a1[4 * e4 + 1] += static_cast<int64_t>(xv.y) * t1;
+              a0[4 * e4 + 2] += static_cast<int64_t>(xv.z) * t0;
+              a1[4 * e4 + 2] += static_cast<int64_t>(xv.z) * t1;
+              a0[4 * e4 + 3] += static_cast<int64_t>(xv.w) * t0;
+              a1[4 * e4 + 3] += static_cast<int64_t>(xv.w) * t1;
+            }
+          }
+        }
+#pragma unroll
+        for (int e = 0; e < 16; e++) {
+          v0[e] = add_mod(v0[e], mont_reduce(a0[e], p0, pi0), p0);
+          v1[e] = add_mod(v1[e], mont_reduce(a1[e], p1, pi1), p1);
+        }
+      }
+    }
+  };
+  // radix-8 row groups of one target from the exchange buffer to HBM
+  auto finish = [&](int m, const uint32_t (&v)[16]) {
+    const int g = jb.dst_gidx[m];
+    const uint32_t p = __ldg(b.primes + g);
+    const uint2 *tw = b.tw + (static_cast<size_t>(g) << 16);
 #pragma unroll
     for (int e = 0; e < 16; e++) ex[exi(rg + 8 * e, cl)] = v[e];
     __syncthreads();
@@ -121,6 +168,27 @@ __global__ void __launch_bounds__(128) k_modswitch_cols(const __grid_constant__ 
       for (int u = 0; u < 8; u++) dst[(8 * j + u) * 512 + col] = y[u];
     }
     __syncthreads();
+  };
+  int m = 0;
+  for (; m + 1 < jb.M; m += 2) {
+    uint32_t v0[16], v1[16];
+    bconv2(m, m + 1, v0, v1);
+    {
+      const uint32_t p0 = __ldg(b.primes + jb.dst_gidx[m]), p1 = __ldg(b.primes + jb.dst_gidx[m + 1]);
+      const uint2 *tw0 = b.tw + (static_cast<size_t>(jb.dst_gidx[m]) << 16);
+      const uint2 *tw1 = b.tw + (static_cast<size_t>(jb.dst_gidx[m + 1]) << 16);
+      radix16_cols_fwd(v0, tw0, p0);  // stages m = 1, 2, 4, 8 on rows rg + 8e
+      radix16_cols_fwd(v1, tw1, p1);
+    }
+    finish(m, v0);
+    finish(m + 1, v1);
+  }
+  if (m < jb.M) {
+    uint32_t v[16];
+    bconv(m, v);
+    const uint2 *tw = b.tw + (static_cast<size_t>(jb.dst_gidx[m]) << 16);
+    radix16_cols_fwd(v, tw, __ldg(b.primes + jb.dst_gidx[m]));
+    finish(m, v);
   }
 }
 
