@@ -18,6 +18,9 @@ Reported (one JSON line on rank 0):
   cpu_baseline  the CPU oracle's HMult on the host cores (bounded sample)
   bootstrap  full-slot bootstrapping throughput at N = 2^16 (bootstraps/s;
              --boot-precision adds a real-key run with decoded precision)
+  ks_engines  the same step with the ModUp / ModDown column passes on each
+             engine (--ks-engine picks the measured one; default cuda, the
+             faster one on this workload)
   bconv_engines  base conversion on CUDA cores vs tcgen05 tensor cores
 `--impl reference` times the CPU implementation of the path (the oracle;
 the reference itself has no CPU path and cannot be built here) on the same
@@ -156,6 +159,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-boot", action="store_true", help="skip the bootstrapping measurement")
     ap.add_argument("--boot-batch", type=int, default=8)
+    ap.add_argument("--ks-engine", default="cuda", choices=["cuda", "tensor"],
+                    help="base conversion inside the ModUp / ModDown column passes of the measured path")
     ap.add_argument("--boot-precision", action="store_true",
                     help="also bootstrap one ciphertext with real keys (oracle key generation, slow) "
                          "and report decoded precision in bits")
@@ -181,6 +186,7 @@ def main():
     ctx = chd.Context(json.dumps(params), device=local)
     stream = torch.cuda.Stream()
     ctx.set_stream(stream.cuda_stream)
+    ctx.ks_engine = ks_engine_id(chd, args)
     lvl = ctx.max_level
     nq = ctx.num_q(lvl)
     n = ctx.n
@@ -243,6 +249,9 @@ def main():
     roof = roofline_from_stages(ctx, lvl, B, stages, args.steps)
     launches = sum(nl for _, nl in stages.values())
 
+    # ---- the same step with each column-pass engine ----
+    ks_cmp = ks_engines(ctx, chd, step, stream, args.steps, B)
+
     # ---- base conversion as a dense contraction: CUDA cores vs tensor cores ----
     bconv_cmp = bconv_engines(ctx, chd, stream)
 
@@ -260,7 +269,8 @@ def main():
                                "(31-bit), dnum=3, top level", "batch_per_gpu": B,
                    "l2": "inputs larger than L2 (batch x 24 MB + 48 MB key)",
                    "parallelism": f"replicas x{world}"},
-        "e2e": e2e, "roofline": roof, "clocks": sampler.summary(), "bconv_engines": bconv_cmp,
+        "e2e": e2e, "roofline": roof, "clocks": sampler.summary(), "ks_engine": args.ks_engine,
+        "ks_engines": ks_cmp, "bconv_engines": bconv_cmp,
         "bootstrap": boot, "hoisted_and_mixed": hoist_mixed,
         "gpu_launches": launches,
     }
@@ -412,6 +422,43 @@ def roofline_from_stages(ctx, lvl, batch, stages, steps):
             "algorithmic_bytes_per_launch": algo, "ms_per_launch": ms,
             "stage_ms_per_step": {k: v[0] / steps for k, v in stages.items()},
             "stage_launches_per_step": {k: v[1] / steps for k, v in stages.items()}}
+
+
+def ks_engine_id(chd, args):
+    return chd.BCONV_TENSOR_CORE if args.ks_engine == "tensor" else chd.BCONV_CUDA_CORE
+
+
+def ks_engines(ctx, chd, step, stream, steps, B):
+    """The HMult step with the ModUp / ModDown column passes on each engine
+    (CUDA-core int64 BConv vs tcgen05 INT8 byte-limb MMAs); residues are
+    identical (tests), only the time differs."""
+    import torch
+    old = ctx.ks_engine
+    out = {}
+    for name, e in (("cuda_core", chd.BCONV_CUDA_CORE), ("tensor_core", chd.BCONV_TENSOR_CORE)):
+        ctx.ks_engine = e
+        for _ in range(3):
+            step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        ctx.stage_timing(True)
+        for _ in range(steps):
+            step()
+        st = ctx.stage_times()
+        ctx.stage_timing(False)
+        out[name] = {"hmult_per_s": B * steps / (ms / 1e3), "ms_per_step": ms / steps,
+                     "modup_cols_ms": st["modup_cols"][0] / steps, "moddown_cols_ms": st["moddown_cols"][0] / steps}
+    ctx.ks_engine = old
+    out["speedup_tensor_vs_cuda_core"] = out["tensor_core"]["hmult_per_s"] / out["cuda_core"]["hmult_per_s"]
+    out["column_pass_speedup"] = ((out["cuda_core"]["modup_cols_ms"] + out["cuda_core"]["moddown_cols_ms"]) /
+                                  (out["tensor_core"]["modup_cols_ms"] + out["tensor_core"]["moddown_cols_ms"]))
+    return out
 
 
 def bconv_engines(ctx, chd, stream, npoly=64, reps=10):
@@ -576,6 +623,7 @@ def boot_bench(chd, args, stream, dist):
     params = json.load(open(os.path.join(chd.PARAM_DIR, BOOT_PARAM_FILE)))
     ctx = chd.Context(json.dumps(params), device=torch.cuda.current_device())
     ctx.set_stream(stream.cuda_stream)
+    ctx.ks_engine = ks_engine_id(chd, args)
     t0 = time.time()
     bc = chd.BootContext(ctx)
     plan_s = time.time() - t0
@@ -650,10 +698,29 @@ def boot_bench(chd, args, stream, dist):
     ctx.synchronize()
     torch.cuda.synchronize()
     ms_mk = e2.elapsed_time(e3)
+    # the same bootstraps with each column-pass engine
+    engines = {}
+    main_engine = ctx.ks_engine
+    for name, e in (("cuda_core", chd.BCONV_CUDA_CORE), ("tensor_core", chd.BCONV_TENSOR_CORE)):
+        ctx.ks_engine = e
+        step()
+        ctx.synchronize()
+        e2.record(stream)
+        for _ in range(steps):
+            step()
+        e3.record(stream)
+        ctx.synchronize()
+        torch.cuda.synchronize()
+        t = e2.elapsed_time(e3)
+        engines[name] = {"ms_per_boot": t / (B * steps), "bootstraps_per_s": B * steps / (t / 1e3)}
+    ctx.ks_engine = main_engine
+    engines["speedup_tensor_vs_cuda_core"] = (engines["tensor_core"]["bootstraps_per_s"] /
+                                              engines["cuda_core"]["bootstraps_per_s"])
     res = {"metric": "bootstraps/s (full slots, N=2^16)", "value": world * B * steps / (ms / 1e3),
            "min_ks": {"ms_per_boot": ms_mk / (B * steps), "bootstraps_per_s": B * steps / (ms_mk / 1e3),
                       "rotation_keys": len(bc.rotations(min_ks=True))},
            "unit": "bootstraps/s", "ms_per_boot": ms / (B * steps), "batch_per_gpu": B, "steps": steps,
+           "ks_engine": args.ks_engine, "ks_engines": engines,
            "warmup": 2, "params": "48 q primes (bootparam_30 level shape), alpha=12, 4 CtS + 3 StC levels, "
                                   "EvalMod deg-30 Chebyshev cosine + 3 double angles",
            "rotation_keys": len(bc.rotations()), "plan_seconds": plan_s,

@@ -56,6 +56,8 @@ def lib():
         "chd_context_set_stream": (i, [vp, vp]),
         "chd_context_synchronize": (i, [vp]),
         "chd_stage_timing": (i, [vp, i]),
+        "chd_set_ks_engine": (i, [vp, i]),
+        "chd_get_ks_engine": (i, [vp]),
         "chd_stage_times": (i, [vp, vp, vp]),
         "chd_level_np": (i, [vp, i, C.POINTER(i), C.POINTER(i)]),
         "chd_max_level": (i, [vp]),
@@ -209,6 +211,16 @@ class Context:
         g = C.c_void_p()
         _check(lib().chd_graph_end(self.ptr, C.byref(g)))
         return Graph(self, g)
+
+    @property
+    def ks_engine(self):
+        """Base-conversion engine of the key-switching and rescaling paths:
+        BCONV_CUDA_CORE or BCONV_TENSOR_CORE (bit-identical residues)."""
+        return lib().chd_get_ks_engine(self.ptr)
+
+    @ks_engine.setter
+    def ks_engine(self, engine):
+        _check(lib().chd_set_ks_engine(self.ptr, int(engine)))
 
     def stage_timing(self, enable):
         """Start (clearing earlier records) or stop device timing of the fused

@@ -132,6 +132,16 @@ int chd_stage_timing(chd_context *ctx, int enable) {
   return CHD_OK;
 }
 
+int chd_set_ks_engine(chd_context *ctx, int engine) {
+  CHD_NOTNULL(ctx);
+  if (engine != CHD_BCONV_CUDA_CORE && engine != CHD_BCONV_TENSOR_CORE)
+    return fail(CHD_ERR_INVALID_ARG, "chd_set_ks_engine: engine must be CHD_BCONV_CUDA_CORE or CHD_BCONV_TENSOR_CORE");
+  ctx->c->ks_engine = engine;
+  return CHD_OK;
+}
+
+int chd_get_ks_engine(const chd_context *ctx) { return ctx ? ctx->c->ks_engine : -1; }
+
 int chd_stage_times(chd_context *ctx, double *ms, int *launches) {
   CHD_NOTNULL(ctx);
   if (!ms || !launches) return fail(CHD_ERR_INVALID_ARG, "chd_stage_times: null output");

@@ -1069,6 +1069,8 @@ Status Context::modup_fused(int level, int count, const uint32_t *const *src, ui
     }
   for_row_batches(rows, [&](const RowBatch &rb) { launch_ntt_inv_rows(rb, P->log_n, stream); });
   MSColBatch b{};
+  b.engine = ks_engine;
+  b.err = d_err;
   b.tw = d_tw;
   b.itw = d_itw;
   b.primes = d_primes;
@@ -1212,6 +1214,8 @@ Status Context::key_switch_fused(int level, int count, const KSIn *in, const Dev
     nl = 0;
     t0 = timer_mark();
     MSColBatch b{};
+    b.engine = ks_engine;
+    b.err = d_err;
     b.tw = d_tw;
     b.itw = d_itw;
     b.primes = d_primes;
@@ -1300,6 +1304,8 @@ Status Context::key_switch_fused(int level, int count, const KSIn *in, const Dev
   // 4. ModDown column pass per (ciphertext, part)
   {
     MSColBatch b{};
+    b.engine = ks_engine;
+    b.err = d_err;
     b.tw = d_tw;
     b.itw = d_itw;
     b.primes = d_primes;
@@ -1418,6 +1424,8 @@ Status Context::moddown(int level, MDType type, const uint32_t *const *src, uint
   if (fused) {
     for_row_batches(rows, [&](const RowBatch &rb) { launch_ntt_inv_rows(rb, P->log_n, stream); });
     MSColBatch b{};
+    b.engine = ks_engine;
+    b.err = d_err;
     b.tw = d_tw;
     b.itw = d_itw;
     b.primes = d_primes;

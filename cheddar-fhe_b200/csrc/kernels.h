@@ -158,12 +158,17 @@ struct MSColJob {
 constexpr int kMaxMSColJobs = 24;
 struct MSColBatch {
   int count;
+  int engine;             // base conversion on 0: CUDA cores, 1: tensor cores
+  int *err;               // set to 1 when a tensor-core wait gives up
   const uint2 *tw, *itw;  // twiddle tables [nprimes][N]
   const uint32_t *primes;
   const int32_t *qinvs;
   MSColJob jobs[kMaxMSColJobs];
 };
 void launch_modswitch_cols(const MSColBatch &b, int log_n, cudaStream_t s);
+// tensor-core column pass (modswitch_tc.cu); every job has K <= 16
+void launch_modswitch_cols_tc(const MSColBatch &b, int max_k, cudaStream_t s);
+size_t modswitch_cols_tc_smem(int kmax);
 void launch_ntt_inv_rows(const RowBatch &rb, int log_n, cudaStream_t s);
 
 // Fused key-switching row pass (N = 2^16), see keyswitch.cu.  Modes:

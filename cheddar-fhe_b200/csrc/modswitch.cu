@@ -14,21 +14,18 @@
 // the same stage schedule as ntt.cu (radix-16 on rows rg + 8k in registers,
 // radix-8 on rows 8j + u after one shared-memory exchange).
 #include "arith.cuh"
+#include "colpass.cuh"
 #include "kernels.h"
 #include "ntt_common.cuh"
 
 namespace chd {
 namespace {
 
-constexpr int kTC = 16;          // columns per tile
-constexpr int kExRows = 136;     // 128 rows + one padding row per 16 rows
-
-// exchange-buffer index: a 16-word gap every 16 rows keeps both access
-// patterns (rows rg + 8k and rows 8j + u) free of bank conflicts
-__device__ __forceinline__ int exi(int row, int col) { return (row + (row >> 4)) * kTC + col; }
-
-template <int KMAX>
-__global__ void __launch_bounds__(128) k_modswitch_cols(const __grid_constant__ MSColBatch b) {
+// KMAX sources live in shared memory; with KR > 0 the sources KMAX ..
+// KMAX + KR - 1 stay in registers (so that K = 13, 14 do not need
+// the shared memory, and the lower occupancy, of the next larger KMAX).
+template <int KMAX, int KR>
+__global__ void __launch_bounds__(128, KMAX <= 8 ? 3 : 2) k_modswitch_cols(const __grid_constant__ MSColBatch b) {
   extern __shared__ uint32_t smem[];
   const MSColJob &jb = b.jobs[blockIdx.y];
   uint32_t *ex = smem;
@@ -39,6 +36,8 @@ __global__ void __launch_bounds__(128) k_modswitch_cols(const __grid_constant__ 
   const int cl = lane & 15, rg = 2 * w + (lane >> 4);
   const int col = blockIdx.x * kTC + cl;
   const int K = jb.K;
+  const int Ks = K < KMAX ? K : KMAX;  // sources in shared memory
+  int32_t xr[KR > 0 ? KR : 1][16];     // sources in registers
 
   // ---- phase A: INTT column stages, output constant, centring -> xs
   for (int k = 0; k < K; k++) {
@@ -65,11 +64,37 @@ __global__ void __launch_bounds__(128) k_modswitch_cols(const __grid_constant__ 
     int32_t v[16];
 #pragma unroll
     for (int e = 0; e < 16; e++) v[e] = centre(reduce2q(shoup_lazy(x[e], c0, c0s, q), q), q);
+    if (k < KMAX) {
 #pragma unroll
-    for (int e4 = 0; e4 < 4; e4++)
-      xs4[(k * 4 + e4) * 128 + t] = make_int4(v[4 * e4], v[4 * e4 + 1], v[4 * e4 + 2], v[4 * e4 + 3]);
+      for (int e4 = 0; e4 < 4; e4++)
+        xs4[(k * 4 + e4) * 128 + t] = make_int4(v[4 * e4], v[4 * e4 + 1], v[4 * e4 + 2], v[4 * e4 + 3]);
+    } else {
+#pragma unroll
+      for (int r = 0; r < KR; r++)
+        if (k == KMAX + r)
+#pragma unroll
+          for (int e = 0; e < 16; e++) xr[r][e] = v[e];
+    }
     __syncthreads();
   }
+  // register sources of target row T: one more Montgomery chunk (at most 4 terms)
+  auto reg_part = [&](const int32_t *T, uint32_t p, int32_t pinv, uint32_t (&v)[16]) {
+    if (KR > 0 && K > KMAX) {
+      int64_t a[16];
+#pragma unroll
+      for (int e = 0; e < 16; e++) a[e] = 0;
+#pragma unroll
+      for (int r = 0; r < KR; r++) {
+        if (KMAX + r < K) {
+          const int64_t tk = __ldg(T + KMAX + r);
+#pragma unroll
+          for (int e = 0; e < 16; e++) a[e] += static_cast<int64_t>(xr[r][e]) * tk;
+        }
+      }
+#pragma unroll
+      for (int e = 0; e < 16; e++) v[e] = add_mod(v[e], mont_reduce(a[e], p, pinv), p);
+    }
+  };
 
   // ---- phase B: exact BConv per target, then NTT column stages.  Targets
   // go in pairs: the two BConv accumulations share the source loads from
@@ -86,13 +111,13 @@ __global__ void __launch_bounds__(128) k_modswitch_cols(const __grid_constant__ 
     for (int e = 0; e < 16; e++) v[e] = 0;
 #pragma unroll
     for (int k0 = 0; k0 < KMAX; k0 += 4) {
-      if (k0 < K) {
+      if (k0 < Ks) {
         int64_t a[16];
 #pragma unroll
         for (int e = 0; e < 16; e++) a[e] = 0;
 #pragma unroll
         for (int k = k0; k < k0 + 4; k++) {
-          if (k < K) {
+          if (k < Ks) {
             const int64_t tk = __ldg(T + k);
 #pragma unroll
             for (int e4 = 0; e4 < 4; e4++) {
@@ -108,6 +133,7 @@ __global__ void __launch_bounds__(128) k_modswitch_cols(const __grid_constant__ 
         for (int e = 0; e < 16; e++) v[e] = add_mod(v[e], mont_reduce(a[e], p, pinv), p);
       }
     }
+    reg_part(T, p, pinv, v);
   };
   auto bconv2 = [&](int m0, int m1, uint32_t (&v0)[16], uint32_t (&v1)[16]) {
     const int g0 = jb.dst_gidx[m0], g1 = jb.dst_gidx[m1];
@@ -118,13 +144,13 @@ __global__ void __launch_bounds__(128) k_modswitch_cols(const __grid_constant__ 
     for (int e = 0; e < 16; e++) v0[e] = v1[e] = 0;
 #pragma unroll
     for (int k0 = 0; k0 < KMAX; k0 += 4) {
-      if (k0 < K) {
+      if (k0 < Ks) {
         int64_t a0[16], a1[16];
 #pragma unroll
         for (int e = 0; e < 16; e++) a0[e] = a1[e] = 0;
 #pragma unroll
         for (int k = k0; k < k0 + 4; k++) {
-          if (k < K) {
+          if (k < Ks) {
             const int64_t t0 = __ldg(T0 + k), t1 = __ldg(T1 + k);
 #pragma unroll
             for (int e4 = 0; e4 < 4; e4++) {
@@ -147,6 +173,8 @@ __global__ void __launch_bounds__(128) k_modswitch_cols(const __grid_constant__ 
         }
       }
     }
+    reg_part(T0, p0, pi0, v0);
+    reg_part(T1, p1, pi1, v1);
   };
   // radix-8 row groups of one target from the exchange buffer to HBM
   auto finish = [&](int m, const uint32_t (&v)[16]) {
@@ -201,20 +229,27 @@ namespace {
 void launch_batch(const MSColBatch &b, cudaStream_t s) {
   int max_k = 0;
   for (int j = 0; j < b.count; j++) max_k = b.jobs[j].K > max_k ? b.jobs[j].K : max_k;
-  const dim3 grid(512 / kTC, b.count);
-  if (max_k <= 8) {
-    const size_t sm = modswitch_cols_smem(8);
-    cudaFuncSetAttribute(k_modswitch_cols<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm));
-    k_modswitch_cols<8><<<grid, 128, sm, s>>>(b);
-  } else if (max_k <= 12) {
-    const size_t sm = modswitch_cols_smem(12);
-    cudaFuncSetAttribute(k_modswitch_cols<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm));
-    k_modswitch_cols<12><<<grid, 128, sm, s>>>(b);
-  } else {
-    const size_t sm = modswitch_cols_smem(16);
-    cudaFuncSetAttribute(k_modswitch_cols<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm));
-    k_modswitch_cols<16><<<grid, 128, sm, s>>>(b);
+  if (b.engine == 1) {
+    launch_modswitch_cols_tc(b, max_k, s);
+    return;
   }
+  const dim3 grid(512 / kTC, b.count);
+  auto go = [&](auto kern, int kmax) {
+    const size_t sm = modswitch_cols_smem(kmax);
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm));
+    kern<<<grid, 128, sm, s>>>(b);
+  };
+  // K = 9 stays with KMAX = 12: at 3 CTAs per SM (KMAX = 8 and one
+  // register source) the 168-register cap and the second wave of a
+  // 512-CTA grid cost more than the occupancy gains
+  if (max_k <= 8)
+    go(k_modswitch_cols<8, 0>, 8);
+  else if (max_k <= 12)
+    go(k_modswitch_cols<12, 0>, 12);
+  else if (max_k <= 14)
+    go(k_modswitch_cols<12, 2>, 12);
+  else
+    go(k_modswitch_cols<16, 0>, 16);
 }
 
 int sm_count() {

@@ -307,6 +307,18 @@ void chd_graph_destroy(chd_graph *g);
 int chd_bconv_batch(chd_context *ctx, int engine, int npoly, const int32_t *xt_dev, const int *src_gidx, int K,
                     const int *dst_gidx, int M, uint32_t *out_dev);
 
+/* Engine of the base conversion inside every ModUp / ModDown of the fused
+ * key-switching, rescaling and bootstrapping paths (HMult, relinearize,
+ * rotations, hoisted rotations, linear transforms, ModDown epilogues):
+ * CHD_BCONV_CUDA_CORE (int64 multiply-adds) or CHD_BCONV_TENSOR_CORE (the
+ * column pass issues INT8 byte-limb MMAs on the tcgen05 tensor cores with
+ * int32 accumulation in TMEM).  Both give bit-identical residues.  No
+ * reference counterpart (the reference has one CUDA-core implementation,
+ * src/core/ModSwitch.cu:23-171).  chd_get_ks_engine returns the engine, -1
+ * for a null context. */
+int chd_set_ks_engine(chd_context *ctx, int engine);
+int chd_get_ks_engine(const chd_context *ctx);
+
 /* ModUp like chd_modup_raw, but allocating no device memory: for callers
  * that must not allocate once running (latency-critical servers, where a
  * cudaMalloc can synchronise the device; hosts whose device memory belongs
