@@ -26,6 +26,8 @@ void unused_paths(cheddar_b200::Context &ctx, const cheddar_b200::EvaluationKey 
   m.SetSparseToDenseKey(k);
   bc.Boot(b, a, m);
   std::vector<uint32_t> cx = ctx.EncodeConstant(0, 1.0, 0.5);
+  ctx.SetKeySwitchEngine(CHD_BCONV_TENSOR_CORE);
+  int eng = ctx.KeySwitchEngine();
   ctx.HMultBatch({&b}, {&a}, {&a}, k, true);
   ctx.BeginGraph();
   chd_graph *g = ctx.EndGraph();
@@ -33,6 +35,7 @@ void unused_paths(cheddar_b200::Context &ctx, const cheddar_b200::EvaluationKey 
   chd_graph_destroy(g);
   (void)r;
   (void)cx;
+  (void)eng;
 }
 int main() {
   try {
