@@ -126,6 +126,7 @@ def lib():
         "chd_program_run": (i, [vp, vp, vp, vp, vp]),
         "chd_boot_mod_coefficients": (i, [vp, i]),
         "chd_boot_create": (i, [vp, i, i, i, i, pp]),
+        "chd_boot_create_variant": (i, [vp, i, i, i, i, i, pp]),
         "chd_boot_destroy": (None, [vp]),
         "chd_boot_rotations": (i, [vp, i, vp, i, C.POINTER(i)]),
         "chd_boot_levels": (i, [vp, vp, vp]),
@@ -609,16 +610,22 @@ class Program:
         return res
 
 
-class BootContext:
-    """BootContext prepared for `num_slots` (full slots): CoeffToSlot,
-    EvalMod, SlotToCoeff (src/extension/BootContext.cpp)."""
+BOOT_NORMAL, BOOT_IMAGINARY_REMOVING, BOOT_MERGE_TWO_REAL = 0, 1, 2   # BootVariant
 
-    def __init__(self, ctx, num_slots=None, num_cts_levels=4, num_stc_levels=3, log_message_ratio=5):
+
+class BootContext:
+    """BootContext prepared for `num_slots` (a power of two from 256 to N/2)
+    and a BootVariant: CoeffToSlot, EvalMod, SlotToCoeff
+    (src/extension/BootContext.cpp)."""
+
+    def __init__(self, ctx, num_slots=None, num_cts_levels=4, num_stc_levels=3, log_message_ratio=5,
+                 variant=BOOT_NORMAL):
         self.ctx = ctx
         self.ptr = C.c_void_p()
         ns = num_slots if num_slots is not None else ctx.n // 2
-        _check(lib().chd_boot_create(ctx.ptr, ns, num_cts_levels, num_stc_levels, log_message_ratio,
-                                     C.byref(self.ptr)))
+        self.num_slots, self.variant = ns, variant
+        _check(lib().chd_boot_create_variant(ctx.ptr, ns, variant, num_cts_levels, num_stc_levels,
+                                             log_message_ratio, C.byref(self.ptr)))
         lv = (C.c_int * 5)()
         sc = (C.c_double * 5)()
         _check(lib().chd_boot_levels(self.ptr, lv, sc))

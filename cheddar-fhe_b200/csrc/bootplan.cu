@@ -11,7 +11,11 @@
 //   BootContext::Boot (BootContext.cpp:296-370): scale-up at level -1,
 //     ModUpToMax, CoeffToSlot, real / imaginary split, EvalMod on each,
 //     recombination, SlotToCoeff.
-// Full-slot bootstrapping (N/2 slots) without sparse-secret encapsulation.
+// Any power-of-two slot count from 256 to N/2.  With fewer than N/2 slots
+// (BootContext.cpp:321-360, EvalSpecialFFT.cpp:212-226, 268-282, 350-362):
+// a Trace after ModUpToMax, the last CtS and the first StC phase extended
+// to 2n x 2n matrices (the real and imaginary parts side by side), one
+// EvalMod on HConj(x) + x, and a final HRotAdd by n.
 #include <algorithm>
 #include <cmath>
 
@@ -53,16 +57,38 @@ std::pair<int, int> bsgs_split(int num_diag) {
   return {bs, (num_diag + bs - 1) / bs};
 }
 
+// The 2n x 2n matrix [[D, 0], [0, D f]] in diagonal form (rotation index i
+// >= n/2 moves to i + n): the last CtS phase (f = -i) and the first StC
+// phase (f = i) of a sparse-slot bootstrap, EvalSpecialFFT.cpp:212-226,
+// 268-282
+SMat extend_sparse(const SMat &ph, int ns, cd f) {
+  SMat e;
+  e.h = e.w = 2 * ns;
+  for (const auto &d : ph.d) {
+    const int dst = d.first >= ns / 2 ? d.first + ns : d.first;
+    std::vector<cd> &v = e.d.emplace(dst, std::vector<cd>(2 * ns, cd(0))).first->second;
+    for (int j = 0; j < ns; j++) {
+      v[j] = d.second[j];
+      v[j + ns] = d.second[j] * f;
+    }
+  }
+  return e;
+}
+
 }  // namespace
 
-Status Context::boot_build(int num_slots, int num_cts, int num_stc, int log_msg_ratio, BootPlan *out) {
+Status Context::boot_build(int num_slots, int variant, int num_cts, int num_stc, int log_msg_ratio, BootPlan *out) {
   const int half = P->n / 2;
-  CHD_CHECK(num_slots == half, kErrUnsupported, "Boot: only full-slot bootstrapping (N/2 slots) is supported");
-  CHD_CHECK(num_slots >= 256 && is_pow2(num_slots), kErrInvalidArg, "Boot: power-of-two slots >= 256");
+  CHD_CHECK(num_slots >= 256 && is_pow2(num_slots), kErrInvalidArg, "Number of slots must be a power of 2, >= 256");
+  CHD_CHECK(num_slots <= half, kErrInvalidArg, "num_slots exceeds max_num_slots");
+  CHD_CHECK(variant >= 0 && variant <= 2, kErrInvalidArg,
+            "Boot: variant must be kNormal (0), kImaginaryRemoving (1) or kMergeTwoReal (2)");
+  const bool full = num_slots == half;
   CHD_CHECK(num_cts >= 2 && num_stc >= 2, kErrInvalidArg, "Boot: use at least 2 levels for CtS and StC");
   BootPlan &bp = *out;
   bp = BootPlan{};
   bp.num_slots = num_slots;
+  bp.variant = variant;
   // BootParameter levels, BootParameter.cpp:25-41
   const auto &mod_co = boot_mod_coefficients();
   const int num_da = 3, initial_K = 2;
@@ -95,6 +121,8 @@ Status Context::boot_build(int num_slots, int num_cts, int num_stc, int log_msg_
   for (int i = 0; i < em_levels; i++) em_end = em_end * em_end / P->rescale_prod.at(bp.em_start - i);
   bp.cts_const = static_cast<double>(uint64_t{1} << (log_em_start - P->log_n)) / (q0_prod * actual_K);
   bp.stc_const = (q0_prod * P->scale.at(bp.end_level)) / (em_end * level_zero_scale);
+  // GetStCConst(variant), BootContext.cpp:116-121
+  if (variant != 0) bp.stc_const /= 2;
 
   // ---- special FFT stages (EvalSpecialFFT::PopulatePlainMatrices) ----
   const int ns = num_slots, M = 2 * P->n, stages = log2_ceil(ns);
@@ -151,6 +179,7 @@ Status Context::boot_build(int num_slots, int num_cts, int num_stc, int log_msg_
     left -= st;
     SMat ph = ifft[cumul];
     for (int j = cumul + 1; j < cumul + st; j++) ph = smat_mult(ifft[j], ph);
+    if (i == num_cts - 1 && !full) ph = extend_sparse(ph, ns, cd(0, -1));
     ph = smat_scale(ph, cd(cts_div));
     int eff = static_cast<int>(ph.d.size());
     if (i == num_cts - 1) eff += 1;
@@ -175,6 +204,7 @@ Status Context::boot_build(int num_slots, int num_cts, int num_stc, int log_msg_
     left -= st;
     SMat ph = fft[cumul];
     for (int j = cumul + 1; j < cumul + st; j++) ph = smat_mult(fft[j], ph);
+    if (i == 0 && !full) ph = extend_sparse(ph, ns, cd(0, 1));
     ph = smat_scale(ph, cd(stc_div));
     int eff = static_cast<int>(ph.d.size());
     if (i == 0) eff += 1;
@@ -203,6 +233,12 @@ Status Context::boot_build(int num_slots, int num_cts, int num_stc, int log_msg_
       for (int x : l.gs_idx)
         if (x) r.push_back(x);
     }
+    // AddRequiredRotations, BootContext.cpp:175-184 and
+    // EvalSpecialFFT.cpp:323-325: Trace distances n, 2n, .., N/4 and the
+    // StC fold by n
+    if (!full)
+      for (int d = ns; d < half; d *= 2) bp.extra_rotations.push_back(d);
+    for (int x : bp.extra_rotations) r.push_back(x);
     std::sort(r.begin(), r.end());
     r.erase(std::unique(r.begin(), r.end()), r.end());
     bp.rotations = r;
@@ -230,8 +266,33 @@ Status Context::boot_build(int num_slots, int num_cts, int num_stc, int log_msg_
     o.c = su;
     o.level = -1;
     pg.ops.push_back(o);
-    // 1. ModUpToMax (no sparse-secret encapsulation); full slots: no trace
+    // 1. ModUpToMax (with sparse-secret encapsulation when the parameters
+    // have it), then the Trace over the N/2 slots (BootContext::Trace,
+    // BootContext.cpp:368-400): x += HRot(x, n 2^i) for i < log2(N / 2n)
     int x = op(OpKind::kModUpToMax, o.dst);
+    auto set_slots = [&](int reg, int slots) {
+      ProgOp m;
+      m.kind = OpKind::kSetSlots;
+      m.dst = reg;
+      m.a = reg;
+      m.rot = slots;
+      pg.ops.push_back(m);
+    };
+    auto hrot_add = [&](int a, int rot) {
+      ProgOp h;
+      h.kind = OpKind::kHRotAdd;
+      h.dst = pg.reg();
+      h.a = a;
+      h.b = a;
+      h.rot = rot;
+      pg.ops.push_back(h);
+      return h.dst;
+    };
+    if (!full) {
+      set_slots(x, half);
+      for (int d = ns; d < half; d *= 2) x = hrot_add(x, d % half);
+      set_slots(x, ns);
+    }
     // 2. CoeffToSlot
     for (int i = 0; i < num_cts; i++) {
       ProgOp l;
@@ -242,7 +303,9 @@ Status Context::boot_build(int num_slots, int num_cts, int num_stc, int log_msg_
       pg.ops.push_back(l);
       x = l.dst;
     }
-    // 3. real / imaginary parts, EvalMod on each
+    if (!full) set_slots(x, 2 * ns);
+    // 3. real / imaginary parts, EvalMod on each (full slots), or both
+    // parts side by side in 2n slots: EvalMod(HConj(x) + x)
     int em_reg = -1, em_level = 0;
     double s0 = 0, s1 = 0;
     {
@@ -261,15 +324,21 @@ Status Context::boot_build(int num_slots, int num_cts, int num_stc, int log_msg_
     ss.scale = s0;
     pg.ops.push_back(ss);
     const int conj = op(OpKind::kHConj, x);
-    int re = op(OpKind::kAdd, x, conj);
-    int im = op(OpKind::kSub, conj, x);
-    im = op(OpKind::kMultImag, im);
-    int re_out = -1, im_out = -1;
-    CHD_TRY(compile_evalmod(pg, re, bp.em_start, mod_co, num_da, initial_K, &re_out, &em_level, &s0, &s1));
-    CHD_TRY(compile_evalmod(pg, im, bp.em_start, mod_co, num_da, initial_K, &im_out, &em_level, &s0, &s1));
+    if (full) {
+      int re = op(OpKind::kAdd, x, conj);
+      int im = op(OpKind::kSub, conj, x);
+      im = op(OpKind::kMultImag, im);
+      int re_out = -1, im_out = -1;
+      CHD_TRY(compile_evalmod(pg, re, bp.em_start, mod_co, num_da, initial_K, &re_out, &em_level, &s0, &s1));
+      CHD_TRY(compile_evalmod(pg, im, bp.em_start, mod_co, num_da, initial_K, &im_out, &em_level, &s0, &s1));
+      im_out = op(OpKind::kMultImag, im_out);
+      x = op(OpKind::kAdd, re_out, im_out);
+    } else {
+      // HConjAdd(res, x, x) = HConj(x) + x (Context.cpp:836-860)
+      const int merged = op(OpKind::kAdd, conj, x);
+      CHD_TRY(compile_evalmod(pg, merged, bp.em_start, mod_co, num_da, initial_K, &x, &em_level, &s0, &s1));
+    }
     CHD_CHECK(em_level == bp.stc_start, kErrInvalidLevel, "Boot: EvalMod level bookkeeping mismatch");
-    im_out = op(OpKind::kMultImag, im_out);
-    x = op(OpKind::kAdd, re_out, im_out);
     // 4. SlotToCoeff
     for (int i = 0; i < num_stc; i++) {
       ProgOp l;
@@ -279,6 +348,17 @@ Status Context::boot_build(int num_slots, int num_cts, int num_stc, int log_msg_
       l.rot = num_cts + i;
       pg.ops.push_back(l);
       x = l.dst;
+    }
+    if (!full) {
+      // EvaluateStC, EvalSpecialFFT.cpp:350-362: fold the two halves
+      set_slots(x, 2 * ns);
+      x = hrot_add(x, ns);
+      set_slots(x, ns);
+    }
+    if (variant == 1) {
+      // kImaginaryRemoving: res = HConj(res) + res (BootContext.cpp:354-357)
+      const int c = op(OpKind::kHConj, x);
+      x = op(OpKind::kAdd, c, x);
     }
     bp.final_scale = P->scale.at(bp.end_level);
     ProgOp fs;
@@ -301,6 +381,12 @@ Status Context::boot_run(const BootPlan &bp, DeviceCt &res, const DeviceCt &in, 
   const int in_level = P->np_to_level(in.np);
   CHD_CHECK(in_level >= 0 && in_level <= P->spec.default_encryption_level, kErrInvalidLevel,
             "Boot: input level must be in [0, default encryption level]");
+  // GetBootEnabledNumSlots (BootContext.cpp:124-147): the input's slots must
+  // fit the prepared slot count (a smaller power of two is periodic in it)
+  const int in_slots = in.num_slots > 0 ? in.num_slots : P->n / 2;
+  CHD_CHECK(in_slots <= bp.num_slots, kErrInvalidArg,
+            "Boot: not prepared for " + std::to_string(in_slots) + " slots (prepared: " +
+                std::to_string(bp.num_slots) + ")");
   CHD_CHECK(keys.mult && keys.conj && keys.rot, kErrKey, "Boot: multiplication, conjugation and rotation keys needed");
   std::vector<DeviceCt> local;
   std::vector<DeviceCt> &regs = regs_io ? *regs_io : local;

@@ -739,10 +739,16 @@ int chd_program_run(chd_context *ctx, const chd_program *p, chd_ciphertext *res,
 
 int chd_boot_create(chd_context *ctx, int num_slots, int num_cts_levels, int num_stc_levels, int log_message_ratio,
                     chd_boot **out) {
+  return chd_boot_create_variant(ctx, num_slots, CHD_BOOT_NORMAL, num_cts_levels, num_stc_levels, log_message_ratio,
+                                 out);
+}
+
+int chd_boot_create_variant(chd_context *ctx, int num_slots, int variant, int num_cts_levels, int num_stc_levels,
+                            int log_message_ratio, chd_boot **out) {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(out);
   auto *b = new chd_boot();
-  int rc = ctx->c->boot_build(num_slots, num_cts_levels, num_stc_levels, log_message_ratio, &b->plan);
+  int rc = ctx->c->boot_build(num_slots, variant, num_cts_levels, num_stc_levels, log_message_ratio, &b->plan);
   if (rc != CHD_OK) {
     delete b;
     return rc;
@@ -761,6 +767,7 @@ int chd_boot_rotations(const chd_boot *b, int min_ks, int *out, int cap, int *co
     int rc = plan_rotations(l, min_ks != 0, &r);
     if (rc != CHD_OK) return rc;
   }
+  for (int x : b->plan.extra_rotations) r.push_back(x);
   std::sort(r.begin(), r.end());
   r.erase(std::unique(r.begin(), r.end()), r.end());
   *count = static_cast<int>(r.size());

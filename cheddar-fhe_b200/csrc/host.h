@@ -254,6 +254,7 @@ enum class OpKind : int {
   kModUpToMax = 13, // dst = ModUpToMax(a)
   kHRotAdd = 14,    // dst = HRot(a, r) + b
   kLinTrans = 15,   // dst = lin_trans[lt](a)
+  kSetSlots = 16,   // metadata only: dst.num_slots = rot
 };
 struct ProgOp {
   OpKind kind = OpKind::kCopy;
@@ -280,11 +281,13 @@ struct Program {
 // slot count): the CtS then StC linear transforms and the Boot program.
 struct BootPlan {
   int num_slots = 0, max_level = 0, cts_start = 0, em_start = 0, stc_start = 0, end_level = 0, log_scaleup = 0;
+  int variant = 0;  // BootVariant: 0 kNormal, 1 kImaginaryRemoving, 2 kMergeTwoReal
   double cts_const = 0, stc_const = 0, em_start_scale = 0, em_end_scale = 0, final_scale = 0;
   std::vector<LTPlan> lts;
   std::vector<const LTPlan *> lt_ptrs;
   Program prog;
   std::vector<int> rotations;  // rotation keys the transforms use
+  std::vector<int> extra_rotations;  // sparse slots: Trace and the last StC fold
 };
 
 // EvalMod cosine polynomial of the reference's BootParameter
@@ -446,7 +449,7 @@ class Context {
   Status program_regs(const Program &prog, std::vector<DeviceCt> &regs);
   // BootContext (bootplan.cu): prepare full-slot bootstrapping with
   // num_cts / num_stc levels for CoeffToSlot / SlotToCoeff
-  Status boot_build(int num_slots, int num_cts, int num_stc, int log_msg_ratio, BootPlan *out);
+  Status boot_build(int num_slots, int variant, int num_cts, int num_stc, int log_msg_ratio, BootPlan *out);
   // BootContext::Boot: in at level 0 -> res at the end level.  regs_io,
   // when given, keeps the program registers allocated across calls.
   Status boot_run(const BootPlan &bp, DeviceCt &res, const DeviceCt &in, const ProgKeys &keys,

@@ -261,6 +261,9 @@ Status Context::run_program(const Program &prog, std::vector<DeviceCt> &regs, co
       case OpKind::kSetScale:
         regs.at(op.dst).scale = op.scale;
         continue;
+      case OpKind::kSetSlots:
+        regs.at(op.dst).num_slots = op.rot;
+        continue;
       case OpKind::kHConj:
         CHD_CHECK(conj_key, kErrKey, "program: conjugation key missing");
         CHD_TRY(hconj(t, regs.at(op.a), *conj_key));

@@ -272,6 +272,18 @@ int chd_program_run(chd_context *ctx, const chd_program *p, chd_ciphertext *res,
 typedef struct chd_boot chd_boot;
 int chd_boot_create(chd_context *ctx, int num_slots, int num_cts_levels, int num_stc_levels, int log_message_ratio,
                     chd_boot **out);
+/* PrepareEvalSpecialFFT(num_slots, variant) (BootContext.h:16-20, 96-97):
+ * num_slots a power of two from 256 to N/2 (below N/2: Trace after
+ * ModUpToMax, extended 2n x 2n CtS / StC phases, one EvalMod on both parts,
+ * a final HRotAdd by n); variant CHD_BOOT_NORMAL, CHD_BOOT_IMAGINARY_REMOVING
+ * (StC constant / 2 and res = HConj(res) + res at the end: a real result) or
+ * CHD_BOOT_MERGE_TWO_REAL (StC constant / 2; the caller combines two real
+ * inputs before and after).  chd_boot_create is variant CHD_BOOT_NORMAL. */
+#define CHD_BOOT_NORMAL 0
+#define CHD_BOOT_IMAGINARY_REMOVING 1
+#define CHD_BOOT_MERGE_TWO_REAL 2
+int chd_boot_create_variant(chd_context *ctx, int num_slots, int variant, int num_cts_levels, int num_stc_levels,
+                            int log_message_ratio, chd_boot **out);
 void chd_boot_destroy(chd_boot *b);
 int chd_boot_rotations(const chd_boot *b, int min_ks, int *out, int cap, int *count);
 int chd_boot_levels(const chd_boot *b, int *levels, double *scales);

@@ -238,10 +238,13 @@ class EvkMap {
 // PrepareEvalMod + PrepareEvalSpecialFFT at construction, then Boot.
 class BootContext {
  public:
+  // PrepareEvalSpecialFFT(num_slots, variant): variant CHD_BOOT_NORMAL,
+  // CHD_BOOT_IMAGINARY_REMOVING or CHD_BOOT_MERGE_TWO_REAL
   BootContext(Context &ctx, int num_slots, int num_cts_levels = 4, int num_stc_levels = 3,
-              int log_message_ratio = 5)
+              int log_message_ratio = 5, int variant = CHD_BOOT_NORMAL)
       : ctx_(ctx) {
-    check(chd_boot_create(ctx.raw(), num_slots, num_cts_levels, num_stc_levels, log_message_ratio, &b_));
+    check(chd_boot_create_variant(ctx.raw(), num_slots, variant, num_cts_levels, num_stc_levels, log_message_ratio,
+                                  &b_));
   }
   ~BootContext() { chd_boot_destroy(b_); }
   BootContext(const BootContext &) = delete;

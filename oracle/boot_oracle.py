@@ -214,7 +214,7 @@ def lt_evaluate(o, level, ct, ct_scale, pts, pt_scale, keys, min_ks=False):
 # ---------------------------------------------------------------------------
 
 K_CONST_MULT, K_TENSOR, K_CACCUM, K_ADD_CONST, K_ADD, K_RELIN_RESCALE, K_RESCALE, K_LEVEL_DOWN, \
-    K_COPY, K_SET_SCALE, K_SUB, K_HCONJ, K_MULT_IMAG, K_MODUP_TO_MAX, K_HROT_ADD, K_LIN_TRANS = range(16)
+    K_COPY, K_SET_SCALE, K_SUB, K_HCONJ, K_MULT_IMAG, K_MODUP_TO_MAX, K_HROT_ADD, K_LIN_TRANS, K_SET_SLOTS = range(17)
 
 
 class Ct:
@@ -333,6 +333,8 @@ def run_program(o, prog, inp, mult_key=None, conj_key=None, rot_keys=None, lts=N
             regs[d] = Ct(x.level, [p.copy() for p in x.parts], x.scale)
         elif k == K_SET_SCALE:
             regs[d].scale = op["sc"]
+        elif k == K_SET_SLOTS:
+            pass  # slot counts only normalise rotation distances, which the program states
         elif k == K_HCONJ:
             x = regs[a]
             rb, ra = o.hconj(x.level, x.parts, conj_key)
@@ -390,7 +392,7 @@ def plain_program(prog, x):
             regs[d] = regs[a] - regs[b]
         elif k in (K_RELIN_RESCALE, K_RESCALE, K_LEVEL_DOWN, K_COPY):
             regs[d] = regs[a]
-        elif k == K_SET_SCALE:
+        elif k in (K_SET_SCALE, K_SET_SLOTS):
             pass
         else:
             raise ValueError(f"plain evaluation does not cover op {k}")

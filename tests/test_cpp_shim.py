@@ -19,6 +19,7 @@ void unused_paths(cheddar_b200::Context &ctx, const cheddar_b200::EvaluationKey 
   m.SetConjugationKey(k);
   m.AddRotationKey(1, k);
   cheddar_b200::BootContext bc(ctx, 1 << 15);
+  cheddar_b200::BootContext bc_sparse(ctx, 1 << 12, 4, 3, 5, CHD_BOOT_IMAGINARY_REMOVING);
   std::vector<int> r = bc.RequiredRotations();
   cheddar_b200::Ciphertext a(ctx), b(ctx);
   bc.ModUpToMax(b, a, m);
