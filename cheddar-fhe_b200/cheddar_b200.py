@@ -127,6 +127,7 @@ def lib():
         "chd_boot_mod_coefficients": (i, [vp, i]),
         "chd_boot_create": (i, [vp, i, i, i, i, pp]),
         "chd_boot_create_variant": (i, [vp, i, i, i, i, i, pp]),
+        "chd_boot_run_batch": (i, [vp, vp, i, pp, pp, vp, i]),
         "chd_boot_destroy": (None, [vp]),
         "chd_boot_rotations": (i, [vp, i, vp, i, C.POINTER(i)]),
         "chd_boot_levels": (i, [vp, vp, vp]),
@@ -678,6 +679,17 @@ class BootContext:
         res = res if res is not None else Ciphertext(self.ctx)
         _check(lib().chd_boot_run(self.ctx.ptr, self.ptr, res.ptr, ct.ptr, keys.ptr, int(min_ks)))
         return res
+
+    def BootBatch(self, cts, keys, res_list=None, min_ks=False):
+        """Boot of every ciphertext in `cts` in one call, key switches and
+        linear transforms batched across them; equals Boot on each."""
+        res_list = res_list if res_list is not None else [Ciphertext(self.ctx) for _ in cts]
+        n = len(cts)
+        ins = (C.c_void_p * n)(*[c.ptr.value for c in cts])
+        outs = (C.c_void_p * n)(*[r.ptr.value for r in res_list])
+        _check(lib().chd_boot_run_batch(self.ctx.ptr, self.ptr, n, C.cast(outs, C.POINTER(C.c_void_p)),
+                                        C.cast(ins, C.POINTER(C.c_void_p)), keys.ptr, int(min_ks)))
+        return res_list
 
 
 class Ciphertext:

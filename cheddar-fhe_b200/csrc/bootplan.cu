@@ -374,64 +374,86 @@ Status Context::boot_build(int num_slots, int variant, int num_cts, int num_stc,
 
 Status Context::boot_run(const BootPlan &bp, DeviceCt &res, const DeviceCt &in, const ProgKeys &keys,
                          std::vector<DeviceCt> *regs_io) {
-  // BootContext::Boot (BootContext.cpp:296-370); an input above level 0 is
-  // first brought down with Context::LevelDown (Context.cpp:917-929): per
-  // level, times the constant 1 at that level's scale, then Rescale
-  CHD_CHECK(in.np.aux == 0 && !in.has_rx, kErrShape, "Boot: input must be relinearised without aux primes");
-  const int in_level = P->np_to_level(in.np);
-  CHD_CHECK(in_level >= 0 && in_level <= P->spec.default_encryption_level, kErrInvalidLevel,
-            "Boot: input level must be in [0, default encryption level]");
-  // GetBootEnabledNumSlots (BootContext.cpp:124-147): the input's slots must
-  // fit the prepared slot count (a smaller power of two is periodic in it)
-  const int in_slots = in.num_slots > 0 ? in.num_slots : P->n / 2;
-  CHD_CHECK(in_slots <= bp.num_slots, kErrInvalidArg,
-            "Boot: not prepared for " + std::to_string(in_slots) + " slots (prepared: " +
-                std::to_string(bp.num_slots) + ")");
-  CHD_CHECK(keys.mult && keys.conj && keys.rot, kErrKey, "Boot: multiplication, conjugation and rotation keys needed");
   std::vector<DeviceCt> local;
-  std::vector<DeviceCt> &regs = regs_io ? *regs_io : local;
-  CHD_TRY(program_regs(bp.prog, regs));
-  DeviceCt &r0 = regs[bp.prog.input];
-  CHD_TRY(r0.reserve(in.np, false, P->n));
-  const size_t bytes = static_cast<size_t>(in.np.total()) * P->n * 4;
-  cudaMemcpyAsync(r0.bx, in.bx, bytes, cudaMemcpyDeviceToDevice, stream);
-  cudaMemcpyAsync(r0.ax, in.ax, bytes, cudaMemcpyDeviceToDevice, stream);
-  r0.scale = in.scale;
-  r0.num_slots = in.num_slots;
-  if (in_level > 0) {
-    Program ld;
-    ld.input = ld.reg();
-    int x = ld.input;
-    for (int i = in_level; i > 0; i--) {
-      ProgOp m;
-      m.kind = OpKind::kConstMult;
-      m.dst = ld.reg();
-      m.a = x;
-      m.c = ld.add_const(i, P->scale.at(i), 1.0);
-      m.level = i;
-      ld.ops.push_back(m);
-      ProgOp r;
-      r.kind = OpKind::kRescale;
-      r.dst = ld.reg();
-      r.a = m.dst;
-      ld.ops.push_back(r);
-      x = r.dst;
-    }
-    ld.output = x;
-    std::vector<DeviceCt> lregs;
-    CHD_TRY(program_regs(ld, lregs));
-    swap_regs(lregs[ld.input], r0);
-    CHD_TRY(run_program(ld, lregs, keys, nullptr));
-    swap_regs(lregs[ld.output], r0);
+  std::vector<DeviceCt> *regs = regs_io ? regs_io : &local;
+  DeviceCt *r = &res;
+  const DeviceCt *i = &in;
+  return boot_run_batch(bp, 1, &r, &i, keys, &regs);
+}
+
+Status Context::boot_run_batch(const BootPlan &bp, int count, DeviceCt *const *res, const DeviceCt *const *in,
+                               const ProgKeys &keys, std::vector<DeviceCt> *const *regs) {
+  // BootContext::Boot (BootContext.cpp:296-370) on `count` ciphertexts with
+  // the program's key switches, rescales and linear transforms batched
+  // across them; an input above level 0 is first brought down with
+  // Context::LevelDown (Context.cpp:917-929): per level, times the constant 1
+  // at that level's scale, then Rescale
+  CHD_CHECK(count >= 1, kErrInvalidArg, "Boot: empty batch");
+  CHD_CHECK(keys.mult && keys.conj && keys.rot, kErrKey, "Boot: multiplication, conjugation and rotation keys needed");
+  for (int c = 0; c < count; c++) {
+    CHD_CHECK(in[c]->np.aux == 0 && !in[c]->has_rx, kErrShape, "Boot: input must be relinearised without aux primes");
+    const int in_level = P->np_to_level(in[c]->np);
+    CHD_CHECK(in_level >= 0 && in_level <= P->spec.default_encryption_level, kErrInvalidLevel,
+              "Boot: input level must be in [0, default encryption level]");
+    // GetBootEnabledNumSlots (BootContext.cpp:124-147): the input's slots
+    // must fit the prepared slot count (a smaller power of two is periodic
+    // in it)
+    const int in_slots = in[c]->num_slots > 0 ? in[c]->num_slots : P->n / 2;
+    CHD_CHECK(in_slots <= bp.num_slots, kErrInvalidArg,
+              "Boot: not prepared for " + std::to_string(in_slots) + " slots (prepared: " +
+                  std::to_string(bp.num_slots) + ")");
+    for (int d = 0; d < c; d++) CHD_CHECK(regs[c] != regs[d], kErrInvalidArg, "Boot: batch members share registers");
   }
-  CHD_TRY(run_program(bp.prog, regs, keys, &bp.lt_ptrs));
-  const DeviceCt &o = regs[bp.prog.output];
-  CHD_TRY(res.reserve(o.np, false, P->n));
-  const size_t ob = static_cast<size_t>(o.np.total()) * P->n * 4;
-  cudaMemcpyAsync(res.bx, o.bx, ob, cudaMemcpyDeviceToDevice, stream);
-  cudaMemcpyAsync(res.ax, o.ax, ob, cudaMemcpyDeviceToDevice, stream);
-  res.scale = bp.final_scale;
-  res.num_slots = in.num_slots;
+  for (int c = 0; c < count; c++) {
+    std::vector<DeviceCt> &rg = *regs[c];
+    CHD_TRY(program_regs(bp.prog, rg));
+    DeviceCt &r0 = rg[bp.prog.input];
+    const DeviceCt &x = *in[c];
+    const int in_level = P->np_to_level(x.np);
+    CHD_TRY(r0.reserve(x.np, false, P->n));
+    const size_t bytes = static_cast<size_t>(x.np.total()) * P->n * 4;
+    cudaMemcpyAsync(r0.bx, x.bx, bytes, cudaMemcpyDeviceToDevice, stream);
+    cudaMemcpyAsync(r0.ax, x.ax, bytes, cudaMemcpyDeviceToDevice, stream);
+    r0.scale = x.scale;
+    r0.num_slots = x.num_slots;
+    if (in_level > 0) {
+      Program ld;
+      ld.input = ld.reg();
+      int y = ld.input;
+      for (int i = in_level; i > 0; i--) {
+        ProgOp m;
+        m.kind = OpKind::kConstMult;
+        m.dst = ld.reg();
+        m.a = y;
+        m.c = ld.add_const(i, P->scale.at(i), 1.0);
+        m.level = i;
+        ld.ops.push_back(m);
+        ProgOp r;
+        r.kind = OpKind::kRescale;
+        r.dst = ld.reg();
+        r.a = m.dst;
+        ld.ops.push_back(r);
+        y = r.dst;
+      }
+      ld.output = y;
+      std::vector<DeviceCt> lregs;
+      CHD_TRY(program_regs(ld, lregs));
+      swap_regs(lregs[ld.input], r0);
+      CHD_TRY(run_program(ld, lregs, keys, nullptr));
+      swap_regs(lregs[ld.output], r0);
+    }
+  }
+  CHD_TRY(run_program_batch(bp.prog, count, regs, keys, &bp.lt_ptrs));
+  for (int c = 0; c < count; c++) {
+    const DeviceCt &o = (*regs[c])[bp.prog.output];
+    const int in_slots = in[c]->num_slots;
+    CHD_TRY(res[c]->reserve(o.np, false, P->n));
+    const size_t ob = static_cast<size_t>(o.np.total()) * P->n * 4;
+    cudaMemcpyAsync(res[c]->bx, o.bx, ob, cudaMemcpyDeviceToDevice, stream);
+    cudaMemcpyAsync(res[c]->ax, o.ax, ob, cudaMemcpyDeviceToDevice, stream);
+    res[c]->scale = bp.final_scale;
+    res[c]->num_slots = in_slots;
+  }
   return check_cuda("boot");
 }
 

@@ -37,6 +37,7 @@ struct chd_lintrans {
 struct chd_boot {
   BootPlan plan;
   std::vector<DeviceCt> regs;  // program registers kept across calls
+  std::vector<std::vector<DeviceCt>> batch_regs;  // per batch member, chd_boot_run_batch
 };
 struct chd_graph {
   cudaGraph_t graph = nullptr;
@@ -856,6 +857,53 @@ int chd_boot_run(chd_context *ctx, chd_boot *b, chd_ciphertext *res, const chd_c
     return CHD_OK;
   }
   return ctx->c->boot_run(b->plan, res->ct, in->ct, pk, &b->regs);
+}
+
+int chd_boot_run_batch(chd_context *ctx, chd_boot *b, int count, chd_ciphertext *const *res,
+                       const chd_ciphertext *const *in, const chd_evk_map *keys, int min_ks) {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(b);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(in);
+  CHD_NOTNULL(keys);
+  if (count < 1) return fail(CHD_ERR_INVALID_ARG, "chd_boot_run_batch: count must be positive");
+  if (!keys->mult || !keys->conj) return fail(CHD_ERR_KEY, "chd_boot_run: multiplication and conjugation keys required");
+  for (int c = 0; c < count; c++) {
+    if (!res[c] || !in[c]) return fail(CHD_ERR_INVALID_ARG, "chd_boot_run_batch: null ciphertext");
+    for (int d = 0; d < count; d++)
+      if (d != c && res[c] == res[d]) return fail(CHD_ERR_INVALID_ARG, "chd_boot_run_batch: results must differ");
+  }
+  ProgKeys pk = keys->keys();
+  pk.min_ks = min_ks != 0;
+  if (static_cast<int>(b->batch_regs.size()) < count) b->batch_regs.resize(count);
+  std::vector<std::vector<DeviceCt> *> regs(count);
+  // results written into fresh ciphertexts first when one aliases an input
+  std::vector<DeviceCt> tmp(count);
+  std::vector<DeviceCt *> out(count);
+  std::vector<const DeviceCt *> src(count);
+  for (int c = 0; c < count; c++) {
+    regs[c] = &b->batch_regs[c];
+    src[c] = &in[c]->ct;
+    bool alias = false;
+    for (int d = 0; d < count; d++) alias = alias || res[c] == in[d];
+    out[c] = alias ? &tmp[c] : &res[c]->ct;
+  }
+  int rc = ctx->c->boot_run_batch(b->plan, count, out.data(), src.data(), pk, regs.data());
+  if (rc != CHD_OK) return rc;
+  for (int c = 0; c < count; c++) {
+    if (out[c] != &tmp[c]) continue;
+    DeviceCt &r = res[c]->ct;
+    std::swap(r.bx, tmp[c].bx);
+    std::swap(r.ax, tmp[c].ax);
+    std::swap(r.rx, tmp[c].rx);
+    std::swap(r.cap_words, tmp[c].cap_words);
+    std::swap(r.owned, tmp[c].owned);
+    r.np = tmp[c].np;
+    r.has_rx = false;
+    r.scale = tmp[c].scale;
+    r.num_slots = tmp[c].num_slots;
+  }
+  return CHD_OK;
 }
 
 int chd_graph_begin(chd_context *ctx) {

@@ -428,6 +428,9 @@ class Context {
                   int additional_pt_rot, bool suppress_swap, LTPlan *out);
   // HoistHandler::Evaluate (Hoist.cu:554-975): res at pt_level - 1
   Status lt_evaluate(DeviceCt &res, const DeviceCt &in, const LTPlan &pl, const RotKeys &keys);
+  // the same transform on `count` ciphertexts at one level, launches batched
+  Status lt_evaluate_batch(int count, DeviceCt *const *res, const DeviceCt *const *in, const LTPlan &pl,
+                           const RotKeys &keys);
   // the min-KS evaluation (Hoist.cu:490-552): two rotation keys per transform
   Status lt_evaluate_min_ks(DeviceCt &res, const DeviceCt &in, const LTPlan &pl, const RotKeys &keys);
 
@@ -444,6 +447,10 @@ class Context {
   // Runs a program (program.cu): regs[input] holds the input
   Status run_program(const Program &prog, std::vector<DeviceCt> &regs, const ProgKeys &keys,
                      const std::vector<const LTPlan *> *lts);
+  // the program on `count` ciphertexts (registers R[c]); key switches,
+  // rescales and linear transforms batched across them
+  Status run_program_batch(const Program &prog, int count, std::vector<DeviceCt> *const *R, const ProgKeys &keys,
+                           const std::vector<const LTPlan *> *lts);
   bool mult_unsafe_compatible(int l1, int l2) const;
   // sizes the registers of a program (plus two spares) at top-level capacity
   Status program_regs(const Program &prog, std::vector<DeviceCt> &regs);
@@ -454,6 +461,10 @@ class Context {
   // when given, keeps the program registers allocated across calls.
   Status boot_run(const BootPlan &bp, DeviceCt &res, const DeviceCt &in, const ProgKeys &keys,
                   std::vector<DeviceCt> *regs_io);
+  // Boot of `count` ciphertexts (each with its own program registers),
+  // key switches, rescales and linear transforms batched across them
+  Status boot_run_batch(const BootPlan &bp, int count, DeviceCt *const *res, const DeviceCt *const *in,
+                        const ProgKeys &keys, std::vector<DeviceCt> *const *regs);
 
   // ---- optional device timing of the fused key-switch stages ----
   // Events recorded on the context stream around each stage's launches.

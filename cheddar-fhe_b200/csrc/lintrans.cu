@@ -294,110 +294,134 @@ Status Context::lt_evaluate_min_ks(DeviceCt &res, const DeviceCt &in, const LTPl
   return check_cuda("linear transform (min-KS)");
 }
 
-Status Context::lt_evaluate(DeviceCt &res, const DeviceCt &in, const LTPlan &pl, const RotKeys &keys) {
-  // HoistHandler::Evaluate, Hoist.cu:554-975 (non-min-KS, fused kernels)
-  const int level = pl.pt_level;
-  const int n = P->n;
-  CHD_CHECK(!in.has_rx && in.np.aux == 0, kErrShape, "Hoist: input should be relinearized and mod-down");
-  CHD_CHECK(in.np == P->level_np(level), kErrShape, "Hoist: input level mismatch");
-  const NP qp = P->level_np(level, P->alpha);
-  const int nq = qp.q(), tot = qp.total();
-  const LevelMS &m = lms(level);
-  std::vector<int> g(tot);
-  P->gidx(qp, g.data());
-  const int prime_offset = P->max_ter - qp.ter;
-  const size_t tw_ = static_cast<size_t>(tot) * n;
-  auto key_of = [&](int r) -> const DeviceEvk * {
-    auto it = keys.find(r);
-    return it == keys.end() ? nullptr : it->second;
-  };
-  ArenaScope scope(arena);
-  auto alloc = [&](size_t words) { return static_cast<uint32_t *>(arena.alloc(words * 4)); };
+namespace {
+
+// Row-level building blocks of the hoisted evaluation at one level (Q u P
+// basis of that level), shared by the single and the batched paths.
+struct HoistOps {
+  Context &C;
+  const int level, n;
+  const NP qp;
+  const int nq, tot, prime_offset;
+  const LevelMS &m;
+  std::vector<int> g;
+  const size_t tw;  // words of one Q u P polynomial
+
+  HoistOps(Context &c, int lvl)
+      : C(c),
+        level(lvl),
+        n(c.P->n),
+        qp(c.P->level_np(lvl, c.P->alpha)),
+        nq(qp.q()),
+        tot(qp.total()),
+        prime_offset(c.P->max_ter - qp.ter),
+        m(c.lms(lvl)),
+        g(tot),
+        tw(static_cast<size_t>(tot) * c.P->n) {
+    c.P->gidx(qp, g.data());
+  }
   // P * x on q rows, zero on aux rows (PseudoModUp + ZeroExtend)
-  auto pseudo_modup = [&](const uint32_t *src, uint32_t *dst) {
+  void pseudo_modup(const uint32_t *src, uint32_t *dst) const {
     ConstAccumDesc d{};
     d.terms = 1;
     d.src[0][0] = src;
     d.src_row0[0] = 0;
     d.dst[0] = dst;
     for (int r = 0; r < nq; r++) {
-      d.q[r] = P->primes[g[r]];
-      d.qinv[r] = P->qinv[g[r]];
-      d.c[0][r] = p_prod[prime_offset + r];
+      d.q[r] = C.P->primes[g[r]];
+      d.qinv[r] = C.P->qinv[g[r]];
+      d.c[0][r] = C.p_prod[prime_offset + r];
     }
     d.rows = nq;
     d.parts = 1;
     d.n = n;
-    launch_const_accum(d, stream);
-    cudaMemsetAsync(dst + static_cast<size_t>(nq) * n, 0, static_cast<size_t>(tot - nq) * n * 4, stream);
-  };
+    launch_const_accum(d, C.stream);
+    cudaMemsetAsync(dst + static_cast<size_t>(nq) * n, 0, static_cast<size_t>(tot - nq) * n * 4, C.stream);
+  }
   // sum_i ModUp(x)_i (.) key_i over Q u P (MultKeyNoModDown, Context.cpp:610-648)
-  auto key_mult = [&](uint32_t *const *mu, const DeviceEvk &k, uint32_t *ob, uint32_t *oa) -> Status {
-    CHD_CHECK(k.np.aux == P->alpha && k.np.q() == P->L, kErrKey, "Hoist: key basis mismatch");
-    KeyMacDesc d{};
-    const size_t kstride = static_cast<size_t>(P->L + P->alpha) * n;
-    int nb = 0;
-    for (int i = 0; i < m.beta; i++) {
-      if (m.dig_e[i] <= 0) continue;
-      CHD_CHECK(i < k.beta, kErrKey, "Hoist: key has too few digits");
-      d.kb[nb] = k.bx + i * kstride;
-      d.ka[nb] = k.ax + i * kstride;
-      d.ct[0].mu[nb] = mu[i];
-      nb++;
+  // for `count` ciphertexts sharing the key: mu[c][digit]
+  Status key_mult(int count, uint32_t *const *const *mu, const DeviceEvk &k, uint32_t *const *ob,
+                  uint32_t *const *oa) const {
+    if (!(k.np.aux == C.P->alpha && k.np.q() == C.P->L)) {
+      set_error("Hoist: key basis mismatch");
+      return kErrKey;
     }
-    d.beta = nb;
-    d.rows = tot;
-    d.nq = nq;
-    d.count = 1;
-    for (int r = 0; r < tot; r++) {
-      d.q[r] = P->primes[g[r]];
-      d.qinv[r] = P->qinv[g[r]];
-      d.p_prod[r] = 0;
-      d.key_row[r] = static_cast<int16_t>(r < nq ? prime_offset + r : P->L + (r - nq));
+    const size_t kstride = static_cast<size_t>(C.P->L + C.P->alpha) * n;
+    for (int c0 = 0; c0 < count; c0 += kMaxKeyMacCts) {
+      KeyMacDesc d{};
+      int nb = 0;
+      for (int i = 0; i < m.beta; i++) {
+        if (m.dig_e[i] <= 0) continue;
+        if (i >= k.beta) {
+          set_error("Hoist: key has too few digits");
+          return kErrKey;
+        }
+        d.kb[nb] = k.bx + i * kstride;
+        d.ka[nb] = k.ax + i * kstride;
+        nb++;
+      }
+      d.beta = nb;
+      d.rows = tot;
+      d.nq = nq;
+      d.count = std::min(kMaxKeyMacCts, count - c0);
+      for (int r = 0; r < tot; r++) {
+        d.q[r] = C.P->primes[g[r]];
+        d.qinv[r] = C.P->qinv[g[r]];
+        d.p_prod[r] = 0;
+        d.key_row[r] = static_cast<int16_t>(r < nq ? prime_offset + r : C.P->L + (r - nq));
+      }
+      for (int c = 0; c < d.count; c++) {
+        int b = 0;
+        for (int i = 0; i < m.beta; i++)
+          if (m.dig_e[i] > 0) d.ct[c].mu[b++] = mu[c0 + c][i];
+        d.ct[c].d0 = d.ct[c].d1 = nullptr;
+        d.ct[c].acc_b = ob[c0 + c];
+        d.ct[c].acc_a = oa[c0 + c];
+      }
+      launch_key_mac(d, C.P->log_n, C.stream);
     }
-    d.ct[0].d0 = d.ct[0].d1 = nullptr;
-    d.ct[0].acc_b = ob;
-    d.ct[0].acc_a = oa;
-    launch_key_mac(d, P->log_n, stream);
     return kOk;
-  };
+  }
   // dst (+)= Permute_g(src) over the Q u P rows of one part
-  auto permute_rows = [&](const uint32_t *src, uint32_t *dst, const uint32_t *add, int amount) {
+  void permute_rows(const uint32_t *src, uint32_t *dst, const uint32_t *add, int amount) const {
     PermuteBatch pb{};
-    pb.galois = P->galois_of(amount);
+    pb.galois = C.P->galois_of(amount);
     for (int r = 0; r < tot; r++) {
       if (pb.count == 64) {
-        launch_permute(pb, P->log_n, stream);
+        launch_permute(pb, C.P->log_n, C.stream);
         pb.count = 0;
       }
       PermuteRow &pr = pb.rows[pb.count++];
       pr.src = src + static_cast<size_t>(r) * n;
       pr.dst = dst + static_cast<size_t>(r) * n;
       pr.add = add ? add + static_cast<size_t>(r) * n : nullptr;
-      pr.q = P->primes[g[r]];
+      pr.q = C.P->primes[g[r]];
     }
-    launch_permute(pb, P->log_n, stream);
-  };
-  auto add_rows = [&](const uint32_t *a, const uint32_t *b, uint32_t *dst, int rows) {
+    launch_permute(pb, C.P->log_n, C.stream);
+  }
+  void add_rows(const uint32_t *a, const uint32_t *b, uint32_t *dst, int rows) const {
     ElemBatch eb{};
     for (int r = 0; r < rows; r++) {
       if (eb.count == kMaxElemRows) {
-        launch_elementwise(ElemOp::kAdd, eb, P->log_n, stream);
+        launch_elementwise(ElemOp::kAdd, eb, C.P->log_n, C.stream);
         eb.count = 0;
       }
       ElemRow &e = eb.rows[eb.count++];
       e.a = a + static_cast<size_t>(r) * n;
       e.b = b + static_cast<size_t>(r) * n;
       e.dst = dst + static_cast<size_t>(r) * n;
-      e.q = P->primes[g[r]];
-      e.qinv = P->qinv[g[r]];
+      e.q = C.P->primes[g[r]];
+      e.qinv = C.P->qinv[g[r]];
     }
-    launch_elementwise(ElemOp::kAdd, eb, P->log_n, stream);
-  };
-  auto pt_accum = [&](const std::vector<std::pair<const uint32_t *, const uint32_t *>> &ins,
-                      const std::vector<std::vector<std::pair<int, const uint32_t *>>> &terms,
-                      const std::vector<std::pair<uint32_t *, uint32_t *>> &outs) -> Status {
-    CHD_CHECK(static_cast<int>(ins.size()) <= kMaxPtAccumIn, kErrUnsupported, "Hoist: too many baby steps");
+    launch_elementwise(ElemOp::kAdd, eb, C.P->log_n, C.stream);
+  }
+  Status pt_accum(const std::vector<std::pair<const uint32_t *, const uint32_t *>> &ins,
+                  const std::vector<std::vector<std::pair<int, const uint32_t *>>> &terms,
+                  const std::vector<std::pair<uint32_t *, uint32_t *>> &outs) const {
+    if (static_cast<int>(ins.size()) > kMaxPtAccumIn) {
+      set_error("Hoist: too many baby steps");
+      return kErrUnsupported;
+    }
     for (size_t o0 = 0; o0 < outs.size(); o0 += kMaxPtAccumOuts) {
       PtAccumDesc d{};
       for (size_t i = 0; i < ins.size(); i++) {
@@ -405,15 +429,18 @@ Status Context::lt_evaluate(DeviceCt &res, const DeviceCt &in, const LTPlan &pl,
         d.in_a[i] = ins[i].second;
       }
       for (int r = 0; r < tot; r++) {
-        d.q[r] = P->primes[g[r]];
-        d.qinv[r] = P->qinv[g[r]];
+        d.q[r] = C.P->primes[g[r]];
+        d.qinv[r] = C.P->qinv[g[r]];
       }
       d.rows = tot;
       d.n = n;
       d.outs = static_cast<int>(std::min<size_t>(kMaxPtAccumOuts, outs.size() - o0));
       for (int o = 0; o < d.outs; o++) {
         const auto &t = terms[o0 + o];
-        CHD_CHECK(static_cast<int>(t.size()) <= kMaxPtAccumTerms, kErrUnsupported, "Hoist: too many terms");
+        if (static_cast<int>(t.size()) > kMaxPtAccumTerms) {
+          set_error("Hoist: too many terms");
+          return kErrUnsupported;
+        }
         PtAccumOut &po = d.out[o];
         po.b = outs[o0 + o].first;
         po.a = outs[o0 + o].second;
@@ -423,127 +450,75 @@ Status Context::lt_evaluate(DeviceCt &res, const DeviceCt &in, const LTPlan &pl,
           po.pt[k] = t[k].second;
         }
       }
-      launch_pt_accum(d, stream);
+      launch_pt_accum(d, C.stream);
     }
     return kOk;
-  };
+  }
+};
 
-  std::vector<uint32_t *> mu(m.beta);
-  for (int i = 0; i < m.beta; i++) {
+}  // namespace
+
+Status Context::lt_evaluate(DeviceCt &res, const DeviceCt &in, const LTPlan &pl, const RotKeys &keys) {
+  // HoistHandler::Evaluate, Hoist.cu:554-975 (non-min-KS, fused kernels)
+  const bool only_gs = pl.bs_idx.size() == 1 && pl.bs_idx[0] == 0;
+  if (!only_gs) {
+    DeviceCt *r = &res;
+    const DeviceCt *i = &in;
+    return lt_evaluate_batch(1, &r, &i, pl, keys);
+  }
+  const int level = pl.pt_level;
+  const int n = P->n;
+  CHD_CHECK(!in.has_rx && in.np.aux == 0, kErrShape, "Hoist: input should be relinearized and mod-down");
+  CHD_CHECK(in.np == P->level_np(level), kErrShape, "Hoist: input level mismatch");
+  const HoistOps H(*this, level);
+  const size_t tw_ = H.tw;
+  auto key_of = [&](int r) -> const DeviceEvk * {
+    auto it = keys.find(r);
+    return it == keys.end() ? nullptr : it->second;
+  };
+  ArenaScope scope(arena);
+  auto alloc = [&](size_t words) { return static_cast<uint32_t *>(arena.alloc(words * 4)); };
+  std::vector<uint32_t *> mu(H.m.beta);
+  for (int i = 0; i < H.m.beta; i++) {
     mu[i] = alloc(tw_);
     CHD_CHECK(mu[i], kErrAlloc, "Hoist: scratch allocation failed");
   }
   uint32_t *fb = alloc(tw_), *fa = alloc(tw_);  // final accumulator (Q u P)
   CHD_CHECK(fb && fa, kErrAlloc, "Hoist: scratch allocation failed");
-  const bool only_gs = pl.bs_idx.size() == 1 && pl.bs_idx[0] == 0;
-  if (only_gs) {
-    // Hoist.cu:706-808: ModUp(a) once, per giant step key mult + P b, times pt,
-    // then PermuteAccum
-    CHD_TRY(modup(level, in.ax, mu.data()));
-    uint32_t *bxp = alloc(tw_), *tb = alloc(tw_), *ta = alloc(tw_);
-    uint32_t *p0b = alloc(tw_), *p0a = alloc(tw_);
-    CHD_CHECK(bxp && tb && ta && p0b && p0a, kErrAlloc, "Hoist: scratch allocation failed");
-    pseudo_modup(in.bx, bxp);
-    bool have0 = false;
-    bool first_sum = true;
-    for (const auto &pt : pl.pts) {
-      if (pt.gs == 0) {
-        pseudo_modup(in.ax, p0a);
-        CHD_TRY(pt_accum({{bxp, p0a}}, {{{0, pt.dev}}}, {{fb, fa}}));
-        have0 = true;
-      }
-    }
-    for (const auto &pt : pl.pts) {
-      if (pt.gs == 0) continue;
-      const DeviceEvk *k = key_of(pt.gs);
-      CHD_CHECK(k, kErrKey, "Hoist: missing rotation key " + std::to_string(pt.gs));
-      CHD_TRY(key_mult(mu.data(), *k, tb, ta));
-      add_rows(tb, bxp, tb, nq);
-      CHD_TRY(pt_accum({{tb, ta}}, {{{0, pt.dev}}}, {{p0b, p0a}}));
-      if (!have0 && first_sum) {
-        permute_rows(p0b, fb, nullptr, pt.gs);
-        permute_rows(p0a, fa, nullptr, pt.gs);
-      } else {
-        permute_rows(p0b, fb, fb, pt.gs);
-        permute_rows(p0a, fa, fa, pt.gs);
-      }
-      first_sum = false;
-    }
-    CHD_CHECK(have0 || !first_sum, kErrInvalidArg, "Hoist: empty plan");
-  } else {
-    // baby steps (Hoist.cu:578-691)
-    std::vector<DeviceCt> bs(pl.bs_idx.size());
-    for (size_t i = 0; i < pl.bs_idx.size(); i++)
-      if (pl.bs_idx[i] != 0) CHD_TRY(scratch_ct(arena, bs[i], qp, false, n));
-    std::vector<int> rot_d;
-    std::vector<const DeviceEvk *> rot_k;
-    std::vector<DeviceCt *> rot_o;
-    std::map<int, int> slot_of;
-    for (size_t i = 0; i < pl.bs_idx.size(); i++) {
-      const int r = pl.bs_idx[i];
-      slot_of[r] = static_cast<int>(i);
-      if (r == 0) continue;
-      const DeviceEvk *k = key_of(r);
-      CHD_CHECK(k, kErrKey, "Hoist: missing rotation key " + std::to_string(r));
-      rot_d.push_back(r);
-      rot_k.push_back(k);
-      rot_o.push_back(&bs[i]);
-    }
-    if (!rot_d.empty()) CHD_TRY(hoisted_rotate(in, static_cast<int>(rot_d.size()), rot_d.data(), rot_k.data(), rot_o.data()));
-    std::vector<std::pair<const uint32_t *, const uint32_t *>> ins(pl.bs_idx.size());
-    for (size_t i = 0; i < pl.bs_idx.size(); i++) {
-      if (pl.bs_idx[i] == 0) {
-        uint32_t *b0 = alloc(tw_), *a0 = alloc(tw_);
-        CHD_CHECK(b0 && a0, kErrAlloc, "Hoist: scratch allocation failed");
-        pseudo_modup(in.bx, b0);
-        pseudo_modup(in.ax, a0);
-        ins[i] = {b0, a0};
-      } else {
-        ins[i] = {bs[i].bx, bs[i].ax};
-      }
-    }
-    // giant-step plaintext accumulation (GSFusedPAccum, Hoist.cu:329-420)
-    std::vector<std::vector<std::pair<int, const uint32_t *>>> terms(pl.gs_idx.size());
-    std::vector<std::pair<uint32_t *, uint32_t *>> outs(pl.gs_idx.size());
-    std::map<int, int> gpos;
-    for (size_t i = 0; i < pl.gs_idx.size(); i++) gpos[pl.gs_idx[i]] = static_cast<int>(i);
-    for (const auto &pt : pl.pts) terms[gpos[pt.gs]].push_back({slot_of[pt.bs], pt.dev});
-    bool have0 = false;
-    for (size_t i = 0; i < pl.gs_idx.size(); i++) {
-      if (pl.gs_idx[i] == 0) {
-        outs[i] = {fb, fa};
-        have0 = true;
-      } else {
-        uint32_t *b = alloc(tw_), *a = alloc(tw_);
-        CHD_CHECK(b && a, kErrAlloc, "Hoist: scratch allocation failed");
-        outs[i] = {b, a};
-      }
-    }
-    CHD_TRY(pt_accum(ins, terms, outs));
-    if (!have0) {
-      // no giant step 0: the accumulator starts from zero
-      cudaMemsetAsync(fb, 0, tw_ * 4, stream);
-      cudaMemsetAsync(fa, 0, tw_ * 4, stream);
-    }
-    // giant-step rotations (EvaluateGiantStepOptimized, Hoist.cu:860-975)
-    uint32_t *md = alloc(static_cast<size_t>(nq) * n), *tb = alloc(tw_), *ta = alloc(tw_);
-    CHD_CHECK(md && tb && ta, kErrAlloc, "Hoist: scratch allocation failed");
-    for (size_t i = 0; i < pl.gs_idx.size(); i++) {
-      const int gsr = pl.gs_idx[i];
-      if (gsr == 0) continue;
-      const DeviceEvk *k = key_of(gsr);
-      CHD_CHECK(k, kErrKey, "Hoist: missing rotation key " + std::to_string(gsr));
-      const uint32_t *src[1] = {outs[i].second};
-      uint32_t *dst[1] = {md};
-      CHD_TRY(moddown(level, MDType::kModDown, src, dst, 1));
-      CHD_TRY(modup(level, md, mu.data()));
-      CHD_TRY(key_mult(mu.data(), *k, tb, ta));
-      // key-switched part plus the accumulator's own b, both rotated
-      add_rows(tb, outs[i].first, tb, tot);
-      permute_rows(tb, fb, fb, gsr);
-      permute_rows(ta, fa, fa, gsr);
+  // Hoist.cu:706-808: ModUp(a) once, per giant step key mult + P b, times pt,
+  // then PermuteAccum
+  CHD_TRY(modup(level, in.ax, mu.data()));
+  uint32_t *bxp = alloc(tw_), *tb = alloc(tw_), *ta = alloc(tw_);
+  uint32_t *p0b = alloc(tw_), *p0a = alloc(tw_);
+  CHD_CHECK(bxp && tb && ta && p0b && p0a, kErrAlloc, "Hoist: scratch allocation failed");
+  H.pseudo_modup(in.bx, bxp);
+  bool have0 = false;
+  bool first_sum = true;
+  for (const auto &pt : pl.pts) {
+    if (pt.gs == 0) {
+      H.pseudo_modup(in.ax, p0a);
+      CHD_TRY(H.pt_accum({{bxp, p0a}}, {{{0, pt.dev}}}, {{fb, fa}}));
+      have0 = true;
     }
   }
+  uint32_t *const *mu1[1] = {mu.data()};
+  for (const auto &pt : pl.pts) {
+    if (pt.gs == 0) continue;
+    const DeviceEvk *k = key_of(pt.gs);
+    CHD_CHECK(k, kErrKey, "Hoist: missing rotation key " + std::to_string(pt.gs));
+    CHD_TRY(H.key_mult(1, mu1, *k, &tb, &ta));
+    H.add_rows(tb, bxp, tb, H.nq);
+    CHD_TRY(H.pt_accum({{tb, ta}}, {{{0, pt.dev}}}, {{p0b, p0a}}));
+    if (!have0 && first_sum) {
+      H.permute_rows(p0b, fb, nullptr, pt.gs);
+      H.permute_rows(p0a, fa, nullptr, pt.gs);
+    } else {
+      H.permute_rows(p0b, fb, fb, pt.gs);
+      H.permute_rows(p0a, fa, fa, pt.gs);
+    }
+    first_sum = false;
+  }
+  CHD_CHECK(have0 || !first_sum, kErrInvalidArg, "Hoist: empty plan");
   // EvaluateFinalModDown, Hoist.cu:460-488
   const double in_scale = in.scale;
   const int in_slots = in.num_slots;
@@ -553,6 +528,155 @@ Status Context::lt_evaluate(DeviceCt &res, const DeviceCt &in, const LTPlan &pl,
   CHD_TRY(moddown(level, MDType::kModDownRescale, src, dst, 2));
   res.scale = pl.pt_scale * in_scale / P->rescale_prod[level];
   res.num_slots = std::max(in_slots, pl.pt_slots);
+  return check_cuda("linear transform");
+}
+
+Status Context::lt_evaluate_batch(int count, DeviceCt *const *res, const DeviceCt *const *in, const LTPlan &pl,
+                                  const RotKeys &keys) {
+  // HoistHandler::Evaluate (Hoist.cu:554-975) for `count` ciphertexts at one
+  // level: per ciphertext the hoisted baby steps and the giant-step
+  // plaintext accumulation; across the batch every giant step's ModDown,
+  // ModUp and key product, and the final ModDownAndRescale, run as one
+  // batched launch sequence.  Each ciphertext's result equals lt_evaluate's.
+  const bool only_gs = pl.bs_idx.size() == 1 && pl.bs_idx[0] == 0;
+  if (only_gs) {
+    for (int c = 0; c < count; c++) CHD_TRY(lt_evaluate(*res[c], *in[c], pl, keys));
+    return kOk;
+  }
+  const int level = pl.pt_level;
+  const int n = P->n;
+  for (int c = 0; c < count; c++) {
+    CHD_CHECK(!in[c]->has_rx && in[c]->np.aux == 0, kErrShape, "Hoist: input should be relinearized and mod-down");
+    CHD_CHECK(in[c]->np == P->level_np(level), kErrShape, "Hoist: input level mismatch");
+    for (int d = 0; d < count; d++)
+      CHD_CHECK(c == d || res[c] != in[d], kErrInvalidArg, "Hoist: a result aliases another input of the batch");
+  }
+  const HoistOps H(*this, level);
+  const size_t tw_ = H.tw;
+  const NP qp = H.qp;
+  auto key_of = [&](int r) -> const DeviceEvk * {
+    auto it = keys.find(r);
+    return it == keys.end() ? nullptr : it->second;
+  };
+  ArenaScope scope(arena);
+  auto alloc = [&](size_t words) { return static_cast<uint32_t *>(arena.alloc(words * 4)); };
+  // per ciphertext, for the whole call: ModUp digits, the final accumulator,
+  // scratch of the giant steps and the giant-step sums
+  std::vector<std::vector<uint32_t *>> mu(count, std::vector<uint32_t *>(H.m.beta));
+  std::vector<uint32_t *const *> mu_p(count);
+  std::vector<uint32_t *> fb(count), fa(count), md(count), tb(count), ta(count);
+  std::vector<std::vector<std::pair<uint32_t *, uint32_t *>>> outs(count);
+  std::map<int, int> slot_of, gpos;
+  for (size_t i = 0; i < pl.bs_idx.size(); i++) slot_of[pl.bs_idx[i]] = static_cast<int>(i);
+  for (size_t i = 0; i < pl.gs_idx.size(); i++) gpos[pl.gs_idx[i]] = static_cast<int>(i);
+  std::vector<std::vector<std::pair<int, const uint32_t *>>> terms(pl.gs_idx.size());
+  for (const auto &pt : pl.pts) terms[gpos[pt.gs]].push_back({slot_of[pt.bs], pt.dev});
+  bool have0 = false;
+  for (int x : pl.gs_idx) have0 = have0 || x == 0;
+  for (int c = 0; c < count; c++) {
+    for (int i = 0; i < H.m.beta; i++) {
+      mu[c][i] = alloc(tw_);
+      CHD_CHECK(mu[c][i], kErrAlloc, "Hoist: scratch allocation failed");
+    }
+    mu_p[c] = mu[c].data();
+    fb[c] = alloc(tw_);
+    fa[c] = alloc(tw_);
+    md[c] = alloc(static_cast<size_t>(H.nq) * n);
+    tb[c] = alloc(tw_);
+    ta[c] = alloc(tw_);
+    CHD_CHECK(fb[c] && fa[c] && md[c] && tb[c] && ta[c], kErrAlloc, "Hoist: scratch allocation failed");
+    outs[c].resize(pl.gs_idx.size());
+    for (size_t i = 0; i < pl.gs_idx.size(); i++) {
+      if (pl.gs_idx[i] == 0) {
+        outs[c][i] = {fb[c], fa[c]};
+      } else {
+        uint32_t *b = alloc(tw_), *a = alloc(tw_);
+        CHD_CHECK(b && a, kErrAlloc, "Hoist: scratch allocation failed");
+        outs[c][i] = {b, a};
+      }
+    }
+  }
+  for (int c = 0; c < count; c++) {
+    // baby steps (Hoist.cu:578-691), released after this ciphertext's
+    // accumulation (stream order makes the reuse by the next one safe)
+    ArenaScope bs_scope(arena);
+    std::vector<DeviceCt> bs(pl.bs_idx.size());
+    for (size_t i = 0; i < pl.bs_idx.size(); i++)
+      if (pl.bs_idx[i] != 0) CHD_TRY(scratch_ct(arena, bs[i], qp, false, n));
+    std::vector<int> rot_d;
+    std::vector<const DeviceEvk *> rot_k;
+    std::vector<DeviceCt *> rot_o;
+    for (size_t i = 0; i < pl.bs_idx.size(); i++) {
+      const int r = pl.bs_idx[i];
+      if (r == 0) continue;
+      const DeviceEvk *k = key_of(r);
+      CHD_CHECK(k, kErrKey, "Hoist: missing rotation key " + std::to_string(r));
+      rot_d.push_back(r);
+      rot_k.push_back(k);
+      rot_o.push_back(&bs[i]);
+    }
+    if (!rot_d.empty())
+      CHD_TRY(hoisted_rotate(*in[c], static_cast<int>(rot_d.size()), rot_d.data(), rot_k.data(), rot_o.data()));
+    std::vector<std::pair<const uint32_t *, const uint32_t *>> ins(pl.bs_idx.size());
+    for (size_t i = 0; i < pl.bs_idx.size(); i++) {
+      if (pl.bs_idx[i] == 0) {
+        uint32_t *b0 = alloc(tw_), *a0 = alloc(tw_);
+        CHD_CHECK(b0 && a0, kErrAlloc, "Hoist: scratch allocation failed");
+        H.pseudo_modup(in[c]->bx, b0);
+        H.pseudo_modup(in[c]->ax, a0);
+        ins[i] = {b0, a0};
+      } else {
+        ins[i] = {bs[i].bx, bs[i].ax};
+      }
+    }
+    // giant-step plaintext accumulation (GSFusedPAccum, Hoist.cu:329-420)
+    CHD_TRY(H.pt_accum(ins, terms, outs[c]));
+    if (!have0) {
+      // no giant step 0: the accumulator starts from zero
+      cudaMemsetAsync(fb[c], 0, tw_ * 4, stream);
+      cudaMemsetAsync(fa[c], 0, tw_ * 4, stream);
+    }
+  }
+  // giant-step rotations (EvaluateGiantStepOptimized, Hoist.cu:860-975),
+  // each step batched over the ciphertexts
+  std::vector<const uint32_t *> src(count);
+  for (size_t i = 0; i < pl.gs_idx.size(); i++) {
+    const int gsr = pl.gs_idx[i];
+    if (gsr == 0) continue;
+    const DeviceEvk *k = key_of(gsr);
+    CHD_CHECK(k, kErrKey, "Hoist: missing rotation key " + std::to_string(gsr));
+    for (int c = 0; c < count; c++) src[c] = outs[c][i].second;
+    CHD_TRY(moddown(level, MDType::kModDown, src.data(), md.data(), count));
+    CHD_TRY(modup_many(level, count, md.data(), mu_p.data()));
+    CHD_TRY(H.key_mult(count, mu_p.data(), *k, tb.data(), ta.data()));
+    for (int c = 0; c < count; c++) {
+      // key-switched part plus the accumulator's own b, both rotated
+      H.add_rows(tb[c], outs[c][i].first, tb[c], H.tot);
+      H.permute_rows(tb[c], fb[c], fb[c], gsr);
+      H.permute_rows(ta[c], fa[c], fa[c], gsr);
+    }
+  }
+  // EvaluateFinalModDown, Hoist.cu:460-488, all ciphertexts at once
+  std::vector<const uint32_t *> fsrc(2 * count);
+  std::vector<uint32_t *> fdst(2 * count);
+  std::vector<double> in_scale(count);
+  std::vector<int> in_slots(count);
+  for (int c = 0; c < count; c++) {
+    in_scale[c] = in[c]->scale;
+    in_slots[c] = in[c]->num_slots;
+  }
+  for (int c = 0; c < count; c++) {
+    CHD_TRY(res[c]->reserve(P->level_np(level - 1), false, n));
+    fsrc[2 * c] = fb[c];
+    fsrc[2 * c + 1] = fa[c];
+    fdst[2 * c] = res[c]->bx;
+    fdst[2 * c + 1] = res[c]->ax;
+  }
+  CHD_TRY(moddown(level, MDType::kModDownRescale, fsrc.data(), fdst.data(), 2 * count));
+  for (int c = 0; c < count; c++) {
+    res[c]->scale = pl.pt_scale * in_scale[c] / P->rescale_prod[level];
+    res[c]->num_slots = std::max(in_slots[c], pl.pt_slots);
+  }
   return check_cuda("linear transform");
 }
 

@@ -57,9 +57,21 @@ Status Context::program_regs(const Program &prog, std::vector<DeviceCt> &regs) {
 
 Status Context::run_program(const Program &prog, std::vector<DeviceCt> &regs, const ProgKeys &keys,
                             const std::vector<const LTPlan *> *lts) {
+  std::vector<DeviceCt> *r = &regs;
+  return run_program_batch(prog, 1, &r, keys, lts);
+}
+
+Status Context::run_program_batch(const Program &prog, int count, std::vector<DeviceCt> *const *R,
+                                  const ProgKeys &keys, const std::vector<const LTPlan *> *lts) {
+  // The program on `count` ciphertexts, each with its own registers R[c]:
+  // key switches (RelinearizeRescale, HConj, HRotAdd), rescales and linear
+  // transforms run once over the whole batch (fused launches of all its
+  // ciphertexts); the element-wise ops run per ciphertext.  Every
+  // ciphertext's result equals a run of the program on it alone.
   const DeviceEvk *mult_key = keys.mult, *conj_key = keys.conj;
   const RotKeys *rot_keys = keys.rot;
-  CHD_TRY(program_regs(prog, regs));
+  CHD_CHECK(count >= 1, kErrInvalidArg, "program: empty batch");
+  for (int c = 0; c < count; c++) CHD_TRY(program_regs(prog, *R[c]));
   const int n = P->n;
   // constants: Montgomery residues over their own level's q primes
   std::vector<std::vector<uint32_t>> cx(prog.consts.size());
@@ -69,7 +81,6 @@ Status Context::run_program(const Program &prog, std::vector<DeviceCt> &regs, co
     encode_const(c.level, c.scale, c.value, 0, &cx[i]);
     cnp[i] = P->level_np(c.level);
   }
-  DeviceCt &spare = regs[prog.nregs], &spare2 = regs[prog.nregs + 1];
   // dst (parts) = sum over terms of src_t (.) c_t, at np, each term reading
   // its source from row `front_t`
   struct Term {
@@ -121,8 +132,169 @@ Status Context::run_program(const Program &prog, std::vector<DeviceCt> &regs, co
     return ones.back().data();
   };
 
+  auto rot_key_of = [&](int r, const DeviceEvk **k) -> Status {
+    CHD_CHECK(rot_keys, kErrKey, "program: rotation keys missing");
+    auto it = rot_keys->find(r);
+    CHD_CHECK(it != rot_keys->end() && it->second, kErrKey, "program: missing rotation key " + std::to_string(r));
+    *k = it->second;
+    return kOk;
+  };
+  // MultKey (key switch + ModDown, no rescale) of register a of every
+  // ciphertext into spare2
+  auto mult_key_batch = [&](int a, const DeviceEvk &key) -> Status {
+    const DeviceCt &a0 = R[0]->at(a);
+    CHD_CHECK(!a0.has_rx && a0.np.aux == 0, kErrShape, "MultKey: ciphertext must be relinearised, no aux primes");
+    const int level = P->np_to_level(a0.np);
+    CHD_CHECK(level >= 0, kErrInvalidLevel, "MultKey: invalid level");
+    std::vector<KSIn> ins(count);
+    for (int c = 0; c < count; c++) {
+      const DeviceCt &x = R[c]->at(a);
+      CHD_CHECK(x.np == a0.np && !x.has_rx, kErrShape, "program: batch members at different levels");
+      DeviceCt &o = R[c]->at(prog.nregs + 1);
+      CHD_TRY(o.reserve(x.np, false, n));
+      ins[c] = KSIn{1, x.bx, x.ax, nullptr, nullptr, o.bx, o.ax};
+    }
+    CHD_TRY(key_switch_fused(level, count, ins.data(), key, MDType::kModDown));
+    for (int c = 0; c < count; c++) {
+      DeviceCt &o = R[c]->at(prog.nregs + 1);
+      o.scale = R[c]->at(a).scale;
+      o.num_slots = R[c]->at(a).num_slots;
+    }
+    return kOk;
+  };
+  const bool fused_ks = n == 65536 && count > 1;
+
   for (const ProgOp &op : prog.ops) {
+    // ---- ops that run once over the whole batch ----
+    bool batched = true;
+    switch (op.kind) {
+      case OpKind::kRelinRescale: {
+        if (!fused_ks) {
+          batched = false;
+          break;
+        }
+        CHD_CHECK(mult_key, kErrKey, "program: multiplication key missing");
+        const DeviceCt &a0 = R[0]->at(op.a);
+        CHD_CHECK(a0.has_rx && a0.np.aux == 0, kErrShape, "Relinearize requires a ciphertext with rx");
+        const int level = P->np_to_level(a0.np);
+        CHD_CHECK(level >= 1, kErrInvalidLevel, "Not enough q primes to rescale");
+        const NP out_np = P->level_np(level - 1, 0);
+        std::vector<KSIn> ins(count);
+        for (int c = 0; c < count; c++) {
+          const DeviceCt &x = R[c]->at(op.a);
+          CHD_CHECK(x.np == a0.np && x.has_rx, kErrShape, "program: batch members at different levels");
+          DeviceCt &t = R[c]->at(prog.nregs);
+          CHD_TRY(t.reserve(out_np, false, n));
+          ins[c] = KSIn{2, x.bx, x.ax, nullptr, x.rx, t.bx, t.ax};
+        }
+        CHD_TRY(key_switch_fused(level, count, ins.data(), *mult_key, MDType::kModDownRescale));
+        for (int c = 0; c < count; c++) {
+          DeviceCt &t = R[c]->at(prog.nregs);
+          t.scale = R[c]->at(op.a).scale / P->rescale_prod[level];
+          t.num_slots = R[c]->at(op.a).num_slots;
+        }
+        break;
+      }
+      case OpKind::kRescale:
+      case OpKind::kLevelDown: {
+        if (count == 1) {
+          batched = false;
+          break;
+        }
+        const DeviceCt &a0 = R[0]->at(op.a);
+        CHD_CHECK(a0.np.aux == 0, kErrShape, "Rescale is not supported for ciphertexts with p primes");
+        const int level = P->np_to_level(a0.np);
+        CHD_CHECK(level >= 1, kErrInvalidLevel, "Not enough q primes to rescale");
+        const int parts = a0.has_rx ? 3 : 2;
+        std::vector<const uint32_t *> src;
+        std::vector<uint32_t *> dst;
+        for (int c = 0; c < count; c++) {
+          const DeviceCt &x = R[c]->at(op.a);
+          CHD_CHECK(x.np == a0.np && x.has_rx == a0.has_rx, kErrShape, "program: batch members at different levels");
+          const DeviceCt *in = &x;
+          if (op.kind == OpKind::kLevelDown) {
+            // times the constant 1 at this level's rescale prime product, into spare2
+            DeviceCt &m = R[c]->at(prog.nregs + 1);
+            CHD_TRY(check_subset(x.np, cnp.at(op.c)));
+            CHD_TRY(m.reserve(x.np, x.has_rx, n));
+            const uint32_t *cc = cx[op.c].data() + front_of(cnp[op.c], x.np);
+            CHD_TRY(const_accum(m, x.np, parts, {{&x, 0, cc}}));
+            m.scale = x.scale * prog.consts[op.c].scale;
+            m.num_slots = x.num_slots;
+            in = &m;
+          }
+          DeviceCt &t = R[c]->at(prog.nregs);
+          CHD_TRY(t.reserve(P->level_np(level - 1, 0), x.has_rx, n));
+          for (int p = 0; p < parts; p++) {
+            src.push_back(part_of(*in, p));
+            dst.push_back(part_of(t, p));
+          }
+          t.scale = in->scale / P->rescale_prod[level];
+          t.num_slots = in->num_slots;
+        }
+        CHD_TRY(moddown(level, MDType::kRescale, src.data(), dst.data(), static_cast<int>(src.size())));
+        break;
+      }
+      case OpKind::kHConj: {
+        if (!fused_ks) {
+          batched = false;
+          break;
+        }
+        CHD_CHECK(conj_key, kErrKey, "program: conjugation key missing");
+        CHD_TRY(mult_key_batch(op.a, *conj_key));
+        for (int c = 0; c < count; c++) CHD_TRY(permute(R[c]->at(prog.nregs), R[c]->at(prog.nregs + 1), -1));
+        break;
+      }
+      case OpKind::kHRotAdd: {
+        const DeviceCt &a0 = R[0]->at(op.a);
+        const int slots = a0.num_slots > 0 ? a0.num_slots : n / 2;
+        int dist = op.rot % slots;
+        if (dist < 0) dist += slots;
+        if (!fused_ks || dist == 0) {
+          batched = false;
+          break;
+        }
+        const DeviceEvk *k = nullptr;
+        CHD_TRY(rot_key_of(op.rot, &k));
+        CHD_TRY(mult_key_batch(op.a, *k));
+        for (int c = 0; c < count; c++) {
+          // res = Permute(MultKey(a)) + b (Context.cpp:800-830)
+          DeviceCt &t = R[c]->at(prog.nregs);
+          CHD_TRY(permute(t, R[c]->at(prog.nregs + 1), dist));
+          CHD_TRY(add(t, t, R[c]->at(op.b)));
+        }
+        break;
+      }
+      case OpKind::kLinTrans: {
+        if (count == 1 || keys.min_ks) {
+          batched = false;
+          break;
+        }
+        CHD_CHECK(lts && op.rot >= 0 && op.rot < static_cast<int>(lts->size()) && rot_keys, kErrInvalidArg,
+                  "program: linear transform missing");
+        std::vector<DeviceCt *> out(count);
+        std::vector<const DeviceCt *> in(count);
+        for (int c = 0; c < count; c++) {
+          out[c] = &R[c]->at(prog.nregs);
+          in[c] = &R[c]->at(op.a);
+        }
+        CHD_TRY(lt_evaluate_batch(count, out.data(), in.data(), *(*lts)[op.rot], *rot_keys));
+        break;
+      }
+      default:
+        batched = false;
+        break;
+    }
+    if (batched) {
+      for (int c = 0; c < count; c++) swap_regs(R[c]->at(op.dst), R[c]->at(prog.nregs));
+      continue;
+    }
+    // ---- ops that run per ciphertext ----
+    for (int bc = 0; bc < count; bc++) {
+    std::vector<DeviceCt> &regs = *R[bc];
+    DeviceCt &spare = regs[prog.nregs], &spare2 = regs[prog.nregs + 1];
     DeviceCt &t = spare;
+    bool meta = false;
     switch (op.kind) {
       case OpKind::kConstMult:
       case OpKind::kLevelDown: {
@@ -260,10 +432,12 @@ Status Context::run_program(const Program &prog, std::vector<DeviceCt> &regs, co
       }
       case OpKind::kSetScale:
         regs.at(op.dst).scale = op.scale;
-        continue;
+        meta = true;
+        break;
       case OpKind::kSetSlots:
         regs.at(op.dst).num_slots = op.rot;
-        continue;
+        meta = true;
+        break;
       case OpKind::kHConj:
         CHD_CHECK(conj_key, kErrKey, "program: conjugation key missing");
         CHD_TRY(hconj(t, regs.at(op.a), *conj_key));
@@ -298,7 +472,8 @@ Status Context::run_program(const Program &prog, std::vector<DeviceCt> &regs, co
         }
         break;
     }
-    swap_regs(regs.at(op.dst), t);
+    if (!meta) swap_regs(regs.at(op.dst), t);
+    }
   }
   return check_cuda("program");
 }

@@ -293,6 +293,14 @@ int chd_boot_lt_pt(const chd_boot *b, int i, int j, int *gs, int *bs, double *re
 /* Boot(res, input, evk_map, min_ks) (BootContext.h:139-140) */
 int chd_boot_run(chd_context *ctx, chd_boot *b, chd_ciphertext *res, const chd_ciphertext *in, const chd_evk_map *keys,
                  int min_ks);
+/* Boot of `count` ciphertexts in one call (no reference counterpart; the
+ * reference bootstraps one ciphertext per call): every key switch, rescale
+ * and linear transform of the bootstrapping program runs once over the
+ * whole batch.  Each res[i] equals chd_boot_run(res[i], in[i]); results must
+ * be distinct (a result may alias an input).  Inputs may sit at different
+ * levels (each is brought down to level 0 first). */
+int chd_boot_run_batch(chd_context *ctx, chd_boot *b, int count, chd_ciphertext *const *res,
+                       const chd_ciphertext *const *in, const chd_evk_map *keys, int min_ks);
 
 /* CUDA graphs of library calls (no reference counterpart; the reference
  * issues every kernel from the host).  chd_graph_begin starts capturing the

@@ -268,6 +268,18 @@ class BootContext {
   void Boot(Ciphertext &res, const Ciphertext &in, const EvkMap &evk_map, bool min_ks = false) {
     check(chd_boot_run(ctx_.raw(), b_, res.raw(), in.raw(), evk_map.raw(), min_ks ? 1 : 0));
   }
+  // every ciphertext of the batch in one call (key switches batched)
+  void BootBatch(const std::vector<Ciphertext *> &res, const std::vector<const Ciphertext *> &in,
+                 const EvkMap &evk_map, bool min_ks = false) {
+    std::vector<chd_ciphertext *> r;
+    std::vector<const chd_ciphertext *> x;
+    for (size_t i = 0; i < res.size(); i++) {
+      r.push_back(res[i]->raw());
+      x.push_back(in[i]->raw());
+    }
+    check(chd_boot_run_batch(ctx_.raw(), b_, static_cast<int>(r.size()), r.data(), x.data(), evk_map.raw(),
+                             min_ks ? 1 : 0));
+  }
 
  private:
   Context &ctx_;

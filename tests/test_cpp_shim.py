@@ -26,6 +26,7 @@ void unused_paths(cheddar_b200::Context &ctx, const cheddar_b200::EvaluationKey 
   m.SetDenseToSparseKey(k);
   m.SetSparseToDenseKey(k);
   bc.Boot(b, a, m);
+  bc.BootBatch({&b}, {&a}, m);
   std::vector<uint32_t> cx = ctx.EncodeConstant(0, 1.0, 0.5);
   ctx.SetKeySwitchEngine(CHD_BCONV_TENSOR_CORE);
   int eng = ctx.KeySwitchEngine();

@@ -82,3 +82,31 @@ def test_boot_min_ks_bit_exact_and_precision(cuda_ok):
     err = np.abs(dec - msg).max()
     print(f"min-KS bootstrapping precision: {-np.log2(err):.2f} bits")
     assert -np.log2(err) > 10
+
+
+def test_boot_batch_equals_single(cuda_ok):
+    # BootBatch: every key switch, rescale and linear transform of the
+    # program runs once over the batch; each result equals a single Boot,
+    # also with the min-KS transforms and with a result aliasing its input
+    o, g, bc, s, mk, ck, rks, keys = _setup()
+    rng = np.random.default_rng(77)
+    half = o.n // 2
+    sc0 = o.scale(0)
+    cts = []
+    for i in range(3):
+        msg = (rng.random(half) * 2 - 1) + 1j * (rng.random(half) * 2 - 1)
+        bx, ax = o.encrypt(40 + i, s, 0, o.encode(0, sc0, msg))
+        cts.append((bx, ax))
+    for min_ks in (False, True):
+        single = [bc.Boot(g.import_ct(0, list(c), sc0), keys, min_ks=min_ks).numpy() for c in cts]
+        ins = [g.import_ct(0, list(c), sc0) for c in cts]
+        outs = bc.BootBatch(ins, keys, min_ks=min_ks)
+        for a, b in zip(outs, single):
+            p = a.numpy()
+            assert np.array_equal(p[0], b[0]) and np.array_equal(p[1], b[1])
+        # in place: results alias the inputs
+        ins = [g.import_ct(0, list(c), sc0) for c in cts]
+        bc.BootBatch(ins, keys, res_list=ins, min_ks=min_ks)
+        for a, b in zip(ins, single):
+            p = a.numpy()
+            assert np.array_equal(p[0], b[0]) and np.array_equal(p[1], b[1])

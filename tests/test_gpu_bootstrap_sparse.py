@@ -112,3 +112,16 @@ def test_merge_two_real(cuda_ok):
     msg, dec, _ = _run(512, chd.BOOT_MERGE_TWO_REAL, 4242)
     err = np.abs(dec - msg / 2).max()
     assert -np.log2(err) > 10
+
+
+def test_sparse_boot_batch(cuda_ok):
+    o, g, s, mk, ck = _keys()
+    bc, rks, keys = _setup(512, chd.BOOT_NORMAL)
+    sc0 = o.scale(0)
+    rng = np.random.default_rng(8)
+    cts = [o.encrypt(60 + i, s, 0, o.encode(0, sc0, rng.random(512) - 0.5)) for i in range(2)]
+    single = [bc.Boot(g.import_ct(0, list(c), sc0, num_slots=512), keys).numpy() for c in cts]
+    outs = bc.BootBatch([g.import_ct(0, list(c), sc0, num_slots=512) for c in cts], keys)
+    for a, b in zip(outs, single):
+        p = a.numpy()
+        assert np.array_equal(p[0], b[0]) and np.array_equal(p[1], b[1])
