@@ -1909,6 +1909,44 @@ Status Context::hconj(DeviceCt &res, const DeviceCt &a, const DeviceEvk &key) {
   return permute(res, tmp, -1);
 }
 
+Status Context::hrot_batch(int count, DeviceCt *const *res, const DeviceCt *const *a, const DeviceEvk &key,
+                           int dist) {
+  const DeviceCt &a0 = *a[0];
+  int d = dist;
+  if (d != -1) {
+    const int slots = a0.num_slots > 0 ? a0.num_slots : P->n / 2;
+    d %= slots;
+    if (d < 0) d += slots;
+  }
+  if (P->log_n != 16 || count == 1 || d == 0) {
+    for (int c = 0; c < count; c++) {
+      if (dist == -1)
+        CHD_TRY(hconj(*res[c], *a[c], key));
+      else
+        CHD_TRY(hrot(*res[c], *a[c], key, dist));
+    }
+    return kOk;
+  }
+  CHD_CHECK(!a0.has_rx && a0.np.aux == 0, kErrShape, "MultKey: ciphertext must be relinearised, no aux primes");
+  const int level = level_of(*P, a0);
+  CHD_CHECK(level >= 0, kErrInvalidLevel, "MultKey: invalid level");
+  ArenaScope scope(arena);
+  std::vector<DeviceCt> tmp(count);
+  std::vector<KSIn> ins(count);
+  for (int c = 0; c < count; c++) {
+    CHD_CHECK(a[c]->np == a0.np && !a[c]->has_rx, kErrShape, "HRot batch: ciphertexts at different levels");
+    CHD_TRY(scratch_ct(arena, tmp[c], a0.np, false, P->n));
+    ins[c] = KSIn{1, a[c]->bx, a[c]->ax, nullptr, nullptr, tmp[c].bx, tmp[c].ax};
+  }
+  CHD_TRY(key_switch_fused(level, count, ins.data(), key, MDType::kModDown));
+  for (int c = 0; c < count; c++) {
+    tmp[c].scale = a[c]->scale;
+    tmp[c].num_slots = a[c]->num_slots;
+    CHD_TRY(permute(*res[c], tmp[c], d));
+  }
+  return kOk;
+}
+
 Status Context::hrot_add(DeviceCt &res, const DeviceCt &a, const DeviceCt &b, const DeviceEvk &key, int dist) {
   // Context.cpp:800-830: res = Permute(MultKey(a)) + b
   CHD_CHECK(a.np == b.np, kErrShape, "HRotAdd: level mismatch");

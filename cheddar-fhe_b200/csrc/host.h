@@ -433,6 +433,12 @@ class Context {
                            const RotKeys &keys);
   // the min-KS evaluation (Hoist.cu:490-552): two rotation keys per transform
   Status lt_evaluate_min_ks(DeviceCt &res, const DeviceCt &in, const LTPlan &pl, const RotKeys &keys);
+  Status lt_evaluate_min_ks_batch(int count, DeviceCt *const *res, const DeviceCt *const *in, const LTPlan &pl,
+                                  const RotKeys &keys);
+  // HRot (dist >= 0) or HConj (dist = -1) of `count` ciphertexts at one
+  // level with one key: a single fused key switch over the batch, then the
+  // automorphisms; res[c] may alias a[c]
+  Status hrot_batch(int count, DeviceCt *const *res, const DeviceCt *const *a, const DeviceEvk &key, int dist);
 
   // EvalPoly::Compile (EvalPoly.cpp:750-830) of a polynomial in the
   // Chebyshev (or power) basis for an input at (input_level, input_scale):

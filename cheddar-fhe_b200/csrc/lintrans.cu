@@ -184,14 +184,24 @@ Status lt_min_ks_strides(const LTPlan &pl, int *bs_stride, int *gs_stride) {
 }
 
 Status Context::lt_evaluate_min_ks(DeviceCt &res, const DeviceCt &in, const LTPlan &pl, const RotKeys &keys) {
+  DeviceCt *r = &res;
+  const DeviceCt *i = &in;
+  return lt_evaluate_min_ks_batch(1, &r, &i, pl, keys);
+}
+
+Status Context::lt_evaluate_min_ks_batch(int count, DeviceCt *const *res, const DeviceCt *const *in,
+                                         const LTPlan &pl, const RotKeys &keys) {
   // HoistHandler::EvaluateMinKSBabyStep / EvaluateMinKSGiantStep
   // (Hoist.cu:490-552): baby steps by repeated HRot with the baby stride,
   // giant steps in reverse order, accumulate, HRot by the giant stride,
-  // then Rescale.  Works in the Q basis of pt_level.
+  // then Rescale.  Works in the Q basis of pt_level.  Every rotation and the
+  // final rescale run once over the `count` ciphertexts.
   const int level = pl.pt_level;
   const int n = P->n;
-  CHD_CHECK(!in.has_rx && in.np.aux == 0, kErrShape, "Hoist: input should be relinearized and mod-down");
-  CHD_CHECK(in.np == P->level_np(level), kErrShape, "Hoist: input level mismatch");
+  for (int c = 0; c < count; c++) {
+    CHD_CHECK(!in[c]->has_rx && in[c]->np.aux == 0, kErrShape, "Hoist: input should be relinearized and mod-down");
+    CHD_CHECK(in[c]->np == P->level_np(level), kErrShape, "Hoist: input level mismatch");
+  }
   CHD_CHECK(!(pl.bs_idx.size() == 1 && pl.bs_idx[0] == 0), kErrInvalidArg,
             "Hoist: min_ks should be false for bs == 1 case");
   int bs_stride = 0, gs_stride = 0;
@@ -202,95 +212,125 @@ Status Context::lt_evaluate_min_ks(DeviceCt &res, const DeviceCt &in, const LTPl
   };
   const NP np = P->level_np(level);
   const int nq = np.q();
+  const size_t bytes = static_cast<size_t>(nq) * n * 4;
   std::vector<int> g(nq);
   P->gidx(np, g.data());
   ArenaScope scope(arena);
   // baby steps in the Q basis
-  std::vector<DeviceCt> bs(pl.bs_idx.size());
+  std::vector<std::vector<DeviceCt>> bs(count);
   std::map<int, int> slot_of;
-  for (size_t i = 0; i < pl.bs_idx.size(); i++) {
-    CHD_TRY(scratch_ct(arena, bs[i], np, false, n));
-    slot_of[pl.bs_idx[i]] = static_cast<int>(i);
+  for (size_t i = 0; i < pl.bs_idx.size(); i++) slot_of[pl.bs_idx[i]] = static_cast<int>(i);
+  for (int c = 0; c < count; c++) {
+    bs[c].resize(pl.bs_idx.size());
+    for (size_t i = 0; i < pl.bs_idx.size(); i++) CHD_TRY(scratch_ct(arena, bs[c][i], np, false, n));
   }
   const DeviceEvk *kb = key_of(bs_stride);
+  std::vector<DeviceCt *> dst(count);
+  std::vector<const DeviceCt *> src(count);
   for (size_t i = 0; i < pl.bs_idx.size(); i++) {
     const int r = pl.bs_idx[i];
     if (r == 0) {
-      const size_t bytes = static_cast<size_t>(nq) * n * 4;
-      cudaMemcpyAsync(bs[i].bx, in.bx, bytes, cudaMemcpyDeviceToDevice, stream);
-      cudaMemcpyAsync(bs[i].ax, in.ax, bytes, cudaMemcpyDeviceToDevice, stream);
-      bs[i].scale = in.scale;
-      bs[i].num_slots = in.num_slots;
+      for (int c = 0; c < count; c++) {
+        cudaMemcpyAsync(bs[c][i].bx, in[c]->bx, bytes, cudaMemcpyDeviceToDevice, stream);
+        cudaMemcpyAsync(bs[c][i].ax, in[c]->ax, bytes, cudaMemcpyDeviceToDevice, stream);
+        bs[c][i].scale = in[c]->scale;
+        bs[c][i].num_slots = in[c]->num_slots;
+      }
     } else {
       CHD_CHECK(kb, kErrKey, "Hoist: missing rotation key " + std::to_string(bs_stride));
       auto it = slot_of.find(r - bs_stride);
       CHD_CHECK(it != slot_of.end(), kErrInvalidArg, "Hoist: MinKS baby-step sequence is not complete");
-      CHD_TRY(hrot(bs[i], bs[it->second], *kb, bs_stride));
+      for (int c = 0; c < count; c++) {
+        dst[c] = &bs[c][i];
+        src[c] = &bs[c][it->second];
+      }
+      CHD_TRY(hrot_batch(count, dst.data(), src.data(), *kb, bs_stride));
     }
   }
   // giant steps, reversed
-  DeviceCt acc, tmp;
-  CHD_TRY(scratch_ct(arena, acc, np, false, n));
-  CHD_TRY(scratch_ct(arena, tmp, np, false, n));
+  std::vector<DeviceCt> acc(count), tmp(count);
+  for (int c = 0; c < count; c++) {
+    CHD_TRY(scratch_ct(arena, acc[c], np, false, n));
+    CHD_TRY(scratch_ct(arena, tmp[c], np, false, n));
+  }
   const DeviceEvk *kg = key_of(gs_stride);
   bool first = true;
   int prev = 0;
   for (auto git = pl.gs_idx.rbegin(); git != pl.gs_idx.rend(); ++git) {
     const int gsi = *git;
-    PtAccumDesc d{};
-    int nin = 0;
-    std::map<int, int> in_of;
-    PtAccumOut &po = d.out[0];
-    for (const auto &pt : pl.pts) {
-      if (pt.gs != gsi) continue;
-      auto f = in_of.find(pt.bs);
-      if (f == in_of.end()) {
-        CHD_CHECK(nin < kMaxPtAccumIn, kErrUnsupported, "Hoist: too many baby steps");
-        const DeviceCt &b = bs[slot_of.at(pt.bs)];
-        d.in_b[nin] = b.bx;
-        d.in_a[nin] = b.ax;
-        f = in_of.emplace(pt.bs, nin++).first;
+    CHD_CHECK(first || prev == gsi + gs_stride, kErrInvalidArg, "Hoist: MinKS giant-step sequence is not complete");
+    for (int c = 0; c < count; c++) {
+      PtAccumDesc d{};
+      int nin = 0;
+      std::map<int, int> in_of;
+      PtAccumOut &po = d.out[0];
+      for (const auto &pt : pl.pts) {
+        if (pt.gs != gsi) continue;
+        auto f = in_of.find(pt.bs);
+        if (f == in_of.end()) {
+          CHD_CHECK(nin < kMaxPtAccumIn, kErrUnsupported, "Hoist: too many baby steps");
+          const DeviceCt &b = bs[c][slot_of.at(pt.bs)];
+          d.in_b[nin] = b.bx;
+          d.in_a[nin] = b.ax;
+          f = in_of.emplace(pt.bs, nin++).first;
+        }
+        CHD_CHECK(po.terms < kMaxPtAccumTerms, kErrUnsupported, "Hoist: too many terms");
+        po.term[po.terms] = static_cast<int16_t>(f->second);
+        po.pt[po.terms] = pt.dev;  // the first nq rows are the q primes
+        po.terms++;
       }
-      CHD_CHECK(po.terms < kMaxPtAccumTerms, kErrUnsupported, "Hoist: too many terms");
-      po.term[po.terms] = static_cast<int16_t>(f->second);
-      po.pt[po.terms] = pt.dev;  // the first nq rows are the q primes
-      po.terms++;
+      for (int r = 0; r < nq; r++) {
+        d.q[r] = P->primes[g[r]];
+        d.qinv[r] = P->qinv[g[r]];
+      }
+      d.rows = nq;
+      d.n = n;
+      d.outs = 1;
+      if (first) {
+        po.b = acc[c].bx;
+        po.a = acc[c].ax;
+        launch_pt_accum(d, stream);
+      } else {
+        po.b = tmp[c].bx;
+        po.a = tmp[c].ax;
+        launch_pt_accum(d, stream);
+        CHD_TRY(add(acc[c], acc[c], tmp[c]));
+      }
+      acc[c].scale = in[c]->scale * pl.pt_scale;
+      acc[c].num_slots = std::max(in[c]->num_slots, pl.pt_slots);
     }
-    for (int r = 0; r < nq; r++) {
-      d.q[r] = P->primes[g[r]];
-      d.qinv[r] = P->qinv[g[r]];
-    }
-    d.rows = nq;
-    d.n = n;
-    d.outs = 1;
-    if (first) {
-      po.b = acc.bx;
-      po.a = acc.ax;
-      launch_pt_accum(d, stream);
-    } else {
-      CHD_CHECK(prev == gsi + gs_stride, kErrInvalidArg, "Hoist: MinKS giant-step sequence is not complete");
-      po.b = tmp.bx;
-      po.a = tmp.ax;
-      launch_pt_accum(d, stream);
-      CHD_TRY(add(acc, acc, tmp));
-    }
-    acc.scale = in.scale * pl.pt_scale;
-    acc.num_slots = std::max(in.num_slots, pl.pt_slots);
     if (gsi != 0) {
       CHD_CHECK(kg, kErrKey, "Hoist: missing rotation key " + std::to_string(gs_stride));
-      CHD_TRY(hrot(tmp, acc, *kg, gs_stride));
-      const size_t bytes = static_cast<size_t>(nq) * n * 4;
-      cudaMemcpyAsync(acc.bx, tmp.bx, bytes, cudaMemcpyDeviceToDevice, stream);
-      cudaMemcpyAsync(acc.ax, tmp.ax, bytes, cudaMemcpyDeviceToDevice, stream);
+      for (int c = 0; c < count; c++) {
+        dst[c] = &tmp[c];
+        src[c] = &acc[c];
+      }
+      CHD_TRY(hrot_batch(count, dst.data(), src.data(), *kg, gs_stride));
+      for (int c = 0; c < count; c++) {
+        cudaMemcpyAsync(acc[c].bx, tmp[c].bx, bytes, cudaMemcpyDeviceToDevice, stream);
+        cudaMemcpyAsync(acc[c].ax, tmp[c].ax, bytes, cudaMemcpyDeviceToDevice, stream);
+      }
     } else {
       CHD_CHECK(first || prev == gs_stride, kErrInvalidArg, "Hoist: MinKS giant-step sequence is not complete");
     }
     first = false;
     prev = gsi;
   }
-  const double sc = acc.scale;
-  CHD_TRY(rescale(res, acc));
-  res.scale = sc / P->rescale_prod[level];
+  // final Rescale of every accumulator in one ModDown launch sequence
+  std::vector<const uint32_t *> rsrc(2 * count);
+  std::vector<uint32_t *> rdst(2 * count);
+  for (int c = 0; c < count; c++) {
+    CHD_TRY(res[c]->reserve(P->level_np(level - 1, 0), false, n));
+    rsrc[2 * c] = acc[c].bx;
+    rsrc[2 * c + 1] = acc[c].ax;
+    rdst[2 * c] = res[c]->bx;
+    rdst[2 * c + 1] = res[c]->ax;
+  }
+  CHD_TRY(moddown(level, MDType::kRescale, rsrc.data(), rdst.data(), 2 * count));
+  for (int c = 0; c < count; c++) {
+    res[c]->scale = acc[c].scale / P->rescale_prod[level];
+    res[c]->num_slots = acc[c].num_slots;
+  }
   return check_cuda("linear transform (min-KS)");
 }
 

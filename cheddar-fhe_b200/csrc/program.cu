@@ -266,7 +266,7 @@ Status Context::run_program_batch(const Program &prog, int count, std::vector<De
         break;
       }
       case OpKind::kLinTrans: {
-        if (count == 1 || keys.min_ks) {
+        if (count == 1) {
           batched = false;
           break;
         }
@@ -278,7 +278,10 @@ Status Context::run_program_batch(const Program &prog, int count, std::vector<De
           out[c] = &R[c]->at(prog.nregs);
           in[c] = &R[c]->at(op.a);
         }
-        CHD_TRY(lt_evaluate_batch(count, out.data(), in.data(), *(*lts)[op.rot], *rot_keys));
+        if (keys.min_ks)
+          CHD_TRY(lt_evaluate_min_ks_batch(count, out.data(), in.data(), *(*lts)[op.rot], *rot_keys));
+        else
+          CHD_TRY(lt_evaluate_batch(count, out.data(), in.data(), *(*lts)[op.rot], *rot_keys));
         break;
       }
       default:
