@@ -5,9 +5,10 @@
 //    (kernel::ModUpToMax1 / ModUpToMax2, src/core/ElementWise.cu:575-623):
 //    two base primes are combined by CRT into the centred representative
 //    of (-q0 q1 / 2, q0 q1 / 2]; one base prime is lifted as is.
-//  * k_pt_accum: sum_i pt_i (.) ct_i over limbs for several outputs at once
-//    (the giant-step plaintext accumulation of HoistHandler::GSFusedPAccum,
-//    src/extension/Hoist.cu:329-420, and ElementWiseHandler::PAccum).
+//  * k_pt_accum: sum_i pt_i (.) ct_i over limbs for several outputs and
+//    several ciphertexts at once (the giant-step plaintext accumulation of
+//    HoistHandler::GSFusedPAccum, src/extension/Hoist.cu:329-420, and
+//    ElementWiseHandler::PAccum).
 //  * k_const_accum: sum_i c_i * ct_i with one constant per limb and term
 //    (ElementWiseHandler::CAccum, src/core/ElementWise.cu:1355-1643).
 #include "arith.cuh"
@@ -40,29 +41,32 @@ __global__ void k_modup_to_max(const __grid_constant__ ModUpToMaxDesc d) {
   }
 }
 
-// out[o][r] = sum_t pt[o][t][r] (.) in[t][r]  (Montgomery products, canonical)
-// One thread owns one coefficient of one row for every output, so the
-// baby-step values it reads for the first giant step are L1 hits for the
-// others.
+// out[c][o][r] = sum_t pt[o][t][r] (.) in[c][t][r]  (Montgomery products,
+// canonical).  Block x = ciphertext + count * column block: the blocks of the
+// ciphertexts of one batch that read the same plaintext tile are neighbours
+// in launch order, so the plaintexts come from HBM once per batch.  One
+// thread owns one coefficient of one row for every output, so the baby-step
+// values it reads for the first giant step are L1 hits for the others.
 __global__ void k_pt_accum(const __grid_constant__ PtAccumDesc d) {
   const int r = blockIdx.y;
+  const int c = blockIdx.x % d.count, xb = blockIdx.x / d.count, nxb = gridDim.x / d.count;
   const uint32_t q = d.q[r];
   const int32_t qi = d.qinv[r];
   const size_t n = static_cast<size_t>(d.n);
   const size_t off = static_cast<size_t>(r) * n;
-  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
-       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+  for (size_t i = xb * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(nxb) * blockDim.x) {
     for (int o = 0; o < d.outs; o++) {
       const PtAccumOut &out = d.out[o];
       uint32_t sb = 0, sa = 0;
       for (int t = 0; t < out.terms; t++) {
         const int ti = out.term[t];
         const uint32_t m = out.pt[t][off + i];
-        sb = add_mod(sb, mont_mul(d.in_b[ti][off + i], m, q, qi), q);
-        sa = add_mod(sa, mont_mul(d.in_a[ti][off + i], m, q, qi), q);
+        sb = add_mod(sb, mont_mul(d.in_b[c][ti][off + i], m, q, qi), q);
+        sa = add_mod(sa, mont_mul(d.in_a[c][ti][off + i], m, q, qi), q);
       }
-      out.b[off + i] = sb;
-      out.a[off + i] = sa;
+      d.out_b[c][o][off + i] = sb;
+      d.out_a[c][o][off + i] = sa;
     }
   }
 }
@@ -93,8 +97,8 @@ void launch_modup_to_max(const ModUpToMaxDesc &d, cudaStream_t s) {
 }
 
 void launch_pt_accum(const PtAccumDesc &d, cudaStream_t s) {
-  if (d.rows <= 0 || d.outs <= 0) return;
-  k_pt_accum<<<dim3(64, d.rows), 256, 0, s>>>(d);
+  if (d.rows <= 0 || d.outs <= 0 || d.count <= 0 || d.count > kMaxPtAccumCts) return;
+  k_pt_accum<<<dim3(64 * d.count, d.rows), 256, 0, s>>>(d);
 }
 
 void launch_const_accum(const ConstAccumDesc &d, cudaStream_t s) {

@@ -1976,11 +1976,24 @@ Status Context::moddown_ct(DeviceCt &res, const DeviceCt &a) {
 
 Status Context::hoisted_rotate(const DeviceCt &a, int R, const int *dists, const DeviceEvk *const *keys,
                                DeviceCt *const *out) {
-  // Hoist.cu:578-691 with the fused BS kernel of Hoist.cu:21-78: one ModUp,
-  // then every rotation in one launch, results left in Q u P
-  CHD_CHECK(!a.has_rx && a.np.aux == 0, kErrShape, "hoisted rotate: input must be relinearised");
-  const int level = level_of(*P, a);
+  const DeviceCt *ap = &a;
+  DeviceCt *const *op = out;
+  return hoisted_rotate_batch(1, &ap, R, dists, keys, &op);
+}
+
+Status Context::hoisted_rotate_batch(int count, const DeviceCt *const *a, int R, const int *dists,
+                                     const DeviceEvk *const *keys, DeviceCt *const *const *out) {
+  // Hoist.cu:578-691 with the fused BS kernel of Hoist.cu:21-78: one ModUp
+  // per ciphertext (all of them in one batched ModUp), then every rotation
+  // of every ciphertext in one launch per kMaxHoistCts ciphertexts, results
+  // left in Q u P
+  CHD_CHECK(count >= 1, kErrInvalidArg, "hoisted rotate: empty batch");
+  const DeviceCt &a0 = *a[0];
+  CHD_CHECK(!a0.has_rx && a0.np.aux == 0, kErrShape, "hoisted rotate: input must be relinearised");
+  const int level = level_of(*P, a0);
   CHD_CHECK(level >= 0, kErrInvalidLevel, "hoisted rotate: invalid level");
+  for (int c = 0; c < count; c++)
+    CHD_CHECK(a[c]->np == a0.np && !a[c]->has_rx, kErrShape, "hoisted rotate: batch members at different levels");
   const LevelMS &m = lms(level);
   const int n = P->n;
   NP np = P->level_np(level, P->alpha);
@@ -1988,76 +2001,93 @@ Status Context::hoisted_rotate(const DeviceCt &a, int R, const int *dists, const
   CHD_CHECK(tot <= 64 && m.beta <= 8, kErrUnsupported, "hoisted rotate: too many primes");
   const int prime_offset = P->max_ter - np.ter;
   ArenaScope scope(arena);
-  std::vector<uint32_t *> mu(m.beta, nullptr);
-  for (int i = 0; i < m.beta; i++) {
-    mu[i] = static_cast<uint32_t *>(arena.alloc(static_cast<size_t>(tot) * n * 4));
-    CHD_CHECK(mu[i], kErrAlloc, "hoisted rotate: scratch allocation failed");
+  std::vector<std::vector<uint32_t *>> mu(count, std::vector<uint32_t *>(m.beta, nullptr));
+  std::vector<uint32_t *const *> mu_p(count);
+  std::vector<uint32_t *> bxp(count);
+  std::vector<const uint32_t *> src(count);
+  for (int c = 0; c < count; c++) {
+    for (int i = 0; i < m.beta; i++) {
+      mu[c][i] = static_cast<uint32_t *>(arena.alloc(static_cast<size_t>(tot) * n * 4));
+      CHD_CHECK(mu[c][i], kErrAlloc, "hoisted rotate: scratch allocation failed");
+    }
+    mu_p[c] = mu[c].data();
+    bxp[c] = static_cast<uint32_t *>(arena.alloc(static_cast<size_t>(nq) * n * 4));
+    CHD_CHECK(bxp[c], kErrAlloc, "hoisted rotate: scratch allocation failed");
+    src[c] = a[c]->ax;
   }
-  uint32_t *bxp = static_cast<uint32_t *>(arena.alloc(static_cast<size_t>(nq) * n * 4));
-  CHD_CHECK(bxp, kErrAlloc, "hoisted rotate: scratch allocation failed");
-  CHD_TRY(modup(level, a.ax, mu.data()));
+  CHD_TRY(modup_many(level, count, src.data(), mu_p.data()));
   std::vector<int> g(tot);
   P->gidx(np, g.data());
   {
     ElemBatch eb{};
-    for (int r = 0; r < nq; r++) {
-      if (eb.count == kMaxElemRows) {
-        launch_elementwise(ElemOp::kMultConst, eb, P->log_n, stream);
-        eb.count = 0;
+    for (int c = 0; c < count; c++)
+      for (int r = 0; r < nq; r++) {
+        if (eb.count == kMaxElemRows) {
+          launch_elementwise(ElemOp::kMultConst, eb, P->log_n, stream);
+          eb.count = 0;
+        }
+        ElemRow &e = eb.rows[eb.count++];
+        e.a = a[c]->bx + static_cast<size_t>(r) * n;
+        e.dst = bxp[c] + static_cast<size_t>(r) * n;
+        e.q = P->primes[g[r]];
+        e.qinv = P->qinv[g[r]];
+        e.k = p_prod[prime_offset + r];
       }
-      ElemRow &e = eb.rows[eb.count++];
-      e.a = a.bx + static_cast<size_t>(r) * n;
-      e.dst = bxp + static_cast<size_t>(r) * n;
-      e.q = P->primes[g[r]];
-      e.qinv = P->qinv[g[r]];
-      e.k = p_prod[prime_offset + r];
-    }
     launch_elementwise(ElemOp::kMultConst, eb, P->log_n, stream);
   }
+  const int slots = a0.num_slots > 0 ? a0.num_slots : n / 2;
+  std::vector<int> dd(R);
   for (int j = 0; j < R; j++) {
-    int slots = a.num_slots > 0 ? a.num_slots : n / 2;
-    int dd = dists[j] % slots;
-    if (dd < 0) dd += slots;
-    CHD_CHECK(dd > 0 && dd < n / 2, kErrInvalidArg, "hoisted rotate: invalid rotation");
-    CHD_TRY(out[j]->reserve(np, false, n));
-    out[j]->scale = a.scale;
-    out[j]->num_slots = a.num_slots;
+    dd[j] = dists[j] % slots;
+    if (dd[j] < 0) dd[j] += slots;
+    CHD_CHECK(dd[j] > 0 && dd[j] < n / 2, kErrInvalidArg, "hoisted rotate: invalid rotation");
+    for (int c = 0; c < count; c++) {
+      DeviceCt *o = out[c][j];
+      CHD_TRY(o->reserve(np, false, n));
+      o->scale = a[c]->scale;
+      o->num_slots = a[c]->num_slots;
+    }
   }
   const size_t kstride = static_cast<size_t>(P->L + P->alpha) * n;
   for (int j0 = 0; j0 < R; j0 += kMaxHoist) {
-    HoistDesc d{};
-    int nb = 0;
-    for (int i = 0; i < m.beta; i++)
-      if (m.dig_e[i] > 0) d.mu[nb++] = mu[i];
-    d.beta = nb;
-    d.bxp = bxp;
-    d.rows = tot;
-    d.nq = nq;
-    d.R = std::min(kMaxHoist, R - j0);
-    for (int r = 0; r < tot; r++) {
-      d.q[r] = P->primes[g[r]];
-      d.qinv[r] = P->qinv[g[r]];
-      d.key_row[r] = static_cast<int16_t>(r < nq ? prime_offset + r : P->L + (r - nq));
-    }
-    for (int j = 0; j < d.R; j++) {
-      const DeviceEvk &k = *keys[j0 + j];
-      CHD_CHECK(k.np.aux == P->alpha && k.np.q() == P->L, kErrKey, "hoisted rotate: key basis mismatch");
-      int slots = a.num_slots > 0 ? a.num_slots : n / 2;
-      int dd = dists[j0 + j] % slots;
-      if (dd < 0) dd += slots;
-      int b = 0;
+    for (int c0 = 0; c0 < count; c0 += kMaxHoistCts) {
+      HoistDesc d{};
+      d.count = std::min(kMaxHoistCts, count - c0);
+      int nb = 0;
       for (int i = 0; i < m.beta; i++) {
         if (m.dig_e[i] <= 0) continue;
-        CHD_CHECK(i < k.beta, kErrKey, "hoisted rotate: key has too few digits");
-        d.kb[j][b] = k.bx + i * kstride;
-        d.ka[j][b] = k.ax + i * kstride;
-        b++;
+        for (int c = 0; c < d.count; c++) d.mu[c][nb] = mu[c0 + c][i];
+        nb++;
       }
-      d.out_b[j] = out[j0 + j]->bx;
-      d.out_a[j] = out[j0 + j]->ax;
-      d.galois_inv[j] = P->galois_of(n / 2 - dd);
+      for (int c = 0; c < d.count; c++) d.bxp[c] = bxp[c0 + c];
+      d.beta = nb;
+      d.rows = tot;
+      d.nq = nq;
+      d.R = std::min(kMaxHoist, R - j0);
+      for (int r = 0; r < tot; r++) {
+        d.q[r] = P->primes[g[r]];
+        d.qinv[r] = P->qinv[g[r]];
+        d.key_row[r] = static_cast<int16_t>(r < nq ? prime_offset + r : P->L + (r - nq));
+      }
+      for (int j = 0; j < d.R; j++) {
+        const DeviceEvk &k = *keys[j0 + j];
+        CHD_CHECK(k.np.aux == P->alpha && k.np.q() == P->L, kErrKey, "hoisted rotate: key basis mismatch");
+        int b = 0;
+        for (int i = 0; i < m.beta; i++) {
+          if (m.dig_e[i] <= 0) continue;
+          CHD_CHECK(i < k.beta, kErrKey, "hoisted rotate: key has too few digits");
+          d.kb[j][b] = k.bx + i * kstride;
+          d.ka[j][b] = k.ax + i * kstride;
+          b++;
+        }
+        for (int c = 0; c < d.count; c++) {
+          d.out_b[c][j] = out[c0 + c][j0 + j]->bx;
+          d.out_a[c][j] = out[c0 + c][j0 + j]->ax;
+        }
+        d.galois_inv[j] = P->galois_of(n / 2 - dd[j0 + j]);
+      }
+      launch_hoisted(d, P->log_n, stream);
     }
-    launch_hoisted(d, P->log_n, stream);
   }
   return check_cuda("hoisted rotate");
 }

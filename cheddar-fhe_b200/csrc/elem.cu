@@ -195,10 +195,14 @@ __global__ void __launch_bounds__(256) k_permute(const __grid_constant__ Permute
 // Hoisted rotations (one launch for all R rotations).  Each thread loads the
 // beta ModUp values of its coefficient once, then for every rotation forms
 // the key inner products and scatters them through the inverse automorphism.
+// grid (count, N / 256, rows): the ciphertexts of a batch that read the
+// same key tile are neighbours in launch order, so the keys come from HBM
+// once per batch
 __global__ void __launch_bounds__(256) k_hoisted(const __grid_constant__ HoistDesc d, int log_n) {
   const int n = 1 << log_n;
-  const int r = blockIdx.y;
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = blockIdx.x;
+  const int r = blockIdx.z;
+  const int k = blockIdx.y * blockDim.x + threadIdx.x;
   if (k >= n) return;
   const uint32_t q = d.q[r];
   const int32_t qi = d.qinv[r];
@@ -207,8 +211,8 @@ __global__ void __launch_bounds__(256) k_hoisted(const __grid_constant__ HoistDe
   uint32_t mu[8];
 #pragma unroll
   for (int i = 0; i < 8; i++)
-    if (i < d.beta) mu[i] = __ldg(d.mu[i] + off);
-  const uint32_t bxp = (r < d.nq) ? __ldg(d.bxp + off) : 0u;
+    if (i < d.beta) mu[i] = __ldg(d.mu[c][i] + off);
+  const uint32_t bxp = (r < d.nq) ? __ldg(d.bxp[c] + off) : 0u;
   for (int j = 0; j < d.R; j++) {
     uint32_t sb = bxp, sa = 0;
 #pragma unroll
@@ -222,8 +226,8 @@ __global__ void __launch_bounds__(256) k_hoisted(const __grid_constant__ HoistDe
     }
     const uint32_t dk = galois_src(k, d.galois_inv[j], log_n);
     const size_t o = static_cast<size_t>(r) * n + dk;
-    d.out_b[j][o] = sb;
-    d.out_a[j][o] = sa;
+    d.out_b[c][j][o] = sb;
+    d.out_a[c][j][o] = sa;
   }
 }
 
@@ -292,7 +296,8 @@ void launch_permute(const PermuteBatch &b, int log_n, cudaStream_t s) {
 void launch_hoisted(const HoistDesc &d, int log_n, cudaStream_t s) {
   if (d.rows <= 0 || d.R <= 0) return;
   const int n = 1 << log_n;
-  k_hoisted<<<dim3((n + 255) / 256, d.rows), 256, 0, s>>>(d, log_n);
+  if (d.count <= 0 || d.count > kMaxHoistCts) return;
+  k_hoisted<<<dim3(d.count, (n + 255) / 256, d.rows), 256, 0, s>>>(d, log_n);
 }
 
 }  // namespace chd

@@ -401,6 +401,11 @@ class Context {
   // hoisted baby-step rotations, outputs stay in the Q u P basis
   Status hoisted_rotate(const DeviceCt &a, int R, const int *dists, const DeviceEvk *const *keys,
                         DeviceCt *const *out);
+  // the same rotations of `count` ciphertexts at one level: one batched
+  // ModUp, keys read once per launch for up to kMaxHoistCts ciphertexts;
+  // out[c][j] is rotation j of ciphertext c
+  Status hoisted_rotate_batch(int count, const DeviceCt *const *a, int R, const int *dists,
+                              const DeviceEvk *const *keys, DeviceCt *const *const *out);
   // ModDown of a Q u P ciphertext back to Q
   Status moddown_ct(DeviceCt &res, const DeviceCt &a);
 

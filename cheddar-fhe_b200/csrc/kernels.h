@@ -113,16 +113,20 @@ constexpr int kMaxPtAccumIn = 64;
 constexpr int kMaxPtAccumTerms = 32;
 constexpr int kMaxPtAccumOuts = 16;
 struct PtAccumOut {
-  uint32_t *b, *a;
   int terms;
   int16_t term[kMaxPtAccumTerms];
   const uint32_t *pt[kMaxPtAccumTerms];
 };
+// Up to kMaxPtAccumCts ciphertexts sharing the plaintexts: ciphertext c
+// reads in_b[c][i] / in_a[c][i] and writes out_b[c][o] / out_a[c][o]; the
+// terms of output o (baby-step index, plaintext) are shared.
+constexpr int kMaxPtAccumCts = 8;
 struct PtAccumDesc {
-  const uint32_t *in_b[kMaxPtAccumIn], *in_a[kMaxPtAccumIn];
+  const uint32_t *in_b[kMaxPtAccumCts][kMaxPtAccumIn], *in_a[kMaxPtAccumCts][kMaxPtAccumIn];
+  uint32_t *out_b[kMaxPtAccumCts][kMaxPtAccumOuts], *out_a[kMaxPtAccumCts][kMaxPtAccumOuts];
   uint32_t q[64];
   int32_t qinv[64];
-  int rows, outs, n;
+  int rows, outs, n, count;
   PtAccumOut out[kMaxPtAccumOuts];
 };
 void launch_pt_accum(const PtAccumDesc &d, cudaStream_t s);
@@ -273,18 +277,19 @@ void launch_permute(const PermuteBatch &b, int log_n, cudaStream_t s);
 // scattered through the automorphism: out_j[galois_src(k, g_j)] = v[k] with
 // g_j the Galois factor of N/2 - r_j (the inverse of rotation r_j).
 constexpr int kMaxHoist = 32;
+constexpr int kMaxHoistCts = 8;  // ciphertexts sharing the keys of one launch
 struct HoistDesc {
-  const uint32_t *mu[8];
-  const uint32_t *bxp;                   // P * bx on q rows, [nq][N]
+  const uint32_t *mu[kMaxHoistCts][8];
+  const uint32_t *bxp[kMaxHoistCts];     // P * bx on q rows, [nq][N]
   const uint32_t *kb[kMaxHoist][8];      // key row-0 pointers per rotation/digit
   const uint32_t *ka[kMaxHoist][8];
-  uint32_t *out_b[kMaxHoist];            // outputs [rows][N]
-  uint32_t *out_a[kMaxHoist];
+  uint32_t *out_b[kMaxHoistCts][kMaxHoist];  // outputs [rows][N]
+  uint32_t *out_a[kMaxHoistCts][kMaxHoist];
   uint32_t galois_inv[kMaxHoist];
   uint32_t q[64];
   int32_t qinv[64];
   int16_t key_row[64];
-  int beta, rows, nq, R;
+  int beta, rows, nq, R, count;
 };
 void launch_hoisted(const HoistDesc &d, int log_n, cudaStream_t s);
 
