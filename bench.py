@@ -19,8 +19,8 @@ Reported (one JSON line on rank 0):
   bootstrap  full-slot bootstrapping throughput at N = 2^16 (bootstraps/s;
              --boot-precision adds a real-key run with decoded precision)
   ks_engines  the same step with the ModUp / ModDown column passes on each
-             engine (--ks-engine picks the measured one; default cuda, the
-             faster one on this workload)
+             engine (--ks-engine picks the measured one; default tensor,
+             1-2 % ahead of the CUDA-core engine on both workloads)
   bconv_engines  base conversion on CUDA cores vs tcgen05 tensor cores
 `--impl reference` times the CPU implementation of the path (the oracle;
 the reference itself has no CPU path and cannot be built here) on the same
@@ -159,7 +159,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-boot", action="store_true", help="skip the bootstrapping measurement")
     ap.add_argument("--boot-batch", type=int, default=8)
-    ap.add_argument("--ks-engine", default="cuda", choices=["cuda", "tensor"],
+    ap.add_argument("--boot-profile", action="store_true",
+                    help="profiling aid: set up the bootstrapping workload, run two BootBatch calls of "
+                         "--boot-batch ciphertexts (the second is the one to read in a launch list) and exit")
+    ap.add_argument("--ks-engine", default="tensor", choices=["cuda", "tensor"],
                     help="base conversion inside the ModUp / ModDown column passes of the measured path")
     ap.add_argument("--boot-precision", action="store_true",
                     help="also bootstrap one ciphertext with real keys (oracle key generation, slow) "
@@ -182,6 +185,10 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
 
+    if args.boot_profile:
+        stream = torch.cuda.Stream()
+        boot_bench(chd, args, stream, None, profile=True)
+        return
     params = json.load(open(os.path.join(chd.PARAM_DIR, PARAM_FILE)))
     ctx = chd.Context(json.dumps(params), device=local)
     stream = torch.cuda.Stream()
@@ -610,7 +617,7 @@ def hoist_mixed_bench(ctx, chd, key, uniform, stream, reps=5):
 BOOT_PARAM_FILE = "boot_l34_a12.json"
 
 
-def boot_bench(chd, args, stream, dist):
+def boot_bench(chd, args, stream, dist, profile=False):
     """Full-slot bootstrapping (N = 2^16, 2^15 slots; 48 q primes with the
     reference's bootparam_30 level shape, alpha = 12, 4 CoeffToSlot and 3
     SlotToCoeff levels, EvalMod with the reference's cosine polynomial and 3
@@ -670,6 +677,13 @@ def boot_bench(chd, args, stream, dist):
     def step():
         # one batched call: every key switch / linear transform over all B
         bc.BootBatch(ins, keys, res_list=outs)
+
+    if profile:
+        step()
+        step()
+        ctx.synchronize()
+        print(json.dumps({"boot_profile": "2 BootBatch calls", "batch": B}))
+        return None
 
     for _ in range(2):
         step()
