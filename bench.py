@@ -42,9 +42,7 @@ METRIC = "HMult+relin+rescale/s (keyswitch/s) at N=2^16, L=24, alpha=8, dnum=3"
 UNIT = "HMult/s"
 
 
-def env_rank():
-    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(
-        os.environ.get("LOCAL_RANK", "0"))
+from replicas import barrier, env_rank, finish, init_group, job_throughput, max_over_ranks, rank_seed  # noqa: E402
 
 
 class ClockSampler:
@@ -179,11 +177,7 @@ def main():
 
     rank, world, local = env_rank()
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    dist = init_group(world, "nccl")
 
     if args.boot_profile:
         stream = torch.cuda.Stream()
@@ -199,7 +193,7 @@ def main():
     n = ctx.n
     beta = -(-ctx.L // ctx.alpha)
     primes = torch.tensor(chd_primes(ctx), dtype=torch.int64, device="cuda")
-    gen = torch.Generator(device="cuda").manual_seed(1234 + rank)
+    gen = torch.Generator(device="cuda").manual_seed(rank_seed(1234, rank))
 
     def uniform(rows, gidx):
         q = primes[gidx][:, None]
@@ -228,7 +222,7 @@ def main():
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     sampler = ClockSampler(torch.cuda.current_device())
     if dist:
-        dist.barrier()
+        barrier(dist)
     torch.cuda.synchronize()
     with sampler:
         ev0.record(stream)
@@ -236,13 +230,9 @@ def main():
             step()
         ev1.record(stream)
         torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(dist, ev0.elapsed_time(ev1), "cuda")
     ms_step = ms / args.steps
-    value = world * B * args.steps / (ms / 1e3)
+    value = job_throughput(world, B, args.steps, ms)
 
     # ---- end to end through the C ABI with host buffers ----
     e2e = e2e_run(ctx, chd, key, lvl, nq, n, B, args, stream, dist)
@@ -294,9 +284,7 @@ def main():
         print(json.dumps(line))
     del outs, a_cts, b_cts, key
     ctx.close()
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    finish(dist)
     return 0
 
 
@@ -334,21 +322,16 @@ def e2e_run(ctx, chd, key, lvl, nq, n, B, args, stream, dist):
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if dist:
-        dist.barrier()
+        barrier(dist)
     ev0.record(stream)
     steps = max(3, args.steps // 2)
     for _ in range(steps):
         step()
     ev1.record(stream)
     torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
-    world = 1
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        world = dist.get_world_size()
-    return {"value": world * B * steps / (ms / 1e3), "unit": UNIT,
+    ms = max_over_ranks(dist, ev0.elapsed_time(ev1), "cuda")
+    world = dist.get_world_size() if dist else 1
+    return {"value": job_throughput(world, B, steps, ms), "unit": UNIT,
             "h2d_bytes_per_step": B * 4 * words * 4,
             "d2h_bytes_per_step": B * 2 * ctx.num_q(lvl - 1) * n * 4}
 
@@ -700,8 +683,7 @@ def boot_bench(chd, args, stream, dist, profile=False):
     torch.cuda.synchronize()
     ms_single = es0.elapsed_time(es1)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    if dist:
-        dist.barrier()
+    barrier(dist)
     torch.cuda.synchronize()
     e0.record(stream)
     for _ in range(steps):
@@ -709,13 +691,8 @@ def boot_bench(chd, args, stream, dist, profile=False):
     e1.record(stream)
     ctx.synchronize()
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    world = 1
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        world = dist.get_world_size()
+    ms = max_over_ranks(dist, e0.elapsed_time(e1), "cuda")
+    world = dist.get_world_size() if dist else 1
     # graph-captured batch (the configuration's form): the B bootstraps of a
     # step captured once as a CUDA graph and replayed
     ctx.graph_begin()
@@ -730,11 +707,7 @@ def boot_bench(chd, args, stream, dist, profile=False):
     eg1.record(stream)
     ctx.synchronize()
     torch.cuda.synchronize()
-    ms_graph = eg0.elapsed_time(eg1)
-    if dist:
-        t = torch.tensor([ms_graph], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_graph = float(t.item())
+    ms_graph = max_over_ranks(dist, eg0.elapsed_time(eg1), "cuda")
     del graph
     # the min-KS form (two rotation keys per transform, Boot(..., min_ks=true))
     bc.BootBatch(ins, keys, res_list=outs, min_ks=True)
@@ -766,7 +739,7 @@ def boot_bench(chd, args, stream, dist, profile=False):
     engines["speedup_tensor_vs_cuda_core"] = (engines["tensor_core"]["bootstraps_per_s"] /
                                               engines["cuda_core"]["bootstraps_per_s"])
     res = {"metric": "bootstraps/s (full slots, N=2^16, batched call, graph-captured)",
-           "value": world * B * steps / (ms_graph / 1e3),
+           "value": job_throughput(world, B, steps, ms_graph),
            "eager": {"bootstraps_per_s": world * B * steps / (ms / 1e3), "ms_per_boot": ms / (B * steps)},
            "one_by_one_eager": {"bootstraps_per_s": world * B * steps / (ms_single / 1e3),
                                 "ms_per_boot": ms_single / (B * steps)},
