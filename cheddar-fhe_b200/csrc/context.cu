@@ -924,9 +924,10 @@ Status Context::bconv_many(int engine, int npoly, const int32_t *xt, int K, cons
   d.npoly = npoly;
   d.ksteps = (4 * K + 31) / 32;
   d.nb = std::max(16, (4 * M + 15) / 16 * 16);
-  // tiles per iteration: 4 while the two accumulator buffers leave room for
-  // two CTAs per SM in TMEM
-  d.tpi = 8 * d.nb <= 256 ? 4 : (4 * d.nb <= 256 ? 2 : 1);
+  // tiles per iteration: as many (up to 4) as keep the two accumulator
+  // buffers within 128 TMEM columns, so that four CTAs share an SM (the
+  // kernel is bound by the HBM loads in flight, not by the MMAs)
+  d.tpi = 2 * 4 * d.nb <= 128 ? 4 : (2 * 2 * d.nb <= 128 ? 2 : 1);
   while ((P->n / 128) % d.tpi != 0) d.tpi /= 2;
   d.tmem_cols = 32;
   while (d.tmem_cols < 2 * d.tpi * d.nb) d.tmem_cols *= 2;
