@@ -22,6 +22,7 @@ Reported (one JSON line on rank 0):
              engine (--ks-engine picks the measured one; default tensor,
              1-2 % ahead of the CUDA-core engine on both workloads)
   bconv_engines  base conversion on CUDA cores vs tcgen05 tensor cores
+  ntt        forward + inverse NTT round trip, 24 primes, HBM fraction
 `--impl reference` times the CPU implementation of the path (the oracle;
 the reference itself has no CPU path and cannot be built here) on the same
 configuration.
@@ -252,6 +253,9 @@ def main():
     # ---- base conversion as a dense contraction: CUDA cores vs tensor cores ----
     bconv_cmp = bconv_engines(ctx, chd, stream)
 
+    # ---- NTT round trip (forward + inverse), 24 primes ----
+    ntt_cmp = ntt_bench(ctx, chd, stream)
+
     # ---- hoisted rotations and a mixed-level batch ----
     hoist_mixed = hoist_mixed_bench(ctx, chd, key, uniform, stream)
 
@@ -267,7 +271,7 @@ def main():
                    "l2": "inputs larger than L2 (batch x 24 MB + 48 MB key)",
                    "parallelism": f"replicas x{world}"},
         "e2e": e2e, "roofline": roof, "clocks": sampler.summary(), "ks_engine": args.ks_engine,
-        "ks_engines": ks_cmp, "bconv_engines": bconv_cmp,
+        "ks_engines": ks_cmp, "bconv_engines": bconv_cmp, "ntt": ntt_cmp,
         "bootstrap": boot, "hoisted_and_mixed": hoist_mixed,
         "gpu_launches": launches,
     }
@@ -476,6 +480,55 @@ def ks_engines(ctx, chd, step, stream, steps, B):
     out["column_pass_speedup"] = ((out["cuda_core"]["modup_cols_ms"] + out["cuda_core"]["moddown_cols_ms"]) /
                                   (out["tensor_core"]["modup_cols_ms"] + out["tensor_core"]["moddown_cols_ms"]))
     return out
+
+
+def ntt_bench(ctx, chd, stream, count=32, reps=10):
+    """Negacyclic NTT round trip (forward, then inverse) at N = 2^16 over the
+    24 q primes of the key-switching parameter set, `count` polynomials per
+    launch pair (32 x 24 limbs = 201 MB, larger than L2).  Uniform residues
+    from a seed; the round trip must return the input unchanged.
+    Algorithmic bytes per polynomial: 2 transforms x (read + write) x 24
+    limbs x 256 KiB = 25.17 MB."""
+    import torch
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    lvl = ctx.max_level
+    m, t = ctx.level_np(lvl)
+    n = ctx.n
+    allp = torch.tensor(chd_primes(ctx), dtype=torch.int64, device="cuda")
+    g = torch.tensor(ctx.gidx(m, t, 0), dtype=torch.int64, device="cuda")
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    q = allp[g][None, :, None]
+    x = (torch.randint(0, 2 ** 62, (count, m + t, n), generator=gen, device="cuda", dtype=torch.int64) % q)
+    x = x.to(torch.int32).contiguous()
+    ref = x.clone()
+    torch.cuda.synchronize()
+
+    def trip():
+        ctx.ntt_raw(m, t, 0, x, mont=True, count=count)
+        ctx.intt_raw(m, t, 0, x, mont=True, count=count)
+
+    for _ in range(3):
+        trip()
+    ctx.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        trip()
+    e1.record(stream)
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / (reps * count)  # per polynomial round trip
+    exact = bool(torch.equal(x, ref))
+    nbytes = 2 * 2 * (m + t) * n * 4
+    return {"workload": f"NTT + INTT round trip, N=2^16, {m + t} primes, {count} polys per launch pair",
+            "round_trips_per_s": 1e3 / ms, "us_per_round_trip": 1e3 * ms,
+            "GB/s": nbytes / (ms * 1e-3) / 1e9, "hbm_frac": nbytes / (ms * 1e-3) / 1e9 / hbm,
+            "algorithmic_bytes_per_round_trip": nbytes, "round_trip_exact": exact}
 
 
 def bconv_engines(ctx, chd, stream, npoly=64, reps=10):
