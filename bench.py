@@ -249,6 +249,7 @@ def main():
 
     # ---- the same step with each column-pass engine ----
     ks_cmp = ks_engines(ctx, chd, step, stream, args.steps, B)
+    ks_cmp["plain_vs_tensor_batched"] = plain_vs_batched_hmult(ctx, chd, key, a_cts, b_cts, outs, stream, args.steps)
 
     # ---- base conversion as a dense contraction: CUDA cores vs tensor cores ----
     bconv_cmp = bconv_engines(ctx, chd, stream)
@@ -480,6 +481,49 @@ def ks_engines(ctx, chd, step, stream, steps, B):
     out["column_pass_speedup"] = ((out["cuda_core"]["modup_cols_ms"] + out["cuda_core"]["moddown_cols_ms"]) /
                                   (out["tensor_core"]["modup_cols_ms"] + out["tensor_core"]["moddown_cols_ms"]))
     return out
+
+
+def plain_vs_batched_hmult(ctx, chd, key, a_cts, b_cts, outs, stream, steps):
+    """The two forms the design targets compare, same B pairs:
+    plain = one HMult call per pair, CUDA-core column passes, eager launches;
+    tensor-core batched = one HMultBatch over all B on the tensor-core
+    engine, captured once as a CUDA graph and replayed."""
+    import torch
+    old = ctx.ks_engine
+    B = len(a_cts)
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        ctx.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        ctx.synchronize()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    ctx.ks_engine = chd.BCONV_CUDA_CORE
+
+    def plain():
+        for i in range(B):
+            ctx.HMult(a_cts[i], b_cts[i], key, rescale=True, res=outs[i])
+
+    ms_plain = timed(plain)
+    ctx.ks_engine = chd.BCONV_TENSOR_CORE
+    ctx.HMultBatch(a_cts, b_cts, key, rescale=True, res_list=outs)
+    ctx.synchronize()
+    ctx.graph_begin()
+    ctx.HMultBatch(a_cts, b_cts, key, rescale=True, res_list=outs)
+    graph = ctx.graph_end()
+    ms_tc = timed(graph.launch)
+    del graph
+    ctx.ks_engine = old
+    return {"plain_cuda_core_one_by_one": {"hmult_per_s": B / (ms_plain / 1e3), "ms_per_step": ms_plain},
+            "tensor_core_batched_graph": {"hmult_per_s": B / (ms_tc / 1e3), "ms_per_step": ms_tc},
+            "speedup": ms_plain / ms_tc}
 
 
 def ntt_bench(ctx, chd, stream, count=32, reps=10):
@@ -762,6 +806,19 @@ def boot_bench(chd, args, stream, dist, profile=False):
     ctx.synchronize()
     torch.cuda.synchronize()
     ms_single = es0.elapsed_time(es1)
+    # the plain form: one ciphertext per call on the CUDA-core engine
+    main_engine = ctx.ks_engine
+    ctx.ks_engine = chd.BCONV_CUDA_CORE
+    step_single()
+    ctx.synchronize()
+    es0.record(stream)
+    for _ in range(steps):
+        step_single()
+    es1.record(stream)
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    ms_plain = es0.elapsed_time(es1)
+    ctx.ks_engine = main_engine
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier(dist)
     torch.cuda.synchronize()
@@ -823,6 +880,10 @@ def boot_bench(chd, args, stream, dist, profile=False):
            "eager": {"bootstraps_per_s": world * B * steps / (ms / 1e3), "ms_per_boot": ms / (B * steps)},
            "one_by_one_eager": {"bootstraps_per_s": world * B * steps / (ms_single / 1e3),
                                 "ms_per_boot": ms_single / (B * steps)},
+           "plain_vs_tensor_batched": {
+               "plain_cuda_core_one_by_one_ms_per_boot": ms_plain / (B * steps),
+               "tensor_core_batched_graph_ms_per_boot": ms_graph / (B * steps),
+               "speedup": ms_plain / ms_graph},
            "min_ks": {"ms_per_boot": ms_mk / (B * steps), "bootstraps_per_s": B * steps / (ms_mk / 1e3),
                       "rotation_keys": len(bc.rotations(min_ks=True))},
            "unit": "bootstraps/s", "ms_per_boot": ms_graph / (B * steps), "batch_per_gpu": B, "steps": steps,
