@@ -19,8 +19,9 @@ Reported (one JSON line on rank 0):
   bootstrap  full-slot bootstrapping throughput at N = 2^16 (bootstraps/s;
              --boot-precision adds a real-key run with decoded precision)
   ks_engines  the same step with the ModUp / ModDown column passes on each
-             engine (--ks-engine picks the measured one; default tensor,
-             1-2 % ahead of the CUDA-core engine on both workloads)
+             engine (--ks-engine picks the measured one; default auto: the
+             library times both engines on the first launch of each shape
+             and keeps the faster)
   bconv_engines  base conversion on CUDA cores vs tcgen05 tensor cores
   ntt        forward + inverse NTT round trip, 24 primes, HBM fraction
 `--impl reference` times the CPU implementation of the path (the oracle;
@@ -161,7 +162,7 @@ def main():
     ap.add_argument("--boot-profile", action="store_true",
                     help="profiling aid: set up the bootstrapping workload, run two BootBatch calls of "
                          "--boot-batch ciphertexts (the second is the one to read in a launch list) and exit")
-    ap.add_argument("--ks-engine", default="tensor", choices=["cuda", "tensor"],
+    ap.add_argument("--ks-engine", default="auto", choices=["cuda", "tensor", "auto"],
                     help="base conversion inside the ModUp / ModDown column passes of the measured path")
     ap.add_argument("--boot-precision", action="store_true",
                     help="also bootstrap one ciphertext with real keys (oracle key generation, slow) "
@@ -447,7 +448,7 @@ def roofline_from_stages(ctx, lvl, batch, stages, steps):
 
 
 def ks_engine_id(chd, args):
-    return chd.BCONV_TENSOR_CORE if args.ks_engine == "tensor" else chd.BCONV_CUDA_CORE
+    return {"cuda": chd.BCONV_CUDA_CORE, "tensor": chd.BCONV_TENSOR_CORE, "auto": chd.BCONV_AUTO}[args.ks_engine]
 
 
 def ks_engines(ctx, chd, step, stream, steps, B):
@@ -457,7 +458,8 @@ def ks_engines(ctx, chd, step, stream, steps, B):
     import torch
     old = ctx.ks_engine
     out = {}
-    for name, e in (("cuda_core", chd.BCONV_CUDA_CORE), ("tensor_core", chd.BCONV_TENSOR_CORE)):
+    for name, e in (("cuda_core", chd.BCONV_CUDA_CORE), ("tensor_core", chd.BCONV_TENSOR_CORE),
+                    ("auto", chd.BCONV_AUTO)):
         ctx.ks_engine = e
         for _ in range(3):
             step()
@@ -818,6 +820,17 @@ def boot_bench(chd, args, stream, dist, profile=False):
     ctx.synchronize()
     torch.cuda.synchronize()
     ms_plain = es0.elapsed_time(es1)
+    # one ciphertext per call with the autotuned engine
+    ctx.ks_engine = chd.BCONV_AUTO
+    step_single()
+    ctx.synchronize()
+    es0.record(stream)
+    for _ in range(steps):
+        step_single()
+    es1.record(stream)
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    ms_single_auto = es0.elapsed_time(es1)
     ctx.ks_engine = main_engine
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier(dist)
@@ -860,7 +873,8 @@ def boot_bench(chd, args, stream, dist, profile=False):
     # the same bootstraps with each column-pass engine
     engines = {}
     main_engine = ctx.ks_engine
-    for name, e in (("cuda_core", chd.BCONV_CUDA_CORE), ("tensor_core", chd.BCONV_TENSOR_CORE)):
+    for name, e in (("cuda_core", chd.BCONV_CUDA_CORE), ("tensor_core", chd.BCONV_TENSOR_CORE),
+                    ("auto", chd.BCONV_AUTO)):
         ctx.ks_engine = e
         step()
         ctx.synchronize()
@@ -879,7 +893,8 @@ def boot_bench(chd, args, stream, dist, profile=False):
            "value": job_throughput(world, B, steps, ms_graph),
            "eager": {"bootstraps_per_s": world * B * steps / (ms / 1e3), "ms_per_boot": ms / (B * steps)},
            "one_by_one_eager": {"bootstraps_per_s": world * B * steps / (ms_single / 1e3),
-                                "ms_per_boot": ms_single / (B * steps)},
+                                "ms_per_boot": ms_single / (B * steps),
+                                "ms_per_boot_auto_engine": ms_single_auto / (B * steps)},
            "plain_vs_tensor_batched": {
                "plain_cuda_core_one_by_one_ms_per_boot": ms_plain / (B * steps),
                "tensor_core_batched_graph_ms_per_boot": ms_graph / (B * steps),

@@ -19,6 +19,7 @@ PARAM_DIR = os.path.join(_HERE, "params")
 
 CHD_MODDOWN, CHD_RESCALE, CHD_MODDOWN_RESCALE = 0, 1, 2
 BCONV_CUDA_CORE, BCONV_TENSOR_CORE = 0, 1   # chd_bconv_batch engines
+BCONV_AUTO = 2                                # Context.ks_engine only: autotuned per launch shape
 
 # stages of the fused N = 2^16 key switch (chd_stage_times), in launch order
 KS_STAGE_NAMES = ("modup_inv_rows", "modup_cols", "ks_rows", "moddown_cols", "fwd_rows_epilogue")
@@ -217,7 +218,9 @@ class Context:
     @property
     def ks_engine(self):
         """Base-conversion engine of the key-switching and rescaling paths:
-        BCONV_CUDA_CORE or BCONV_TENSOR_CORE (bit-identical residues)."""
+        BCONV_CUDA_CORE, BCONV_TENSOR_CORE or BCONV_AUTO (the faster of the
+        two per launch shape, measured on first use); residues are
+        bit-identical."""
         return lib().chd_get_ks_engine(self.ptr)
 
     @ks_engine.setter

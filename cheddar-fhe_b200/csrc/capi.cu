@@ -135,8 +135,9 @@ int chd_stage_timing(chd_context *ctx, int enable) {
 
 int chd_set_ks_engine(chd_context *ctx, int engine) {
   CHD_NOTNULL(ctx);
-  if (engine != CHD_BCONV_CUDA_CORE && engine != CHD_BCONV_TENSOR_CORE)
-    return fail(CHD_ERR_INVALID_ARG, "chd_set_ks_engine: engine must be CHD_BCONV_CUDA_CORE or CHD_BCONV_TENSOR_CORE");
+  if (engine != CHD_BCONV_CUDA_CORE && engine != CHD_BCONV_TENSOR_CORE && engine != CHD_BCONV_AUTO)
+    return fail(CHD_ERR_INVALID_ARG,
+                "chd_set_ks_engine: engine must be CHD_BCONV_CUDA_CORE, CHD_BCONV_TENSOR_CORE or CHD_BCONV_AUTO");
   ctx->c->ks_engine = engine;
   return CHD_OK;
 }

@@ -327,7 +327,7 @@ class Context {
   int32_t *d_qinv = nullptr;
   int *d_err = nullptr;   // set by kernels whose bounded waits ran out
   int num_sms = 0;
-  int ks_engine = 0;      // ModUp / ModDown column-pass base conversion: 0 CUDA cores, 1 tensor cores
+  int ks_engine = 0;      // ModUp / ModDown column-pass base conversion: 0 CUDA cores, 1 tensor cores, 2 autotuned
   uint2 *d_tw = nullptr, *d_itw = nullptr;  // [nprimes][N] (psi_rev, Shoup companion)
   std::vector<uint32_t> n_inv, n_inv_mont, mont_conv, p_prod, imag_unit;
   std::vector<uint32_t> r_inv;  // 2^-32 mod q per global prime

@@ -13,6 +13,10 @@
 // Per tile and thread: 16 elements of one column.  The column transforms use
 // the same stage schedule as ntt.cu (radix-16 on rows rg + 8k in registers,
 // radix-8 on rows 8j + u after one shared-memory exchange).
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include "arith.cuh"
 #include "colpass.cuh"
 #include "kernels.h"
@@ -226,10 +230,8 @@ size_t modswitch_cols_smem(int kmax) { return (static_cast<size_t>(kExRows) * kT
 
 namespace {
 
-void launch_batch(const MSColBatch &b, cudaStream_t s) {
-  int max_k = 0;
-  for (int j = 0; j < b.count; j++) max_k = b.jobs[j].K > max_k ? b.jobs[j].K : max_k;
-  if (b.engine == 1) {
+void launch_engine(const MSColBatch &b, int engine, int max_k, cudaStream_t s) {
+  if (engine == 1) {
     launch_modswitch_cols_tc(b, max_k, s);
     return;
   }
@@ -250,6 +252,66 @@ void launch_batch(const MSColBatch &b, cudaStream_t s) {
     go(k_modswitch_cols<12, 2>, 12);
   else
     go(k_modswitch_cols<16, 0>, 16);
+}
+
+// Engine autotuning (engine 2): the CUDA-core pass wins on small launches
+// (one ciphertext), the tensor-core pass on large ones.  The first launch of
+// a shape (device, largest K, jobs, largest M) outside a stream capture runs
+// both engines twice, times the second runs with CUDA events (a host
+// synchronisation, once per shape), keeps the faster and caches the choice
+// for the process.  Both engines write identical residues, so the tuning
+// launches leave the same outputs.  During a capture an untuned shape uses
+// the tensor cores.  Returns true when the tuning launches have done the work.
+bool tune_and_launch(const MSColBatch &b, int max_k, cudaStream_t s, int *engine) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, int, int, int>, int> cache;
+  int dev = 0, max_m = 0;
+  cudaGetDevice(&dev);
+  for (int j = 0; j < b.count; j++) max_m = b.jobs[j].M > max_m ? b.jobs[j].M : max_m;
+  const auto key = std::make_tuple(dev, max_k, b.count, max_m);
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) {
+      *engine = it->second;
+      return false;
+    }
+  }
+  *engine = 1;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return false;
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  for (auto &e : ev)
+    if (cudaEventCreate(&e) != cudaSuccess) {
+      for (auto &f : ev)
+        if (f) cudaEventDestroy(f);
+      return false;
+    }
+  launch_engine(b, 0, max_k, s);  // warm-up: module load, attributes
+  launch_engine(b, 1, max_k, s);
+  cudaEventRecord(ev[0], s);
+  launch_engine(b, 0, max_k, s);
+  cudaEventRecord(ev[1], s);
+  launch_engine(b, 1, max_k, s);
+  cudaEventRecord(ev[2], s);
+  float t_cuda = 0.f, t_tc = 0.f;
+  const bool ok = cudaEventSynchronize(ev[2]) == cudaSuccess && cudaEventElapsedTime(&t_cuda, ev[0], ev[1]) == cudaSuccess &&
+                  cudaEventElapsedTime(&t_tc, ev[1], ev[2]) == cudaSuccess;
+  for (auto &e : ev) cudaEventDestroy(e);
+  if (ok) {
+    *engine = t_tc <= t_cuda ? 1 : 0;
+    std::lock_guard<std::mutex> lock(mu);
+    cache[key] = *engine;
+  }
+  return true;
+}
+
+void launch_batch(const MSColBatch &b, cudaStream_t s) {
+  int max_k = 0;
+  for (int j = 0; j < b.count; j++) max_k = b.jobs[j].K > max_k ? b.jobs[j].K : max_k;
+  int engine = b.engine;
+  if (engine == 2 && tune_and_launch(b, max_k, s, &engine)) return;
+  launch_engine(b, engine, max_k, s);
 }
 
 int sm_count() {

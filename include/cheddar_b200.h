@@ -324,6 +324,7 @@ void chd_graph_destroy(chd_graph *g);
  * tensor-core wait that ran out. */
 #define CHD_BCONV_CUDA_CORE 0
 #define CHD_BCONV_TENSOR_CORE 1
+#define CHD_BCONV_AUTO 2 /* chd_set_ks_engine only: autotuned per launch shape */
 int chd_bconv_batch(chd_context *ctx, int engine, int npoly, const int32_t *xt_dev, const int *src_gidx, int K,
                     const int *dst_gidx, int M, uint32_t *out_dev);
 
@@ -332,10 +333,14 @@ int chd_bconv_batch(chd_context *ctx, int engine, int npoly, const int32_t *xt_d
  * rotations, hoisted rotations, linear transforms, ModDown epilogues):
  * CHD_BCONV_CUDA_CORE (int64 multiply-adds) or CHD_BCONV_TENSOR_CORE (the
  * column pass issues INT8 byte-limb MMAs on the tcgen05 tensor cores with
- * int32 accumulation in TMEM).  Both give bit-identical residues.  No
- * reference counterpart (the reference has one CUDA-core implementation,
- * src/core/ModSwitch.cu:23-171).  chd_get_ks_engine returns the engine, -1
- * for a null context. */
+ * int32 accumulation in TMEM).  Both give bit-identical residues.
+ * CHD_BCONV_AUTO autotunes: the first column pass of each launch shape
+ * (device, sources, jobs, targets) outside a stream capture runs both
+ * engines, times them (one host synchronisation per shape and process) and
+ * keeps the faster; an untuned shape met during a capture uses the tensor
+ * cores.  No reference counterpart (the reference has one CUDA-core
+ * implementation, src/core/ModSwitch.cu:23-171).  chd_get_ks_engine returns
+ * the engine, -1 for a null context. */
 int chd_set_ks_engine(chd_context *ctx, int engine);
 int chd_get_ks_engine(const chd_context *ctx);
 

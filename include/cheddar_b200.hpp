@@ -129,8 +129,8 @@ class Context {
   double GetRescalePrimeProd(int level) const { return chd_rescale_prime_prod(c_, level); }
   void SetStream(void *cuda_stream) { check(chd_context_set_stream(c_, cuda_stream)); }
   void Synchronize() { check(chd_context_synchronize(c_)); }
-  // Base-conversion engine of every ModUp / ModDown (CHD_BCONV_CUDA_CORE or
-  // CHD_BCONV_TENSOR_CORE); results are bit-identical.
+  // Base-conversion engine of every ModUp / ModDown (CHD_BCONV_CUDA_CORE,
+  // CHD_BCONV_TENSOR_CORE or CHD_BCONV_AUTO); results are bit-identical.
   void SetKeySwitchEngine(int engine) { check(chd_set_ks_engine(c_, engine)); }
   int KeySwitchEngine() const { return chd_get_ks_engine(c_); }
 

@@ -216,3 +216,34 @@ def test_boot_params_column_passes(cuda_ok, eng, level):
         g.moddown_raw(level, chd.CHD_RESCALE, _dev(x), out1)
         g.synchronize()
         assert np.array_equal(_host(out1), o.rescale(level, x))
+
+
+def test_auto_engine(cuda_ok):
+    """CHD_BCONV_AUTO: the first launch of each shape runs and times both
+    engines, later ones use the faster; every result equals the oracle's
+    (single HMult, a batch, raw ModUp / ModDown, a rotation)."""
+    o, g = pair(KS)
+    (kb, ka), key = mult_key(KS)
+    with engine(g, chd.BCONV_AUTO):
+        assert g.ks_engine == chd.BCONV_AUTO
+        for rep in range(2):  # first call tunes, second uses the cache
+            lvl = 22
+            a = uniform_parts(KS, lvl, 1100 + rep)
+            b = uniform_parts(KS, lvl, 1200 + rep)
+            _eq(g.HMult(g.import_ct(lvl, a), g.import_ct(lvl, b), key, rescale=True),
+                o.hmult(lvl, a, b, (kb, ka), rescale=True))
+            pairs = [(uniform_parts(KS, 20, 1300 + 10 * rep + i), uniform_parts(KS, 20, 1400 + 10 * rep + i))
+                     for i in range(4)]
+            outs = g.HMultBatch([g.import_ct(20, x) for x, _ in pairs], [g.import_ct(20, y) for _, y in pairs], key,
+                                rescale=True)
+            for (x, y), r in zip(pairs, outs):
+                _eq(r, o.hmult(20, x, y, (kb, ka), rescale=True))
+            x = o.uniform(30 + rep, 15)
+            mu = torch.zeros((o.beta(15), o.num_q(15) + o.alpha, o.n), dtype=torch.int32, device="cuda")
+            g.modup_raw(15, _dev(x), mu)
+            g.synchronize()
+            ref = o.modup(15, x)
+            assert np.array_equal(_host(mu).reshape(ref.shape), ref)
+        (rb, ra), rk = rot_key(KS, 5)
+        a = uniform_parts(KS, 21, 1500)
+        _eq(g.HRot(g.import_ct(21, a), rk, 5), o.hrot(21, a, (rb, ra), 5))
