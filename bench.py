@@ -90,7 +90,8 @@ class ClockSampler:
         reasons = sorted({names[i] for s in self.samples for i in range(4)
                           if len(s) > 5 + i and s[5 + i].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+                "reasons": reasons, "samples": len(self.samples),
+                "window": "the timed steps plus 1 s of the same step right after them"}
 
 
 def cpu_baseline_run(max_seconds=20.0, reps=None):
@@ -232,6 +233,14 @@ def main():
             step()
         ev1.record(stream)
         torch.cuda.synchronize()
+        # the timed steps last a few ms, less than the 200 ms sampling
+        # interval: the same step keeps running, untimed, for another second
+        # so that the clock record covers this load
+        t_end = time.time() + 1.0
+        while time.time() < t_end:
+            for _ in range(20):
+                step()
+            torch.cuda.synchronize()
     ms = max_over_ranks(dist, ev0.elapsed_time(ev1), "cuda")
     ms_step = ms / args.steps
     value = job_throughput(world, B, args.steps, ms)
