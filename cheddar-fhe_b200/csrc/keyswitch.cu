@@ -57,10 +57,10 @@ __global__ void __launch_bounds__(256, 3) k_ks_rows(const __grid_constant__ KSRo
       const uint32_t *src = c.mu[i] + static_cast<size_t>(j) * 65536 + r * 512;
 #pragma unroll
       for (int k = 0; k < 8; k++) v[k] = src[t + 64 * k];
-      row_fwd(v, srow, tw, r, t, q);
+      row_fwd(v, srow, tw, r, t, q, 1 + rl);
 #pragma unroll
       for (int k = 0; k < 8; k++) v[k] = reduce2q(v[k], q);
-      __syncthreads();
+      row_sync(1 + rl);
     }
     uint32_t kb[8], ka[8];
     ld8(d.kb[i] + koff, kb);
@@ -108,10 +108,10 @@ __global__ void __launch_bounds__(256, 3) k_ks_rows(const __grid_constant__ KSRo
 #pragma unroll
   for (int p = 0; p < 2; p++) {
     uint32_t *x = p == 0 ? sb : sa;
-    row_inv(x, srow, itw, r, t, q);
+    row_inv(x, srow, itw, r, t, q, 1 + rl);
 #pragma unroll
     for (int k = 0; k < 8; k++) outs[p][t + 64 * k] = x[k];
-    __syncthreads();
+    row_sync(1 + rl);
   }
 }
 

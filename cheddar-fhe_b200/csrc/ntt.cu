@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(256) k_fwd_rows16(const __grid_constant__ RowB
   uint32_t x[8];
 #pragma unroll
   for (int k = 0; k < 8; k++) x[k] = src[t + 64 * k];
-  row_fwd(x, srow, tw, r, t, q);
+  row_fwd(x, srow, tw, r, t, q, -1);
 #pragma unroll
   for (int k = 0; k < 8; k++) x[k] = reduce2q(x[k], q);
   const int base = r * 512 + 8 * t;
@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(256) k_inv_rows16(const __grid_constant__ RowB
 #pragma unroll
     for (int k = 0; k < 8; k++) x[k] = mont_mul(x[k], y[k], q, rd.qinv);
   }
-  row_inv(x, srow, tw, r, t, q);
+  row_inv(x, srow, tw, r, t, q, -1);
   uint32_t *dst = rd.dst + r * 512;
 #pragma unroll
   for (int k = 0; k < 8; k++) dst[t + 64 * k] = x[k];

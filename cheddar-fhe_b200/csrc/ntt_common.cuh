@@ -99,23 +99,37 @@ __device__ __forceinline__ void radix16_cols_inv(uint32_t *x, const uint2 *tw, u
 // 8t + k, t the lane) are all bank-conflict free under this bijection.
 __device__ __forceinline__ int rsw(int c) { return c ^ ((c >> 3) & 31); }
 
+// Barrier of the 64 threads (two warps) that own one row: named barrier
+// `bar` (1 .. 15), so that the rows of a CTA do not wait for each other, or
+// the CTA-wide barrier for bar < 0.  The key-switch row pass (several loads
+// and MACs between its row transforms) gains from the per-row form; the
+// plain row kernels measured faster with the CTA-wide one.
+__device__ __forceinline__ void row_sync(int bar) {
+  if (bar < 0)
+    __syncthreads();
+  else
+    asm volatile("bar.sync %0, 64;" ::"r"(bar) : "memory");
+}
+
 // The 9 row stages (m = 128 .. 32768) of the forward transform on one
 // 512-element row r held by 64 threads (thread t), 8 elements each.  Input
 // x[k] = element t + 64k; output x[k] = element 8t + k.  srow is the row's
-// 512-word shared buffer; the caller synchronises before reusing it.
-__device__ __forceinline__ void row_fwd(uint32_t *x, uint32_t *srow, const uint2 *tw, int r, int t, uint32_t q) {
+// 512-word shared buffer, bar the row's named barrier; the caller
+// synchronises (row_sync) before reusing srow.
+__device__ __forceinline__ void row_fwd(uint32_t *x, uint32_t *srow, const uint2 *tw, int r, int t, uint32_t q,
+                                        int bar) {
   const int b = t >> 3, u0 = t & 7;
   radix8_fwd(x, tw, 128 + r, 256 + 2 * r, 512 + 4 * r, q);
 #pragma unroll
   for (int k = 0; k < 8; k++) srow[rsw(t + 64 * k)] = x[k];
-  __syncthreads();
+  row_sync(bar);
 #pragma unroll
   for (int k = 0; k < 8; k++) x[k] = srow[rsw(64 * b + u0 + 8 * k)];
   radix8_fwd(x, tw, 1024 + 8 * r + b, 2048 + 16 * r + 2 * b, 4096 + 32 * r + 4 * b, q);
-  __syncthreads();
+  row_sync(bar);
 #pragma unroll
   for (int k = 0; k < 8; k++) srow[rsw(64 * b + u0 + 8 * k)] = x[k];
-  __syncthreads();
+  row_sync(bar);
 #pragma unroll
   for (int k = 0; k < 8; k++) x[k] = srow[rsw(8 * t + k)];
   radix8_fwd(x, tw, 8192 + 64 * r + t, 16384 + 128 * r + 2 * t, 32768 + 256 * r + 4 * t, q);
@@ -123,19 +137,20 @@ __device__ __forceinline__ void row_fwd(uint32_t *x, uint32_t *srow, const uint2
 
 // The 9 row stages of the inverse transform (m = 32768 .. 128): input x[k] =
 // element 8t + k, output x[k] = element t + 64k.
-__device__ __forceinline__ void row_inv(uint32_t *x, uint32_t *srow, const uint2 *tw, int r, int t, uint32_t q) {
+__device__ __forceinline__ void row_inv(uint32_t *x, uint32_t *srow, const uint2 *tw, int r, int t, uint32_t q,
+                                        int bar) {
   const int b = t >> 3, u0 = t & 7;
   radix8_inv(x, tw, 8192 + 64 * r + t, 16384 + 128 * r + 2 * t, 32768 + 256 * r + 4 * t, q);
 #pragma unroll
   for (int k = 0; k < 8; k++) srow[rsw(8 * t + k)] = x[k];
-  __syncthreads();
+  row_sync(bar);
 #pragma unroll
   for (int k = 0; k < 8; k++) x[k] = srow[rsw(64 * b + u0 + 8 * k)];
   radix8_inv(x, tw, 1024 + 8 * r + b, 2048 + 16 * r + 2 * b, 4096 + 32 * r + 4 * b, q);
-  __syncthreads();
+  row_sync(bar);
 #pragma unroll
   for (int k = 0; k < 8; k++) srow[rsw(64 * b + u0 + 8 * k)] = x[k];
-  __syncthreads();
+  row_sync(bar);
 #pragma unroll
   for (int k = 0; k < 8; k++) x[k] = srow[rsw(t + 64 * k)];
   radix8_inv(x, tw, 128 + r, 256 + 2 * r, 512 + 4 * r, q);
