@@ -58,6 +58,16 @@ def lib():
         "chd_context_synchronize": (i, [vp]),
         "chd_stage_timing": (i, [vp, i]),
         "chd_set_ks_engine": (i, [vp, i]),
+        "chd_copy": (i, [vp, vp, vp]),
+        "chd_mult_unsafe": (i, [vp, vp, vp, vp, i]),
+        "chd_mult_unsafe_const": (i, [vp, vp, vp, vp, i, d, i]),
+        "chd_mad_unsafe": (i, [vp, vp, vp, vp, i, d]),
+        "chd_permute": (i, [vp, vp, vp, i]),
+        "chd_permute_conjugate": (i, [vp, vp, vp]),
+        "chd_hconj_add": (i, [vp, vp, vp, vp, vp]),
+        "chd_level_down": (i, [vp, vp, vp, i]),
+        "chd_mult_key_no_moddown": (i, [vp, vp, vp, vp]),
+        "chd_mult_unsafe_compatible": (i, [vp, i, i]),
         "chd_get_ks_engine": (i, [vp]),
         "chd_stage_times": (i, [vp, vp, vp]),
         "chd_level_np": (i, [vp, i, C.POINTER(i), C.POINTER(i)]),
@@ -375,6 +385,64 @@ class Context:
         res = self._new(res)
         _check(lib().chd_hrot_add(self.ptr, res.ptr, a.ptr, b.ptr, rot_key.ptr, rot_dist))
         return res
+
+    def Copy(self, a, res=None):
+        res = self._new(res)
+        _check(lib().chd_copy(self.ptr, res.ptr, a.ptr))
+        return res
+
+    def MultUnsafe(self, a, b, level=-1, res=None):
+        """Tensor product at `level` (-1: the lower input level)."""
+        res = self._new(res)
+        _check(lib().chd_mult_unsafe(self.ptr, res.ptr, a.ptr, b.ptr, level))
+        return res
+
+    def MultUnsafeConst(self, a, cx, const_level, const_scale, level=-1, res=None):
+        """a times a constant (cx: Montgomery residues over const_level's q
+        primes, as encode_const gives them) at `level`."""
+        res = self._new(res)
+        c = np.ascontiguousarray(cx, dtype=np.uint32)
+        _check(lib().chd_mult_unsafe_const(self.ptr, res.ptr, a.ptr, c.ctypes.data, const_level, float(const_scale),
+                                           level))
+        return res
+
+    def MadUnsafe(self, res, a, cx, const_level, const_scale):
+        """res += a times a constant."""
+        c = np.ascontiguousarray(cx, dtype=np.uint32)
+        _check(lib().chd_mad_unsafe(self.ptr, res.ptr, a.ptr, c.ctypes.data, const_level, float(const_scale)))
+        return res
+
+    def Permute(self, a, rot_dist, res=None):
+        res = self._new(res)
+        _check(lib().chd_permute(self.ptr, res.ptr, a.ptr, rot_dist))
+        return res
+
+    def PermuteConjugate(self, a, res=None):
+        res = self._new(res)
+        _check(lib().chd_permute_conjugate(self.ptr, res.ptr, a.ptr))
+        return res
+
+    def HConjAdd(self, a, b, conj_key, res=None):
+        res = self._new(res)
+        _check(lib().chd_hconj_add(self.ptr, res.ptr, a.ptr, b.ptr, conj_key.ptr))
+        return res
+
+    def LevelDown(self, a, target_level, res=None):
+        res = self._new(res)
+        _check(lib().chd_level_down(self.ptr, res.ptr, a.ptr, target_level))
+        return res
+
+    def MultKeyNoModDown(self, a, key, res=None):
+        """Relinearisation of a (with rx) left in the extended basis."""
+        res = self._new(res)
+        _check(lib().chd_mult_key_no_moddown(self.ptr, res.ptr, a.ptr, key.ptr))
+        return res
+
+    def IsMultUnsafeCompatible(self, level1, level2):
+        r = lib().chd_mult_unsafe_compatible(self.ptr, level1, level2)
+        if r < 0:
+            raise CheddarError(1, "IsMultUnsafeCompatible: invalid level")
+        return bool(r)
 
     def HoistedRotate(self, a, rot_keys, rot_dists, outs=None):
         n = len(rot_dists)

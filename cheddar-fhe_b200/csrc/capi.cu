@@ -2,6 +2,7 @@
 #include <cstring>
 
 #include <algorithm>
+#include <exception>
 #include <complex>
 
 #include "../../include/cheddar_b200.h"
@@ -66,7 +67,7 @@ extern "C" {
 
 const char *chd_last_error(void) { return last_error(); }
 
-int chd_context_create_json(const char *json_text, int device, chd_context **out) {
+int chd_context_create_json(const char *json_text, int device, chd_context **out) try {
   CHD_NOTNULL(json_text);
   CHD_NOTNULL(out);
   ParamSpec spec;
@@ -76,12 +77,16 @@ int chd_context_create_json(const char *json_text, int device, chd_context **out
   if (!c) return fail(CHD_ERR_INVALID_ARG, err);
   *out = new chd_context{std::move(c)};
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 int chd_context_create(int log_degree, double base_scale, int default_encryption_level, const int *level_config,
                        int num_levels, const uint32_t *main_primes, int num_main, const uint32_t *aux_primes,
                        int num_aux, const uint32_t *ter_primes, int num_ter, int additional_main,
-                       int additional_ter, int device, chd_context **out) {
+                       int additional_ter, int device, chd_context **out) try {
   CHD_NOTNULL(level_config);
   CHD_NOTNULL(main_primes);
   CHD_NOTNULL(aux_primes);
@@ -101,11 +106,15 @@ int chd_context_create(int log_degree, double base_scale, int default_encryption
   if (!c) return fail(CHD_ERR_INVALID_ARG, err);
   *out = new chd_context{std::move(c)};
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 void chd_context_destroy(chd_context *ctx) { delete ctx; }
 
-int chd_context_set_stream(chd_context *ctx, void *cuda_stream) {
+int chd_context_set_stream(chd_context *ctx, void *cuda_stream) try {
   CHD_NOTNULL(ctx);
   Context &C = *ctx->c;
   if (C.own_stream && C.stream) {
@@ -120,9 +129,13 @@ int chd_context_set_stream(chd_context *ctx, void *cuda_stream) {
     C.own_stream = true;
   }
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_stage_timing(chd_context *ctx, int enable) {
+int chd_stage_timing(chd_context *ctx, int enable) try {
   CHD_NOTNULL(ctx);
   Context &C = *ctx->c;
   if (enable) {
@@ -131,26 +144,158 @@ int chd_stage_timing(chd_context *ctx, int enable) {
   }
   C.timer.on = enable != 0;
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_set_ks_engine(chd_context *ctx, int engine) {
+int chd_copy(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) try {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  return ctx->c->copy_ct(res->ct, a->ct);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
+}
+
+int chd_mult_unsafe(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_ciphertext *b,
+                    int level) try {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  CHD_NOTNULL(b);
+  return ctx->c->mult_unsafe(res->ct, a->ct, b->ct, level);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
+}
+
+int chd_mult_unsafe_const(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *cx,
+                          int const_level, double const_scale, int level) try {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  CHD_NOTNULL(cx);
+  return ctx->c->mult_unsafe_const(res->ct, a->ct, cx, const_level, const_scale, level);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
+}
+
+int chd_mad_unsafe(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *cx,
+                   int const_level, double const_scale) try {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  CHD_NOTNULL(cx);
+  return ctx->c->mad_unsafe(res->ct, a->ct, cx, const_level, const_scale);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
+}
+
+int chd_permute(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, int rot_dist) try {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  return ctx->c->permute_ct(res->ct, a->ct, rot_dist, false);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
+}
+
+int chd_permute_conjugate(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) try {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  return ctx->c->permute_ct(res->ct, a->ct, 0, true);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
+}
+
+int chd_hconj_add(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_ciphertext *b,
+                  const chd_evk *conj_key) try {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  CHD_NOTNULL(b);
+  CHD_NOTNULL(conj_key);
+  return ctx->c->hconj_add(res->ct, a->ct, b->ct, conj_key->k);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
+}
+
+int chd_level_down(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, int target_level) try {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  return ctx->c->level_down(res->ct, a->ct, target_level);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
+}
+
+int chd_mult_key_no_moddown(chd_context *ctx, chd_ciphertext *accum, const chd_ciphertext *a, const chd_evk *key) try {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(accum);
+  CHD_NOTNULL(a);
+  CHD_NOTNULL(key);
+  return ctx->c->mult_key_no_moddown(accum->ct, a->ct, key->k);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
+}
+
+int chd_mult_unsafe_compatible(const chd_context *ctx, int level1, int level2) try {
+  if (!ctx) return -1;
+  const int ml = ctx->c->P->max_level;
+  if (level1 < 0 || level2 < 0 || level1 > ml || level2 > ml) return -1;
+  return ctx->c->mult_unsafe_compatible(level1, level2) ? 1 : 0;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
+}
+
+int chd_set_ks_engine(chd_context *ctx, int engine) try {
   CHD_NOTNULL(ctx);
   if (engine != CHD_BCONV_CUDA_CORE && engine != CHD_BCONV_TENSOR_CORE && engine != CHD_BCONV_AUTO)
     return fail(CHD_ERR_INVALID_ARG,
                 "chd_set_ks_engine: engine must be CHD_BCONV_CUDA_CORE, CHD_BCONV_TENSOR_CORE or CHD_BCONV_AUTO");
   ctx->c->ks_engine = engine;
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 int chd_get_ks_engine(const chd_context *ctx) { return ctx ? ctx->c->ks_engine : -1; }
 
-int chd_stage_times(chd_context *ctx, double *ms, int *launches) {
+int chd_stage_times(chd_context *ctx, double *ms, int *launches) try {
   CHD_NOTNULL(ctx);
   if (!ms || !launches) return fail(CHD_ERR_INVALID_ARG, "chd_stage_times: null output");
   return ctx->c->timer_read(ms, launches);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_context_synchronize(chd_context *ctx) {
+int chd_context_synchronize(chd_context *ctx) try {
   CHD_NOTNULL(ctx);
   Context &C = *ctx->c;
   cudaError_t e = cudaStreamSynchronize(C.stream);
@@ -164,9 +309,13 @@ int chd_context_synchronize(chd_context *ctx) {
     return fail(CHD_ERR_CUDA, "a kernel gave up waiting for its tensor-core work (bounded wait ran out)");
   }
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_level_np(const chd_context *ctx, int level, int *num_main, int *num_ter) {
+int chd_level_np(const chd_context *ctx, int level, int *num_main, int *num_ter) try {
   CHD_NOTNULL(ctx);
   const Params &P = *ctx->c->P;
   if (level < -1 || level > P.max_level) return fail(CHD_ERR_INVALID_LEVEL, "invalid level");
@@ -174,6 +323,10 @@ int chd_level_np(const chd_context *ctx, int level, int *num_main, int *num_ter)
   if (num_main) *num_main = np.main;
   if (num_ter) *num_ter = np.ter;
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 int chd_max_level(const chd_context *ctx) { return ctx ? ctx->c->P->max_level : -1; }
 int chd_degree(const chd_context *ctx) { return ctx ? ctx->c->P->n : -1; }
@@ -192,25 +345,33 @@ double chd_rescale_prime_prod(const chd_context *ctx, int level) {
   if (level < 1 || level > P.max_level) return 0.0;
   return P.rescale_prod[level];
 }
-int chd_prime_gidx(const chd_context *ctx, int num_main, int num_ter, int num_aux, int *out) {
+int chd_prime_gidx(const chd_context *ctx, int num_main, int num_ter, int num_aux, int *out) try {
   if (!ctx || !out) return -1;
   NP np{num_main, num_ter, num_aux};
   ctx->c->P->gidx(np, out);
   return np.total();
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_ct_create(chd_context *ctx, chd_ciphertext **out) {
+int chd_ct_create(chd_context *ctx, chd_ciphertext **out) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(out);
   *out = new chd_ciphertext();
   (*out)->ct.num_slots = ctx->c->P->n / 2;
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 void chd_ct_destroy(chd_ciphertext *ct) { delete ct; }
 
 int chd_ct_wrap(chd_context *ctx, int num_main, int num_ter, int num_aux, int has_rx, double scale, int num_slots,
-                uint32_t *bx, uint32_t *ax, uint32_t *rx, size_t words_per_part, chd_ciphertext **out) {
+                uint32_t *bx, uint32_t *ax, uint32_t *rx, size_t words_per_part, chd_ciphertext **out) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(out);
   CHD_NOTNULL(bx);
@@ -231,11 +392,15 @@ int chd_ct_wrap(chd_context *ctx, int num_main, int num_ter, int num_aux, int ha
   c->ct.cap_words = words_per_part;
   *out = c;
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 int chd_ct_import(chd_context *ctx, chd_ciphertext *ct, int num_main, int num_ter, int num_aux, int has_rx,
                   double scale, int num_slots, const uint32_t *bx, const uint32_t *ax, const uint32_t *rx,
-                  int src_on_device) {
+                  int src_on_device) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(ct);
   CHD_NOTNULL(bx);
@@ -258,10 +423,14 @@ int chd_ct_import(chd_context *ctx, chd_ciphertext *ct, int num_main, int num_te
   if (e != cudaSuccess) return fail(CHD_ERR_CUDA, cudaGetErrorString(e));
   if (!src_on_device) cudaStreamSynchronize(C.stream);
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 int chd_ct_export(chd_context *ctx, const chd_ciphertext *ct, uint32_t *bx, uint32_t *ax, uint32_t *rx,
-                  int dst_on_device) {
+                  int dst_on_device) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(ct);
   Context &C = *ctx->c;
@@ -273,10 +442,14 @@ int chd_ct_export(chd_context *ctx, const chd_ciphertext *ct, uint32_t *bx, uint
   cudaError_t e = cudaStreamSynchronize(C.stream);
   if (e != cudaSuccess) return fail(CHD_ERR_CUDA, cudaGetErrorString(e));
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 int chd_ct_info(const chd_ciphertext *ct, int *num_main, int *num_ter, int *num_aux, int *has_rx, double *scale,
-                int *num_slots) {
+                int *num_slots) try {
   CHD_NOTNULL(ct);
   if (num_main) *num_main = ct->ct.np.main;
   if (num_ter) *num_ter = ct->ct.np.ter;
@@ -285,18 +458,26 @@ int chd_ct_info(const chd_ciphertext *ct, int *num_main, int *num_ter, int *num_
   if (scale) *scale = ct->ct.scale;
   if (num_slots) *num_slots = ct->ct.num_slots;
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_ct_device_ptrs(const chd_ciphertext *ct, uint32_t **bx, uint32_t **ax, uint32_t **rx) {
+int chd_ct_device_ptrs(const chd_ciphertext *ct, uint32_t **bx, uint32_t **ax, uint32_t **rx) try {
   CHD_NOTNULL(ct);
   if (bx) *bx = ct->ct.bx;
   if (ax) *ax = ct->ct.ax;
   if (rx) *rx = ct->ct.rx;
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 int chd_evk_create(chd_context *ctx, int beta, const uint32_t *bx, const uint32_t *ax, int src_on_device,
-                   chd_evk **out) {
+                   chd_evk **out) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(bx);
   CHD_NOTNULL(ax);
@@ -322,6 +503,10 @@ int chd_evk_create(chd_context *ctx, int beta, const uint32_t *bx, const uint32_
   }
   *out = k;
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 void chd_evk_destroy(chd_evk *evk) { delete evk; }
@@ -339,55 +524,79 @@ CTX_CT3(chd_sub, sub)
 CTX_CT3(chd_mult, mult_tensor)
 #undef CTX_CT3
 
-int chd_neg(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) {
+int chd_neg(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   return ctx->c->neg(res->ct, a->ct);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 int chd_mult_const(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *cx,
-                   double const_scale) {
+                   double const_scale) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(cx);
   return ctx->c->mult_const(res->ct, a->ct, cx, const_scale);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_add_const(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *cx) {
+int chd_add_const(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *cx) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(cx);
   return ctx->c->add_const(res->ct, a->ct, cx);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 int chd_mult_plain(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *pt_dev,
-                   double pt_scale) {
+                   double pt_scale) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(pt_dev);
   return ctx->c->mult_plain(res->ct, a->ct, pt_dev, pt_scale);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_mult_imaginary_unit(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) {
+int chd_mult_imaginary_unit(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   return ctx->c->mult_imag_unit(res->ct, a->ct);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_rescale(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) {
+int chd_rescale(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   return ctx->c->rescale(res->ct, a->ct);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 int chd_encode(chd_context *ctx, int level, double scale, const double *re, const double *im, int msg_len,
-               int num_aux, uint32_t *pt_dev, int *num_slots) {
+               int num_aux, uint32_t *pt_dev, int *num_slots) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(re);
   CHD_NOTNULL(im);
@@ -396,9 +605,13 @@ int chd_encode(chd_context *ctx, int level, double scale, const double *re, cons
   std::vector<std::complex<double>> msg(msg_len);
   for (int i = 0; i < msg_len; i++) msg[i] = std::complex<double>(re[i], im[i]);
   return ctx->c->encode(level, scale, msg.data(), msg_len, num_aux, pt_dev, num_slots);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_encode_const(chd_context *ctx, int level, double scale, double value, int num_aux, uint32_t *cx) {
+int chd_encode_const(chd_context *ctx, int level, double scale, double value, int num_aux, uint32_t *cx) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(cx);
   const Params &P = *ctx->c->P;
@@ -408,9 +621,13 @@ int chd_encode_const(chd_context *ctx, int level, double scale, double value, in
   ctx->c->encode_const(level, scale, value, num_aux, &v);
   std::copy(v.begin(), v.end(), cx);
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_modup_to_max(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk_map *keys) {
+int chd_modup_to_max(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk_map *keys) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
@@ -428,55 +645,83 @@ int chd_modup_to_max(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext
     return C.modup_to_max_sse(res->ct, a->ct, *keys->dts, *keys->std_key);
   }
   return C.modup_to_max(res->ct, a->ct);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_evk_map_create(chd_context *ctx, chd_evk_map **out) {
+int chd_evk_map_create(chd_context *ctx, chd_evk_map **out) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(out);
   *out = new chd_evk_map();
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 void chd_evk_map_destroy(chd_evk_map *m) { delete m; }
 
-int chd_evk_map_set_rotation(chd_evk_map *m, int rot_idx, const chd_evk *key) {
+int chd_evk_map_set_rotation(chd_evk_map *m, int rot_idx, const chd_evk *key) try {
   CHD_NOTNULL(m);
   CHD_NOTNULL(key);
   if (rot_idx <= 0) return fail(CHD_ERR_INVALID_ARG, "chd_evk_map_set_rotation: rotation index must be positive");
   m->rot[rot_idx] = &key->k;
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_evk_map_set_conjugation(chd_evk_map *m, const chd_evk *key) {
+int chd_evk_map_set_conjugation(chd_evk_map *m, const chd_evk *key) try {
   CHD_NOTNULL(m);
   CHD_NOTNULL(key);
   m->conj = &key->k;
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_evk_map_set_mult(chd_evk_map *m, const chd_evk *key) {
+int chd_evk_map_set_mult(chd_evk_map *m, const chd_evk *key) try {
   CHD_NOTNULL(m);
   CHD_NOTNULL(key);
   m->mult = &key->k;
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_evk_map_set_dense_to_sparse(chd_evk_map *m, const chd_evk *key) {
+int chd_evk_map_set_dense_to_sparse(chd_evk_map *m, const chd_evk *key) try {
   CHD_NOTNULL(m);
   CHD_NOTNULL(key);
   m->dts = &key->k;
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_evk_map_set_sparse_to_dense(chd_evk_map *m, const chd_evk *key) {
+int chd_evk_map_set_sparse_to_dense(chd_evk_map *m, const chd_evk *key) try {
   CHD_NOTNULL(m);
   CHD_NOTNULL(key);
   m->std_key = &key->k;
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 int chd_evk_create_np(chd_context *ctx, int num_main, int num_ter, int num_aux, int beta, const uint32_t *bx,
-                      const uint32_t *ax, int src_on_device, chd_evk **out) {
+                      const uint32_t *ax, int src_on_device, chd_evk **out) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(bx);
   CHD_NOTNULL(ax);
@@ -503,11 +748,15 @@ int chd_evk_create_np(chd_context *ctx, int num_main, int num_ter, int num_aux, 
   }
   *out = k;
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 int chd_lintrans_create(chd_context *ctx, int width, int n_diag, const int *diag_idx, const double *re,
                         const double *im, int pt_level, double pt_scale, int bs, int gs, int pre_rotation,
-                        int additional_pt_rot, chd_lintrans **out) {
+                        int additional_pt_rot, chd_lintrans **out) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(diag_idx);
   CHD_NOTNULL(re);
@@ -531,6 +780,10 @@ int chd_lintrans_create(chd_context *ctx, int width, int n_diag, const int *diag
   }
   *out = lt;
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 void chd_lintrans_destroy(chd_lintrans *lt) { delete lt; }
@@ -554,7 +807,7 @@ int plan_rotations(const LTPlan &p, bool min_ks, std::vector<int> *r) {
 }
 }  // namespace
 
-int chd_lintrans_rotations(const chd_lintrans *lt, int min_ks, int *out, int cap, int *count) {
+int chd_lintrans_rotations(const chd_lintrans *lt, int min_ks, int *out, int cap, int *count) try {
   CHD_NOTNULL(lt);
   CHD_NOTNULL(count);
   std::vector<int> r;
@@ -566,16 +819,24 @@ int chd_lintrans_rotations(const chd_lintrans *lt, int min_ks, int *out, int cap
   if (out)
     for (int i = 0; i < std::min(cap, *count); i++) out[i] = r[i];
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_lintrans_num_pts(const chd_lintrans *lt, int *count) {
+int chd_lintrans_num_pts(const chd_lintrans *lt, int *count) try {
   CHD_NOTNULL(lt);
   CHD_NOTNULL(count);
   *count = static_cast<int>(lt->plan.pts.size());
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_lintrans_pt(const chd_lintrans *lt, int i, int *gs, int *bs, double *re, double *im) {
+int chd_lintrans_pt(const chd_lintrans *lt, int i, int *gs, int *bs, double *re, double *im) try {
   CHD_NOTNULL(lt);
   if (i < 0 || i >= static_cast<int>(lt->plan.pts.size())) return fail(CHD_ERR_INVALID_ARG, "chd_lintrans_pt: index");
   const LTPlan::Pt &p = lt->plan.pts[i];
@@ -586,10 +847,14 @@ int chd_lintrans_pt(const chd_lintrans *lt, int i, int *gs, int *bs, double *re,
     if (im) im[k] = p.msg[k].imag();
   }
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 int chd_lintrans_evaluate(chd_context *ctx, const chd_lintrans *lt, chd_ciphertext *res, const chd_ciphertext *in,
-                          const chd_evk_map *keys, int min_ks) {
+                          const chd_evk_map *keys, int min_ks) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(lt);
   CHD_NOTNULL(res);
@@ -621,10 +886,14 @@ int chd_lintrans_evaluate(chd_context *ctx, const chd_lintrans *lt, chd_cipherte
     return CHD_OK;
   }
   return ctx->c->lt_evaluate(res->ct, in->ct, lt->plan, keys->rot);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 int chd_poly_create(chd_context *ctx, const double *coeffs, int n, int input_level, double input_scale,
-                    double target_scale, int chebyshev, chd_program **out) {
+                    double target_scale, int chebyshev, chd_program **out) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(coeffs);
   CHD_NOTNULL(out);
@@ -643,10 +912,14 @@ int chd_poly_create(chd_context *ctx, const double *coeffs, int n, int input_lev
   pg->end_scale = target_scale;
   *out = pg;
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 int chd_evalmod_create(chd_context *ctx, int start_level, const double *coeffs, int n, int num_double_angle,
-                       int initial_K, chd_program **out, double *start_scale, double *end_scale) {
+                       int initial_K, chd_program **out, double *start_scale, double *end_scale) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(coeffs);
   CHD_NOTNULL(out);
@@ -665,18 +938,26 @@ int chd_evalmod_create(chd_context *ctx, int start_level, const double *coeffs, 
   if (end_scale) *end_scale = pg->end_scale;
   *out = pg;
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 void chd_program_destroy(chd_program *p) { delete p; }
 
-int chd_boot_mod_coefficients(double *out, int cap) {
+int chd_boot_mod_coefficients(double *out, int cap) try {
   const auto &c = boot_mod_coefficients();
   if (out)
     for (int i = 0; i < std::min(cap, static_cast<int>(c.size())); i++) out[i] = c[i];
   return static_cast<int>(c.size());
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_program_json(const chd_program *p, char *buf, size_t cap, size_t *len) {
+int chd_program_json(const chd_program *p, char *buf, size_t cap, size_t *len) try {
   CHD_NOTNULL(p);
   CHD_NOTNULL(len);
   const Program &g = p->prog;
@@ -705,6 +986,10 @@ int chd_program_json(const chd_program *p, char *buf, size_t cap, size_t *len) {
   *len = s.size() + 1;
   if (buf && cap >= s.size() + 1) memcpy(buf, s.c_str(), s.size() + 1);
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 namespace {
@@ -721,7 +1006,7 @@ Status copy_ct(Context &C, DeviceCt &dst, const DeviceCt &src) {
 }  // namespace
 
 int chd_program_run(chd_context *ctx, const chd_program *p, chd_ciphertext *res, const chd_ciphertext *in,
-                    const chd_evk_map *keys) {
+                    const chd_evk_map *keys) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(p);
   CHD_NOTNULL(res);
@@ -737,16 +1022,24 @@ int chd_program_run(chd_context *ctx, const chd_program *p, chd_ciphertext *res,
   rc = copy_ct(C, res->ct, regs[p->prog.output]);
   if (rc != CHD_OK) return rc;
   return cudaStreamSynchronize(C.stream) == cudaSuccess ? CHD_OK : fail(CHD_ERR_CUDA, "chd_program_run: CUDA error");
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 int chd_boot_create(chd_context *ctx, int num_slots, int num_cts_levels, int num_stc_levels, int log_message_ratio,
-                    chd_boot **out) {
+                    chd_boot **out) try {
   return chd_boot_create_variant(ctx, num_slots, CHD_BOOT_NORMAL, num_cts_levels, num_stc_levels, log_message_ratio,
                                  out);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 int chd_boot_create_variant(chd_context *ctx, int num_slots, int variant, int num_cts_levels, int num_stc_levels,
-                            int log_message_ratio, chd_boot **out) {
+                            int log_message_ratio, chd_boot **out) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(out);
   auto *b = new chd_boot();
@@ -757,11 +1050,15 @@ int chd_boot_create_variant(chd_context *ctx, int num_slots, int variant, int nu
   }
   *out = b;
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 void chd_boot_destroy(chd_boot *b) { delete b; }
 
-int chd_boot_rotations(const chd_boot *b, int min_ks, int *out, int cap, int *count) {
+int chd_boot_rotations(const chd_boot *b, int min_ks, int *out, int cap, int *count) try {
   CHD_NOTNULL(b);
   CHD_NOTNULL(count);
   std::vector<int> r;
@@ -776,9 +1073,13 @@ int chd_boot_rotations(const chd_boot *b, int min_ks, int *out, int cap, int *co
   if (out)
     for (int i = 0; i < std::min(cap, *count); i++) out[i] = r[i];
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_boot_levels(const chd_boot *b, int *levels, double *scales) {
+int chd_boot_levels(const chd_boot *b, int *levels, double *scales) try {
   CHD_NOTNULL(b);
   const BootPlan &p = b->plan;
   if (levels) {
@@ -796,17 +1097,25 @@ int chd_boot_levels(const chd_boot *b, int *levels, double *scales) {
     scales[4] = p.final_scale;
   }
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_boot_json(const chd_boot *b, char *buf, size_t cap, size_t *len) {
+int chd_boot_json(const chd_boot *b, char *buf, size_t cap, size_t *len) try {
   CHD_NOTNULL(b);
   chd_program tmp;
   tmp.prog = b->plan.prog;
   tmp.out_level = b->plan.end_level;
   return chd_program_json(&tmp, buf, cap, len);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_boot_lt_info(const chd_boot *b, int i, int *level, double *scale, int *npts, int *width) {
+int chd_boot_lt_info(const chd_boot *b, int i, int *level, double *scale, int *npts, int *width) try {
   CHD_NOTNULL(b);
   if (i < 0 || i >= static_cast<int>(b->plan.lts.size())) return fail(CHD_ERR_INVALID_ARG, "chd_boot_lt_info: index");
   const LTPlan &l = b->plan.lts[i];
@@ -815,9 +1124,13 @@ int chd_boot_lt_info(const chd_boot *b, int i, int *level, double *scale, int *n
   if (npts) *npts = static_cast<int>(l.pts.size());
   if (width) *width = l.width;
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_boot_lt_pt(const chd_boot *b, int i, int j, int *gs, int *bs, double *re, double *im) {
+int chd_boot_lt_pt(const chd_boot *b, int i, int j, int *gs, int *bs, double *re, double *im) try {
   CHD_NOTNULL(b);
   if (i < 0 || i >= static_cast<int>(b->plan.lts.size())) return fail(CHD_ERR_INVALID_ARG, "chd_boot_lt_pt: index");
   const LTPlan &l = b->plan.lts[i];
@@ -830,10 +1143,14 @@ int chd_boot_lt_pt(const chd_boot *b, int i, int j, int *gs, int *bs, double *re
     if (im) im[k] = p.msg[k].imag();
   }
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 int chd_boot_run(chd_context *ctx, chd_boot *b, chd_ciphertext *res, const chd_ciphertext *in, const chd_evk_map *keys,
-                 int min_ks) {
+                 int min_ks) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(b);
   CHD_NOTNULL(res);
@@ -858,10 +1175,14 @@ int chd_boot_run(chd_context *ctx, chd_boot *b, chd_ciphertext *res, const chd_c
     return CHD_OK;
   }
   return ctx->c->boot_run(b->plan, res->ct, in->ct, pk, &b->regs);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 int chd_boot_run_batch(chd_context *ctx, chd_boot *b, int count, chd_ciphertext *const *res,
-                       const chd_ciphertext *const *in, const chd_evk_map *keys, int min_ks) {
+                       const chd_ciphertext *const *in, const chd_evk_map *keys, int min_ks) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(b);
   CHD_NOTNULL(res);
@@ -905,18 +1226,26 @@ int chd_boot_run_batch(chd_context *ctx, chd_boot *b, int count, chd_ciphertext 
     r.num_slots = tmp[c].num_slots;
   }
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_graph_begin(chd_context *ctx) {
+int chd_graph_begin(chd_context *ctx) try {
   CHD_NOTNULL(ctx);
   Context &C = *ctx->c;
   if (!C.stream) return fail(CHD_ERR_INVALID_ARG, "chd_graph_begin: capture needs a non-default context stream");
   cudaError_t e = cudaStreamBeginCapture(C.stream, cudaStreamCaptureModeRelaxed);
   if (e != cudaSuccess) return fail(CHD_ERR_CUDA, std::string("chd_graph_begin: ") + cudaGetErrorString(e));
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_graph_end(chd_context *ctx, chd_graph **out) {
+int chd_graph_end(chd_context *ctx, chd_graph **out) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(out);
   Context &C = *ctx->c;
@@ -930,54 +1259,78 @@ int chd_graph_end(chd_context *ctx, chd_graph **out) {
   }
   *out = g;
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_graph_launch(chd_context *ctx, const chd_graph *g) {
+int chd_graph_launch(chd_context *ctx, const chd_graph *g) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(g);
   cudaError_t e = cudaGraphLaunch(g->exec, ctx->c->stream);
   if (e != cudaSuccess) return fail(CHD_ERR_CUDA, std::string("chd_graph_launch: ") + cudaGetErrorString(e));
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 void chd_graph_destroy(chd_graph *g) { delete g; }
 
-int chd_relinearize(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *key) {
+int chd_relinearize(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *key) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(key);
   return ctx->c->relinearize(res->ct, a->ct, key->k, false);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_relinearize_rescale(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *key) {
+int chd_relinearize_rescale(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *key) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(key);
   return ctx->c->relinearize(res->ct, a->ct, key->k, true);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_mult_key(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *key) {
+int chd_mult_key(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *key) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(key);
   return ctx->c->mult_key(res->ct, a->ct, key->k);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 int chd_hmult(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_ciphertext *b,
-              const chd_evk *mult_key, int rescale) {
+              const chd_evk *mult_key, int rescale) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(b);
   CHD_NOTNULL(mult_key);
   return ctx->c->hmult(res->ct, a->ct, b->ct, mult_key->k, rescale != 0);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 int chd_hmult_batch(chd_context *ctx, int count, chd_ciphertext *const *res, const chd_ciphertext *const *a,
-                    const chd_ciphertext *const *b, const chd_evk *mult_key, int rescale) {
+                    const chd_ciphertext *const *b, const chd_evk *mult_key, int rescale) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
@@ -993,36 +1346,52 @@ int chd_hmult_batch(chd_context *ctx, int count, chd_ciphertext *const *res, con
     y[i] = &b[i]->ct;
   }
   return ctx->c->hmult_batch(count, r.data(), x.data(), y.data(), mult_key->k, rescale != 0);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_hrot(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *rot_key, int rot_dist) {
+int chd_hrot(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *rot_key, int rot_dist) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(rot_key);
   return ctx->c->hrot(res->ct, a->ct, rot_key->k, rot_dist);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_hconj(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *conj_key) {
+int chd_hconj(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *conj_key) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(conj_key);
   return ctx->c->hconj(res->ct, a->ct, conj_key->k);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 int chd_hrot_add(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_ciphertext *b,
-                 const chd_evk *rot_key, int rot_dist) {
+                 const chd_evk *rot_key, int rot_dist) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(b);
   CHD_NOTNULL(rot_key);
   return ctx->c->hrot_add(res->ct, a->ct, b->ct, rot_key->k, rot_dist);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 int chd_hoisted_rotate(chd_context *ctx, const chd_ciphertext *a, int count, const int *rot_dists,
-                       const chd_evk *const *rot_keys, chd_ciphertext *const *out) {
+                       const chd_evk *const *rot_keys, chd_ciphertext *const *out) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(a);
   CHD_NOTNULL(rot_dists);
@@ -1037,16 +1406,24 @@ int chd_hoisted_rotate(chd_context *ctx, const chd_ciphertext *a, int count, con
     o[i] = &out[i]->ct;
   }
   return ctx->c->hoisted_rotate(a->ct, count, rot_dists, k.data(), o.data());
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_moddown(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) {
+int chd_moddown(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   return ctx->c->moddown_ct(res->ct, a->ct);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_ntt(chd_context *ctx, int num_main, int num_ter, int num_aux, uint32_t *data_dev, int mont, int count) {
+int chd_ntt(chd_context *ctx, int num_main, int num_ter, int num_aux, uint32_t *data_dev, int mont, int count) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(data_dev);
   NP np{num_main, num_ter, num_aux};
@@ -1055,9 +1432,13 @@ int chd_ntt(chd_context *ctx, int num_main, int num_ter, int num_aux, uint32_t *
       num_aux > P.alpha || count < 1)
     return fail(CHD_ERR_INVALID_ARG, "chd_ntt: invalid prime counts");
   return ctx->c->ntt(np, data_dev, mont != 0, count, static_cast<size_t>(np.total()) * P.n);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_intt(chd_context *ctx, int num_main, int num_ter, int num_aux, uint32_t *data_dev, int mont, int count) {
+int chd_intt(chd_context *ctx, int num_main, int num_ter, int num_aux, uint32_t *data_dev, int mont, int count) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(data_dev);
   NP np{num_main, num_ter, num_aux};
@@ -1066,9 +1447,13 @@ int chd_intt(chd_context *ctx, int num_main, int num_ter, int num_aux, uint32_t 
       num_aux > P.alpha || count < 1)
     return fail(CHD_ERR_INVALID_ARG, "chd_intt: invalid prime counts");
   return ctx->c->intt(np, data_dev, mont != 0, count, static_cast<size_t>(np.total()) * P.n);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_modup_raw(chd_context *ctx, int level, const uint32_t *src_dev, uint32_t *dst_dev) {
+int chd_modup_raw(chd_context *ctx, int level, const uint32_t *src_dev, uint32_t *dst_dev) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(src_dev);
   CHD_NOTNULL(dst_dev);
@@ -1079,9 +1464,13 @@ int chd_modup_raw(chd_context *ctx, int level, const uint32_t *src_dev, uint32_t
   std::vector<uint32_t *> d(m.beta);
   for (int i = 0; i < m.beta; i++) d[i] = dst_dev + i * stride;
   return C.modup(level, src_dev, d.data());
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-int chd_moddown_raw(chd_context *ctx, int level, int type, const uint32_t *src_dev, uint32_t *dst_dev, int npoly) {
+int chd_moddown_raw(chd_context *ctx, int level, int type, const uint32_t *src_dev, uint32_t *dst_dev, int npoly) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(src_dev);
   CHD_NOTNULL(dst_dev);
@@ -1102,6 +1491,10 @@ int chd_moddown_raw(chd_context *ctx, int level, int type, const uint32_t *src_d
   Context::MDType t = type == CHD_MODDOWN ? Context::MDType::kModDown
                       : type == CHD_RESCALE ? Context::MDType::kRescale : Context::MDType::kModDownRescale;
   return C.moddown(level, t, s.data(), d.data(), npoly);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 namespace {
@@ -1130,7 +1523,7 @@ int bconv_table(const Context &C, const int *src_gidx, int K, const int *dst_gid
 }  // namespace
 
 int chd_bconv_raw(chd_context *ctx, const int32_t *xt_dev, const int *src_gidx, int K, const int *dst_gidx, int M,
-                  uint32_t *out_dev) {
+                  uint32_t *out_dev) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(xt_dev);
   CHD_NOTNULL(src_gidx);
@@ -1147,10 +1540,14 @@ int chd_bconv_raw(chd_context *ctx, const int32_t *xt_dev, const int *src_gidx, 
   cudaStreamSynchronize(C.stream);
   cudaFree(dt);
   return rc;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 int chd_bconv_batch(chd_context *ctx, int engine, int npoly, const int32_t *xt_dev, const int *src_gidx, int K,
-                    const int *dst_gidx, int M, uint32_t *out_dev) {
+                    const int *dst_gidx, int M, uint32_t *out_dev) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(src_gidx);
   CHD_NOTNULL(dst_gidx);
@@ -1163,10 +1560,14 @@ int chd_bconv_batch(chd_context *ctx, int engine, int npoly, const int32_t *xt_d
   int rc = bconv_table(C, src_gidx, K, dst_gidx, M, &t, "chd_bconv_batch");
   if (rc != CHD_OK) return rc;
   return C.bconv_many(engine, npoly, xt_dev, K, t, dst_gidx, M, out_dev);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 int chd_params_level_consts(const char *json_text, int level, int kind, int digit, uint32_t *c1, int32_t *table,
-                            uint32_t *inv, uint32_t *pad, int *dims) {
+                            uint32_t *inv, uint32_t *pad, int *dims) try {
   CHD_NOTNULL(json_text);
   CHD_NOTNULL(dims);
   ParamSpec spec;
@@ -1221,6 +1622,10 @@ int chd_params_level_consts(const char *json_text, int level, int kind, int digi
   if (vi && inv) std::copy(vi->begin(), vi->end(), inv);
   if (vp && pad) std::copy(vp->begin(), vp->end(), pad);
   return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
 }  // extern "C"

@@ -463,6 +463,16 @@ class Context {
   Status run_program_batch(const Program &prog, int count, std::vector<DeviceCt> *const *R, const ProgKeys &keys,
                            const std::vector<const LTPlan *> *lts);
   bool mult_unsafe_compatible(int l1, int l2) const;
+  // the remaining public Context operations (ops_ext.cu)
+  Status copy_ct(DeviceCt &res, const DeviceCt &a);
+  Status mult_unsafe(DeviceCt &res, const DeviceCt &a, const DeviceCt &b, int level);
+  Status mult_unsafe_const(DeviceCt &res, const DeviceCt &a, const uint32_t *cx, int const_level, double const_scale,
+                           int level);
+  Status mad_unsafe(DeviceCt &res, const DeviceCt &a, const uint32_t *cx, int const_level, double const_scale);
+  Status permute_ct(DeviceCt &res, const DeviceCt &a, int rot_dist, bool conjugate);
+  Status hconj_add(DeviceCt &res, const DeviceCt &a, const DeviceCt &b, const DeviceEvk &key);
+  Status level_down(DeviceCt &res, const DeviceCt &a, int target_level);
+  Status mult_key_no_moddown(DeviceCt &accum, const DeviceCt &a, const DeviceEvk &key);
   // sizes the registers of a program (plus two spares) at top-level capacity
   Status program_regs(const Program &prog, std::vector<DeviceCt> &regs);
   // BootContext (bootplan.cu): prepare full-slot bootstrapping with

@@ -38,6 +38,7 @@ extern "C" {
 #define CHD_ERR_UNSUPPORTED 6
 #define CHD_ERR_KEY 7
 #define CHD_ERR_PARSE 8
+#define CHD_ERR_INTERNAL 9 /* an unexpected failure inside the library (message in chd_last_error) */
 
 /* ModDown family selector for chd_moddown_raw */
 #define CHD_MODDOWN 0
@@ -139,6 +140,44 @@ int chd_hmult(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a,
 int chd_hmult_batch(chd_context *ctx, int count, chd_ciphertext *const *res,
                     const chd_ciphertext *const *a, const chd_ciphertext *const *b,
                     const chd_evk *mult_key, int rescale);
+/* Context::Copy (Context.cpp:132-143) */
+int chd_copy(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a);
+/* Context::MultUnsafe(Ct, Ct, Ct, level) (Context.cpp:370-412): tensor
+ * product at `level` (-1: the lower input level), reading each input past
+ * its extra terminal primes; result carries rx.  Inputs without rx or aux. */
+int chd_mult_unsafe(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_ciphertext *b,
+                    int level);
+/* Context::MultUnsafe(Ct, Ct, Const, level) (Context.cpp:458-500): cx = the
+ * constant's Montgomery residues over the q primes of const_level (as
+ * chd_encode_const writes them), const_scale its scale; result at `level`
+ * (-1: the lower of the two levels). */
+int chd_mult_unsafe_const(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *cx,
+                          int const_level, double const_scale, int level);
+/* Context::MadUnsafe (Context.cpp:873-915): res += a * const over res's
+ * primes; res's scale must equal a's times const_scale, the slot counts
+ * match, res gains a zero rx when a has one. */
+int chd_mad_unsafe(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *cx,
+                   int const_level, double const_scale);
+/* Context::Permute / PermuteConjugate (Context.cpp:502-547): the automorphism
+ * alone (use after chd_mult_key); rotation by 0 copies. */
+int chd_permute(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, int rot_dist);
+int chd_permute_conjugate(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a);
+/* Context::HConjAdd (Context.cpp:836-860): res = HConj(a) + b */
+int chd_hconj_add(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_ciphertext *b,
+                  const chd_evk *conj_key);
+/* Context::LevelDown (Context.cpp:917-929): per level, times the constant 1
+ * at that level's scale, then Rescale, down to target_level */
+int chd_level_down(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, int target_level);
+/* Context::MultKeyNoModDown(Ct, Ct, Evk) (Context.cpp:650-700): the
+ * relinearisation of a (which must carry rx) left in the extended basis Q u P:
+ * ModUp(rx) (.) key + P * (bx, ax); chd_moddown finishes it.  The
+ * reference's branch for an input without rx is empty (the accumulator is
+ * left unset); here that input is an error. */
+int chd_mult_key_no_moddown(chd_context *ctx, chd_ciphertext *accum, const chd_ciphertext *a, const chd_evk *key);
+/* Context::IsMultUnsafeCompatible (Context.cpp:357-368): 1 / 0, -1 for a
+ * null context or a level out of range */
+int chd_mult_unsafe_compatible(const chd_context *ctx, int level1, int level2);
+
 /* Context::HRot / HConj / HRotAdd (Context.cpp:776-830) */
 int chd_hrot(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *rot_key,
              int rot_dist);

@@ -171,6 +171,35 @@ class Context {
   void HRotAdd(Ct &res, const Ct &a, const Ct &b, const Evk &rot_key, int rot_dist) const {
     check(chd_hrot_add(c_, res.raw(), a.raw(), b.raw(), rot_key.raw(), rot_dist));
   }
+  void Copy(Ct &res, const Ct &a) const { check(chd_copy(c_, res.raw(), a.raw())); }
+  // MultUnsafe at a designated level (-1: the lower input level)
+  void MultUnsafe(Ct &res, const Ct &a, const Ct &b, int level = -1) const {
+    check(chd_mult_unsafe(c_, res.raw(), a.raw(), b.raw(), level));
+  }
+  // constants: Montgomery residues over const_level's q primes (EncodeConstant)
+  void MultUnsafe(Ct &res, const Ct &a, const std::vector<uint32_t> &cx, int const_level, double const_scale,
+                  int level = -1) const {
+    check(chd_mult_unsafe_const(c_, res.raw(), a.raw(), cx.data(), const_level, const_scale, level));
+  }
+  void MadUnsafe(Ct &res, const Ct &a, const std::vector<uint32_t> &cx, int const_level, double const_scale) const {
+    check(chd_mad_unsafe(c_, res.raw(), a.raw(), cx.data(), const_level, const_scale));
+  }
+  void Permute(Ct &res, const Ct &a, int rot_dist) const { check(chd_permute(c_, res.raw(), a.raw(), rot_dist)); }
+  void PermuteConjugate(Ct &res, const Ct &a) const { check(chd_permute_conjugate(c_, res.raw(), a.raw())); }
+  void HConjAdd(Ct &res, const Ct &a, const Ct &b, const Evk &conj_key) const {
+    check(chd_hconj_add(c_, res.raw(), a.raw(), b.raw(), conj_key.raw()));
+  }
+  void LevelDown(Ct &res, const Ct &a, int target_level) const {
+    check(chd_level_down(c_, res.raw(), a.raw(), target_level));
+  }
+  void MultKeyNoModDown(Ct &accum, const Ct &a, const Evk &key) const {
+    check(chd_mult_key_no_moddown(c_, accum.raw(), a.raw(), key.raw()));
+  }
+  bool IsMultUnsafeCompatible(int level1, int level2) const {
+    const int r = chd_mult_unsafe_compatible(c_, level1, level2);
+    if (r < 0) throw Error(CHD_ERR_INVALID_ARG, "IsMultUnsafeCompatible: invalid level");
+    return r != 0;
+  }
   // batched HMult over independent pairs (one fused pipeline per level)
   void HMultBatch(const std::vector<Ct *> &res, const std::vector<const Ct *> &a,
                   const std::vector<const Ct *> &b, const Evk &mult_key, bool rescale = true) const {

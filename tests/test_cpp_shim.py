@@ -29,6 +29,17 @@ void unused_paths(cheddar_b200::Context &ctx, const cheddar_b200::EvaluationKey 
   bc.BootBatch({&b}, {&a}, m);
   std::vector<uint32_t> cx = ctx.EncodeConstant(0, 1.0, 0.5);
   ctx.SetKeySwitchEngine(CHD_BCONV_TENSOR_CORE);
+  ctx.Copy(b, a);
+  ctx.MultUnsafe(b, a, a, 3);
+  ctx.MultUnsafe(b, a, cx, 0, 1.0);
+  ctx.MadUnsafe(b, a, cx, 0, 1.0);
+  ctx.Permute(b, a, 3);
+  ctx.PermuteConjugate(b, a);
+  ctx.HConjAdd(b, a, a, k);
+  ctx.LevelDown(b, a, 0);
+  ctx.MultKeyNoModDown(b, a, k);
+  bool compat = ctx.IsMultUnsafeCompatible(1, 2);
+  (void)compat;
   int eng = ctx.KeySwitchEngine();
   ctx.HMultBatch({&b}, {&a}, {&a}, k, true);
   ctx.BeginGraph();
