@@ -68,6 +68,12 @@ def lib():
         "chd_level_down": (i, [vp, vp, vp, i]),
         "chd_mult_key_no_moddown": (i, [vp, vp, vp, vp]),
         "chd_mult_unsafe_compatible": (i, [vp, i, i]),
+        "chd_add_plain": (i, [vp, vp, vp, vp, d]),
+        "chd_sub_plain": (i, [vp, vp, vp, vp, d]),
+        "chd_sub_const": (i, [vp, vp, vp, u32p]),
+        "chd_sub_plain_ct": (i, [vp, vp, vp, d, vp]),
+        "chd_sub_const_ct": (i, [vp, vp, u32p, d, vp]),
+        "chd_mult_unsafe_plain": (i, [vp, vp, vp, vp, i, i, d, i]),
         "chd_get_ks_engine": (i, [vp]),
         "chd_stage_times": (i, [vp, vp, vp]),
         "chd_level_np": (i, [vp, i, C.POINTER(i), C.POINTER(i)]),
@@ -333,6 +339,53 @@ class Context:
         _check(lib().chd_add_const(self.ptr, res.ptr, a.ptr, cx.ctypes.data))
         return res
 
+    def SubConst(self, a, cx, res=None):
+        """a - c (Context::Sub(Ct, Ct, Const))."""
+        res = self._new(res)
+        cx = np.ascontiguousarray(cx, dtype=np.uint32)
+        _check(lib().chd_sub_const(self.ptr, res.ptr, a.ptr, cx.ctypes.data))
+        return res
+
+    def SubConstCt(self, cx, const_scale, b, res=None):
+        """c - b (Context::Sub(Ct, Const, Ct))."""
+        res = self._new(res)
+        cx = np.ascontiguousarray(cx, dtype=np.uint32)
+        _check(lib().chd_sub_const_ct(self.ptr, res.ptr, cx.ctypes.data, float(const_scale), b.ptr))
+        return res
+
+    def MultPlain(self, a, pt, pt_scale, res=None):
+        """a (.) pt (Context::Mult(Ct, Ct, Pt)); pt: device residues over a's
+        primes, as encode() gives them."""
+        res = self._new(res)
+        _check(lib().chd_mult_plain(self.ptr, res.ptr, a.ptr, _ptr(pt), float(pt_scale)))
+        return res
+
+    def AddPlain(self, a, pt, pt_scale, res=None):
+        """a + pt (Context::Add(Ct, Ct, Pt)); the scales must match."""
+        res = self._new(res)
+        _check(lib().chd_add_plain(self.ptr, res.ptr, a.ptr, _ptr(pt), float(pt_scale)))
+        return res
+
+    def SubPlain(self, a, pt, pt_scale, res=None):
+        """a - pt (Context::Sub(Ct, Ct, Pt))."""
+        res = self._new(res)
+        _check(lib().chd_sub_plain(self.ptr, res.ptr, a.ptr, _ptr(pt), float(pt_scale)))
+        return res
+
+    def SubPlainCt(self, pt, pt_scale, b, res=None):
+        """pt - b (Context::Sub(Ct, Pt, Ct))."""
+        res = self._new(res)
+        _check(lib().chd_sub_plain_ct(self.ptr, res.ptr, _ptr(pt), float(pt_scale), b.ptr))
+        return res
+
+    def MultUnsafePlain(self, a, pt, pt_level, pt_scale, pt_num_aux=0, level=-1, res=None):
+        """a (.) pt at `level` (-1: the lower level), reading both past their
+        extra terminal primes (Context::MultUnsafe(Ct, Ct, Pt, level))."""
+        res = self._new(res)
+        _check(lib().chd_mult_unsafe_plain(self.ptr, res.ptr, a.ptr, _ptr(pt), pt_level, pt_num_aux,
+                                           float(pt_scale), level))
+        return res
+
     def MultImaginaryUnit(self, a, res=None):
         res = self._new(res)
         _check(lib().chd_mult_imaginary_unit(self.ptr, res.ptr, a.ptr))
@@ -433,7 +486,8 @@ class Context:
         return res
 
     def MultKeyNoModDown(self, a, key, res=None):
-        """Relinearisation of a (with rx) left in the extended basis."""
+        """Key switch of a left in the extended basis (relinearisation when a
+        carries rx, else the key switch of a rotation)."""
         res = self._new(res)
         _check(lib().chd_mult_key_no_moddown(self.ptr, res.ptr, a.ptr, key.ptr))
         return res

@@ -265,6 +265,85 @@ int chd_mult_unsafe_compatible(const chd_context *ctx, int level1, int level2) t
   if (level1 < 0 || level2 < 0 || level1 > ml || level2 > ml) return -1;
   return ctx->c->mult_unsafe_compatible(level1, level2) ? 1 : 0;
 } catch (const std::exception &e) {
+  fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+  return -1;
+} catch (...) {
+  fail(CHD_ERR_INTERNAL, "internal error");
+  return -1;
+}
+
+int chd_add_plain(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *pt_dev,
+                  double pt_scale) try {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  CHD_NOTNULL(pt_dev);
+  return ctx->c->add_sub_plain(res->ct, a->ct, pt_dev, pt_scale, false);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
+}
+
+int chd_sub_plain(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *pt_dev,
+                  double pt_scale) try {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  CHD_NOTNULL(pt_dev);
+  return ctx->c->add_sub_plain(res->ct, a->ct, pt_dev, pt_scale, true);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
+}
+
+int chd_sub_const(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *cx) try {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  CHD_NOTNULL(cx);
+  return ctx->c->sub_const(res->ct, a->ct, cx);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
+}
+
+int chd_sub_plain_ct(chd_context *ctx, chd_ciphertext *res, const uint32_t *pt_dev, double pt_scale,
+                     const chd_ciphertext *b) try {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(pt_dev);
+  CHD_NOTNULL(b);
+  return ctx->c->sub_from(res->ct, pt_dev, nullptr, pt_scale, b->ct);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
+}
+
+int chd_sub_const_ct(chd_context *ctx, chd_ciphertext *res, const uint32_t *cx, double const_scale,
+                     const chd_ciphertext *b) try {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(cx);
+  CHD_NOTNULL(b);
+  return ctx->c->sub_from(res->ct, nullptr, cx, const_scale, b->ct);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
+}
+
+int chd_mult_unsafe_plain(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *pt_dev,
+                          int pt_level, int pt_num_aux, double pt_scale, int level) try {
+  CHD_NOTNULL(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  CHD_NOTNULL(pt_dev);
+  return ctx->c->mult_unsafe_plain(res->ct, a->ct, pt_dev, pt_level, pt_num_aux, pt_scale, level);
+} catch (const std::exception &e) {
   return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
 } catch (...) {
   return fail(CHD_ERR_INTERNAL, "internal error");

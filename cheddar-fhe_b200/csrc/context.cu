@@ -2094,7 +2094,8 @@ Status Context::hoisted_rotate_batch(int count, const DeviceCt *const *a, int R,
 }
 
 // ------------------------------------------------------- element-wise ops
-namespace {
+// one element-wise op over `parts` parts of every row of np (row r of
+// part p at dst[p] + r * N, likewise a / b), per-row constant k[r]
 Status elem_parts(Context &C, ElemOp op, const NP &np, int parts, uint32_t *const *dst, const uint32_t *const *a,
                   const uint32_t *const *b, const uint32_t *k) {
   const int n = C.P->n, tot = np.total();
@@ -2124,7 +2125,6 @@ Status elem_parts(Context &C, ElemOp op, const NP &np, int parts, uint32_t *cons
   }
   return kOk;
 }
-}  // namespace
 
 Status Context::add(DeviceCt &res, const DeviceCt &a, const DeviceCt &b) {
   // Context.cpp:145-172
@@ -2133,6 +2133,14 @@ Status Context::add(DeviceCt &res, const DeviceCt &a, const DeviceCt &b) {
   const DeviceCt *rx_src = a.has_rx ? &a : (b.has_rx ? &b : nullptr);
   const uint32_t *keep_rx = (!both_rx && rx_src) ? rx_src->rx : nullptr;
   const bool out_rx = a.has_rx || b.has_rx;
+  if ((&res == &a || &res == &b) && out_rx && !res.rx && res.owned) {
+    // the result needs an rx buffer its aliased input lacks: growing it
+    // would free the input before it is read
+    DeviceCt tmp;
+    CHD_TRY(add(tmp, a, b));
+    res = std::move(tmp);
+    return kOk;
+  }
   const NP np = a.np;
   const uint32_t *pa[3] = {a.bx, a.ax, a.rx}, *pb[3] = {b.bx, b.ax, b.rx};
   const double sc = a.scale;
@@ -2148,16 +2156,34 @@ Status Context::add(DeviceCt &res, const DeviceCt &a, const DeviceCt &b) {
 }
 
 Status Context::sub(DeviceCt &res, const DeviceCt &a, const DeviceCt &b) {
+  // Context.cpp:205-229: with rx on one side only, res.rx = a.rx or -b.rx
   CHD_CHECK(a.np == b.np, kErrShape, "Sub: level mismatch");
-  CHD_CHECK(a.has_rx == b.has_rx, kErrUnsupported, "Sub: mixed rx operands are not supported");
+  const bool both_rx = a.has_rx && b.has_rx;
+  const bool out_rx = a.has_rx || b.has_rx;
+  const uint32_t *only_rx = (!both_rx && out_rx) ? (a.has_rx ? a.rx : b.rx) : nullptr;
+  const bool neg_rx = !both_rx && b.has_rx;
+  if ((&res == &a || &res == &b) && out_rx && !res.rx && res.owned) {
+    // the result needs an rx buffer its aliased input lacks: growing it
+    // would free the input before it is read
+    DeviceCt tmp;
+    CHD_TRY(sub(tmp, a, b));
+    res = std::move(tmp);
+    return kOk;
+  }
   const NP np = a.np;
   const uint32_t *pa[3] = {a.bx, a.ax, a.rx}, *pb[3] = {b.bx, b.ax, b.rx};
   const double sc = a.scale;
   const int slots = std::max(a.num_slots, b.num_slots);
-  const bool rx = a.has_rx;
-  CHD_TRY(res.reserve(np, rx, P->n));
+  CHD_TRY(res.reserve(np, out_rx, P->n));
   uint32_t *pd[3] = {res.bx, res.ax, res.rx};
-  CHD_TRY(elem_parts(*this, ElemOp::kSub, np, rx ? 3 : 2, pd, pa, pb, nullptr));
+  CHD_TRY(elem_parts(*this, ElemOp::kSub, np, both_rx ? 3 : 2, pd, pa, pb, nullptr));
+  if (neg_rx) {
+    const uint32_t *src[1] = {only_rx};
+    uint32_t *dst[1] = {res.rx};
+    CHD_TRY(elem_parts(*this, ElemOp::kNeg, np, 1, dst, src, nullptr, nullptr));
+  } else if (only_rx && only_rx != res.rx) {
+    cudaMemcpyAsync(res.rx, only_rx, static_cast<size_t>(np.total()) * P->n * 4, cudaMemcpyDeviceToDevice, stream);
+  }
   res.scale = sc;
   res.num_slots = slots;
   return kOk;

@@ -473,6 +473,11 @@ class Context {
   Status hconj_add(DeviceCt &res, const DeviceCt &a, const DeviceCt &b, const DeviceEvk &key);
   Status level_down(DeviceCt &res, const DeviceCt &a, int target_level);
   Status mult_key_no_moddown(DeviceCt &accum, const DeviceCt &a, const DeviceEvk &key);
+  Status add_sub_plain(DeviceCt &res, const DeviceCt &a, const uint32_t *pt, double pscale, bool subtract);
+  Status sub_const(DeviceCt &res, const DeviceCt &a, const uint32_t *cx);
+  Status sub_from(DeviceCt &res, const uint32_t *pt, const uint32_t *cx, double scale, const DeviceCt &b);
+  Status mult_unsafe_plain(DeviceCt &res, const DeviceCt &a, const uint32_t *pt, int pt_level, int pt_aux,
+                           double pscale, int level);
   // sizes the registers of a program (plus two spares) at top-level capacity
   Status program_regs(const Program &prog, std::vector<DeviceCt> &regs);
   // BootContext (bootplan.cu): prepare full-slot bootstrapping with
@@ -515,5 +520,10 @@ class Context {
                          const DeviceEvk &key, uint32_t *acc_b, uint32_t *acc_a);
   Status key_switch_many(int level, int count, const KSJob *jobs, const DeviceEvk &key);
 };
+
+// one element-wise op over `parts` parts of every row of np (row r of part
+// p at dst[p] + r * N, likewise a / b), per-row constant k[r]
+Status elem_parts(Context &C, ElemOp op, const NP &np, int parts, uint32_t *const *dst, const uint32_t *const *a,
+                  const uint32_t *const *b, const uint32_t *k);
 
 }  // namespace chd

@@ -3,7 +3,10 @@
 //   Copy (:132-143), MultUnsafe Ct x Ct and Ct x Const at a target level
 //   (:357-500, reading past the inputs' extra terminal primes), MadUnsafe
 //   (:873-915), Permute / PermuteConjugate (:502-547), HConjAdd (:836-860),
-//   LevelDown (:917-929) and MultKeyNoModDown (:650-700);
+//   LevelDown (:917-929), MultKeyNoModDown (:650-700), Add / Sub with a
+//   plaintext (:171-186, :231-246), Sub of a constant (:248-263), the
+//   reversed Sub(Pt, Ct) / Sub(Const, Ct) (:265-304) and MultUnsafe Ct x Pt
+//   (:414-456);
 //   IsMultUnsafeCompatible (:357-368) is in evalmod.cu.
 #include <cmath>
 
@@ -48,6 +51,9 @@ void caccum(Context &C, DeviceCt &dst, const NP &np, int parts, const std::vecto
 }
 
 bool subset(const NP &sub, const NP &sup) { return sub.main <= sup.main && sub.ter <= sup.ter; }
+
+// Context.cpp:54-60 (AssertSameScale)
+bool same_scale(double s1, double s2) { return std::fabs(s1 - s2) < 1e-12 * s1; }
 
 }  // namespace
 
@@ -231,17 +237,115 @@ Status Context::level_down(DeviceCt &res, const DeviceCt &a, int target_level) {
 Status Context::mult_key_no_moddown(DeviceCt &accum, const DeviceCt &a, const DeviceEvk &key) {
   CHD_CHECK(a.np.aux == 0, kErrShape, "MultKeyNoModDown is not supported for ciphertexts with p primes");
   CHD_CHECK(&accum != &a, kErrInvalidArg, "In-place operation is not supported for MultKeyNoModDown");
-  CHD_CHECK(a.has_rx, kErrShape,
-            "MultKeyNoModDown needs a ciphertext with rx (relinearisation without ModDown)");
   const int level = P->np_to_level(a.np);
   CHD_CHECK(level >= 0, kErrInvalidLevel, "MultKeyNoModDown: invalid level");
   const double sc = a.scale;
   const int slots = a.num_slots;
   CHD_TRY(accum.reserve(P->level_np(level, P->alpha), false, P->n));
-  CHD_TRY(key_switch_core(level, a.bx, a.ax, a.rx, key, accum.bx, accum.ax));
+  // with rx: ModUp(rx) (.) key + P * (bx, ax) (relinearisation); without:
+  // ModUp(ax) (.) key + (P * bx, 0) (the key switch of a rotation)
+  if (a.has_rx)
+    CHD_TRY(key_switch_core(level, a.bx, a.ax, a.rx, key, accum.bx, accum.ax));
+  else
+    CHD_TRY(key_switch_core(level, a.bx, nullptr, a.ax, key, accum.bx, accum.ax));
   accum.scale = sc;
   accum.num_slots = slots;
   return check_cuda("mult key no moddown");
+}
+
+// res.bx = a.bx (+/-) pt, ax and rx copied (Context.cpp:171-186, 231-246)
+Status Context::add_sub_plain(DeviceCt &res, const DeviceCt &a, const uint32_t *pt, double pscale, bool subtract) {
+  CHD_CHECK(same_scale(a.scale, pscale), kErrInvalidArg, "Scale mismatch");
+  const NP np = a.np;
+  const bool rx = a.has_rx;
+  const double sc = a.scale;
+  const int slots = a.num_slots;
+  const uint32_t *pa[1] = {a.bx}, *pb[1] = {pt};
+  const uint32_t *keep[2] = {a.ax, a.rx};
+  CHD_TRY(res.reserve(np, rx, P->n));
+  uint32_t *pd[1] = {res.bx};
+  CHD_TRY(elem_parts(*this, subtract ? ElemOp::kSub : ElemOp::kAdd, np, 1, pd, pa, pb, nullptr));
+  const size_t bytes = static_cast<size_t>(np.total()) * P->n * 4;
+  if (keep[0] != res.ax) cudaMemcpyAsync(res.ax, keep[0], bytes, cudaMemcpyDeviceToDevice, stream);
+  if (rx && keep[1] != res.rx) cudaMemcpyAsync(res.rx, keep[1], bytes, cudaMemcpyDeviceToDevice, stream);
+  res.scale = sc;
+  res.num_slots = slots;
+  return check_cuda("add / sub plain");
+}
+
+// res.bx = a.bx - c, ax and rx copied (Context.cpp:248-263)
+Status Context::sub_const(DeviceCt &res, const DeviceCt &a, const uint32_t *cx) {
+  const NP np = a.np;
+  const bool rx = a.has_rx;
+  const double sc = a.scale;
+  const int slots = a.num_slots;
+  const uint32_t *pa[1] = {a.bx};
+  const uint32_t *keep[2] = {a.ax, a.rx};
+  CHD_TRY(res.reserve(np, rx, P->n));
+  uint32_t *pd[1] = {res.bx};
+  CHD_TRY(elem_parts(*this, ElemOp::kSubConst, np, 1, pd, pa, nullptr, cx));
+  const size_t bytes = static_cast<size_t>(np.total()) * P->n * 4;
+  if (keep[0] != res.ax) cudaMemcpyAsync(res.ax, keep[0], bytes, cudaMemcpyDeviceToDevice, stream);
+  if (rx && keep[1] != res.rx) cudaMemcpyAsync(res.rx, keep[1], bytes, cudaMemcpyDeviceToDevice, stream);
+  res.scale = sc;
+  res.num_slots = slots;
+  return check_cuda("sub const");
+}
+
+// res = pt - b or c - b: bx = pt - b.bx (c - b.bx), ax = -b.ax, rx = -b.rx
+// (Context.cpp:265-304); exactly one of pt / cx is given
+Status Context::sub_from(DeviceCt &res, const uint32_t *pt, const uint32_t *cx, double scale, const DeviceCt &b) {
+  CHD_CHECK((pt != nullptr) != (cx != nullptr), kErrInvalidArg, "Sub: give a plaintext or a constant");
+  CHD_CHECK(same_scale(scale, b.scale), kErrInvalidArg, "Scale mismatch");
+  const NP np = b.np;
+  const bool rx = b.has_rx;
+  const int slots = b.num_slots;
+  const uint32_t *pbx[1] = {b.bx}, *ppt[1] = {pt};
+  const uint32_t *prest[2] = {b.ax, b.rx};
+  CHD_TRY(res.reserve(np, rx, P->n));
+  uint32_t *pd[1] = {res.bx};
+  if (pt)
+    CHD_TRY(elem_parts(*this, ElemOp::kSub, np, 1, pd, ppt, pbx, nullptr));
+  else
+    CHD_TRY(elem_parts(*this, ElemOp::kSubOppConst, np, 1, pd, pbx, nullptr, cx));
+  uint32_t *prd[2] = {res.ax, res.rx};
+  CHD_TRY(elem_parts(*this, ElemOp::kNeg, np, rx ? 2 : 1, prd, prest, nullptr, nullptr));
+  res.scale = scale;
+  res.num_slots = slots;
+  return check_cuda("sub from");
+}
+
+// Context.cpp:414-456: res = a (.) pt at `level` (-1: the lower level), both
+// read past their extra terminal primes; aux primes: the fewer of the two
+Status Context::mult_unsafe_plain(DeviceCt &res, const DeviceCt &a, const uint32_t *pt, int pt_level, int pt_aux,
+                                  double pscale, int level) {
+  const int la = P->np_to_level(NP{a.np.main, a.np.ter, 0});
+  CHD_CHECK(la >= 0, kErrInvalidLevel, "MultUnsafe: invalid input level");
+  CHD_CHECK(pt_level >= 0 && pt_level <= P->max_level, kErrInvalidLevel, "MultUnsafe: invalid plaintext level");
+  CHD_CHECK(pt_aux >= 0 && pt_aux <= P->alpha, kErrShape, "MultUnsafe: invalid plaintext aux prime count");
+  if (level == -1) level = std::min(la, pt_level);
+  CHD_CHECK(level >= 0 && level <= P->max_level, kErrInvalidLevel, "MultUnsafe: invalid target level");
+  const int aux = std::min(a.np.aux, pt_aux);
+  const NP np = P->level_np(level, aux), pnp = P->level_np(pt_level, pt_aux);
+  CHD_CHECK(subset(np, a.np) && subset(np, pnp), kErrShape, "Incompatible levels for MultUnsafe Ct x Pt");
+  if (&res == &a && la != level) {
+    DeviceCt tmp;
+    CHD_TRY(mult_unsafe_plain(tmp, a, pt, pt_level, pt_aux, pscale, level));
+    res = std::move(tmp);
+    return kOk;
+  }
+  const bool rx = a.has_rx;
+  const double sc = a.scale * pscale;
+  const int slots = a.num_slots;
+  const size_t n = P->n, fa = (a.np.ter - np.ter) * n, fp = (pnp.ter - np.ter) * n;
+  const uint32_t *pa[3] = {a.bx + fa, a.ax + fa, rx ? a.rx + fa : nullptr};
+  const uint32_t *pp[3] = {pt + fp, pt + fp, pt + fp};
+  CHD_TRY(res.reserve(np, rx, P->n));
+  uint32_t *pd[3] = {res.bx, res.ax, res.rx};
+  CHD_TRY(elem_parts(*this, ElemOp::kMult, np, rx ? 3 : 2, pd, pa, pp, nullptr));
+  res.scale = sc;
+  res.num_slots = slots;
+  return check_cuda("mult unsafe plain");
 }
 
 }  // namespace chd

@@ -169,14 +169,35 @@ int chd_hconj_add(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a
  * at that level's scale, then Rescale, down to target_level */
 int chd_level_down(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, int target_level);
 /* Context::MultKeyNoModDown(Ct, Ct, Evk) (Context.cpp:650-700): the
- * relinearisation of a (which must carry rx) left in the extended basis Q u P:
- * ModUp(rx) (.) key + P * (bx, ax); chd_moddown finishes it.  The
- * reference's branch for an input without rx is empty (the accumulator is
- * left unset); here that input is an error. */
+ * key switch of a left in the extended basis Q u P; with rx (relinearisation):
+ * ModUp(rx) (.) key + P * (bx, ax); chd_moddown finishes it.  Without rx
+ * (a rotation's key switch): ModUp(ax) (.) key + (P * bx, 0). */
 int chd_mult_key_no_moddown(chd_context *ctx, chd_ciphertext *accum, const chd_ciphertext *a, const chd_evk *key);
 /* Context::IsMultUnsafeCompatible (Context.cpp:357-368): 1 / 0, -1 for a
  * null context or a level out of range */
 int chd_mult_unsafe_compatible(const chd_context *ctx, int level1, int level2);
+/* Context::Add(Ct, Ct, Pt) / Sub(Ct, Ct, Pt) (Context.cpp:171-186,
+ * 231-246): res.bx = a.bx +/- pt, ax and rx copied; pt_dev = [num_q + num_aux
+ * of a][N] device residues, pt_scale must equal a's scale (relative 1e-12). */
+int chd_add_plain(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *pt_dev,
+                  double pt_scale);
+int chd_sub_plain(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *pt_dev,
+                  double pt_scale);
+/* Context::Sub(Ct, Ct, Const) (Context.cpp:248-263): res.bx = a.bx - c */
+int chd_sub_const(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *cx);
+/* Context::Sub(Ct, Pt, Ct) / Sub(Ct, Const, Ct) (Context.cpp:265-304):
+ * res = pt - b (c - b): bx = pt - b.bx, ax = -b.ax, rx = -b.rx; the
+ * plaintext's / constant's scale must equal b's and becomes res's. */
+int chd_sub_plain_ct(chd_context *ctx, chd_ciphertext *res, const uint32_t *pt_dev, double pt_scale,
+                     const chd_ciphertext *b);
+int chd_sub_const_ct(chd_context *ctx, chd_ciphertext *res, const uint32_t *cx, double const_scale,
+                     const chd_ciphertext *b);
+/* Context::MultUnsafe(Ct, Ct, Pt, level) (Context.cpp:414-456): pt_dev =
+ * [num_q(pt_level) + pt_num_aux][N] (as chd_encode writes it); result at
+ * `level` (-1: the lower level) with the fewer aux primes of the two, both
+ * read past their extra terminal primes. */
+int chd_mult_unsafe_plain(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *pt_dev,
+                          int pt_level, int pt_num_aux, double pt_scale, int level);
 
 /* Context::HRot / HConj / HRotAdd (Context.cpp:776-830) */
 int chd_hrot(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *rot_key,

@@ -195,6 +195,36 @@ class Context {
   void MultKeyNoModDown(Ct &accum, const Ct &a, const Evk &key) const {
     check(chd_mult_key_no_moddown(c_, accum.raw(), a.raw(), key.raw()));
   }
+  // plaintexts: device residues over the ciphertext's primes (chd_encode)
+  void Add(Ct &res, const Ct &a, const uint32_t *pt_dev, double pt_scale) const {
+    check(chd_add_plain(c_, res.raw(), a.raw(), pt_dev, pt_scale));
+  }
+  void Sub(Ct &res, const Ct &a, const uint32_t *pt_dev, double pt_scale) const {
+    check(chd_sub_plain(c_, res.raw(), a.raw(), pt_dev, pt_scale));
+  }
+  void Sub(Ct &res, const uint32_t *pt_dev, double pt_scale, const Ct &b) const {
+    check(chd_sub_plain_ct(c_, res.raw(), pt_dev, pt_scale, b.raw()));
+  }
+  void Mult(Ct &res, const Ct &a, const uint32_t *pt_dev, double pt_scale) const {
+    check(chd_mult_plain(c_, res.raw(), a.raw(), pt_dev, pt_scale));
+  }
+  void MultUnsafe(Ct &res, const Ct &a, const uint32_t *pt_dev, int pt_level, int pt_num_aux, double pt_scale,
+                  int level = -1) const {
+    check(chd_mult_unsafe_plain(c_, res.raw(), a.raw(), pt_dev, pt_level, pt_num_aux, pt_scale, level));
+  }
+  // constants: Montgomery residues per prime (EncodeConstant)
+  void Add(Ct &res, const Ct &a, const std::vector<uint32_t> &cx) const {
+    check(chd_add_const(c_, res.raw(), a.raw(), cx.data()));
+  }
+  void Mult(Ct &res, const Ct &a, const std::vector<uint32_t> &cx, double const_scale) const {
+    check(chd_mult_const(c_, res.raw(), a.raw(), cx.data(), const_scale));
+  }
+  void Sub(Ct &res, const Ct &a, const std::vector<uint32_t> &cx) const {
+    check(chd_sub_const(c_, res.raw(), a.raw(), cx.data()));
+  }
+  void Sub(Ct &res, const std::vector<uint32_t> &cx, double const_scale, const Ct &b) const {
+    check(chd_sub_const_ct(c_, res.raw(), cx.data(), const_scale, b.raw()));
+  }
   bool IsMultUnsafeCompatible(int level1, int level2) const {
     const int r = chd_mult_unsafe_compatible(c_, level1, level2);
     if (r < 0) throw Error(CHD_ERR_INVALID_ARG, "IsMultUnsafeCompatible: invalid level");

@@ -38,6 +38,16 @@ void unused_paths(cheddar_b200::Context &ctx, const cheddar_b200::EvaluationKey 
   ctx.HConjAdd(b, a, a, k);
   ctx.LevelDown(b, a, 0);
   ctx.MultKeyNoModDown(b, a, k);
+  const uint32_t *pt = nullptr;
+  ctx.Add(b, a, pt, 1.0);
+  ctx.Sub(b, a, pt, 1.0);
+  ctx.Sub(b, pt, 1.0, a);
+  ctx.Mult(b, a, pt, 1.0);
+  ctx.MultUnsafe(b, a, pt, 3, 0, 1.0, -1);
+  ctx.Add(b, a, cx);
+  ctx.Mult(b, a, cx, 1.0);
+  ctx.Sub(b, a, cx);
+  ctx.Sub(b, cx, 1.0, a);
   bool compat = ctx.IsMultUnsafeCompatible(1, 2);
   (void)compat;
   int eng = ctx.KeySwitchEngine();

@@ -142,7 +142,7 @@ def test_mult_key_no_moddown(cuda_ok):
     assert acc.info()["num_aux"] == o.alpha and not acc.info()["has_rx"]
     _eq(g.ModDown(acc), o.hmult(lvl, a, b, (kb, ka), rescale=False))
     with pytest.raises(chd.CheddarError):
-        g.MultKeyNoModDown(g.import_ct(lvl, a), key)  # no rx
+        g.MultKeyNoModDown(g.import_ct(lvl, uniform_parts(KS, lvl, 73, num_aux=2), num_aux=2), key)  # aux primes
 
 
 @pytest.mark.parametrize("name,log_n", [(KS, None), (RAT, 12)])
@@ -155,3 +155,108 @@ def test_mult_unsafe_compatible(cuda_ok, name, log_n):
             assert g.IsMultUnsafeCompatible(l1, l2) == want
     with pytest.raises(chd.CheddarError):
         g.IsMultUnsafeCompatible(-1, 0)
+
+
+def _i64(x):
+    return np.asarray(x, dtype=np.int64)
+
+
+def _sub(x, y, Q):
+    return ((_i64(x) - _i64(y)) % Q).astype(np.uint32)
+
+
+def _add(x, y, Q):
+    return ((_i64(x) + _i64(y)) % Q).astype(np.uint32)
+
+
+def _dev(x):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(x, dtype=np.uint32).view(np.int32)).cuda()
+
+
+@pytest.mark.parametrize("name,log_n,level,rx,aux", [(KS, None, 20, False, 0), (KS, None, 13, True, 0),
+                                                     (KS, None, 18, False, 8), (RAT, 12, 9, True, 0)])
+def test_plain_and_const_ops(cuda_ok, name, log_n, level, rx, aux):
+    # Add / Sub / Mult with a plaintext, Sub with a constant, and the
+    # reversed Sub(Pt, Ct) / Sub(Const, Ct) (Context.cpp:171-304, 333-343)
+    o, g = pair(name, log_n)
+    parts = uniform_parts(name, level, 81, nparts=3 if rx else 2, log_n=log_n, num_aux=aux)
+    qs = o.primes(level, aux)
+    Q = _i64(qs)[:, None]
+    pt = o.uniform(90, level, num_aux=aux)
+    ptd = _dev(pt)
+    sc = 2.0 ** 40
+    ga = g.import_ct(level, parts, sc, num_aux=aux)
+    _eq(g.AddPlain(ga, ptd, sc), [_add(parts[0], pt, Q)] + parts[1:])
+    _eq(g.SubPlain(ga, ptd, sc), [_sub(parts[0], pt, Q)] + parts[1:])
+    neg = [_sub(0, p, Q) for p in parts[1:]]
+    _eq(g.SubPlainCt(ptd, sc, ga), [_sub(pt, parts[0], Q)] + neg)
+    pr = g.MultPlain(ga, ptd, 3.0)
+    _eq(pr, [np.stack([mont_mul(p[r], pt[r], int(qs[r])) for r in range(len(qs))]) for p in parts])
+    assert pr.info()["scale"] == sc * 3.0
+    cx = o.encode_const(level, sc, -0.625, num_aux=aux)
+    C = _i64(cx)[:, None]
+    _eq(g.SubConst(ga, cx), [_sub(parts[0], C, Q)] + parts[1:])
+    _eq(g.SubConstCt(cx, sc, ga), [_sub(C, parts[0], Q)] + neg)
+    with pytest.raises(chd.CheddarError):
+        g.AddPlain(ga, ptd, sc * 2)  # scale mismatch
+    with pytest.raises(chd.CheddarError):
+        g.SubConstCt(cx, sc * (1 + 1e-9), ga)
+    # in place: res aliases the ciphertext operand
+    gi = g.import_ct(level, parts, sc, num_aux=aux)
+    g.SubPlainCt(ptd, sc, gi, res=gi)
+    _eq(gi, [_sub(pt, parts[0], Q)] + neg)
+
+
+@pytest.mark.parametrize("name,log_n,la,a_aux,lp,p_aux,level", [
+    (KS, None, 20, 0, 18, 0, -1), (KS, None, 20, 8, 20, 8, -1), (KS, None, 20, 8, 20, 0, -1),
+    (KS, None, 19, 0, 21, 0, 12), (RAT, 12, 9, 0, 8, 0, -1), (RAT, 12, 9, 0, 9, 0, 6), (RAT, 12, 8, 0, 9, 0, 3)])
+def test_mult_unsafe_plain(cuda_ok, name, log_n, la, a_aux, lp, p_aux, level):
+    o, g = pair(name, log_n)
+    tgt = min(la, lp) if level == -1 else level
+    aux = min(a_aux, p_aux)
+    a = uniform_parts(name, la, 101, log_n=log_n, num_aux=a_aux)
+    pt = o.uniform(102, lp, num_aux=p_aux)
+    qs = o.primes(tgt, aux)
+    fa, fp = _front(o, la, tgt), _front(o, lp, tgt)
+    ref = [np.stack([mont_mul(p[fa + r], pt[fp + r], int(qs[r])) for r in range(len(qs))]) for p in a]
+    ga = g.import_ct(la, a, 2.0, num_aux=a_aux)
+    r = g.MultUnsafePlain(ga, _dev(pt), lp, 5.0, pt_num_aux=p_aux, level=level)
+    _eq(r, ref)
+    info = r.info()
+    assert info["num_aux"] == aux and info["scale"] == 10.0
+    # in place with a level change goes through a temporary
+    g.MultUnsafePlain(ga, _dev(pt), lp, 5.0, pt_num_aux=p_aux, level=level, res=ga)
+    _eq(ga, ref)
+
+
+@pytest.mark.parametrize("rot", [5, -1])
+def test_mult_key_no_moddown_rotation(cuda_ok, rot):
+    # without rx: ModUp(ax) (.) key + (P * bx, 0); ModDown of it = MultKey
+    o, g = pair(KS)
+    _, key = rot_key(KS, rot)
+    a = uniform_parts(KS, 17, 111)
+    ga = g.import_ct(17, a)
+    acc = g.MultKeyNoModDown(ga, key)
+    assert acc.info()["num_aux"] == o.alpha
+    _eq(g.ModDown(acc), g.MultKey(ga, key).numpy())
+
+
+def test_add_sub_mixed_rx(cuda_ok):
+    # Context.cpp:146-229: with rx on one side only, res.rx = a.rx, or b.rx /
+    # -b.rx; the result may alias the operand without rx
+    o, g = pair(KS)
+    lvl = 16
+    Q = _i64(o.primes(lvl))[:, None]
+    x = uniform_parts(KS, lvl, 121, nparts=3)
+    y = uniform_parts(KS, lvl, 124)
+    gx, gy = g.import_ct(lvl, x), g.import_ct(lvl, y)
+    _eq(g.Add(gx, gy), [_add(x[0], y[0], Q), _add(x[1], y[1], Q), x[2]])
+    _eq(g.Add(gy, gx), [_add(y[0], x[0], Q), _add(y[1], x[1], Q), x[2]])
+    _eq(g.Sub(gx, gy), [_sub(x[0], y[0], Q), _sub(x[1], y[1], Q), x[2]])
+    _eq(g.Sub(gy, gx), [_sub(y[0], x[0], Q), _sub(y[1], x[1], Q), _sub(0, x[2], Q)])
+    g.Add(gx, gy, res=gy)
+    _eq(gy, [_add(x[0], y[0], Q), _add(x[1], y[1], Q), x[2]])
+    gy = g.import_ct(lvl, y)
+    g.Sub(gy, gx, res=gy)
+    _eq(gy, [_sub(y[0], x[0], Q), _sub(y[1], x[1], Q), _sub(0, x[2], Q)])
