@@ -42,33 +42,41 @@ __global__ void k_modup_to_max(const __grid_constant__ ModUpToMaxDesc d) {
 }
 
 // out[c][o][r] = sum_t pt[o][t][r] (.) in[c][t][r]  (Montgomery products,
-// canonical).  Block x = ciphertext + count * column block: the blocks of the
-// ciphertexts of one batch that read the same plaintext tile are neighbours
-// in launch order, so the plaintexts come from HBM once per batch.  One
-// thread owns one coefficient of one row for every output, so the baby-step
-// values it reads for the first giant step are L1 hits for the others.
-__global__ void k_pt_accum(const __grid_constant__ PtAccumDesc d) {
+// canonical).  One thread owns one coefficient of one row of one ciphertext:
+// it reads each baby-step value once and keeps the G giant-step sums in
+// registers, so no value is re-read.  Block x = ciphertext + count * column
+// block: the blocks of a batch that read the same plaintext tile run back to
+// back and share it through L2.
+template <int G>
+__global__ void __launch_bounds__(256) k_pt_accum(const __grid_constant__ PtAccumDesc d) {
   const int r = blockIdx.y;
-  const int c = blockIdx.x % d.count, xb = blockIdx.x / d.count, nxb = gridDim.x / d.count;
+  const int c = blockIdx.x % d.count, xb = blockIdx.x / d.count;
   const uint32_t q = d.q[r];
   const int32_t qi = d.qinv[r];
-  const size_t n = static_cast<size_t>(d.n);
-  const size_t off = static_cast<size_t>(r) * n;
-  for (size_t i = xb * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
-       i += static_cast<size_t>(nxb) * blockDim.x) {
-    for (int o = 0; o < d.outs; o++) {
-      const PtAccumOut &out = d.out[o];
-      uint32_t sb = 0, sa = 0;
-      for (int t = 0; t < out.terms; t++) {
-        const int ti = out.term[t];
-        const uint32_t m = out.pt[t][off + i];
-        sb = add_mod(sb, mont_mul(d.in_b[c][ti][off + i], m, q, qi), q);
-        sa = add_mod(sa, mont_mul(d.in_a[c][ti][off + i], m, q, qi), q);
+  const size_t i = static_cast<size_t>(xb) * blockDim.x + threadIdx.x;
+  if (i >= static_cast<size_t>(d.n)) return;
+  const size_t idx = static_cast<size_t>(r) * d.n + i;
+  uint32_t sb[G], sa[G];
+#pragma unroll
+  for (int o = 0; o < G; o++) sb[o] = sa[o] = 0;
+  for (int t = 0; t < d.ins; t++) {
+    const uint32_t xb_ = d.in_b[c][t][idx], xa_ = d.in_a[c][t][idx];
+#pragma unroll
+    for (int o = 0; o < G; o++) {
+      const uint32_t *p = d.pt[o][t];
+      if (o < d.outs && p != nullptr) {
+        const uint32_t m = p[idx];
+        sb[o] = add_mod(sb[o], mont_mul(xb_, m, q, qi), q);
+        sa[o] = add_mod(sa[o], mont_mul(xa_, m, q, qi), q);
       }
-      d.out_b[c][o][off + i] = sb;
-      d.out_a[c][o][off + i] = sa;
     }
   }
+#pragma unroll
+  for (int o = 0; o < G; o++)
+    if (o < d.outs) {
+      d.out_b[c][o][idx] = sb[o];
+      d.out_a[c][o][idx] = sa[o];
+    }
 }
 
 // dst[p][r] = sum_t c[t][r] * src[t][p][r]  (Montgomery constants, canonical)
@@ -97,8 +105,18 @@ void launch_modup_to_max(const ModUpToMaxDesc &d, cudaStream_t s) {
 }
 
 void launch_pt_accum(const PtAccumDesc &d, cudaStream_t s) {
-  if (d.rows <= 0 || d.outs <= 0 || d.count <= 0 || d.count > kMaxPtAccumCts) return;
-  k_pt_accum<<<dim3(64 * d.count, d.rows), 256, 0, s>>>(d);
+  if (d.rows <= 0 || d.rows > 64 || d.outs <= 0 || d.outs > kMaxPtAccumOuts || d.ins <= 0 ||
+      d.ins > kMaxPtAccumIn || d.count <= 0 || d.count > kMaxPtAccumCts)
+    return;
+  const dim3 grid(d.count * ((d.n + 255) / 256), d.rows);
+  if (d.outs <= 1)
+    k_pt_accum<1><<<grid, 256, 0, s>>>(d);
+  else if (d.outs <= 4)
+    k_pt_accum<4><<<grid, 256, 0, s>>>(d);
+  else if (d.outs <= 8)
+    k_pt_accum<8><<<grid, 256, 0, s>>>(d);
+  else
+    k_pt_accum<16><<<grid, 256, 0, s>>>(d);
 }
 
 void launch_const_accum(const ConstAccumDesc &d, cudaStream_t s) {

@@ -108,26 +108,19 @@ struct ModUpToMaxDesc {
 };
 void launch_modup_to_max(const ModUpToMaxDesc &d, cudaStream_t s);
 
-// out[o].(b, a)[r] = sum_t pt[o][t][r] (.) in_(b, a)[term[o][t]][r]
+// out_(b, a)[c][o][r] = sum_t pt[o][t][r] (.) in_(b, a)[c][t][r] over the
+// (o, t) pairs with a plaintext (pt[o][t] == nullptr: no term).  Up to
+// kMaxPtAccumCts ciphertexts share the plaintexts.
 constexpr int kMaxPtAccumIn = 64;
-constexpr int kMaxPtAccumTerms = 32;
 constexpr int kMaxPtAccumOuts = 16;
-struct PtAccumOut {
-  int terms;
-  int16_t term[kMaxPtAccumTerms];
-  const uint32_t *pt[kMaxPtAccumTerms];
-};
-// Up to kMaxPtAccumCts ciphertexts sharing the plaintexts: ciphertext c
-// reads in_b[c][i] / in_a[c][i] and writes out_b[c][o] / out_a[c][o]; the
-// terms of output o (baby-step index, plaintext) are shared.
 constexpr int kMaxPtAccumCts = 8;
 struct PtAccumDesc {
   const uint32_t *in_b[kMaxPtAccumCts][kMaxPtAccumIn], *in_a[kMaxPtAccumCts][kMaxPtAccumIn];
   uint32_t *out_b[kMaxPtAccumCts][kMaxPtAccumOuts], *out_a[kMaxPtAccumCts][kMaxPtAccumOuts];
+  const uint32_t *pt[kMaxPtAccumOuts][kMaxPtAccumIn];
   uint32_t q[64];
   int32_t qinv[64];
-  int rows, outs, n, count;
-  PtAccumOut out[kMaxPtAccumOuts];
+  int rows, ins, outs, n, count;
 };
 void launch_pt_accum(const PtAccumDesc &d, cudaStream_t s);
 

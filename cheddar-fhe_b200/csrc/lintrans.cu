@@ -262,25 +262,27 @@ Status Context::lt_evaluate_min_ks_batch(int count, DeviceCt *const *res, const 
     // this giant step's terms (shared) and each ciphertext's baby steps
     std::vector<int> in_slot;
     std::map<int, int> in_of;
-    PtAccumOut po{};
+    std::vector<const uint32_t *> pts;
     for (const auto &pt : pl.pts) {
       if (pt.gs != gsi) continue;
-      auto f = in_of.find(pt.bs);
-      if (f == in_of.end()) {
-        CHD_CHECK(static_cast<int>(in_slot.size()) < kMaxPtAccumIn, kErrUnsupported, "Hoist: too many baby steps");
-        f = in_of.emplace(pt.bs, static_cast<int>(in_slot.size())).first;
-        in_slot.push_back(slot_of.at(pt.bs));
-      }
-      CHD_CHECK(po.terms < kMaxPtAccumTerms, kErrUnsupported, "Hoist: too many terms");
-      po.term[po.terms] = static_cast<int16_t>(f->second);
-      po.pt[po.terms] = pt.dev;  // the first nq rows are the q primes
-      po.terms++;
+      CHD_CHECK(!in_of.count(pt.bs), kErrInvalidArg, "Hoist: a giant step names one baby step twice");
+      CHD_CHECK(static_cast<int>(in_slot.size()) < kMaxPtAccumIn, kErrUnsupported, "Hoist: too many baby steps");
+      in_of.emplace(pt.bs, static_cast<int>(in_slot.size()));
+      in_slot.push_back(slot_of.at(pt.bs));
+      pts.push_back(pt.dev);  // the first nq rows are the q primes
     }
-    for (int c0 = 0; c0 < count; c0++) {  // one launch per ciphertext (see HoistOps::pt_accum)
+    for (int c = 0; c < count && in_slot.empty(); c++) {  // no plaintexts: a zero sum
+      DeviceCt &o = first ? acc[c] : tmp[c];
+      cudaMemsetAsync(o.bx, 0, static_cast<size_t>(nq) * n * 4, stream);
+      cudaMemsetAsync(o.ax, 0, static_cast<size_t>(nq) * n * 4, stream);
+    }
+    for (int c0 = 0; c0 < count && !in_slot.empty(); c0 += kMaxPtAccumCts) {
       PtAccumDesc d{};
-      d.count = 1;
+      d.count = std::min(kMaxPtAccumCts, count - c0);
+      d.ins = static_cast<int>(in_slot.size());
+      for (int k = 0; k < d.ins; k++) d.pt[0][k] = pts[k];
       for (int c = 0; c < d.count; c++) {
-        for (size_t k = 0; k < in_slot.size(); k++) {
+        for (int k = 0; k < d.ins; k++) {
           d.in_b[c][k] = bs[c0 + c][in_slot[k]].bx;
           d.in_a[c][k] = bs[c0 + c][in_slot[k]].ax;
         }
@@ -295,7 +297,6 @@ Status Context::lt_evaluate_min_ks_batch(int count, DeviceCt *const *res, const 
       d.rows = nq;
       d.n = n;
       d.outs = 1;
-      d.out[0] = po;
       launch_pt_accum(d, stream);
     }
     for (int c = 0; c < count; c++) {
@@ -466,21 +467,20 @@ struct HoistOps {
   Status pt_accum(int count, const std::vector<Pairs> &ins,
                   const std::vector<std::vector<std::pair<int, const uint32_t *>>> &terms,
                   const std::vector<OutPairs> &outs) const {
-    if (static_cast<int>(ins[0].size()) > kMaxPtAccumIn) {
+    const int nin = static_cast<int>(ins[0].size());
+    if (nin > kMaxPtAccumIn) {
       set_error("Hoist: too many baby steps");
       return kErrUnsupported;
     }
-    // One launch per ciphertext: a launch over several ciphertexts shares
-    // the plaintext reads but streams every ciphertext's baby steps through
-    // each SM at once, which measured 2.6x slower at N = 2^16.
     const size_t nout = outs[0].size();
-    for (int c0 = 0; c0 < count; c0++) {
-      const int cn = 1;
+    for (int c0 = 0; c0 < count; c0 += kMaxPtAccumCts) {
+      const int cn = std::min(kMaxPtAccumCts, count - c0);
       for (size_t o0 = 0; o0 < nout; o0 += kMaxPtAccumOuts) {
         PtAccumDesc d{};
         d.count = cn;
+        d.ins = nin;
         for (int c = 0; c < cn; c++)
-          for (size_t i = 0; i < ins[c0 + c].size(); i++) {
+          for (int i = 0; i < nin; i++) {
             d.in_b[c][i] = ins[c0 + c][i].first;
             d.in_a[c][i] = ins[c0 + c][i].second;
           }
@@ -492,16 +492,12 @@ struct HoistOps {
         d.n = n;
         d.outs = static_cast<int>(std::min<size_t>(kMaxPtAccumOuts, nout - o0));
         for (int o = 0; o < d.outs; o++) {
-          const auto &t = terms[o0 + o];
-          if (static_cast<int>(t.size()) > kMaxPtAccumTerms) {
-            set_error("Hoist: too many terms");
-            return kErrUnsupported;
-          }
-          PtAccumOut &po = d.out[o];
-          po.terms = static_cast<int>(t.size());
-          for (size_t k = 0; k < t.size(); k++) {
-            po.term[k] = static_cast<int16_t>(t[k].first);
-            po.pt[k] = t[k].second;
+          for (const auto &t : terms[o0 + o]) {
+            if (t.first < 0 || t.first >= nin || d.pt[o][t.first]) {
+              set_error("Hoist: a giant step names one baby step twice or one that does not exist");
+              return kErrInvalidArg;
+            }
+            d.pt[o][t.first] = t.second;
           }
           for (int c = 0; c < cn; c++) {
             d.out_b[c][o] = outs[c0 + c][o0 + o].first;
