@@ -41,41 +41,72 @@ __global__ void k_modup_to_max(const __grid_constant__ ModUpToMaxDesc d) {
   }
 }
 
+template <int V>
+__device__ __forceinline__ void ld_vec(const uint32_t *p, uint32_t (&x)[V]) {
+  if constexpr (V == 4) {
+    const uint4 u = *reinterpret_cast<const uint4 *>(p);
+    x[0] = u.x, x[1] = u.y, x[2] = u.z, x[3] = u.w;
+  } else if constexpr (V == 2) {
+    const uint2 u = *reinterpret_cast<const uint2 *>(p);
+    x[0] = u.x, x[1] = u.y;
+  } else {
+    x[0] = *p;
+  }
+}
+template <int V>
+__device__ __forceinline__ void st_vec(uint32_t *p, const uint32_t (&x)[V]) {
+  if constexpr (V == 4) {
+    *reinterpret_cast<uint4 *>(p) = make_uint4(x[0], x[1], x[2], x[3]);
+  } else if constexpr (V == 2) {
+    *reinterpret_cast<uint2 *>(p) = make_uint2(x[0], x[1]);
+  } else {
+    *p = x[0];
+  }
+}
+
 // out[c][o][r] = sum_t pt[o][t][r] (.) in[c][t][r]  (Montgomery products,
-// canonical).  One thread owns one coefficient of one row of one ciphertext:
-// it reads each baby-step value once and keeps the G giant-step sums in
-// registers, so no value is re-read.  Block x = ciphertext + count * column
-// block: the blocks of a batch that read the same plaintext tile run back to
-// back and share it through L2.
-template <int G>
+// canonical).  One thread owns V adjacent coefficients of one row of one
+// ciphertext: it reads each baby-step value once (V-word vector loads) and
+// keeps the G giant-step sums in registers, so no value is re-read.  Block
+// x = ciphertext + count * column block: the blocks of a batch that read the
+// same plaintext tile run back to back and share it through L2.
+template <int G, int V>
 __global__ void __launch_bounds__(256) k_pt_accum(const __grid_constant__ PtAccumDesc d) {
   const int r = blockIdx.y;
   const int c = blockIdx.x % d.count, xb = blockIdx.x / d.count;
   const uint32_t q = d.q[r];
   const int32_t qi = d.qinv[r];
-  const size_t i = static_cast<size_t>(xb) * blockDim.x + threadIdx.x;
+  const size_t i = (static_cast<size_t>(xb) * blockDim.x + threadIdx.x) * V;
   if (i >= static_cast<size_t>(d.n)) return;
   const size_t idx = static_cast<size_t>(r) * d.n + i;
-  uint32_t sb[G], sa[G];
+  uint32_t sb[G][V], sa[G][V];
 #pragma unroll
-  for (int o = 0; o < G; o++) sb[o] = sa[o] = 0;
+  for (int o = 0; o < G; o++)
+#pragma unroll
+    for (int v = 0; v < V; v++) sb[o][v] = sa[o][v] = 0;
   for (int t = 0; t < d.ins; t++) {
-    const uint32_t xb_ = d.in_b[c][t][idx], xa_ = d.in_a[c][t][idx];
+    uint32_t xb_[V], xa_[V];
+    ld_vec<V>(d.in_b[c][t] + idx, xb_);
+    ld_vec<V>(d.in_a[c][t] + idx, xa_);
 #pragma unroll
     for (int o = 0; o < G; o++) {
       const uint32_t *p = d.pt[o][t];
       if (o < d.outs && p != nullptr) {
-        const uint32_t m = p[idx];
-        sb[o] = add_mod(sb[o], mont_mul(xb_, m, q, qi), q);
-        sa[o] = add_mod(sa[o], mont_mul(xa_, m, q, qi), q);
+        uint32_t m[V];
+        ld_vec<V>(p + idx, m);
+#pragma unroll
+        for (int v = 0; v < V; v++) {
+          sb[o][v] = add_mod(sb[o][v], mont_mul(xb_[v], m[v], q, qi), q);
+          sa[o][v] = add_mod(sa[o][v], mont_mul(xa_[v], m[v], q, qi), q);
+        }
       }
     }
   }
 #pragma unroll
   for (int o = 0; o < G; o++)
     if (o < d.outs) {
-      d.out_b[c][o][idx] = sb[o];
-      d.out_a[c][o][idx] = sa[o];
+      st_vec<V>(d.out_b[c][o] + idx, sb[o]);
+      st_vec<V>(d.out_a[c][o] + idx, sa[o]);
     }
 }
 
@@ -108,15 +139,26 @@ void launch_pt_accum(const PtAccumDesc &d, cudaStream_t s) {
   if (d.rows <= 0 || d.rows > 64 || d.outs <= 0 || d.outs > kMaxPtAccumOuts || d.ins <= 0 ||
       d.ins > kMaxPtAccumIn || d.count <= 0 || d.count > kMaxPtAccumCts)
     return;
-  const dim3 grid(d.count * ((d.n + 255) / 256), d.rows);
-  if (d.outs <= 1)
-    k_pt_accum<1><<<grid, 256, 0, s>>>(d);
+  // vector width: every pointer 16-byte aligned and N a multiple of 4
+  uintptr_t bits = static_cast<uintptr_t>(d.n) * 4;
+  for (int c = 0; c < d.count; c++) {
+    for (int t = 0; t < d.ins; t++)
+      bits |= reinterpret_cast<uintptr_t>(d.in_b[c][t]) | reinterpret_cast<uintptr_t>(d.in_a[c][t]);
+    for (int o = 0; o < d.outs; o++)
+      bits |= reinterpret_cast<uintptr_t>(d.out_b[c][o]) | reinterpret_cast<uintptr_t>(d.out_a[c][o]);
+  }
+  for (int o = 0; o < d.outs; o++)
+    for (int t = 0; t < d.ins; t++) bits |= reinterpret_cast<uintptr_t>(d.pt[o][t]);
+  const bool vec = (bits & 15) == 0;
+  auto grid = [&](int v) { return dim3(d.count * ((d.n / v + 255) / 256), d.rows); };
+  if (!vec)
+    k_pt_accum<16, 1><<<grid(1), 256, 0, s>>>(d);
   else if (d.outs <= 4)
-    k_pt_accum<4><<<grid, 256, 0, s>>>(d);
+    k_pt_accum<4, 4><<<grid(4), 256, 0, s>>>(d);
   else if (d.outs <= 8)
-    k_pt_accum<8><<<grid, 256, 0, s>>>(d);
+    k_pt_accum<8, 2><<<grid(2), 256, 0, s>>>(d);
   else
-    k_pt_accum<16><<<grid, 256, 0, s>>>(d);
+    k_pt_accum<16, 1><<<grid(1), 256, 0, s>>>(d);
 }
 
 void launch_const_accum(const ConstAccumDesc &d, cudaStream_t s) {
