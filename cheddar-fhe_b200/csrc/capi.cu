@@ -61,6 +61,10 @@ int fail(int code, const std::string &msg) {
 }
 #define CHD_NOTNULL(p) \
   if (!(p)) return fail(CHD_ERR_INVALID_ARG, std::string(__func__) + ": null argument " #p)
+// the kernels move device data in 16-byte vectors
+#define CHD_ALIGNED(p)                                    \
+  if (reinterpret_cast<uintptr_t>(p) & 15)                \
+  return fail(CHD_ERR_INVALID_ARG, std::string(__func__) + ": device pointer " #p " is not 16-byte aligned")
 }  // namespace
 
 extern "C" {
@@ -278,6 +282,7 @@ int chd_add_plain(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(pt_dev);
+  CHD_ALIGNED(pt_dev);
   return ctx->c->add_sub_plain(res->ct, a->ct, pt_dev, pt_scale, false);
 } catch (const std::exception &e) {
   return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
@@ -291,6 +296,7 @@ int chd_sub_plain(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(pt_dev);
+  CHD_ALIGNED(pt_dev);
   return ctx->c->add_sub_plain(res->ct, a->ct, pt_dev, pt_scale, true);
 } catch (const std::exception &e) {
   return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
@@ -315,6 +321,7 @@ int chd_sub_plain_ct(chd_context *ctx, chd_ciphertext *res, const uint32_t *pt_d
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(pt_dev);
+  CHD_ALIGNED(pt_dev);
   CHD_NOTNULL(b);
   return ctx->c->sub_from(res->ct, pt_dev, nullptr, pt_scale, b->ct);
 } catch (const std::exception &e) {
@@ -342,6 +349,7 @@ int chd_mult_unsafe_plain(chd_context *ctx, chd_ciphertext *res, const chd_ciphe
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(pt_dev);
+  CHD_ALIGNED(pt_dev);
   return ctx->c->mult_unsafe_plain(res->ct, a->ct, pt_dev, pt_level, pt_num_aux, pt_scale, level);
 } catch (const std::exception &e) {
   return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
@@ -456,6 +464,9 @@ int chd_ct_wrap(chd_context *ctx, int num_main, int num_ter, int num_aux, int ha
   CHD_NOTNULL(bx);
   CHD_NOTNULL(ax);
   if (has_rx && !rx) return fail(CHD_ERR_INVALID_ARG, "chd_ct_wrap: rx is null");
+  CHD_ALIGNED(bx);
+  CHD_ALIGNED(ax);
+  CHD_ALIGNED(has_rx ? rx : nullptr);
   NP np{num_main, num_ter, num_aux};
   if (static_cast<size_t>(np.total()) * ctx->c->P->n > words_per_part)
     return fail(CHD_ERR_SHAPE, "chd_ct_wrap: buffers smaller than the ciphertext");
@@ -645,6 +656,7 @@ int chd_mult_plain(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(pt_dev);
+  CHD_ALIGNED(pt_dev);
   return ctx->c->mult_plain(res->ct, a->ct, pt_dev, pt_scale);
 } catch (const std::exception &e) {
   return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
@@ -680,6 +692,7 @@ int chd_encode(chd_context *ctx, int level, double scale, const double *re, cons
   CHD_NOTNULL(re);
   CHD_NOTNULL(im);
   CHD_NOTNULL(pt_dev);
+  CHD_ALIGNED(pt_dev);
   if (msg_len < 1) return fail(CHD_ERR_INVALID_ARG, "chd_encode: empty message");
   std::vector<std::complex<double>> msg(msg_len);
   for (int i = 0; i < msg_len; i++) msg[i] = std::complex<double>(re[i], im[i]);
@@ -1505,6 +1518,7 @@ int chd_moddown(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) 
 int chd_ntt(chd_context *ctx, int num_main, int num_ter, int num_aux, uint32_t *data_dev, int mont, int count) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(data_dev);
+  CHD_ALIGNED(data_dev);
   NP np{num_main, num_ter, num_aux};
   const Params &P = *ctx->c->P;
   if (num_main < 0 || num_ter < 0 || num_aux < 0 || num_main > P.max_main || num_ter > P.max_ter ||
@@ -1520,6 +1534,7 @@ int chd_ntt(chd_context *ctx, int num_main, int num_ter, int num_aux, uint32_t *
 int chd_intt(chd_context *ctx, int num_main, int num_ter, int num_aux, uint32_t *data_dev, int mont, int count) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(data_dev);
+  CHD_ALIGNED(data_dev);
   NP np{num_main, num_ter, num_aux};
   const Params &P = *ctx->c->P;
   if (num_main < 0 || num_ter < 0 || num_aux < 0 || num_main > P.max_main || num_ter > P.max_ter ||
@@ -1535,7 +1550,9 @@ int chd_intt(chd_context *ctx, int num_main, int num_ter, int num_aux, uint32_t 
 int chd_modup_raw(chd_context *ctx, int level, const uint32_t *src_dev, uint32_t *dst_dev) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(src_dev);
+  CHD_ALIGNED(src_dev);
   CHD_NOTNULL(dst_dev);
+  CHD_ALIGNED(dst_dev);
   Context &C = *ctx->c;
   if (level < -1 || level > C.P->max_level) return fail(CHD_ERR_INVALID_LEVEL, "chd_modup_raw: invalid level");
   const LevelMS &m = C.lms(level);
@@ -1552,7 +1569,9 @@ int chd_modup_raw(chd_context *ctx, int level, const uint32_t *src_dev, uint32_t
 int chd_moddown_raw(chd_context *ctx, int level, int type, const uint32_t *src_dev, uint32_t *dst_dev, int npoly) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(src_dev);
+  CHD_ALIGNED(src_dev);
   CHD_NOTNULL(dst_dev);
+  CHD_ALIGNED(dst_dev);
   Context &C = *ctx->c;
   if (level < -1 || level > C.P->max_level) return fail(CHD_ERR_INVALID_LEVEL, "chd_moddown_raw: invalid level");
   if (type < 0 || type > 2 || npoly < 1) return fail(CHD_ERR_INVALID_ARG, "chd_moddown_raw: bad type or npoly");
@@ -1605,9 +1624,11 @@ int chd_bconv_raw(chd_context *ctx, const int32_t *xt_dev, const int *src_gidx, 
                   uint32_t *out_dev) try {
   CHD_NOTNULL(ctx);
   CHD_NOTNULL(xt_dev);
+  CHD_ALIGNED(xt_dev);
   CHD_NOTNULL(src_gidx);
   CHD_NOTNULL(dst_gidx);
   CHD_NOTNULL(out_dev);
+  CHD_ALIGNED(out_dev);
   Context &C = *ctx->c;
   std::vector<int32_t> t;
   int rc = bconv_table(C, src_gidx, K, dst_gidx, M, &t, "chd_bconv_raw");

@@ -72,9 +72,12 @@ __global__ void __launch_bounds__(256) k_bconv(const __grid_constant__ BConvBatc
 // ---------------------------------------------------------------- key MAC
 __global__ void __launch_bounds__(256) k_key_mac(const __grid_constant__ KeyMacDesc d, int log_n) {
   const int n = 1 << log_n;
+  // block x = ciphertext + count * column block: the ciphertexts reading
+  // the same key tile are neighbours in launch order (the key comes from HBM
+  // once per batch)
   const int r = blockIdx.y;
-  const KeyMacCt &c = d.ct[blockIdx.z];
-  const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  const KeyMacCt &c = d.ct[blockIdx.x % d.count];
+  const int i0 = ((blockIdx.x / d.count) * blockDim.x + threadIdx.x) * 4;
   if (i0 >= n) return;
   const uint32_t q = d.q[r];
   const int32_t qi = d.qinv[r];
@@ -193,41 +196,61 @@ __global__ void __launch_bounds__(256) k_permute(const __grid_constant__ Permute
 }
 
 // Hoisted rotations (one launch for all R rotations).  Each thread loads the
-// beta ModUp values of its coefficient once, then for every rotation forms
-// the key inner products and scatters them through the inverse automorphism.
-// grid (count, N / 256, rows): the ciphertexts of a batch that read the
-// same key tile are neighbours in launch order, so the keys come from HBM
-// once per batch
+// beta ModUp values of 4 adjacent coefficients once, then for every rotation
+// forms the key inner products and stores them through the inverse
+// automorphism.  In the bit-reversed domain the automorphism maps an aligned
+// group of 4 coefficients onto an aligned group of 4 (only the two top bits
+// of the exponent differ, and they become the two low bits of the
+// destination), so the 4 results leave as one 16-byte store after a
+// permutation in registers.  Grid (count, N / 1024, rows): the ciphertexts of
+// a batch that read the same key tile are neighbours in launch order, so the
+// keys come from HBM once per batch.
 __global__ void __launch_bounds__(256) k_hoisted(const __grid_constant__ HoistDesc d, int log_n) {
   const int n = 1 << log_n;
   const int c = blockIdx.x;
   const int r = blockIdx.z;
-  const int k = blockIdx.y * blockDim.x + threadIdx.x;
-  if (k >= n) return;
+  const int k0 = (blockIdx.y * blockDim.x + threadIdx.x) * 4;
+  if (k0 >= n) return;
   const uint32_t q = d.q[r];
   const int32_t qi = d.qinv[r];
-  const size_t off = static_cast<size_t>(r) * n + k;
-  const size_t koff = static_cast<size_t>(d.key_row[r]) * n + k;
-  uint32_t mu[8];
+  const size_t off = static_cast<size_t>(r) * n + k0;
+  const size_t koff = static_cast<size_t>(d.key_row[r]) * n + k0;
+  uint32_t mu[8][4];
 #pragma unroll
   for (int i = 0; i < 8; i++)
-    if (i < d.beta) mu[i] = __ldg(d.mu[c][i] + off);
-  const uint32_t bxp = (r < d.nq) ? __ldg(d.bxp[c] + off) : 0u;
+    if (i < d.beta) unpack(ld4(d.mu[c][i] + off), mu[i]);
+  uint32_t bxp[4] = {0, 0, 0, 0};
+  if (r < d.nq) unpack(ld4(d.bxp[c] + off), bxp);
   for (int j = 0; j < d.R; j++) {
-    uint32_t sb = bxp, sa = 0;
+    uint32_t sb[4], sa[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int l = 0; l < 4; l++) sb[l] = bxp[l];
 #pragma unroll
     for (int i = 0; i < 8; i++) {
       if (i < d.beta) {
-        const uint32_t kb = __ldg(d.kb[j][i] + koff);
-        const uint32_t ka = __ldg(d.ka[j][i] + koff);
-        sb = add_mod(sb, mont_mul(mu[i], kb, q, qi), q);
-        sa = add_mod(sa, mont_mul(mu[i], ka, q, qi), q);
+        uint32_t kb[4], ka[4];
+        unpack(ld4(d.kb[j][i] + koff), kb);
+        unpack(ld4(d.ka[j][i] + koff), ka);
+#pragma unroll
+        for (int l = 0; l < 4; l++) {
+          sb[l] = add_mod(sb[l], mont_mul(mu[i][l], kb[l], q, qi), q);
+          sa[l] = add_mod(sa[l], mont_mul(mu[i][l], ka[l], q, qi), q);
+        }
       }
     }
-    const uint32_t dk = galois_src(k, d.galois_inv[j], log_n);
-    const size_t o = static_cast<size_t>(r) * n + dk;
-    d.out_b[c][j][o] = sb;
-    d.out_a[c][j][o] = sa;
+    uint32_t slot[4];
+#pragma unroll
+    for (int l = 0; l < 4; l++) slot[l] = galois_src(k0 + l, d.galois_inv[j], log_n);
+    const size_t o = static_cast<size_t>(r) * n + (slot[0] & ~3u);
+    uint32_t ob[4], oa[4];
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+      const uint32_t u = static_cast<uint32_t>(m);
+      ob[m] = (slot[0] & 3u) == u ? sb[0] : (slot[1] & 3u) == u ? sb[1] : (slot[2] & 3u) == u ? sb[2] : sb[3];
+      oa[m] = (slot[0] & 3u) == u ? sa[0] : (slot[1] & 3u) == u ? sa[1] : (slot[2] & 3u) == u ? sa[2] : sa[3];
+    }
+    st4(d.out_b[c][j] + o, ob[0], ob[1], ob[2], ob[3]);
+    st4(d.out_a[c][j] + o, oa[0], oa[1], oa[2], oa[3]);
   }
 }
 
@@ -255,7 +278,7 @@ void launch_bconv(const BConvBatch &b, int log_n, cudaStream_t s) {
 void launch_key_mac(const KeyMacDesc &d, int log_n, cudaStream_t s) {
   if (d.rows <= 0 || d.count <= 0) return;
   const int n = 1 << log_n;
-  k_key_mac<<<dim3((n / 4 + 255) / 256, d.rows, d.count), 256, 0, s>>>(d, log_n);
+  k_key_mac<<<dim3(d.count * ((n / 4 + 255) / 256), d.rows), 256, 0, s>>>(d, log_n);
 }
 
 void launch_elementwise(ElemOp op, const ElemBatch &b, int log_n, cudaStream_t s) {
@@ -297,7 +320,7 @@ void launch_hoisted(const HoistDesc &d, int log_n, cudaStream_t s) {
   if (d.rows <= 0 || d.R <= 0) return;
   const int n = 1 << log_n;
   if (d.count <= 0 || d.count > kMaxHoistCts) return;
-  k_hoisted<<<dim3(d.count, (n + 255) / 256, d.rows), 256, 0, s>>>(d, log_n);
+  k_hoisted<<<dim3(d.count, (n / 4 + 255) / 256, d.rows), 256, 0, s>>>(d, log_n);
 }
 
 }  // namespace chd

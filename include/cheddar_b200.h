@@ -14,6 +14,9 @@
  * bit-reversed evaluation domain and in Montgomery form (x * 2^32 mod q).
  * Evaluation keys are beta pairs (bx, ax), each over the key basis of all
  * L = main + terminal primes followed by the alpha auxiliary primes.
+ * Device buffers handed to the library (wrapped ciphertexts, plaintexts, the
+ * raw NTT / ModUp / ModDown / BConv operands) start on a 16-byte boundary;
+ * other pointers are rejected with CHD_ERR_INVALID_ARG.
  *
  * Threading: a context is not re-entrant; all its work is ordered on one CUDA
  * stream (chd_context_set_stream).  Calls return before the GPU finishes;

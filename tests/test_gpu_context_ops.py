@@ -260,3 +260,24 @@ def test_add_sub_mixed_rx(cuda_ok):
     gy = g.import_ct(lvl, y)
     g.Sub(gy, gx, res=gy)
     _eq(gy, [_sub(y[0], x[0], Q), _sub(y[1], x[1], Q), _sub(0, x[2], Q)])
+
+
+def test_misaligned_device_buffers_rejected(cuda_ok):
+    # the kernels move device data in 16-byte vectors: a buffer that does
+    # not start on a 16-byte boundary is an argument error, not a launch
+    import torch
+    o, g = pair(KS)
+    lvl = 3
+    rows = o.num_q(lvl)
+    buf = torch.zeros(2, rows * o.n + 4, dtype=torch.int32, device="cuda")
+    with pytest.raises(chd.CheddarError) as e:
+        g.wrap_ct(lvl, [buf[0][1:], buf[1][1:]])
+    assert e.value.code == 1
+    ga = g.import_ct(lvl, uniform_parts(KS, lvl, 131))
+    pt = torch.zeros(rows * o.n + 4, dtype=torch.int32, device="cuda")
+    with pytest.raises(chd.CheddarError):
+        g.MultPlain(ga, pt[2:], 1.0)
+    with pytest.raises(chd.CheddarError):
+        g.AddPlain(ga, pt[1:], 1.0)
+    # aligned views work
+    g.wrap_ct(lvl, [buf[0][4:], buf[1][4:]])
