@@ -110,22 +110,25 @@ __global__ void __launch_bounds__(256) k_pt_accum(const __grid_constant__ PtAccu
     }
 }
 
-// dst[p][r] = sum_t c[t][r] * src[t][p][r]  (Montgomery constants, canonical)
-__global__ void k_const_accum(const __grid_constant__ ConstAccumDesc d) {
+// dst[p][r] = sum_t c[t][r] * src[t][p][r]  (Montgomery constants, canonical),
+// 4 coefficients per thread in 16-byte vectors
+__global__ void __launch_bounds__(256) k_const_accum(const __grid_constant__ ConstAccumDesc d) {
   const int r = blockIdx.y;
   const int part = blockIdx.z;
   const uint32_t q = d.q[r];
   const int32_t qi = d.qinv[r];
   const size_t n = static_cast<size_t>(d.n);
-  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
-       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-    uint32_t s = 0;
-    for (int t = 0; t < d.terms; t++) {
-      const uint32_t *src = d.src[t][part] + static_cast<size_t>(d.src_row0[t] + r) * n;
-      s = add_mod(s, mont_mul(src[i], d.c[t][r], q, qi), q);
-    }
-    d.dst[part][static_cast<size_t>(r) * n + i] = s;
+  const size_t i = (static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x) * 4;
+  if (i >= n) return;
+  uint32_t s[4] = {0, 0, 0, 0};
+  for (int t = 0; t < d.terms; t++) {
+    uint32_t x[4];
+    ld_vec<4>(d.src[t][part] + static_cast<size_t>(d.src_row0[t] + r) * n + i, x);
+    const uint32_t c = d.c[t][r];
+#pragma unroll
+    for (int l = 0; l < 4; l++) s[l] = add_mod(s[l], mont_mul(x[l], c, q, qi), q);
   }
+  st_vec<4>(d.dst[part] + static_cast<size_t>(r) * n + i, s);
 }
 
 }  // namespace
@@ -163,7 +166,7 @@ void launch_pt_accum(const PtAccumDesc &d, cudaStream_t s) {
 
 void launch_const_accum(const ConstAccumDesc &d, cudaStream_t s) {
   if (d.rows <= 0 || d.parts <= 0 || d.terms <= 0) return;
-  k_const_accum<<<dim3(64, d.rows, d.parts), 256, 0, s>>>(d);
+  k_const_accum<<<dim3((d.n / 4 + 255) / 256, d.rows, d.parts), 256, 0, s>>>(d);
 }
 
 }  // namespace chd

@@ -185,14 +185,32 @@ __device__ __forceinline__ uint32_t galois_src(uint32_t k, uint32_t g, int log_n
   return brev_bits(e & ((1u << lb) - 1u), lb);
 }
 
+// dst[k] = src[galois_src(k)] (+ add[k]).  An aligned group of 4
+// destinations gathers from one aligned group of 4 sources (the bit-reversed
+// automorphism only reorders the two low bits), so every thread moves 4
+// coefficients with one 16-byte load and store each.
 __global__ void __launch_bounds__(256) k_permute(const __grid_constant__ PermuteBatch pb, int log_n) {
   const int n = 1 << log_n;
   const PermuteRow &p = pb.rows[blockIdx.y];
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  uint32_t v = __ldg(p.src + galois_src(k, pb.galois, log_n));
-  if (p.add) v = add_mod(v, __ldg(p.add + k), p.q);
-  p.dst[k] = v;
+  const int k0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  if (k0 >= n) return;
+  uint32_t slot[4];
+#pragma unroll
+  for (int l = 0; l < 4; l++) slot[l] = galois_src(k0 + l, pb.galois, log_n);
+  uint32_t x[4], v[4];
+  unpack(ld4(p.src + (slot[0] & ~3u)), x);
+#pragma unroll
+  for (int l = 0; l < 4; l++) {
+    const uint32_t m = slot[l] & 3u;
+    v[l] = m == 0 ? x[0] : m == 1 ? x[1] : m == 2 ? x[2] : x[3];
+  }
+  if (p.add) {
+    uint32_t a[4];
+    unpack(ld4(p.add + k0), a);
+#pragma unroll
+    for (int l = 0; l < 4; l++) v[l] = add_mod(v[l], a[l], p.q);
+  }
+  st4(p.dst + k0, v[0], v[1], v[2], v[3]);
 }
 
 // Hoisted rotations (one launch for all R rotations).  Each thread loads the
@@ -313,7 +331,7 @@ void launch_tensor(const TensorBatch &b, int log_n, cudaStream_t s) {
 void launch_permute(const PermuteBatch &b, int log_n, cudaStream_t s) {
   if (b.count <= 0) return;
   const int n = 1 << log_n;
-  k_permute<<<dim3((n + 255) / 256, b.count), 256, 0, s>>>(b, log_n);
+  k_permute<<<dim3((n / 4 + 255) / 256, b.count), 256, 0, s>>>(b, log_n);
 }
 
 void launch_hoisted(const HoistDesc &d, int log_n, cudaStream_t s) {
