@@ -257,8 +257,8 @@ void launch_engine(const MSColBatch &b, int engine, int max_k, cudaStream_t s) {
 // Engine autotuning (engine 2): the CUDA-core pass wins on small launches
 // (one ciphertext), the tensor-core pass on large ones.  The first launch of
 // a shape (device, largest K, jobs, largest M) outside a stream capture runs
-// both engines twice, times the second runs with CUDA events (a host
-// synchronisation, once per shape), keeps the faster and caches the choice
+// both engines four times, times the last three of each with CUDA events (a
+// host synchronisation, once per shape), keeps the faster and caches the choice
 // for the process.  Both engines write identical residues, so the tuning
 // launches leave the same outputs.  During a capture an untuned shape uses
 // the tensor cores.  Returns true when the tuning launches have done the work.
@@ -280,7 +280,11 @@ bool tune_and_launch(const MSColBatch &b, int max_k, cudaStream_t s, int *engine
   *engine = 1;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return false;
-  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  // three rounds of (CUDA cores, tensor cores) after a warm-up of each; the
+  // fastest launch of each engine decides (one launch each was noisy enough
+  // to flip the choice between runs)
+  constexpr int kRounds = 3;
+  cudaEvent_t ev[2 * kRounds + 1] = {};
   for (auto &e : ev)
     if (cudaEventCreate(&e) != cudaSuccess) {
       for (auto &f : ev)
@@ -290,13 +294,21 @@ bool tune_and_launch(const MSColBatch &b, int max_k, cudaStream_t s, int *engine
   launch_engine(b, 0, max_k, s);  // warm-up: module load, attributes
   launch_engine(b, 1, max_k, s);
   cudaEventRecord(ev[0], s);
-  launch_engine(b, 0, max_k, s);
-  cudaEventRecord(ev[1], s);
-  launch_engine(b, 1, max_k, s);
-  cudaEventRecord(ev[2], s);
-  float t_cuda = 0.f, t_tc = 0.f;
-  const bool ok = cudaEventSynchronize(ev[2]) == cudaSuccess && cudaEventElapsedTime(&t_cuda, ev[0], ev[1]) == cudaSuccess &&
-                  cudaEventElapsedTime(&t_tc, ev[1], ev[2]) == cudaSuccess;
+  for (int i = 0; i < kRounds; i++) {
+    launch_engine(b, 0, max_k, s);
+    cudaEventRecord(ev[2 * i + 1], s);
+    launch_engine(b, 1, max_k, s);
+    cudaEventRecord(ev[2 * i + 2], s);
+  }
+  bool ok = cudaEventSynchronize(ev[2 * kRounds]) == cudaSuccess;
+  float t_cuda = 1e30f, t_tc = 1e30f;
+  for (int i = 0; ok && i < kRounds; i++) {
+    float a = 0.f, c = 0.f;
+    ok = cudaEventElapsedTime(&a, ev[2 * i], ev[2 * i + 1]) == cudaSuccess &&
+         cudaEventElapsedTime(&c, ev[2 * i + 1], ev[2 * i + 2]) == cudaSuccess;
+    t_cuda = a < t_cuda ? a : t_cuda;
+    t_tc = c < t_tc ? c : t_tc;
+  }
   for (auto &e : ev) cudaEventDestroy(e);
   if (ok) {
     *engine = t_tc <= t_cuda ? 1 : 0;
