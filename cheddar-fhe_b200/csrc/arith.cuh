@@ -64,6 +64,24 @@ __device__ __forceinline__ int32_t centre(uint32_t a, uint32_t q) {
   return a > (q >> 1) ? static_cast<int32_t>(a) - static_cast<int32_t>(q) : static_cast<int32_t>(a);
 }
 
+// ---- two Montgomery products for one reduction (unsigned Montgomery
+// reduction, P. Montgomery 1985).  For canonical a_i, b_i < q < 2^31 the sum
+// s = a1 b1 + a2 b2 < 2 q^2 < 2^63; with m = s (-q^-1) mod 2^32 the value
+// s + m q (< 2^64) is divisible by 2^32 and (s + m q) / 2^32 < 2q, congruent
+// to s 2^-32, i.e. to mont_mul(a1, b1) + mont_mul(a2, b2).  qneg = -q^-1
+// mod 2^32 (the negated qinv).
+__device__ __forceinline__ uint32_t mont_redc2(uint64_t s, uint32_t q, uint32_t qneg) {
+  const uint32_t m = static_cast<uint32_t>(s) * qneg;
+  return static_cast<uint32_t>((s + static_cast<uint64_t>(m) * q) >> 32);
+}
+// canonical mont_mul(a1, b1) + mont_mul(a2, b2) for canonical operands
+__device__ __forceinline__ uint32_t mont_mac2(uint32_t a1, uint32_t b1, uint32_t a2, uint32_t b2, uint32_t q,
+                                              uint32_t qneg) {
+  const uint64_t s = static_cast<uint64_t>(a1) * b1 + static_cast<uint64_t>(a2) * b2;
+  const uint32_t r = mont_redc2(s, q, qneg);
+  return r >= q ? r - q : r;
+}
+
 // Cooley-Tukey butterfly on canonical values: (a, b) -> (a + w b, a - w b)
 __device__ __forceinline__ void ct_bfly(uint32_t &a, uint32_t &b, uint32_t w, uint32_t q, int32_t qinv) {
   uint32_t t = mont_mul(b, w, q, qinv);

@@ -67,7 +67,8 @@ __device__ __forceinline__ void st_vec(uint32_t *p, const uint32_t (&x)[V]) {
 // out[c][o][r] = sum_t pt[o][t][r] (.) in[c][t][r]  (Montgomery products,
 // canonical).  One thread owns V adjacent coefficients of one row of one
 // ciphertext: it reads each baby-step value once (V-word vector loads) and
-// keeps the G giant-step sums in registers, so no value is re-read.  Block
+// keeps the G giant-step sums in registers, so no value is re-read; two baby
+// steps share one Montgomery reduction (mont_mac2).  Block
 // x = ciphertext + count * column block: the blocks of a batch that read the
 // same plaintext tile run back to back and share it through L2.
 template <int G, int V>
@@ -79,12 +80,46 @@ __global__ void __launch_bounds__(256) k_pt_accum(const __grid_constant__ PtAccu
   const size_t i = (static_cast<size_t>(xb) * blockDim.x + threadIdx.x) * V;
   if (i >= static_cast<size_t>(d.n)) return;
   const size_t idx = static_cast<size_t>(r) * d.n + i;
+  const uint32_t qn = 0u - static_cast<uint32_t>(qi);
   uint32_t sb[G][V], sa[G][V];
 #pragma unroll
   for (int o = 0; o < G; o++)
 #pragma unroll
     for (int v = 0; v < V; v++) sb[o][v] = sa[o][v] = 0;
-  for (int t = 0; t < d.ins; t++) {
+  // baby steps in pairs: two products per Montgomery reduction
+  int t = 0;
+  for (; t + 1 < d.ins; t += 2) {
+    uint32_t xb0[V], xa0[V], xb1[V], xa1[V];
+    ld_vec<V>(d.in_b[c][t] + idx, xb0);
+    ld_vec<V>(d.in_a[c][t] + idx, xa0);
+    ld_vec<V>(d.in_b[c][t + 1] + idx, xb1);
+    ld_vec<V>(d.in_a[c][t + 1] + idx, xa1);
+#pragma unroll
+    for (int o = 0; o < G; o++) {
+      if (o >= d.outs) continue;
+      const uint32_t *p0 = d.pt[o][t], *p1 = d.pt[o][t + 1];
+      if (p0 != nullptr && p1 != nullptr) {
+        uint32_t m0[V], m1[V];
+        ld_vec<V>(p0 + idx, m0);
+        ld_vec<V>(p1 + idx, m1);
+#pragma unroll
+        for (int v = 0; v < V; v++) {
+          sb[o][v] = add_mod(sb[o][v], mont_mac2(xb0[v], m0[v], xb1[v], m1[v], q, qn), q);
+          sa[o][v] = add_mod(sa[o][v], mont_mac2(xa0[v], m0[v], xa1[v], m1[v], q, qn), q);
+        }
+      } else if (p0 != nullptr || p1 != nullptr) {
+        const bool first = p0 != nullptr;
+        uint32_t m[V];
+        ld_vec<V>((first ? p0 : p1) + idx, m);
+#pragma unroll
+        for (int v = 0; v < V; v++) {
+          sb[o][v] = add_mod(sb[o][v], mont_mul(first ? xb0[v] : xb1[v], m[v], q, qi), q);
+          sa[o][v] = add_mod(sa[o][v], mont_mul(first ? xa0[v] : xa1[v], m[v], q, qi), q);
+        }
+      }
+    }
+  }
+  if (t < d.ins) {
     uint32_t xb_[V], xa_[V];
     ld_vec<V>(d.in_b[c][t] + idx, xb_);
     ld_vec<V>(d.in_a[c][t] + idx, xa_);

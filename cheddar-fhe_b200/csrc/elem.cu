@@ -83,8 +83,24 @@ __global__ void __launch_bounds__(256) k_key_mac(const __grid_constant__ KeyMacD
   const int32_t qi = d.qinv[r];
   const size_t off = static_cast<size_t>(r) * n + i0;
   const size_t koff = static_cast<size_t>(d.key_row[r]) * n + i0;
+  const uint32_t qn = 0u - static_cast<uint32_t>(qi);
   uint32_t sb[4] = {0, 0, 0, 0}, sa[4] = {0, 0, 0, 0};
-  for (int i = 0; i < d.beta; i++) {
+  int i = 0;
+  for (; i + 1 < d.beta; i += 2) {  // two digits per Montgomery reduction
+    uint32_t mu0[4], kb0[4], ka0[4], mu1[4], kb1[4], ka1[4];
+    unpack(ld4(c.mu[i] + off), mu0);
+    unpack(ld4(d.kb[i] + koff), kb0);
+    unpack(ld4(d.ka[i] + koff), ka0);
+    unpack(ld4(c.mu[i + 1] + off), mu1);
+    unpack(ld4(d.kb[i + 1] + koff), kb1);
+    unpack(ld4(d.ka[i + 1] + koff), ka1);
+#pragma unroll
+    for (int l = 0; l < 4; l++) {
+      sb[l] = add_mod(sb[l], mont_mac2(mu0[l], kb0[l], mu1[l], kb1[l], q, qn), q);
+      sa[l] = add_mod(sa[l], mont_mac2(mu0[l], ka0[l], mu1[l], ka1[l], q, qn), q);
+    }
+  }
+  if (i < d.beta) {
     uint32_t mu[4], kb[4], ka[4];
     unpack(ld4(c.mu[i] + off), mu);
     unpack(ld4(d.kb[i] + koff), kb);
@@ -169,7 +185,7 @@ __global__ void __launch_bounds__(256) k_tensor(const __grid_constant__ TensorBa
   for (int l = 0; l < 4; l++) {
     o0[l] = mont_mul(b1[l], b2[l], q, qi);
     o2[l] = mont_mul(a1[l], a2[l], q, qi);
-    o1[l] = add_mod(mont_mul(b1[l], a2[l], q, qi), mont_mul(a1[l], b2[l], q, qi), q);
+    o1[l] = mont_mac2(b1[l], a2[l], a1[l], b2[l], q, 0u - static_cast<uint32_t>(qi));
   }
   st4(t.d0 + i0, o0[0], o0[1], o0[2], o0[3]);
   st4(t.d1 + i0, o1[0], o1[1], o1[2], o1[3]);
@@ -233,6 +249,7 @@ __global__ void __launch_bounds__(256) k_hoisted(const __grid_constant__ HoistDe
   const int32_t qi = d.qinv[r];
   const size_t off = static_cast<size_t>(r) * n + k0;
   const size_t koff = static_cast<size_t>(d.key_row[r]) * n + k0;
+  const uint32_t qn = 0u - static_cast<uint32_t>(qi);
   uint32_t mu[8][4];
 #pragma unroll
   for (int i = 0; i < 8; i++)
@@ -244,8 +261,19 @@ __global__ void __launch_bounds__(256) k_hoisted(const __grid_constant__ HoistDe
 #pragma unroll
     for (int l = 0; l < 4; l++) sb[l] = bxp[l];
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
-      if (i < d.beta) {
+    for (int i = 0; i < 8; i += 2) {
+      if (i + 1 < d.beta) {  // two digits per Montgomery reduction
+        uint32_t kb0[4], ka0[4], kb1[4], ka1[4];
+        unpack(ld4(d.kb[j][i] + koff), kb0);
+        unpack(ld4(d.ka[j][i] + koff), ka0);
+        unpack(ld4(d.kb[j][i + 1] + koff), kb1);
+        unpack(ld4(d.ka[j][i + 1] + koff), ka1);
+#pragma unroll
+        for (int l = 0; l < 4; l++) {
+          sb[l] = add_mod(sb[l], mont_mac2(mu[i][l], kb0[l], mu[i + 1][l], kb1[l], q, qn), q);
+          sa[l] = add_mod(sa[l], mont_mac2(mu[i][l], ka0[l], mu[i + 1][l], ka1[l], q, qn), q);
+        }
+      } else if (i < d.beta) {
         uint32_t kb[4], ka[4];
         unpack(ld4(d.kb[j][i] + koff), kb);
         unpack(ld4(d.ka[j][i] + koff), ka);

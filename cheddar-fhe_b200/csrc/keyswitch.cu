@@ -83,7 +83,7 @@ __global__ void __launch_bounds__(256, 3) k_ks_rows(const __grid_constant__ KSRo
 #pragma unroll
       for (int k = 0; k < 8; k++) {
         const uint32_t d0 = mont_mul(b1[k], b2[k], q, qi);
-        const uint32_t d1 = add_mod(mont_mul(b1[k], a2[k], q, qi), mont_mul(a1[k], b2[k], q, qi), q);
+        const uint32_t d1 = mont_mac2(b1[k], a2[k], a1[k], b2[k], q, 0u - static_cast<uint32_t>(qi));
         sb[k] = add_mod(sb[k], mont_mul(d0, pp, q, qi), q);
         sa[k] = add_mod(sa[k], mont_mul(d1, pp, q, qi), q);
       }
