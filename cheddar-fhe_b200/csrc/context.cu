@@ -1158,9 +1158,11 @@ Status Context::moddown_plan(int level, MDType type, MDPlan *pl) const {
   return kOk;
 }
 
-Status Context::key_switch_fused(int level, int count, const KSIn *in, const DeviceEvk &key, MDType type) {
+Status Context::key_switch_fused(int level, int count, const KSIn *in, const DeviceEvk &key, MDType type,
+                                 bool keep_ext) {
   CHD_CHECK(P->log_n == 16, kErrUnsupported, "fused key switch needs N = 2^16");
-  CHD_CHECK(type != MDType::kRescale, kErrInvalidArg, "fused key switch ends in ModDown or ModDownAndRescale");
+  CHD_CHECK(keep_ext || type != MDType::kRescale, kErrInvalidArg,
+            "fused key switch ends in ModDown or ModDownAndRescale");
   const LevelMS &m = lms(level);
   const int n = P->n;
   NP np = P->level_np(level, P->alpha);
@@ -1168,7 +1170,7 @@ Status Context::key_switch_fused(int level, int count, const KSIn *in, const Dev
   CHD_CHECK(tot <= 64 && m.beta <= 8, kErrUnsupported, "key switch: more than 64 primes or 8 digits");
   CHD_CHECK(key.np.aux == P->alpha && key.np.q() == P->L, kErrKey, "key switch: key basis mismatch");
   MDPlan pl;
-  CHD_TRY(moddown_plan(level, type, &pl));
+  if (!keep_ext) CHD_TRY(moddown_plan(level, type, &pl));
   const int prime_offset = P->max_ter - np.ter;
   std::vector<int> g(tot);
   P->gidx(np, g.data());
@@ -1183,9 +1185,11 @@ Status Context::key_switch_fused(int level, int count, const KSIn *in, const Dev
   const size_t N = static_cast<size_t>(n);
   uint32_t *t1 = static_cast<uint32_t *>(arena.alloc(count * nq * N * 4));
   uint32_t *mu = static_cast<uint32_t *>(arena.alloc(count * nb * tot * N * 4));
-  uint32_t *acc = static_cast<uint32_t *>(arena.alloc(count * 2 * tot * N * 4));
-  uint32_t *drop = static_cast<uint32_t *>(arena.alloc(count * 2 * pl.src_len * N * 4));
-  CHD_CHECK(t1 && mu && acc && drop, kErrAlloc, "key switch: scratch allocation failed");
+  // keep_ext: the accumulators go straight to the callers' buffers and
+  // nothing is dropped
+  uint32_t *acc = keep_ext ? nullptr : static_cast<uint32_t *>(arena.alloc(count * 2 * tot * N * 4));
+  uint32_t *drop = keep_ext ? nullptr : static_cast<uint32_t *>(arena.alloc(count * 2 * pl.src_len * N * 4));
+  CHD_CHECK(t1 && mu && (keep_ext || (acc && drop)), kErrAlloc, "key switch: scratch allocation failed");
   auto MU = [&](int c, int b) { return mu + (static_cast<size_t>(c) * nb + b) * tot * N; };
   // 1. ModUp INTT row phase of the key-switched input (a1 a2 / ax / rx)
   std::vector<RowDesc> rows;
@@ -1278,7 +1282,8 @@ Status Context::key_switch_fused(int level, int count, const KSIn *in, const Dev
       for (int bi = 0; bi < nb; bi++)
         if (r >= m.dig_s[digits[bi]] && r < m.dig_e[digits[bi]]) d.own_digit[r] = static_cast<int8_t>(bi);
     }
-    for (int i = 0; i < pl.src_len; i++) d.drop_idx[pl.srows[i]] = static_cast<int8_t>(i);
+    if (!keep_ext)
+      for (int i = 0; i < pl.src_len; i++) d.drop_idx[pl.srows[i]] = static_cast<int8_t>(i);
     nl = 0;
     t0 = timer_mark();
     for (int c0 = 0; c0 < count; c0 += kMaxKSRowsCts) {
@@ -1292,16 +1297,22 @@ Status Context::key_switch_fused(int level, int count, const KSIn *in, const Dev
         k.a1 = x.a1;
         k.b2 = x.b2;
         k.a2 = x.a2;
-        k.acc_b = acc + static_cast<size_t>(c0 + c) * 2 * tot * N;
-        k.acc_a = k.acc_b + static_cast<size_t>(tot) * N;
-        k.drop_b = drop + static_cast<size_t>(c0 + c) * 2 * pl.src_len * N;
-        k.drop_a = k.drop_b + static_cast<size_t>(pl.src_len) * N;
+        if (keep_ext) {
+          k.acc_b = x.out_b;
+          k.acc_a = x.out_a;
+        } else {
+          k.acc_b = acc + static_cast<size_t>(c0 + c) * 2 * tot * N;
+          k.acc_a = k.acc_b + static_cast<size_t>(tot) * N;
+          k.drop_b = drop + static_cast<size_t>(c0 + c) * 2 * pl.src_len * N;
+          k.drop_a = k.drop_b + static_cast<size_t>(pl.src_len) * N;
+        }
       }
       launch_ks_rows(d, P->log_n, stream);
       nl++;
     }
     timer_span(kKsRows, t0, nl);
   }
+  if (keep_ext) return check_cuda("key switch");
   // 4. ModDown column pass per (ciphertext, part)
   {
     MSColBatch b{};

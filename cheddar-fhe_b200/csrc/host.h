@@ -368,7 +368,14 @@ class Context {
     const uint32_t *b1, *a1, *b2, *a2;
     uint32_t *out_b, *out_a;
   };
-  Status key_switch_fused(int level, int count, const KSIn *in, const DeviceEvk &key, MDType type);
+  // INTT rows -> ModUp column pass -> key-switch row pass -> ModDown column
+  // pass -> NTT rows with the ModDown epilogue, for `count` inputs.  With
+  // keep_ext the pipeline stops after the row pass: out_b / out_a receive the
+  // accumulators over every prime of Q u P (evaluation domain), `type` is
+  // unused, and mode 1 with b1 == nullptr leaves out the P * bx term (the
+  // bare inner product sum_i ModUp(a1)_i (.) key_i).
+  Status key_switch_fused(int level, int count, const KSIn *in, const DeviceEvk &key, MDType type,
+                          bool keep_ext = false);
   // ModDown family on npoly polys
   Status moddown(int level, MDType type, const uint32_t *const *src, uint32_t *const *dst, int npoly);
   Status bconv(const int32_t *xt, int K, const int32_t *table, const int *dst_gidx, int M, uint32_t *out);

@@ -71,9 +71,9 @@ __global__ void __launch_bounds__(256, 3) k_ks_rows(const __grid_constant__ KSRo
       sa[k] = add_mod(sa[k], mont_mul(v[k], ka[k], q, qi), q);
     }
   }
-  if (is_q) {
+  if (is_q && c.b1 != nullptr) {
     // P * (d0, d1): HMult d0 = b1 b2, d1 = b1 a2 + a1 b2; MultKey d0 = bx;
-    // Relinearize d0 = bx, d1 = ax
+    // Relinearize d0 = bx, d1 = ax.  Without b1: the bare inner product.
     const uint32_t pp = d.p_prod[j];
     uint32_t b1[8];
     ld8(c.b1 + qoff, b1);

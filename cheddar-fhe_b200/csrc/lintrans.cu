@@ -710,8 +710,16 @@ Status Context::lt_evaluate_batch(int count, DeviceCt *const *res, const DeviceC
     CHD_CHECK(k, kErrKey, "Hoist: missing rotation key " + std::to_string(gsr));
     for (int c = 0; c < count; c++) src[c] = outs[c][i].second;
     CHD_TRY(moddown(level, MDType::kModDown, src.data(), md.data(), count));
-    CHD_TRY(modup_many(level, count, md.data(), mu_p.data()));
-    CHD_TRY(H.key_mult(count, mu_p.data(), *k, tb.data(), ta.data()));
+    if (P->log_n == 16) {
+      // ModUp and key product fused: the ModUp NTT rows feed the inner
+      // product without a round trip through HBM
+      std::vector<KSIn> ks(count);
+      for (int c = 0; c < count; c++) ks[c] = KSIn{1, nullptr, md[c], nullptr, nullptr, tb[c], ta[c]};
+      CHD_TRY(key_switch_fused(level, count, ks.data(), *k, MDType::kModDown, true));
+    } else {
+      CHD_TRY(modup_many(level, count, md.data(), mu_p.data()));
+      CHD_TRY(H.key_mult(count, mu_p.data(), *k, tb.data(), ta.data()));
+    }
     for (int c = 0; c < count; c++) {
       // key-switched part plus the accumulator's own b, both rotated
       H.add_rows(tb[c], outs[c][i].first, tb[c], H.tot);
