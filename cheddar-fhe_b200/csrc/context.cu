@@ -812,11 +812,16 @@ namespace {
 // Splits a long list of rows into RowBatch launches.
 template <typename F>
 void for_row_batches(const std::vector<RowDesc> &rows, F &&launch) {
+  // as few launches as kMaxRows allows, with the rows spread evenly over
+  // them (a short last launch would leave most SMs idle)
+  const int total = static_cast<int>(rows.size());
+  const int nbat = (total + kMaxRows - 1) / kMaxRows;
+  const int per = nbat > 0 ? (total + nbat - 1) / nbat : kMaxRows;
   RowBatch rb;
   rb.count = 0;
   for (const RowDesc &r : rows) {
     rb.rows[rb.count++] = r;
-    if (rb.count == kMaxRows) {
+    if (rb.count == per) {
       launch(rb);
       rb.count = 0;
     }
