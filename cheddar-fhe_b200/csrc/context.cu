@@ -332,8 +332,10 @@ std::unique_ptr<Params> Params::create(const ParamSpec &spec, std::string *err) 
     }
   const int nm = static_cast<int>(spec.main_primes.size()), nt = static_cast<int>(spec.ter_primes.size());
   const int na = static_cast<int>(spec.aux_primes.size());
-  if (nm + nt + na > 250) {
-    *err = "too many primes";
+  if (nm + nt + na > 64) {
+    // the key switch and the per-limb descriptors of the kernels hold the
+    // extended basis Q u P in 64-entry tables
+    *err = "too many primes: at most 64 (main + terminal + auxiliary) are supported";
     return nullptr;
   }
   std::pair<int, int> prev{0, 0};

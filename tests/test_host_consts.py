@@ -40,3 +40,22 @@ def test_level_constants_match_oracle(path):
                         assert np.array_equal(x, y), (lvl, kind, d)
                     checked += 1
     assert checked > o.max_level
+
+
+def test_more_than_64_primes_rejected():
+    # the extended basis lives in 64-entry tables: a parameter set with more
+    # primes is refused when parsed (no GPU needed), not overrun later
+    p = json.load(open(PARAMS[0]))
+    p["log_degree"] = 12
+    step = 2 << 12
+    p["main_primes"] = [1 + step * k for k in range(1, 58)]
+    p["terminal_primes"] = []
+    p["auxiliary_primes"] = [1 + step * k for k in range(100, 108)]
+    p["level_config"] = [[k, 0] for k in range(2, 58)]
+    L = chd.lib()
+    L.chd_params_level_consts.restype = C.c_int
+    a = [np.zeros(64, np.uint32), np.zeros(64 * 16, np.int32), np.zeros(64, np.uint32),
+         np.zeros(64, np.uint32), np.zeros(6, np.int32)]
+    rc = L.chd_params_level_consts(json.dumps(p).encode(), 0, 0, 0, *[x.ctypes.data_as(C.c_void_p) for x in a])
+    assert rc != 0
+    assert b"64" in L.chd_last_error()
