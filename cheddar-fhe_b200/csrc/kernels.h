@@ -197,7 +197,8 @@ void launch_ks_rows(const KSRowsDesc &d, int log_n, cudaStream_t s);
 // Key-switching inner product with the P * (d0, d1) term folded in:
 //   acc_b[r] = sum_i mu_i[r] * kb_i[r] + (r < nq ? p_prod[r] * d0[r] : 0)
 //   acc_a[r] = sum_i mu_i[r] * ka_i[r] + (r < nq && d1 ? p_prod[r] * d1[r] : 0)
-// for up to kMaxKeyMacCts ciphertexts sharing one key (grid.z = ciphertext).
+// for up to kMaxKeyMacCts ciphertexts sharing one key (the ciphertext is the
+// fastest-varying part of grid.x, so the key tile is shared through L2).
 constexpr int kMaxKeyMacCts = 16;
 struct KeyMacCt {
   const uint32_t *mu[8];     // beta ModUp outputs, each [rows][N]
