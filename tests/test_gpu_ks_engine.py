@@ -247,3 +247,21 @@ def test_auto_engine(cuda_ok):
         (rb, ra), rk = rot_key(KS, 5)
         a = uniform_parts(KS, 21, 1500)
         _eq(g.HRot(g.import_ct(21, a), rk, 5), o.hrot(21, a, (rb, ra), 5))
+
+
+def test_hmult_and_hrot_every_level_both_engines(cuda_ok):
+    # every level of the key-switching set (1 .. 22, digit counts 1 .. 3,
+    # ModDownAndRescale constants of each level) on both column-pass engines,
+    # against the oracle: HMult with rescale, and a rotation
+    o, g = pair(KS)
+    (kb, ka), key = mult_key(KS)
+    (rb, ra), rkey = rot_key(KS, 5)
+    for lvl in range(1, o.max_level + 1):
+        a = uniform_parts(KS, lvl, 900 + lvl)
+        b = uniform_parts(KS, lvl, 950 + lvl)
+        ref_m = o.hmult(lvl, a, b, (kb, ka), rescale=True)
+        ref_r = o.hrot(lvl, a, (rb, ra), 5)
+        for e in (chd.BCONV_CUDA_CORE, chd.BCONV_TENSOR_CORE):
+            with engine(g, e):
+                _eq(g.HMult(g.import_ct(lvl, a), g.import_ct(lvl, b), key, rescale=True), ref_m)
+                _eq(g.HRot(g.import_ct(lvl, a), rkey, 5), ref_r)
