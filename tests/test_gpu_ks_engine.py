@@ -265,3 +265,24 @@ def test_hmult_and_hrot_every_level_both_engines(cuda_ok):
             with engine(g, e):
                 _eq(g.HMult(g.import_ct(lvl, a), g.import_ct(lvl, b), key, rescale=True), ref_m)
                 _eq(g.HRot(g.import_ct(lvl, a), rkey, 5), ref_r)
+
+
+def test_terminal_primes_n16_every_level_both_engines(cuda_ok):
+    # the terminal-prime set (rational rescale, levels alternating between
+    # 0, 2 and 4 terminal primes) at its own N = 2^16, where the key switches
+    # take the fused pipeline: HMult with rescale and a rotation at every
+    # level, both column-pass engines, against the oracle
+    rat = "rational_t4_m10_a6.json"
+    o, g = pair(rat)
+    assert g.n == 65536
+    (kb, ka), key = mult_key(rat)
+    (rb, ra), rkey = rot_key(rat, 3)
+    for lvl in range(1, o.max_level + 1):
+        a = uniform_parts(rat, lvl, 1100 + lvl)
+        b = uniform_parts(rat, lvl, 1150 + lvl)
+        ref_m = o.hmult(lvl, a, b, (kb, ka), rescale=True)
+        ref_r = o.hrot(lvl, a, (rb, ra), 3)
+        for e in (chd.BCONV_CUDA_CORE, chd.BCONV_TENSOR_CORE):
+            with engine(g, e):
+                _eq(g.HMult(g.import_ct(lvl, a), g.import_ct(lvl, b), key, rescale=True), ref_m)
+                _eq(g.HRot(g.import_ct(lvl, a), rkey, 3), ref_r)
