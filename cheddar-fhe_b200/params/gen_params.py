@@ -139,6 +139,38 @@ def boot_params(log_n=16):
     }
 
 
+def boot40_params(log_n=16):
+    """The shape of the reference's bootparam_40.json (40-bit scale from
+    32-bit words by rational rescale): 4 terminal primes near 2^25, 23 main
+    primes near 2^30 for the levels that mix main and terminal primes, 16
+    near 2^29 for the two-prime bootstrapping levels, 4 more near 2^30, and
+    12 auxiliary primes; its level table (the primes each level holds, a
+    property of the workload, kept as the reference defines it); 4 CtS and 3
+    StC levels; sparse-secret encapsulation on (dense Hamming weight 32768,
+    sparse 32).  The primes are this generator's own."""
+    used = set()
+    aux = primes_near((1 << 31) - 1, 12, used, -1)
+    ter = primes_near(1 << 25, 4, used, +1)
+    main = alternating(1 << 30, 23, used) + alternating(1 << 29, 16, used) + alternating(1 << 30, 4, used)
+    levels = [[0, 2], [3, 0], [1, 4], [4, 2], [7, 0], [5, 4], [8, 2], [11, 0], [9, 4], [12, 2], [15, 0],
+              [13, 4], [16, 2], [19, 0], [17, 4], [20, 2]] + [[k, 0] for k in range(23, 44, 2)] + [[43, 2], [43, 4]]
+    return {
+        "log_degree": log_n,
+        "log_default_scale": 40,
+        "boot": True,
+        "dense_hamming_weight": 32768,
+        "sparse_hamming_weight": 32,
+        "num_cts_levels": 4,
+        "num_stc_levels": 3,
+        "terminal_primes": ter,
+        "main_primes": main,
+        "auxiliary_primes": aux,
+        "default_encryption_level": 16,
+        "level_config": levels,
+        "additional_base": [0, 0],
+    }
+
+
 def main():
     here = os.path.dirname(os.path.abspath(__file__))
     files = {
@@ -152,6 +184,9 @@ def main():
         # the same with sparse-secret encapsulation (dense Hamming weight
         # 32768 > sparse 32), as the reference's bootparam_*.json files
         "boot_l34_a12_sse.json": dict(boot_params(), dense_hamming_weight=32768),
+        # bootstrapping with the reference's 40-bit parameter shape: 4
+        # terminal + 43 main primes (max level 28), alpha = 12
+        "boot40_l28_a12.json": boot40_params(),
     }
     for name, obj in files.items():
         with open(os.path.join(here, name), "w") as f:

@@ -1,5 +1,6 @@
-"""Batched bootstrapping at the full size (N = 2^16, 2^15 slots, the
-bootstrapping parameter set with 48 q primes and alpha = 12): BootBatch of
+"""Batched bootstrapping at the full size (N = 2^16, 2^15 slots; the
+bootstrapping parameter sets with 48 q primes, and with the reference's
+40-bit shape of 4 terminal + 43 main primes, alpha = 12): BootBatch of
 three ciphertexts equals Boot of each, bit for bit, with the hoisted and
 with the min-KS linear transforms.  At N = 2^16 every key switch runs the
 fused pipeline (column passes, key-switch row pass) and the batched kernels
@@ -18,14 +19,14 @@ import pytest
 import cheddar_b200 as chd
 
 pytestmark = pytest.mark.gpu
-BOOT = "boot_l34_a12.json"
+BOOTS = ["boot_l34_a12.json", "boot40_l28_a12.json"]
 B = 3
 
 
 @functools.lru_cache(maxsize=None)
-def _setup():
+def _setup(name):
     import torch
-    params = json.load(open(os.path.join(chd.PARAM_DIR, BOOT)))
+    params = json.load(open(os.path.join(chd.PARAM_DIR, name)))
     ctx = chd.Context(json.dumps(params))
     bc = chd.BootContext(ctx)
     rots = sorted(set(bc.rotations()) | set(bc.rotations(min_ks=True)))
@@ -55,14 +56,29 @@ def _setup():
     keys.set_conjugation(ukey())
     for r in rots:
         keys.set_rotation(r, ukey())
+    if params["dense_hamming_weight"] != params["sparse_hamming_weight"]:
+        # sparse-secret encapsulation: the dense-to-sparse key over the level
+        # -1 primes and as many auxiliary primes, the sparse-to-dense key as
+        # one digit over the whole key basis
+        m, t = ctx.level_np(-1)
+        g_dts = list(ctx.gidx(m, t, m + t))
+        dts = chd.EvaluationKey(ctx, uniform(g_dts)[None].contiguous(), uniform(g_dts)[None].contiguous(),
+                                on_device=True, basis=(m, t, m + t))
+        mm, tt = ctx.level_np(ctx.max_level)
+        std = chd.EvaluationKey(ctx, uniform(kg)[None].contiguous(), uniform(kg)[None].contiguous(),
+                                on_device=True, basis=(mm, tt, a))
+        held += [dts, std]
+        keys.set_dense_to_sparse(dts)
+        keys.set_sparse_to_dense(std)
     g0 = list(ctx.gidx(*ctx.level_np(0), 0))
     ins = [ctx.import_ct(0, [uniform(g0), uniform(g0)], on_device=True, scale=ctx.scale(0)) for _ in range(B)]
     return ctx, bc, keys, held, ins
 
 
+@pytest.mark.parametrize("name", BOOTS)
 @pytest.mark.parametrize("min_ks", [False, True])
-def test_boot_batch_equals_single_n16(cuda_ok, min_ks):
-    ctx, bc, keys, _, ins = _setup()
+def test_boot_batch_equals_single_n16(cuda_ok, name, min_ks):
+    ctx, bc, keys, _, ins = _setup(name)
     batch = bc.BootBatch(ins, keys, min_ks=min_ks)
     for i in range(B):
         one = bc.Boot(ins[i], keys, min_ks=min_ks).numpy()
