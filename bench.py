@@ -17,7 +17,7 @@ Reported (one JSON line on rank 0):
              second pass of the same steps), algorithmic bytes per launch
   cpu_baseline  the CPU oracle's HMult on the host cores (bounded sample)
   bootstrap  full-slot bootstrapping throughput at N = 2^16 (bootstraps/s;
-             --boot-precision adds a real-key run with decoded precision)
+             decoded precision with real keys: tests/boot_precision_n16.py)
   ks_engines  the same step with the ModUp / ModDown column passes on each
              engine (--ks-engine picks the measured one; default auto: the
              library times both engines on the first launch of each shape
@@ -165,9 +165,6 @@ def main():
                          "--boot-batch ciphertexts (the second is the one to read in a launch list) and exit")
     ap.add_argument("--ks-engine", default="auto", choices=["cuda", "tensor", "auto"],
                     help="base conversion inside the ModUp / ModDown column passes of the measured path")
-    ap.add_argument("--boot-precision", action="store_true",
-                    help="also bootstrap one ciphertext with real keys (oracle key generation, slow) "
-                         "and report decoded precision in bits")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -732,12 +729,13 @@ def hoist_mixed_bench(ctx, chd, key, uniform, stream, reps=5):
     return res
 
 
-BOOT_PARAM_FILE = "boot_l34_a12.json"
+BOOT_PARAM_FILE = "boot40_l28_a12.json"
 
 
 def boot_bench(chd, args, stream, dist, profile=False):
-    """Full-slot bootstrapping (N = 2^16, 2^15 slots; 48 q primes with the
-    reference's bootparam_30 level shape, alpha = 12, 4 CoeffToSlot and 3
+    """Full-slot bootstrapping (N = 2^16, 2^15 slots; the reference's 40-bit
+    bootstrapping parameter shape: 4 terminal + 43 main primes, max level 28,
+    alpha = 12, sparse-secret encapsulation, 4 CoeffToSlot and 3
     SlotToCoeff levels, EvalMod with the reference's cosine polynomial and 3
     double angles).  A step bootstraps a batch of level-0 ciphertexts in one
     BootBatch call (key switches and linear transforms batched across the
@@ -746,7 +744,7 @@ def boot_bench(chd, args, stream, dist, profile=False):
     the context stream, inputs resident.
     The evaluation keys are uniform random residues (the work is that of
     real keys; decoded precision is measured with real keys by the tests
-    and by --boot-precision)."""
+    and by tests/boot_precision_n16.py)."""
     import torch
     params = json.load(open(os.path.join(chd.PARAM_DIR, BOOT_PARAM_FILE)))
     ctx = chd.Context(json.dumps(params), device=torch.cuda.current_device())
@@ -782,6 +780,19 @@ def boot_bench(chd, args, stream, dist, profile=False):
     keys.set_conjugation(ukey())
     for r in rots:
         keys.set_rotation(r, ukey())
+    if params["dense_hamming_weight"] != params["sparse_hamming_weight"]:
+        # sparse-secret encapsulation: the dense-to-sparse key over the level
+        # -1 primes and as many auxiliary primes, the sparse-to-dense key as
+        # one digit over the whole key basis
+        m1, t1 = ctx.level_np(-1)
+        g_dts = list(ctx.gidx(m1, t1, m1 + t1))
+        held.append(chd.EvaluationKey(ctx, uniform(g_dts)[None].contiguous(), uniform(g_dts)[None].contiguous(),
+                                      on_device=True, basis=(m1, t1, m1 + t1)))
+        keys.set_dense_to_sparse(held[-1])
+        mm, tt = ctx.level_np(ctx.max_level)
+        held.append(chd.EvaluationKey(ctx, uniform(kg)[None].contiguous(), uniform(kg)[None].contiguous(),
+                                      on_device=True, basis=(mm, tt, a)))
+        keys.set_sparse_to_dense(held[-1])
     g0 = list(ctx.gidx(*ctx.level_np(0), 0))
     B = args.boot_batch
     ins = [ctx.import_ct(0, [uniform(g0), uniform(g0)], on_device=True, scale=ctx.scale(0)) for _ in range(B)]
@@ -912,42 +923,16 @@ def boot_bench(chd, args, stream, dist, profile=False):
                       "rotation_keys": len(bc.rotations(min_ks=True))},
            "unit": "bootstraps/s", "ms_per_boot": ms_graph / (B * steps), "batch_per_gpu": B, "steps": steps,
            "ks_engine": args.ks_engine, "ks_engines": engines,
-           "warmup": 2, "params": "48 q primes (bootparam_30 level shape), alpha=12, 4 CtS + 3 StC levels, "
-                                  "EvalMod deg-30 Chebyshev cosine + 3 double angles",
+           "warmup": 2, "params": f"{BOOT_PARAM_FILE}: the reference's 40-bit bootstrapping shape (4 terminal + "
+                                  "43 main primes, max level 28, alpha=12, sparse-secret encapsulation), "
+                                  "4 CtS + 3 StC levels, EvalMod deg-30 Chebyshev cosine + 3 double angles",
            "rotation_keys": len(bc.rotations()), "plan_seconds": plan_s,
            "keys": "uniform random residues (same work as real keys)",
            "levels": {"cts_start": bc.cts_start, "eval_mod_start": bc.eval_mod_start,
                       "stc_start": bc.stc_start, "end": bc.end_level}}
-    if args.boot_precision:
-        res["precision"] = boot_precision(chd, ctx, bc, params)
     del ins, outs, keys, held
     ctx.close()
     return res
-
-
-def boot_precision(chd, ctx, bc, params):
-    """One bootstrap with real keys (oracle key generation): decoded
-    precision in bits against the input slots (uniform in [-1, 1]^2)."""
-    import numpy as np
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import pyoracle as po
-    o = po.Oracle(params)
-    s = o.gen_secret(99, 32)
-    keys = chd.EvkMap(ctx)
-    held = [ctx.evk(*o.gen_mult_key(77, s)), ctx.evk(*o.gen_conj_key(78, s))]
-    keys.set_mult(held[0])
-    keys.set_conjugation(held[1])
-    for r in bc.rotations():
-        k = ctx.evk(*o.gen_rot_key(1000 + r, s, r))
-        held.append(k)
-        keys.set_rotation(r, k)
-    rng = np.random.default_rng(2024)
-    msg = (rng.random(o.n // 2) * 2 - 1) + 1j * (rng.random(o.n // 2) * 2 - 1)
-    bx, ax = o.encrypt(5, s, 0, o.encode(0, o.scale(0), msg))
-    r = bc.Boot(ctx.import_ct(0, [bx, ax], o.scale(0)), keys)
-    dec = o.decode(bc.end_level, bc.final_scale, o.decrypt(s, bc.end_level, r.numpy()), o.n // 2)
-    err = float(np.abs(dec - msg).max())
-    return {"bits": -float(np.log2(err)), "max_abs_error": err, "slots": o.n // 2}
 
 
 KERNEL_OF_STAGE = {
