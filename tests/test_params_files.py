@@ -1,0 +1,55 @@
+"""The parameter files shipped with the library are exactly what
+cheddar-fhe_b200/params/gen_params.py generates, and every prime in them is
+distinct, below 2^31, prime and NTT-friendly for N = 2^16 (p = 1 mod 2^17),
+as Parameter.cu:40-62 of the reference requires (no GPU needed)."""
+import importlib.util
+import json
+import os
+
+import pytest
+
+PARAMS = os.path.join(os.path.dirname(__file__), "..", "cheddar-fhe_b200", "params")
+
+
+def _gen():
+    spec = importlib.util.spec_from_file_location("gen_params", os.path.join(PARAMS, "gen_params.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+GEN = _gen()
+FILES = {
+    "keyswitch_l24_a8.json": lambda: GEN.keyswitch_params(24, 8),
+    "keyswitch_l8_a3.json": lambda: GEN.keyswitch_params(8, 3),
+    "rational_t4_m10_a6.json": GEN.rational_params,
+    "boot_l34_a12.json": GEN.boot_params,
+    "boot_l34_a12_sse.json": lambda: dict(GEN.boot_params(), dense_hamming_weight=32768),
+    "boot40_l28_a12.json": GEN.boot40_params,
+}
+
+
+@pytest.mark.parametrize("name", sorted(FILES))
+def test_file_is_generated(name):
+    assert json.load(open(os.path.join(PARAMS, name))) == FILES[name]()
+
+
+@pytest.mark.parametrize("name", sorted(FILES))
+def test_primes_valid(name):
+    p = json.load(open(os.path.join(PARAMS, name)))
+    primes = p["terminal_primes"] + p["main_primes"] + p["auxiliary_primes"]
+    assert len(set(primes)) == len(primes)
+    for q in primes:
+        assert q < (1 << 31) and q % (1 << 17) == 1 and GEN.is_prime(q)
+    assert len(primes) <= 64
+    # every level holds at most the primes the set has, and the top level all of them
+    main, ter = len(p["main_primes"]), len(p["terminal_primes"])
+    assert all(0 <= m <= main and 0 <= t <= ter for m, t in p["level_config"])
+    assert p["level_config"][-1] == [main, ter]
+
+
+def test_boot40_shape():
+    p = json.load(open(os.path.join(PARAMS, "boot40_l28_a12.json")))
+    assert (len(p["terminal_primes"]), len(p["main_primes"]), len(p["auxiliary_primes"])) == (4, 43, 12)
+    assert len(p["level_config"]) == 29 and p["default_encryption_level"] == 16
+    assert p["log_default_scale"] == 40 and p["dense_hamming_weight"] != p["sparse_hamming_weight"]
