@@ -8,7 +8,7 @@ fused pipeline (column passes, key-switch row pass) and the batched kernels
 giant-step key switches kept in Q u P), which the N = 2^12 bootstrapping
 tests do not reach.  Keys and inputs are uniform random residues: the
 residue arithmetic, not decryption, is under test (decoded precision at this
-size is measured by bench.py --boot-precision)."""
+size is measured by tests/boot_precision_n16.py)."""
 import functools
 import json
 import os
