@@ -105,7 +105,9 @@ int chd_ct_export(chd_context *ctx, const chd_ciphertext *ct, uint32_t *bx, uint
 /* Ciphertext::GetNP / HasRx / GetScale / GetNumSlots */
 int chd_ct_info(const chd_ciphertext *ct, int *num_main, int *num_ter, int *num_aux, int *has_rx,
                 double *scale, int *num_slots);
-/* device pointers of the parts (valid until the ciphertext changes shape) */
+/* device pointers of the parts (valid until the ciphertext changes shape);
+ * the reference exposes them as the public bx_ / ax_ / rx_ DeviceVectors
+ * (include/core/Container.h:147-156) */
 int chd_ct_device_ptrs(const chd_ciphertext *ct, uint32_t **bx, uint32_t **ax, uint32_t **rx);
 
 /* ---- evaluation keys (include/core/Container.h:283-344, EvkMap.h:23-26) --- */
@@ -115,6 +117,7 @@ int chd_evk_create(chd_context *ctx, int beta, const uint32_t *bx, const uint32_
 void chd_evk_destroy(chd_evk *evk);
 
 /* ---- evaluator (include/core/Context.h:101-423) ----------------------------- */
+/* Context::Add / Sub / Neg (Context.cpp:146-169, 205-229, 306-315) */
 int chd_add(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_ciphertext *b);
 int chd_sub(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_ciphertext *b);
 int chd_neg(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a);
@@ -128,11 +131,15 @@ int chd_add_const(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a
 /* Context::Mult(Ct, Ct, Pt): pt_dev = [num_q][N] device residues */
 int chd_mult_plain(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a,
                    const uint32_t *pt_dev, double pt_scale);
+/* Context::MultImaginaryUnit (Context.cpp:550-560) */
 int chd_mult_imaginary_unit(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a);
+/* Context::Rescale (Context.cpp:740-775) */
 int chd_rescale(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a);
+/* Context::Relinearize / RelinearizeRescale (Context.cpp:562-565, 715-738) */
 int chd_relinearize(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *key);
 int chd_relinearize_rescale(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a,
                             const chd_evk *key);
+/* Context::MultKey (Context.cpp:585-608) */
 int chd_mult_key(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *key);
 /* Context::HMult(res, a, b, mult_key, rescale) (Context.cpp:862-871) */
 int chd_hmult(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a,
@@ -350,6 +357,8 @@ int chd_boot_create_variant(chd_context *ctx, int num_slots, int variant, int nu
 void chd_boot_destroy(chd_boot *b);
 int chd_boot_rotations(const chd_boot *b, int min_ks, int *out, int cap, int *count);
 int chd_boot_levels(const chd_boot *b, int *levels, double *scales);
+/* (no counterpart: exports of the compiled plan -- op program, linear
+ * transforms and their plaintexts -- for checkers) */
 int chd_boot_json(const chd_boot *b, char *buf, size_t cap, size_t *len);
 int chd_boot_lt_info(const chd_boot *b, int i, int *level, double *scale, int *npts, int *width);
 int chd_boot_lt_pt(const chd_boot *b, int i, int j, int *gs, int *bs, double *re, double *im);
