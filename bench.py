@@ -163,6 +163,8 @@ def main():
     ap.add_argument("--boot-profile", action="store_true",
                     help="profiling aid: set up the bootstrapping workload, run two BootBatch calls of "
                          "--boot-batch ciphertexts (the second is the one to read in a launch list) and exit")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own sm_100a build on the same workloads")
     ap.add_argument("--ks-engine", default="auto", choices=["cuda", "tensor", "auto"],
                     help="base conversion inside the ModUp / ModDown column passes of the measured path")
     args = ap.parse_args()
@@ -262,7 +264,7 @@ def main():
     bconv_cmp = bconv_engines(ctx, chd, stream)
 
     # ---- NTT round trip (forward + inverse), 24 primes ----
-    ntt_cmp = ntt_bench(ctx, chd, stream)
+    ntt_cmp = ntt_bench(chd, stream)
 
     # ---- hoisted rotations and a mixed-level batch ----
     hoist_mixed = hoist_mixed_bench(ctx, chd, key, uniform, stream)
@@ -283,6 +285,23 @@ def main():
         "bootstrap": boot, "hoisted_and_mixed": hoist_mixed,
         "gpu_launches": launches,
     }
+    if rank == 0 and world == 1 and not args.no_reference_gpu:
+        ref = reference_gpu_run(args)
+        try:
+            ref["hmult_ours_over_reference"] = value / ref["hmult"]["hmult_per_s"]
+            ref["e2e_hmult_ours_over_reference"] = e2e["value"] / ref["hmult"]["hmult_per_s"]
+        except (KeyError, TypeError, ZeroDivisionError):
+            pass
+        try:
+            ref["ntt_ours_over_reference"] = (ref["ntt"]["us_per_roundtrip"] /
+                                              ntt_cmp["batched"]["us_per_round_trip"])
+        except (KeyError, TypeError, ZeroDivisionError):
+            pass
+        try:
+            ref["boot_ours_over_reference"] = (ref["bootstrap"]["hoisted"]["ms_per_boot"] / boot["ms_per_boot"])
+        except (KeyError, TypeError, ZeroDivisionError):
+            pass
+        line["reference_gpu"] = ref
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             v, cnt, el = cpu_baseline_run(max_seconds=20.0)
@@ -534,13 +553,18 @@ def plain_vs_batched_hmult(ctx, chd, key, a_cts, b_cts, outs, stream, steps):
             "speedup": ms_plain / ms_tc}
 
 
-def ntt_bench(ctx, chd, stream, count=32, reps=10):
+NTT_PARAM_FILE = "ntt_bootparam30_p24.json"
+
+
+def ntt_bench(chd, stream, counts=(32, 1), reps=10):
     """Negacyclic NTT round trip (forward, then inverse) at N = 2^16 over the
-    24 q primes of the key-switching parameter set, `count` polynomials per
-    launch pair (32 x 24 limbs = 201 MB, larger than L2).  Uniform residues
-    from a seed; the round trip must return the input unchanged.
-    Algorithmic bytes per polynomial: 2 transforms x (read + write) x 24
-    limbs x 256 KiB = 25.17 MB."""
+    24 primes main_primes[2..25] of the reference's bootparam_30.json
+    (params/ntt_bootparam30_p24.json), `count` polynomials per launch pair:
+    32 (32 x 24 limbs = 201 MB, larger than L2) for throughput, and 1 for
+    the single-polynomial latency.  Uniform residues from a seed; the round
+    trip must return the input unchanged.  Algorithmic bytes per
+    polynomial: 2 transforms x (read + write) x 24 limbs x 256 KiB =
+    25.17 MB."""
     import torch
     peaks = {}
     try:
@@ -548,39 +572,78 @@ def ntt_bench(ctx, chd, stream, count=32, reps=10):
     except Exception:
         pass
     hbm = peaks.get("hbm_gbs", 6650.0)
+    params = json.load(open(os.path.join(chd.PARAM_DIR, NTT_PARAM_FILE)))
+    ctx = chd.Context(json.dumps(params), device=torch.cuda.current_device())
+    ctx.set_stream(stream.cuda_stream)
     lvl = ctx.max_level
     m, t = ctx.level_np(lvl)
     n = ctx.n
-    allp = torch.tensor(chd_primes(ctx), dtype=torch.int64, device="cuda")
-    g = torch.tensor(ctx.gidx(m, t, 0), dtype=torch.int64, device="cuda")
+    allp = torch.tensor(params["main_primes"], dtype=torch.int64, device="cuda")
     gen = torch.Generator(device="cuda").manual_seed(0)
-    q = allp[g][None, :, None]
-    x = (torch.randint(0, 2 ** 62, (count, m + t, n), generator=gen, device="cuda", dtype=torch.int64) % q)
-    x = x.to(torch.int32).contiguous()
-    ref = x.clone()
-    torch.cuda.synchronize()
+    q = allp[None, :m, None]
+    out = {"params": f"{NTT_PARAM_FILE}: main_primes[2..25] of the reference's bootparam_30.json"}
+    for count in counts:
+        x = (torch.randint(0, 2 ** 62, (count, m + t, n), generator=gen, device="cuda", dtype=torch.int64) % q)
+        x = x.to(torch.int32).contiguous()
+        ref = x.clone()
+        torch.cuda.synchronize()
 
-    def trip():
-        ctx.ntt_raw(m, t, 0, x, mont=True, count=count)
-        ctx.intt_raw(m, t, 0, x, mont=True, count=count)
+        def trip():
+            ctx.ntt_raw(m, t, 0, x, mont=True, count=count)
+            ctx.intt_raw(m, t, 0, x, mont=True, count=count)
 
-    for _ in range(3):
-        trip()
-    ctx.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(reps):
-        trip()
-    e1.record(stream)
-    ctx.synchronize()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / (reps * count)  # per polynomial round trip
-    exact = bool(torch.equal(x, ref))
-    nbytes = 2 * 2 * (m + t) * n * 4
-    return {"workload": f"NTT + INTT round trip, N=2^16, {m + t} primes, {count} polys per launch pair",
-            "round_trips_per_s": 1e3 / ms, "us_per_round_trip": 1e3 * ms,
-            "GB/s": nbytes / (ms * 1e-3) / 1e9, "hbm_frac": nbytes / (ms * 1e-3) / 1e9 / hbm,
-            "algorithmic_bytes_per_round_trip": nbytes, "round_trip_exact": exact}
+        for _ in range(3):
+            trip()
+        ctx.synchronize()
+        r = reps if count > 1 else 10 * reps
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(r):
+            trip()
+        e1.record(stream)
+        ctx.synchronize()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / (r * count)  # per polynomial round trip
+        exact = bool(torch.equal(x, ref))
+        nbytes = 2 * 2 * (m + t) * n * 4
+        key = "batched" if count > 1 else "one_polynomial"
+        out[key] = {"workload": f"NTT + INTT round trip, N=2^16, {m + t} primes, {count} polys per launch pair",
+                    "round_trips_per_s": 1e3 / ms, "us_per_round_trip": 1e3 * ms,
+                    "GB/s": nbytes / (ms * 1e-3) / 1e9, "hbm_frac": nbytes / (ms * 1e-3) / 1e9 / hbm,
+                    "algorithmic_bytes_per_round_trip": nbytes, "round_trip_exact": exact}
+        del x, ref
+    ctx.close()
+    return out
+
+
+def reference_gpu_run(args):
+    """The reference's own evaluator (its sources compiled for sm_100a,
+    oracle/_ref/libcheddar_ref.so) timed on this GPU on the same workloads:
+    HMult+relin+rescale at the top level of the key-switching set (`batch`
+    distinct pairs per step, one HMult per call: the reference has no
+    batched entry point), the 24-prime NTT round trip, and full-slot
+    bootstrapping of bootparam_40.json (hoisted and min-KS).  Each workload
+    runs in its own process (the reference keeps per-parameter-set state
+    process-wide); CUDA events on the legacy stream the reference uses."""
+    script = os.path.join(ROOT, "oracle", "ref_bench.py")
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libcheddar_ref.so")):
+        return {"unavailable": "oracle/_ref/libcheddar_ref.so not built"}
+    jobs = [("hmult", ["hmult", PARAM_FILE, str(args.batch), str(max(args.steps, 10)), "3"]),
+            ("ntt", ["ntt", "24", "32", "10", "3"]),
+            ("ntt_one_polynomial", ["ntt", "24", "1", "100", "3"])]
+    if not args.no_boot:
+        jobs.append(("bootstrap", ["boot", BOOT_PARAM_FILE, "5", "2"]))
+    out = {"build": "the reference's src/core, src/extension, src/UserInterface.cu compiled for sm_100a "
+                    "(oracle/Makefile target ref) with project-written rmm / libtommath stand-ins"}
+    for name, argv in jobs:
+        try:
+            r = subprocess.run([sys.executable, script] + argv, capture_output=True, text=True, timeout=1200)
+            lines = [x for x in r.stdout.splitlines() if x.startswith("{")]
+            out[name] = json.loads(lines[-1]) if r.returncode == 0 and lines else \
+                {"failed": f"rc {r.returncode}: {r.stderr[-300:]}"}
+        except Exception as e:  # pragma: no cover
+            out[name] = {"failed": str(e)}
+    return out
 
 
 def bconv_engines(ctx, chd, stream, npoly=64, reps=10):
@@ -729,22 +792,22 @@ def hoist_mixed_bench(ctx, chd, key, uniform, stream, reps=5):
     return res
 
 
-BOOT_PARAM_FILE = "boot40_l28_a12.json"
+BOOT_PARAM_FILE = "bootparam_40.json"
 
 
 def boot_bench(chd, args, stream, dist, profile=False):
-    """Full-slot bootstrapping (N = 2^16, 2^15 slots; the reference's 40-bit
-    bootstrapping parameter shape: 4 terminal + 43 main primes, max level 28,
-    alpha = 12, sparse-secret encapsulation, 4 CoeffToSlot and 3
-    SlotToCoeff levels, EvalMod with the reference's cosine polynomial and 3
-    double angles).  A step bootstraps a batch of level-0 ciphertexts in one
+    """Full-slot bootstrapping (N = 2^16, 2^15 slots) on the reference's own
+    bootparam_40.json (4 terminal + 43 main primes, max level 28, alpha = 12,
+    sparse-secret encapsulation, 4 CoeffToSlot and 3 SlotToCoeff levels,
+    EvalMod with the reference's cosine polynomial and 3 double angles).  A step bootstraps a batch of level-0 ciphertexts in one
     BootBatch call (key switches and linear transforms batched across the
     ciphertexts), captured once as a CUDA graph and replayed; the eager
     batched call and one Boot per ciphertext are timed too.  CUDA events on
     the context stream, inputs resident.
     The evaluation keys are uniform random residues (the work is that of
-    real keys; decoded precision is measured with real keys by the tests
-    and by tests/boot_precision_n16.py)."""
+    real keys; decoded precision with the reference's own keys is measured
+    by tests/test_gpu_refpin.py, whose bootstraps equal the reference's
+    residue for residue)."""
     import torch
     params = json.load(open(os.path.join(chd.PARAM_DIR, BOOT_PARAM_FILE)))
     ctx = chd.Context(json.dumps(params), device=torch.cuda.current_device())
@@ -923,9 +986,10 @@ def boot_bench(chd, args, stream, dist, profile=False):
                       "rotation_keys": len(bc.rotations(min_ks=True))},
            "unit": "bootstraps/s", "ms_per_boot": ms_graph / (B * steps), "batch_per_gpu": B, "steps": steps,
            "ks_engine": args.ks_engine, "ks_engines": engines,
-           "warmup": 2, "params": f"{BOOT_PARAM_FILE}: the reference's 40-bit bootstrapping shape (4 terminal + "
-                                  "43 main primes, max level 28, alpha=12, sparse-secret encapsulation), "
-                                  "4 CtS + 3 StC levels, EvalMod deg-30 Chebyshev cosine + 3 double angles",
+           "warmup": 2, "params": f"{BOOT_PARAM_FILE}: the reference's own 40-bit bootstrapping parameter file "
+                                  "(4 terminal + 43 main primes, max level 28, alpha=12, sparse-secret "
+                                  "encapsulation), 4 CtS + 3 StC levels, EvalMod deg-30 Chebyshev cosine + 3 "
+                                  "double angles",
            "rotation_keys": len(bc.rotations()), "plan_seconds": plan_s,
            "keys": "uniform random residues (same work as real keys)",
            "levels": {"cts_start": bc.cts_start, "eval_mod_start": bc.eval_mod_start,

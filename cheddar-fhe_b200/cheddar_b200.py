@@ -119,6 +119,7 @@ def lib():
         "chd_moddown_raw": (i, [vp, i, i, vp, vp, i]),
         "chd_bconv_raw": (i, [vp, vp, i32p, i, i32p, i, vp]),
         "chd_bconv_batch": (i, [vp, i, i, vp, i32p, i, i32p, i, vp]),
+        "chd_debug_stall_tensor_waits": (i, [vp, i]),
         "chd_encode": (i, [vp, i, d, vp, vp, i, i, vp, C.POINTER(i)]),
         "chd_encode_const": (i, [vp, i, d, d, i, vp]),
         "chd_modup_to_max": (i, [vp, vp, vp, vp]),

@@ -56,7 +56,7 @@ __device__ __forceinline__ uint32_t split_s8(int32_t x) {
 template <int TPI>
 __global__ void __launch_bounds__(128) k_bconv_tc(const __grid_constant__ BConvTcDesc d) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ __align__(8) uint64_t mbar[3];  // two accumulator buffers + the stall-test barrier
   __shared__ uint32_t tmem_slot;
   const int t = threadIdx.x, w = t >> 5;
   const int KS = d.ksteps, NB = d.nb, K = d.K, M = d.M;
@@ -65,6 +65,7 @@ __global__ void __launch_bounds__(128) k_bconv_tc(const __grid_constant__ BConvT
   uint8_t *sb = smem + 2 * abuf;                      // KS x NB x 32 bytes
   const uint32_t sa_u = smem_u32(sa), sb_u = smem_u32(sb);
   const uint32_t bar0 = smem_u32(&mbar[0]), bar1 = smem_u32(&mbar[1]);
+  const uint32_t bar_never = smem_u32(&mbar[2]);  // initialised, never arrived at
 
   // B operand: already in the canonical layout, copy linearly
   {
@@ -75,6 +76,7 @@ __global__ void __launch_bounds__(128) k_bconv_tc(const __grid_constant__ BConvT
   if (t == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0) : "memory");
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar1) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_never) : "memory");
   }
   if (w == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
@@ -137,6 +139,7 @@ __global__ void __launch_bounds__(128) k_bconv_tc(const __grid_constant__ BConvT
   // phase parity of each accumulator buffer's mbarrier (bit b), kept in a
   // register
   uint32_t parity = 0u;
+  uint32_t pending = 0u;  // accumulator buffers with committed MMAs not yet waited for
   bool ok = true;
   int prev = -1;  // iteration whose accumulators wait for their epilogue
   int it = blockIdx.x;
@@ -178,16 +181,20 @@ __global__ void __launch_bounds__(128) k_bconv_tc(const __grid_constant__ BConvT
                                                                                                           : bar0)
                    : "memory");
     }
+    pending |= 1u << b;
     // next iteration's loads go out while the MMAs run
     if (it + static_cast<int>(gridDim.x) < nits) load(it + gridDim.x);
     if (prev >= 0) {
       const int pb = b ^ 1;
       // every thread polls with a limit; the CTA leaves together if any gave up
-      if (!__syncthreads_and(mbar_wait(pb ? bar1 : bar0, (parity >> pb) & 1u) ? 1 : 0)) {
+      const bool got = d.stall_polls ? mbar_wait(bar_never, 0u, d.stall_polls)
+                                     : mbar_wait(pb ? bar1 : bar0, (parity >> pb) & 1u);
+      if (!__syncthreads_and(got ? 1 : 0)) {
         ok = false;
         break;
       }
       parity ^= 1u << pb;
+      pending &= ~(1u << pb);
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       epilogue(prev, pb);
       // TMEM reads of buffer pb finish before MMAs overwrite it
@@ -199,8 +206,11 @@ __global__ void __launch_bounds__(128) k_bconv_tc(const __grid_constant__ BConvT
     // the last iteration's accumulators sit in buffer ((iterations - 1) & 1)
     const int nmine = (nits - 1 - static_cast<int>(blockIdx.x)) / static_cast<int>(gridDim.x) + 1;
     const int pb = (nmine - 1) & 1;
-    if (__syncthreads_and(mbar_wait(pb ? bar1 : bar0, (parity >> pb) & 1u) ? 1 : 0)) {
+    const bool got = d.stall_polls ? mbar_wait(bar_never, 0u, d.stall_polls)
+                                   : mbar_wait(pb ? bar1 : bar0, (parity >> pb) & 1u);
+    if (__syncthreads_and(got ? 1 : 0)) {
       parity ^= 1u << pb;
+      pending &= ~(1u << pb);
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       epilogue(prev, pb);
     } else {
@@ -209,9 +219,10 @@ __global__ void __launch_bounds__(128) k_bconv_tc(const __grid_constant__ BConvT
   }
   if (!ok) {
     if (t == 0 && d.err) atomicExch(d.err, 1);
-    // give the MMAs in flight a second bounded chance to land before TMEM is freed
-    mbar_wait(bar0, parity & 1u);
-    mbar_wait(bar1, (parity >> 1) & 1u);
+    // give the MMAs in flight (committed, not yet waited for) a second
+    // bounded chance to land before TMEM is freed
+    if (pending & 1u) mbar_wait(bar0, parity & 1u);
+    if (pending & 2u) mbar_wait(bar1, (parity >> 1) & 1u);
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();

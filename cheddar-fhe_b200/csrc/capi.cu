@@ -10,9 +10,6 @@
 
 using namespace chd;
 
-struct chd_context {
-  std::unique_ptr<Context> c;
-};
 struct chd_ciphertext {
   DeviceCt ct;
 };
@@ -61,6 +58,10 @@ int fail(int code, const std::string &msg) {
 }
 #define CHD_NOTNULL(p) \
   if (!(p)) return fail(CHD_ERR_INVALID_ARG, std::string(__func__) + ": null argument " #p)
+// a non-null context, made current (its device) for the rest of the call
+#define CHD_CTX(ctx) \
+  CHD_NOTNULL(ctx);  \
+  DeviceGuard device_guard_(ctx->c->device)
 // the kernels move device data in 16-byte vectors
 #define CHD_ALIGNED(p)                                    \
   if (reinterpret_cast<uintptr_t>(p) & 15)                \
@@ -116,10 +117,14 @@ int chd_context_create(int log_degree, double base_scale, int default_encryption
   return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
-void chd_context_destroy(chd_context *ctx) { delete ctx; }
+void chd_context_destroy(chd_context *ctx) {
+  if (!ctx) return;
+  DeviceGuard device_guard(ctx->c->device);
+  delete ctx;
+}
 
 int chd_context_set_stream(chd_context *ctx, void *cuda_stream) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   Context &C = *ctx->c;
   if (C.own_stream && C.stream) {
     cudaStreamSynchronize(C.stream);
@@ -140,7 +145,7 @@ int chd_context_set_stream(chd_context *ctx, void *cuda_stream) try {
 }
 
 int chd_stage_timing(chd_context *ctx, int enable) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   Context &C = *ctx->c;
   if (enable) {
     C.timer.used = 0;
@@ -155,7 +160,7 @@ int chd_stage_timing(chd_context *ctx, int enable) try {
 }
 
 int chd_copy(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   return ctx->c->copy_ct(res->ct, a->ct);
@@ -167,7 +172,7 @@ int chd_copy(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) try
 
 int chd_mult_unsafe(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_ciphertext *b,
                     int level) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(b);
@@ -180,7 +185,7 @@ int chd_mult_unsafe(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext 
 
 int chd_mult_unsafe_const(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *cx,
                           int const_level, double const_scale, int level) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(cx);
@@ -193,7 +198,7 @@ int chd_mult_unsafe_const(chd_context *ctx, chd_ciphertext *res, const chd_ciphe
 
 int chd_mad_unsafe(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *cx,
                    int const_level, double const_scale) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(cx);
@@ -205,7 +210,7 @@ int chd_mad_unsafe(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *
 }
 
 int chd_permute(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, int rot_dist) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   return ctx->c->permute_ct(res->ct, a->ct, rot_dist, false);
@@ -216,7 +221,7 @@ int chd_permute(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, 
 }
 
 int chd_permute_conjugate(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   return ctx->c->permute_ct(res->ct, a->ct, 0, true);
@@ -228,7 +233,7 @@ int chd_permute_conjugate(chd_context *ctx, chd_ciphertext *res, const chd_ciphe
 
 int chd_hconj_add(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_ciphertext *b,
                   const chd_evk *conj_key) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(b);
@@ -241,7 +246,7 @@ int chd_hconj_add(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a
 }
 
 int chd_level_down(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, int target_level) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   return ctx->c->level_down(res->ct, a->ct, target_level);
@@ -252,7 +257,7 @@ int chd_level_down(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *
 }
 
 int chd_mult_key_no_moddown(chd_context *ctx, chd_ciphertext *accum, const chd_ciphertext *a, const chd_evk *key) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(accum);
   CHD_NOTNULL(a);
   CHD_NOTNULL(key);
@@ -278,7 +283,7 @@ int chd_mult_unsafe_compatible(const chd_context *ctx, int level1, int level2) t
 
 int chd_add_plain(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *pt_dev,
                   double pt_scale) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(pt_dev);
@@ -292,7 +297,7 @@ int chd_add_plain(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a
 
 int chd_sub_plain(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *pt_dev,
                   double pt_scale) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(pt_dev);
@@ -305,7 +310,7 @@ int chd_sub_plain(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a
 }
 
 int chd_sub_const(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *cx) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(cx);
@@ -318,7 +323,7 @@ int chd_sub_const(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a
 
 int chd_sub_plain_ct(chd_context *ctx, chd_ciphertext *res, const uint32_t *pt_dev, double pt_scale,
                      const chd_ciphertext *b) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(pt_dev);
   CHD_ALIGNED(pt_dev);
@@ -332,7 +337,7 @@ int chd_sub_plain_ct(chd_context *ctx, chd_ciphertext *res, const uint32_t *pt_d
 
 int chd_sub_const_ct(chd_context *ctx, chd_ciphertext *res, const uint32_t *cx, double const_scale,
                      const chd_ciphertext *b) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(cx);
   CHD_NOTNULL(b);
@@ -345,7 +350,7 @@ int chd_sub_const_ct(chd_context *ctx, chd_ciphertext *res, const uint32_t *cx, 
 
 int chd_mult_unsafe_plain(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *pt_dev,
                           int pt_level, int pt_num_aux, double pt_scale, int level) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(pt_dev);
@@ -358,7 +363,7 @@ int chd_mult_unsafe_plain(chd_context *ctx, chd_ciphertext *res, const chd_ciphe
 }
 
 int chd_set_ks_engine(chd_context *ctx, int engine) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   if (engine != CHD_BCONV_CUDA_CORE && engine != CHD_BCONV_TENSOR_CORE && engine != CHD_BCONV_AUTO)
     return fail(CHD_ERR_INVALID_ARG,
                 "chd_set_ks_engine: engine must be CHD_BCONV_CUDA_CORE, CHD_BCONV_TENSOR_CORE or CHD_BCONV_AUTO");
@@ -373,7 +378,7 @@ int chd_set_ks_engine(chd_context *ctx, int engine) try {
 int chd_get_ks_engine(const chd_context *ctx) { return ctx ? ctx->c->ks_engine : -1; }
 
 int chd_stage_times(chd_context *ctx, double *ms, int *launches) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   if (!ms || !launches) return fail(CHD_ERR_INVALID_ARG, "chd_stage_times: null output");
   return ctx->c->timer_read(ms, launches);
 } catch (const std::exception &e) {
@@ -383,7 +388,7 @@ int chd_stage_times(chd_context *ctx, double *ms, int *launches) try {
 }
 
 int chd_context_synchronize(chd_context *ctx) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   Context &C = *ctx->c;
   cudaError_t e = cudaStreamSynchronize(C.stream);
   if (e != cudaSuccess) return fail(CHD_ERR_CUDA, cudaGetErrorString(e));
@@ -402,8 +407,19 @@ int chd_context_synchronize(chd_context *ctx) try {
   return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
+int chd_debug_stall_tensor_waits(chd_context *ctx, int polls) try {
+  CHD_CTX(ctx);
+  if (polls < 0) return fail(CHD_ERR_INVALID_ARG, "chd_debug_stall_tensor_waits: polls must be >= 0");
+  ctx->c->tc_stall_polls = static_cast<uint32_t>(polls);
+  return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
+}
+
 int chd_level_np(const chd_context *ctx, int level, int *num_main, int *num_ter) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   const Params &P = *ctx->c->P;
   if (level < -1 || level > P.max_level) return fail(CHD_ERR_INVALID_LEVEL, "invalid level");
   NP np = P.level_np(level, 0);
@@ -444,7 +460,7 @@ int chd_prime_gidx(const chd_context *ctx, int num_main, int num_ter, int num_au
 }
 
 int chd_ct_create(chd_context *ctx, chd_ciphertext **out) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(out);
   *out = new chd_ciphertext();
   (*out)->ct.num_slots = ctx->c->P->n / 2;
@@ -459,7 +475,7 @@ void chd_ct_destroy(chd_ciphertext *ct) { delete ct; }
 
 int chd_ct_wrap(chd_context *ctx, int num_main, int num_ter, int num_aux, int has_rx, double scale, int num_slots,
                 uint32_t *bx, uint32_t *ax, uint32_t *rx, size_t words_per_part, chd_ciphertext **out) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(out);
   CHD_NOTNULL(bx);
   CHD_NOTNULL(ax);
@@ -491,7 +507,7 @@ int chd_ct_wrap(chd_context *ctx, int num_main, int num_ter, int num_aux, int ha
 int chd_ct_import(chd_context *ctx, chd_ciphertext *ct, int num_main, int num_ter, int num_aux, int has_rx,
                   double scale, int num_slots, const uint32_t *bx, const uint32_t *ax, const uint32_t *rx,
                   int src_on_device) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(ct);
   CHD_NOTNULL(bx);
   CHD_NOTNULL(ax);
@@ -521,7 +537,7 @@ int chd_ct_import(chd_context *ctx, chd_ciphertext *ct, int num_main, int num_te
 
 int chd_ct_export(chd_context *ctx, const chd_ciphertext *ct, uint32_t *bx, uint32_t *ax, uint32_t *rx,
                   int dst_on_device) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(ct);
   Context &C = *ctx->c;
   const size_t bytes = static_cast<size_t>(ct->ct.np.total()) * C.P->n * 4;
@@ -568,7 +584,7 @@ int chd_ct_device_ptrs(const chd_ciphertext *ct, uint32_t **bx, uint32_t **ax, u
 
 int chd_evk_create(chd_context *ctx, int beta, const uint32_t *bx, const uint32_t *ax, int src_on_device,
                    chd_evk **out) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(bx);
   CHD_NOTNULL(ax);
   CHD_NOTNULL(out);
@@ -603,7 +619,7 @@ void chd_evk_destroy(chd_evk *evk) { delete evk; }
 
 #define CTX_CT3(name, call)                                                                              \
   int name(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_ciphertext *b) { \
-    CHD_NOTNULL(ctx);                                                                                  \
+    CHD_CTX(ctx);                                                                                  \
     CHD_NOTNULL(res);                                                                                  \
     CHD_NOTNULL(a);                                                                                    \
     CHD_NOTNULL(b);                                                                                    \
@@ -615,7 +631,7 @@ CTX_CT3(chd_mult, mult_tensor)
 #undef CTX_CT3
 
 int chd_neg(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   return ctx->c->neg(res->ct, a->ct);
@@ -627,7 +643,7 @@ int chd_neg(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) try 
 
 int chd_mult_const(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *cx,
                    double const_scale) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(cx);
@@ -639,7 +655,7 @@ int chd_mult_const(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *
 }
 
 int chd_add_const(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *cx) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(cx);
@@ -652,7 +668,7 @@ int chd_add_const(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a
 
 int chd_mult_plain(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const uint32_t *pt_dev,
                    double pt_scale) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(pt_dev);
@@ -665,7 +681,7 @@ int chd_mult_plain(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *
 }
 
 int chd_mult_imaginary_unit(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   return ctx->c->mult_imag_unit(res->ct, a->ct);
@@ -676,7 +692,7 @@ int chd_mult_imaginary_unit(chd_context *ctx, chd_ciphertext *res, const chd_cip
 }
 
 int chd_rescale(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   return ctx->c->rescale(res->ct, a->ct);
@@ -688,7 +704,7 @@ int chd_rescale(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) 
 
 int chd_encode(chd_context *ctx, int level, double scale, const double *re, const double *im, int msg_len,
                int num_aux, uint32_t *pt_dev, int *num_slots) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(re);
   CHD_NOTNULL(im);
   CHD_NOTNULL(pt_dev);
@@ -704,7 +720,7 @@ int chd_encode(chd_context *ctx, int level, double scale, const double *re, cons
 }
 
 int chd_encode_const(chd_context *ctx, int level, double scale, double value, int num_aux, uint32_t *cx) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(cx);
   const Params &P = *ctx->c->P;
   if (level < -1 || level > P.max_level) return fail(CHD_ERR_INVALID_LEVEL, "chd_encode_const: invalid level");
@@ -720,7 +736,7 @@ int chd_encode_const(chd_context *ctx, int level, double scale, double value, in
 }
 
 int chd_modup_to_max(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk_map *keys) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   Context &C = *ctx->c;
@@ -744,7 +760,7 @@ int chd_modup_to_max(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext
 }
 
 int chd_evk_map_create(chd_context *ctx, chd_evk_map **out) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(out);
   *out = new chd_evk_map();
   return CHD_OK;
@@ -814,7 +830,7 @@ int chd_evk_map_set_sparse_to_dense(chd_evk_map *m, const chd_evk *key) try {
 
 int chd_evk_create_np(chd_context *ctx, int num_main, int num_ter, int num_aux, int beta, const uint32_t *bx,
                       const uint32_t *ax, int src_on_device, chd_evk **out) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(bx);
   CHD_NOTNULL(ax);
   CHD_NOTNULL(out);
@@ -849,7 +865,7 @@ int chd_evk_create_np(chd_context *ctx, int num_main, int num_ter, int num_aux, 
 int chd_lintrans_create(chd_context *ctx, int width, int n_diag, const int *diag_idx, const double *re,
                         const double *im, int pt_level, double pt_scale, int bs, int gs, int pre_rotation,
                         int additional_pt_rot, chd_lintrans **out) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(diag_idx);
   CHD_NOTNULL(re);
   CHD_NOTNULL(im);
@@ -947,7 +963,7 @@ int chd_lintrans_pt(const chd_lintrans *lt, int i, int *gs, int *bs, double *re,
 
 int chd_lintrans_evaluate(chd_context *ctx, const chd_lintrans *lt, chd_ciphertext *res, const chd_ciphertext *in,
                           const chd_evk_map *keys, int min_ks) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(lt);
   CHD_NOTNULL(res);
   CHD_NOTNULL(in);
@@ -986,7 +1002,7 @@ int chd_lintrans_evaluate(chd_context *ctx, const chd_lintrans *lt, chd_cipherte
 
 int chd_poly_create(chd_context *ctx, const double *coeffs, int n, int input_level, double input_scale,
                     double target_scale, int chebyshev, chd_program **out) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(coeffs);
   CHD_NOTNULL(out);
   if (n < 1) return fail(CHD_ERR_INVALID_ARG, "chd_poly_create: no coefficients");
@@ -1012,7 +1028,7 @@ int chd_poly_create(chd_context *ctx, const double *coeffs, int n, int input_lev
 
 int chd_evalmod_create(chd_context *ctx, int start_level, const double *coeffs, int n, int num_double_angle,
                        int initial_K, chd_program **out, double *start_scale, double *end_scale) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(coeffs);
   CHD_NOTNULL(out);
   auto *pg = new chd_program();
@@ -1099,7 +1115,7 @@ Status copy_ct(Context &C, DeviceCt &dst, const DeviceCt &src) {
 
 int chd_program_run(chd_context *ctx, const chd_program *p, chd_ciphertext *res, const chd_ciphertext *in,
                     const chd_evk_map *keys) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(p);
   CHD_NOTNULL(res);
   CHD_NOTNULL(in);
@@ -1132,7 +1148,7 @@ int chd_boot_create(chd_context *ctx, int num_slots, int num_cts_levels, int num
 
 int chd_boot_create_variant(chd_context *ctx, int num_slots, int variant, int num_cts_levels, int num_stc_levels,
                             int log_message_ratio, chd_boot **out) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(out);
   auto *b = new chd_boot();
   int rc = ctx->c->boot_build(num_slots, variant, num_cts_levels, num_stc_levels, log_message_ratio, &b->plan);
@@ -1243,7 +1259,7 @@ int chd_boot_lt_pt(const chd_boot *b, int i, int j, int *gs, int *bs, double *re
 
 int chd_boot_run(chd_context *ctx, chd_boot *b, chd_ciphertext *res, const chd_ciphertext *in, const chd_evk_map *keys,
                  int min_ks) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(b);
   CHD_NOTNULL(res);
   CHD_NOTNULL(in);
@@ -1275,7 +1291,7 @@ int chd_boot_run(chd_context *ctx, chd_boot *b, chd_ciphertext *res, const chd_c
 
 int chd_boot_run_batch(chd_context *ctx, chd_boot *b, int count, chd_ciphertext *const *res,
                        const chd_ciphertext *const *in, const chd_evk_map *keys, int min_ks) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(b);
   CHD_NOTNULL(res);
   CHD_NOTNULL(in);
@@ -1325,7 +1341,7 @@ int chd_boot_run_batch(chd_context *ctx, chd_boot *b, int count, chd_ciphertext 
 }
 
 int chd_graph_begin(chd_context *ctx) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   Context &C = *ctx->c;
   if (!C.stream) return fail(CHD_ERR_INVALID_ARG, "chd_graph_begin: capture needs a non-default context stream");
   cudaError_t e = cudaStreamBeginCapture(C.stream, cudaStreamCaptureModeRelaxed);
@@ -1338,7 +1354,7 @@ int chd_graph_begin(chd_context *ctx) try {
 }
 
 int chd_graph_end(chd_context *ctx, chd_graph **out) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(out);
   Context &C = *ctx->c;
   auto *g = new chd_graph();
@@ -1358,7 +1374,7 @@ int chd_graph_end(chd_context *ctx, chd_graph **out) try {
 }
 
 int chd_graph_launch(chd_context *ctx, const chd_graph *g) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(g);
   cudaError_t e = cudaGraphLaunch(g->exec, ctx->c->stream);
   if (e != cudaSuccess) return fail(CHD_ERR_CUDA, std::string("chd_graph_launch: ") + cudaGetErrorString(e));
@@ -1372,7 +1388,7 @@ int chd_graph_launch(chd_context *ctx, const chd_graph *g) try {
 void chd_graph_destroy(chd_graph *g) { delete g; }
 
 int chd_relinearize(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *key) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(key);
@@ -1384,7 +1400,7 @@ int chd_relinearize(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext 
 }
 
 int chd_relinearize_rescale(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *key) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(key);
@@ -1396,7 +1412,7 @@ int chd_relinearize_rescale(chd_context *ctx, chd_ciphertext *res, const chd_cip
 }
 
 int chd_mult_key(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *key) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(key);
@@ -1409,7 +1425,7 @@ int chd_mult_key(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a,
 
 int chd_hmult(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_ciphertext *b,
               const chd_evk *mult_key, int rescale) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(b);
@@ -1423,7 +1439,7 @@ int chd_hmult(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, co
 
 int chd_hmult_batch(chd_context *ctx, int count, chd_ciphertext *const *res, const chd_ciphertext *const *a,
                     const chd_ciphertext *const *b, const chd_evk *mult_key, int rescale) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(b);
@@ -1445,7 +1461,7 @@ int chd_hmult_batch(chd_context *ctx, int count, chd_ciphertext *const *res, con
 }
 
 int chd_hrot(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *rot_key, int rot_dist) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(rot_key);
@@ -1457,7 +1473,7 @@ int chd_hrot(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, con
 }
 
 int chd_hconj(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_evk *conj_key) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(conj_key);
@@ -1470,7 +1486,7 @@ int chd_hconj(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, co
 
 int chd_hrot_add(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_ciphertext *b,
                  const chd_evk *rot_key, int rot_dist) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   CHD_NOTNULL(b);
@@ -1484,7 +1500,7 @@ int chd_hrot_add(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a,
 
 int chd_hoisted_rotate(chd_context *ctx, const chd_ciphertext *a, int count, const int *rot_dists,
                        const chd_evk *const *rot_keys, chd_ciphertext *const *out) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(a);
   CHD_NOTNULL(rot_dists);
   CHD_NOTNULL(rot_keys);
@@ -1505,7 +1521,7 @@ int chd_hoisted_rotate(chd_context *ctx, const chd_ciphertext *a, int count, con
 }
 
 int chd_moddown(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(res);
   CHD_NOTNULL(a);
   return ctx->c->moddown_ct(res->ct, a->ct);
@@ -1516,7 +1532,7 @@ int chd_moddown(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) 
 }
 
 int chd_ntt(chd_context *ctx, int num_main, int num_ter, int num_aux, uint32_t *data_dev, int mont, int count) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(data_dev);
   CHD_ALIGNED(data_dev);
   NP np{num_main, num_ter, num_aux};
@@ -1532,7 +1548,7 @@ int chd_ntt(chd_context *ctx, int num_main, int num_ter, int num_aux, uint32_t *
 }
 
 int chd_intt(chd_context *ctx, int num_main, int num_ter, int num_aux, uint32_t *data_dev, int mont, int count) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(data_dev);
   CHD_ALIGNED(data_dev);
   NP np{num_main, num_ter, num_aux};
@@ -1548,7 +1564,7 @@ int chd_intt(chd_context *ctx, int num_main, int num_ter, int num_aux, uint32_t 
 }
 
 int chd_modup_raw(chd_context *ctx, int level, const uint32_t *src_dev, uint32_t *dst_dev) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(src_dev);
   CHD_ALIGNED(src_dev);
   CHD_NOTNULL(dst_dev);
@@ -1567,7 +1583,7 @@ int chd_modup_raw(chd_context *ctx, int level, const uint32_t *src_dev, uint32_t
 }
 
 int chd_moddown_raw(chd_context *ctx, int level, int type, const uint32_t *src_dev, uint32_t *dst_dev, int npoly) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(src_dev);
   CHD_ALIGNED(src_dev);
   CHD_NOTNULL(dst_dev);
@@ -1622,7 +1638,7 @@ int bconv_table(const Context &C, const int *src_gidx, int K, const int *dst_gid
 
 int chd_bconv_raw(chd_context *ctx, const int32_t *xt_dev, const int *src_gidx, int K, const int *dst_gidx, int M,
                   uint32_t *out_dev) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(xt_dev);
   CHD_ALIGNED(xt_dev);
   CHD_NOTNULL(src_gidx);
@@ -1648,7 +1664,7 @@ int chd_bconv_raw(chd_context *ctx, const int32_t *xt_dev, const int *src_gidx, 
 
 int chd_bconv_batch(chd_context *ctx, int engine, int npoly, const int32_t *xt_dev, const int *src_gidx, int K,
                     const int *dst_gidx, int M, uint32_t *out_dev) try {
-  CHD_NOTNULL(ctx);
+  CHD_CTX(ctx);
   CHD_NOTNULL(src_gidx);
   CHD_NOTNULL(dst_gidx);
   if (npoly < 0) return fail(CHD_ERR_INVALID_ARG, "chd_bconv_batch: negative npoly");

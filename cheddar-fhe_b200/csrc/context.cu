@@ -969,6 +969,7 @@ Status Context::bconv_many(int engine, int npoly, const int32_t *xt, int K, cons
   d.out = out;
   d.bmat = dimg;
   d.err = d_err;
+  d.stall_polls = tc_stall_polls;
   const int rc = launch_bconv_tc(d, num_sms, stream);
   CHD_CHECK(rc == 0, kErrCuda, "bconv: tensor-core launch configuration failed");
   return check_cuda("bconv (tensor cores)");

@@ -326,6 +326,9 @@ class Context {
   uint32_t *d_primes = nullptr;
   int32_t *d_qinv = nullptr;
   int *d_err = nullptr;   // set by kernels whose bounded waits ran out
+  // test hook (chd_debug_stall_tensor_waits): > 0 makes the stand-alone
+  // tensor-core base conversion's bounded waits run out
+  uint32_t tc_stall_polls = 0;
   int num_sms = 0;
   int ks_engine = 0;      // ModUp / ModDown column-pass base conversion: 0 CUDA cores, 1 tensor cores, 2 autotuned
   uint2 *d_tw = nullptr, *d_itw = nullptr;  // [nprimes][N] (psi_rev, Shoup companion)
@@ -533,4 +536,30 @@ class Context {
 Status elem_parts(Context &C, ElemOp op, const NP &np, int parts, uint32_t *const *dst, const uint32_t *const *a,
                   const uint32_t *const *b, const uint32_t *k);
 
+// Makes `device` current for the scope of a C ABI call and restores the
+// caller's device afterwards: kernels, allocations and stream work of a
+// context always run on the device it was created on, whichever device the
+// calling thread has current.
+class DeviceGuard {
+ public:
+  explicit DeviceGuard(int device) {
+    if (cudaGetDevice(&prev_) == cudaSuccess && prev_ != device) changed_ = cudaSetDevice(device) == cudaSuccess;
+  }
+  ~DeviceGuard() {
+    if (changed_) cudaSetDevice(prev_);
+  }
+  DeviceGuard(const DeviceGuard &) = delete;
+  DeviceGuard &operator=(const DeviceGuard &) = delete;
+
+ private:
+  int prev_ = -1;
+  bool changed_ = false;
+};
+
 }  // namespace chd
+
+// The C ABI's opaque context handle (include/cheddar_b200.h), shared by the
+// translation units that implement entry points.
+struct chd_context {
+  std::unique_ptr<chd::Context> c;
+};

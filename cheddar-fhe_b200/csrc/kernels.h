@@ -90,6 +90,11 @@ struct BConvTcDesc {
   int tpi;         // 128-row tiles per CTA iteration (1, 2 or 4), each with nb TMEM columns
   int tmem_cols;   // power of two >= max(32, 2 * tpi * nb) (two accumulator buffers), <= 512
   uint32_t idesc;  // tcgen05 instruction descriptor (kind::i8, s8 x u8 -> s32, M = 128, N = nb)
+  // test hook, 0 in normal use: > 0 makes each CTA's first accumulator wait
+  // poll an mbarrier that nothing signals, this many times, so that the
+  // bounded wait runs out and the give-up path (error word, drain of the
+  // MMAs in flight, TMEM release) runs
+  uint32_t stall_polls;
   uint32_t p[64];
   int32_t pinv[64];
 };

@@ -19,16 +19,15 @@
 //     streams, other contexts on the same device) race; the scratch is fully
 //     written before it is read, so nothing needs clearing between calls;
 //   * the array's device address is looked up once per device, on the
-//     first call made with that device current; make that first call before
-//     any stream capture.
+//     first call for a context of that device (the call makes the context's
+//     device current while it runs); make that first call before any stream
+//     capture.
+#include <cstdint>
+#include <exception>
 #include <mutex>
 
 #include "../../include/cheddar_b200.h"
 #include "host.h"
-
-struct chd_context {
-  std::unique_ptr<chd::Context> c;
-};
 
 namespace chd {
 namespace {
@@ -40,11 +39,17 @@ constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 uint32_t *g_scratch_addr[kMaxDevices] = {};
 
-// Device address of g_modup_scratch on the current device (looked up once).
+// Device address of g_modup_scratch on `device`, which must be the current
+// device (looked up once per device).
 Status scratch_address(int device, uint32_t **out) {
   if (device < 0 || device >= kMaxDevices) {
     set_error("chd_modup_raw_noalloc: device index out of range");
     return kErrInvalidArg;
+  }
+  int cur = -1;
+  if (cudaGetDevice(&cur) != cudaSuccess || cur != device) {
+    set_error("chd_modup_raw_noalloc: the context's device is not current");
+    return kErrCuda;
   }
   std::lock_guard<std::mutex> lock(g_mu);
   if (!g_scratch_addr[device]) {
@@ -67,6 +72,15 @@ Status modup_small(Context &C, int level, const uint32_t *src, uint32_t *const *
   const int n = C.P->n;
   NP np = C.P->level_np(level, m.num_aux);
   const int nq = np.q(), tot = np.total();
+  // k_bconv holds at most 16 sources and 64 targets per job, as in
+  // Context::modup_many: check every digit before any work is issued
+  for (int i = 0; i < m.beta; i++) {
+    const int s = m.dig_s[i], e = m.dig_e[i];
+    if (e > 0 && (e - s > 16 || tot - (e - s) > 64)) {
+      set_error("chd_modup_raw_noalloc: a digit of more than 16 primes or more than 64 targets");
+      return kErrUnsupported;
+    }
+  }
   int g[256];
   C.P->gidx(np, g);
   RowBatch rb{};
@@ -142,13 +156,20 @@ Status modup_small(Context &C, int level, const uint32_t *src, uint32_t *const *
 }  // namespace
 }  // namespace chd
 
-extern "C" int chd_modup_raw_noalloc(chd_context *ctx, int level, const uint32_t *src_dev, uint32_t *dst_dev) {
+extern "C" int chd_modup_raw_noalloc(chd_context *ctx, int level, const uint32_t *src_dev,
+                                     uint32_t *dst_dev) try {
   using namespace chd;
   if (!ctx || !src_dev || !dst_dev) {
     set_error("chd_modup_raw_noalloc: null argument");
     return CHD_ERR_INVALID_ARG;
   }
+  // the kernels move device data in 16-byte vectors
+  if ((reinterpret_cast<uintptr_t>(src_dev) | reinterpret_cast<uintptr_t>(dst_dev)) & 15) {
+    set_error("chd_modup_raw_noalloc: device pointers must be 16-byte aligned");
+    return CHD_ERR_INVALID_ARG;
+  }
   Context &C = *ctx->c;
+  DeviceGuard device_guard(C.device);
   if (level < -1 || level > C.P->max_level) {
     set_error("chd_modup_raw_noalloc: invalid level");
     return CHD_ERR_INVALID_LEVEL;
@@ -176,4 +197,10 @@ extern "C" int chd_modup_raw_noalloc(chd_context *ctx, int level, const uint32_t
     return C.modup_fused(level, 1, srcs, dsts, scratch);
   }
   return modup_small(C, level, src_dev, dst, scratch);
+} catch (const std::exception &e) {
+  chd::set_error(std::string("chd_modup_raw_noalloc: internal error: ") + e.what());
+  return CHD_ERR_INTERNAL;
+} catch (...) {
+  chd::set_error("chd_modup_raw_noalloc: internal error");
+  return CHD_ERR_INTERNAL;
 }

@@ -171,6 +171,29 @@ def boot40_params(log_n=16):
     }
 
 
+def ntt_bootparam30_params():
+    """The NTT workload's primes: main_primes[2..25] of the reference's own
+    bootparam_30.json (shipped beside this script), the 24 primes near 2^30
+    that follow its two ~20-bit base primes, as the q basis of a 24-level
+    chain (one prime per level), with that file's first 8 auxiliary
+    primes."""
+    here = os.path.dirname(os.path.abspath(__file__))
+    ref = json.load(open(os.path.join(here, "bootparam_30.json")))
+    return {
+        "log_degree": 16,
+        "log_default_scale": 30,
+        "boot": False,
+        "dense_hamming_weight": 192,
+        "sparse_hamming_weight": 32,
+        "terminal_primes": [],
+        "main_primes": ref["main_primes"][2:26],
+        "auxiliary_primes": ref["auxiliary_primes"][:8],
+        "default_encryption_level": 23,
+        "level_config": [[i, 0] for i in range(1, 25)],
+        "additional_base": [0, 0],
+    }
+
+
 def main():
     here = os.path.dirname(os.path.abspath(__file__))
     files = {
@@ -187,6 +210,8 @@ def main():
         # bootstrapping with the reference's 40-bit parameter shape: 4
         # terminal + 43 main primes (max level 28), alpha = 12
         "boot40_l28_a12.json": boot40_params(),
+        # the NTT workload on the reference's own primes
+        "ntt_bootparam30_p24.json": ntt_bootparam30_params(),
     }
     for name, obj in files.items():
         with open(os.path.join(here, name), "w") as f:

@@ -416,6 +416,18 @@ int chd_bconv_batch(chd_context *ctx, int engine, int npoly, const int32_t *xt_d
 int chd_set_ks_engine(chd_context *ctx, int engine);
 int chd_get_ks_engine(const chd_context *ctx);
 
+/* Test hook for the bounded waits of the tensor-core kernels (no reference
+ * counterpart: the reference's kernels have no tensor-core waits).  With
+ * polls > 0 every later stand-alone tensor-core base conversion
+ * (chd_bconv_batch, engine 1) makes each CTA's first accumulator wait poll an
+ * mbarrier that nothing signals, `polls` times: the wait runs out, the
+ * kernel records the failure in the context's device error word, waits
+ * (bounded) for its MMAs in flight, releases its tensor memory and returns,
+ * and the next chd_context_synchronize reports CHD_ERR_CUDA.  Outputs of
+ * such launches are undefined.  polls = 0 (the default) restores normal
+ * operation. */
+int chd_debug_stall_tensor_waits(chd_context *ctx, int polls);
+
 /* ModUp like chd_modup_raw, but allocating no device memory: for callers
  * that must not allocate once running (latency-critical servers, where a
  * cudaMalloc can synchronise the device; hosts whose device memory belongs

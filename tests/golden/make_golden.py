@@ -10,7 +10,7 @@ reference's code.  The oracle is checked against this file in
 tests/test_oracle_pins.py.
 
 Run from the repository root (needs the reference tree; no GPU):
-    python tests/golden/make_golden.py
+    CHEDDAR_REFERENCE=<reference tree> python tests/golden/make_golden.py
 """
 import glob
 import json
@@ -22,16 +22,12 @@ ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 
 
 def main():
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    tree = os.environ.get("CHEDDAR_REFERENCE")
+    if not tree:
+        raise SystemExit("set CHEDDAR_REFERENCE to the reference source tree")
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={tree}"], check=True)
     primes = set()
     for f in sorted(glob.glob(os.path.join(ROOT, "cheddar-fhe_b200", "params", "*.json"))):
-        d = json.load(open(f))
-        for k in ("main_primes", "auxiliary_primes", "terminal_primes"):
-            primes.update(d.get(k, []))
-    ref_params = os.environ.get("CHEDDAR_REFERENCE", "/root/reference") + "/parameters"
-    for f in sorted(glob.glob(os.path.join(ref_params, "bootparam_[34]*.json"))):
-        if "64bit" in f:
-            continue
         d = json.load(open(f))
         for k in ("main_primes", "auxiliary_primes", "terminal_primes"):
             primes.update(d.get(k, []))

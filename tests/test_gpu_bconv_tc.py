@@ -82,3 +82,42 @@ def test_bconv_batch_rejects_bad_engine(cuda_ok):
     out = torch.zeros((1, 1, o.n), dtype=torch.int32, device="cuda")
     with pytest.raises(chd.CheddarError):
         g.bconv_batch(xd, [0], [1], out, engine=7)
+
+
+@pytest.mark.parametrize("npoly", [1, 8])
+def test_bounded_wait_runs_out_and_context_recovers(cuda_ok, npoly):
+    """The tensor-core kernel's bounded mbarrier wait gives up, without a
+    fault: with the stall hook on, each CTA's first accumulator wait polls a
+    barrier nothing signals (64 polls), the kernel sets the context's error
+    word, drains its MMAs in flight, frees its tensor memory and returns;
+    chd_context_synchronize reports CHD_ERR_CUDA with the bounded-wait
+    message, clears the word, and the next launch on the same context is
+    exact again.  npoly = 1 gives every CTA one iteration (the wait after the
+    loop runs out), npoly = 8 several (the wait inside the loop)."""
+    o, g = pair(KS)
+    primes = o.all_primes()
+    rng = np.random.default_rng(99)
+    src, dst = np.arange(12), np.arange(24, 28)
+    xt = _inputs(primes, src, npoly, o.n, rng)
+    T = o.bconv_table(primes[src], primes[dst])
+    ref = np.stack([o.bconv(xt[i], T, primes[dst]) for i in range(npoly)])
+    xd = torch.from_numpy(xt).cuda()
+    out = torch.zeros((npoly, 4, o.n), dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    L = chd.lib()
+    assert L.chd_debug_stall_tensor_waits(g.ptr, 64) == 0
+    try:
+        g.bconv_batch(xd, src, dst, out, engine=chd.BCONV_TENSOR_CORE, npoly=npoly)
+        with pytest.raises(chd.CheddarError) as e:
+            g.synchronize()
+        assert e.value.code == 4  # CHD_ERR_CUDA
+        assert "bounded wait ran out" in str(e.value)
+    finally:
+        assert L.chd_debug_stall_tensor_waits(g.ptr, 0) == 0
+    g.synchronize()  # the error word was cleared
+    out.zero_()
+    torch.cuda.synchronize()
+    g.bconv_batch(xd, src, dst, out, engine=chd.BCONV_TENSOR_CORE, npoly=npoly)
+    g.synchronize()
+    assert np.array_equal(_host(out), ref)
+    assert L.chd_debug_stall_tensor_waits(g.ptr, -1) == 1  # CHD_ERR_INVALID_ARG

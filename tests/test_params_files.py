@@ -26,7 +26,10 @@ FILES = {
     "boot_l34_a12.json": GEN.boot_params,
     "boot_l34_a12_sse.json": lambda: dict(GEN.boot_params(), dense_hamming_weight=32768),
     "boot40_l28_a12.json": GEN.boot40_params,
+    "ntt_bootparam30_p24.json": GEN.ntt_bootparam30_params,
 }
+# the reference's own parameter sets, shipped unchanged
+REFERENCE_FILES = ["bootparam_30.json", "bootparam_35.json", "bootparam_40.json"]
 
 
 @pytest.mark.parametrize("name", sorted(FILES))
@@ -53,3 +56,32 @@ def test_boot40_shape():
     assert (len(p["terminal_primes"]), len(p["main_primes"]), len(p["auxiliary_primes"])) == (4, 43, 12)
     assert len(p["level_config"]) == 29 and p["default_encryption_level"] == 16
     assert p["log_default_scale"] == 40 and p["dense_hamming_weight"] != p["sparse_hamming_weight"]
+
+
+# sha256 of the reference's parameter files (parameters/bootparam_*.json of
+# scale-snu/cheddar-fhe), which ship here unchanged
+REFERENCE_SHA256 = {
+    "bootparam_30.json": "17d0b20eeb75759598146222e9734aee6bdd2cc42d27eba441e9fdd6b57cf787",
+    "bootparam_35.json": "402f088aeb29dfb1908760f5d072e1c9f03713a83dbca5e793f58fe99fc7a9ad",
+    "bootparam_40.json": "a54027c59166d3e28c02fd619d9e7eea4fc2b14524b32c789aee60b114686e2e",
+}
+
+
+@pytest.mark.parametrize("name", REFERENCE_FILES)
+def test_reference_parameter_files(name):
+    import hashlib
+    path = os.path.join(PARAMS, name)
+    assert hashlib.sha256(open(path, "rb").read()).hexdigest() == REFERENCE_SHA256[name]
+    p = json.load(open(path))
+    primes = p["terminal_primes"] + p["main_primes"] + p["auxiliary_primes"]
+    assert len(set(primes)) == len(primes) and len(primes) <= 64
+    for q in primes:
+        assert q < (1 << 31) and q % (1 << 17) == 1 and GEN.is_prime(q)
+    main, ter = len(p["main_primes"]), len(p["terminal_primes"])
+    assert p["level_config"][-1] == [main, ter]
+
+
+def test_bootparam40_shape():
+    p = json.load(open(os.path.join(PARAMS, "bootparam_40.json")))
+    assert (len(p["terminal_primes"]), len(p["main_primes"]), len(p["auxiliary_primes"])) == (4, 43, 12)
+    assert (p["num_cts_levels"], p["num_stc_levels"], p["default_encryption_level"]) == (4, 3, 16)

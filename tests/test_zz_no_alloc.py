@@ -4,8 +4,10 @@ device, and hosts whose device memory belongs to another allocator or a
 fixed budget).  Its scratch is a static device array of 2^21 words; the test
 checks, through the C ABI, that two calls in a row give exactly the residues
 of the allocating chd_modup_raw (integer work: bit-exact), at N = 2^16 and
-on the small-degree path, and that a level whose limbs exceed the static
-scratch is refused with a clear error."""
+on the small-degree path; that the call leaves the device's free memory
+unchanged on a fresh context (whose arena has never grown); that a level
+whose limbs exceed the static scratch, and device pointers off a 16-byte
+boundary, are refused with a clear error."""
 import ctypes as C
 import json
 
@@ -52,6 +54,49 @@ def test_noalloc_modup_matches_allocating_modup(cuda_ok, log_n):
         ctx.synchronize()
         torch.cuda.synchronize()
         assert torch.equal(ref, got), f"level {level}"
+
+
+def test_noalloc_allocates_nothing(cuda_ok):
+    """On a context whose device arena is still empty the call takes no
+    device memory: free memory is the same before and after it.  A warm-up
+    call on another context first loads the library's kernels (lazy module
+    loading allocates their code and static arrays once per process)."""
+    p = json.dumps(param_json("keyswitch_l24_a8.json"))
+    warm = chd.Context(p)
+    lvl = warm.max_level
+    beta = -(-(warm.num_q(lvl)) // warm.alpha)
+    shape = (beta, warm.num_q(lvl) + warm.alpha, warm.n)
+    x = _uniform(warm, lvl, 7)
+    got = torch.zeros(shape, dtype=torch.int32, device="cuda")
+    ref = torch.zeros(shape, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    assert _noalloc(warm, lvl, x, got) == 0, chd.lib().chd_last_error()
+    warm.synchronize()
+    fresh = chd.Context(p)
+    fresh.synchronize()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    assert _noalloc(fresh, lvl, x, got) == 0, chd.lib().chd_last_error()
+    fresh.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, f"device free memory moved by {free0 - free1} bytes"
+    fresh.modup_raw(lvl, x, ref)
+    fresh.synchronize()
+    assert torch.equal(ref, got)
+
+
+def test_noalloc_refuses_misaligned_pointers(cuda_ok):
+    ctx = chd.Context(json.dumps(param_json("keyswitch_l24_a8.json", 13)))
+    lvl = ctx.max_level
+    x = _uniform(ctx, lvl, 8)
+    out = torch.zeros((4, ctx.num_q(lvl) + ctx.alpha, ctx.n), dtype=torch.int32, device="cuda")
+    L = chd.lib()
+    f = L.chd_modup_raw_noalloc
+    rc = f(ctx.ptr, lvl, C.c_void_p(x.data_ptr() + 4), C.c_void_p(out.data_ptr()))
+    assert rc == 1  # CHD_ERR_INVALID_ARG
+    assert "16-byte aligned" in L.chd_last_error().decode()
+    rc = f(ctx.ptr, lvl, C.c_void_p(x.data_ptr()), C.c_void_p(out.data_ptr() + 8))
+    assert rc == 1
 
 
 def test_noalloc_refuses_oversized_levels(cuda_ok):
