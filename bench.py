@@ -752,11 +752,19 @@ def hoist_mixed_bench(ctx, chd, key, uniform, stream, reps=5):
     ms_h = timed(hoisted)
     ms_s = timed(separate)
     R = len(offsets)
+    # algorithmic limbs: the input (2 q), every rotation key once
+    # (2 beta (q + alpha)) and every rotated result (2 q)
+    nq = ctx.num_q(lvl)
+    limbs = 2 * nq + R * 2 * beta * (nq + a) + R * 2 * nq
+    algo = limbs * n * 4
+    hbm = _peaks().get("hbm_gbs", 6650.0)
     res = {"hoisted_rotations": {
         "workload": f"{R} rotations of one ciphertext at level {lvl} (N=2^16, L=24, alpha=8)",
         "offsets": R, "hoisted_ms": ms_h, "separate_ms": ms_s,
         "hoisted_rotations_per_s": R / (ms_h / 1e3), "separate_rotations_per_s": R / (ms_s / 1e3),
-        "speedup": ms_s / ms_h}}
+        "speedup": ms_s / ms_h, "algorithmic_limbs": limbs, "algorithmic_bytes": algo,
+        "hoisted_GB/s": algo / (ms_h / 1e3) / 1e9, "hoisted_hbm_frac": algo / (ms_h / 1e3) / 1e9 / hbm,
+        "separate_hbm_frac": algo / (ms_s / 1e3) / 1e9 / hbm}}
     del keys, qp_outs, outs
     # (ii) mixed-level batch
     levels = [int(x) for x in np.random.default_rng(0).integers(5, 23, 16)]
@@ -793,6 +801,116 @@ def hoist_mixed_bench(ctx, chd, key, uniform, stream, reps=5):
 
 
 BOOT_PARAM_FILE = "bootparam_40.json"
+
+
+def _peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+def boot_trace_limbs(ctx, bc, params):
+    """Algorithmic limbs (N-word polynomials) of one bootstrap: the sum over
+    its op trace (the compiled Boot program, op for op as the library and
+    the reference run it) of every operand read once and every result
+    written once.  Per op at level l, with q = num_q(l), beta(l) digits and
+    alpha auxiliary primes:
+      key switch (RelinearizeRescale, HConj, HRotAdd): inputs, the key rows
+        it reads (2 beta (q + alpha)), the result;
+      linear transform: input 2q, one key per nonzero baby / giant step,
+        every plaintext diagonal (q + alpha), result 2 q(l - 1);
+      ModUpToMax: 2 q(-1) in, 2 q(max) out (+ the dense-to-sparse and
+        sparse-to-dense key rows with encapsulation);
+      element-wise, rescale, level-down, tensor: inputs and result.
+    Returns (ciphertext-data limbs, key + plaintext limbs): a batch of B
+    bootstraps reads the second part once in an ideal schedule."""
+    prog = bc.json()
+    lts = bc.transforms()
+    a = ctx.alpha
+    max_ter = len(params.get("terminal_primes", []))
+
+    def q(l):
+        return ctx.num_q(l)
+
+    def key(l):
+        m, t = ctx.level_np(l)
+        beta = -(-(m + t + max_ter - t) // a)
+        return 2 * beta * (q(l) + a)
+
+    regs = {prog["input"]: (0, 2)}  # register -> (level, parts)
+    data = const = 0
+    for op in prog["ops"]:
+        k, d, x, y, lvl = op["k"], op["d"], op["a"], op["b"], op["l"]
+        if k in (0, 7):  # constant multiply / level-down (product, then rescale)
+            lx, px = regs[x]
+            level = lx if k == 7 else lvl
+            data += px * q(lx if k == 7 else level)
+            out = (level - 1, px) if k == 7 else (level, px)
+            data += out[1] * q(out[0])
+            regs[d] = out
+        elif k == 1:  # tensor
+            data += 2 * q(lvl) * 2 + 3 * q(lvl)
+            regs[d] = (lvl, 3)
+        elif k == 2:  # constant accumulation
+            nparts = 2
+            for src in op["s"]:
+                ls, ps = regs[src]
+                data += min(ps, 2) * q(lvl)
+            if op["p"] >= 0:
+                nparts = regs[op["p"]][1]
+                data += nparts * q(lvl)
+            data += nparts * q(lvl)
+            regs[d] = (lvl, nparts)
+        elif k in (3, 8, 12):  # add constant, copy, times i
+            lx, px = regs[x]
+            data += 2 * px * q(lx)
+            regs[d] = (lx, px)
+        elif k in (4, 10):  # add / sub
+            lx, px = regs[x]
+            py = regs[y][1]
+            data += (px + py + max(px, py)) * q(lx)
+            regs[d] = (lx, max(px, py))
+        elif k == 5:  # RelinearizeRescale
+            lx, px = regs[x]
+            data += px * q(lx) + 2 * q(lx - 1)
+            const += key(lx)
+            regs[d] = (lx - 1, 2)
+        elif k == 6:  # rescale
+            lx, px = regs[x]
+            data += px * (q(lx) + q(lx - 1))
+            regs[d] = (lx - 1, px)
+        elif k in (9, 16):  # metadata
+            pass
+        elif k == 11:  # HConj
+            lx, _ = regs[x]
+            data += 4 * q(lx)
+            const += key(lx)
+            regs[d] = (lx, 2)
+        elif k == 13:  # ModUpToMax
+            top = ctx.max_level
+            lx, _ = regs[x]
+            data += 2 * q(lx) + 2 * q(top)
+            if params.get("dense_hamming_weight") != params.get("sparse_hamming_weight"):
+                const += 2 * (2 * q(-1)) + 2 * (q(top) + a)
+            regs[d] = (top, 2)
+        elif k == 14:  # HRotAdd
+            lx, _ = regs[x]
+            data += 6 * q(lx)
+            const += key(lx)
+            regs[d] = (lx, 2)
+        elif k == 15:  # linear transform
+            plan = lts[op["r"]]
+            l = plan["level"]
+            bs = {b for (_, b, _) in plan["pts"]}
+            gs = {g for (g, _, _) in plan["pts"]}
+            data += 2 * q(l) + 2 * q(l - 1)
+            const += (len([b for b in bs if b]) + len([g for g in gs if g])) * key(l)
+            const += len(plan["pts"]) * (q(l) + a)
+            regs[d] = (l - 1, 2)
+        else:
+            raise ValueError(f"unknown op kind {k}")
+    return data, const
 
 
 def boot_bench(chd, args, stream, dist, profile=False):
@@ -972,7 +1090,24 @@ def boot_bench(chd, args, stream, dist, profile=False):
     ctx.ks_engine = main_engine
     engines["speedup_tensor_vs_cuda_core"] = (engines["tensor_core"]["bootstraps_per_s"] /
                                               engines["cuda_core"]["bootstraps_per_s"])
+    try:
+        data_l, const_l = boot_trace_limbs(ctx, bc, params)
+        hbm = _peaks().get("hbm_gbs", 6650.0)
+        batch_bytes = (B * data_l + const_l) * n * 4
+        one_bytes = (data_l + const_l) * n * 4
+        roof = {"bound": "hbm", "unit": "GB/s", "peak": hbm,
+                "achieved": batch_bytes / (ms_graph / steps / 1e3) / 1e9,
+                "frac": batch_bytes / (ms_graph / steps / 1e3) / 1e9 / hbm,
+                "algorithmic_bytes_per_batch": batch_bytes, "algorithmic_bytes_one_boot": one_bytes,
+                "ciphertext_limbs_per_boot": data_l, "key_and_plaintext_limbs": const_l,
+                "one_by_one_frac": one_bytes / (ms_single / (B * steps) / 1e3) / 1e9 / hbm,
+                "what": "algorithmic bytes of the op trace (each operand read once, each result written once; "
+                        "keys and plaintext diagonals once per batch) / graph-replayed batch time; peak = "
+                        "measured HBM copy"}
+    except Exception as e:  # pragma: no cover
+        roof = {"error": f"trace count failed: {e}"}
     res = {"metric": "bootstraps/s (full slots, N=2^16, batched call, graph-captured)",
+           "roofline": roof,
            "value": job_throughput(world, B, steps, ms_graph),
            "eager": {"bootstraps_per_s": world * B * steps / (ms / 1e3), "ms_per_boot": ms / (B * steps)},
            "one_by_one_eager": {"bootstraps_per_s": world * B * steps / (ms_single / 1e3),

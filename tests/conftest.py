@@ -11,8 +11,19 @@ for p in (PKG, ORACLE, ROOT):
         sys.path.insert(0, p)
 
 
+# figures tests want shown in the run's summary (precision bits, rates)
+REPORT = []
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
+
+
+def pytest_terminal_summary(terminalreporter):
+    if REPORT:
+        terminalreporter.write_line("figures reported by the tests:")
+        for line in REPORT:
+            terminalreporter.write_line("  " + line)
 
 
 def param_path(name):

@@ -69,6 +69,13 @@ def precision_bits(dec, msg):
     return -float(np.log2(err)) if err > 0 else 99.0
 
 
+def max_component_error(dec, msg):
+    """Largest error of a real or imaginary part: the reference's test
+    criterion is 1e-3 (unittest/Testbed.h:93, 318-322)."""
+    d = np.asarray(dec) - np.asarray(msg)
+    return float(max(np.abs(d.real).max(), np.abs(d.imag).max()))
+
+
 class Trio:
     """The reference, this library and the oracle on one parameter set."""
 
@@ -316,7 +323,10 @@ def _context_ops(name, levels):
         pairs += [("Rescale", g.Rescale(gr), ref.Rescale(rr)),
                   ("Permute", g.Permute(g.MultKey(ga, rk), rot), ref.unary("Permute", ref.unary("MultKeyRot", ra, rot),
                                                                          rot))]
-        if lvl >= 2:
+        # the reference's level-down constants exist up to the default
+        # encryption level (Context.cpp:102-107); above it LevelDown reads
+        # past them, so it is compared only where it is defined
+        if 2 <= lvl <= t.p["default_encryption_level"]:
             pairs.append(("LevelDown", g.LevelDown(ga, lvl - 2), ref.unary("LevelDown", ra, lvl - 2)))
         if lvl >= 1 and g.IsMultUnsafeCompatible(lvl, lvl - 1):
             pairs.append(("MultUnsafe", g.MultUnsafe(ga, gb, lvl - 1), ref.binary("MultUnsafe", ra, rb, lvl - 1)))
@@ -386,10 +396,12 @@ def _boot_case(name, num_slots=None, min_bits=18.5):
         r_ref1 = ref.Boot(rin[1], min_ks=min_ks)
         eq(f"BootBatch[1] ({tag}) vs reference", batch[1].numpy(), r_ref1.numpy())
         inf = r_ref.info()
-        bits = min(precision_bits(ref.decrypt_decode(r_ref), msgs[0]),
-                   precision_bits(ref.decrypt_decode(r_ref1), msgs[1]))
-        res[tag] = {"precision_bits": round(bits, 2), "end_level": t.level_of(inf),
+        d0, d1 = ref.decrypt_decode(r_ref), ref.decrypt_decode(r_ref1)
+        bits = min(precision_bits(d0, msgs[0]), precision_bits(d1, msgs[1]))
+        comp = max(max_component_error(d0, msgs[0]), max_component_error(d1, msgs[1]))
+        res[tag] = {"precision_bits": round(bits, 2), "max_component_error": comp, "end_level": t.level_of(inf),
                     "end_scale_log2": round(float(np.log2(inf["scale"])), 4)}
+        assert comp <= 1e-3, (tag, comp)
         assert bits >= min_bits, (tag, bits)
     return res
 
@@ -404,18 +416,18 @@ def case_boot40():
 def case_boot30():
     """Full-slot bootstrapping on bootparam_30.json (48 main primes, no
     terminal primes)."""
-    return _boot_case("bootparam_30.json", min_bits=15.0)
+    return _boot_case("bootparam_30.json", min_bits=9.9)
 
 
 def case_boot35():
     """Full-slot bootstrapping on bootparam_35.json (5 terminal primes)."""
-    return _boot_case("bootparam_35.json", min_bits=15.0)
+    return _boot_case("bootparam_35.json", min_bits=9.9)
 
 
 def case_boot40_sparse():
     """Bootstrapping of 2^10 slots (sparse packing: Trace, the 2n x 2n
     CoeffToSlot / SlotToCoeff phases) on bootparam_40.json."""
-    return _boot_case("bootparam_40.json", num_slots=1 << 10, min_bits=15.0)
+    return _boot_case("bootparam_40.json", num_slots=1 << 10, min_bits=9.9)
 
 
 CASES = {k[5:]: v for k, v in globals().items() if k.startswith("case_")}

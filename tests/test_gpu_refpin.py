@@ -28,6 +28,7 @@ import sys
 
 import pytest
 
+import conftest
 import refdrv
 
 pytestmark = pytest.mark.gpu
@@ -46,3 +47,4 @@ def test_reference_parity(cuda_ok, case):
     assert r.returncode == 0, f"case {case} failed (rc {r.returncode}):\n{r.stderr[-3000:]}"
     line = [x for x in r.stdout.splitlines() if x.startswith("{")][-1]
     assert json.loads(line)["case"] == case
+    conftest.REPORT.append(line)
