@@ -120,6 +120,22 @@ def lib():
         "chd_bconv_raw": (i, [vp, vp, i32p, i, i32p, i, vp]),
         "chd_bconv_batch": (i, [vp, i, i, vp, i32p, i, i32p, i, vp]),
         "chd_debug_stall_tensor_waits": (i, [vp, i]),
+        "chd_decode": (i, [vp, i, C.c_double, vp, i, vp, vp]),
+        "chd_evk_info": (i, [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(i)]),
+        "chd_ct_serialize": (i, [vp, vp, vp, C.c_size_t, C.POINTER(C.c_size_t)]),
+        "chd_ct_deserialize": (i, [vp, vp, vp, C.c_size_t]),
+        "chd_evk_serialize": (i, [vp, vp, vp, C.c_size_t, C.POINTER(C.c_size_t)]),
+        "chd_evk_deserialize": (i, [vp, vp, C.c_size_t, pp]),
+        "chd_evk_export": (i, [vp, vp, vp, vp, i]),
+        "chd_client_create": (i, [vp, C.c_uint64, pp]),
+        "chd_client_destroy": (None, [vp]),
+        "chd_client_secret": (i, [vp, vp, i, vp]),
+        "chd_client_mult_key": (i, [vp, vp, pp]),
+        "chd_client_rotation_key": (i, [vp, vp, i, pp]),
+        "chd_client_conjugation_key": (i, [vp, vp, pp]),
+        "chd_client_sse_keys": (i, [vp, vp, pp, pp]),
+        "chd_client_encrypt": (i, [vp, vp, C.c_uint64, i, C.c_double, i, vp, vp]),
+        "chd_client_decrypt": (i, [vp, vp, vp, vp]),
         "chd_encode": (i, [vp, i, d, vp, vp, i, i, vp, C.POINTER(i)]),
         "chd_encode_const": (i, [vp, i, d, d, i, vp]),
         "chd_modup_to_max": (i, [vp, vp, vp, vp]),
@@ -271,6 +287,13 @@ class Context:
     def rescale_prime_prod(self, level):
         return lib().chd_rescale_prime_prod(self.ptr, level)
 
+    def level_of(self, num_main, num_ter):
+        """The level whose q primes are (num_main, num_ter)."""
+        for lv in range(-1, self.max_level + 1):
+            if self.level_np(lv) == (num_main, num_ter):
+                return lv
+        raise CheddarError(2, f"no level holds {num_main} main and {num_ter} terminal primes")
+
     def gidx(self, num_main, num_ter, num_aux):
         out = np.zeros(256, dtype=np.int32)
         k = lib().chd_prime_gidx(self.ptr, num_main, num_ter, num_aux, out.ctypes.data)
@@ -300,6 +323,22 @@ class Context:
                                  num_slots or self.n // 2, _ptr(parts[0]), _ptr(parts[1]), rx,
                                  words, C.byref(ct.ptr)))
         return ct
+
+    def load_ct(self, data):
+        """A ciphertext from bytes written by Ciphertext.serialize."""
+        ct = Ciphertext(self)
+        buf = C.create_string_buffer(bytes(data), len(data))
+        _check(lib().chd_ct_deserialize(self.ptr, ct.ptr, buf, len(data)))
+        return ct
+
+    def load_evk(self, data):
+        """An evaluation key from bytes written by EvaluationKey.serialize."""
+        k = EvaluationKey.__new__(EvaluationKey)
+        k.ctx = self
+        k.ptr = C.c_void_p()
+        buf = C.create_string_buffer(bytes(data), len(data))
+        _check(lib().chd_evk_deserialize(self.ptr, buf, len(data), C.byref(k.ptr)))
+        return k
 
     def evk(self, bx, ax, on_device=False):
         return EvaluationKey(self, bx, ax, on_device)
@@ -545,6 +584,15 @@ class Context:
         _check(lib().chd_encode(self.ptr, level, scale, re.ctypes.data, im.ctypes.data, len(msg), num_aux,
                                 _ptr(out), C.byref(ns)))
         return out
+
+    def decode(self, level, scale, pt, num_slots=None):
+        """Encoder::Decode: device plaintext (torch int32 [num_q(level)][N],
+        evaluation domain, Montgomery form) -> num_slots complex slots."""
+        ns = num_slots or self.n // 2
+        re = np.zeros(ns)
+        im = np.zeros(ns)
+        _check(lib().chd_decode(self.ptr, level, scale, _ptr(pt), ns, re.ctypes.data, im.ctypes.data))
+        return re + 1j * im
 
     def encode_const(self, level, scale, value, num_aux=0):
         """Encoder::EncodeConstant: Montgomery residues per prime (host)."""
@@ -856,6 +904,15 @@ class Ciphertext:
         return dict(num_main=m.value, num_ter=t.value, num_aux=a.value, has_rx=bool(rx.value),
                     scale=sc.value, num_slots=ns.value)
 
+    def serialize(self):
+        """The ciphertext as bytes (magic, shape, scale, slot count, primes,
+        residues); Context.load_ct reads them back."""
+        n = C.c_size_t()
+        _check(lib().chd_ct_serialize(self.ctx.ptr, self.ptr, None, 0, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        _check(lib().chd_ct_serialize(self.ctx.ptr, self.ptr, buf, n.value, C.byref(n)))
+        return buf.raw
+
     def numpy(self):
         inf = self.info()
         rows = inf["num_main"] + inf["num_ter"] + inf["num_aux"]
@@ -863,6 +920,76 @@ class Ciphertext:
         _check(lib().chd_ct_export(self.ctx.ptr, self.ptr, parts[0].ctypes.data, parts[1].ctypes.data,
                                    parts[2].ctypes.data if len(parts) > 2 else None, 0))
         return parts
+
+
+class Client:
+    """Test-only client on the device (the reference's UserInterface,
+    src/UserInterface.cu): secrets, evaluation keys, encryption and
+    decryption, reproducible from `seed`."""
+
+    def __init__(self, ctx, seed):
+        self.ctx = ctx
+        self.ptr = C.c_void_p()
+        _check(lib().chd_client_create(ctx.ptr, seed, C.byref(self.ptr)))
+
+    def __del__(self):
+        try:
+            if self.ptr.value:
+                lib().chd_client_destroy(self.ptr)
+                self.ptr = C.c_void_p()
+        except Exception:
+            pass
+
+    def secret(self, sparse=False):
+        rows = self.ctx.L + self.ctx.alpha
+        out = np.zeros((rows, self.ctx.n), dtype=np.uint32)
+        _check(lib().chd_client_secret(self.ctx.ptr, self.ptr, int(sparse), out.ctypes.data))
+        return out
+
+    def _key(self, fn, *args):
+        k = EvaluationKey.__new__(EvaluationKey)
+        k.ctx = self.ctx
+        k.ptr = C.c_void_p()
+        _check(fn(self.ctx.ptr, self.ptr, *args, C.byref(k.ptr)))
+        return k
+
+    def mult_key(self):
+        return self._key(lib().chd_client_mult_key)
+
+    def rotation_key(self, rot_idx):
+        return self._key(lib().chd_client_rotation_key, rot_idx)
+
+    def conjugation_key(self):
+        return self._key(lib().chd_client_conjugation_key)
+
+    def sse_keys(self):
+        dts = EvaluationKey.__new__(EvaluationKey)
+        std = EvaluationKey.__new__(EvaluationKey)
+        dts.ctx = std.ctx = self.ctx
+        dts.ptr, std.ptr = C.c_void_p(), C.c_void_p()
+        _check(lib().chd_client_sse_keys(self.ctx.ptr, self.ptr, C.byref(dts.ptr), C.byref(std.ptr)))
+        return dts, std
+
+    def encrypt(self, pt, level, scale, num_slots=None, nonce=0):
+        """pt: device plaintext (torch int32 [num_q(level)][N], as
+        Context.encode returns it)."""
+        ct = Ciphertext(self.ctx)
+        _check(lib().chd_client_encrypt(self.ctx.ptr, self.ptr, nonce, level, scale,
+                                        num_slots or self.ctx.n // 2, _ptr(pt), ct.ptr))
+        return ct
+
+    def decrypt(self, ct):
+        import torch
+        inf = ct.info()
+        out = torch.empty((inf["num_main"] + inf["num_ter"], self.ctx.n), dtype=torch.int32, device="cuda")
+        _check(lib().chd_client_decrypt(self.ctx.ptr, self.ptr, ct.ptr, _ptr(out)))
+        return out
+
+    def decrypt_decode(self, ct):
+        """Decrypt, then decode with the ciphertext's level, scale and slot count."""
+        inf = ct.info()
+        level = self.ctx.level_of(inf["num_main"], inf["num_ter"])
+        return self.ctx.decode(level, inf["scale"], self.decrypt(ct), inf["num_slots"])
 
 
 class EvaluationKey:
@@ -887,6 +1014,27 @@ class EvaluationKey:
         else:
             _check(lib().chd_evk_create_np(ctx.ptr, basis[0], basis[1], basis[2], beta, pb, pa, int(on_device),
                                            C.byref(self.ptr)))
+
+    def info(self):
+        b, m, t, a = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        _check(lib().chd_evk_info(self.ptr, C.byref(b), C.byref(m), C.byref(t), C.byref(a)))
+        return b.value, (m.value, t.value, a.value)
+
+    def serialize(self):
+        """The key as bytes; Context.load_evk reads them back."""
+        n = C.c_size_t()
+        _check(lib().chd_evk_serialize(self.ctx.ptr, self.ptr, None, 0, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        _check(lib().chd_evk_serialize(self.ctx.ptr, self.ptr, buf, n.value, C.byref(n)))
+        return buf.raw
+
+    def numpy(self):
+        """(bx, ax) as [beta][np][N] uint32 host arrays."""
+        beta, (m, t, a) = self.info()
+        bx = np.zeros((beta, m + t + a, self.ctx.n), dtype=np.uint32)
+        ax = np.zeros_like(bx)
+        _check(lib().chd_evk_export(self.ctx.ptr, self.ptr, bx.ctypes.data, ax.ctypes.data, 0))
+        return bx, ax
 
     def __del__(self):
         try:

@@ -1,14 +1,8 @@
-// Host side of the bootstrapping path: the encoder (plaintexts and
-// constants for the linear transforms and EvalMod) and ModUpToMax.
-//
-// Encoder (src/core/Encode.cpp of the reference): slots -> special IFFT in
-// FP64 with the twiddle table e^(2 pi i k / 2N) -> value * scale truncated
-// toward zero to an integer (BigInt(double), include/core/BigInt.h:24) ->
-// residues -> NTT with Montgomery conversion on the device.  The FP64 steps
-// follow the reference's operation order exactly, so the residues are
-// bit-identical wherever the reference's host build evaluates the same
-// IEEE expressions (no fused multiply-add; this file is built with
-// -ffp-contract=off).
+// Host side of the bootstrapping path: constants for the linear transforms
+// and EvalMod (Encoder::EncodeConstant: value * scale truncated toward zero
+// to an integer, BigInt(double) of include/core/BigInt.h:24, then residues),
+// the encoder's twiddle table, and ModUpToMax.  The plaintext encoder and
+// the decoder run on the device (codec.cu).
 #include <cmath>
 #include <complex>
 
@@ -19,12 +13,6 @@ namespace chd {
 namespace {
 
 using cd = std::complex<double>;
-
-unsigned brev_bits(unsigned x, int bits) {
-  unsigned r = 0;
-  for (int i = 0; i < bits; i++) r |= ((x >> i) & 1u) << (bits - 1 - i);
-  return r;
-}
 
 // round-toward-zero integer of v, reduced to [0, p): exact for every finite
 // double (|v| >= 2^53 is already an integer m * 2^e)
@@ -77,89 +65,6 @@ const std::vector<std::complex<double>> &Context::enc_twiddles() {
     for (int i = 0; i < M; i++) enc_tw[i] = std::polar(1.0, 2.0 * M_PI * i / M);
   }
   return enc_tw;
-}
-
-void Context::special_ifft(std::vector<std::complex<double>> &d) {
-  // Encoder::SpecialIFFT, Encode.cpp:84-107
-  const auto &tw = enc_twiddles();
-  const int ns = static_cast<int>(d.size()), M = 2 * P->n;
-  for (int stride = ns / 2; stride >= 1; stride /= 2) {
-    const int sg = stride * 2, st8 = stride << 3, gap = M / st8;
-    for (int i = 0; i < ns; i += sg)
-      for (int j = 0; j < stride; j++) {
-        const int ti = (st8 - static_cast<int>(P->galois[j] % st8)) * gap;
-        cd x = d[i + j] + d[i + j + stride];
-        cd y = d[i + j] - d[i + j + stride];
-        y *= tw[ti];
-        d[i + j] = x;
-        d[i + j + stride] = y;
-      }
-  }
-  int lb = 0;
-  while ((1 << lb) < ns) lb++;
-  for (int i = 0; i < ns; i++) {
-    const int j = static_cast<int>(brev_bits(static_cast<unsigned>(i), lb));
-    if (i < j) std::swap(d[i], d[j]);
-  }
-  for (int i = 0; i < ns; i++) d[i] /= static_cast<double>(ns);
-}
-
-void Context::special_fft(std::vector<std::complex<double>> &d) {
-  // Encoder::SpecialFFT, Encode.cpp:109-133
-  const auto &tw = enc_twiddles();
-  const int ns = static_cast<int>(d.size()), M = 2 * P->n;
-  int lb = 0;
-  while ((1 << lb) < ns) lb++;
-  for (int i = 0; i < ns; i++) {
-    const int j = static_cast<int>(brev_bits(static_cast<unsigned>(i), lb));
-    if (i < j) std::swap(d[i], d[j]);
-  }
-  for (int stride = 1; stride < ns; stride *= 2) {
-    const int sg = stride * 2, st8 = stride << 3, gap = M / st8;
-    for (int i = 0; i < ns; i += sg)
-      for (int j = 0; j < stride; j++) {
-        const int ti = static_cast<int>(P->galois[j] % st8) * gap;
-        cd x = d[i + j];
-        cd y = d[i + j + stride];
-        y *= tw[ti];
-        d[i + j] = x + y;
-        d[i + j + stride] = x - y;
-      }
-  }
-}
-
-Status Context::encode(int level, double scale, const std::complex<double> *msg, int msg_len, int num_aux,
-                       uint32_t *pt_dev, int *num_slots_out) {
-  // Encoder::Encode / EncodeWorker / ComplexVectorToPlaintext,
-  // Encode.cpp:23-41, 135-190
-  CHD_CHECK(msg_len >= 1 && msg_len <= P->n / 2, kErrInvalidArg, "Encode: 1 <= message length <= N/2");
-  CHD_CHECK(num_aux >= 0 && num_aux <= P->alpha, kErrInvalidArg, "Encode: invalid number of aux primes");
-  CHD_CHECK(level >= -1 && level <= P->max_level, kErrInvalidLevel, "Encode: invalid level");
-  int ns = 1;
-  while (ns < msg_len) ns *= 2;
-  std::vector<cd> d(ns, cd(0.0, 0.0));
-  for (int i = 0; i < msg_len; i++) d[i] = msg[i];
-  special_ifft(d);
-  const NP np = P->level_np(level, num_aux);
-  const int tot = np.total(), n = P->n, half = n / 2, gap = half / ns;
-  std::vector<int> g(tot);
-  P->gidx(np, g.data());
-  std::vector<uint32_t> mx(static_cast<size_t>(tot) * n, 0);
-  for (int i = 0; i < ns; i++) {
-    const cd v = d[i] * scale;
-    const double re = v.real(), im = v.imag();
-    for (int k = 0; k < tot; k++) {
-      const uint32_t p = P->primes[g[k]];
-      mx[static_cast<size_t>(k) * n + i * gap] = trunc_mod(re, p);
-      mx[static_cast<size_t>(k) * n + i * gap + half] = trunc_mod(im, p);
-    }
-  }
-  cudaMemcpyAsync(pt_dev, mx.data(), mx.size() * 4, cudaMemcpyHostToDevice, stream);
-  if (num_slots_out) *num_slots_out = ns;
-  // NTT(..., true): to the evaluation domain, Montgomery form
-  CHD_TRY(ntt(np, pt_dev, true));
-  // the host buffer must outlive the copy
-  return cudaStreamSynchronize(stream) == cudaSuccess ? kOk : check_cuda("encode");
 }
 
 void Context::encode_const(int level, double scale, double value, int num_aux, std::vector<uint32_t> *cx) const {

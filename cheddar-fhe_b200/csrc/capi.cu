@@ -10,12 +10,6 @@
 
 using namespace chd;
 
-struct chd_ciphertext {
-  DeviceCt ct;
-};
-struct chd_evk {
-  DeviceEvk k;
-};
 struct chd_evk_map {
   RotKeys rot;
   const DeviceEvk *conj = nullptr, *mult = nullptr, *dts = nullptr, *std_key = nullptr;
@@ -377,6 +371,8 @@ int chd_set_ks_engine(chd_context *ctx, int engine) try {
 
 int chd_get_ks_engine(const chd_context *ctx) { return ctx ? ctx->c->ks_engine : -1; }
 
+int chd_ks_tuned_shapes(int *out, int cap) { return modswitch_tuned_shapes(out, cap); }
+
 int chd_stage_times(chd_context *ctx, double *ms, int *launches) try {
   CHD_CTX(ctx);
   if (!ms || !launches) return fail(CHD_ERR_INVALID_ARG, "chd_stage_times: null output");
@@ -617,6 +613,37 @@ int chd_evk_create(chd_context *ctx, int beta, const uint32_t *bx, const uint32_
 
 void chd_evk_destroy(chd_evk *evk) { delete evk; }
 
+int chd_evk_info(const chd_evk *evk, int *beta, int *num_main, int *num_ter, int *num_aux) try {
+  CHD_NOTNULL(evk);
+  if (beta) *beta = evk->k.beta;
+  if (num_main) *num_main = evk->k.np.main;
+  if (num_ter) *num_ter = evk->k.np.ter;
+  if (num_aux) *num_aux = evk->k.np.aux;
+  return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
+}
+
+int chd_evk_export(chd_context *ctx, const chd_evk *evk, uint32_t *bx, uint32_t *ax, int dst_on_device) try {
+  CHD_CTX(ctx);
+  CHD_NOTNULL(evk);
+  CHD_NOTNULL(bx);
+  CHD_NOTNULL(ax);
+  const size_t bytes = static_cast<size_t>(evk->k.beta) * evk->k.np.total() * ctx->c->P->n * 4;
+  const cudaMemcpyKind kind = dst_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  Context &C = *ctx->c;
+  cudaMemcpyAsync(bx, evk->k.bx, bytes, kind, C.stream);
+  cudaMemcpyAsync(ax, evk->k.ax, bytes, kind, C.stream);
+  const cudaError_t e = cudaStreamSynchronize(C.stream);
+  return e == cudaSuccess ? CHD_OK : fail(CHD_ERR_CUDA, cudaGetErrorString(e));
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
+}
+
 #define CTX_CT3(name, call)                                                                              \
   int name(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a, const chd_ciphertext *b) { \
     CHD_CTX(ctx);                                                                                  \
@@ -713,6 +740,27 @@ int chd_encode(chd_context *ctx, int level, double scale, const double *re, cons
   std::vector<std::complex<double>> msg(msg_len);
   for (int i = 0; i < msg_len; i++) msg[i] = std::complex<double>(re[i], im[i]);
   return ctx->c->encode(level, scale, msg.data(), msg_len, num_aux, pt_dev, num_slots);
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
+}
+
+int chd_decode(chd_context *ctx, int level, double scale, const uint32_t *pt_dev, int num_slots, double *re,
+               double *im) try {
+  CHD_CTX(ctx);
+  CHD_NOTNULL(pt_dev);
+  CHD_NOTNULL(re);
+  CHD_NOTNULL(im);
+  CHD_ALIGNED(pt_dev);
+  std::vector<std::complex<double>> out(num_slots > 0 ? num_slots : 1);
+  int rc = ctx->c->decode(level, scale, pt_dev, num_slots, out.data());
+  if (rc != CHD_OK) return rc;
+  for (int i = 0; i < num_slots; i++) {
+    re[i] = out[i].real();
+    im[i] = out[i].imag();
+  }
+  return CHD_OK;
 } catch (const std::exception &e) {
   return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
 } catch (...) {

@@ -547,6 +547,8 @@ Context::~Context() {
   cudaFree(d_err);
   cudaFree(d_tw);
   cudaFree(d_itw);
+  cudaFree(d_enc_tw);
+  cudaFree(d_galois);
   for (cudaEvent_t e : timer.ev) cudaEventDestroy(e);
   if (own_stream && stream) cudaStreamDestroy(stream);
 }
@@ -810,27 +812,6 @@ Status Context::init(const ParamSpec &spec, int dev, std::string *err) {
 }
 
 // ------------------------------------------------------- building blocks
-namespace {
-// Splits a long list of rows into RowBatch launches.
-template <typename F>
-void for_row_batches(const std::vector<RowDesc> &rows, F &&launch) {
-  // as few launches as kMaxRows allows, with the rows spread evenly over
-  // them (a short last launch would leave most SMs idle)
-  const int total = static_cast<int>(rows.size());
-  const int nbat = (total + kMaxRows - 1) / kMaxRows;
-  const int per = nbat > 0 ? (total + nbat - 1) / nbat : kMaxRows;
-  RowBatch rb;
-  rb.count = 0;
-  for (const RowDesc &r : rows) {
-    rb.rows[rb.count++] = r;
-    if (rb.count == per) {
-      launch(rb);
-      rb.count = 0;
-    }
-  }
-  if (rb.count) launch(rb);
-}
-}  // namespace
 
 Status Context::ntt(const NP &np, uint32_t *data, bool mont, int count, size_t stride) {
   const int tot = np.total(), n = P->n;

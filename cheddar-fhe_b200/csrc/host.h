@@ -427,15 +427,24 @@ class Context {
                 uint32_t *pt_dev, int *num_slots_out);
   // Encoder::EncodeConstant (Encode.cpp:250-275): Montgomery residues
   void encode_const(int level, double scale, double value, int num_aux, std::vector<uint32_t> *cx) const;
-  void special_ifft(std::vector<std::complex<double>> &d);
-  void special_fft(std::vector<std::complex<double>> &d);
+  // Encoder::Decode (Encode.cpp:45-70, 109-133, 192-248): plaintext at
+  // `level` (no aux primes, NTT Montgomery domain) -> num_slots complex
+  // slots (a power of two <= N/2) at out; waits for the result.
+  Status decode(int level, double scale, const uint32_t *pt_dev, int num_slots, std::complex<double> *out);
+  // device copies of the encoder's twiddles e^(2 pi i k / 2N) and 5^i mod 2N
+  double2 *d_enc_tw = nullptr;
+  int *d_galois = nullptr;
+  Status codec_tables();
   // BootContext::ModUpToMax without sparse-secret encapsulation
   // (BootContext.cpp:186-270): level -1 -> top level
   Status modup_to_max(DeviceCt &res, const DeviceCt &a);
   // ... with sparse-secret encapsulation: dense-to-sparse key switch at level
   // -1, lift, single-digit sparse-to-dense key switch, ModDown
   Status modup_to_max_sse(DeviceCt &res, const DeviceCt &a, const DeviceEvk &dts, const DeviceEvk &std_key);
-  bool uses_sse() const { return P->spec.dense_hw > 0 && P->spec.dense_hw > P->spec.sparse_hw; }
+  // Parameter::IsUsingSparseSecretEncapsulation (Parameter.cu:246-248),
+  // with the reference's default dense Hamming weight N/2 (Parameter.cu:40)
+  int dense_hw() const { return P->spec.dense_hw > 0 ? P->spec.dense_hw : P->n / 2; }
+  bool uses_sse() const { return dense_hw() > P->spec.sparse_hw; }
 
   // Linear transform planning and evaluation (lintrans.cu): LinearTransform
   // ctor + HoistHandler ctor (LinearTransform.cpp:8-75, Hoist.cu:120-167)
@@ -536,6 +545,26 @@ class Context {
 Status elem_parts(Context &C, ElemOp op, const NP &np, int parts, uint32_t *const *dst, const uint32_t *const *a,
                   const uint32_t *const *b, const uint32_t *k);
 
+// Splits a long list of rows into RowBatch launches: as few launches as
+// kMaxRows allows, with the rows spread evenly over them (a short last
+// launch would leave most SMs idle).
+template <typename F>
+void for_row_batches(const std::vector<RowDesc> &rows, F &&launch) {
+  const int total = static_cast<int>(rows.size());
+  const int nbat = (total + kMaxRows - 1) / kMaxRows;
+  const int per = nbat > 0 ? (total + nbat - 1) / nbat : kMaxRows;
+  RowBatch rb;
+  rb.count = 0;
+  for (const RowDesc &r : rows) {
+    rb.rows[rb.count++] = r;
+    if (rb.count == per) {
+      launch(rb);
+      rb.count = 0;
+    }
+  }
+  if (rb.count) launch(rb);
+}
+
 // Makes `device` current for the scope of a C ABI call and restores the
 // caller's device afterwards: kernels, allocations and stream work of a
 // context always run on the device it was created on, whichever device the
@@ -558,8 +587,14 @@ class DeviceGuard {
 
 }  // namespace chd
 
-// The C ABI's opaque context handle (include/cheddar_b200.h), shared by the
-// translation units that implement entry points.
+// The C ABI's opaque handles (include/cheddar_b200.h) that more than one
+// translation unit implementing entry points uses.
 struct chd_context {
   std::unique_ptr<chd::Context> c;
+};
+struct chd_ciphertext {
+  chd::DeviceCt ct;
+};
+struct chd_evk {
+  chd::DeviceEvk k;
 };

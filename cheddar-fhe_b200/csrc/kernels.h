@@ -168,6 +168,9 @@ struct MSColBatch {
   MSColJob jobs[kMaxMSColJobs];
 };
 void launch_modswitch_cols(const MSColBatch &b, int log_n, cudaStream_t s);
+// the autotuned choices (engine, target split) cached so far: 6 ints per
+// shape (device, largest K, jobs, largest M, engine, split); returns the count
+int modswitch_tuned_shapes(int *out, int cap);
 // tensor-core column pass (modswitch_tc.cu); every job has K <= 16
 void launch_modswitch_cols_tc(const MSColBatch &b, int max_k, cudaStream_t s);
 size_t modswitch_cols_tc_smem(int kmax);

@@ -16,6 +16,7 @@
 #include <map>
 #include <mutex>
 #include <tuple>
+#include <vector>
 
 #include "arith.cuh"
 #include "colpass.cuh"
@@ -254,78 +255,6 @@ void launch_engine(const MSColBatch &b, int engine, int max_k, cudaStream_t s) {
     go(k_modswitch_cols<16, 0>, 16);
 }
 
-// Engine autotuning (engine 2): the CUDA-core pass wins on small launches
-// (one ciphertext), the tensor-core pass on large ones.  The first launch of
-// a shape (device, largest K, jobs, largest M) outside a stream capture runs
-// both engines four times, times the last three of each with CUDA events (a
-// host synchronisation, once per shape), keeps the faster and caches the choice
-// for the process.  Both engines write identical residues, so the tuning
-// launches leave the same outputs.  During a capture an untuned shape uses
-// the tensor cores.  Returns true when the tuning launches have done the work.
-bool tune_and_launch(const MSColBatch &b, int max_k, cudaStream_t s, int *engine) {
-  static std::mutex mu;
-  static std::map<std::tuple<int, int, int, int>, int> cache;
-  int dev = 0, max_m = 0;
-  cudaGetDevice(&dev);
-  for (int j = 0; j < b.count; j++) max_m = b.jobs[j].M > max_m ? b.jobs[j].M : max_m;
-  const auto key = std::make_tuple(dev, max_k, b.count, max_m);
-  {
-    std::lock_guard<std::mutex> lock(mu);
-    auto it = cache.find(key);
-    if (it != cache.end()) {
-      *engine = it->second;
-      return false;
-    }
-  }
-  *engine = 1;
-  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return false;
-  // three rounds of (CUDA cores, tensor cores) after a warm-up of each; the
-  // fastest launch of each engine decides (one launch each was noisy enough
-  // to flip the choice between runs)
-  constexpr int kRounds = 3;
-  cudaEvent_t ev[2 * kRounds + 1] = {};
-  for (auto &e : ev)
-    if (cudaEventCreate(&e) != cudaSuccess) {
-      for (auto &f : ev)
-        if (f) cudaEventDestroy(f);
-      return false;
-    }
-  launch_engine(b, 0, max_k, s);  // warm-up: module load, attributes
-  launch_engine(b, 1, max_k, s);
-  cudaEventRecord(ev[0], s);
-  for (int i = 0; i < kRounds; i++) {
-    launch_engine(b, 0, max_k, s);
-    cudaEventRecord(ev[2 * i + 1], s);
-    launch_engine(b, 1, max_k, s);
-    cudaEventRecord(ev[2 * i + 2], s);
-  }
-  bool ok = cudaEventSynchronize(ev[2 * kRounds]) == cudaSuccess;
-  float t_cuda = 1e30f, t_tc = 1e30f;
-  for (int i = 0; ok && i < kRounds; i++) {
-    float a = 0.f, c = 0.f;
-    ok = cudaEventElapsedTime(&a, ev[2 * i], ev[2 * i + 1]) == cudaSuccess &&
-         cudaEventElapsedTime(&c, ev[2 * i + 1], ev[2 * i + 2]) == cudaSuccess;
-    t_cuda = a < t_cuda ? a : t_cuda;
-    t_tc = c < t_tc ? c : t_tc;
-  }
-  for (auto &e : ev) cudaEventDestroy(e);
-  if (ok) {
-    *engine = t_tc <= t_cuda ? 1 : 0;
-    std::lock_guard<std::mutex> lock(mu);
-    cache[key] = *engine;
-  }
-  return true;
-}
-
-void launch_batch(const MSColBatch &b, cudaStream_t s) {
-  int max_k = 0;
-  for (int j = 0; j < b.count; j++) max_k = b.jobs[j].K > max_k ? b.jobs[j].K : max_k;
-  int engine = b.engine;
-  if (engine == 2 && tune_and_launch(b, max_k, s, &engine)) return;
-  launch_engine(b, engine, max_k, s);
-}
-
 int sm_count() {
   static int n = 0;
   if (!n) {
@@ -337,24 +266,13 @@ int sm_count() {
   return n;
 }
 
-}  // namespace
-
-void launch_modswitch_cols(const MSColBatch &b, int log_n, cudaStream_t s) {
-  if (b.count <= 0 || log_n != 16) return;
-  // A small batch (one ciphertext: a few jobs x 32 column tiles) leaves
-  // most SMs idle.  Spread each job's targets over `groups` sub-jobs (each
-  // repeats the job's INTT column stages for its own subset of targets) so
-  // that the grid covers about two CTAs per SM; at least 4 targets each.
-  const int tiles = 512 / kTC;
-  const int want = 2 * sm_count();
-  int max_m = 0;
-  for (int j = 0; j < b.count; j++) max_m = b.jobs[j].M > max_m ? b.jobs[j].M : max_m;
-  int groups = (want + tiles * b.count - 1) / (tiles * b.count);
-  groups = groups < 1 ? 1 : groups;
-  const int by_m = max_m / 4 > 1 ? max_m / 4 : 1;
-  groups = groups > by_m ? by_m : groups;
-  if (groups == 1) {
-    launch_batch(b, s);
+// Launches b with every job's targets spread over `groups` sub-jobs (each
+// repeats its job's INTT column stages for its own subset of targets, at
+// least 4 targets each): more, smaller CTAs for launches that would leave
+// SMs idle.
+void launch_split(const MSColBatch &b, int groups, int engine, int max_k, cudaStream_t s) {
+  if (groups <= 1) {
+    launch_engine(b, engine, max_k, s);
     return;
   }
   MSColBatch e = b;
@@ -373,12 +291,139 @@ void launch_modswitch_cols(const MSColBatch &b, int log_n, cudaStream_t s) {
         d.dst_gidx[m] = src.dst_gidx[m0 + m];
       }
       if (e.count == kMaxMSColJobs) {
-        launch_batch(e, s);
+        launch_engine(e, engine, max_k, s);
         e.count = 0;
       }
     }
   }
-  if (e.count) launch_batch(e, s);
+  if (e.count) launch_engine(e, engine, max_k, s);
+}
+
+// the split of the fixed engines: about two CTAs per SM, at least 4 targets
+// per sub-job
+int heuristic_groups(const MSColBatch &b, int max_m) {
+  const int tiles = 512 / kTC;
+  const int want = 2 * sm_count();
+  int groups = (want + tiles * b.count - 1) / (tiles * b.count);
+  groups = groups < 1 ? 1 : groups;
+  const int by_m = max_m / 4 > 1 ? max_m / 4 : 1;
+  return groups > by_m ? by_m : groups;
+}
+
+// Autotuning (engine 2, CHD_BCONV_AUTO): which engine and which target split
+// are fastest depends on the launch (the CUDA-core pass wins when a launch
+// holds one ciphertext's few jobs, the tensor-core pass on batches; small
+// launches gain from the split).  The first launch of a shape (device,
+// largest K, jobs, largest M) outside a stream capture times every
+// candidate (engine x split in {1, 2, 4, heuristic}) three times after a
+// warm-up, interleaved, with CUDA events (a host synchronisation, once per
+// shape), keeps the fastest launch and caches the choice for the process.
+// Every candidate writes identical residues, so the tuning launches leave
+// the right outputs.  During a capture an untuned shape uses the tensor
+// cores with the heuristic split.  Returns true when the tuning launches
+// have done the work; *engine and *groups receive the choice otherwise.
+struct Choice {
+  int engine, groups;
+};
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int>, Choice> g_tune_cache;
+
+bool tune_and_launch(const MSColBatch &b, int max_k, int max_m, cudaStream_t s, Choice *out) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const auto key = std::make_tuple(dev, max_k, b.count, max_m);
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      *out = it->second;
+      return false;
+    }
+  }
+  const int hg = heuristic_groups(b, max_m);
+  *out = Choice{1, hg};
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return false;
+  std::vector<Choice> cand;
+  const int by_m = max_m / 4 > 1 ? max_m / 4 : 1;
+  for (int e = 0; e < 2; e++)
+    for (int g : {1, 2, 4, hg})
+      if (g <= by_m) {
+        bool seen = false;
+        for (const Choice &c : cand) seen |= c.engine == e && c.groups == g;
+        if (!seen) cand.push_back(Choice{e, g});
+      }
+  constexpr int kRounds = 3;
+  const int nc = static_cast<int>(cand.size());
+  std::vector<cudaEvent_t> ev(nc * kRounds + 1, nullptr);
+  for (auto &x : ev)
+    if (cudaEventCreate(&x) != cudaSuccess) {
+      for (auto &f : ev)
+        if (f) cudaEventDestroy(f);
+      return false;
+    }
+  for (const Choice &c : cand) launch_split(b, c.groups, c.engine, max_k, s);  // warm-up
+  cudaEventRecord(ev[0], s);
+  for (int r = 0; r < kRounds; r++)
+    for (int i = 0; i < nc; i++) {
+      launch_split(b, cand[i].groups, cand[i].engine, max_k, s);
+      cudaEventRecord(ev[r * nc + i + 1], s);
+    }
+  bool ok = cudaEventSynchronize(ev.back()) == cudaSuccess;
+  std::vector<float> best(nc, 1e30f);
+  for (int r = 0; ok && r < kRounds; r++)
+    for (int i = 0; ok && i < nc; i++) {
+      float t = 0.f;
+      ok = cudaEventElapsedTime(&t, ev[r * nc + i], ev[r * nc + i + 1]) == cudaSuccess;
+      best[i] = t < best[i] ? t : best[i];
+    }
+  for (auto &x : ev) cudaEventDestroy(x);
+  if (ok) {
+    int bi = 0;
+    for (int i = 1; i < nc; i++)
+      if (best[i] < best[bi]) bi = i;
+    *out = cand[bi];
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune_cache[key] = cand[bi];
+  }
+  return true;
+}
+
+}  // namespace
+
+void launch_modswitch_cols(const MSColBatch &b, int log_n, cudaStream_t s) {
+  if (b.count <= 0 || log_n != 16) return;
+  int max_k = 0, max_m = 0;
+  for (int j = 0; j < b.count; j++) {
+    max_k = b.jobs[j].K > max_k ? b.jobs[j].K : max_k;
+    max_m = b.jobs[j].M > max_m ? b.jobs[j].M : max_m;
+  }
+  if (b.engine == 2) {
+    Choice c{1, 1};
+    if (tune_and_launch(b, max_k, max_m, s, &c)) return;
+    launch_split(b, c.groups, c.engine, max_k, s);
+    return;
+  }
+  launch_split(b, heuristic_groups(b, max_m), b.engine, max_k, s);
+}
+
+int modswitch_tuned_shapes(int *out, int cap) {
+  // (device, max_k, jobs, max_m, engine, groups) per cached shape
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  int k = 0;
+  for (const auto &kv : g_tune_cache) {
+    if (out && k < cap) {
+      int *o = out + 6 * k;
+      o[0] = std::get<0>(kv.first);
+      o[1] = std::get<1>(kv.first);
+      o[2] = std::get<2>(kv.first);
+      o[3] = std::get<3>(kv.first);
+      o[4] = kv.second.engine;
+      o[5] = kv.second.groups;
+    }
+    k++;
+  }
+  return k;
 }
 
 }  // namespace chd

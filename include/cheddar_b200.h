@@ -115,6 +115,11 @@ int chd_ct_device_ptrs(const chd_ciphertext *ct, uint32_t **bx, uint32_t **ax, u
 int chd_evk_create(chd_context *ctx, int beta, const uint32_t *bx, const uint32_t *ax,
                    int src_on_device, chd_evk **out);
 void chd_evk_destroy(chd_evk *evk);
+/* EvaluationKey::GetBeta / GetNP (Container.h:300-312): digits and key basis */
+int chd_evk_info(const chd_evk *evk, int *beta, int *num_main, int *num_ter, int *num_aux);
+/* the key's beta pairs [beta][np.total][N] to host (or device) buffers, the
+ * layout chd_evk_create / chd_evk_create_np take */
+int chd_evk_export(chd_context *ctx, const chd_evk *evk, uint32_t *bx, uint32_t *ax, int dst_on_device);
 
 /* ---- evaluator (include/core/Context.h:101-423) ----------------------------- */
 /* Context::Add / Sub / Neg (Context.cpp:146-169, 205-229, 306-315) */
@@ -248,10 +253,19 @@ int chd_bconv_raw(chd_context *ctx, const int32_t *xt_dev, const int *src_gidx, 
  * complex slots (re, im; padded to a power of two, written to *num_slots)
  * at `scale` -> plaintext [num_q(level) + num_aux][N] at pt_dev, evaluation
  * domain, Montgomery form (prime order: terminal reversed, main, aux).
- * FP64 special IFFT on the host, truncation toward zero, device NTT;
- * returns after the upload. */
+ * On the device: FP64 special IFFT, truncation toward zero, residues, NTT;
+ * returns when the plaintext is written. */
 int chd_encode(chd_context *ctx, int level, double scale, const double *re, const double *im, int msg_len,
                int num_aux, uint32_t *pt_dev, int *num_slots);
+/* Encoder::Decode (src/core/Encode.cpp:45-70, 109-133, 192-248): plaintext
+ * [num_q(level)][N] at pt_dev (evaluation domain, Montgomery form, no aux
+ * primes) at `scale` -> num_slots complex slots (a power of two <= N/2)
+ * written to the host arrays re, im.  On the device: INTT times
+ * (N q-hat)^-1, CRT to the centred integer (exact while its magnitude is
+ * below 2^127), double / scale, FP64 special FFT; the same doubles as the
+ * reference's decoder.  Returns when the slots are written. */
+int chd_decode(chd_context *ctx, int level, double scale, const uint32_t *pt_dev, int num_slots, double *re,
+               double *im);
 /* Encoder::EncodeConstant (Encode.cpp:250-275): cx[num_q(level) + num_aux]
  * Montgomery residues of trunc(value * scale), host memory. */
 int chd_encode_const(chd_context *ctx, int level, double scale, double value, int num_aux, uint32_t *cx);
@@ -407,14 +421,67 @@ int chd_bconv_batch(chd_context *ctx, int engine, int npoly, const int32_t *xt_d
  * column pass issues INT8 byte-limb MMAs on the tcgen05 tensor cores with
  * int32 accumulation in TMEM).  Both give bit-identical residues.
  * CHD_BCONV_AUTO autotunes: the first column pass of each launch shape
- * (device, sources, jobs, targets) outside a stream capture runs both
- * engines, times them (one host synchronisation per shape and process) and
- * keeps the faster; an untuned shape met during a capture uses the tensor
- * cores.  No reference counterpart (the reference has one CUDA-core
+ * (device, sources, jobs, targets) outside a stream capture times both
+ * engines with each split of the targets over 1, 2, 4 or the heuristic
+ * number of CTAs per column tile (one host synchronisation per shape and
+ * process) and keeps the fastest; an untuned shape met during a capture
+ * uses the tensor cores with the heuristic split.  No reference counterpart (the reference has one CUDA-core
  * implementation, src/core/ModSwitch.cu:23-171).  chd_get_ks_engine returns
  * the engine, -1 for a null context. */
 int chd_set_ks_engine(chd_context *ctx, int engine);
 int chd_get_ks_engine(const chd_context *ctx);
+/* The autotuner's choices so far (no reference counterpart): per launch
+ * shape six ints (device, largest source count K, jobs, largest target
+ * count M, engine 0/1, target split) into out (capacity cap shapes);
+ * returns the number of shapes tuned in this process. */
+int chd_ks_tuned_shapes(int *out, int cap);
+
+/* ---- residue serialization (no counterpart in the reference, whose objects
+ * live only in device memory): a ciphertext or key as a self-describing
+ * byte buffer (magic, ring degree, prime counts, scale and slot count,
+ * the primes of its rows, then the residues in their device layout).
+ * Loading checks the degree and every prime against the context.  With buf
+ * null, *len receives the size needed. ---- */
+int chd_ct_serialize(chd_context *ctx, const chd_ciphertext *ct, void *buf, size_t cap, size_t *len);
+int chd_ct_deserialize(chd_context *ctx, chd_ciphertext *ct, const void *buf, size_t len);
+int chd_evk_serialize(chd_context *ctx, const chd_evk *evk, void *buf, size_t cap, size_t *len);
+int chd_evk_deserialize(chd_context *ctx, const void *buf, size_t len, chd_evk **out);
+
+/* ---- test-only client (the reference's UserInterface, src/UserInterface.cu:
+ * 110-541, "not secure, for testing"): secrets, evaluation keys, encryption
+ * and decryption on the device, reproducible from a seed.  The key and
+ * ciphertext structure is the reference's; the randomness is a seeded
+ * counter-based generator (the reference draws from an unseeded
+ * std::random_device / mt19937_64), errors with the reference's
+ * distribution, round(N(0, 3.2^2)) clamped at 6 sigma. ---- */
+typedef struct chd_client chd_client;
+/* UserInterface constructor (PrepareSecrets, UserInterface.cu:224-276): the
+ * dense ternary secret (the parameters' dense Hamming weight, N/2 when
+ * unset) and, with sparse-secret encapsulation, the sparse one, over the
+ * full key basis in the NTT Montgomery domain. */
+int chd_client_create(chd_context *ctx, uint64_t seed, chd_client **out);
+void chd_client_destroy(chd_client *cl);
+/* the secret's residues [L + alpha][N] (NTT Montgomery domain) to host
+ * memory; sparse != 0 for the sparse secret (tests only) */
+int chd_client_secret(chd_context *ctx, const chd_client *cl, int sparse, uint32_t *out);
+/* PrepareBasicEvks / PrepareRotationKey (UserInterface.cu:278-364): keys
+ * over the max-level key basis (beta digits) as chd_evk objects */
+int chd_client_mult_key(chd_context *ctx, chd_client *cl, chd_evk **out);
+int chd_client_rotation_key(chd_context *ctx, chd_client *cl, int rot_idx, chd_evk **out);
+int chd_client_conjugation_key(chd_context *ctx, chd_client *cl, chd_evk **out);
+/* sparse-secret encapsulation keys: dense-to-sparse over the level -1 primes
+ * and as many aux primes, sparse-to-dense as one digit over the key basis
+ * (UserInterface.cu:335-352), for chd_evk_map_set_dense_to_sparse /
+ * _sparse_to_dense */
+int chd_client_sse_keys(chd_context *ctx, chd_client *cl, chd_evk **dense_to_sparse, chd_evk **sparse_to_dense);
+/* UserInterface::Encrypt (UserInterface.cu:132-183): plaintext
+ * [num_q(level)][N] at pt_dev (as chd_encode writes it) -> ct at `level`
+ * with `scale` and `num_slots`; `nonce` selects the encryption randomness. */
+int chd_client_encrypt(chd_context *ctx, chd_client *cl, uint64_t nonce, int level, double scale, int num_slots,
+                       const uint32_t *pt_dev, chd_ciphertext *ct);
+/* UserInterface::Decrypt (UserInterface.cu:185-206): ct (relinearised, no
+ * aux primes) -> plaintext [num_q][N] at pt_dev, for chd_decode. */
+int chd_client_decrypt(chd_context *ctx, const chd_client *cl, const chd_ciphertext *ct, uint32_t *pt_dev);
 
 /* Test hook for the bounded waits of the tensor-core kernels (no reference
  * counterpart: the reference's kernels have no tensor-core waits).  With

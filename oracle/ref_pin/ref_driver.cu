@@ -274,6 +274,38 @@ int refx_decrypt_decode(void *p, void *c, double *re, double *im) {
   return last_cuda();
 }
 
+// UserInterface::Decrypt (UserInterface.cu:185-206): plaintext residues
+// [np.total][N] (evaluation domain, Montgomery form) of a ciphertext.
+int refx_decrypt(void *p, void *c, uint32_t *pt_out, double *scale, int *num_slots) {
+  auto *R = static_cast<RefCtx *>(p);
+  Plaintext<word> pt;
+  R->ui->Decrypt(pt, *static_cast<Ciphertext<word> *>(c));
+  copy_out(pt_out, pt.mx_, poly_words(pt.GetNP(), R->degree));
+  *scale = pt.GetScale();
+  *num_slots = pt.GetNumSlots();
+  return last_cuda();
+}
+
+// Encoder::Decode (Encode.cpp:45-70, 192-248) of plaintext residues at a
+// level (no aux primes), scale and slot count.
+int refx_decode(void *p, int level, double scale, int num_slots, const uint32_t *pt_host, double *re,
+                double *im) {
+  auto *R = static_cast<RefCtx *>(p);
+  Plaintext<word> pt;
+  NPInfo np = R->param->LevelToNP(level);
+  pt.ModifyNP(np);
+  pt.SetScale(scale);
+  pt.SetNumSlots(num_slots);
+  copy_in(pt.mx_, pt_host, poly_words(np, R->degree));
+  std::vector<Complex> msg;
+  R->ctx->encoder_.Decode(msg, pt);
+  for (size_t i = 0; i < msg.size(); i++) {
+    re[i] = msg[i].real();
+    im[i] = msg[i].imag();
+  }
+  return last_cuda();
+}
+
 // Encoded plaintext residues (Encode.cpp:135-190) of a message at a level,
 // scale and number of aux primes: out = [np.total][N].
 int refx_encode(void *p, int level, double scale, const double *re, const double *im, int num_slots,

@@ -61,6 +61,8 @@ def lib():
             "refx_ct_import": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, u32p, u32p]),
             "refx_ct_encrypt": (C.c_int, [vp, vp, C.c_int, C.c_void_p, C.c_void_p, C.c_int]),
             "refx_decrypt_decode": (C.c_int, [vp, vp, C.c_void_p, C.c_void_p]),
+            "refx_decrypt": (C.c_int, [vp, vp, u32p, C.POINTER(C.c_double), ip]),
+            "refx_decode": (C.c_int, [vp, C.c_int, C.c_double, C.c_int, u32p, C.c_void_p, C.c_void_p]),
             "refx_encode": (C.c_int, [vp, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_int, C.c_int, u32p]),
             "refx_hmult": (C.c_int, [vp, vp, vp, vp, C.c_int]),
             "refx_hrot": (C.c_int, [vp, vp, vp, C.c_int]),
@@ -198,6 +200,22 @@ class RefContext:
         re = np.zeros(ns)
         im = np.zeros(ns)
         _chk(lib().refx_decrypt_decode(self.ptr, c.ptr, re.ctypes.data, im.ctypes.data), "decrypt")
+        return re + 1j * im
+
+    def decrypt(self, c):
+        """(plaintext residues [num_q][N], scale, num_slots) of a ciphertext."""
+        inf = c.info()
+        out = np.zeros((inf["num_main"] + inf["num_ter"], self.n), dtype=np.uint32)
+        sc, ns = C.c_double(), C.c_int()
+        _chk(lib().refx_decrypt(self.ptr, c.ptr, out.ctypes.data, C.byref(sc), C.byref(ns)), "decrypt")
+        return out, sc.value, ns.value
+
+    def decode(self, level, scale, num_slots, pt):
+        p = _u32(pt)
+        re = np.zeros(num_slots)
+        im = np.zeros(num_slots)
+        _chk(lib().refx_decode(self.ptr, level, scale, num_slots, p.ctypes.data, re.ctypes.data, im.ctypes.data),
+             "decode")
         return re + 1j * im
 
     def encode(self, level, scale, msg, num_aux=0):

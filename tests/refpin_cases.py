@@ -346,6 +346,41 @@ def case_context_ops40():
     return _context_ops("bootparam_40.json", [(28, 1), (16, 2), (5, 3), (4, 4), (3, 5), (2, 6), (1, 7)])
 
 
+def case_decode():
+    """Encoder::Decode (Encode.cpp:45-70, 192-248) of the reference against
+    this library's device decoder, double for double: plaintexts the
+    reference decrypts from its own encryptions (at several levels and slot
+    counts of bootparam_40.json, terminal primes included) and from products
+    (HMult), and plaintexts of the library's encoder."""
+    import torch
+    t = Trio(load("bootparam_40.json"))
+    g, ref = t.g, t.ref
+    checked = 0
+    for lvl, ns, seed in [(0, t.n // 2, 1), (3, 1 << 10, 2), (13, t.n // 2, 3), (16, 256, 4), (28, t.n // 2, 5)]:
+        msg = t.message(seed, slots=ns, lo=-1.0, hi=1.0)
+        pt, sc, nsl = ref.decrypt(ref.encrypt(lvl, msg))
+        assert nsl == ns
+        want = ref.decode(lvl, sc, ns, pt)
+        got = g.decode(lvl, sc, torch.from_numpy(pt.view(np.int32)).cuda(), ns)
+        assert np.array_equal(got, want), f"decode level {lvl}: max diff {np.abs(got - want).max()}"
+        assert max_component_error(got, msg) < 1e-3
+        checked += 1
+        enc = g.encode(lvl, ref.test_scale(lvl), msg)
+        g.synchronize()
+        pt2 = enc.cpu().numpy().view(np.uint32)
+        want = ref.decode(lvl, ref.test_scale(lvl), ns, pt2)
+        got = g.decode(lvl, ref.test_scale(lvl), enc, ns)
+        assert np.array_equal(got, want), f"decode of an encoding, level {lvl}"
+        checked += 1
+    lvl = 16
+    ra, rb = ref.encrypt(lvl, t.message(9)), ref.encrypt(lvl, t.message(10))
+    pt, sc, ns = ref.decrypt(ref.HMult(ra, rb))
+    want = ref.decode(lvl - 1, sc, ns, pt)
+    got = g.decode(lvl - 1, sc, torch.from_numpy(pt.view(np.int32)).cuda(), ns)
+    assert np.array_equal(got, want), "decode of a product"
+    return {"checked": checked + 1}
+
+
 def _boot_trio(name, num_slots=None):
     t = Trio(load(name))
     g, ref = t.g, t.ref

@@ -14,7 +14,8 @@ reference's own keys and encryptions; every residue must be equal:
   Rescale, MultKey, Permute, MultImaginaryUnit, LevelDown, HRotAdd,
   HConjAdd, MultUnsafe, HMult, on the L = 24 set and on bootparam_40.json
   (terminal primes, rational rescale);
-* encode: the encoder at several levels, scales and aux counts;
+* encode, decode: the encoder at several levels, scales and aux counts; the
+  decoder, double for double, on the reference's decryptions;
 * boot40, boot30, boot35: full-slot Boot, hoisted and min-KS, and
   BootBatch, on the reference's bootparam_{40,30,35}.json exactly, with the
   reference's decoded precision; boot40_sparse: 2^10 slots.
@@ -36,7 +37,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 @pytest.mark.parametrize("case", ["ntt24", "modswitch", "keyswitch", "hoisted", "context_ops", "context_ops40",
-                                  "encode", "boot40", "boot30", "boot35", "boot40_sparse"])
+                                  "encode", "decode", "boot40", "boot30", "boot35", "boot40_sparse"])
 def test_reference_parity(cuda_ok, case):
     if not refdrv.available():
         pytest.fail("oracle/_ref/libcheddar_ref.so is missing: build it with `make -C oracle ref REF=<tree>`")
