@@ -285,11 +285,15 @@ def main():
         "bootstrap": boot, "hoisted_and_mixed": hoist_mixed,
         "gpu_launches": launches,
     }
+    # the autotuner's choice per column-pass launch shape (largest source
+    # count K, jobs, largest target count M) -> engine / target split
+    line["config"]["autotuned_column_passes"] = [
+        f"K{t['K']} jobs{t['jobs']} M{t['M']}: {'tensor_core' if t['engine'] else 'cuda_core'}/split{t['split']}"
+        for t in chd.ks_tuned_shapes()]
     if rank == 0 and world == 1 and not args.no_reference_gpu:
         ref = reference_gpu_run(args)
         try:
             ref["hmult_ours_over_reference"] = value / ref["hmult"]["hmult_per_s"]
-            ref["e2e_hmult_ours_over_reference"] = e2e["value"] / ref["hmult"]["hmult_per_s"]
         except (KeyError, TypeError, ZeroDivisionError):
             pass
         try:
@@ -388,10 +392,25 @@ def e2e_run(ctx, chd, key, lvl, nq, n, B, args, stream, dist):
     torch.cuda.synchronize()
     ms = max_over_ranks(dist, ev0.elapsed_time(ev1), "cuda")
     world = dist.get_world_size() if dist else 1
-    return {"value": job_throughput(world, B, steps, ms), "unit": UNIT,
-            "h2d_bytes_per_step": B * 4 * words * 4,
+    # the PCIe bound of this pipeline: one step's host-to-device bytes at the
+    # bandwidth of the same copies alone (no kernels, no reads back)
+    h2d_bytes = B * 4 * words * 4
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(h2d):
+        c0.record(h2d)
+        for r in range(3):
+            for k in range(B):
+                dev_in[r & 1][k].copy_(host_in[r & 1][k], non_blocking=True)
+        c1.record(h2d)
+    torch.cuda.synchronize()
+    h2d_gbs = 3 * h2d_bytes / (c0.elapsed_time(c1) / 1e3) / 1e9
+    value = job_throughput(world, B, steps, ms)
+    bound = world * B / (h2d_bytes / (h2d_gbs * 1e9))  # every rank has its own link
+    return {"value": value, "unit": UNIT,
+            "h2d_bytes_per_step": h2d_bytes,
             "d2h_bytes_per_step": B * 2 * nout * n * 4,
-            "pipeline": "double-buffered: H2D of step i+1, HMult of step i, D2H of step i-1 on three streams"}
+            "pipeline": "double-buffered: H2D of step i+1, HMult of step i, D2H of step i-1 on three streams",
+            "pcie_h2d_GB/s": h2d_gbs, "pcie_bound_hmult_per_s": bound, "frac_of_pcie_bound": value / bound}
 
 
 _cudart = None
@@ -703,11 +722,12 @@ def bconv_engines(ctx, chd, stream, npoly=64, reps=10):
 def hoist_mixed_bench(ctx, chd, key, uniform, stream, reps=5):
     """(i) One ciphertext at the top level rotated by the 30 distinct offsets
     {+-2^k, k < 15} u {1..4} mod 2^15: all rotations of one ModUp in one
-    launch (HoistedRotate, results in Q u P, then ModDown) against 30
-    separate HRot calls.  (ii) 16 HMult+relin+rescale pairs at levels drawn
+    launch (HoistedRotate, results in Q u P, then one batched ModDown of
+    the 30 results) against 30 separate HRot calls.  (ii) 16 HMult+relin+rescale pairs at levels drawn
     uniformly from 5..22 (seed 0; 22 is this set's top level): one HMult
-    call per pair, the batched call (one fused pipeline per level), and the
-    batched call captured once in a CUDA graph and replayed.  Keys are
+    call per pair, the batched call (one fused pipeline over every level:
+    a launch per stage, the row pass taking up to 8 levels per launch), and
+    the batched call captured once in a CUDA graph and replayed.  Keys are
     uniform random residues; CUDA events on the context stream."""
     import numpy as np
     import torch
@@ -742,8 +762,7 @@ def hoist_mixed_bench(ctx, chd, key, uniform, stream, reps=5):
 
     def hoisted():
         ctx.HoistedRotate(ct, keys, offsets, outs=qp_outs)
-        for q, o in zip(qp_outs, outs):
-            ctx.ModDown(q, res=o)
+        ctx.ModDownBatch(qp_outs, res_list=outs)
 
     def separate():
         for k, r, o in zip(keys, offsets, outs):

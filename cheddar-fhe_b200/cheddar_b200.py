@@ -122,6 +122,8 @@ def lib():
         "chd_debug_stall_tensor_waits": (i, [vp, i]),
         "chd_decode": (i, [vp, i, C.c_double, vp, i, vp, vp]),
         "chd_evk_info": (i, [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(i)]),
+        "chd_ks_tuned_shapes": (i, [vp, i]),
+        "chd_moddown_batch": (i, [vp, i, vp, vp]),
         "chd_ct_serialize": (i, [vp, vp, vp, C.c_size_t, C.POINTER(C.c_size_t)]),
         "chd_ct_deserialize": (i, [vp, vp, vp, C.c_size_t]),
         "chd_evk_serialize": (i, [vp, vp, vp, C.c_size_t, C.POINTER(C.c_size_t)]),
@@ -196,6 +198,17 @@ def _ptr(a):
     if hasattr(a, "data_ptr"):
         return a.data_ptr()
     return a.ctypes.data
+
+
+def ks_tuned_shapes():
+    """The column-pass autotuner's choices in this process: one dict per
+    launch shape (largest source count K, jobs, largest target count M) with
+    the engine (0 CUDA cores, 1 tensor cores) and the target split."""
+    n = lib().chd_ks_tuned_shapes(None, 0)
+    out = (C.c_int * (6 * max(1, n)))()
+    n = lib().chd_ks_tuned_shapes(out, n)
+    return [dict(device=out[6 * i], K=out[6 * i + 1], jobs=out[6 * i + 2], M=out[6 * i + 3],
+                 engine=out[6 * i + 4], split=out[6 * i + 5]) for i in range(n)]
 
 
 def load_params(name_or_path):
@@ -551,6 +564,16 @@ class Context:
         res = self._new(res)
         _check(lib().chd_moddown(self.ptr, res.ptr, a.ptr))
         return res
+
+    def ModDownBatch(self, cts, res_list=None):
+        """ModDown of every ciphertext of `cts` (one level, Q u P) in one
+        pipeline; equals ModDown on each."""
+        res_list = res_list if res_list is not None else [Ciphertext(self) for _ in cts]
+        n = len(cts)
+        ins = (C.c_void_p * n)(*[c.ptr.value for c in cts])
+        outs = (C.c_void_p * n)(*[r.ptr.value for r in res_list])
+        _check(lib().chd_moddown_batch(self.ptr, n, outs, ins))
+        return res_list
 
     # ---- raw device-buffer kernels (parity entry points) ----
     def ntt_raw(self, num_main, num_ter, num_aux, dev_ptr, mont=False, count=1):

@@ -1579,6 +1579,25 @@ int chd_moddown(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a) 
   return fail(CHD_ERR_INTERNAL, "internal error");
 }
 
+int chd_moddown_batch(chd_context *ctx, int count, chd_ciphertext *const *res, const chd_ciphertext *const *a) try {
+  CHD_CTX(ctx);
+  CHD_NOTNULL(res);
+  CHD_NOTNULL(a);
+  if (count < 1) return fail(CHD_ERR_INVALID_ARG, "chd_moddown_batch: empty batch");
+  std::vector<DeviceCt *> r(count);
+  std::vector<const DeviceCt *> x(count);
+  for (int i = 0; i < count; i++) {
+    if (!res[i] || !a[i]) return fail(CHD_ERR_INVALID_ARG, "chd_moddown_batch: null ciphertext");
+    r[i] = &res[i]->ct;
+    x[i] = &a[i]->ct;
+  }
+  return ctx->c->moddown_batch(count, r.data(), x.data());
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
+}
+
 int chd_ntt(chd_context *ctx, int num_main, int num_ter, int num_aux, uint32_t *data_dev, int mont, int count) try {
   CHD_CTX(ctx);
   CHD_NOTNULL(data_dev);

@@ -1149,91 +1149,133 @@ Status Context::moddown_plan(int level, MDType type, MDPlan *pl) const {
 
 Status Context::key_switch_fused(int level, int count, const KSIn *in, const DeviceEvk &key, MDType type,
                                  bool keep_ext) {
+  std::vector<int> levels(std::max(count, 0), level);
+  return key_switch_fused_levels(levels.data(), count, in, key, type, keep_ext);
+}
+
+Status Context::key_switch_fused_levels(const int *levels, int count, const KSIn *in, const DeviceEvk &key,
+                                        MDType type, bool keep_ext) {
   CHD_CHECK(P->log_n == 16, kErrUnsupported, "fused key switch needs N = 2^16");
   CHD_CHECK(keep_ext || type != MDType::kRescale, kErrInvalidArg,
             "fused key switch ends in ModDown or ModDownAndRescale");
-  const LevelMS &m = lms(level);
-  const int n = P->n;
-  NP np = P->level_np(level, P->alpha);
-  const int nq = np.q(), tot = np.total();
-  CHD_CHECK(tot <= 64 && m.beta <= 8, kErrUnsupported, "key switch: more than 64 primes or 8 digits");
   CHD_CHECK(key.np.aux == P->alpha && key.np.q() == P->L, kErrKey, "key switch: key basis mismatch");
-  MDPlan pl;
-  if (!keep_ext) CHD_TRY(moddown_plan(level, type, &pl));
-  const int prime_offset = P->max_ter - np.ter;
-  std::vector<int> g(tot);
-  P->gidx(np, g.data());
-  std::vector<int> digits;
-  for (int i = 0; i < m.beta; i++)
-    if (m.dig_e[i] > 0) {
-      CHD_CHECK(i < key.beta, kErrKey, "key switch: key has too few digits");
-      digits.push_back(i);
+  if (count <= 0) return kOk;
+  // per-level shapes, shared by the ciphertexts at that level
+  struct Shape {
+    const LevelMS *m;
+    int nq, tot, prime_offset;
+    std::vector<int> g, digits;
+    MDPlan pl;
+  };
+  std::map<int, Shape> shapes;
+  for (int c = 0; c < count; c++) {
+    const int level = levels[c];
+    if (shapes.count(level)) continue;
+    CHD_CHECK(level >= 0 && level <= P->max_level, kErrInvalidLevel, "key switch: invalid level");
+    Shape &sh = shapes[level];
+    sh.m = &lms(level);
+    const NP np = P->level_np(level, P->alpha);
+    sh.nq = np.q();
+    sh.tot = np.total();
+    CHD_CHECK(sh.tot <= 64 && sh.m->beta <= 8, kErrUnsupported, "key switch: more than 64 primes or 8 digits");
+    sh.prime_offset = P->max_ter - np.ter;
+    sh.g.resize(sh.tot);
+    P->gidx(np, sh.g.data());
+    for (int i = 0; i < sh.m->beta; i++)
+      if (sh.m->dig_e[i] > 0) {
+        CHD_CHECK(i < key.beta, kErrKey, "key switch: key has too few digits");
+        sh.digits.push_back(i);
+      }
+    if (!keep_ext) CHD_TRY(moddown_plan(level, type, &sh.pl));
+  }
+  const int mode = in[0].mode;
+  for (int c = 0; c < count; c++)
+    CHD_CHECK(in[c].mode == mode, kErrInvalidArg, "key switch: mixed modes in one batch");
+  // scratch offsets (in polynomials of N words) per ciphertext
+  const size_t N = static_cast<size_t>(P->n);
+  std::vector<size_t> o_t1(count), o_mu(count), o_acc(count), o_drop(count);
+  size_t n_t1 = 0, n_mu = 0, n_acc = 0, n_drop = 0;
+  for (int c = 0; c < count; c++) {
+    const Shape &sh = shapes[levels[c]];
+    o_t1[c] = n_t1;
+    n_t1 += sh.nq;
+    o_mu[c] = n_mu;
+    n_mu += sh.digits.size() * sh.tot;
+    o_acc[c] = n_acc;
+    o_drop[c] = n_drop;
+    if (!keep_ext) {
+      n_acc += 2 * sh.tot;
+      n_drop += 2 * sh.pl.src_len;
     }
-  const int nb = static_cast<int>(digits.size());
+  }
   ArenaScope scope(arena);
-  const size_t N = static_cast<size_t>(n);
-  uint32_t *t1 = static_cast<uint32_t *>(arena.alloc(count * nq * N * 4));
-  uint32_t *mu = static_cast<uint32_t *>(arena.alloc(count * nb * tot * N * 4));
+  uint32_t *t1 = static_cast<uint32_t *>(arena.alloc(n_t1 * N * 4));
+  uint32_t *mu = static_cast<uint32_t *>(arena.alloc(n_mu * N * 4));
   // keep_ext: the accumulators go straight to the callers' buffers and
   // nothing is dropped
-  uint32_t *acc = keep_ext ? nullptr : static_cast<uint32_t *>(arena.alloc(count * 2 * tot * N * 4));
-  uint32_t *drop = keep_ext ? nullptr : static_cast<uint32_t *>(arena.alloc(count * 2 * pl.src_len * N * 4));
+  uint32_t *acc = keep_ext ? nullptr : static_cast<uint32_t *>(arena.alloc(n_acc * N * 4));
+  uint32_t *drop = keep_ext ? nullptr : static_cast<uint32_t *>(arena.alloc(n_drop * N * 4));
   CHD_CHECK(t1 && mu && (keep_ext || (acc && drop)), kErrAlloc, "key switch: scratch allocation failed");
-  auto MU = [&](int c, int b) { return mu + (static_cast<size_t>(c) * nb + b) * tot * N; };
+  auto MU = [&](int c, int b) { return mu + (o_mu[c] + static_cast<size_t>(b) * shapes[levels[c]].tot) * N; };
   // 1. ModUp INTT row phase of the key-switched input (a1 a2 / ax / rx)
   std::vector<RowDesc> rows;
-  for (int c = 0; c < count; c++)
-    for (int r = 0; r < nq; r++) {
+  for (int c = 0; c < count; c++) {
+    const Shape &sh = shapes[levels[c]];
+    for (int r = 0; r < sh.nq; r++) {
       RowDesc d{};
       const size_t o = static_cast<size_t>(r) * N;
       d.src = (in[c].mode == 2 ? in[c].a2 : in[c].a1) + o;
       if (in[c].mode == 0) {
         d.src2 = in[c].a2 + o;
         d.flags = kMulSrc2;
-        d.qinv = P->qinv[g[r]];
+        d.qinv = P->qinv[sh.g[r]];
       }
-      d.dst = t1 + (static_cast<size_t>(c) * nq + r) * N;
-      d.tw = itw(g[r]);
-      d.q = P->primes[g[r]];
+      d.dst = t1 + (o_t1[c] + r) * N;
+      d.tw = itw(sh.g[r]);
+      d.q = P->primes[sh.g[r]];
       rows.push_back(d);
     }
+  }
   int nl = 0, t0 = timer_mark();
   for_row_batches(rows, [&](const RowBatch &rb) {
     launch_ntt_inv_rows(rb, P->log_n, stream);
     nl++;
   });
   timer_span(kKsInvRows, t0, nl);
+  MSColBatch b{};
+  b.engine = ks_engine;
+  b.err = d_err;
+  b.tw = d_tw;
+  b.itw = d_itw;
+  b.primes = d_primes;
+  b.qinvs = d_qinv;
   // 2. ModUp column pass per (ciphertext, digit)
   {
     nl = 0;
     t0 = timer_mark();
-    MSColBatch b{};
-    b.engine = ks_engine;
-    b.err = d_err;
-    b.tw = d_tw;
-    b.itw = d_itw;
-    b.primes = d_primes;
-    b.qinvs = d_qinv;
-    for (int c = 0; c < count; c++)
-      for (int bi = 0; bi < nb; bi++) {
-        const int i = digits[bi], s = m.dig_s[i], e = m.dig_e[i];
+    b.count = 0;
+    for (int c = 0; c < count; c++) {
+      const Shape &sh = shapes[levels[c]];
+      const LevelMS &m = *sh.m;
+      for (size_t bi = 0; bi < sh.digits.size(); bi++) {
+        const int i = sh.digits[bi], s = m.dig_s[i], e = m.dig_e[i];
         MSColJob &j = b.jobs[b.count++];
-        j.src = t1 + static_cast<size_t>(c) * nq * N;
-        j.dst = MU(c, bi);
+        j.src = t1 + o_t1[c] * N;
+        j.dst = MU(c, static_cast<int>(bi));
         j.table = m.d_mod_up2[i];
         j.K = e - s;
-        j.M = tot - (e - s);
+        j.M = sh.tot - (e - s);
         CHD_CHECK(j.K <= 16 && j.M <= 64, kErrUnsupported, "modup: digit too large");
         for (int k = 0; k < j.K; k++) {
           j.src_row[k] = static_cast<uint8_t>(s + k);
-          j.src_gidx[k] = static_cast<uint8_t>(g[s + k]);
-          mont_as_shoup(m.mod_up1[s + k], g[s + k], &j.c0[k], &j.c0s[k]);
+          j.src_gidx[k] = static_cast<uint8_t>(sh.g[s + k]);
+          mont_as_shoup(m.mod_up1[s + k], sh.g[s + k], &j.c0[k], &j.c0s[k]);
         }
         int k = 0;
-        for (int r = 0; r < tot; r++) {
+        for (int r = 0; r < sh.tot; r++) {
           if (r >= s && r < e) continue;
           j.dst_row[k] = static_cast<uint8_t>(r);
-          j.dst_gidx[k] = static_cast<uint8_t>(g[r]);
+          j.dst_gidx[k] = static_cast<uint8_t>(sh.g[r]);
           k++;
         }
         if (b.count == kMaxMSColJobs) {
@@ -1242,81 +1284,99 @@ Status Context::key_switch_fused(int level, int count, const KSIn *in, const Dev
           b.count = 0;
         }
       }
+    }
     launch_modswitch_cols(b, P->log_n, stream);
     timer_span(kKsModUpCols, t0, nl + (b.count > 0));
   }
   // 3. row pass: ModUp NTT rows, key inner product, P (d0, d1), INTT rows of
-  //    the dropped primes
+  //    the dropped primes; a launch takes up to kMaxKSRowsCts ciphertexts
+  //    over up to kMaxKSRowsLevels levels
   {
-    KSRowsDesc d{};
     const size_t kstride = static_cast<size_t>(key.np.total()) * N;
-    for (int bi = 0; bi < nb; bi++) {
-      d.kb[bi] = key.bx + digits[bi] * kstride;
-      d.ka[bi] = key.ax + digits[bi] * kstride;
-    }
+    auto fill_level = [&](int level, KSRowsLevel &lv) {
+      const Shape &sh = shapes[level];
+      const LevelMS &m = *sh.m;
+      const int nb = static_cast<int>(sh.digits.size());
+      for (int bi = 0; bi < nb; bi++) {
+        lv.kb[bi] = key.bx + sh.digits[bi] * kstride;
+        lv.ka[bi] = key.ax + sh.digits[bi] * kstride;
+      }
+      lv.beta = nb;
+      lv.rows = sh.tot;
+      lv.nq = sh.nq;
+      for (int r = 0; r < sh.tot; r++) {
+        lv.p_prod[r] = r < sh.nq ? p_prod[sh.prime_offset + r] : 0;
+        lv.key_row[r] = static_cast<int16_t>(r < sh.nq ? sh.prime_offset + r : P->L + (r - sh.nq));
+        lv.gidx[r] = static_cast<uint8_t>(sh.g[r]);
+        lv.own_digit[r] = -1;
+        lv.drop_idx[r] = -1;
+        for (int bi = 0; bi < nb; bi++)
+          if (r >= m.dig_s[sh.digits[bi]] && r < m.dig_e[sh.digits[bi]]) lv.own_digit[r] = static_cast<int8_t>(bi);
+      }
+      if (!keep_ext)
+        for (int i = 0; i < sh.pl.src_len; i++) lv.drop_idx[sh.pl.srows[i]] = static_cast<int8_t>(i);
+    };
+    KSRowsDesc d{};
     d.tw = d_tw;
     d.itw = d_itw;
-    d.beta = nb;
-    d.rows = tot;
-    d.nq = nq;
-    d.mode = in[0].mode;
-    for (int r = 0; r < tot; r++) {
-      d.q[r] = P->primes[g[r]];
-      d.qinv[r] = P->qinv[g[r]];
-      d.p_prod[r] = r < nq ? p_prod[prime_offset + r] : 0;
-      d.key_row[r] = static_cast<int16_t>(r < nq ? prime_offset + r : P->L + (r - nq));
-      d.gidx[r] = static_cast<uint8_t>(g[r]);
-      d.own_digit[r] = -1;
-      d.drop_idx[r] = -1;
-      for (int bi = 0; bi < nb; bi++)
-        if (r >= m.dig_s[digits[bi]] && r < m.dig_e[digits[bi]]) d.own_digit[r] = static_cast<int8_t>(bi);
-    }
-    if (!keep_ext)
-      for (int i = 0; i < pl.src_len; i++) d.drop_idx[pl.srows[i]] = static_cast<int8_t>(i);
+    d.primes = d_primes;
+    d.qinvs = d_qinv;
+    d.mode = mode;
+    std::map<int, int> lv_of;  // level -> entry of d.lv in the launch being built
     nl = 0;
     t0 = timer_mark();
-    for (int c0 = 0; c0 < count; c0 += kMaxKSRowsCts) {
-      d.count = std::min(kMaxKSRowsCts, count - c0);
-      for (int c = 0; c < d.count; c++) {
-        const KSIn &x = in[c0 + c];
-        CHD_CHECK(x.mode == d.mode, kErrInvalidArg, "key switch: mixed modes in one batch");
-        KSRowsCt &k = d.ct[c];
-        for (int bi = 0; bi < nb; bi++) k.mu[bi] = MU(c0 + c, bi);
-        k.b1 = x.b1;
-        k.a1 = x.a1;
-        k.b2 = x.b2;
-        k.a2 = x.a2;
-        if (keep_ext) {
-          k.acc_b = x.out_b;
-          k.acc_a = x.out_a;
-        } else {
-          k.acc_b = acc + static_cast<size_t>(c0 + c) * 2 * tot * N;
-          k.acc_a = k.acc_b + static_cast<size_t>(tot) * N;
-          k.drop_b = drop + static_cast<size_t>(c0 + c) * 2 * pl.src_len * N;
-          k.drop_a = k.drop_b + static_cast<size_t>(pl.src_len) * N;
-        }
-      }
+    auto flush = [&]() {
+      if (d.count == 0) return;
       launch_ks_rows(d, P->log_n, stream);
       nl++;
+      d.count = d.nlv = d.max_rows = 0;
+      lv_of.clear();
+    };
+    for (int c = 0; c < count; c++) {
+      const int level = levels[c];
+      if (d.count == kMaxKSRowsCts || (!lv_of.count(level) && d.nlv == kMaxKSRowsLevels)) flush();
+      auto it = lv_of.find(level);
+      if (it == lv_of.end()) {
+        KSRowsLevel &lv = d.lv[d.nlv];
+        lv = KSRowsLevel{};
+        fill_level(level, lv);
+        d.max_rows = std::max(d.max_rows, lv.rows);
+        it = lv_of.emplace(level, d.nlv++).first;
+      }
+      const Shape &sh = shapes[level];
+      const KSIn &x = in[c];
+      KSRowsCt &k = d.ct[d.count++];
+      k = KSRowsCt{};
+      k.lv = it->second;
+      for (size_t bi = 0; bi < sh.digits.size(); bi++) k.mu[bi] = MU(c, static_cast<int>(bi));
+      k.b1 = x.b1;
+      k.a1 = x.a1;
+      k.b2 = x.b2;
+      k.a2 = x.a2;
+      if (keep_ext) {
+        k.acc_b = x.out_b;
+        k.acc_a = x.out_a;
+      } else {
+        k.acc_b = acc + o_acc[c] * N;
+        k.acc_a = k.acc_b + static_cast<size_t>(sh.tot) * N;
+        k.drop_b = drop + o_drop[c] * N;
+        k.drop_a = k.drop_b + static_cast<size_t>(sh.pl.src_len) * N;
+      }
     }
+    flush();
     timer_span(kKsRows, t0, nl);
   }
   if (keep_ext) return check_cuda("key switch");
   // 4. ModDown column pass per (ciphertext, part)
   {
-    MSColBatch b{};
-    b.engine = ks_engine;
-    b.err = d_err;
-    b.tw = d_tw;
-    b.itw = d_itw;
-    b.primes = d_primes;
-    b.qinvs = d_qinv;
     nl = 0;
     t0 = timer_mark();
-    for (int c = 0; c < count; c++)
+    b.count = 0;
+    for (int c = 0; c < count; c++) {
+      const MDPlan &pl = shapes[levels[c]].pl;
       for (int p = 0; p < 2; p++) {
         MSColJob &j = b.jobs[b.count++];
-        j.src = drop + (static_cast<size_t>(c) * 2 + p) * pl.src_len * N;
+        j.src = drop + (o_drop[c] + static_cast<size_t>(p) * pl.src_len) * N;
         j.dst = p == 0 ? in[c].out_b : in[c].out_a;
         j.table = pl.table;
         j.K = pl.src_len;
@@ -1337,14 +1397,17 @@ Status Context::key_switch_fused(int level, int count, const KSIn *in, const Dev
           b.count = 0;
         }
       }
+    }
     launch_modswitch_cols(b, P->log_n, stream);
     timer_span(kKsModDownCols, t0, nl + (b.count > 0));
   }
   // 5. NTT row phase with the ModDown epilogue (src2 = kept accumulators)
   rows.clear();
-  for (int c = 0; c < count; c++)
+  for (int c = 0; c < count; c++) {
+    const Shape &sh = shapes[levels[c]];
+    const MDPlan &pl = sh.pl;
     for (int p = 0; p < 2; p++) {
-      const uint32_t *src = acc + (static_cast<size_t>(c) * 2 + p) * tot * N;
+      const uint32_t *src = acc + (o_acc[c] + static_cast<size_t>(p) * sh.tot) * N;
       uint32_t *dst = p == 0 ? in[c].out_b : in[c].out_a;
       for (int y = 0; y < pl.dst_len; y++) {
         RowDesc d{};
@@ -1364,6 +1427,7 @@ Status Context::key_switch_fused(int level, int count, const KSIn *in, const Dev
         rows.push_back(d);
       }
     }
+  }
   nl = 0;
   t0 = timer_mark();
   for_row_batches(rows, [&](const RowBatch &rb) {
@@ -1647,8 +1711,10 @@ Status Context::hmult(DeviceCt &res, const DeviceCt &a, const DeviceCt &b, const
 Status Context::hmult_batch(int count, DeviceCt *const *res, const DeviceCt *const *a, const DeviceCt *const *b,
                             const DeviceEvk &key, bool rescale) {
   // Batched Context::HMult: every stage (tensor, ModUp, key MAC, merged
-  // ModDown+Rescale) runs once for the whole batch.  Ciphertexts must share
-  // a level and must not alias each other's results.
+  // ModDown+Rescale) runs once for the whole batch.  At N = 2^16 the pairs
+  // may sit at different levels (one pipeline over all of them); below it a
+  // mixed batch runs one pipeline per level.  Results must not alias other
+  // pairs' operands (such a batch runs one pair at a time).
   if (count <= 0) return kOk;
   bool uniform = true, aliased = false;
   for (int i = 0; i < count; i++) {
@@ -1661,6 +1727,27 @@ Status Context::hmult_batch(int count, DeviceCt *const *res, const DeviceCt *con
   if (aliased) {  // results overwrite operands of other pairs: one by one
     for (int i = 0; i < count; i++) CHD_TRY(hmult(*res[i], *a[i], *b[i], key, rescale));
     return kOk;
+  }
+  if (P->log_n == 16) {
+    std::vector<KSIn> in(count);
+    std::vector<int> levels(count);
+    for (int c = 0; c < count; c++) {
+      const int level = level_of(*P, *a[c]);
+      CHD_CHECK(level >= 0, kErrInvalidLevel, "HMult: invalid level");
+      CHD_CHECK(!rescale || level >= 1, kErrInvalidLevel, "Not enough q primes to rescale");
+      CHD_CHECK(a[c]->np.q() + P->alpha <= 64, kErrUnsupported, "HMult: more than 64 primes in the extended basis");
+      levels[c] = level;
+      const double sa = a[c]->scale, sb = b[c]->scale;
+      const int slots = std::max(a[c]->num_slots, b[c]->num_slots);
+      in[c] = KSIn{0, a[c]->bx, a[c]->ax, b[c]->bx, b[c]->ax, nullptr, nullptr};
+      CHD_TRY(res[c]->reserve(P->level_np(rescale ? level - 1 : level, 0), false, P->n));
+      res[c]->scale = rescale ? sa * sb / P->rescale_prod[level] : sa * sb;
+      res[c]->num_slots = slots;
+      in[c].out_b = res[c]->bx;
+      in[c].out_a = res[c]->ax;
+    }
+    return key_switch_fused_levels(levels.data(), count, in.data(), key,
+                                   rescale ? MDType::kModDownRescale : MDType::kModDown);
   }
   if (!uniform) {
     // mixed levels: one batched pipeline per level, in level order
@@ -1683,21 +1770,6 @@ Status Context::hmult_batch(int count, DeviceCt *const *res, const DeviceCt *con
   CHD_CHECK(!rescale || level >= 1, kErrInvalidLevel, "Not enough q primes to rescale");
   const int n = P->n, nq = a[0]->np.q(), tot = nq + P->alpha;
   CHD_CHECK(tot <= 64, kErrUnsupported, "HMult: more than 64 primes in the extended basis");
-  if (P->log_n == 16) {
-    std::vector<KSIn> in(count);
-    NP out_np = P->level_np(rescale ? level - 1 : level, 0);
-    for (int c = 0; c < count; c++) {
-      const double sa = a[c]->scale, sb = b[c]->scale;
-      const int slots = std::max(a[c]->num_slots, b[c]->num_slots);
-      in[c] = KSIn{0, a[c]->bx, a[c]->ax, b[c]->bx, b[c]->ax, nullptr, nullptr};
-      CHD_TRY(res[c]->reserve(out_np, false, n));
-      res[c]->scale = rescale ? sa * sb / P->rescale_prod[level] : sa * sb;
-      res[c]->num_slots = slots;
-      in[c].out_b = res[c]->bx;
-      in[c].out_a = res[c]->ax;
-    }
-    return key_switch_fused(level, count, in.data(), key, rescale ? MDType::kModDownRescale : MDType::kModDown);
-  }
   ArenaScope scope(arena);
   const size_t qw = static_cast<size_t>(nq) * n, tw_ = static_cast<size_t>(tot) * n;
   uint32_t *d = static_cast<uint32_t *>(arena.alloc(static_cast<size_t>(count) * 3 * qw * 4));
@@ -1972,6 +2044,34 @@ Status Context::moddown_ct(DeviceCt &res, const DeviceCt &a) {
   CHD_TRY(moddown(level, MDType::kModDown, srcs, dsts, 2));
   res.scale = sc;
   res.num_slots = slots;
+  return kOk;
+}
+
+Status Context::moddown_batch(int count, DeviceCt *const *res, const DeviceCt *const *a) {
+  // ModDown of several ciphertexts at one level through one pipeline: the
+  // 2 * count polynomials share the column pass and the row launches
+  CHD_CHECK(count >= 1, kErrInvalidArg, "ModDown: empty batch");
+  const NP np = a[0]->np;
+  CHD_CHECK(np.aux == P->alpha, kErrShape, "ModDown: input must carry all aux primes");
+  const int level = P->np_to_level(NP{np.main, np.ter, 0});
+  CHD_CHECK(level >= 0, kErrInvalidLevel, "ModDown: invalid level");
+  std::vector<const uint32_t *> srcs;
+  std::vector<uint32_t *> dsts;
+  for (int c = 0; c < count; c++) {
+    CHD_CHECK(a[c]->np == np && !a[c]->has_rx, kErrShape, "ModDown: batch members at different levels");
+    for (int d = 0; d < count; d++)
+      CHD_CHECK(res[c] != a[d], kErrInvalidArg, "ModDown does not support in-place operation");
+    CHD_TRY(res[c]->reserve(NP{np.main, np.ter, 0}, false, P->n));
+    srcs.push_back(a[c]->bx);
+    srcs.push_back(a[c]->ax);
+    dsts.push_back(res[c]->bx);
+    dsts.push_back(res[c]->ax);
+  }
+  CHD_TRY(moddown(level, MDType::kModDown, srcs.data(), dsts.data(), 2 * count));
+  for (int c = 0; c < count; c++) {
+    res[c]->scale = a[c]->scale;
+    res[c]->num_slots = a[c]->num_slots;
+  }
   return kOk;
 }
 

@@ -379,6 +379,10 @@ class Context {
   // bare inner product sum_i ModUp(a1)_i (.) key_i).
   Status key_switch_fused(int level, int count, const KSIn *in, const DeviceEvk &key, MDType type,
                           bool keep_ext = false);
+  // The same pipeline with ciphertext c at levels[c]: every stage is one
+  // launch (or a few, by the per-launch job limits) over all levels.
+  Status key_switch_fused_levels(const int *levels, int count, const KSIn *in, const DeviceEvk &key, MDType type,
+                                 bool keep_ext = false);
   // ModDown family on npoly polys
   Status moddown(int level, MDType type, const uint32_t *const *src, uint32_t *const *dst, int npoly);
   Status bconv(const int32_t *xt, int K, const int32_t *table, const int *dst_gidx, int M, uint32_t *out);
@@ -418,6 +422,7 @@ class Context {
                               const DeviceEvk *const *keys, DeviceCt *const *const *out);
   // ModDown of a Q u P ciphertext back to Q
   Status moddown_ct(DeviceCt &res, const DeviceCt &a);
+  Status moddown_batch(int count, DeviceCt *const *res, const DeviceCt *const *a);
 
   // ---- bootstrapping building blocks (boot.cu) ----
   // Encoder::Encode (Encode.cpp:23-41, 84-107, 135-190): msg_len complex

@@ -185,19 +185,27 @@ struct KSRowsCt {
   const uint32_t *b1, *a1, *b2, *a2; // inputs [nq][N]
   uint32_t *acc_b, *acc_a;           // kept primes: evaluation-domain accumulators [tot][N]
   uint32_t *drop_b, *drop_a;         // dropped primes: INTT row-phase output [ndrop][N]
+  int lv;                            // entry of KSRowsDesc::lv describing its level
 };
-constexpr int kMaxKSRowsCts = 16;
-struct KSRowsDesc {
+// Row tables of one level of the extended basis Q u P (row j of a
+// ciphertext at that level); several levels can share one launch.
+struct KSRowsLevel {
   const uint32_t *kb[8], *ka[8];     // key digit pointers (row 0 of the key basis)
-  const uint2 *tw, *itw;
-  int beta, rows, nq, count, mode;
-  uint32_t q[64];
-  int32_t qinv[64];
-  uint32_t p_prod[64];
+  int beta, rows, nq;
   int16_t key_row[64];
   uint8_t gidx[64];
   int8_t own_digit[64];              // digit owning row j (q primes), else -1
   int8_t drop_idx[64];               // row of j in the drop buffers, else -1
+  uint32_t p_prod[64];               // Montgomery P mod q_j (q rows)
+};
+constexpr int kMaxKSRowsCts = 16;
+constexpr int kMaxKSRowsLevels = 8;
+struct KSRowsDesc {
+  const uint2 *tw, *itw;
+  const uint32_t *primes;            // [nprimes] by global index
+  const int32_t *qinvs;
+  int count, mode, nlv, max_rows;
+  KSRowsLevel lv[kMaxKSRowsLevels];
   KSRowsCt ct[kMaxKSRowsCts];
 };
 void launch_ks_rows(const KSRowsDesc &d, int log_n, cudaStream_t s);

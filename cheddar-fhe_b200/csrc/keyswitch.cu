@@ -10,7 +10,9 @@
 //   * and, for the primes that ModDown drops, the INTT row phase
 //     (NTT.cu:973-1128, INTTForModDown).
 // One CTA owns 4 rows of one prime of the extended basis Q u P for one
-// ciphertext; it reads each input row once and writes either the
+// ciphertext (each ciphertext names the row tables of its own level, so
+// ciphertexts at different levels share a launch); it reads each input row
+// once and writes either the
 // evaluation-domain accumulator (kept primes, consumed by the ModDown
 // epilogue) or the INTT row-phase output (dropped primes, consumed by the
 // ModDown column pass).
@@ -23,21 +25,23 @@ namespace {
 
 __global__ void __launch_bounds__(256, 3) k_ks_rows(const __grid_constant__ KSRowsDesc d) {
   __shared__ uint32_t sm[4][512];
-  // grid (count, 32, rows): the ciphertexts sharing one key row are
+  // grid (count, 32, max_rows): the ciphertexts sharing one key row are
   // neighbours in launch order, so the key row comes from HBM once
   const int j = blockIdx.z;
   const KSRowsCt &c = d.ct[blockIdx.x];
-  const uint32_t q = d.q[j];
-  const int32_t qi = d.qinv[j];
-  const int g = d.gidx[j];
+  const KSRowsLevel &L = d.lv[c.lv];
+  if (j >= L.rows) return;  // a ciphertext below the launch's largest level
+  const int g = L.gidx[j];
+  const uint32_t q = __ldg(d.primes + g);
+  const int32_t qi = __ldg(d.qinvs + g);
   const uint2 *tw = d.tw + (static_cast<size_t>(g) << 16);
   const int t = threadIdx.x & 63, rl = threadIdx.x >> 6;
   const int r = blockIdx.y * 4 + rl;
   uint32_t *srow = sm[rl];
   const size_t off = static_cast<size_t>(j) * 65536 + r * 512 + 8 * t;       // accumulator-row offset
-  const size_t koff = static_cast<size_t>(d.key_row[j]) * 65536 + r * 512 + 8 * t;
+  const size_t koff = static_cast<size_t>(L.key_row[j]) * 65536 + r * 512 + 8 * t;
   const size_t qoff = off;  // input rows share the accumulator row index for q primes
-  const bool is_q = j < d.nq;
+  const bool is_q = j < L.nq;
   const int mode = d.mode;
   uint32_t a1[8], a2[8];
   if (is_q) {
@@ -47,9 +51,9 @@ __global__ void __launch_bounds__(256, 3) k_ks_rows(const __grid_constant__ KSRo
   uint32_t sb[8], sa[8];
 #pragma unroll
   for (int k = 0; k < 8; k++) sb[k] = sa[k] = 0;
-  for (int i = 0; i < d.beta; i++) {
+  for (int i = 0; i < L.beta; i++) {
     uint32_t v[8];
-    if (d.own_digit[j] == i) {
+    if (L.own_digit[j] == i) {
       // own primes of the digit: the ModUp value is the key-switched input
 #pragma unroll
       for (int k = 0; k < 8; k++) v[k] = mode == 0 ? mont_mul(a1[k], a2[k], q, qi) : (mode == 1 ? a1[k] : a2[k]);
@@ -63,8 +67,8 @@ __global__ void __launch_bounds__(256, 3) k_ks_rows(const __grid_constant__ KSRo
       row_sync(1 + rl);
     }
     uint32_t kb[8], ka[8];
-    ld8(d.kb[i] + koff, kb);
-    ld8(d.ka[i] + koff, ka);
+    ld8(L.kb[i] + koff, kb);
+    ld8(L.ka[i] + koff, ka);
 #pragma unroll
     for (int k = 0; k < 8; k++) {
       sb[k] = add_mod(sb[k], mont_mul(v[k], kb[k], q, qi), q);
@@ -74,7 +78,7 @@ __global__ void __launch_bounds__(256, 3) k_ks_rows(const __grid_constant__ KSRo
   if (is_q && c.b1 != nullptr) {
     // P * (d0, d1): HMult d0 = b1 b2, d1 = b1 a2 + a1 b2; MultKey d0 = bx;
     // Relinearize d0 = bx, d1 = ax.  Without b1: the bare inner product.
-    const uint32_t pp = d.p_prod[j];
+    const uint32_t pp = L.p_prod[j];
     uint32_t b1[8];
     ld8(c.b1 + qoff, b1);
     if (mode == 0) {
@@ -95,7 +99,7 @@ __global__ void __launch_bounds__(256, 3) k_ks_rows(const __grid_constant__ KSRo
       }
     }
   }
-  const int di = d.drop_idx[j];
+  const int di = L.drop_idx[j];
   if (di < 0) {
     st8(c.acc_b + off, sb);
     st8(c.acc_a + off, sa);
@@ -118,8 +122,8 @@ __global__ void __launch_bounds__(256, 3) k_ks_rows(const __grid_constant__ KSRo
 }  // namespace
 
 void launch_ks_rows(const KSRowsDesc &d, int log_n, cudaStream_t s) {
-  if (d.count <= 0 || d.rows <= 0 || log_n != 16) return;
-  k_ks_rows<<<dim3(d.count, 32, d.rows), 256, 0, s>>>(d);
+  if (d.count <= 0 || d.max_rows <= 0 || log_n != 16) return;
+  k_ks_rows<<<dim3(d.count, 32, d.max_rows), 256, 0, s>>>(d);
 }
 
 }  // namespace chd

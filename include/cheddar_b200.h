@@ -227,6 +227,12 @@ int chd_hoisted_rotate(chd_context *ctx, const chd_ciphertext *a, int count, con
                        const chd_evk *const *rot_keys, chd_ciphertext *const *out);
 /* ModSwitchHandler::ModDown of an extended-basis ciphertext (ModSwitch.cu:511-527) */
 int chd_moddown(chd_context *ctx, chd_ciphertext *res, const chd_ciphertext *a);
+/* ModDown of `count` ciphertexts at one level (Q u P -> Q), e.g. the
+ * rotations of one hoisted set, through one fused pipeline: the same
+ * residues as chd_moddown on each (no reference counterpart; the reference
+ * keeps hoisted rotations in Q u P and reduces them one accumulation at a
+ * time, Hoist.cu:695-975). */
+int chd_moddown_batch(chd_context *ctx, int count, chd_ciphertext *const *res, const chd_ciphertext *const *a);
 
 /* ---- raw kernels on device buffers (parity entry points) -------------------- */
 /* NTTHandler::NTT / INTT (include/core/NTT.h:55-62): count consecutive

@@ -1,5 +1,6 @@
-"""Mixed-level HMult batches (one batched pipeline per level) and CUDA-graph
-capture of library calls: a captured batch replayed on refreshed inputs and
+"""Mixed-level HMult batches (at N = 2^16 one pipeline over every level: a
+launch per stage, the key-switch row pass taking several levels per launch)
+and CUDA-graph capture of library calls: a captured batch replayed on refreshed inputs and
 a captured bootstrap replayed give the oracle's residues, bit for bit."""
 import numpy as np
 import pytest
@@ -25,6 +26,29 @@ def test_mixed_level_batch(cuda_ok):
     gb = [g.import_ct(lvl, b) for lvl, _, b in pairs]
     outs = g.HMultBatch(ga, gb, key, rescale=True)
     for r, ref in zip(outs, _oracle_hmults(o, (kb, ka), pairs)):
+        parts = r.numpy()
+        assert np.array_equal(parts[0], ref[0]) and np.array_equal(parts[1], ref[1])
+
+
+def test_mixed_level_batch_beyond_launch_limits(cuda_ok):
+    # 18 pairs at 18 distinct levels: more ciphertexts than one row-pass
+    # launch takes (16) and more levels than one launch describes (8)
+    o, g = pair(KS)
+    (kb, ka), key = mult_key(KS)
+    levels = [22, 1, 3, 5, 7, 9, 11, 13, 15, 17, 19, 21, 2, 4, 6, 8, 10, 12]
+    pairs = [(lvl, uniform_parts(KS, lvl, 1300 + i), uniform_parts(KS, lvl, 1350 + i)) for i, lvl in enumerate(levels)]
+    ga = [g.import_ct(lvl, a) for lvl, a, _ in pairs]
+    gb = [g.import_ct(lvl, b) for lvl, _, b in pairs]
+    for rescale in (True, False):
+        outs = g.HMultBatch(ga, gb, key, rescale=rescale)
+        singles = [g.HMult(x, y, key, rescale=rescale) for x, y in zip(ga, gb)]
+        for r, s1, (lvl, _, _) in zip(outs, singles, pairs):
+            ri, si = r.info(), s1.info()
+            assert g.level_of(ri["num_main"], ri["num_ter"]) == (lvl - 1 if rescale else lvl)
+            assert ri == si
+            for x, y in zip(r.numpy(), s1.numpy()):
+                assert np.array_equal(x, y)
+    for r, ref in zip(g.HMultBatch(ga[:6], gb[:6], key, rescale=True), _oracle_hmults(o, (kb, ka), pairs[:6])):
         parts = r.numpy()
         assert np.array_equal(parts[0], ref[0]) and np.array_equal(parts[1], ref[1])
 

@@ -286,3 +286,21 @@ def test_terminal_primes_n16_every_level_both_engines(cuda_ok):
             with engine(g, e):
                 _eq(g.HMult(g.import_ct(lvl, a), g.import_ct(lvl, b), key, rescale=True), ref_m)
                 _eq(g.HRot(g.import_ct(lvl, a), rkey, 3), ref_r)
+
+
+def test_moddown_batch_equals_single(cuda_ok):
+    """ModDownBatch of the 30 hoisted rotations of one ciphertext (one fused
+    pipeline for all 60 polynomials) equals ModDown of each, and the oracle's
+    HRot."""
+    o, g = pair(KS)
+    lvl = o.max_level
+    half = o.n // 2
+    offs = sorted({(s * (1 << k)) % half for k in range(15) for s in (1, -1)} | {1, 2, 3, 4})
+    a = uniform_parts(KS, lvl, 950)
+    keys = [rot_key(KS, r) for r in offs]
+    ga = g.import_ct(lvl, a)
+    qp = g.HoistedRotate(ga, [k[1] for k in keys], offs)
+    batch = g.ModDownBatch(qp)
+    for i in (0, 7, 29):
+        _eq(batch[i], g.ModDown(qp[i]).numpy())
+    _eq(batch[3], o.hrot(lvl, a, keys[3][0], offs[3]))
