@@ -20,6 +20,7 @@ PARAM_DIR = os.path.join(_HERE, "params")
 CHD_MODDOWN, CHD_RESCALE, CHD_MODDOWN_RESCALE = 0, 1, 2
 BCONV_CUDA_CORE, BCONV_TENSOR_CORE = 0, 1   # chd_bconv_batch engines
 BCONV_AUTO = 2                                # Context.ks_engine only: autotuned per launch shape
+BCONV_TENSOR_CORE_WIDE = 3                    # Context.ks_engine only: tensor cores, 256-thread tiles (K <= 12)
 
 # stages of the fused N = 2^16 key switch (chd_stage_times), in launch order
 KS_STAGE_NAMES = ("modup_inv_rows", "modup_cols", "ks_rows", "moddown_cols", "fwd_rows_epilogue")

@@ -358,9 +358,11 @@ int chd_mult_unsafe_plain(chd_context *ctx, chd_ciphertext *res, const chd_ciphe
 
 int chd_set_ks_engine(chd_context *ctx, int engine) try {
   CHD_CTX(ctx);
-  if (engine != CHD_BCONV_CUDA_CORE && engine != CHD_BCONV_TENSOR_CORE && engine != CHD_BCONV_AUTO)
+  if (engine != CHD_BCONV_CUDA_CORE && engine != CHD_BCONV_TENSOR_CORE && engine != CHD_BCONV_AUTO &&
+      engine != CHD_BCONV_TENSOR_CORE_WIDE)
     return fail(CHD_ERR_INVALID_ARG,
-                "chd_set_ks_engine: engine must be CHD_BCONV_CUDA_CORE, CHD_BCONV_TENSOR_CORE or CHD_BCONV_AUTO");
+                "chd_set_ks_engine: engine must be CHD_BCONV_CUDA_CORE, CHD_BCONV_TENSOR_CORE, "
+                "CHD_BCONV_TENSOR_CORE_WIDE or CHD_BCONV_AUTO");
   ctx->c->ks_engine = engine;
   return CHD_OK;
 } catch (const std::exception &e) {

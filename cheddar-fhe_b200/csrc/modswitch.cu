@@ -232,7 +232,11 @@ size_t modswitch_cols_smem(int kmax) { return (static_cast<size_t>(kExRows) * kT
 namespace {
 
 void launch_engine(const MSColBatch &b, int engine, int max_k, cudaStream_t s) {
-  if (engine == 1) {
+  if (engine == 3 && modswitch_cols_tc8_supports(max_k)) {
+    launch_modswitch_cols_tc8(b, max_k, s);
+    return;
+  }
+  if (engine == 1 || engine == 3) {
     launch_modswitch_cols_tc(b, max_k, s);
     return;
   }
@@ -310,12 +314,14 @@ int heuristic_groups(const MSColBatch &b, int max_m) {
   return groups > by_m ? by_m : groups;
 }
 
-// Autotuning (engine 2, CHD_BCONV_AUTO): which engine and which target split
-// are fastest depends on the launch (the CUDA-core pass wins when a launch
-// holds one ciphertext's few jobs, the tensor-core pass on batches; small
-// launches gain from the split).  The first launch of a shape (device,
-// largest K, jobs, largest M) outside a stream capture times every
-// candidate (engine x split in {1, 2, 4, heuristic}) three times after a
+// Autotuning (engine 2, CHD_BCONV_AUTO): which engine and tile and which
+// target split are fastest depends on the launch (the CUDA-core pass wins
+// when a launch holds one ciphertext's few jobs, the tensor-core passes on
+// batches; small launches gain from the split).  The first launch of a shape
+// (device, largest K, jobs, largest M) outside a stream capture times every
+// candidate (engine in {CUDA cores, tensor cores with 128-thread tiles,
+// tensor cores with 256-thread tiles for K <= 12} x split in
+// {1, 2, 4, heuristic}) three times after a
 // warm-up, interleaved, with CUDA events (a host synchronisation, once per
 // shape), keeps the fastest launch and caches the choice for the process.
 // Every candidate writes identical residues, so the tuning launches leave
@@ -346,12 +352,12 @@ bool tune_and_launch(const MSColBatch &b, int max_k, int max_m, cudaStream_t s, 
   if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return false;
   std::vector<Choice> cand;
   const int by_m = max_m / 4 > 1 ? max_m / 4 : 1;
-  for (int e = 0; e < 2; e++)
+  for (int e : {0, 1, 3})
     for (int g : {1, 2, 4, hg})
       if (g <= by_m) {
         bool seen = false;
         for (const Choice &c : cand) seen |= c.engine == e && c.groups == g;
-        if (!seen) cand.push_back(Choice{e, g});
+        if (!seen && (e != 3 || modswitch_cols_tc8_supports(max_k))) cand.push_back(Choice{e, g});
       }
   constexpr int kRounds = 3;
   const int nc = static_cast<int>(cand.size());

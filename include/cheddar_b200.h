@@ -417,18 +417,24 @@ void chd_graph_destroy(chd_graph *g);
 #define CHD_BCONV_CUDA_CORE 0
 #define CHD_BCONV_TENSOR_CORE 1
 #define CHD_BCONV_AUTO 2 /* chd_set_ks_engine only: autotuned per launch shape */
+/* chd_set_ks_engine only: the tensor-core column pass on 256-thread tiles
+ * (8 coefficients per thread, twice the warps per SM) for ModUp / ModDown
+ * with at most 12 sources; larger ones use CHD_BCONV_TENSOR_CORE */
+#define CHD_BCONV_TENSOR_CORE_WIDE 3
 int chd_bconv_batch(chd_context *ctx, int engine, int npoly, const int32_t *xt_dev, const int *src_gidx, int K,
                     const int *dst_gidx, int M, uint32_t *out_dev);
 
 /* Engine of the base conversion inside every ModUp / ModDown of the fused
  * key-switching, rescaling and bootstrapping paths (HMult, relinearize,
  * rotations, hoisted rotations, linear transforms, ModDown epilogues):
- * CHD_BCONV_CUDA_CORE (int64 multiply-adds) or CHD_BCONV_TENSOR_CORE (the
+ * CHD_BCONV_CUDA_CORE (int64 multiply-adds), CHD_BCONV_TENSOR_CORE (the
  * column pass issues INT8 byte-limb MMAs on the tcgen05 tensor cores with
- * int32 accumulation in TMEM).  Both give bit-identical residues.
+ * int32 accumulation in TMEM, 128-thread tiles) or
+ * CHD_BCONV_TENSOR_CORE_WIDE (the same on 256-thread tiles).  All give
+ * bit-identical residues.
  * CHD_BCONV_AUTO autotunes: the first column pass of each launch shape
- * (device, sources, jobs, targets) outside a stream capture times both
- * engines with each split of the targets over 1, 2, 4 or the heuristic
+ * (device, sources, jobs, targets) outside a stream capture times the
+ * three with each split of the targets over 1, 2, 4 or the heuristic
  * number of CTAs per column tile (one host synchronisation per shape and
  * process) and keeps the fastest; an untuned shape met during a capture
  * uses the tensor cores with the heuristic split.  No reference counterpart (the reference has one CUDA-core

@@ -244,6 +244,30 @@ def case_keyswitch():
     return out
 
 
+def case_mixed_batch():
+    """One HMultBatch call over the reference's encryptions at ten different
+    levels of the L = 24, alpha = 8 set (this library runs them as one fused
+    pipeline, the row pass taking several levels per launch) against one
+    Context::HMult call of the reference per pair (Context.cpp:862-871),
+    with and without rescale."""
+    t = Trio(load("keyswitch_l24_a8.json"))
+    g, ref = t.g, t.ref
+    _, mk = t.key(ref.MULT)
+    levels = [22, 3, 17, 9, 1, 20, 12, 5, 14, 7]
+    ras, rbs, gas, gbs = [], [], [], []
+    for i, lvl in enumerate(levels):
+        ra, rb = ref.encrypt(lvl, t.message(300 + i)), ref.encrypt(lvl, t.message(400 + i))
+        ras.append(ra)
+        rbs.append(rb)
+        gas.append(t.ct(ra)[1])
+        gbs.append(t.ct(rb)[1])
+    for rescale in (True, False):
+        outs = g.HMultBatch(gas, gbs, mk, rescale=rescale)
+        for lvl, ra, rb, r in zip(levels, ras, rbs, outs):
+            eq(f"HMultBatch level {lvl} rescale {rescale}", r.numpy(), ref.HMult(ra, rb, rescale=rescale).numpy())
+    return {"levels": levels, "pairs": len(levels)}
+
+
 def case_hoisted():
     """Hoisted rotations: the reference's HoistHandler::EvaluateBabyStep
     (Hoist.cu:578-691; one ModUp, every rotation's key product and

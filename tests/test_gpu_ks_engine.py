@@ -1,7 +1,7 @@
-"""The tensor-core engine of the fused ModUp / ModDown column pass (base
-conversion as INT8 byte-limb MMAs on tcgen05, int32 accumulation in TMEM)
-gives the same residues as the oracle and as the CUDA-core engine, bit for
-bit: raw ModUp / ModDown / Rescale, HMult with relinearisation and rescale,
+"""The tensor-core engines of the fused ModUp / ModDown column pass (base
+conversion as INT8 byte-limb MMAs on tcgen05, int32 accumulation in TMEM;
+128-thread tiles, and 256-thread tiles for up to 12 sources) give the same
+residues as the oracle and as the CUDA-core engine, bit for bit: raw ModUp / ModDown / Rescale, HMult with relinearisation and rescale,
 batches, rotations, hoisted rotations, and a full-slot bootstrap at
 N = 2^16 (every ModUp / ModDown / rescale of the bootstrapping program)."""
 import contextlib
@@ -17,6 +17,8 @@ from gpu_common import mult_key, pair, rot_key, uniform_parts
 
 pytestmark = pytest.mark.gpu
 KS = "keyswitch_l24_a8.json"
+TC_ENGINES = [chd.BCONV_TENSOR_CORE, chd.BCONV_TENSOR_CORE_WIDE]
+ALL_ENGINES = (chd.BCONV_CUDA_CORE, chd.BCONV_TENSOR_CORE, chd.BCONV_TENSOR_CORE_WIDE)
 
 
 @contextlib.contextmanager
@@ -52,12 +54,15 @@ def test_engine_setting(cuda_ok):
         with pytest.raises(chd.CheddarError):
             g.ks_engine = 7
         assert g.ks_engine == chd.BCONV_TENSOR_CORE
+    with engine(g, chd.BCONV_TENSOR_CORE_WIDE):
+        assert g.ks_engine == chd.BCONV_TENSOR_CORE_WIDE
 
 
+@pytest.mark.parametrize("eng", TC_ENGINES)
 @pytest.mark.parametrize("level", [22, 21, 15, 6, 0])
-def test_modup_moddown_tc(cuda_ok, level):
+def test_modup_moddown_tc(cuda_ok, level, eng):
     o, g = pair(KS)
-    with engine(g, chd.BCONV_TENSOR_CORE):
+    with engine(g, eng):
         x = o.uniform(30 + level, level)
         mu = torch.zeros((o.beta(level), o.num_q(level) + o.alpha, o.n), dtype=torch.int32, device="cuda")
         g.modup_raw(level, _dev(x), mu)
@@ -80,13 +85,14 @@ def test_modup_moddown_tc(cuda_ok, level):
             assert np.array_equal(_host(out1), o.moddown_rescale(level, xa[0]))
 
 
+@pytest.mark.parametrize("eng", TC_ENGINES)
 @pytest.mark.parametrize("level,rescale", [(22, True), (22, False), (13, True), (1, True)])
-def test_hmult_tc(cuda_ok, level, rescale):
+def test_hmult_tc(cuda_ok, level, rescale, eng):
     o, g = pair(KS)
     (kb, ka), key = mult_key(KS)
     a = uniform_parts(KS, level, 100 + level)
     b = uniform_parts(KS, level, 200 + level)
-    with engine(g, chd.BCONV_TENSOR_CORE):
+    with engine(g, eng):
         res = g.HMult(g.import_ct(level, a), g.import_ct(level, b), key, rescale=rescale)
         _eq(res, o.hmult(level, a, b, (kb, ka), rescale=rescale))
 
@@ -99,7 +105,7 @@ def test_hmult_batch_mixed_levels_tc(cuda_ok):
     levels = [20, 16, 9, 22, 5]
     pairs = [(uniform_parts(KS, l, 300 + i), uniform_parts(KS, l, 400 + i)) for i, l in enumerate(levels)]
     outs = {}
-    for e in (chd.BCONV_CUDA_CORE, chd.BCONV_TENSOR_CORE):
+    for e in ALL_ENGINES:
         with engine(g, e):
             ga = [g.import_ct(l, a) for l, (a, _) in zip(levels, pairs)]
             gb = [g.import_ct(l, b) for l, (_, b) in zip(levels, pairs)]
@@ -111,23 +117,25 @@ def test_hmult_batch_mixed_levels_tc(cuda_ok):
                 assert np.array_equal(x, y)
 
 
+@pytest.mark.parametrize("eng", TC_ENGINES)
 @pytest.mark.parametrize("rot", [1, 1234, 32767])
-def test_hrot_tc(cuda_ok, rot):
+def test_hrot_tc(cuda_ok, rot, eng):
     o, g = pair(KS)
     (kb, ka), key = rot_key(KS, rot)
     lvl = 21
     a = uniform_parts(KS, lvl, 700)
-    with engine(g, chd.BCONV_TENSOR_CORE):
+    with engine(g, eng):
         _eq(g.HRot(g.import_ct(lvl, a), key, rot), o.hrot(lvl, a, (kb, ka), rot))
 
 
-def test_hoisted_rotations_tc(cuda_ok):
+@pytest.mark.parametrize("eng", TC_ENGINES)
+def test_hoisted_rotations_tc(cuda_ok, eng):
     o, g = pair(KS)
     lvl = o.max_level
     offs = [1, 2, 3, 4, 16, 1024, 32767]
     a = uniform_parts(KS, lvl, 900)
     keys = [rot_key(KS, r) for r in offs]
-    with engine(g, chd.BCONV_TENSOR_CORE):
+    with engine(g, eng):
         ga = g.import_ct(lvl, a)
         outs = g.HoistedRotate(ga, [k[1] for k in keys], offs)
         hb, ha = o.hoisted_rotate(lvl, a, [k[0] for k in keys], offs)
@@ -176,18 +184,19 @@ def test_bootstrap_n16_engines_equal(cuda_ok):
     ct = ctx.import_ct(0, [uniform(g0), uniform(g0)], on_device=True, scale=ctx.scale(0))
     torch.cuda.synchronize()
     res = {}
-    for e in (chd.BCONV_CUDA_CORE, chd.BCONV_TENSOR_CORE):
+    for e in ALL_ENGINES:
         with engine(ctx, e):
             res[e] = bc.Boot(ct, keys).numpy()
     ctx.synchronize()
-    for x, y in zip(res[chd.BCONV_CUDA_CORE], res[chd.BCONV_TENSOR_CORE]):
-        assert np.array_equal(x, y)
+    for e in (chd.BCONV_TENSOR_CORE, chd.BCONV_TENSOR_CORE_WIDE):
+        for x, y in zip(res[chd.BCONV_CUDA_CORE], res[e]):
+            assert np.array_equal(x, y)
 
 
 BOOT = "boot_l34_a12.json"
 
 
-@pytest.mark.parametrize("eng", ["cuda", "tensor"])
+@pytest.mark.parametrize("eng", ["cuda", "tensor", "tensor_wide"])
 @pytest.mark.parametrize("level", [34, 30, 22, 10])
 def test_boot_params_column_passes(cuda_ok, eng, level):
     """Bootstrapping parameter set at N = 2^16 (alpha = 12): ModUp digits of
@@ -196,7 +205,8 @@ def test_boot_params_column_passes(cuda_ok, eng, level):
     levels above 24), whose last sources are held in registers; every
     engine equals the oracle."""
     o, g = pair(BOOT)
-    e = chd.BCONV_TENSOR_CORE if eng == "tensor" else chd.BCONV_CUDA_CORE
+    e = {"cuda": chd.BCONV_CUDA_CORE, "tensor": chd.BCONV_TENSOR_CORE,
+         "tensor_wide": chd.BCONV_TENSOR_CORE_WIDE}[eng]
     with engine(g, e):
         x = o.uniform(130 + level, level)
         mu = torch.zeros((o.beta(level), o.num_q(level) + o.alpha, o.n), dtype=torch.int32, device="cuda")
@@ -261,7 +271,7 @@ def test_hmult_and_hrot_every_level_both_engines(cuda_ok):
         b = uniform_parts(KS, lvl, 950 + lvl)
         ref_m = o.hmult(lvl, a, b, (kb, ka), rescale=True)
         ref_r = o.hrot(lvl, a, (rb, ra), 5)
-        for e in (chd.BCONV_CUDA_CORE, chd.BCONV_TENSOR_CORE):
+        for e in ALL_ENGINES:
             with engine(g, e):
                 _eq(g.HMult(g.import_ct(lvl, a), g.import_ct(lvl, b), key, rescale=True), ref_m)
                 _eq(g.HRot(g.import_ct(lvl, a), rkey, 5), ref_r)
@@ -282,7 +292,7 @@ def test_terminal_primes_n16_every_level_both_engines(cuda_ok):
         b = uniform_parts(rat, lvl, 1150 + lvl)
         ref_m = o.hmult(lvl, a, b, (kb, ka), rescale=True)
         ref_r = o.hrot(lvl, a, (rb, ra), 3)
-        for e in (chd.BCONV_CUDA_CORE, chd.BCONV_TENSOR_CORE):
+        for e in ALL_ENGINES:
             with engine(g, e):
                 _eq(g.HMult(g.import_ct(lvl, a), g.import_ct(lvl, b), key, rescale=True), ref_m)
                 _eq(g.HRot(g.import_ct(lvl, a), rkey, 3), ref_r)

@@ -114,3 +114,23 @@ def test_noalloc_refuses_oversized_levels(cuda_ok):
     rc = _noalloc(ctx, lvl, x, out)
     assert rc == 6  # CHD_ERR_UNSUPPORTED
     assert "exceeds the static scratch" in chd.lib().chd_last_error().decode()
+
+
+def test_noalloc_refuses_digits_beyond_the_bconv_limits(cuda_ok):
+    # alpha = 20 at N = 2^13 (the unfused small-degree path): a digit of 20
+    # primes exceeds the base conversion's 16 sources; refused before any
+    # work, like the allocating chd_modup_raw
+    from importlib import util
+    import os
+    spec = util.spec_from_file_location("gen_params", os.path.join(chd.PARAM_DIR, "gen_params.py"))
+    gp = util.module_from_spec(spec)
+    spec.loader.exec_module(gp)
+    ctx = chd.Context(json.dumps(gp.keyswitch_params(24, 20, log_n=13)))
+    lvl = ctx.max_level
+    nq = ctx.num_q(lvl)
+    x = torch.zeros((nq, ctx.n), dtype=torch.int32, device="cuda")
+    out = torch.zeros((-(-nq // 20), nq + 20, ctx.n), dtype=torch.int32, device="cuda")
+    assert _noalloc(ctx, lvl, x, out) == 6  # CHD_ERR_UNSUPPORTED
+    assert "more than 16 primes" in chd.lib().chd_last_error().decode()
+    with pytest.raises(chd.CheddarError):
+        ctx.modup_raw(lvl, x, out)
