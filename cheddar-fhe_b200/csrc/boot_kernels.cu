@@ -157,8 +157,10 @@ __global__ void __launch_bounds__(256) k_const_accum(const __grid_constant__ Con
   if (i >= n) return;
   uint32_t s[4] = {0, 0, 0, 0};
   for (int t = 0; t < d.terms; t++) {
+    const uint32_t *src = d.src[t][part];
+    if (!src) continue;
     uint32_t x[4];
-    ld_vec<4>(d.src[t][part] + static_cast<size_t>(d.src_row0[t] + r) * n + i, x);
+    ld_vec<4>(src + static_cast<size_t>(d.src_row0[t] + r) * n + i, x);
     const uint32_t c = d.c[t][r];
 #pragma unroll
     for (int l = 0; l < 4; l++) s[l] = add_mod(s[l], mont_mul(x[l], c, q, qi), q);
@@ -200,7 +202,7 @@ void launch_pt_accum(const PtAccumDesc &d, cudaStream_t s) {
 }
 
 void launch_const_accum(const ConstAccumDesc &d, cudaStream_t s) {
-  if (d.rows <= 0 || d.parts <= 0 || d.terms <= 0) return;
+  if (d.rows <= 0 || d.parts <= 0 || d.parts > kMaxConstAccumOuts || d.terms <= 0) return;
   k_const_accum<<<dim3((d.n / 4 + 255) / 256, d.rows, d.parts), 256, 0, s>>>(d);
 }
 

@@ -248,7 +248,7 @@ Status permuted_secret(Context &C, const uint32_t *s, int amount, uint32_t *out)
   PermuteBatch pb{};
   pb.galois = C.P->galois_of(amount);
   for (int r = 0; r < tot; r++) {
-    if (pb.count == 64) {
+    if (pb.count == kMaxPermuteRows) {
       launch_permute(pb, C.P->log_n, C.stream);
       pb.count = 0;
     }
@@ -256,6 +256,7 @@ Status permuted_secret(Context &C, const uint32_t *s, int amount, uint32_t *out)
     pr.src = s + static_cast<size_t>(r) * n;
     pr.dst = out + static_cast<size_t>(r) * n;
     pr.add = nullptr;
+    pr.src2 = nullptr;
     pr.q = C.P->primes[g[r]];
   }
   launch_permute(pb, C.P->log_n, C.stream);

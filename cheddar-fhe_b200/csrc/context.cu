@@ -1915,7 +1915,7 @@ Status Context::permute(DeviceCt &res, const DeviceCt &a, int amount) {
   const int parts = a.has_rx ? 3 : 2;
   for (int p = 0; p < parts; p++)
     for (int r = 0; r < tot; r++) {
-      if (pb.count == 64) {
+      if (pb.count == kMaxPermuteRows) {
         launch_permute(pb, P->log_n, stream);
         pb.count = 0;
       }
@@ -1923,6 +1923,7 @@ Status Context::permute(DeviceCt &res, const DeviceCt &a, int amount) {
       pr.src = src[p] + static_cast<size_t>(r) * n;
       pr.dst = dst[p] + static_cast<size_t>(r) * n;
       pr.add = nullptr;
+      pr.src2 = nullptr;
       pr.q = P->primes[g[r]];
     }
   launch_permute(pb, P->log_n, stream);

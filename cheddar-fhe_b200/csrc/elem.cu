@@ -215,6 +215,12 @@ __global__ void __launch_bounds__(256) k_permute(const __grid_constant__ Permute
   for (int l = 0; l < 4; l++) slot[l] = galois_src(k0 + l, pb.galois, log_n);
   uint32_t x[4], v[4];
   unpack(ld4(p.src + (slot[0] & ~3u)), x);
+  if (p.src2) {
+    uint32_t y[4];
+    unpack(ld4(p.src2 + (slot[0] & ~3u)), y);
+#pragma unroll
+    for (int l = 0; l < 4; l++) x[l] = add_mod(x[l], y[l], p.q);
+  }
 #pragma unroll
   for (int l = 0; l < 4; l++) {
     const uint32_t m = slot[l] & 3u;

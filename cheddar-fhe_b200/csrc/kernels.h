@@ -129,16 +129,19 @@ struct PtAccumDesc {
 };
 void launch_pt_accum(const PtAccumDesc &d, cudaStream_t s);
 
-// dst[part][r] = sum_t c[t][r] * src[t][part][src_row0[t] + r]
+// dst[o][r] = sum_t c[t][r] * src[t][o][src_row0[t] + r] for every output o
+// (a ciphertext part; several ciphertexts sharing the terms' constants fill
+// one launch); a null src[t][o] leaves term t out of output o
 constexpr int kMaxConstAccumTerms = 16;
+constexpr int kMaxConstAccumOuts = 24;
 struct ConstAccumDesc {
-  const uint32_t *src[kMaxConstAccumTerms][3];
+  const uint32_t *src[kMaxConstAccumTerms][kMaxConstAccumOuts];
   int src_row0[kMaxConstAccumTerms];
   uint32_t c[kMaxConstAccumTerms][64];
-  uint32_t *dst[3];
+  uint32_t *dst[kMaxConstAccumOuts];
   uint32_t q[64];
   int32_t qinv[64];
-  int terms, rows, parts, n;
+  int terms, rows, parts, n;  // parts: the number of outputs
 };
 void launch_const_accum(const ConstAccumDesc &d, cudaStream_t s);
 
@@ -273,16 +276,19 @@ void launch_tensor(const TensorBatch &b, int log_n, cudaStream_t s);
 
 // Automorphism X -> X^g in the bit-reversed evaluation domain (gather):
 // dst[k] = src[brev(((2 brev(k) + 1) g - 1) mod 2N)]
+// dst = Permute(src (+ src2)) (+ add), one limb per row
 struct PermuteRow {
   const uint32_t *src;
+  const uint32_t *src2;  // optional second source, added before the gather
   uint32_t *dst;
-  const uint32_t *add;  // optional addend (PermuteAccum with src0)
+  const uint32_t *add;   // optional addend (PermuteAccum with src0)
   uint32_t q;
 };
+constexpr int kMaxPermuteRows = 128;
 struct PermuteBatch {
   int count;
   uint32_t galois;
-  PermuteRow rows[64];
+  PermuteRow rows[kMaxPermuteRows];
 };
 void launch_permute(const PermuteBatch &b, int log_n, cudaStream_t s);
 

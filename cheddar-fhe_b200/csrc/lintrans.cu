@@ -432,7 +432,7 @@ struct HoistOps {
     PermuteBatch pb{};
     pb.galois = C.P->galois_of(amount);
     for (int r = 0; r < tot; r++) {
-      if (pb.count == 64) {
+      if (pb.count == kMaxPermuteRows) {
         launch_permute(pb, C.P->log_n, C.stream);
         pb.count = 0;
       }
@@ -440,8 +440,31 @@ struct HoistOps {
       pr.src = src + static_cast<size_t>(r) * n;
       pr.dst = dst + static_cast<size_t>(r) * n;
       pr.add = add ? add + static_cast<size_t>(r) * n : nullptr;
+      pr.src2 = nullptr;
       pr.q = C.P->primes[g[r]];
     }
+    launch_permute(pb, C.P->log_n, C.stream);
+  }
+  // dst_j += Permute_g(src_j + src2_j) over the Q u P rows of nparts parts
+  // (src2_j may be null), the rows of all parts filling each launch
+  void permute_add_many(int nparts, const uint32_t *const *src, const uint32_t *const *src2, uint32_t *const *dst,
+                        int amount) const {
+    PermuteBatch pb{};
+    pb.galois = C.P->galois_of(amount);
+    for (int j = 0; j < nparts; j++)
+      for (int r = 0; r < tot; r++) {
+        if (pb.count == kMaxPermuteRows) {
+          launch_permute(pb, C.P->log_n, C.stream);
+          pb.count = 0;
+        }
+        const size_t o = static_cast<size_t>(r) * n;
+        PermuteRow &pr = pb.rows[pb.count++];
+        pr.src = src[j] + o;
+        pr.src2 = src2[j] ? src2[j] + o : nullptr;
+        pr.dst = dst[j] + o;
+        pr.add = dst[j] + o;
+        pr.q = C.P->primes[g[r]];
+      }
     launch_permute(pb, C.P->log_n, C.stream);
   }
   void add_rows(const uint32_t *a, const uint32_t *b, uint32_t *dst, int rows) const {
@@ -720,12 +743,19 @@ Status Context::lt_evaluate_batch(int count, DeviceCt *const *res, const DeviceC
       CHD_TRY(modup_many(level, count, md.data(), mu_p.data()));
       CHD_TRY(H.key_mult(count, mu_p.data(), *k, tb.data(), ta.data()));
     }
+    // key-switched part plus the accumulator's own b, both rotated, for
+    // every ciphertext in few launches
+    std::vector<const uint32_t *> ps(2 * count), ps2(2 * count);
+    std::vector<uint32_t *> pd(2 * count);
     for (int c = 0; c < count; c++) {
-      // key-switched part plus the accumulator's own b, both rotated
-      H.add_rows(tb[c], outs[c][i].first, tb[c], H.tot);
-      H.permute_rows(tb[c], fb[c], fb[c], gsr);
-      H.permute_rows(ta[c], fa[c], fa[c], gsr);
+      ps[2 * c] = tb[c];
+      ps2[2 * c] = outs[c][i].first;
+      pd[2 * c] = fb[c];
+      ps[2 * c + 1] = ta[c];
+      ps2[2 * c + 1] = nullptr;
+      pd[2 * c + 1] = fa[c];
     }
+    H.permute_add_many(2 * count, ps.data(), ps2.data(), pd.data(), gsr);
   }
   // EvaluateFinalModDown, Hoist.cu:460-488, all ciphertexts at once
   std::vector<const uint32_t *> fsrc(2 * count);

@@ -30,24 +30,22 @@ void caccum(Context &C, DeviceCt &dst, const NP &np, int parts, const std::vecto
   const int nq = np.q(), n = C.P->n;
   std::vector<int> g(nq);
   C.P->gidx(np, g.data());
-  for (int p = 0; p < parts; p++) {
-    ConstAccumDesc d{};
-    for (const CTerm &t : terms) {
-      d.src[d.terms][0] = part_ptr(*t.src, p);
-      d.src_row0[d.terms] = t.front;
-      for (int r = 0; r < nq; r++) d.c[d.terms][r] = t.c[r];
-      d.terms++;
-    }
-    d.dst[0] = part_ptr(dst, p);
-    for (int r = 0; r < nq; r++) {
-      d.q[r] = C.P->primes[g[r]];
-      d.qinv[r] = C.P->qinv[g[r]];
-    }
-    d.rows = nq;
-    d.parts = 1;
-    d.n = n;
-    launch_const_accum(d, C.stream);
+  ConstAccumDesc d{};
+  for (const CTerm &t : terms) {
+    for (int p = 0; p < parts; p++) d.src[d.terms][p] = part_ptr(*t.src, p);
+    d.src_row0[d.terms] = t.front;
+    for (int r = 0; r < nq; r++) d.c[d.terms][r] = t.c[r];
+    d.terms++;
   }
+  for (int p = 0; p < parts; p++) d.dst[p] = part_ptr(dst, p);
+  for (int r = 0; r < nq; r++) {
+    d.q[r] = C.P->primes[g[r]];
+    d.qinv[r] = C.P->qinv[g[r]];
+  }
+  d.rows = nq;
+  d.parts = parts;
+  d.n = n;
+  launch_const_accum(d, C.stream);
 }
 
 bool subset(const NP &sub, const NP &sup) { return sub.main <= sup.main && sub.ter <= sup.ter; }

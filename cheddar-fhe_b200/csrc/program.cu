@@ -88,34 +88,54 @@ Status Context::run_program_batch(const Program &prog, int count, std::vector<De
     int front;
     const uint32_t *c;  // per dst row constant (Montgomery), already offset
   };
+  // One launch takes every part of the destination; while `defer` is set
+  // (the per-ciphertext loop of one op over a batch), the accumulations of
+  // consecutive ciphertexts, which share the op's constants, join one launch
+  // until its outputs run out or the terms differ; flush_accum launches it.
+  ConstAccumDesc pend{};
+  const uint32_t *pend_c[kMaxConstAccumTerms] = {};
+  bool defer = false;
+  auto flush_accum = [&]() {
+    if (pend.parts > 0) launch_const_accum(pend, stream);
+    pend.parts = 0;
+    pend.terms = 0;
+  };
   auto const_accum = [&](DeviceCt &dst, const NP &np, int parts, const std::vector<Term> &terms) -> Status {
     const int nq = np.q();
-    std::vector<int> g(nq);
-    P->gidx(np, g.data());
-    for (int p = 0; p < parts; p++) {
-      ConstAccumDesc d{};
-      for (const Term &t : terms) {
-        if (p == 2 && !t.src->has_rx) continue;
-        CHD_CHECK(d.terms < kMaxConstAccumTerms, kErrUnsupported, "program: too many accumulation terms");
-        d.src[d.terms][0] = part_of(*t.src, p);
-        d.src_row0[d.terms] = t.front;
-        for (int r = 0; r < nq; r++) d.c[d.terms][r] = t.c[r];
-        d.terms++;
-      }
-      d.dst[0] = part_of(dst, p);
-      for (int r = 0; r < nq; r++) {
-        d.q[r] = P->primes[g[r]];
-        d.qinv[r] = P->qinv[g[r]];
-      }
-      d.rows = nq;
-      d.parts = 1;
-      d.n = n;
-      if (d.terms == 0) {
-        cudaMemsetAsync(d.dst[0], 0, static_cast<size_t>(nq) * n * 4, stream);
-      } else {
-        launch_const_accum(d, stream);
-      }
+    if (terms.empty()) {
+      for (int p = 0; p < parts; p++) cudaMemsetAsync(part_of(dst, p), 0, static_cast<size_t>(nq) * n * 4, stream);
+      return kOk;
     }
+    CHD_CHECK(static_cast<int>(terms.size()) <= kMaxConstAccumTerms, kErrUnsupported,
+              "program: too many accumulation terms");
+    bool same = pend.parts > 0 && pend.rows == nq && pend.terms == static_cast<int>(terms.size()) &&
+                pend.parts + parts <= kMaxConstAccumOuts;
+    for (size_t i = 0; same && i < terms.size(); i++)
+      same = pend_c[i] == terms[i].c && pend.src_row0[i] == terms[i].front;
+    if (!same) {
+      flush_accum();
+      std::vector<int> g(nq);
+      P->gidx(np, g.data());
+      for (size_t i = 0; i < terms.size(); i++) {
+        pend.src_row0[i] = terms[i].front;
+        pend_c[i] = terms[i].c;
+        for (int r = 0; r < nq; r++) pend.c[i][r] = terms[i].c[r];
+      }
+      for (int r = 0; r < nq; r++) {
+        pend.q[r] = P->primes[g[r]];
+        pend.qinv[r] = P->qinv[g[r]];
+      }
+      pend.terms = static_cast<int>(terms.size());
+      pend.rows = nq;
+      pend.n = n;
+    }
+    for (int p = 0; p < parts; p++) {
+      const int o = pend.parts++;
+      for (size_t i = 0; i < terms.size(); i++)
+        pend.src[i][o] = (p == 2 && !terms[i].src->has_rx) ? nullptr : part_of(*terms[i].src, p);
+      pend.dst[o] = part_of(dst, p);
+    }
+    if (!defer) flush_accum();
     return kOk;
   };
   auto front_of = [&](const NP &src, const NP &dst) -> int { return src.ter - dst.ter; };
@@ -123,13 +143,16 @@ Status Context::run_program_batch(const Program &prog, int count, std::vector<De
     CHD_CHECK(sub.main <= sup.main && sub.ter <= sup.ter, kErrShape, "program: incompatible levels");
     return kOk;
   };
-  std::vector<std::vector<uint32_t>> ones;  // Montgomery 1 per level, by q count
+  std::map<std::pair<int, int>, std::vector<uint32_t>> ones;  // Montgomery 1 per level
   auto mont_one = [&](const NP &np) -> const uint32_t * {
-    ones.emplace_back(np.q());
-    std::vector<int> g(np.q());
-    P->gidx(np, g.data());
-    for (int r = 0; r < np.q(); r++) ones.back()[r] = prime::to_mont(1, P->primes[g[r]]);
-    return ones.back().data();
+    std::vector<uint32_t> &v = ones[{np.main, np.ter}];
+    if (v.empty()) {
+      v.resize(np.q());
+      std::vector<int> g(np.q());
+      P->gidx(np, g.data());
+      for (int r = 0; r < np.q(); r++) v[r] = prime::to_mont(1, P->primes[g[r]]);
+    }
+    return v.data();
   };
 
   auto rot_key_of = [&](int r, const DeviceEvk **k) -> Status {
@@ -208,6 +231,7 @@ Status Context::run_program_batch(const Program &prog, int count, std::vector<De
         const int parts = a0.has_rx ? 3 : 2;
         std::vector<const uint32_t *> src;
         std::vector<uint32_t *> dst;
+        defer = true;  // the level-down constants of all ciphertexts in few launches
         for (int c = 0; c < count; c++) {
           const DeviceCt &x = R[c]->at(op.a);
           CHD_CHECK(x.np == a0.np && x.has_rx == a0.has_rx, kErrShape, "program: batch members at different levels");
@@ -232,6 +256,8 @@ Status Context::run_program_batch(const Program &prog, int count, std::vector<De
           t.scale = in->scale / P->rescale_prod[level];
           t.num_slots = in->num_slots;
         }
+        defer = false;
+        flush_accum();
         CHD_TRY(moddown(level, MDType::kRescale, src.data(), dst.data(), static_cast<int>(src.size())));
         break;
       }
@@ -292,7 +318,9 @@ Status Context::run_program_batch(const Program &prog, int count, std::vector<De
       for (int c = 0; c < count; c++) swap_regs(R[c]->at(op.dst), R[c]->at(prog.nregs));
       continue;
     }
-    // ---- ops that run per ciphertext ----
+    // ---- ops that run per ciphertext (constant accumulations of the
+    // batch joined into few launches) ----
+    defer = count > 1 && (op.kind == OpKind::kConstMult || op.kind == OpKind::kConstAccum);
     for (int bc = 0; bc < count; bc++) {
     std::vector<DeviceCt> &regs = *R[bc];
     DeviceCt &spare = regs[prog.nregs], &spare2 = regs[prog.nregs + 1];
@@ -477,6 +505,8 @@ Status Context::run_program_batch(const Program &prog, int count, std::vector<De
     }
     if (!meta) swap_regs(regs.at(op.dst), t);
     }
+    defer = false;
+    flush_accum();
   }
   return check_cuda("program");
 }

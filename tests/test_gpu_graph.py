@@ -44,7 +44,7 @@ def test_mixed_level_batch_beyond_launch_limits(cuda_ok):
         singles = [g.HMult(x, y, key, rescale=rescale) for x, y in zip(ga, gb)]
         for r, s1, (lvl, _, _) in zip(outs, singles, pairs):
             ri, si = r.info(), s1.info()
-            assert g.level_of(ri["num_main"], ri["num_ter"]) == (lvl - 1 if rescale else lvl)
+            assert (ri["num_main"], ri["num_ter"]) == tuple(g.level_np(lvl - 1 if rescale else lvl))
             assert ri == si
             for x, y in zip(r.numpy(), s1.numpy()):
                 assert np.array_equal(x, y)
