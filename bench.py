@@ -289,7 +289,8 @@ def main():
     # count K, jobs, largest target count M) -> engine / target split
     line["config"]["autotuned_column_passes"] = [
         f"K{t['K']} jobs{t['jobs']} M{t['M']}: "
-        f"{({0: 'cuda_core', 1: 'tensor_core', 3: 'tensor_core_wide'}).get(t['engine'], t['engine'])}/split{t['split']}"
+        f"{({0: 'cuda_core', 1: 'tensor_core', 3: 'tensor_core_wide', 4: 'tensor_core_wide_128regs'}).get(t['engine'], t['engine'])}"
+        f"/split{t['split']}"
         for t in chd.ks_tuned_shapes()]
     if rank == 0 and world == 1 and not args.no_reference_gpu:
         ref = reference_gpu_run(args)

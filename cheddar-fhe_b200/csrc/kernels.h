@@ -164,7 +164,8 @@ constexpr int kMaxMSColJobs = 24;
 struct MSColBatch {
   int count;
   int engine;             // base conversion on 0: CUDA cores, 1: tensor cores, 3: tensor cores with
-                          // 256-thread tiles (K <= 12; larger K runs engine 1)
+                          // 256-thread tiles (K <= 12; larger K runs engine 1); 4 (autotuner only):
+                          // 3 with the K <= 8 kernel sized for 2 CTAs per SM
   int *err;               // set to 1 when a tensor-core wait gives up
   const uint2 *tw, *itw;  // twiddle tables [nprimes][N]
   const uint32_t *primes;
@@ -179,9 +180,10 @@ int modswitch_tuned_shapes(int *out, int cap);
 void launch_modswitch_cols_tc(const MSColBatch &b, int max_k, cudaStream_t s);
 size_t modswitch_cols_tc_smem(int kmax);
 // the same on 256-thread tiles, 8 coefficients per thread (modswitch_tc8.cu),
-// for jobs with K <= 12
+// for jobs with K <= 12; regs128 sizes the K <= 8 kernel for 2 CTAs per SM
+// (128 registers) instead of 3 (80)
 bool modswitch_cols_tc8_supports(int max_k);
-void launch_modswitch_cols_tc8(const MSColBatch &b, int max_k, cudaStream_t s);
+void launch_modswitch_cols_tc8(const MSColBatch &b, int max_k, bool regs128, cudaStream_t s);
 void launch_ntt_inv_rows(const RowBatch &rb, int log_n, cudaStream_t s);
 
 // Fused key-switching row pass (N = 2^16), see keyswitch.cu.  Modes:

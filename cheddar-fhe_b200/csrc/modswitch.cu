@@ -232,11 +232,11 @@ size_t modswitch_cols_smem(int kmax) { return (static_cast<size_t>(kExRows) * kT
 namespace {
 
 void launch_engine(const MSColBatch &b, int engine, int max_k, cudaStream_t s) {
-  if (engine == 3 && modswitch_cols_tc8_supports(max_k)) {
-    launch_modswitch_cols_tc8(b, max_k, s);
+  if ((engine == 3 || engine == 4) && modswitch_cols_tc8_supports(max_k)) {
+    launch_modswitch_cols_tc8(b, max_k, engine == 4, s);
     return;
   }
-  if (engine == 1 || engine == 3) {
+  if (engine == 1 || engine == 3 || engine == 4) {
     launch_modswitch_cols_tc(b, max_k, s);
     return;
   }
@@ -319,8 +319,9 @@ int heuristic_groups(const MSColBatch &b, int max_m) {
 // when a launch holds one ciphertext's few jobs, the tensor-core passes on
 // batches; small launches gain from the split).  The first launch of a shape
 // (device, largest K, jobs, largest M) outside a stream capture times every
-// candidate (engine in {CUDA cores, tensor cores with 128-thread tiles,
-// tensor cores with 256-thread tiles for K <= 12} x split in
+// candidate (engine and tile in {CUDA cores, tensor cores with 128-thread
+// tiles, tensor cores with 256-thread tiles for K <= 12 at 80 or, for
+// K <= 8, 128 registers per thread} x split in
 // {1, 2, 4, heuristic}) three times after a
 // warm-up, interleaved, with CUDA events (a host synchronisation, once per
 // shape), keeps the fastest launch and caches the choice for the process.
@@ -352,12 +353,14 @@ bool tune_and_launch(const MSColBatch &b, int max_k, int max_m, cudaStream_t s, 
   if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return false;
   std::vector<Choice> cand;
   const int by_m = max_m / 4 > 1 ? max_m / 4 : 1;
-  for (int e : {0, 1, 3})
+  for (int e : {0, 1, 3, 4})
     for (int g : {1, 2, 4, hg})
       if (g <= by_m) {
         bool seen = false;
         for (const Choice &c : cand) seen |= c.engine == e && c.groups == g;
-        if (!seen && (e != 3 || modswitch_cols_tc8_supports(max_k))) cand.push_back(Choice{e, g});
+        // engine 4 differs from 3 only for K <= 8
+        const bool valid = e < 3 || (modswitch_cols_tc8_supports(max_k) && (e == 3 || max_k <= 8));
+        if (!seen && valid) cand.push_back(Choice{e, g});
       }
   constexpr int kRounds = 3;
   const int nc = static_cast<int>(cand.size());

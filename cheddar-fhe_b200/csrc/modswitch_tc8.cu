@@ -68,9 +68,10 @@ __device__ __forceinline__ int xsw(int row, int c) {
 
 __device__ __forceinline__ uint32_t acc_col(int s) { return 64u * (s & 1) + 16u * ((s >> 1) & 3); }
 
-template <int KMAX>
-__global__ void __launch_bounds__(kThreads, KMAX <= 8 ? 3 : 2)
-    k_modswitch_cols_tc8(const __grid_constant__ MSColBatch b) {
+// MINB: CTAs per SM the register budget is sized for (3: 80 registers, 2:
+// 128); KMAX = 8 fits 3 CTAs in shared memory, KMAX = 12 only 2
+template <int KMAX, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) k_modswitch_cols_tc8(const __grid_constant__ MSColBatch b) {
   using G = Geo8<KMAX>;
   extern __shared__ __align__(16) uint8_t smem[];
   __shared__ __align__(8) uint64_t mbar;
@@ -356,26 +357,30 @@ __global__ void __launch_bounds__(kThreads, KMAX <= 8 ? 3 : 2)
   }
 }
 
-template <int KMAX>
+template <int KMAX, int MINB>
 void launch_kmax8(const MSColBatch &b, cudaStream_t s) {
-  // CTAs per SM: 3 for KMAX = 8 (shared memory and registers), 2 for 12;
-  // their accumulators (128 TMEM columns each) always fit
+  // CTAs per SM: up to 3 for KMAX = 8 (shared memory), 2 for 12; their
+  // accumulators (128 TMEM columns each) always fit
   const size_t sm = Geo8<KMAX>::kSmem;
-  cudaFuncSetAttribute(k_modswitch_cols_tc8<KMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaFuncSetAttribute(k_modswitch_cols_tc8<KMAX, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        static_cast<int>(sm));
-  k_modswitch_cols_tc8<KMAX><<<dim3(512 / kTC, b.count), kThreads, sm, s>>>(b);
+  k_modswitch_cols_tc8<KMAX, MINB><<<dim3(512 / kTC, b.count), kThreads, sm, s>>>(b);
 }
 
 }  // namespace
 
 bool modswitch_cols_tc8_supports(int max_k) { return max_k >= 1 && max_k <= 12; }
 
-void launch_modswitch_cols_tc8(const MSColBatch &b, int max_k, cudaStream_t s) {
+void launch_modswitch_cols_tc8(const MSColBatch &b, int max_k, bool regs128, cudaStream_t s) {
   if (b.count <= 0) return;
-  if (max_k <= 8)
-    launch_kmax8<8>(b, s);
-  else
-    launch_kmax8<12>(b, s);
+  if (max_k <= 8) {
+    if (regs128)
+      launch_kmax8<8, 2>(b, s);
+    else
+      launch_kmax8<8, 3>(b, s);
+  } else {
+    launch_kmax8<12, 2>(b, s);
+  }
 }
 
 }  // namespace chd
