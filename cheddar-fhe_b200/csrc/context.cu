@@ -6,6 +6,8 @@
 // kernels of ntt.cu / elem.cu; this file only computes constants on the host
 // and builds launch descriptors.
 #include <algorithm>
+#include <cerrno>
+#include <limits>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -199,7 +201,8 @@ struct JParser {
       j++;
     if (j == i) return fail("unexpected character");
     v.t = JVal::kNum;
-    v.num = std::strtod(s.substr(i, j - i).c_str(), nullptr);
+    v.s = s.substr(i, j - i);  // the token, for exact integers beyond a double
+    v.num = std::strtod(v.s.c_str(), nullptr);
     i = j;
     return true;
   }
@@ -222,7 +225,8 @@ struct JParser {
 };
 }  // namespace
 
-bool parse_param_json(const std::string &text, ParamSpec *out, std::string *err) {
+template <typename W>
+bool parse_spec(const std::string &text, ParamSpecT<W> *out, std::string *err) {
   // schema of unittest/Testbed.h:95-221 of the reference
   JParser p(text);
   JVal root;
@@ -243,7 +247,7 @@ bool parse_param_json(const std::string &text, ParamSpec *out, std::string *err)
     *v = x->num;
     return true;
   };
-  auto primes = [&](const char *k, std::vector<uint32_t> *v, bool req) -> bool {
+  auto primes = [&](const char *k, std::vector<W> *v, bool req) -> bool {
     const JVal *x = root.get(k);
     if (!x) {
       if (req) *err = std::string("Missing ") + k + " in JSON";
@@ -254,16 +258,19 @@ bool parse_param_json(const std::string &text, ParamSpec *out, std::string *err)
       return false;
     }
     for (auto &e : x->arr) {
-      if (e.t != JVal::kNum) {
+      if (e.t != JVal::kNum || e.s.empty() || e.s.find_first_not_of("0123456789") != std::string::npos) {
         *err = std::string(k) + " should be an array of integers";
         return false;
       }
-      v->push_back(static_cast<uint32_t>(e.num));
+      errno = 0;
+      const unsigned long long x = std::strtoull(e.s.c_str(), nullptr, 10);
+      const bool big = errno == ERANGE || x > static_cast<unsigned long long>(std::numeric_limits<W>::max());
+      v->push_back(big ? std::numeric_limits<W>::max() : static_cast<W>(x));
     }
     return true;
   };
   double d;
-  ParamSpec s;
+  ParamSpecT<W> s;
   if (!num("log_degree", &d, true)) return false;
   s.log_degree = static_cast<int>(d);
   if (!num("log_default_scale", &d, true)) return false;
@@ -299,6 +306,13 @@ bool parse_param_json(const std::string &text, ParamSpec *out, std::string *err)
   if (num("num_stc_levels", &d, false) && root.get("num_stc_levels")) s.num_stc_levels = static_cast<int>(d);
   *out = s;
   return true;
+}
+
+bool parse_param_json(const std::string &text, ParamSpec *out, std::string *err) {
+  return parse_spec(text, out, err);
+}
+bool parse_param_json64(const std::string &text, ParamSpec64 *out, std::string *err) {
+  return parse_spec(text, out, err);
 }
 
 // -------------------------------------------------------------- Params

@@ -58,20 +58,28 @@ struct NP {
   bool operator==(const NP &o) const { return main == o.main && ter == o.ter && aux == o.aux; }
 };
 
-struct ParamSpec {
+// The reference's Parameter fields for word size W (uint32_t, or uint64_t
+// for the 64-bit word path).
+template <typename W>
+struct ParamSpecT {
   int log_degree = 16;
   double base_scale = 0;
   int default_encryption_level = 0;
   std::vector<std::pair<int, int>> level_config;
-  std::vector<uint32_t> main_primes, aux_primes, ter_primes;
+  std::vector<W> main_primes, aux_primes, ter_primes;
   std::pair<int, int> additional_base{0, 0};
   int dense_hw = -1, sparse_hw = 32;
   bool boot = false;
   int num_cts_levels = 0, num_stc_levels = 0;
 };
+using ParamSpec = ParamSpecT<uint32_t>;
+using ParamSpec64 = ParamSpecT<uint64_t>;
 
-// Parses the reference's parameter JSON schema.
+// Parses the reference's parameter JSON schema (primes read as exact
+// integers; a prime beyond the word is kept as the word's maximum, which
+// validation rejects).
 bool parse_param_json(const std::string &text, ParamSpec *out, std::string *err);
+bool parse_param_json64(const std::string &text, ParamSpec64 *out, std::string *err);
 
 class Params {
  public:

@@ -23,35 +23,8 @@
 namespace chd {
 namespace {
 
-// Per-thread staging of one digit's operands, filled by cp.async one digit
-// ahead: the thread's 8 ModUp values (elements t + 64k of its row, words
-// [k][256 threads]) and its 8 + 8 key words (as 4 x 16 bytes,
-// [chunk][256 threads]), so the loads of digit i + 1 fly while digit i's
-// row NTT runs.  Two buffers of 24 KiB, then 16 KiB for the thread's b1 and
-// b2 words of the P * (d0, d1) term, fetched with the first digit.
-constexpr int kStageWords = 8 * 256 + 4 * 256 * 4;
-constexpr int kStageBytes = (2 * kStageWords + 4 * 256 * 4) * 4;
-
-__device__ __forceinline__ void cp_async4(uint32_t *dst, const uint32_t *src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
-               "l"(src)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
-               "l"(src)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
 __global__ void __launch_bounds__(256, 3) k_ks_rows(const __grid_constant__ KSRowsDesc d) {
   __shared__ uint32_t sm[4][512];
-  extern __shared__ uint4 stage_raw[];
-  uint32_t *stage = reinterpret_cast<uint32_t *>(stage_raw);
   // grid (count, 32, max_rows): the ciphertexts sharing one key row are
   // neighbours in launch order, so the key row comes from HBM once
   const int j = blockIdx.z;
@@ -78,83 +51,39 @@ __global__ void __launch_bounds__(256, 3) k_ks_rows(const __grid_constant__ KSRo
   uint32_t sb[8], sa[8];
 #pragma unroll
   for (int k = 0; k < 8; k++) sb[k] = sa[k] = 0;
-  const int tid = threadIdx.x;
-  const int own = L.own_digit[j];
-  // issue digit i's copies into buffer i & 1
-  auto prefetch = [&](int i) {
-    uint32_t *st = stage + (i & 1) * kStageWords;
-    if (own != i) {
-      const uint32_t *src = c.mu[i] + static_cast<size_t>(j) * 65536 + r * 512;
-#pragma unroll
-      for (int k = 0; k < 8; k++) cp_async4(st + k * 256 + tid, src + t + 64 * k);
-    }
-    uint4 *kst = reinterpret_cast<uint4 *>(st + 8 * 256);
-    const uint4 *kb = reinterpret_cast<const uint4 *>(L.kb[i] + koff);
-    const uint4 *ka = reinterpret_cast<const uint4 *>(L.ka[i] + koff);
-    cp_async16(kst + 0 * 256 + tid, kb);
-    cp_async16(kst + 1 * 256 + tid, kb + 1);
-    cp_async16(kst + 2 * 256 + tid, ka);
-    cp_async16(kst + 3 * 256 + tid, ka + 1);
-    cp_async_commit();
-  };
-  uint4 *bst = reinterpret_cast<uint4 *>(stage + 2 * kStageWords);
-  const bool with_p = is_q && c.b1 != nullptr;
-  if (with_p) {
-    const uint4 *b1 = reinterpret_cast<const uint4 *>(c.b1 + qoff);
-    cp_async16(bst + tid, b1);
-    cp_async16(bst + 256 + tid, b1 + 1);
-    if (mode == 0) {
-      const uint4 *b2 = reinterpret_cast<const uint4 *>(c.b2 + qoff);
-      cp_async16(bst + 512 + tid, b2);
-      cp_async16(bst + 768 + tid, b2 + 1);
-    }
-  }
-  if (L.beta > 0)
-    prefetch(0);  // its commit closes the group with b1 / b2
-  else
-    cp_async_commit();
   for (int i = 0; i < L.beta; i++) {
-    if (i + 1 < L.beta) {
-      prefetch(i + 1);
-      cp_async_wait<1>();  // digit i's group has landed (the thread's own words)
-    } else {
-      cp_async_wait<0>();
-    }
-    const uint32_t *st = stage + (i & 1) * kStageWords;
     uint32_t v[8];
-    if (own == i) {
+    if (L.own_digit[j] == i) {
       // own primes of the digit: the ModUp value is the key-switched input
 #pragma unroll
       for (int k = 0; k < 8; k++) v[k] = mode == 0 ? mont_mul(a1[k], a2[k], q, qi) : (mode == 1 ? a1[k] : a2[k]);
     } else {
+      const uint32_t *src = c.mu[i] + static_cast<size_t>(j) * 65536 + r * 512;
 #pragma unroll
-      for (int k = 0; k < 8; k++) v[k] = st[k * 256 + tid];
+      for (int k = 0; k < 8; k++) v[k] = src[t + 64 * k];
       row_fwd(v, srow, tw, r, t, q, 1 + rl);
 #pragma unroll
       for (int k = 0; k < 8; k++) v[k] = reduce2q(v[k], q);
       row_sync(1 + rl);
     }
-    const uint4 *kst = reinterpret_cast<const uint4 *>(st + 8 * 256);
-    const uint4 b0 = kst[tid], b1v = kst[256 + tid], a0 = kst[512 + tid], a1v = kst[768 + tid];
-    const uint32_t kb[8] = {b0.x, b0.y, b0.z, b0.w, b1v.x, b1v.y, b1v.z, b1v.w};
-    const uint32_t ka[8] = {a0.x, a0.y, a0.z, a0.w, a1v.x, a1v.y, a1v.z, a1v.w};
+    uint32_t kb[8], ka[8];
+    ld8(L.kb[i] + koff, kb);
+    ld8(L.ka[i] + koff, ka);
 #pragma unroll
     for (int k = 0; k < 8; k++) {
       sb[k] = add_mod(sb[k], mont_mul(v[k], kb[k], q, qi), q);
       sa[k] = add_mod(sa[k], mont_mul(v[k], ka[k], q, qi), q);
     }
   }
-  cp_async_wait<0>();
-  if (with_p) {
+  if (is_q && c.b1 != nullptr) {
     // P * (d0, d1): HMult d0 = b1 b2, d1 = b1 a2 + a1 b2; MultKey d0 = bx;
     // Relinearize d0 = bx, d1 = ax.  Without b1: the bare inner product.
-    // (The last wait above covered every group, the first one included.)
     const uint32_t pp = L.p_prod[j];
-    const uint4 x0 = bst[tid], x1 = bst[256 + tid];
-    const uint32_t b1[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+    uint32_t b1[8];
+    ld8(c.b1 + qoff, b1);
     if (mode == 0) {
-      const uint4 y0 = bst[512 + tid], y1 = bst[768 + tid];
-      const uint32_t b2[8] = {y0.x, y0.y, y0.z, y0.w, y1.x, y1.y, y1.z, y1.w};
+      uint32_t b2[8];
+      ld8(c.b2 + qoff, b2);
 #pragma unroll
       for (int k = 0; k < 8; k++) {
         const uint32_t d0 = mont_mul(b1[k], b2[k], q, qi);
@@ -194,9 +123,7 @@ __global__ void __launch_bounds__(256, 3) k_ks_rows(const __grid_constant__ KSRo
 
 void launch_ks_rows(const KSRowsDesc &d, int log_n, cudaStream_t s) {
   if (d.count <= 0 || d.max_rows <= 0 || log_n != 16) return;
-  constexpr int smem = kStageBytes;  // 64 KiB of staging beside the 8 KiB row buffers
-  cudaFuncSetAttribute(k_ks_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  k_ks_rows<<<dim3(d.count, 32, d.max_rows), 256, smem, s>>>(d);
+  k_ks_rows<<<dim3(d.count, 32, d.max_rows), 256, 0, s>>>(d);
 }
 
 }  // namespace chd
