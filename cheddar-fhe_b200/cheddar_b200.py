@@ -176,6 +176,26 @@ def lib():
         "chd_graph_end": (i, [vp, pp]),
         "chd_graph_launch": (i, [vp, vp]),
         "chd_graph_destroy": (None, [vp]),
+        "chd64_context_create_json": (i, [C.c_char_p, i, pp]),
+        "chd64_context_destroy": (None, [vp]),
+        "chd64_context_synchronize": (i, [vp]),
+        "chd64_max_level": (i, [vp]),
+        "chd64_alpha": (i, [vp]),
+        "chd64_level_np": (i, [vp, i, C.POINTER(i), C.POINTER(i)]),
+        "chd64_primes": (i, [vp, vp, i]),
+        "chd64_ntt": (i, [vp, i, i, i, vp, i, i, i]),
+        "chd64_modup_raw": (i, [vp, i, vp, vp]),
+        "chd64_moddown_raw": (i, [vp, i, i, vp, vp, i]),
+        "chd64_ct_create": (i, [vp, pp]),
+        "chd64_ct_destroy": (None, [vp]),
+        "chd64_ct_import": (i, [vp, vp, i, d, i, vp, vp, i]),
+        "chd64_ct_export": (i, [vp, vp, vp, vp]),
+        "chd64_ct_info": (i, [vp, C.POINTER(i), C.POINTER(i), C.POINTER(d), C.POINTER(i)]),
+        "chd64_evk_create": (i, [vp, i, vp, vp, i, pp]),
+        "chd64_evk_destroy": (None, [vp]),
+        "chd64_hmult": (i, [vp, vp, vp, vp, vp, i]),
+        "chd64_hrot": (i, [vp, vp, vp, vp, i]),
+        "chd64_rescale": (i, [vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -1067,3 +1087,125 @@ class EvaluationKey:
                 self.ptr = C.c_void_p()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------- 64-bit words
+class Context64:
+    """The 64-bit word path (the reference's Context<uint64_t>): a context
+    from a parameter JSON with primes up to 2^62 (e.g. the reference's
+    bootparam_40_64bit.json), N = 2^16; raw NTT / ModUp / ModDown, HMult and
+    HRot on uint64 residues."""
+
+    def __init__(self, params_json, device=0):
+        self.ptr = C.c_void_p()
+        _check(lib().chd64_context_create_json(params_json.encode(), device, C.byref(self.ptr)))
+        self.params = json.loads(params_json)
+        self.n = 1 << self.params["log_degree"]
+        self.max_level = lib().chd64_max_level(self.ptr)
+        self.alpha = lib().chd64_alpha(self.ptr)
+
+    def __del__(self):
+        if getattr(self, "ptr", None) is not None and self.ptr.value:
+            lib().chd64_context_destroy(self.ptr)
+            self.ptr = C.c_void_p()
+
+    def synchronize(self):
+        _check(lib().chd64_context_synchronize(self.ptr))
+
+    def level_np(self, level):
+        m, t = C.c_int(), C.c_int()
+        _check(lib().chd64_level_np(self.ptr, level, C.byref(m), C.byref(t)))
+        return m.value, t.value
+
+    def primes(self):
+        n = lib().chd64_primes(self.ptr, None, 0)
+        out = np.zeros(n, dtype=np.uint64)
+        lib().chd64_primes(self.ptr, out.ctypes.data, n)
+        return out
+
+    def ntt(self, np_, data_dev, count=1, inverse=False, mont=False):
+        """NTT / INTT in place of `count` polynomials over (main, ter, aux)
+        primes in a device tensor (int64 words)."""
+        _check(lib().chd64_ntt(self.ptr, np_[0], np_[1], np_[2], _ptr(data_dev), count, int(inverse), int(mont)))
+
+    def modup_raw(self, level, src_dev, dst_dev):
+        _check(lib().chd64_modup_raw(self.ptr, level, _ptr(src_dev), _ptr(dst_dev)))
+
+    def moddown_raw(self, level, kind, src_dev, dst_dev, npoly=1):
+        _check(lib().chd64_moddown_raw(self.ptr, level, kind, _ptr(src_dev), _ptr(dst_dev), npoly))
+
+    def import_ct(self, level, parts, scale=1.0, num_slots=None, on_device=False):
+        return Ciphertext64(self).load(level, parts, scale, num_slots, on_device)
+
+    def HMult(self, a, b, key, rescale=True):
+        res = Ciphertext64(self)
+        _check(lib().chd64_hmult(self.ptr, res.ptr, a.ptr, b.ptr, key.ptr, int(rescale)))
+        return res
+
+    def HRot(self, a, key, rot):
+        res = Ciphertext64(self)
+        _check(lib().chd64_hrot(self.ptr, res.ptr, a.ptr, key.ptr, rot))
+        return res
+
+    def Rescale(self, a):
+        res = Ciphertext64(self)
+        _check(lib().chd64_rescale(self.ptr, res.ptr, a.ptr))
+        return res
+
+
+class Ciphertext64:
+    def __init__(self, ctx):
+        self.ctx = ctx
+        self.ptr = C.c_void_p()
+        _check(lib().chd64_ct_create(ctx.ptr, C.byref(self.ptr)))
+
+    def __del__(self):
+        if getattr(self, "ptr", None) is not None and self.ptr.value:
+            lib().chd64_ct_destroy(self.ptr)
+            self.ptr = C.c_void_p()
+
+    def load(self, level, parts, scale=1.0, num_slots=None, on_device=False):
+        ns = self.ctx.n // 2 if num_slots is None else num_slots
+        if on_device:
+            ps = [_ptr(p) for p in parts]
+            keep = parts
+        else:
+            keep = [np.ascontiguousarray(p, dtype=np.uint64) for p in parts]
+            ps = [k.ctypes.data for k in keep]
+        _check(lib().chd64_ct_import(self.ctx.ptr, self.ptr, level, scale, ns, ps[0], ps[1], int(on_device)))
+        del keep
+        return self
+
+    def info(self):
+        m, t, ns = C.c_int(), C.c_int(), C.c_int()
+        sc = C.c_double()
+        _check(lib().chd64_ct_info(self.ptr, C.byref(m), C.byref(t), C.byref(sc), C.byref(ns)))
+        return dict(num_main=m.value, num_ter=t.value, scale=sc.value, num_slots=ns.value)
+
+    def numpy(self):
+        inf = self.info()
+        rows = inf["num_main"] + inf["num_ter"]
+        bx = np.zeros((rows, self.ctx.n), dtype=np.uint64)
+        ax = np.zeros_like(bx)
+        _check(lib().chd64_ct_export(self.ctx.ptr, self.ptr, bx.ctypes.data, ax.ctypes.data))
+        return bx, ax
+
+
+class EvaluationKey64:
+    """beta digits over the max-level key basis: bx, ax [beta][L + alpha][N]."""
+
+    def __init__(self, ctx, bx, ax, on_device=False):
+        self.ctx = ctx
+        self.ptr = C.c_void_p()
+        if on_device:
+            beta, pb, pa, keep = bx.shape[0], _ptr(bx), _ptr(ax), None
+        else:
+            keep = (np.ascontiguousarray(bx, dtype=np.uint64), np.ascontiguousarray(ax, dtype=np.uint64))
+            beta, pb, pa = keep[0].shape[0], keep[0].ctypes.data, keep[1].ctypes.data
+        _check(lib().chd64_evk_create(ctx.ptr, beta, pb, pa, int(on_device), C.byref(self.ptr)))
+        del keep
+
+    def __del__(self):
+        if getattr(self, "ptr", None) is not None and self.ptr.value:
+            lib().chd64_evk_destroy(self.ptr)
+            self.ptr = C.c_void_p()

@@ -540,6 +540,59 @@ int chd_stage_times(chd_context *ctx, double *ms, int *launches);
 int chd_params_level_consts(const char *json_text, int level, int kind, int digit, uint32_t *c1,
                             int32_t *table, uint32_t *inv, uint32_t *pad, int *dims);
 
+/* ---- the 64-bit word path: the reference's Context<uint64_t>
+ * (src/core/NTT.cu:1313, ModSwitch.cu:688, ElementWise.cu:1706,
+ * Context.cpp:952) for parameter files with primes up to 2^62, e.g.
+ * parameters/bootparam_40_64bit.json.  Residues are uint64_t words in the
+ * reference's layout ([num_primes][N], Montgomery form x 2^64 mod q,
+ * bit-reversed evaluation domain).  N = 2^16; the evaluation core: NTT,
+ * ModUp / ModDown / Rescale / ModDownAndRescale, HMult (relinearised,
+ * optionally rescaled), HRot.  Same status codes; chd_last_error describes
+ * failures. ---- */
+typedef struct chd64_context chd64_context;
+typedef struct chd64_ciphertext chd64_ciphertext;
+typedef struct chd64_evk chd64_evk;
+/* Parameter(...) + Context<uint64_t>::Create from the reference's JSON
+ * schema (unittest/Testbed.h:95-221); primes are read as exact integers */
+int chd64_context_create_json(const char *json, int device, chd64_context **out);
+void chd64_context_destroy(chd64_context *ctx);
+int chd64_context_synchronize(chd64_context *ctx);
+int chd64_max_level(const chd64_context *ctx);
+int chd64_alpha(const chd64_context *ctx);
+int chd64_level_np(const chd64_context *ctx, int level, int *num_main, int *num_ter);
+/* the primes in global order (terminal reversed, main, auxiliary); returns
+ * their count, writing at most cap */
+int chd64_primes(const chd64_context *ctx, uint64_t *out, int cap);
+/* NTTHandler<uint64_t>::NTT / INTT (NTT.cu:606-741): count polynomials of
+ * [num_main + num_ter + num_aux][N] at data_dev, in place; mont != 0 converts
+ * into (NTT) or out of (INTT) the Montgomery form */
+int chd64_ntt(chd64_context *ctx, int num_main, int num_ter, int num_aux, uint64_t *data_dev, int count, int inverse,
+              int mont);
+/* ModSwitchHandler<uint64_t>::ModUp (ModSwitch.cu:429-509): [num_q][N] ->
+ * beta x [num_q + alpha][N] */
+int chd64_modup_raw(chd64_context *ctx, int level, const uint64_t *src_dev, uint64_t *dst_dev);
+/* ModDown / Rescale / ModDownAndRescale (ModSwitch.cu:511-684) of npoly
+ * polynomials, type CHD_MODDOWN, CHD_RESCALE or CHD_MODDOWN_RESCALE */
+int chd64_moddown_raw(chd64_context *ctx, int level, int type, const uint64_t *src_dev, uint64_t *dst_dev, int npoly);
+int chd64_ct_create(chd64_context *ctx, chd64_ciphertext **out);
+void chd64_ct_destroy(chd64_ciphertext *ct);
+/* bx, ax: [num_q(level)][N] each, host or device memory */
+int chd64_ct_import(chd64_context *ctx, chd64_ciphertext *ct, int level, double scale, int num_slots,
+                    const uint64_t *bx, const uint64_t *ax, int src_on_device);
+int chd64_ct_export(chd64_context *ctx, const chd64_ciphertext *ct, uint64_t *bx, uint64_t *ax);
+int chd64_ct_info(const chd64_ciphertext *ct, int *num_main, int *num_ter, double *scale, int *num_slots);
+/* EvaluationKey<uint64_t>: beta digits over the max-level key basis,
+ * [beta][L + alpha][N] each for bx and ax */
+int chd64_evk_create(chd64_context *ctx, int beta, const uint64_t *bx, const uint64_t *ax, int src_on_device,
+                     chd64_evk **out);
+void chd64_evk_destroy(chd64_evk *key);
+/* Context<uint64_t>::HMult (Context.cpp:862-871), HRot (:776-791), Rescale
+ * (:739-774); the result must not alias an operand */
+int chd64_hmult(chd64_context *ctx, chd64_ciphertext *res, const chd64_ciphertext *a, const chd64_ciphertext *b,
+                const chd64_evk *key, int rescale);
+int chd64_hrot(chd64_context *ctx, chd64_ciphertext *res, const chd64_ciphertext *a, const chd64_evk *key, int rot);
+int chd64_rescale(chd64_context *ctx, chd64_ciphertext *res, const chd64_ciphertext *a);
+
 #ifdef __cplusplus
 }
 #endif

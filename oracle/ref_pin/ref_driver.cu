@@ -19,7 +19,10 @@
 //    (ModSwitch.cu:429-684), hoisted baby steps (Hoist.cu:578-691) and Boot
 //    (BootContext.cpp:299-365);
 //  * device timing of HMult, HRot, the NTT round trip and Boot with CUDA
-//    events on the legacy stream the reference issues its work on.
+//    events on the legacy stream the reference issues its work on;
+//  * the 64-bit word path (refx64_*): Context<uint64_t> from the same JSON
+//    fields, raw NTT / ModUp / ModDown, and HMult / HRot on imported
+//    ciphertexts and keys (host [np][N] uint64 buffers).
 //
 // The reference reports failures by exiting the process
 // (include/common/Assert.h:9-21); callers must pass valid inputs.
@@ -607,6 +610,162 @@ int refx_time_boot(void *p, void *in, int min_ks, int warmup, int iters, float *
   Ciphertext<word> res;
   auto &A = *static_cast<Ciphertext<word> *>(in);
   return time_loop(warmup, iters, [&] { R->boot->Boot(res, A, R->ui->GetEvkMap(), min_ks != 0); }, ms);
+}
+
+}  // extern "C"
+
+// ---- the 64-bit word path (Context<uint64_t>, Context.cpp:952) ----
+
+namespace {
+using word64 = uint64_t;
+struct RefCtx64 {
+  std::unique_ptr<Parameter<word64>> param;
+  ContextPtr<word64> ctx;
+  int degree = 0;
+};
+void copy_in64(DeviceVector<word64> &dst, const uint64_t *src, size_t words) {
+  dst.resize(static_cast<int>(words));
+  cudaMemcpy(dst.data(), src, words * 8, cudaMemcpyHostToDevice);
+}
+void copy_out64(uint64_t *dst, const DeviceVector<word64> &src, size_t words) {
+  cudaMemcpy(dst, src.data(), words * 8, cudaMemcpyDeviceToHost);
+}
+void ct_in64(RefCtx64 &R, Ciphertext<word64> &ct, int level, const uint64_t *bx, const uint64_t *ax) {
+  NPInfo np = R.param->LevelToNP(level);
+  ct.RemoveRx();
+  ct.ModifyNP(np);
+  ct.SetScale(R.param->GetScale(std::min(level, R.param->default_encryption_level_)));
+  ct.SetNumSlots(R.degree / 2);
+  const size_t w = poly_words(np, R.degree);
+  copy_in64(ct.bx_, bx, w);
+  copy_in64(ct.ax_, ax, w);
+}
+void key_in64(RefCtx64 &R, EvaluationKey<word64> &k, int beta, const uint64_t *bx, const uint64_t *ax) {
+  NPInfo np(R.param->GetMaxNumMain(), R.param->GetMaxNumTer(), R.param->alpha_);
+  k = EvaluationKey<word64>(np, beta);
+  const size_t w = poly_words(np, R.degree);
+  for (int i = 0; i < beta; i++) {
+    copy_in64(k.bx_.at(i), bx + i * w, w);
+    copy_in64(k.ax_.at(i), ax + i * w, w);
+  }
+}
+}  // namespace
+
+extern "C" {
+
+int refx64_create(int log_degree, int log_scale, int enc_level, int n_levels, const int *level_pairs,
+                  const uint64_t *main_primes, int n_main, const uint64_t *aux_primes, int n_aux,
+                  const uint64_t *ter_primes, int n_ter, int add_main, int add_ter, void **out) {
+  auto *R = new RefCtx64();
+  std::vector<std::pair<int, int>> cfg;
+  for (int i = 0; i < n_levels; i++) cfg.emplace_back(level_pairs[2 * i], level_pairs[2 * i + 1]);
+  std::vector<word64> m(main_primes, main_primes + n_main), a(aux_primes, aux_primes + n_aux),
+      t(ter_primes, ter_primes + n_ter);
+  const double scale = static_cast<double>(UINT64_C(1) << log_scale);
+  R->param = std::make_unique<Parameter<word64>>(log_degree, scale, enc_level, cfg, m, a, t,
+                                                 std::make_pair(add_main, add_ter));
+  R->ctx = Context<word64>::Create(*R->param);
+  R->degree = R->param->degree_;
+  *out = R;
+  return last_cuda();
+}
+
+void refx64_destroy(void *p) {
+  cudaDeviceSynchronize();
+  delete static_cast<RefCtx64 *>(p);
+}
+
+int refx64_ntt(void *p, int num_main, int num_ter, int num_aux, uint64_t *data, int count, int inverse,
+               int montgomery) {
+  auto *R = static_cast<RefCtx64 *>(p);
+  NPInfo np(num_main, num_ter, num_aux);
+  const size_t w = poly_words(np, R->degree);
+  DeviceVector<word64> src(static_cast<int>(w)), dst(static_cast<int>(w));
+  for (int k = 0; k < count; k++) {
+    cudaMemcpy(src.data(), data + k * w, w * 8, cudaMemcpyHostToDevice);
+    DvView<word64> dv = dst.View(num_aux * R->degree);
+    DvConstView<word64> sv = src.ConstView(num_aux * R->degree);
+    if (inverse)
+      R->ctx->ntt_handler_.INTT(dv, np, sv, montgomery != 0);
+    else
+      R->ctx->ntt_handler_.NTT(dv, np, sv, montgomery != 0);
+    cudaMemcpy(data + k * w, dst.data(), w * 8, cudaMemcpyDeviceToHost);
+  }
+  return last_cuda();
+}
+
+int refx64_modup(void *p, int level, const uint64_t *src, uint64_t *out) {
+  auto *R = static_cast<RefCtx64 *>(p);
+  NPInfo np = R->param->LevelToNP(level);
+  const int alpha = R->param->alpha_, q = np.GetNumQ();
+  const int offset = R->param->GetMaxNumTer() - np.num_ter_;
+  const int beta = DivCeil(q + offset, alpha);
+  const size_t nq = static_cast<size_t>(q) * R->degree, nqp = static_cast<size_t>(q + alpha) * R->degree;
+  DeviceVector<word64> s(static_cast<int>(nq));
+  cudaMemcpy(s.data(), src, nq * 8, cudaMemcpyHostToDevice);
+  std::vector<DeviceVector<word64>> tmp;
+  std::vector<DvView<word64>> views;
+  for (int i = 0; i < beta; i++) tmp.emplace_back(static_cast<int>(nqp));
+  for (int i = 0; i < beta; i++) views.push_back(tmp[i].View(alpha * R->degree));
+  R->ctx->mod_switch_handlers_.at(level).ModUp(views, s.ConstView());
+  for (int i = 0; i < beta; i++) copy_out64(out + i * nqp, tmp[i], nqp);
+  return last_cuda();
+}
+
+int refx64_moddown(void *p, int level, int kind, const uint64_t *src, uint64_t *out) {
+  auto *R = static_cast<RefCtx64 *>(p);
+  const int alpha = R->param->alpha_;
+  NPInfo np = R->param->LevelToNP(level);
+  NPInfo src_np = np;
+  if (kind != 1) src_np.num_aux_ = alpha;
+  NPInfo dst_np = kind == 0 ? np : R->param->LevelToNP(level - 1);
+  const size_t ws = poly_words(src_np, R->degree), wd = poly_words(dst_np, R->degree);
+  DeviceVector<word64> s(static_cast<int>(ws)), d(static_cast<int>(wd));
+  cudaMemcpy(s.data(), src, ws * 8, cudaMemcpyHostToDevice);
+  DvView<word64> dv = d.View();
+  DvConstView<word64> sv = s.ConstView(src_np.num_aux_ * R->degree);
+  const auto &ms = R->ctx->mod_switch_handlers_.at(level);
+  if (kind == 0)
+    ms.ModDown(dv, sv);
+  else if (kind == 1)
+    ms.Rescale(dv, sv);
+  else
+    ms.ModDownAndRescale(dv, sv);
+  copy_out64(out, d, wd);
+  return last_cuda();
+}
+
+// HMult (rescale 0/1) of two level-`level` ciphertexts with an imported key
+// ([beta][L + alpha][N] per part); the result's parts go to out_bx / out_ax
+// over the result level's q primes.
+int refx64_hmult(void *p, int level, const uint64_t *a_bx, const uint64_t *a_ax, const uint64_t *b_bx,
+                 const uint64_t *b_ax, int beta, const uint64_t *k_bx, const uint64_t *k_ax, int rescale,
+                 uint64_t *out_bx, uint64_t *out_ax) {
+  auto *R = static_cast<RefCtx64 *>(p);
+  Ciphertext<word64> a, b, res;
+  ct_in64(*R, a, level, a_bx, a_ax);
+  ct_in64(*R, b, level, b_bx, b_ax);
+  EvaluationKey<word64> key;
+  key_in64(*R, key, beta, k_bx, k_ax);
+  R->ctx->HMult(res, a, b, key, rescale != 0);
+  const size_t w = poly_words(res.GetNP(), R->degree);
+  copy_out64(out_bx, res.bx_, w);
+  copy_out64(out_ax, res.ax_, w);
+  return last_cuda();
+}
+
+int refx64_hrot(void *p, int level, const uint64_t *a_bx, const uint64_t *a_ax, int beta, const uint64_t *k_bx,
+                const uint64_t *k_ax, int rot, uint64_t *out_bx, uint64_t *out_ax) {
+  auto *R = static_cast<RefCtx64 *>(p);
+  Ciphertext<word64> a, res;
+  ct_in64(*R, a, level, a_bx, a_ax);
+  EvaluationKey<word64> key;
+  key_in64(*R, key, beta, k_bx, k_ax);
+  R->ctx->HRot(res, a, key, rot);
+  const size_t w = poly_words(res.GetNP(), R->degree);
+  copy_out64(out_bx, res.bx_, w);
+  copy_out64(out_ax, res.ax_, w);
+  return last_cuda();
 }
 
 }  // extern "C"

@@ -82,6 +82,14 @@ def lib():
             "refx_time_hrot": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_float)]),
             "refx_time_ntt_roundtrip": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_float)]),
             "refx_time_boot": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_float)]),
+            "refx64_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, vp, C.c_int, vp, C.c_int,
+                                        vp, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+            "refx64_destroy": (None, [vp]),
+            "refx64_ntt": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, vp, C.c_int, C.c_int, C.c_int]),
+            "refx64_modup": (C.c_int, [vp, C.c_int, vp, vp]),
+            "refx64_moddown": (C.c_int, [vp, C.c_int, C.c_int, vp, vp]),
+            "refx64_hmult": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, C.c_int, vp, vp, C.c_int, vp, vp]),
+            "refx64_hrot": (C.c_int, [vp, C.c_int, vp, vp, C.c_int, vp, vp, C.c_int, vp, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -365,3 +373,79 @@ class RefCiphertext:
         _chk(lib().refx_ct_export(self.ctx.ptr, self.ptr, parts[0].ctypes.data, parts[1].ctypes.data,
                                   parts[2].ctypes.data if len(parts) > 2 else None), "ct export")
         return parts
+
+
+def _u64(a):
+    return np.ascontiguousarray(a, dtype=np.uint64)
+
+
+class RefContext64:
+    """The reference's Context<uint64_t> (the 64-bit word path) on a
+    parameter set with primes up to 2^62; keys and ciphertexts are imported
+    ([np][N] uint64 host arrays)."""
+
+    def __init__(self, params):
+        p = json.loads(params) if isinstance(params, str) else params
+        self.params = p
+        lv = np.array([x for pair in p["level_config"] for x in pair], dtype=np.int32)
+        main, aux = _u64(p["main_primes"]), _u64(p["auxiliary_primes"])
+        ter = _u64(p.get("terminal_primes", []) or [0])
+        n_ter = len(p.get("terminal_primes", []))
+        add = p.get("additional_base", [0, 0])
+        self._keep = (lv, main, aux, ter)
+        self.ptr = C.c_void_p()
+        _chk(lib().refx64_create(p["log_degree"], p["log_default_scale"], p["default_encryption_level"],
+                                 len(p["level_config"]), lv.ctypes.data, main.ctypes.data, len(main),
+                                 aux.ctypes.data, len(aux), ter.ctypes.data, n_ter, add[0], add[1],
+                                 C.byref(self.ptr)), "create64")
+        self.n = 1 << p["log_degree"]
+
+    def close(self):
+        if getattr(self, "ptr", None) is not None and self.ptr.value:
+            lib().refx64_destroy(self.ptr)
+            self.ptr = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def ntt(self, np_, data, inverse=False, mont=False):
+        """NTT / INTT of polynomials [count][rows][N] over NPInfo np_ = (main, ter, aux)."""
+        d = _u64(data).copy()
+        count = d.shape[0] if d.ndim == 3 else 1
+        _chk(lib().refx64_ntt(self.ptr, np_[0], np_[1], np_[2], d.ctypes.data, count, int(inverse), int(mont)),
+             "ntt64")
+        return d
+
+    def modup(self, level, src, beta, rows_out):
+        s = _u64(src)
+        out = np.zeros((beta, rows_out, self.n), dtype=np.uint64)
+        _chk(lib().refx64_modup(self.ptr, level, s.ctypes.data, out.ctypes.data), "modup64")
+        return out
+
+    def moddown(self, level, kind, src, rows_out):
+        s = _u64(src)
+        out = np.zeros((rows_out, self.n), dtype=np.uint64)
+        _chk(lib().refx64_moddown(self.ptr, level, kind, s.ctypes.data, out.ctypes.data), "moddown64")
+        return out
+
+    def hmult(self, level, a, b, key, rescale, rows_out):
+        a0, a1, b0, b1 = (_u64(x) for x in (a[0], a[1], b[0], b[1]))
+        kb, ka = _u64(key[0]), _u64(key[1])
+        ob = np.zeros((rows_out, self.n), dtype=np.uint64)
+        oa = np.zeros_like(ob)
+        _chk(lib().refx64_hmult(self.ptr, level, a0.ctypes.data, a1.ctypes.data, b0.ctypes.data, b1.ctypes.data,
+                                kb.shape[0], kb.ctypes.data, ka.ctypes.data, int(rescale), ob.ctypes.data,
+                                oa.ctypes.data), "hmult64")
+        return ob, oa
+
+    def hrot(self, level, a, key, rot, rows_out):
+        a0, a1 = _u64(a[0]), _u64(a[1])
+        kb, ka = _u64(key[0]), _u64(key[1])
+        ob = np.zeros((rows_out, self.n), dtype=np.uint64)
+        oa = np.zeros_like(ob)
+        _chk(lib().refx64_hrot(self.ptr, level, a0.ctypes.data, a1.ctypes.data, kb.shape[0], kb.ctypes.data,
+                               ka.ctypes.data, rot, ob.ctypes.data, oa.ctypes.data), "hrot64")
+        return ob, oa

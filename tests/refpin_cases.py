@@ -268,6 +268,91 @@ def case_mixed_batch():
     return {"levels": levels, "pairs": len(levels)}
 
 
+def case_w64():
+    """The 64-bit word path against the reference's own Context<uint64_t>
+    on its bootparam_40_64bit.json (40-55-bit main primes, 56-bit auxiliary
+    primes, alpha = 7): NTT / INTT with and without the Montgomery
+    conversion (NTT.cu:606-741), ModUp, ModDown, Rescale and
+    ModDownAndRescale (ModSwitch.cu:429-684) at several levels, HMult with
+    and without rescale and HRot (Context.cpp:776-871) on uniform
+    ciphertexts and uniform keys (both are deterministic functions of their
+    inputs), every word equal."""
+    import torch
+    p = load("bootparam_40_64bit.json")
+    ref = refdrv.RefContext64(p)
+    g = chd.Context64(json.dumps(p))
+    n = g.n
+    primes = g.primes()
+    nt, nm, na = len(p["terminal_primes"]), len(p["main_primes"]), len(p["auxiliary_primes"])
+    L = nt + nm
+    rng = np.random.default_rng(64)
+
+    def rows_of(level, aux):
+        m, t = g.level_np(level)
+        return [nt - t + i for i in range(m + t)] + [L + a for a in range(aux)]
+
+    def uniform(rows):
+        return np.stack([rng.integers(0, int(primes[r]), n, dtype=np.uint64) for r in rows])
+
+    def dev(a):
+        t = torch.from_numpy(np.ascontiguousarray(a).view(np.int64)).cuda()
+        torch.cuda.synchronize()  # the context works on its own stream
+        return t
+
+    def host(t):
+        torch.cuda.synchronize()
+        return t.cpu().numpy().view(np.uint64)
+
+    out = {"params": "bootparam_40_64bit.json", "levels": []}
+    # NTT / INTT over the top level with the auxiliary primes
+    m, t = g.level_np(g.max_level)
+    x = np.stack([uniform(rows_of(g.max_level, na)) for _ in range(2)])
+    for inverse in (False, True):
+        for mont in (False, True):
+            d = dev(x)
+            g.ntt((m, t, na), d, count=2, inverse=inverse, mont=mont)
+            g.synchronize()
+            eq(f"64-bit {'INTT' if inverse else 'NTT'} mont={mont}", host(d).reshape(x.shape),
+               ref.ntt((m, t, na), x, inverse=inverse, mont=mont))
+    beta_max = -(-L // na)
+    kb = np.stack([uniform(rows_of(g.max_level, na)) for _ in range(beta_max)])
+    ka = np.stack([uniform(rows_of(g.max_level, na)) for _ in range(beta_max)])
+    key = chd.EvaluationKey64(g, kb, ka)
+    for lvl in (g.max_level, 17, 9, 3, 1):
+        m, t = g.level_np(lvl)
+        q = m + t
+        beta = -(-q // na)
+        src = uniform(rows_of(lvl, 0))
+        mu = torch.zeros((beta, q + na, n), dtype=torch.int64, device="cuda")
+        g.modup_raw(lvl, dev(src), mu)
+        g.synchronize()
+        eq(f"64-bit ModUp level {lvl}", host(mu), ref.modup(lvl, src, beta, q + na))
+        xa = uniform(rows_of(lvl, na))
+        o = torch.zeros((q, n), dtype=torch.int64, device="cuda")
+        g.moddown_raw(lvl, chd.CHD_MODDOWN, dev(xa), o)
+        g.synchronize()
+        eq(f"64-bit ModDown level {lvl}", host(o), ref.moddown(lvl, 0, xa, q))
+        mq = sum(g.level_np(lvl - 1))
+        o1 = torch.zeros((mq, n), dtype=torch.int64, device="cuda")
+        g.moddown_raw(lvl, chd.CHD_RESCALE, dev(src), o1)
+        g.synchronize()
+        eq(f"64-bit Rescale level {lvl}", host(o1), ref.moddown(lvl, 1, src, mq))
+        g.moddown_raw(lvl, chd.CHD_MODDOWN_RESCALE, dev(xa), o1)
+        g.synchronize()
+        eq(f"64-bit ModDownAndRescale level {lvl}", host(o1), ref.moddown(lvl, 2, xa, mq))
+        a = (uniform(rows_of(lvl, 0)), uniform(rows_of(lvl, 0)))
+        b = (uniform(rows_of(lvl, 0)), uniform(rows_of(lvl, 0)))
+        ga, gb = g.import_ct(lvl, a), g.import_ct(lvl, b)
+        for rescale in (True, False):
+            rows_out = mq if rescale else q
+            eq(f"64-bit HMult level {lvl} rescale {rescale}", g.HMult(ga, gb, key, rescale).numpy(),
+               ref.hmult(lvl, a, b, (kb, ka), rescale, rows_out))
+        for rot in ((1, 5, n // 2 - 1) if lvl in (g.max_level, 3) else (2,)):
+            eq(f"64-bit HRot {rot} level {lvl}", g.HRot(ga, key, rot).numpy(), ref.hrot(lvl, a, (kb, ka), rot, q))
+        out["levels"].append(lvl)
+    return out
+
+
 def case_hoisted():
     """Hoisted rotations: the reference's HoistHandler::EvaluateBabyStep
     (Hoist.cu:578-691; one ModUp, every rotation's key product and
