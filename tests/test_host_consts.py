@@ -13,7 +13,9 @@ import pytest
 import cheddar_b200 as chd
 import pyoracle as po
 
-PARAMS = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "..", "cheddar-fhe_b200", "params", "*.json")))
+# 32-bit word parameter sets (the 64-bit word path has its own parity case)
+PARAMS = sorted(p for p in glob.glob(os.path.join(os.path.dirname(__file__), "..", "cheddar-fhe_b200", "params",
+                                                  "*.json")) if not p.endswith("_64bit.json"))
 
 
 @pytest.mark.parametrize("path", PARAMS, ids=[os.path.basename(p) for p in PARAMS])
