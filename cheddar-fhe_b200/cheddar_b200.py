@@ -9,6 +9,7 @@ marshals arguments.  It raises if the library is missing — there is no CPU
 fallback.
 """
 import ctypes as C
+import json
 import os
 
 import numpy as np
