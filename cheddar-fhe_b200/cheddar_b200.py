@@ -197,6 +197,7 @@ def lib():
         "chd64_hmult": (i, [vp, vp, vp, vp, vp, i]),
         "chd64_hrot": (i, [vp, vp, vp, vp, i]),
         "chd64_rescale": (i, [vp, vp, vp]),
+        "chd64_hconj": (i, [vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -1146,6 +1147,11 @@ class Context64:
     def HRot(self, a, key, rot):
         res = Ciphertext64(self)
         _check(lib().chd64_hrot(self.ptr, res.ptr, a.ptr, key.ptr, rot))
+        return res
+
+    def HConj(self, a, key):
+        res = Ciphertext64(self)
+        _check(lib().chd64_hconj(self.ptr, res.ptr, a.ptr, key.ptr))
         return res
 
     def Rescale(self, a):

@@ -845,13 +845,22 @@ Status Context64::hmult(Ct64 &res, const Ct64 &a, const Ct64 &b, const Evk64 &ke
 
 Status Context64::hrot(Ct64 &res, const Ct64 &a, const Evk64 &key, int dist) {
   // Context::HRot (Context.cpp:776-791): MultKey, then the automorphism
+  const int slots = a.num_slots > 0 ? a.num_slots : P->n / 2;
+  dist %= slots;
+  if (dist < 0) dist += slots;
+  return key_switch_permute(res, a, key, P->galois_of(dist));
+}
+
+Status Context64::hconj(Ct64 &res, const Ct64 &a, const Evk64 &key) {
+  // Context::HConj (Context.cpp:793-798): MultKey, then the conjugation
+  return key_switch_permute(res, a, key, P->galois_of(-1));
+}
+
+Status Context64::key_switch_permute(Ct64 &res, const Ct64 &a, const Evk64 &key, u64 galois) {
   CHD_CHECK(a.np.aux == 0, kErrShape, "HRot: no aux primes");
   const int level = level_of(*P, a);
   CHD_CHECK(level >= 0, kErrInvalidLevel, "HRot: invalid level");
   CHD_CHECK(&res != &a, kErrInvalidArg, "HRot64: the result must not alias the input");
-  const int slots = a.num_slots > 0 ? a.num_slots : P->n / 2;
-  dist %= slots;
-  if (dist < 0) dist += slots;
   const int n = P->n, nq = a.np.q(), tot = nq + P->alpha;
   const size_t qw = static_cast<size_t>(nq) * n, tw_ = static_cast<size_t>(tot) * n;
   u64 *acc = nullptr, *ks = nullptr;
@@ -882,11 +891,11 @@ Status Context64::hrot(Ct64 &res, const Ct64 &a, const Evk64 &key, int dist) {
       e.o0 = (p == 0 ? res.bx : res.ax) + static_cast<size_t>(r) * n;
       e.q = P->primes[g[r]];
       if (eb.count == kMaxElem64Rows) {
-        launch_permute64(eb, P->galois_of(dist), stream);
+        launch_permute64(eb, galois, stream);
         eb.count = 0;
       }
     }
-  launch_permute64(eb, P->galois_of(dist), stream);
+  launch_permute64(eb, galois, stream);
   res.scale = sc;
   res.num_slots = sl;
   cudaFreeAsync(acc, stream);
@@ -1136,6 +1145,15 @@ int chd64_hrot(chd64_context *ctx, chd64_ciphertext *res, const chd64_ciphertext
   CHD64_CTX(ctx);
   if (!res || !a || !key) return fail64(CHD_ERR_INVALID_ARG, "chd64_hrot: null argument");
   const Status s = ctx->c->hrot(res->ct, a->ct, key->k, rot);
+  return s == kOk ? CHD_OK : s;
+} catch (const std::exception &e) {
+  return fail64(CHD_ERR_INTERNAL, e.what());
+}
+
+int chd64_hconj(chd64_context *ctx, chd64_ciphertext *res, const chd64_ciphertext *a, const chd64_evk *key) try {
+  CHD64_CTX(ctx);
+  if (!res || !a || !key) return fail64(CHD_ERR_INVALID_ARG, "chd64_hconj: null argument");
+  const Status s = ctx->c->hconj(res->ct, a->ct, key->k);
   return s == kOk ? CHD_OK : s;
 } catch (const std::exception &e) {
   return fail64(CHD_ERR_INTERNAL, e.what());

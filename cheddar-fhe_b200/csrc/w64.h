@@ -121,6 +121,8 @@ class Context64 {
   // evaluator
   Status hmult(Ct64 &res, const Ct64 &a, const Ct64 &b, const Evk64 &key, bool rescale);
   Status hrot(Ct64 &res, const Ct64 &a, const Evk64 &key, int rot);
+  Status hconj(Ct64 &res, const Ct64 &a, const Evk64 &key);
+  Status key_switch_permute(Ct64 &res, const Ct64 &a, const Evk64 &key, u64 galois);
   Status rescale(Ct64 &res, const Ct64 &a);
   // key switch of d (q primes, NTT domain) with key, plus P (d0, d1) on the
   // q rows (either may be null): acc (b, a) over Q u P

@@ -591,6 +591,8 @@ void chd64_evk_destroy(chd64_evk *key);
 int chd64_hmult(chd64_context *ctx, chd64_ciphertext *res, const chd64_ciphertext *a, const chd64_ciphertext *b,
                 const chd64_evk *key, int rescale);
 int chd64_hrot(chd64_context *ctx, chd64_ciphertext *res, const chd64_ciphertext *a, const chd64_evk *key, int rot);
+/* Context<uint64_t>::HConj (Context.cpp:793-798) with a conjugation key */
+int chd64_hconj(chd64_context *ctx, chd64_ciphertext *res, const chd64_ciphertext *a, const chd64_evk *key);
 int chd64_rescale(chd64_context *ctx, chd64_ciphertext *res, const chd64_ciphertext *a);
 
 #ifdef __cplusplus

@@ -754,6 +754,37 @@ int refx64_hmult(void *p, int level, const uint64_t *a_bx, const uint64_t *a_ax,
   return last_cuda();
 }
 
+int refx64_hconj(void *p, int level, const uint64_t *a_bx, const uint64_t *a_ax, int beta, const uint64_t *k_bx,
+                 const uint64_t *k_ax, uint64_t *out_bx, uint64_t *out_ax) {
+  auto *R = static_cast<RefCtx64 *>(p);
+  Ciphertext<word64> a, res;
+  ct_in64(*R, a, level, a_bx, a_ax);
+  EvaluationKey<word64> key;
+  key_in64(*R, key, beta, k_bx, k_ax);
+  R->ctx->HConj(res, a, key);
+  const size_t w = poly_words(res.GetNP(), R->degree);
+  copy_out64(out_bx, res.bx_, w);
+  copy_out64(out_ax, res.ax_, w);
+  return last_cuda();
+}
+
+// Device time of HMult (rescale 0/1) on imported ciphertexts and key: the
+// average over `iters` calls after `warmup`, CUDA events on the legacy
+// stream.
+int refx64_time_hmult(void *p, int level, const uint64_t *a_bx, const uint64_t *a_ax, const uint64_t *b_bx,
+                      const uint64_t *b_ax, int beta, const uint64_t *k_bx, const uint64_t *k_ax, int rescale,
+                      int warmup, int iters, float *ms) {
+  auto *R = static_cast<RefCtx64 *>(p);
+  Ciphertext<word64> a, b, res;
+  ct_in64(*R, a, level, a_bx, a_ax);
+  ct_in64(*R, b, level, b_bx, b_ax);
+  EvaluationKey<word64> key;
+  key_in64(*R, key, beta, k_bx, k_ax);
+  const int rc = time_loop(warmup, iters, [&] { R->ctx->HMult(res, a, b, key, rescale != 0); }, ms);
+  *ms /= iters;
+  return rc;
+}
+
 int refx64_hrot(void *p, int level, const uint64_t *a_bx, const uint64_t *a_ax, int beta, const uint64_t *k_bx,
                 const uint64_t *k_ax, int rot, uint64_t *out_bx, uint64_t *out_ax) {
   auto *R = static_cast<RefCtx64 *>(p);

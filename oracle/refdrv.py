@@ -90,6 +90,9 @@ def lib():
             "refx64_moddown": (C.c_int, [vp, C.c_int, C.c_int, vp, vp]),
             "refx64_hmult": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, C.c_int, vp, vp, C.c_int, vp, vp]),
             "refx64_hrot": (C.c_int, [vp, C.c_int, vp, vp, C.c_int, vp, vp, C.c_int, vp, vp]),
+            "refx64_hconj": (C.c_int, [vp, C.c_int, vp, vp, C.c_int, vp, vp, vp, vp]),
+            "refx64_time_hmult": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, C.c_int, vp, vp, C.c_int, C.c_int, C.c_int,
+                                            C.POINTER(C.c_float)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -449,3 +452,22 @@ class RefContext64:
         _chk(lib().refx64_hrot(self.ptr, level, a0.ctypes.data, a1.ctypes.data, kb.shape[0], kb.ctypes.data,
                                ka.ctypes.data, rot, ob.ctypes.data, oa.ctypes.data), "hrot64")
         return ob, oa
+
+    def hconj(self, level, a, key, rows_out):
+        a0, a1 = _u64(a[0]), _u64(a[1])
+        kb, ka = _u64(key[0]), _u64(key[1])
+        ob = np.zeros((rows_out, self.n), dtype=np.uint64)
+        oa = np.zeros_like(ob)
+        _chk(lib().refx64_hconj(self.ptr, level, a0.ctypes.data, a1.ctypes.data, kb.shape[0], kb.ctypes.data,
+                                ka.ctypes.data, ob.ctypes.data, oa.ctypes.data), "hconj64")
+        return ob, oa
+
+    def time_hmult(self, level, a, b, key, rescale=True, warmup=3, iters=20):
+        """Device milliseconds per HMult of the reference's 64-bit build."""
+        a0, a1, b0, b1 = (_u64(x) for x in (a[0], a[1], b[0], b[1]))
+        kb, ka = _u64(key[0]), _u64(key[1])
+        ms = C.c_float()
+        _chk(lib().refx64_time_hmult(self.ptr, level, a0.ctypes.data, a1.ctypes.data, b0.ctypes.data,
+                                     b1.ctypes.data, kb.shape[0], kb.ctypes.data, ka.ctypes.data, int(rescale),
+                                     warmup, iters, C.byref(ms)), "time_hmult64")
+        return ms.value

@@ -274,7 +274,7 @@ def case_w64():
     primes, alpha = 7): NTT / INTT with and without the Montgomery
     conversion (NTT.cu:606-741), ModUp, ModDown, Rescale and
     ModDownAndRescale (ModSwitch.cu:429-684) at several levels, HMult with
-    and without rescale and HRot (Context.cpp:776-871) on uniform
+    and without rescale, HRot and HConj (Context.cpp:776-871) on uniform
     ciphertexts and uniform keys (both are deterministic functions of their
     inputs), every word equal."""
     import torch
@@ -349,6 +349,7 @@ def case_w64():
                ref.hmult(lvl, a, b, (kb, ka), rescale, rows_out))
         for rot in ((1, 5, n // 2 - 1) if lvl in (g.max_level, 3) else (2,)):
             eq(f"64-bit HRot {rot} level {lvl}", g.HRot(ga, key, rot).numpy(), ref.hrot(lvl, a, (kb, ka), rot, q))
+        eq(f"64-bit HConj level {lvl}", g.HConj(ga, key).numpy(), ref.hconj(lvl, a, (kb, ka), q))
         out["levels"].append(lvl)
     return out
 
