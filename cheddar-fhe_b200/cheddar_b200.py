@@ -1107,9 +1107,12 @@ class Context64:
         self.alpha = lib().chd64_alpha(self.ptr)
 
     def __del__(self):
-        if getattr(self, "ptr", None) is not None and self.ptr.value:
-            lib().chd64_context_destroy(self.ptr)
-            self.ptr = C.c_void_p()
+        try:
+            if getattr(self, "ptr", None) is not None and self.ptr.value:
+                lib().chd64_context_destroy(self.ptr)
+                self.ptr = C.c_void_p()
+        except Exception:  # interpreter teardown
+            pass
 
     def synchronize(self):
         _check(lib().chd64_context_synchronize(self.ptr))
@@ -1139,23 +1142,23 @@ class Context64:
     def import_ct(self, level, parts, scale=1.0, num_slots=None, on_device=False):
         return Ciphertext64(self).load(level, parts, scale, num_slots, on_device)
 
-    def HMult(self, a, b, key, rescale=True):
-        res = Ciphertext64(self)
+    def HMult(self, a, b, key, rescale=True, res=None):
+        res = res or Ciphertext64(self)
         _check(lib().chd64_hmult(self.ptr, res.ptr, a.ptr, b.ptr, key.ptr, int(rescale)))
         return res
 
-    def HRot(self, a, key, rot):
-        res = Ciphertext64(self)
+    def HRot(self, a, key, rot, res=None):
+        res = res or Ciphertext64(self)
         _check(lib().chd64_hrot(self.ptr, res.ptr, a.ptr, key.ptr, rot))
         return res
 
-    def HConj(self, a, key):
-        res = Ciphertext64(self)
+    def HConj(self, a, key, res=None):
+        res = res or Ciphertext64(self)
         _check(lib().chd64_hconj(self.ptr, res.ptr, a.ptr, key.ptr))
         return res
 
-    def Rescale(self, a):
-        res = Ciphertext64(self)
+    def Rescale(self, a, res=None):
+        res = res or Ciphertext64(self)
         _check(lib().chd64_rescale(self.ptr, res.ptr, a.ptr))
         return res
 
@@ -1167,9 +1170,12 @@ class Ciphertext64:
         _check(lib().chd64_ct_create(ctx.ptr, C.byref(self.ptr)))
 
     def __del__(self):
-        if getattr(self, "ptr", None) is not None and self.ptr.value:
-            lib().chd64_ct_destroy(self.ptr)
-            self.ptr = C.c_void_p()
+        try:
+            if getattr(self, "ptr", None) is not None and self.ptr.value:
+                lib().chd64_ct_destroy(self.ptr)
+                self.ptr = C.c_void_p()
+        except Exception:  # interpreter teardown
+            pass
 
     def load(self, level, parts, scale=1.0, num_slots=None, on_device=False):
         ns = self.ctx.n // 2 if num_slots is None else num_slots
@@ -1213,6 +1219,9 @@ class EvaluationKey64:
         del keep
 
     def __del__(self):
-        if getattr(self, "ptr", None) is not None and self.ptr.value:
-            lib().chd64_evk_destroy(self.ptr)
-            self.ptr = C.c_void_p()
+        try:
+            if getattr(self, "ptr", None) is not None and self.ptr.value:
+                lib().chd64_evk_destroy(self.ptr)
+                self.ptr = C.c_void_p()
+        except Exception:  # interpreter teardown
+            pass
