@@ -242,19 +242,33 @@ __global__ void __launch_bounds__(256) k64_inv_cols(const __grid_constant__ RowB
   }
 }
 
-// base conversion: one thread per coefficient and target
+// base conversion: a thread loads its coefficient's K sources once and
+// produces every target; the table and the targets' primes sit in shared
+// memory
 __global__ void __launch_bounds__(256) k64_bconv(const __grid_constant__ BConv64Batch b) {
-  const BConv64Job &j = b.jobs[blockIdx.z];
-  const int m = blockIdx.y;
-  if (m >= j.M) return;
+  __shared__ i64 tab[64 * 16];
+  __shared__ u64 sp[64];
+  __shared__ i64 sq[64];
+  const BConv64Job &j = b.jobs[blockIdx.y];
+  const int K = j.K, M = j.M;
+  for (int t = threadIdx.x; t < M * K; t += blockDim.x) tab[t] = j.table[t];
+  for (int t = threadIdx.x; t < M; t += blockDim.x) {
+    sp[t] = b.primes[j.out_gidx[t]];
+    sq[t] = b.qinvs[j.out_gidx[t]];
+  }
+  __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int g = j.out_gidx[m];
-  const u64 p = b.primes[g];
-  const i64 pinv = b.qinvs[g];
-  i128 acc = 0;
-  for (int k = 0; k < j.K; k++)
-    acc += static_cast<i128>(j.xt[(static_cast<size_t>(k) << 16) + i]) * j.table[m * j.K + k];
-  j.out[(static_cast<size_t>(j.out_row[m]) << 16) + i] = redc(acc, p, pinv);
+  i64 x[16];
+#pragma unroll
+  for (int k = 0; k < 16; k++) x[k] = k < K ? j.xt[(static_cast<size_t>(k) << 16) + i] : 0;
+  for (int m = 0; m < M; m++) {
+    const i64 *tm = tab + m * K;
+    i128 acc = 0;
+#pragma unroll
+    for (int k = 0; k < 16; k++)
+      if (k < K) acc += static_cast<i128>(x[k]) * tm[k];
+    j.out[(static_cast<size_t>(j.out_row[m]) << 16) + i] = redc(acc, sp[m], sq[m]);
+  }
 }
 
 __global__ void __launch_bounds__(256) k64_tensor(const __grid_constant__ Elem64Batch b) {
@@ -314,9 +328,7 @@ void launch_ntt64_inv(const RowBatch64 &rb, cudaStream_t s) {
 
 void launch_bconv64(const BConv64Batch &b, cudaStream_t s) {
   if (b.count <= 0) return;
-  int max_m = 0;
-  for (int j = 0; j < b.count; j++) max_m = b.jobs[j].M > max_m ? b.jobs[j].M : max_m;
-  k64_bconv<<<dim3(65536 / 256, max_m, b.count), 256, 0, s>>>(b);
+  k64_bconv<<<dim3(65536 / 256, b.count), 256, 0, s>>>(b);
 }
 
 void launch_tensor64(const Elem64Batch &b, cudaStream_t s) {
