@@ -268,6 +268,11 @@ def main():
 
     # ---- hoisted rotations and a mixed-level batch ----
     hoist_mixed = hoist_mixed_bench(ctx, chd, key, uniform, stream)
+    # ---- the 64-bit word path ----
+    try:
+        w64 = w64_bench(chd, stream)
+    except Exception as e:  # reported, not fatal: the headline is the 32-bit path
+        w64 = {"failed": str(e)[:300]}
 
     # ---- full-slot bootstrapping at N = 2^16 ----
     boot = None if args.no_boot else boot_bench(chd, args, stream, dist)
@@ -282,7 +287,7 @@ def main():
                    "parallelism": f"replicas x{world}"},
         "e2e": e2e, "roofline": roof, "clocks": sampler.summary(), "ks_engine": args.ks_engine,
         "ks_engines": ks_cmp, "bconv_engines": bconv_cmp, "ntt": ntt_cmp,
-        "bootstrap": boot, "hoisted_and_mixed": hoist_mixed,
+        "bootstrap": boot, "hoisted_and_mixed": hoist_mixed, "w64": w64,
         "gpu_launches": launches,
     }
     # the autotuner's choice per column-pass launch shape (largest source
@@ -305,6 +310,10 @@ def main():
             pass
         try:
             ref["boot_ours_over_reference"] = (ref["bootstrap"]["hoisted"]["ms_per_boot"] / boot["ms_per_boot"])
+        except (KeyError, TypeError, ZeroDivisionError):
+            pass
+        try:
+            ref["hmult64_ours_over_reference"] = ref["hmult64"]["ms_per_hmult"] / w64["ms_per_hmult"]
         except (KeyError, TypeError, ZeroDivisionError):
             pass
         line["reference_gpu"] = ref
@@ -648,7 +657,8 @@ def reference_gpu_run(args):
     HMult+relin+rescale at the top level of the key-switching set (`batch`
     distinct pairs per step, one HMult per call: the reference has no
     batched entry point), the 24-prime NTT round trip, and full-slot
-    bootstrapping of bootparam_40.json (hoisted and min-KS).  Each workload
+    bootstrapping of bootparam_40.json (hoisted and min-KS), and the 64-bit
+    word path's HMult on bootparam_40_64bit.json.  Each workload
     runs in its own process (the reference keeps per-parameter-set state
     process-wide); CUDA events on the legacy stream the reference uses."""
     script = os.path.join(ROOT, "oracle", "ref_bench.py")
@@ -659,6 +669,7 @@ def reference_gpu_run(args):
             ("ntt_one_polynomial", ["ntt", "24", "1", "100", "3"])]
     if not args.no_boot:
         jobs.append(("bootstrap", ["boot", BOOT_PARAM_FILE, "5", "2"]))
+    jobs.append(("hmult64", ["hmult64", W64_PARAM_FILE, "20", "3"]))
     out = {"build": "the reference's src/core, src/extension, src/UserInterface.cu compiled for sm_100a "
                     "(oracle/Makefile target ref) with project-written rmm / libtommath stand-ins"}
     for name, argv in jobs:
@@ -827,6 +838,40 @@ def hoist_mixed_bench(ctx, chd, key, uniform, stream, reps=5):
 
 
 BOOT_PARAM_FILE = "bootparam_40.json"
+W64_PARAM_FILE = "bootparam_40_64bit.json"
+
+
+def w64_bench(chd, stream, steps=20, warmup=3):
+    """The 64-bit word path: HMult+relin+rescale of one pair at the top level
+    of the reference's bootparam_40_64bit.json (26 main primes of 40-55 bits,
+    7 auxiliary of 56 bits, dnum 4), uniform ciphertexts and key (the same
+    residues ref_bench.py gives the reference), CUDA events on the stream the
+    context runs on, the result buffer reused."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from ref_bench import w64_inputs
+    p = json.load(open(os.path.join(chd.PARAM_DIR, W64_PARAM_FILE)))
+    g = chd.Context64(json.dumps(p))
+    g.set_stream(stream.cuda_stream)
+    a, b, key = w64_inputs(p)
+    lvl = g.max_level
+    ga, gb = g.import_ct(lvl, a), g.import_ct(lvl, b)
+    k = chd.EvaluationKey64(g, key[0], key[1])
+    r = chd.Ciphertext64(g)
+    for _ in range(warmup):
+        g.HMult(ga, gb, k, True, res=r)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        g.HMult(ga, gb, k, True, res=r)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    g.set_stream(None)
+    return {"workload": f"64-bit word path: HMult+relin+rescale at the top level of {W64_PARAM_FILE}",
+            "ms_per_hmult": ms, "hmult_per_s": 1e3 / ms, "steps": steps,
+            "kernels": "unfused: two-pass NTT, exact 128-bit base conversion, element-wise"}
 
 
 def _peaks():

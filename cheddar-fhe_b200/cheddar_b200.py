@@ -180,6 +180,7 @@ def lib():
         "chd64_context_create_json": (i, [C.c_char_p, i, pp]),
         "chd64_context_destroy": (None, [vp]),
         "chd64_context_synchronize": (i, [vp]),
+        "chd64_context_set_stream": (i, [vp, vp]),
         "chd64_max_level": (i, [vp]),
         "chd64_alpha": (i, [vp]),
         "chd64_level_np": (i, [vp, i, C.POINTER(i), C.POINTER(i)]),
@@ -1116,6 +1117,11 @@ class Context64:
 
     def synchronize(self):
         _check(lib().chd64_context_synchronize(self.ptr))
+
+    def set_stream(self, stream_handle):
+        """Run this context's work on the given CUDA stream (an int handle,
+        e.g. torch.cuda.Stream().cuda_stream); None restores its own."""
+        _check(lib().chd64_context_set_stream(self.ptr, stream_handle))
 
     def level_np(self, level):
         m, t = C.c_int(), C.c_int()

@@ -424,7 +424,7 @@ Context64::~Context64() {
   cudaFree(d_qinv);
   cudaFree(d_tw);
   cudaFree(d_itw);
-  if (stream) cudaStreamDestroy(stream);
+  if (stream && own_stream) cudaStreamDestroy(stream);
 }
 
 Status Context64::check(const char *where) {
@@ -978,6 +978,23 @@ int chd64_context_synchronize(chd64_context *ctx) try {
   CHD64_CTX(ctx);
   const cudaError_t e = cudaStreamSynchronize(ctx->c->stream);
   return e == cudaSuccess ? CHD_OK : fail64(CHD_ERR_CUDA, cudaGetErrorString(e));
+} catch (const std::exception &e) {
+  return fail64(CHD_ERR_INTERNAL, e.what());
+}
+
+int chd64_context_set_stream(chd64_context *ctx, void *cuda_stream) try {
+  CHD64_CTX(ctx);
+  Context64 &C = *ctx->c;
+  cudaStreamSynchronize(C.stream);
+  if (cuda_stream) {
+    if (C.own_stream) cudaStreamDestroy(C.stream);
+    C.own_stream = false;
+    C.stream = static_cast<cudaStream_t>(cuda_stream);
+  } else if (!C.own_stream) {
+    cudaStreamCreateWithFlags(&C.stream, cudaStreamNonBlocking);
+    C.own_stream = true;
+  }
+  return CHD_OK;
 } catch (const std::exception &e) {
   return fail64(CHD_ERR_INTERNAL, e.what());
 }

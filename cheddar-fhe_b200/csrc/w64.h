@@ -98,6 +98,7 @@ class Context64 {
   std::unique_ptr<Params64> P;
   int device = 0;
   cudaStream_t stream = nullptr;
+  bool own_stream = true;
   u64 *d_primes = nullptr;
   i64 *d_qinv = nullptr;
   ulonglong2 *d_tw = nullptr, *d_itw = nullptr;  // [nprimes][N] (w, floor(w 2^64 / q))

@@ -557,6 +557,8 @@ typedef struct chd64_evk chd64_evk;
 int chd64_context_create_json(const char *json, int device, chd64_context **out);
 void chd64_context_destroy(chd64_context *ctx);
 int chd64_context_synchronize(chd64_context *ctx);
+/* work of the context on the caller's stream (NULL: back to its own) */
+int chd64_context_set_stream(chd64_context *ctx, void *cuda_stream);
 int chd64_max_level(const chd64_context *ctx);
 int chd64_alpha(const chd64_context *ctx);
 int chd64_level_np(const chd64_context *ctx, int level, int *num_main, int *num_ter);

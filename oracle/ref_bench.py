@@ -8,6 +8,7 @@ not the library's.
     python oracle/ref_bench.py hmult <param file> <pairs> <steps> <warmup>
     python oracle/ref_bench.py ntt <primes> <polys> <steps> <warmup>
     python oracle/ref_bench.py boot <param file> <steps> <warmup>
+    python oracle/ref_bench.py hmult64 <param file> <steps> <warmup>
 
 Device time by CUDA events on the legacy stream the reference issues its
 work on (the reference runs one ciphertext per call; it has no batched
@@ -79,6 +80,33 @@ def boot(name, steps, warmup):
     return out
 
 
+def w64_inputs(p, seed=1):
+    """Uniform level-max ciphertext pair and key of the 64-bit word path
+    (the same residues for the reference and the library)."""
+    n = 1 << p["log_degree"]
+    primes = list(reversed(p.get("terminal_primes", []))) + p["main_primes"] + p["auxiliary_primes"]
+    na, L = len(p["auxiliary_primes"]), len(p["main_primes"]) + len(p.get("terminal_primes", []))
+    rng = np.random.default_rng(seed)
+
+    def uni(rows):
+        return np.stack([rng.integers(0, primes[r], n, dtype=np.uint64) for r in rows])
+    beta = -(-L // na)
+    key = (np.stack([uni(range(L + na)) for _ in range(beta)]), np.stack([uni(range(L + na)) for _ in range(beta)]))
+    a = (uni(range(L)), uni(range(L)))
+    b = (uni(range(L)), uni(range(L)))
+    return a, b, key
+
+
+def hmult64(name, steps, warmup):
+    p = _params(name)
+    r = refdrv.RefContext64(p)
+    a, b, key = w64_inputs(p)
+    lvl = len(p["level_config"]) - 1
+    ms = r.time_hmult(lvl, a, b, key, True, warmup, steps)
+    return {"workload": f"64-bit word path: HMult+relin+rescale at the top level of {name}", "steps": steps,
+            "ms_per_hmult": ms, "hmult_per_s": 1e3 / ms}
+
+
 def main(argv):
     kind = argv[1]
     if kind == "hmult":
@@ -87,6 +115,8 @@ def main(argv):
         res = ntt(int(argv[2]), int(argv[3]), int(argv[4]), int(argv[5]))
     elif kind == "boot":
         res = boot(argv[2], int(argv[3]), int(argv[4]))
+    elif kind == "hmult64":
+        res = hmult64(argv[2], int(argv[3]), int(argv[4]))
     else:
         raise SystemExit(f"unknown workload {kind}")
     print(json.dumps({"reference_gpu": kind, **res}), flush=True)
