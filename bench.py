@@ -143,8 +143,10 @@ def run_reference(args):
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": f"{total_n} HMults of the CPU oracle (OpenMP over limbs)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "the reference is GPU-only (no CPU implementation) and needs rmm/libtommath, which "
-                "cannot be built here; the CPU arm is the oracle port of its algorithm",
+        "note": "the reference has no CPU implementation of this path (its evaluator runs only on "
+                "the GPU: compiled from its sources with rmm / libtommath stand-ins, it is timed on the "
+                "same GPU in the main arm's reference_gpu); the CPU arm is the oracle port of its "
+                "algorithm",
     }
     print(json.dumps(line))
     return 0
@@ -844,16 +846,25 @@ W64_PARAM_FILE = "bootparam_40_64bit.json"
 def w64_bench(chd, stream, steps=20, warmup=3):
     """The 64-bit word path: HMult+relin+rescale of one pair at the top level
     of the reference's bootparam_40_64bit.json (26 main primes of 40-55 bits,
-    7 auxiliary of 56 bits, dnum 4), uniform ciphertexts and key (the same
-    residues ref_bench.py gives the reference), CUDA events on the stream the
-    context runs on, the result buffer reused."""
+    7 auxiliary of 56 bits, dnum 4), uniform ciphertexts and key from the
+    generator and seed the reference's timing uses, CUDA events on the stream
+    the context runs on, the result buffer reused."""
+    import numpy as np
     import torch
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    from ref_bench import w64_inputs
     p = json.load(open(os.path.join(chd.PARAM_DIR, W64_PARAM_FILE)))
     g = chd.Context64(json.dumps(p))
     g.set_stream(stream.cuda_stream)
-    a, b, key = w64_inputs(p)
+    n = g.n
+    primes = [int(x) for x in g.primes()]
+    na, L = len(p["auxiliary_primes"]), len(p["main_primes"]) + len(p.get("terminal_primes", []))
+    rng = np.random.default_rng(1)
+
+    def uni(rows):
+        return np.stack([rng.integers(0, primes[r], n, dtype=np.uint64) for r in rows])
+    beta = -(-L // na)
+    key = (np.stack([uni(range(L + na)) for _ in range(beta)]), np.stack([uni(range(L + na)) for _ in range(beta)]))
+    a = (uni(range(L)), uni(range(L)))
+    b = (uni(range(L)), uni(range(L)))
     lvl = g.max_level
     ga, gb = g.import_ct(lvl, a), g.import_ct(lvl, b)
     k = chd.EvaluationKey64(g, key[0], key[1])
