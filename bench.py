@@ -299,6 +299,10 @@ def main():
         f"{({0: 'cuda_core', 1: 'tensor_core', 3: 'tensor_core_wide', 4: 'tensor_core_wide_128regs'}).get(t['engine'], t['engine'])}"
         f"/split{t['split']}"
         for t in chd.ks_tuned_shapes()]
+    # the row pass's choice per shape (ciphertexts, rows, mode) -> variant
+    line["config"]["autotuned_row_passes"] = [
+        f"cts{t['cts']} rows{t['rows']} mode{t['mode']}: {'prefetch' if t['prefetch'] else 'in_place_loads'}"
+        for t in chd.ks_rows_tuned_shapes()]
     if rank == 0 and world == 1 and not args.no_reference_gpu:
         ref = reference_gpu_run(args)
         try:

@@ -125,6 +125,7 @@ def lib():
         "chd_decode": (i, [vp, i, C.c_double, vp, i, vp, vp]),
         "chd_evk_info": (i, [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(i)]),
         "chd_ks_tuned_shapes": (i, [vp, i]),
+        "chd_ks_rows_tuned_shapes": (i, [vp, i]),
         "chd_moddown_batch": (i, [vp, i, vp, vp]),
         "chd_ct_serialize": (i, [vp, vp, vp, C.c_size_t, C.POINTER(C.c_size_t)]),
         "chd_ct_deserialize": (i, [vp, vp, vp, C.c_size_t]),
@@ -233,6 +234,17 @@ def ks_tuned_shapes():
     n = lib().chd_ks_tuned_shapes(out, n)
     return [dict(device=out[6 * i], K=out[6 * i + 1], jobs=out[6 * i + 2], M=out[6 * i + 3],
                  engine=out[6 * i + 4], split=out[6 * i + 5]) for i in range(n)]
+
+
+def ks_rows_tuned_shapes():
+    """The key-switch row pass's autotuned choices in this process: one dict
+    per launch shape with `prefetch` True when the variant that loads ahead
+    won."""
+    n = lib().chd_ks_rows_tuned_shapes(None, 0)
+    out = (C.c_int * (5 * max(1, n)))()
+    n = lib().chd_ks_rows_tuned_shapes(out, n)
+    return [dict(device=out[5 * i], cts=out[5 * i + 1], rows=out[5 * i + 2], mode=out[5 * i + 3],
+                 prefetch=bool(out[5 * i + 4])) for i in range(n)]
 
 
 def load_params(name_or_path):

@@ -375,6 +375,8 @@ int chd_get_ks_engine(const chd_context *ctx) { return ctx ? ctx->c->ks_engine :
 
 int chd_ks_tuned_shapes(int *out, int cap) { return modswitch_tuned_shapes(out, cap); }
 
+int chd_ks_rows_tuned_shapes(int *out, int cap) { return ks_rows_tuned_shapes(out, cap); }
+
 int chd_stage_times(chd_context *ctx, double *ms, int *launches) try {
   CHD_CTX(ctx);
   if (!ms || !launches) return fail(CHD_ERR_INVALID_ARG, "chd_stage_times: null output");

@@ -1341,7 +1341,7 @@ Status Context::key_switch_fused_levels(const int *levels, int count, const KSIn
     t0 = timer_mark();
     auto flush = [&]() {
       if (d.count == 0) return;
-      launch_ks_rows(d, P->log_n, stream);
+      launch_ks_rows(d, P->log_n, stream, ks_engine == 2);
       nl++;
       d.count = d.nlv = d.max_rows = 0;
       lv_of.clear();

@@ -218,7 +218,12 @@ struct KSRowsDesc {
   KSRowsLevel lv[kMaxKSRowsLevels];
   KSRowsCt ct[kMaxKSRowsCts];
 };
-void launch_ks_rows(const KSRowsDesc &d, int log_n, cudaStream_t s);
+// tune: pick the row-pass variant per launch shape by timing both once
+// (the context's CHD_BCONV_AUTO); otherwise the one without prefetching
+void launch_ks_rows(const KSRowsDesc &d, int log_n, cudaStream_t s, bool tune = false);
+// the row-pass choices cached so far: 5 ints per shape (device, ciphertexts,
+// largest row count, mode, prefetching variant); returns the count
+int ks_rows_tuned_shapes(int *out, int cap);
 
 // Key-switching inner product with the P * (d0, d1) term folded in:
 //   acc_b[r] = sum_i mu_i[r] * kb_i[r] + (r < nq ? p_prod[r] * d0[r] : 0)

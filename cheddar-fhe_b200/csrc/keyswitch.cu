@@ -16,6 +16,10 @@
 // evaluation-domain accumulator (kept primes, consumed by the ModDown
 // epilogue) or the INTT row-phase output (dropped primes, consumed by the
 // ModDown column pass).
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include "arith.cuh"
 #include "kernels.h"
 #include "ntt_common.cuh"
@@ -23,7 +27,12 @@
 namespace chd {
 namespace {
 
-__global__ void __launch_bounds__(256, 3) k_ks_rows(const __grid_constant__ KSRowsDesc d) {
+// PREFETCH: each digit's key words are loaded before its row NTT and the
+// next digit's ModUp row during it (more loads in flight per warp, sized for
+// 2 CTAs per SM); otherwise each load is issued where it is used (3 CTAs per
+// SM).  Both compute the same words; the launcher picks per launch shape.
+template <bool PREFETCH>
+__global__ void __launch_bounds__(256, PREFETCH ? 2 : 3) k_ks_rows(const __grid_constant__ KSRowsDesc d) {
   __shared__ uint32_t sm[4][512];
   // grid (count, 32, max_rows): the ciphertexts sharing one key row are
   // neighbours in launch order, so the key row comes from HBM once
@@ -51,24 +60,45 @@ __global__ void __launch_bounds__(256, 3) k_ks_rows(const __grid_constant__ KSRo
   uint32_t sb[8], sa[8];
 #pragma unroll
   for (int k = 0; k < 8; k++) sb[k] = sa[k] = 0;
+  const int own = L.own_digit[j];
+  auto load_mu = [&](int i, uint32_t (&x)[8]) {
+    const uint32_t *src = c.mu[i] + static_cast<size_t>(j) * 65536 + r * 512;
+#pragma unroll
+    for (int k = 0; k < 8; k++) x[k] = src[t + 64 * k];
+  };
+  uint32_t vn[8];
+  if (PREFETCH && L.beta > 0 && own != 0) load_mu(0, vn);
   for (int i = 0; i < L.beta; i++) {
+    uint32_t kb[8], ka[8];
+    if (PREFETCH) {
+      ld8(L.kb[i] + koff, kb);
+      ld8(L.ka[i] + koff, ka);
+    }
     uint32_t v[8];
-    if (L.own_digit[j] == i) {
+    const bool mine = own == i;
+    if (PREFETCH) {
+      if (!mine) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) v[k] = vn[k];
+      }
+      if (i + 1 < L.beta && own != i + 1) load_mu(i + 1, vn);
+    } else if (!mine) {
+      load_mu(i, v);
+    }
+    if (mine) {
       // own primes of the digit: the ModUp value is the key-switched input
 #pragma unroll
       for (int k = 0; k < 8; k++) v[k] = mode == 0 ? mont_mul(a1[k], a2[k], q, qi) : (mode == 1 ? a1[k] : a2[k]);
     } else {
-      const uint32_t *src = c.mu[i] + static_cast<size_t>(j) * 65536 + r * 512;
-#pragma unroll
-      for (int k = 0; k < 8; k++) v[k] = src[t + 64 * k];
       row_fwd(v, srow, tw, r, t, q, 1 + rl);
 #pragma unroll
       for (int k = 0; k < 8; k++) v[k] = reduce2q(v[k], q);
       row_sync(1 + rl);
     }
-    uint32_t kb[8], ka[8];
-    ld8(L.kb[i] + koff, kb);
-    ld8(L.ka[i] + koff, ka);
+    if (!PREFETCH) {
+      ld8(L.kb[i] + koff, kb);
+      ld8(L.ka[i] + koff, ka);
+    }
 #pragma unroll
     for (int k = 0; k < 8; k++) {
       sb[k] = add_mod(sb[k], mont_mul(v[k], kb[k], q, qi), q);
@@ -121,9 +151,92 @@ __global__ void __launch_bounds__(256, 3) k_ks_rows(const __grid_constant__ KSRo
 
 }  // namespace
 
-void launch_ks_rows(const KSRowsDesc &d, int log_n, cudaStream_t s) {
+namespace {
+// Autotuning of the row pass (with the column passes' CHD_BCONV_AUTO): the
+// first launch of a shape (device, ciphertexts, largest row count, mode)
+// outside a stream capture times both variants three times, interleaved,
+// after a warm-up, and caches the faster; every launch writes the same
+// words, so the timing launches leave the right outputs.
+std::mutex g_ksr_mu;
+std::map<std::tuple<int, int, int, int>, bool> g_ksr_cache;
+
+void launch_variant(const KSRowsDesc &d, bool prefetch, cudaStream_t s) {
+  const dim3 grid(d.count, 32, d.max_rows);
+  if (prefetch)
+    k_ks_rows<true><<<grid, 256, 0, s>>>(d);
+  else
+    k_ks_rows<false><<<grid, 256, 0, s>>>(d);
+}
+}  // namespace
+
+void launch_ks_rows(const KSRowsDesc &d, int log_n, cudaStream_t s, bool tune) {
   if (d.count <= 0 || d.max_rows <= 0 || log_n != 16) return;
-  k_ks_rows<<<dim3(d.count, 32, d.max_rows), 256, 0, s>>>(d);
+  if (!tune) {
+    launch_variant(d, false, s);
+    return;
+  }
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const auto key = std::make_tuple(dev, d.count, d.max_rows, d.mode);
+  {
+    std::lock_guard<std::mutex> lock(g_ksr_mu);
+    auto it = g_ksr_cache.find(key);
+    if (it != g_ksr_cache.end()) {
+      launch_variant(d, it->second, s);
+      return;
+    }
+  }
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+    launch_variant(d, false, s);
+    return;
+  }
+  cudaEvent_t ev[7] = {};
+  for (auto &e : ev)
+    if (cudaEventCreate(&e) != cudaSuccess) {
+      for (auto &f : ev)
+        if (f) cudaEventDestroy(f);
+      launch_variant(d, false, s);
+      return;
+    }
+  launch_variant(d, false, s);
+  launch_variant(d, true, s);
+  cudaEventRecord(ev[0], s);
+  for (int r = 0; r < 3; r++) {
+    launch_variant(d, false, s);
+    cudaEventRecord(ev[2 * r + 1], s);
+    launch_variant(d, true, s);
+    cudaEventRecord(ev[2 * r + 2], s);
+  }
+  bool ok = cudaEventSynchronize(ev[6]) == cudaSuccess;
+  float best[2] = {1e30f, 1e30f};
+  for (int r = 0; ok && r < 3; r++)
+    for (int v = 0; ok && v < 2; v++) {
+      float t = 0.f;
+      ok = cudaEventElapsedTime(&t, ev[2 * r + v], ev[2 * r + v + 1]) == cudaSuccess;
+      best[v] = t < best[v] ? t : best[v];
+    }
+  for (auto &e : ev) cudaEventDestroy(e);
+  if (ok) {
+    std::lock_guard<std::mutex> lock(g_ksr_mu);
+    g_ksr_cache[key] = best[1] < best[0];
+  }
+}
+
+int ks_rows_tuned_shapes(int *out, int cap) {
+  std::lock_guard<std::mutex> lock(g_ksr_mu);
+  int k = 0;
+  for (const auto &e : g_ksr_cache) {
+    if (out && k < cap) {
+      out[5 * k] = std::get<0>(e.first);
+      out[5 * k + 1] = std::get<1>(e.first);
+      out[5 * k + 2] = std::get<2>(e.first);
+      out[5 * k + 3] = std::get<3>(e.first);
+      out[5 * k + 4] = e.second ? 1 : 0;
+    }
+    k++;
+  }
+  return k;
 }
 
 }  // namespace chd

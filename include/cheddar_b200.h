@@ -444,9 +444,18 @@ int chd_set_ks_engine(chd_context *ctx, int engine);
 int chd_get_ks_engine(const chd_context *ctx);
 /* The autotuner's choices so far (no reference counterpart): per launch
  * shape six ints (device, largest source count K, jobs, largest target
- * count M, engine 0/1, target split) into out (capacity cap shapes);
+ * count M, engine: 0 CUDA cores, 1 tensor cores, 3 / 4 tensor cores on
+ * 256-thread tiles at 80 / 128 registers, target split) into out
+ * (capacity cap shapes);
  * returns the number of shapes tuned in this process. */
 int chd_ks_tuned_shapes(int *out, int cap);
+/* The same for the key-switch row pass (no reference counterpart): with
+ * CHD_BCONV_AUTO its first launch of each shape times the variant that
+ * loads each digit's key words and the next digit's ModUp row ahead (2 CTAs
+ * per SM) against the one that loads where it computes (3 CTAs per SM);
+ * five ints per shape (device, ciphertexts, largest row count of the
+ * launch, mode, 1 for the prefetching variant); returns the count. */
+int chd_ks_rows_tuned_shapes(int *out, int cap);
 
 /* ---- residue serialization (no counterpart in the reference, whose objects
  * live only in device memory): a ciphertext or key as a self-describing
