@@ -245,7 +245,11 @@ __global__ void __launch_bounds__(256) k_permute(const __grid_constant__ Permute
 // permutation in registers.  Grid (count, N / 1024, rows): the ciphertexts of
 // a batch that read the same key tile are neighbours in launch order, so the
 // keys come from HBM once per batch.
-__global__ void __launch_bounds__(256) k_hoisted(const __grid_constant__ HoistDesc d, int log_n) {
+// BMAX: digits held per thread; with at most 4 (every parameter set here at
+// the levels hoisted rotations run at) the kernel fits 3 CTAs per SM instead
+// of 2
+template <int BMAX>
+__global__ void __launch_bounds__(256, BMAX <= 4 ? 3 : 2) k_hoisted(const __grid_constant__ HoistDesc d, int log_n) {
   const int n = 1 << log_n;
   const int c = blockIdx.x;
   const int r = blockIdx.z;
@@ -256,9 +260,9 @@ __global__ void __launch_bounds__(256) k_hoisted(const __grid_constant__ HoistDe
   const size_t off = static_cast<size_t>(r) * n + k0;
   const size_t koff = static_cast<size_t>(d.key_row[r]) * n + k0;
   const uint32_t qn = 0u - static_cast<uint32_t>(qi);
-  uint32_t mu[8][4];
+  uint32_t mu[BMAX][4];
 #pragma unroll
-  for (int i = 0; i < 8; i++)
+  for (int i = 0; i < BMAX; i++)
     if (i < d.beta) unpack(ld4(d.mu[c][i] + off), mu[i]);
   uint32_t bxp[4] = {0, 0, 0, 0};
   if (r < d.nq) unpack(ld4(d.bxp[c] + off), bxp);
@@ -267,7 +271,7 @@ __global__ void __launch_bounds__(256) k_hoisted(const __grid_constant__ HoistDe
 #pragma unroll
     for (int l = 0; l < 4; l++) sb[l] = bxp[l];
 #pragma unroll
-    for (int i = 0; i < 8; i += 2) {
+    for (int i = 0; i < BMAX; i += 2) {
       if (i + 1 < d.beta) {  // two digits per Montgomery reduction
         uint32_t kb0[4], ka0[4], kb1[4], ka1[4];
         unpack(ld4(d.kb[j][i] + koff), kb0);
@@ -372,7 +376,11 @@ void launch_hoisted(const HoistDesc &d, int log_n, cudaStream_t s) {
   if (d.rows <= 0 || d.R <= 0) return;
   const int n = 1 << log_n;
   if (d.count <= 0 || d.count > kMaxHoistCts) return;
-  k_hoisted<<<dim3(d.count, (n / 4 + 255) / 256, d.rows), 256, 0, s>>>(d, log_n);
+  const dim3 grid(d.count, (n / 4 + 255) / 256, d.rows);
+  if (d.beta <= 4)
+    k_hoisted<4><<<grid, 256, 0, s>>>(d, log_n);
+  else
+    k_hoisted<8><<<grid, 256, 0, s>>>(d, log_n);
 }
 
 }  // namespace chd
