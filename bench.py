@@ -29,6 +29,7 @@ the reference itself has no CPU path and cannot be built here) on the same
 configuration.
 """
 import argparse
+import hashlib
 import json
 import os
 import subprocess
@@ -169,6 +170,8 @@ def main():
                     help="skip timing the reference's own sm_100a build on the same workloads")
     ap.add_argument("--ks-engine", default="auto", choices=["cuda", "tensor", "tensor_wide", "auto"],
                     help="base conversion inside the ModUp / ModDown column passes of the measured path")
+    ap.add_argument("--hmult-only", action="store_true",
+                    help="profiling aid: measure only the HMult step (value, e2e, roofline) and print its line")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -258,26 +261,29 @@ def main():
     roof = roofline_from_stages(ctx, lvl, B, stages, args.steps)
     launches = sum(nl for _, nl in stages.values())
 
-    # ---- the same step with each column-pass engine ----
-    ks_cmp = ks_engines(ctx, chd, step, stream, args.steps, B)
-    ks_cmp["plain_vs_tensor_batched"] = plain_vs_batched_hmult(ctx, chd, key, a_cts, b_cts, outs, stream, args.steps)
+    ks_cmp = bconv_cmp = ntt_cmp = hoist_mixed = w64 = boot = None
+    if not args.hmult_only:
+        # ---- the same step with each column-pass engine ----
+        ks_cmp = ks_engines(ctx, chd, step, stream, args.steps, B)
+        ks_cmp["plain_vs_tensor_batched"] = plain_vs_batched_hmult(ctx, chd, key, a_cts, b_cts, outs, stream,
+                                                                   args.steps)
 
-    # ---- base conversion as a dense contraction: CUDA cores vs tensor cores ----
-    bconv_cmp = bconv_engines(ctx, chd, stream)
+        # ---- base conversion as a dense contraction: CUDA cores vs tensor cores ----
+        bconv_cmp = bconv_engines(ctx, chd, stream)
 
-    # ---- NTT round trip (forward + inverse), 24 primes ----
-    ntt_cmp = ntt_bench(chd, stream)
+        # ---- NTT round trip (forward + inverse), 24 primes ----
+        ntt_cmp = ntt_bench(chd, stream)
 
-    # ---- hoisted rotations and a mixed-level batch ----
-    hoist_mixed = hoist_mixed_bench(ctx, chd, key, uniform, stream)
-    # ---- the 64-bit word path ----
-    try:
-        w64 = w64_bench(chd, stream)
-    except Exception as e:  # reported, not fatal: the headline is the 32-bit path
-        w64 = {"failed": str(e)[:300]}
+        # ---- hoisted rotations and a mixed-level batch ----
+        hoist_mixed = hoist_mixed_bench(ctx, chd, key, uniform, stream)
+        # ---- the 64-bit word path ----
+        try:
+            w64 = w64_bench(chd, stream)
+        except Exception as e:  # reported, not fatal: the headline is the 32-bit path
+            w64 = {"failed": str(e)[:300]}
 
-    # ---- full-slot bootstrapping at N = 2^16 ----
-    boot = None if args.no_boot else boot_bench(chd, args, stream, dist)
+        # ---- full-slot bootstrapping at N = 2^16 ----
+        boot = None if args.no_boot else boot_bench(chd, args, stream, dist)
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -303,7 +309,7 @@ def main():
     line["config"]["autotuned_row_passes"] = [
         f"cts{t['cts']} rows{t['rows']} mode{t['mode']}: {'prefetch' if t['prefetch'] else 'in_place_loads'}"
         for t in chd.ks_rows_tuned_shapes()]
-    if rank == 0 and world == 1 and not args.no_reference_gpu:
+    if rank == 0 and world == 1 and not args.no_reference_gpu and not args.hmult_only:
         ref = reference_gpu_run(args)
         try:
             ref["hmult_ours_over_reference"] = value / ref["hmult"]["hmult_per_s"]
@@ -323,7 +329,7 @@ def main():
         except (KeyError, TypeError, ZeroDivisionError):
             pass
         line["reference_gpu"] = ref
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.hmult_only:
         try:
             v, cnt, el = cpu_baseline_run(max_seconds=20.0)
             line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
@@ -500,9 +506,10 @@ def roofline_from_stages(ctx, lvl, batch, stages, steps):
     algo = (per_ct * batch / launches_per_step + per_launch) * limb_bytes
     ms = ms_total / nl
     achieved = algo / (ms / 1e3) / 1e9
-    traffic = ncu_traffic(name, batch)
+    traffic, traffic_note = ncu_traffic(name, batch)
     return {"kernel": KERNEL_OF_STAGE[name], "bound": "hbm", "achieved": achieved, "peak": peak,
             "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
+            "traffic_source": traffic_note,
             "algorithmic_bytes_per_launch": algo, "ms_per_launch": ms,
             "stage_ms_per_step": {k: v[0] / steps for k, v in stages.items()},
             "stage_launches_per_step": {k: v[1] / steps for k, v in stages.items()}}
@@ -794,12 +801,23 @@ def hoist_mixed_bench(ctx, chd, key, uniform, stream, reps=5):
 
     ms_h = timed(hoisted)
     ms_s = timed(separate)
+    # the two halves of the hoisted form on their own: the ModUp plus the
+    # one rotation launch (results in Q u P), and the batched ModDown
+    ms_rot = timed(lambda: ctx.HoistedRotate(ct, keys, offsets, outs=qp_outs))
+    ms_md = timed(lambda: ctx.ModDownBatch(qp_outs, res_list=outs))
     R = len(offsets)
     # algorithmic limbs: the input (2 q), every rotation key once
     # (2 beta (q + alpha)) and every rotated result (2 q)
     nq = ctx.num_q(lvl)
+    tot = nq + a
     limbs = 2 * nq + R * 2 * beta * (nq + a) + R * 2 * nq
     algo = limbs * n * 4
+    # the rotation half: ModUp (read q, write beta (q + alpha)), P b (read
+    # and write q), k_hoisted (read the beta digits, P b and every key,
+    # write 2 (q + alpha) per rotation); the ModDown half: read 2 (q +
+    # alpha), write 2 q per rotation
+    rot_limbs = (nq + beta * tot) + 2 * nq + (beta * tot + nq + R * 2 * beta * tot + R * 2 * tot)
+    md_limbs = R * 2 * tot + R * 2 * nq
     hbm = _peaks().get("hbm_gbs", 6650.0)
     res = {"hoisted_rotations": {
         "workload": f"{R} rotations of one ciphertext at level {lvl} (N=2^16, L=24, alpha=8)",
@@ -807,7 +825,11 @@ def hoist_mixed_bench(ctx, chd, key, uniform, stream, reps=5):
         "hoisted_rotations_per_s": R / (ms_h / 1e3), "separate_rotations_per_s": R / (ms_s / 1e3),
         "speedup": ms_s / ms_h, "algorithmic_limbs": limbs, "algorithmic_bytes": algo,
         "hoisted_GB/s": algo / (ms_h / 1e3) / 1e9, "hoisted_hbm_frac": algo / (ms_h / 1e3) / 1e9 / hbm,
-        "separate_hbm_frac": algo / (ms_s / 1e3) / 1e9 / hbm}}
+        "separate_hbm_frac": algo / (ms_s / 1e3) / 1e9 / hbm,
+        "rotate_half": {"ms": ms_rot, "algorithmic_limbs": rot_limbs,
+                        "hbm_frac": rot_limbs * n * 4 / (ms_rot / 1e3) / 1e9 / hbm},
+        "moddown_half": {"ms": ms_md, "algorithmic_limbs": md_limbs,
+                         "hbm_frac": md_limbs * n * 4 / (ms_md / 1e3) / 1e9 / hbm}}}
     del keys, qp_outs, outs
     # (ii) mixed-level batch
     levels = [int(x) for x in np.random.default_rng(0).integers(5, 23, 16)]
@@ -1234,19 +1256,41 @@ KERNEL_OF_STAGE = {
 }
 
 
+# sources a stage's kernel is compiled from (cheddar-fhe_b200/csrc): a
+# committed DRAM-traffic capture counts only while their fingerprint matches
+KERNEL_SOURCES = {"ks_rows": ["keyswitch.cu", "arith.cuh", "ntt_common.cuh", "kernels.h"]}
+
+
+def kernel_fingerprint(stage):
+    """First 12 hex digits of the SHA-256 over the stage kernel's source
+    files, or None for a stage without a source list."""
+    files = KERNEL_SOURCES.get(stage)
+    if not files:
+        return None
+    h = hashlib.sha256()
+    for f in files:
+        with open(os.path.join(ROOT, "cheddar-fhe_b200", "csrc", f), "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:12]
+
+
 def ncu_traffic(stage, batch):
     """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of
     the stage's kernel at this batch, from the committed ncu summary
-    profiles/traffic_hmult_l24.md (a line `traffic <stage> <batch> <bytes>`);
-    None when that capture has not been made."""
+    profiles/traffic_hmult_l24.md (a line `traffic <stage> <batch> <bytes>
+    <source fingerprint>`), and a note.  The bytes are None when no capture
+    was made or when the kernel's sources changed after it (the fingerprint
+    differs)."""
     try:
         for ln in open(os.path.join(ROOT, "profiles", "traffic_hmult_l24.md")):
             f = ln.strip().strip("`").split()
-            if len(f) == 4 and f[0] == "traffic" and f[1] == stage and int(f[2]) == batch:
-                return float(f[3])
+            if len(f) == 5 and f[0] == "traffic" and f[1] == stage and int(f[2]) == batch:
+                if f[4] != kernel_fingerprint(stage):
+                    return None, "the committed ncu capture predates the current kernel source"
+                return float(f[3]), "ncu capture of this kernel source (fingerprint " + f[4] + ")"
     except (OSError, ValueError):
         pass
-    return None
+    return None, "no ncu capture of this kernel at this batch"
 
 
 if __name__ == "__main__":

@@ -50,11 +50,21 @@ __device__ __forceinline__ uint32_t split_s8(int32_t x) {
 
 // Software pipeline over iterations (TPI tiles each), two buffers for the A
 // tiles and the TMEM accumulators:
-//   split + store A(i) -> MMA(i) -> loads of i+1 in flight -> epilogue(i-1)
-// so the HBM loads of one iteration overlap the MMAs of the current one and
-// the TMEM read-back and stores of the previous one.
-template <int TPI>
+//   split + store A(i) -> MMA(i) -> loads of i+DEPTH in flight -> epilogue(i-1)
+// so the HBM loads of the next DEPTH iterations overlap the MMAs of the
+// current one and the TMEM read-back and stores of the previous one.  The
+// loads sit in a ring of DEPTH register stages: with few sources per tile
+// (a ModDown from 4 auxiliary primes: 16 bytes per thread and tile) one
+// stage keeps too few bytes in flight for HBM, and the TMEM columns that the
+// targets' accumulators take cap the CTAs per SM.
+template <int TPI, int KMAX>
+struct BConvTcShape {
+  static constexpr int kDepth = TPI * KMAX <= 8 ? 4 : (TPI * KMAX <= 16 ? 2 : 1);
+};
+
+template <int TPI, int KMAX>
 __global__ void __launch_bounds__(128) k_bconv_tc(const __grid_constant__ BConvTcDesc d) {
+  constexpr int DEPTH = BConvTcShape<TPI, KMAX>::kDepth;
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ __align__(8) uint64_t mbar[3];  // two accumulator buffers + the stall-test barrier
   __shared__ uint32_t tmem_slot;
@@ -106,13 +116,13 @@ __global__ void __launch_bounds__(128) k_bconv_tc(const __grid_constant__ BConvT
     return d.out + static_cast<size_t>(tile0 / tiles_per_poly) * M * n +
            static_cast<size_t>(tile0 % tiles_per_poly) * kRows + t;
   };
-  int32_t v[TPI][16];
-  auto load = [&](int it) {
+  int32_t v[DEPTH][TPI][KMAX];
+  auto load = [&](int32_t (&dst)[TPI][KMAX], int it) {
     const int32_t *x = src_of(it);
 #pragma unroll
     for (int u = 0; u < TPI; u++)
 #pragma unroll
-      for (int k = 0; k < 16; k++) v[u][k] = k < K ? __ldg(x + static_cast<size_t>(k) * n + u * kRows) : 0;
+      for (int k = 0; k < KMAX; k++) dst[u][k] = k < K ? __ldg(x + static_cast<size_t>(k) * n + u * kRows) : 0;
   };
   auto epilogue = [&](int it, int b) {
     uint32_t *o = dst_of(it);
@@ -143,64 +153,78 @@ __global__ void __launch_bounds__(128) k_bconv_tc(const __grid_constant__ BConvT
   bool ok = true;
   int prev = -1;  // iteration whose accumulators wait for their epilogue
   int it = blockIdx.x;
-  if (it < nits) load(it);
-  for (int i = 0; it < nits; i++, it += gridDim.x) {
-    const int b = i & 1;
-    // A operand of tile u: row t, chunk c (sources 4c..4c+3) at
-    //   b * abuf + (u * KS + c / 2) * 4096 + (t / 8) * 256 + (c % 2) * 128 + (t % 8) * 16
+  const int grid = static_cast<int>(gridDim.x);
 #pragma unroll
-    for (int u = 0; u < TPI; u++)
+  for (int s = 0; s < DEPTH; s++)
+    if (it + s * grid < nits) load(v[s], it + s * grid);
+  int i = 0;
+  while (ok && it < nits) {
+    // the ring is walked with compile-time stage indices (registers)
 #pragma unroll
-      for (int c = 0; c < 4; c++) {
-        if (c < 2 * KS) {
-          const int off = b * abuf + (u * KS + (c >> 1)) * kATileBytes + (t >> 3) * 256 + (c & 1) * 128 + (t & 7) * 16;
-          *reinterpret_cast<uint4 *>(sa + off) = make_uint4(split_s8(v[u][4 * c]), split_s8(v[u][4 * c + 1]),
-                                                            split_s8(v[u][4 * c + 2]), split_s8(v[u][4 * c + 3]));
-        }
-      }
-    // make the generic-proxy stores visible to the tensor core
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
-    if (t == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    for (int st = 0; st < DEPTH; st++) {
+      if (!ok || it >= nits) continue;
+      const int b = i & 1;
+      // A operand of tile u: row t, chunk c (sources 4c..4c+3) at
+      //   b * abuf + (u * KS + c / 2) * 4096 + (t / 8) * 256 + (c % 2) * 128 + (t % 8) * 16
+#pragma unroll
       for (int u = 0; u < TPI; u++)
-        for (int s = 0; s < KS; s++) {
-          const uint64_t ad = smem_desc(sa_u + b * abuf + (u * KS + s) * kATileBytes, 128, 256);
-          const uint64_t bd = smem_desc(sb_u + s * NB * 32, 128, 256);
-          const uint32_t acc = s > 0 ? 1u : 0u;
-          asm volatile(
-              "{\n\t.reg .pred p;\n\t"
-              "setp.ne.b32 p, %4, 0;\n\t"
-              "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-              ::"r"(tmem + b * tbuf + static_cast<uint32_t>(u * NB)), "l"(ad), "l"(bd), "r"(d.idesc), "r"(acc),
-              "r"(0u), "r"(0u), "r"(0u), "r"(0u)
-              : "memory");
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+          if (c < 2 * KS) {
+            uint32_t wd[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) wd[j] = 4 * c + j < KMAX ? split_s8(v[st][u][(4 * c + j) % KMAX]) : 0u;
+            const int off =
+                b * abuf + (u * KS + (c >> 1)) * kATileBytes + (t >> 3) * 256 + (c & 1) * 128 + (t & 7) * 16;
+            *reinterpret_cast<uint4 *>(sa + off) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
+          }
         }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(b ? bar1
-                                                                                                          : bar0)
-                   : "memory");
-    }
-    pending |= 1u << b;
-    // next iteration's loads go out while the MMAs run
-    if (it + static_cast<int>(gridDim.x) < nits) load(it + gridDim.x);
-    if (prev >= 0) {
-      const int pb = b ^ 1;
-      // every thread polls with a limit; the CTA leaves together if any gave up
-      const bool got = d.stall_polls ? mbar_wait(bar_never, 0u, d.stall_polls)
-                                     : mbar_wait(pb ? bar1 : bar0, (parity >> pb) & 1u);
-      if (!__syncthreads_and(got ? 1 : 0)) {
-        ok = false;
-        break;
-      }
-      parity ^= 1u << pb;
-      pending &= ~(1u << pb);
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      epilogue(prev, pb);
-      // TMEM reads of buffer pb finish before MMAs overwrite it
+      // make the generic-proxy stores visible to the tensor core
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncthreads();
+      if (t == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        for (int u = 0; u < TPI; u++)
+          for (int s = 0; s < KS; s++) {
+            const uint64_t ad = smem_desc(sa_u + b * abuf + (u * KS + s) * kATileBytes, 128, 256);
+            const uint64_t bd = smem_desc(sb_u + s * NB * 32, 128, 256);
+            const uint32_t acc = s > 0 ? 1u : 0u;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "setp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+                ::"r"(tmem + b * tbuf + static_cast<uint32_t>(u * NB)), "l"(ad), "l"(bd), "r"(d.idesc), "r"(acc),
+                "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+                : "memory");
+          }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(b ? bar1
+                                                                                                            : bar0)
+                     : "memory");
+      }
+      pending |= 1u << b;
+      // this stage's next loads (DEPTH iterations ahead) go out while the MMAs run
+      if (it + DEPTH * grid < nits) load(v[st], it + DEPTH * grid);
+      if (prev >= 0) {
+        const int pb = b ^ 1;
+        // every thread polls with a limit; the CTA leaves together if any gave up
+        const bool got = d.stall_polls ? mbar_wait(bar_never, 0u, d.stall_polls)
+                                       : mbar_wait(pb ? bar1 : bar0, (parity >> pb) & 1u);
+        if (!__syncthreads_and(got ? 1 : 0)) {
+          ok = false;
+          continue;
+        }
+        parity ^= 1u << pb;
+        pending &= ~(1u << pb);
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        epilogue(prev, pb);
+        // TMEM reads of buffer pb finish before MMAs overwrite it
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      }
+      prev = it;
+      i++;
+      it += grid;
     }
-    prev = it;
   }
   if (ok && prev >= 0) {
     // the last iteration's accumulators sit in buffer ((iterations - 1) & 1)
@@ -239,7 +263,7 @@ size_t bconv_tc_smem(int tpi, int ksteps, int nb) {
 }
 
 namespace {
-template <int TPI>
+template <int TPI, int KMAX>
 int launch_tpi(const BConvTcDesc &d, int num_sms, cudaStream_t s) {
   // CTAs per SM: TMEM (512 columns), registers, shared memory (228 KiB per
   // SM, 1 KiB reserved per CTA), 16 CTAs of 128 threads; the dynamic shared
@@ -247,12 +271,12 @@ int launch_tpi(const BConvTcDesc &d, int num_sms, cudaStream_t s) {
   const int cap = 512 / d.tmem_cols;
   size_t sm = bconv_tc_smem(TPI, d.ksteps, d.nb);
   cudaFuncAttributes fa{};
-  if (cudaFuncGetAttributes(&fa, k_bconv_tc<TPI>) != cudaSuccess) return -2;
+  if (cudaFuncGetAttributes(&fa, k_bconv_tc<TPI, KMAX>) != cudaSuccess) return -2;
   const size_t per_sm = 233472, reserved = 1024 + fa.sharedSizeBytes;
   const size_t floor_sm = per_sm / (cap + 1) + 16 > reserved ? per_sm / (cap + 1) + 16 - reserved : 0;
   if (sm < floor_sm) sm = floor_sm;
-  if (cudaFuncSetAttribute(k_bconv_tc<TPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)) !=
-      cudaSuccess)
+  if (cudaFuncSetAttribute(k_bconv_tc<TPI, KMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(sm)) != cudaSuccess)
     return -2;
   int per = cap;
   const int regs = fa.numRegs > 0 ? fa.numRegs : 64;
@@ -263,8 +287,16 @@ int launch_tpi(const BConvTcDesc &d, int num_sms, cudaStream_t s) {
   const int nits = d.npoly * (d.n / kRows) / TPI;
   int grid = num_sms * per;
   if (grid > nits) grid = nits;
-  k_bconv_tc<TPI><<<grid, 128, sm, s>>>(d);
+  k_bconv_tc<TPI, KMAX><<<grid, 128, sm, s>>>(d);
   return 0;
+}
+
+template <int TPI>
+int launch_kmax(const BConvTcDesc &d, int num_sms, cudaStream_t s) {
+  if (d.K <= 4) return launch_tpi<TPI, 4>(d, num_sms, s);
+  if (d.K <= 8) return launch_tpi<TPI, 8>(d, num_sms, s);
+  if (d.K <= 12) return launch_tpi<TPI, 12>(d, num_sms, s);
+  return launch_tpi<TPI, 16>(d, num_sms, s);
 }
 }  // namespace
 
@@ -275,9 +307,9 @@ int launch_bconv_tc(const BConvTcDesc &d, int num_sms, cudaStream_t s) {
     return -1;
   if ((d.n / kRows) % d.tpi != 0) return -1;
   switch (d.tpi) {
-    case 1: return launch_tpi<1>(d, num_sms, s);
-    case 2: return launch_tpi<2>(d, num_sms, s);
-    case 4: return launch_tpi<4>(d, num_sms, s);
+    case 1: return launch_kmax<1>(d, num_sms, s);
+    case 2: return launch_kmax<2>(d, num_sms, s);
+    case 4: return launch_kmax<4>(d, num_sms, s);
     default: return -1;
   }
 }
