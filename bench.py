@@ -252,17 +252,30 @@ def main():
     # ---- end to end through the C ABI with host buffers ----
     e2e = e2e_run(ctx, chd, key, lvl, nq, n, B, args, stream, dist)
 
-    # ---- per-stage device timing of the same step: dominant kernel, launches ----
+    # ---- kernel launches of the measured step (two streams) ----
+    ctx.stage_timing(True)
+    for _ in range(args.steps):
+        step()
+    launches = sum(nl for _, nl in ctx.stage_times().values())
+    ctx.stage_timing(False)
+    # ---- per-stage device timing of the one-stream pipeline (kernels one
+    # after another, so that each stage's events time its own launches):
+    # dominant kernel and its roofline ----
+    ctx.stream_split = False
+    for _ in range(3):
+        step()  # the one-stream launch shapes tuned outside the timed spans
     ctx.stage_timing(True)
     for _ in range(args.steps):
         step()
     stages = ctx.stage_times()
     ctx.stage_timing(False)
+    ctx.stream_split = True
     roof = roofline_from_stages(ctx, lvl, B, stages, args.steps)
-    launches = sum(nl for _, nl in stages.values())
 
-    ks_cmp = bconv_cmp = ntt_cmp = hoist_mixed = w64 = boot = None
+    ks_cmp = bconv_cmp = ntt_cmp = hoist_mixed = w64 = boot = split_cmp = None
     if not args.hmult_only:
+        # ---- the same step with the key switch on one stream ----
+        split_cmp = stream_split_cmp(ctx, step, stream, args.steps)
         # ---- the same step with each column-pass engine ----
         ks_cmp = ks_engines(ctx, chd, step, stream, args.steps, B)
         ks_cmp["plain_vs_tensor_batched"] = plain_vs_batched_hmult(ctx, chd, key, a_cts, b_cts, outs, stream,
@@ -295,7 +308,7 @@ def main():
                    "parallelism": f"replicas x{world}"},
         "e2e": e2e, "roofline": roof, "clocks": sampler.summary(), "ks_engine": args.ks_engine,
         "ks_engines": ks_cmp, "bconv_engines": bconv_cmp, "ntt": ntt_cmp,
-        "bootstrap": boot, "hoisted_and_mixed": hoist_mixed, "w64": w64,
+        "bootstrap": boot, "hoisted_and_mixed": hoist_mixed, "w64": w64, "stream_split": split_cmp,
         "gpu_launches": launches,
     }
     # the autotuner's choice per column-pass launch shape (largest source
@@ -523,9 +536,11 @@ def ks_engine_id(chd, args):
 def ks_engines(ctx, chd, step, stream, steps, B):
     """The HMult step with the ModUp / ModDown column passes on each engine
     (CUDA-core int64 BConv vs tcgen05 INT8 byte-limb MMAs); residues are
-    identical (tests), only the time differs."""
+    identical (tests), only the time differs.  The one-stream pipeline, so
+    that the stage events time each column pass alone."""
     import torch
     old = ctx.ks_engine
+    ctx.stream_split = False
     out = {}
     for name, e in (("cuda_core", chd.BCONV_CUDA_CORE), ("tensor_core", chd.BCONV_TENSOR_CORE),
                     ("tensor_core_wide", chd.BCONV_TENSOR_CORE_WIDE), ("auto", chd.BCONV_AUTO)):
@@ -548,6 +563,7 @@ def ks_engines(ctx, chd, step, stream, steps, B):
         out[name] = {"hmult_per_s": B * steps / (ms / 1e3), "ms_per_step": ms / steps,
                      "modup_cols_ms": st["modup_cols"][0] / steps, "moddown_cols_ms": st["moddown_cols"][0] / steps}
     ctx.ks_engine = old
+    ctx.stream_split = True
     out["speedup_tensor_vs_cuda_core"] = out["tensor_core"]["hmult_per_s"] / out["cuda_core"]["hmult_per_s"]
     out["speedup_tensor_wide_vs_cuda_core"] = (out["tensor_core_wide"]["hmult_per_s"] /
                                                out["cuda_core"]["hmult_per_s"])
@@ -556,6 +572,31 @@ def ks_engines(ctx, chd, step, stream, steps, B):
     out["column_pass_speedup"] = cols["cuda_core"] / cols["tensor_core"]
     out["column_pass_speedup_wide"] = cols["cuda_core"] / cols["tensor_core_wide"]
     return out
+
+
+def stream_split_cmp(ctx, step, stream, steps):
+    """The measured step with the fused key switch split over two streams
+    (the default: halves of the batch on the context stream and on the
+    context's second stream) and on the context stream alone; CUDA events on
+    the context stream, which joins the second stream at the end of every
+    key switch."""
+    import torch
+    res = {}
+    for name, on in (("one_stream", False), ("two_streams", True)):
+        ctx.stream_split = on
+        for _ in range(3):
+            step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        res[name + "_ms"] = e0.elapsed_time(e1) / steps
+    ctx.stream_split = True
+    res["speedup"] = res["one_stream_ms"] / res["two_streams_ms"]
+    return res
 
 
 def plain_vs_batched_hmult(ctx, chd, key, a_cts, b_cts, outs, stream, steps):

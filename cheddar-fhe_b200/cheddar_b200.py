@@ -77,6 +77,8 @@ def lib():
         "chd_sub_const_ct": (i, [vp, vp, u32p, d, vp]),
         "chd_mult_unsafe_plain": (i, [vp, vp, vp, vp, i, i, d, i]),
         "chd_get_ks_engine": (i, [vp]),
+        "chd_set_stream_split": (i, [vp, i]),
+        "chd_get_stream_split": (i, [vp]),
         "chd_stage_times": (i, [vp, vp, vp]),
         "chd_level_np": (i, [vp, i, C.POINTER(i), C.POINTER(i)]),
         "chd_max_level": (i, [vp]),
@@ -308,6 +310,17 @@ class Context:
     @ks_engine.setter
     def ks_engine(self, engine):
         _check(lib().chd_set_ks_engine(self.ptr, int(engine)))
+
+    @property
+    def stream_split(self):
+        """Whether a fused key switch of two or more ciphertexts runs its two
+        halves on two streams of the context (on by default; identical
+        residues either way)."""
+        return bool(lib().chd_get_stream_split(self.ptr))
+
+    @stream_split.setter
+    def stream_split(self, on):
+        _check(lib().chd_set_stream_split(self.ptr, 1 if on else 0))
 
     def stage_timing(self, enable):
         """Start (clearing earlier records) or stop device timing of the fused

@@ -377,6 +377,18 @@ int chd_ks_tuned_shapes(int *out, int cap) { return modswitch_tuned_shapes(out, 
 
 int chd_ks_rows_tuned_shapes(int *out, int cap) { return ks_rows_tuned_shapes(out, cap); }
 
+int chd_set_stream_split(chd_context *ctx, int on) try {
+  CHD_CTX(ctx);
+  ctx->c->split_streams = on != 0;
+  return CHD_OK;
+} catch (const std::exception &e) {
+  return fail(CHD_ERR_INTERNAL, std::string("internal error: ") + e.what());
+} catch (...) {
+  return fail(CHD_ERR_INTERNAL, "internal error");
+}
+
+int chd_get_stream_split(const chd_context *ctx) { return ctx ? (ctx->c->split_streams ? 1 : 0) : -1; }
+
 int chd_stage_times(chd_context *ctx, double *ms, int *launches) try {
   CHD_CTX(ctx);
   if (!ms || !launches) return fail(CHD_ERR_INVALID_ARG, "chd_stage_times: null output");

@@ -7,9 +7,11 @@
 // and builds launch descriptors.
 #include <algorithm>
 #include <cerrno>
+#include <cstdlib>
 #include <limits>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <mutex>
 
 #include "host.h"
@@ -564,6 +566,12 @@ Context::~Context() {
   cudaFree(d_enc_tw);
   cudaFree(d_galois);
   for (cudaEvent_t e : timer.ev) cudaEventDestroy(e);
+  if (aux_stream) {
+    cudaStreamSynchronize(aux_stream);
+    cudaStreamDestroy(aux_stream);
+  }
+  if (ev_fork) cudaEventDestroy(ev_fork);
+  if (ev_join) cudaEventDestroy(ev_join);
   if (own_stream && stream) cudaStreamDestroy(stream);
 }
 
@@ -756,6 +764,13 @@ Status Context::init(const ParamSpec &spec, int dev, std::string *err) {
     return kErrCuda;
   }
   own_stream = true;
+  if (cudaStreamCreateWithFlags(&aux_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming) != cudaSuccess) {
+    *err = "auxiliary stream creation failed";
+    return kErrCuda;
+  }
+  if (const char *e = std::getenv("CHD_SPLIT_STREAMS")) split_streams = std::atoi(e) != 0;
   const int n = P->n, np_all = P->L + P->alpha;
   // twiddles, NTT.cu:1233-1299: psi_rev[j] = psi^brev(j); stored plain with
   // the Shoup companion floor(w 2^32 / q)
@@ -842,8 +857,31 @@ Status Context::ntt(const NP &np, uint32_t *data, bool mont, int count, size_t s
       r.flags = mont ? kPreMult : 0u;
       rows.push_back(r);
     }
-  for_row_batches(rows, [&](const RowBatch &rb) { launch_ntt_fwd(rb, P->log_n, stream); });
-  return check_cuda("ntt");
+  return alternate_row_batches(rows, count > 1 && stride >= static_cast<size_t>(tot) * n,
+                               [&](const RowBatch &rb, cudaStream_t s) { launch_ntt_fwd(rb, P->log_n, s); }, "ntt");
+}
+
+Status Context::alternate_row_batches(const std::vector<RowDesc> &rows, bool disjoint,
+                                      const std::function<void(const RowBatch &, cudaStream_t)> &launch,
+                                      const char *what) {
+  // more rows than one launch takes: the launches alternate between the
+  // context stream and aux_stream (forked and joined as in fork_halves), so
+  // that one launch's column phase runs beside the other's row phase; rows
+  // must be distinct limbs (disjoint), each transformed in place
+  const bool split = split_streams && aux_stream != nullptr && disjoint &&
+                     static_cast<int>(rows.size()) > kMaxRows;
+  if (!split) {
+    for_row_batches(rows, [&](const RowBatch &rb) { launch(rb, stream); });
+    return check_cuda(what);
+  }
+  CHD_CHECK(cudaEventRecord(ev_fork, stream) == cudaSuccess && cudaStreamWaitEvent(aux_stream, ev_fork, 0) == cudaSuccess,
+            kErrCuda, "stream fork failed");
+  int k = 0;
+  for_row_batches(rows, [&](const RowBatch &rb) { launch(rb, (k++ & 1) ? aux_stream : stream); });
+  const bool joined =
+      cudaEventRecord(ev_join, aux_stream) == cudaSuccess && cudaStreamWaitEvent(stream, ev_join, 0) == cudaSuccess;
+  CHD_CHECK(joined, kErrCuda, "stream join failed");
+  return check_cuda(what);
 }
 
 Status Context::intt(const NP &np, uint32_t *data, bool mont, int count, size_t stride) {
@@ -860,8 +898,8 @@ Status Context::intt(const NP &np, uint32_t *data, bool mont, int count, size_t 
       mont_as_shoup(mont ? n_inv[g[i]] : n_inv_mont[g[i]], g[i], &r.c0, &r.c0s);
       rows.push_back(r);
     }
-  for_row_batches(rows, [&](const RowBatch &rb) { launch_ntt_inv(rb, P->log_n, stream); });
-  return check_cuda("intt");
+  return alternate_row_batches(rows, count > 1 && stride >= static_cast<size_t>(tot) * n,
+                               [&](const RowBatch &rb, cudaStream_t s) { launch_ntt_inv(rb, P->log_n, s); }, "intt");
 }
 
 Status Context::bconv(const int32_t *xt, int K, const int32_t *table, const int *dst_gidx, int M, uint32_t *out) {
@@ -1169,6 +1207,30 @@ Status Context::key_switch_fused(int level, int count, const KSIn *in, const Dev
 
 Status Context::key_switch_fused_levels(const int *levels, int count, const KSIn *in, const DeviceEvk &key,
                                         MDType type, bool keep_ext) {
+  // Two halves on two streams when the batch has at least two inputs and no
+  // result of one half is an operand or a result of the other (with the
+  // stage timer on, each half's spans are recorded on its own stream)
+  bool split = split_streams && count >= 2 && aux_stream != nullptr;
+  const int h = (count + 1) / 2;
+  if (split) {
+    auto ptrs_in = [&](int c, const void *p) {
+      const KSIn &x = in[c];
+      return p == x.b1 || p == x.a1 || p == x.b2 || p == x.a2 || p == x.out_b || p == x.out_a;
+    };
+    for (int c = 0; c < h && split; c++)
+      for (int e = h; e < count && split; e++)
+        if (ptrs_in(e, in[c].out_b) || ptrs_in(e, in[c].out_a) || ptrs_in(c, in[e].out_b) || ptrs_in(c, in[e].out_a))
+          split = false;
+  }
+  if (!split) return key_switch_fused_pipeline(levels, count, in, key, type, keep_ext, false);
+  return fork_halves([&](bool second) {
+    return second ? key_switch_fused_pipeline(levels + h, count - h, in + h, key, type, keep_ext, true)
+                  : key_switch_fused_pipeline(levels, h, in, key, type, keep_ext, true);
+  });
+}
+
+Status Context::key_switch_fused_pipeline(const int *levels, int count, const KSIn *in, const DeviceEvk &key,
+                                          MDType type, bool keep_ext, bool hold) {
   CHD_CHECK(P->log_n == 16, kErrUnsupported, "fused key switch needs N = 2^16");
   CHD_CHECK(keep_ext || type != MDType::kRescale, kErrInvalidArg,
             "fused key switch ends in ModDown or ModDownAndRescale");
@@ -1222,7 +1284,7 @@ Status Context::key_switch_fused_levels(const int *levels, int count, const KSIn
       n_drop += 2 * sh.pl.src_len;
     }
   }
-  ArenaScope scope(arena);
+  HeldScope scope(arena, hold);
   uint32_t *t1 = static_cast<uint32_t *>(arena.alloc(n_t1 * N * 4));
   uint32_t *mu = static_cast<uint32_t *>(arena.alloc(n_mu * N * 4));
   // keep_ext: the accumulators go straight to the callers' buffers and
@@ -1453,6 +1515,45 @@ Status Context::key_switch_fused_levels(const int *levels, int count, const KSIn
 }
 
 Status Context::moddown(int level, MDType type, const uint32_t *const *src, uint32_t *const *dst, int npoly) {
+  // at N = 2^16 four or more polynomials run as two halves on two streams
+  // (as the fused key switch does), unless a result of one half is an
+  // operand or a result of the other
+  bool split = split_streams && P->log_n == 16 && npoly >= 4 && aux_stream != nullptr;
+  const int h = (npoly + 1) / 2;
+  for (int p = 0; p < h && split; p++)
+    for (int e = h; e < npoly && split; e++)
+      if (dst[p] == src[e] || dst[p] == dst[e] || dst[e] == src[p]) split = false;
+  if (!split) return moddown_pipeline(level, type, src, dst, npoly, false);
+  return fork_halves([&](bool second) {
+    return second ? moddown_pipeline(level, type, src + h, dst + h, npoly - h, true)
+                  : moddown_pipeline(level, type, src, dst, h, true);
+  });
+}
+
+Status Context::fork_halves(const std::function<Status(bool)> &half) {
+  // the halves' scratch stays allocated until both are enqueued; later work
+  // on the context stream is ordered after the join
+  ArenaScope scope(arena);
+  CHD_CHECK(cudaEventRecord(ev_fork, stream) == cudaSuccess && cudaStreamWaitEvent(aux_stream, ev_fork, 0) == cudaSuccess,
+            kErrCuda, "stream fork failed");
+  Status st = half(false);
+  if (st == kOk) {
+    cudaStream_t main_stream = stream;
+    stream = aux_stream;
+    st = half(true);
+    stream = main_stream;
+  }
+  // the join is recorded on every path, so that nothing later on the
+  // context stream overtakes work already enqueued on the auxiliary one
+  const bool joined =
+      cudaEventRecord(ev_join, aux_stream) == cudaSuccess && cudaStreamWaitEvent(stream, ev_join, 0) == cudaSuccess;
+  CHD_TRY(st);
+  CHD_CHECK(joined, kErrCuda, "stream join failed");
+  return kOk;
+}
+
+Status Context::moddown_pipeline(int level, MDType type, const uint32_t *const *src, uint32_t *const *dst, int npoly,
+                                 bool hold) {
   // ModSwitch.cu:566-684 with NTT.cu:973-1128 and the fused epilogue of
   // NTT.cu:456-601
   const LevelMS &m = lms(level);
@@ -1483,7 +1584,7 @@ Status Context::moddown(int level, MDType type, const uint32_t *const *src, uint
     for (int r = 0; r < ns.ter - nn.ter; r++) srows.push_back(r);
   for (int a = 0; a < nsa; a++) srows.push_back(ns.q() + a);
   CHD_CHECK(static_cast<int>(srows.size()) == src_len, kErrInvalidArg, "moddown: internal row mismatch");
-  ArenaScope scope(arena);
+  HeldScope scope(arena, hold);
   int32_t *xt = static_cast<int32_t *>(arena.alloc(static_cast<size_t>(npoly) * src_len * n * 4));
   CHD_CHECK(xt, kErrAlloc, "moddown: scratch allocation failed");
   std::vector<RowDesc> rows;

@@ -12,6 +12,7 @@
 #include <string>
 #include <utility>
 #include <complex>
+#include <functional>
 #include <vector>
 
 #include "kernels.h"
@@ -318,6 +319,16 @@ struct ArenaScope {
   explicit ArenaScope(Arena &x) : a(x), m(x.mark()) {}
   ~ArenaScope() { a.release(m); }
 };
+// The same, or (hold) leaves the allocations to the enclosing scope.
+struct HeldScope {
+  Arena &a;
+  size_t m;
+  bool hold;
+  HeldScope(Arena &x, bool h) : a(x), m(x.mark()), hold(h) {}
+  ~HeldScope() {
+    if (!hold) a.release(m);
+  }
+};
 
 class Context {
  public:
@@ -339,6 +350,14 @@ class Context {
   uint32_t tc_stall_polls = 0;
   int num_sms = 0;
   int ks_engine = 0;      // ModUp / ModDown column-pass base conversion: 0 CUDA cores, 1 tensor cores, 2 autotuned
+  // A fused key switch of two or more ciphertexts runs its two halves on the
+  // context stream and on aux_stream (forked from and joined back into the
+  // context stream by events), so that the kernels of one half fill the
+  // issue slots the other half's kernels leave idle (the column passes wait
+  // on barriers and the tensor cores, the row passes on the ALU)
+  bool split_streams = true;
+  cudaStream_t aux_stream = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   uint2 *d_tw = nullptr, *d_itw = nullptr;  // [nprimes][N] (psi_rev, Shoup companion)
   std::vector<uint32_t> n_inv, n_inv_mont, mont_conv, p_prod, imag_unit;
   std::vector<uint32_t> r_inv;  // 2^-32 mod q per global prime
@@ -391,8 +410,25 @@ class Context {
   // launch (or a few, by the per-launch job limits) over all levels.
   Status key_switch_fused_levels(const int *levels, int count, const KSIn *in, const DeviceEvk &key, MDType type,
                                  bool keep_ext = false);
+  // one pipeline on the context stream; with hold the scratch stays
+  // allocated in the caller's arena scope
+  Status key_switch_fused_pipeline(const int *levels, int count, const KSIn *in, const DeviceEvk &key, MDType type,
+                                   bool keep_ext, bool hold);
   // ModDown family on npoly polys
   Status moddown(int level, MDType type, const uint32_t *const *src, uint32_t *const *dst, int npoly);
+  // one ModDown pipeline on the context stream (hold: as in
+  // key_switch_fused_pipeline)
+  Status moddown_pipeline(int level, MDType type, const uint32_t *const *src, uint32_t *const *dst, int npoly,
+                          bool hold);
+  // half(false) on the context stream, then half(true) on aux_stream,
+  // forked from and joined back into the context stream; both halves'
+  // arena scratch lives until the join is enqueued
+  Status fork_halves(const std::function<Status(bool)> &half);
+  // launch(batch, stream) per batch of for_row_batches, alternating between
+  // the context stream and aux_stream when there are several batches of
+  // disjoint rows
+  Status alternate_row_batches(const std::vector<RowDesc> &rows, bool disjoint,
+                               const std::function<void(const RowBatch &, cudaStream_t)> &launch, const char *what);
   Status bconv(const int32_t *xt, int K, const int32_t *table, const int *dst_gidx, int M, uint32_t *out);
   // BConv of npoly polynomials ([npoly][K][N] -> [npoly][M][N]) with the
   // host table T[m][k] (centred, Montgomery q-hat R^2): engine 0 on the CUDA

@@ -456,6 +456,22 @@ int chd_ks_tuned_shapes(int *out, int cap);
  * five ints per shape (device, ciphertexts, largest row count of the
  * launch, mode, 1 for the prefetching variant); returns the count. */
 int chd_ks_rows_tuned_shapes(int *out, int cap);
+/* Two-stream key switching (no reference counterpart; on by default, the
+ * environment variable CHD_SPLIT_STREAMS=0 turns it off at context
+ * creation): a fused key switch of two or more ciphertexts, and a ModDown
+ * family call on four or more polynomials, at N = 2^16 (HMult / Relinearize
+ * / MultKey / HRot batches, batched ModDown and rescaling, batched
+ * bootstrapping) runs its two halves on the context stream and on a second
+ * stream of the context, forked from and joined back into the context
+ * stream by events (graph capture included), unless a result of one half is
+ * an operand or a result of the other.  Results are identical either way.
+ * With the stage timer on (chd_stage_timing) each half's spans are recorded
+ * on its own stream: the launch counts are the split pipeline's, the summed
+ * times those of kernels that overlap (time the one-stream pipeline for
+ * per-kernel figures).  chd_get_stream_split returns 1 / 0, or -1 for a null
+ * context. */
+int chd_set_stream_split(chd_context *ctx, int on);
+int chd_get_stream_split(const chd_context *ctx);
 
 /* ---- residue serialization (no counterpart in the reference, whose objects
  * live only in device memory): a ciphertext or key as a self-describing

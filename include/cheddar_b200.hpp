@@ -133,6 +133,8 @@ class Context {
   // CHD_BCONV_TENSOR_CORE or CHD_BCONV_AUTO); results are bit-identical.
   void SetKeySwitchEngine(int engine) { check(chd_set_ks_engine(c_, engine)); }
   int KeySwitchEngine() const { return chd_get_ks_engine(c_); }
+  void SetStreamSplit(bool on) { check(chd_set_stream_split(c_, on ? 1 : 0)); }
+  bool StreamSplit() const { return chd_get_stream_split(c_) == 1; }
 
   // residue import / export ([np][N] per part), host or device pointers
   void Import(Ct &ct, int level, int num_aux, double scale, int num_slots, const uint32_t *bx,
