@@ -1215,6 +1215,25 @@ def boot_bench(chd, args, stream, dist, profile=False):
     torch.cuda.synchronize()
     ms_graph = max_over_ranks(dist, eg0.elapsed_time(eg1), "cuda")
     del graph
+    # the same graph-captured batch with every key switch and ModDown on the
+    # context stream alone
+    ctx.stream_split = False
+    step()
+    ctx.synchronize()
+    ctx.graph_begin()
+    step()
+    graph = ctx.graph_end()
+    graph.launch()
+    ctx.synchronize()
+    eg0.record(stream)
+    for _ in range(steps):
+        graph.launch()
+    eg1.record(stream)
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    ms_graph_one = max_over_ranks(dist, eg0.elapsed_time(eg1), "cuda")
+    del graph
+    ctx.stream_split = True
     # the min-KS form (two rotation keys per transform, Boot(..., min_ks=true))
     bc.BootBatch(ins, keys, res_list=outs, min_ks=True)
     ctx.synchronize()
@@ -1274,6 +1293,8 @@ def boot_bench(chd, args, stream, dist, profile=False):
                "plain_cuda_core_one_by_one_ms_per_boot": ms_plain / (B * steps),
                "tensor_core_batched_graph_ms_per_boot": ms_graph / (B * steps),
                "speedup": ms_plain / ms_graph},
+           "stream_split": {"one_stream_ms_per_boot": ms_graph_one / (B * steps),
+                            "two_streams_ms_per_boot": ms_graph / (B * steps), "speedup": ms_graph_one / ms_graph},
            "min_ks": {"ms_per_boot": ms_mk / (B * steps), "bootstraps_per_s": B * steps / (ms_mk / 1e3),
                       "rotation_keys": len(bc.rotations(min_ks=True))},
            "unit": "bootstraps/s", "ms_per_boot": ms_graph / (B * steps), "batch_per_gpu": B, "steps": steps,
