@@ -572,7 +572,6 @@ Context::~Context() {
   }
   if (ev_fork) cudaEventDestroy(ev_fork);
   if (ev_join) cudaEventDestroy(ev_join);
-  if (ev_skew) cudaEventDestroy(ev_skew);
   if (own_stream && stream) cudaStreamDestroy(stream);
 }
 
@@ -767,13 +766,11 @@ Status Context::init(const ParamSpec &spec, int dev, std::string *err) {
   own_stream = true;
   if (cudaStreamCreateWithFlags(&aux_stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&ev_skew, cudaEventDisableTiming) != cudaSuccess) {
+      cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming) != cudaSuccess) {
     *err = "auxiliary stream creation failed";
     return kErrCuda;
   }
   if (const char *e = std::getenv("CHD_SPLIT_STREAMS")) split_streams = std::atoi(e) != 0;
-  if (const char *e = std::getenv("CHD_SPLIT_SKEW")) skew_halves = std::atoi(e) != 0;
   const int n = P->n, np_all = P->L + P->alpha;
   // twiddles, NTT.cu:1233-1299: psi_rev[j] = psi^brev(j); stored plain with
   // the Shoup companion floor(w 2^32 / q)
@@ -1321,7 +1318,6 @@ Status Context::key_switch_fused_pipeline(const int *levels, int count, const KS
     nl++;
   });
   timer_span(kKsInvRows, t0, nl);
-  mark_first_stage();
   MSColBatch b{};
   b.engine = ks_engine;
   b.err = d_err;
@@ -1534,26 +1530,13 @@ Status Context::moddown(int level, MDType type, const uint32_t *const *src, uint
   });
 }
 
-void Context::mark_first_stage() {
-  if (!skew_pending) return;
-  skew_pending = false;
-  skew_recorded = cudaEventRecord(ev_skew, stream) == cudaSuccess;
-}
-
 Status Context::fork_halves(const std::function<Status(bool)> &half) {
   // the halves' scratch stays allocated until both are enqueued; later work
   // on the context stream is ordered after the join
   ArenaScope scope(arena);
   CHD_CHECK(cudaEventRecord(ev_fork, stream) == cudaSuccess && cudaStreamWaitEvent(aux_stream, ev_fork, 0) == cudaSuccess,
             kErrCuda, "stream fork failed");
-  // with skew_halves the second half starts when the first half's first
-  // stage has finished, so that stage k + 1 of one half runs beside stage k
-  // of the other
-  skew_pending = skew_halves;
-  skew_recorded = false;
   Status st = half(false);
-  skew_pending = false;
-  if (st == kOk && skew_recorded) st = cudaStreamWaitEvent(aux_stream, ev_skew, 0) == cudaSuccess ? kOk : kErrCuda;
   if (st == kOk) {
     cudaStream_t main_stream = stream;
     stream = aux_stream;
@@ -1620,7 +1603,6 @@ Status Context::moddown_pipeline(int level, MDType type, const uint32_t *const *
     }
   if (fused) {
     for_row_batches(rows, [&](const RowBatch &rb) { launch_ntt_inv_rows(rb, P->log_n, stream); });
-    mark_first_stage();
     MSColBatch b{};
     b.engine = ks_engine;
     b.err = d_err;

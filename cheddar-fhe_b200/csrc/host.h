@@ -357,10 +357,7 @@ class Context {
   // on barriers and the tensor cores, the row passes on the ALU)
   bool split_streams = true;
   cudaStream_t aux_stream = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_skew = nullptr;
-  // the second half waits for the first half's first stage (see fork_halves)
-  bool skew_halves = false, skew_pending = false, skew_recorded = false;
-  void mark_first_stage();  // records ev_skew once when a fork asks for it
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   uint2 *d_tw = nullptr, *d_itw = nullptr;  // [nprimes][N] (psi_rev, Shoup companion)
   std::vector<uint32_t> n_inv, n_inv_mont, mont_conv, p_prod, imag_unit;
   std::vector<uint32_t> r_inv;  // 2^-32 mod q per global prime
