@@ -580,8 +580,9 @@ Status Context64::modup(int level, const u64 *src, u64 *dst) {
   const int nq = np.q(), tot = np.total();
   std::vector<int> g(tot);
   P->gidx(np, g.data());
-  i64 *xt = nullptr;
-  if (cudaMallocAsync(&xt, static_cast<size_t>(nq) * n * 8, stream) != cudaSuccess) {
+  ArenaScope scope(arena);
+  i64 *xt = static_cast<i64 *>(arena.alloc(static_cast<size_t>(nq) * n * 8));
+  if (!xt) {
     set_error("modup64: scratch allocation failed");
     return kErrAlloc;
   }
@@ -633,7 +634,6 @@ Status Context64::modup(int level, const u64 *src, u64 *dst) {
   }
   launch_bconv64(b, stream);
   for_batches64(rows, [&](const RowBatch64 &rb) { launch_ntt64_fwd(rb, stream); });
-  cudaFreeAsync(xt, stream);
   return check("modup64");
 }
 
@@ -667,8 +667,9 @@ Status Context64::moddown(int level, MDType type, const u64 *const *src, u64 *co
     for (int r = 0; r < ns.ter - nn.ter; r++) srows.push_back(r);
   for (int a = 0; a < nsa; a++) srows.push_back(ns.q() + a);
   CHD_CHECK(static_cast<int>(srows.size()) == src_len, kErrInvalidArg, "moddown64: internal row mismatch");
-  i64 *xt = nullptr;
-  if (cudaMallocAsync(&xt, static_cast<size_t>(npoly) * src_len * n * 8, stream) != cudaSuccess) {
+  ArenaScope scope(arena);
+  i64 *xt = static_cast<i64 *>(arena.alloc(static_cast<size_t>(npoly) * src_len * n * 8));
+  if (!xt) {
     set_error("moddown64: scratch allocation failed");
     return kErrAlloc;
   }
@@ -728,7 +729,6 @@ Status Context64::moddown(int level, MDType type, const u64 *const *src, u64 *co
       rows.push_back(d);
     }
   for_batches64(rows, [&](const RowBatch64 &rb) { launch_ntt64_fwd(rb, stream); });
-  cudaFreeAsync(xt, stream);
   return check("moddown64");
 }
 
@@ -743,9 +743,10 @@ Status Context64::key_mult(int level, const u64 *d, const u64 *d0, const u64 *d1
   const int nq = np.q(), tot = np.total();
   CHD_CHECK(key.np.aux == P->alpha && key.np.q() == P->L, kErrKey, "key switch: key basis mismatch");
   CHD_CHECK(m.beta <= 8, kErrUnsupported, "key switch: more than 8 digits");
-  u64 *mu = nullptr;
   const size_t mw = static_cast<size_t>(tot) * n;
-  if (cudaMallocAsync(&mu, m.beta * mw * 8, stream) != cudaSuccess) {
+  ArenaScope scope(arena);
+  u64 *mu = static_cast<u64 *>(arena.alloc(m.beta * mw * 8));
+  if (!mu) {
     set_error("key switch: scratch allocation failed");
     return kErrAlloc;
   }
@@ -782,7 +783,6 @@ Status Context64::key_mult(int level, const u64 *d, const u64 *d0, const u64 *d1
     }
   }
   launch_key_mac64(kb, stream);
-  cudaFreeAsync(mu, stream);
   return check("key switch64");
 }
 
@@ -800,11 +800,11 @@ Status Context64::hmult(Ct64 &res, const Ct64 &a, const Ct64 &b, const Evk64 &ke
   const int n = P->n, nq = a.np.q(), tot = nq + P->alpha;
   std::vector<int> g(nq);
   P->gidx(a.np, g.data());
-  u64 *d = nullptr, *acc = nullptr;
   const size_t qw = static_cast<size_t>(nq) * n, tw_ = static_cast<size_t>(tot) * n;
-  if (cudaMallocAsync(&d, 3 * qw * 8, stream) != cudaSuccess ||
-      cudaMallocAsync(&acc, 2 * tw_ * 8, stream) != cudaSuccess) {
-    if (d) cudaFreeAsync(d, stream);
+  ArenaScope scope(arena);
+  u64 *d = static_cast<u64 *>(arena.alloc(3 * qw * 8));
+  u64 *acc = static_cast<u64 *>(arena.alloc(2 * tw_ * 8));
+  if (!d || !acc) {
     set_error("HMult: scratch allocation failed");
     return kErrAlloc;
   }
@@ -838,8 +838,6 @@ Status Context64::hmult(Ct64 &res, const Ct64 &a, const Ct64 &b, const Evk64 &ke
   CHD_TRY(moddown(level, do_rescale ? MDType::kModDownRescale : MDType::kModDown, srcs, dsts, 2));
   res.scale = sc;
   res.num_slots = slots;
-  cudaFreeAsync(d, stream);
-  cudaFreeAsync(acc, stream);
   return check("hmult64");
 }
 
@@ -863,10 +861,10 @@ Status Context64::key_switch_permute(Ct64 &res, const Ct64 &a, const Evk64 &key,
   CHD_CHECK(&res != &a, kErrInvalidArg, "HRot64: the result must not alias the input");
   const int n = P->n, nq = a.np.q(), tot = nq + P->alpha;
   const size_t qw = static_cast<size_t>(nq) * n, tw_ = static_cast<size_t>(tot) * n;
-  u64 *acc = nullptr, *ks = nullptr;
-  if (cudaMallocAsync(&acc, 2 * tw_ * 8, stream) != cudaSuccess ||
-      cudaMallocAsync(&ks, 2 * qw * 8, stream) != cudaSuccess) {
-    if (acc) cudaFreeAsync(acc, stream);
+  ArenaScope scope(arena);
+  u64 *acc = static_cast<u64 *>(arena.alloc(2 * tw_ * 8));
+  u64 *ks = static_cast<u64 *>(arena.alloc(2 * qw * 8));
+  if (!acc || !ks) {
     set_error("HRot: scratch allocation failed");
     return kErrAlloc;
   }
@@ -898,8 +896,6 @@ Status Context64::key_switch_permute(Ct64 &res, const Ct64 &a, const Evk64 &key,
   launch_permute64(eb, galois, stream);
   res.scale = sc;
   res.num_slots = sl;
-  cudaFreeAsync(acc, stream);
-  cudaFreeAsync(ks, stream);
   return check("hrot64");
 }
 

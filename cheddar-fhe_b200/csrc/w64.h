@@ -99,6 +99,10 @@ class Context64 {
   int device = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = true;
+  // scratch of the operations: a stack of device chunks reused across calls
+  // (every operation runs on the context stream, so a later call's scratch
+  // may reuse an earlier call's words)
+  Arena arena;
   u64 *d_primes = nullptr;
   i64 *d_qinv = nullptr;
   ulonglong2 *d_tw = nullptr, *d_itw = nullptr;  // [nprimes][N] (w, floor(w 2^64 / q))
