@@ -202,6 +202,25 @@ def lib():
         "chd64_hrot": (i, [vp, vp, vp, vp, i]),
         "chd64_rescale": (i, [vp, vp, vp]),
         "chd64_hconj": (i, [vp, vp, vp, vp]),
+        "chd64_ct_set_rx": (i, [vp, vp, vp, i]),
+        "chd64_ct_export_rx": (i, [vp, vp, vp]),
+        "chd64_ct_has_rx": (i, [vp]),
+        "chd64_scale": (C.c_double, [vp, i]),
+        "chd64_encode_const": (i, [vp, i, C.c_double, C.c_double, i, vp]),
+        "chd64_copy": (i, [vp, vp, vp]),
+        "chd64_neg": (i, [vp, vp, vp]),
+        "chd64_mult_imaginary_unit": (i, [vp, vp, vp]),
+        "chd64_add": (i, [vp, vp, vp, vp]),
+        "chd64_sub": (i, [vp, vp, vp, vp]),
+        "chd64_mult": (i, [vp, vp, vp, vp]),
+        "chd64_relinearize": (i, [vp, vp, vp, vp, i]),
+        "chd64_mult_key": (i, [vp, vp, vp, vp]),
+        "chd64_permute": (i, [vp, vp, vp, i, i]),
+        "chd64_hrot_add": (i, [vp, vp, vp, vp, vp, i]),
+        "chd64_hconj_add": (i, [vp, vp, vp, vp, vp]),
+        "chd64_mult_const": (i, [vp, vp, vp, vp, C.c_double]),
+        "chd64_add_const": (i, [vp, vp, vp, vp]),
+        "chd64_level_down": (i, [vp, vp, vp, i]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -1153,6 +1172,10 @@ class Context64:
         _check(lib().chd64_level_np(self.ptr, level, C.byref(m), C.byref(t)))
         return m.value, t.value
 
+    def scale(self, level):
+        """Parameter::GetScale(level), up to the default encryption level."""
+        return lib().chd64_scale(self.ptr, level)
+
     def primes(self):
         n = lib().chd64_primes(self.ptr, None, 0)
         out = np.zeros(n, dtype=np.uint64)
@@ -1193,6 +1216,70 @@ class Context64:
         _check(lib().chd64_rescale(self.ptr, res.ptr, a.ptr))
         return res
 
+    # ---- Context<uint64_t> operations (Context.h:101-423) ----
+    def _op(self, fn, res, *args):
+        res = res or Ciphertext64(self)
+        _check(fn(self.ptr, res.ptr, *args))
+        return res
+
+    def Copy(self, a, res=None):
+        return self._op(lib().chd64_copy, res, a.ptr)
+
+    def Neg(self, a, res=None):
+        return self._op(lib().chd64_neg, res, a.ptr)
+
+    def MultImaginaryUnit(self, a, res=None):
+        return self._op(lib().chd64_mult_imaginary_unit, res, a.ptr)
+
+    def Add(self, a, b, res=None):
+        return self._op(lib().chd64_add, res, a.ptr, b.ptr)
+
+    def Sub(self, a, b, res=None):
+        return self._op(lib().chd64_sub, res, a.ptr, b.ptr)
+
+    def Mult(self, a, b, res=None):
+        """The three-part tensor (bx, ax, rx) of two ciphertexts."""
+        return self._op(lib().chd64_mult, res, a.ptr, b.ptr)
+
+    def Relinearize(self, a, key, res=None):
+        return self._op(lib().chd64_relinearize, res, a.ptr, key.ptr, 0)
+
+    def RelinearizeRescale(self, a, key, res=None):
+        return self._op(lib().chd64_relinearize, res, a.ptr, key.ptr, 1)
+
+    def MultKey(self, a, key, res=None):
+        return self._op(lib().chd64_mult_key, res, a.ptr, key.ptr)
+
+    def Permute(self, a, rot, res=None):
+        return self._op(lib().chd64_permute, res, a.ptr, rot, 0)
+
+    def PermuteConjugate(self, a, res=None):
+        return self._op(lib().chd64_permute, res, a.ptr, 0, 1)
+
+    def HRotAdd(self, a, b, key, rot, res=None):
+        return self._op(lib().chd64_hrot_add, res, a.ptr, b.ptr, key.ptr, rot)
+
+    def HConjAdd(self, a, b, key, res=None):
+        return self._op(lib().chd64_hconj_add, res, a.ptr, b.ptr, key.ptr)
+
+    def encode_const(self, level, scale, value, num_aux=0):
+        """Encoder::EncodeConstant: one Montgomery word per prime."""
+        m, t = self.level_np(level)
+        out = np.zeros(m + t + num_aux, dtype=np.uint64)
+        _check(lib().chd64_encode_const(self.ptr, level, float(scale), float(value), num_aux, out.ctypes.data))
+        return out
+
+    def MultConst(self, a, cx, const_scale, res=None):
+        cx = np.ascontiguousarray(cx, dtype=np.uint64)
+        return self._op(lib().chd64_mult_const, res, a.ptr, cx.ctypes.data, float(const_scale))
+
+    def AddConst(self, a, cx, res=None):
+        cx = np.ascontiguousarray(cx, dtype=np.uint64)
+        return self._op(lib().chd64_add_const, res, a.ptr, cx.ctypes.data)
+
+    def LevelDown(self, a, target_level, res=None):
+        return self._op(lib().chd64_level_down, res, a.ptr, target_level)
+
 
 class Ciphertext64:
     def __init__(self, ctx):
@@ -1227,12 +1314,22 @@ class Ciphertext64:
         return dict(num_main=m.value, num_ter=t.value, scale=sc.value, num_slots=ns.value)
 
     def numpy(self):
+        """(bx, ax), or (bx, ax, rx) for an unrelinearised ciphertext."""
         inf = self.info()
         rows = inf["num_main"] + inf["num_ter"]
         bx = np.zeros((rows, self.ctx.n), dtype=np.uint64)
         ax = np.zeros_like(bx)
         _check(lib().chd64_ct_export(self.ctx.ptr, self.ptr, bx.ctypes.data, ax.ctypes.data))
+        if lib().chd64_ct_has_rx(self.ptr) == 1:
+            rx = np.zeros_like(bx)
+            _check(lib().chd64_ct_export_rx(self.ctx.ptr, self.ptr, rx.ctypes.data))
+            return bx, ax, rx
         return bx, ax
+
+    def set_rx(self, rx, on_device=False):
+        keep = rx if on_device else np.ascontiguousarray(rx, dtype=np.uint64)
+        _check(lib().chd64_ct_set_rx(self.ctx.ptr, self.ptr, _ptr(keep), int(on_device)))
+        return self
 
 
 class EvaluationKey64:

@@ -229,6 +229,12 @@ std::unique_ptr<Params64> Params64::create(const ParamSpec64 &spec, std::string 
       for (int j = 0; j < -md; j++) den *= static_cast<double>(spec.main_primes[up.main + j]);
     P->rescale_prod[i] = num / den;
   }
+  // scales, Parameter.cu:145-190: the geometric mean of the level below's
+  // scale and the rescale prime product, up to the default encryption level
+  P->scale.assign(spec.default_encryption_level + 1, 0.0);
+  if (!P->scale.empty()) P->scale[0] = spec.base_scale;
+  for (int i = 1; i <= spec.default_encryption_level && i <= P->max_level; i++)
+    P->scale[i] = std::sqrt(P->scale[i - 1] * P->rescale_prod[i]);
   return P;
 }
 
@@ -387,9 +393,10 @@ void build_level_ms64(const Params64 &P, int level, LevelMS64 *out) {
 Ct64::~Ct64() {
   cudaFree(bx);
   cudaFree(ax);
+  cudaFree(rx);
 }
 
-Status Ct64::reserve(const NP &want, int n) {
+Status Ct64::reserve(const NP &want, int n, bool with_rx) {
   const size_t words = static_cast<size_t>(want.total()) * n;
   if (words > cap_words) {
     cudaFree(bx);
@@ -402,8 +409,31 @@ Status Ct64::reserve(const NP &want, int n) {
     }
     cap_words = words;
   }
+  if (with_rx && words > rx_cap_words) {
+    cudaFree(rx);
+    rx = nullptr;
+    rx_cap_words = 0;
+    if (cudaMalloc(&rx, words * 8) != cudaSuccess) {
+      set_error("ciphertext allocation failed");
+      return kErrAlloc;
+    }
+    rx_cap_words = words;
+  }
   np = want;
+  has_rx = with_rx;
   return kOk;
+}
+
+void Ct64::swap(Ct64 &o) {
+  std::swap(np, o.np);
+  std::swap(scale, o.scale);
+  std::swap(num_slots, o.num_slots);
+  std::swap(has_rx, o.has_rx);
+  std::swap(bx, o.bx);
+  std::swap(ax, o.ax);
+  std::swap(rx, o.rx);
+  std::swap(cap_words, o.cap_words);
+  std::swap(rx_cap_words, o.rx_cap_words);
 }
 
 Evk64::~Evk64() {
@@ -473,6 +503,7 @@ Status Context64::init(const ParamSpec64 &spec, int dev, std::string *err) {
       pw[j] = mul_mod(pw[j - 1], psi, q);
       pwi[j] = mul_mod(pwi[j - 1], psi_inv, q);
     }
+    imag_unit.push_back(to_mont(pw[n / 2], q));  // psi^(N/2) = psi_rev[1]
     for (int j = 0; j < n; j++) {
       const unsigned r = brev(j, P->log_n);
       auto sh = [q](u64 w) { return static_cast<u64>((static_cast<u128>(w) << 64) / q); };
@@ -913,6 +944,375 @@ Status Context64::rescale(Ct64 &res, const Ct64 &a) {
   return kOk;
 }
 
+// ---- Context<uint64_t> operations (Context.cpp:101-949) ----------------
+
+namespace {
+// round-toward-zero integer of v reduced to [0, p), exact for every finite
+// double (|v| >= 2^53 is an integer m 2^e)
+u64 trunc_mod64(double v, u64 p) {
+  if (v == 0.0) return 0;
+  const bool neg = v < 0;
+  const double a = std::fabs(v);
+  u64 r;
+  if (a < 18446744073709551616.0) {
+    r = static_cast<u64>(a) % p;
+  } else {
+    int e;
+    const double m = std::frexp(a, &e);
+    const u64 mi = static_cast<u64>(std::ldexp(m, 53));
+    r = mul_mod(mi % p, pow_mod(2, e - 53, p), p);
+  }
+  if (neg && r) r = p - r;
+  return r;
+}
+}  // namespace
+
+void Context64::encode_const(int level, double scale, double value, int num_aux, std::vector<u64> *cx) const {
+  const NP np = P->level_np(level, num_aux);
+  std::vector<int> g(np.total());
+  P->gidx(np, g.data());
+  cx->resize(np.total());
+  const double v = value * scale;
+  for (int k = 0; k < np.total(); k++) (*cx)[k] = to_mont(trunc_mod64(v, P->primes[g[k]]), P->primes[g[k]]);
+}
+
+namespace {
+// one element-wise op over `parts` parts of every row of np
+Status elem_parts64(Context64 &C, Elem64Op op, const NP &np, int parts, u64 *const *dst, const u64 *const *a,
+                    const u64 *const *b, const u64 *k) {
+  const int n = C.P->n, tot = np.total();
+  std::vector<int> g(tot);
+  C.P->gidx(np, g.data());
+  Elem64Batch eb{};
+  for (int p = 0; p < parts; p++)
+    for (int r = 0; r < tot; r++) {
+      Elem64Row &e = eb.rows[eb.count++];
+      e = Elem64Row{};
+      const size_t o = static_cast<size_t>(r) * n;
+      e.a1 = a[p] + o;
+      e.b1 = b ? b[p] + o : nullptr;
+      e.o0 = dst[p] + o;
+      e.q = C.P->primes[g[r]];
+      e.qinv = C.P->qinv[g[r]];
+      e.c = k ? k[r] : 0;
+      if (eb.count == kMaxElem64Rows) {
+        launch_elem64(op, eb, C.stream);
+        eb.count = 0;
+      }
+    }
+  launch_elem64(op, eb, C.stream);
+  return C.check("elementwise64");
+}
+
+// the result of an operation that grows `res` while res is also an operand:
+// compute into a temporary, then take its buffers
+template <class F>
+Status via_temp(Ct64 &res, F &&f) {
+  Ct64 tmp;
+  CHD_TRY(f(tmp));
+  res.swap(tmp);
+  return kOk;
+}
+}  // namespace
+
+Status Context64::copy(Ct64 &res, const Ct64 &a) {
+  if (&res == &a) return kOk;
+  const NP np = a.np;
+  CHD_TRY(res.reserve(np, P->n, a.has_rx));
+  const size_t bytes = static_cast<size_t>(np.total()) * P->n * 8;
+  cudaMemcpyAsync(res.bx, a.bx, bytes, cudaMemcpyDeviceToDevice, stream);
+  cudaMemcpyAsync(res.ax, a.ax, bytes, cudaMemcpyDeviceToDevice, stream);
+  if (a.has_rx) cudaMemcpyAsync(res.rx, a.rx, bytes, cudaMemcpyDeviceToDevice, stream);
+  res.scale = a.scale;
+  res.num_slots = a.num_slots;
+  return check("copy64");
+}
+
+Status Context64::add(Ct64 &res, const Ct64 &a, const Ct64 &b) {
+  // Context.cpp:145-172: with rx on one side only, the result keeps it
+  CHD_CHECK(a.np == b.np, kErrShape, "Add: level mismatch");
+  const bool out_rx = a.has_rx || b.has_rx, both_rx = a.has_rx && b.has_rx;
+  if ((&res == &a || &res == &b) && out_rx && !res.has_rx)
+    return via_temp(res, [&](Ct64 &t) { return add(t, a, b); });
+  const u64 *keep_rx = (!both_rx && out_rx) ? (a.has_rx ? a.rx : b.rx) : nullptr;
+  const NP np = a.np;
+  const u64 *pa[3] = {a.bx, a.ax, a.rx}, *pb[3] = {b.bx, b.ax, b.rx};
+  const double sc = a.scale;
+  const int slots = std::max(a.num_slots, b.num_slots);
+  CHD_TRY(res.reserve(np, P->n, out_rx));
+  u64 *pd[3] = {res.bx, res.ax, res.rx};
+  CHD_TRY(elem_parts64(*this, Elem64Op::kAdd, np, both_rx ? 3 : 2, pd, pa, pb, nullptr));
+  if (keep_rx && keep_rx != res.rx)
+    cudaMemcpyAsync(res.rx, keep_rx, static_cast<size_t>(np.total()) * P->n * 8, cudaMemcpyDeviceToDevice, stream);
+  res.scale = sc;
+  res.num_slots = slots;
+  return check("add64");
+}
+
+Status Context64::sub(Ct64 &res, const Ct64 &a, const Ct64 &b) {
+  // Context.cpp:205-229: with rx on one side only, res.rx = a.rx or -b.rx
+  CHD_CHECK(a.np == b.np, kErrShape, "Sub: level mismatch");
+  const bool out_rx = a.has_rx || b.has_rx, both_rx = a.has_rx && b.has_rx;
+  if ((&res == &a || &res == &b) && out_rx && !res.has_rx)
+    return via_temp(res, [&](Ct64 &t) { return sub(t, a, b); });
+  const u64 *only_rx = (!both_rx && out_rx) ? (a.has_rx ? a.rx : b.rx) : nullptr;
+  const bool neg_rx = !both_rx && b.has_rx;
+  const NP np = a.np;
+  const u64 *pa[3] = {a.bx, a.ax, a.rx}, *pb[3] = {b.bx, b.ax, b.rx};
+  const double sc = a.scale;
+  const int slots = std::max(a.num_slots, b.num_slots);
+  CHD_TRY(res.reserve(np, P->n, out_rx));
+  u64 *pd[3] = {res.bx, res.ax, res.rx};
+  CHD_TRY(elem_parts64(*this, Elem64Op::kSub, np, both_rx ? 3 : 2, pd, pa, pb, nullptr));
+  if (neg_rx) {
+    const u64 *src[1] = {only_rx};
+    u64 *dst[1] = {res.rx};
+    CHD_TRY(elem_parts64(*this, Elem64Op::kNeg, np, 1, dst, src, nullptr, nullptr));
+  } else if (only_rx && only_rx != res.rx) {
+    cudaMemcpyAsync(res.rx, only_rx, static_cast<size_t>(np.total()) * P->n * 8, cudaMemcpyDeviceToDevice, stream);
+  }
+  res.scale = sc;
+  res.num_slots = slots;
+  return check("sub64");
+}
+
+Status Context64::neg(Ct64 &res, const Ct64 &a) {
+  const NP np = a.np;
+  const bool rx = a.has_rx;
+  const u64 *pa[3] = {a.bx, a.ax, a.rx};
+  const double sc = a.scale;
+  const int slots = a.num_slots;
+  CHD_TRY(res.reserve(np, P->n, rx));
+  u64 *pd[3] = {res.bx, res.ax, res.rx};
+  CHD_TRY(elem_parts64(*this, Elem64Op::kNeg, np, rx ? 3 : 2, pd, pa, nullptr, nullptr));
+  res.scale = sc;
+  res.num_slots = slots;
+  return kOk;
+}
+
+Status Context64::mult_tensor(Ct64 &res, const Ct64 &a, const Ct64 &b) {
+  // Context.cpp:316-330: (b1 b2, b1 a2 + a1 b2, a1 a2)
+  CHD_CHECK(a.np == b.np && a.np.aux == 0, kErrShape, "Mult: level mismatch");
+  CHD_CHECK(!a.has_rx && !b.has_rx, kErrShape, "Relinearization required before Mult Ct x Ct");
+  CHD_CHECK(&res != &a && &res != &b, kErrInvalidArg, "Mult: result must not alias an operand");
+  const int n = P->n, nq = a.np.q();
+  CHD_TRY(res.reserve(a.np, n, true));
+  std::vector<int> g(nq);
+  P->gidx(a.np, g.data());
+  Elem64Batch eb{};
+  for (int r = 0; r < nq; r++) {
+    Elem64Row &e = eb.rows[eb.count++];
+    e = Elem64Row{};
+    const size_t o = static_cast<size_t>(r) * n;
+    e.b1 = a.bx + o;
+    e.a1 = a.ax + o;
+    e.b2 = b.bx + o;
+    e.a2 = b.ax + o;
+    e.o0 = res.bx + o;
+    e.o1 = res.ax + o;
+    e.o2 = res.rx + o;
+    e.q = P->primes[g[r]];
+    e.qinv = P->qinv[g[r]];
+    if (eb.count == kMaxElem64Rows) {
+      launch_tensor64(eb, stream);
+      eb.count = 0;
+    }
+  }
+  launch_tensor64(eb, stream);
+  res.scale = a.scale * b.scale;
+  res.num_slots = std::max(a.num_slots, b.num_slots);
+  return check("mult64");
+}
+
+Status Context64::relinearize(Ct64 &res, const Ct64 &a, const Evk64 &key, bool do_rescale) {
+  // Relinearize / RelinearizeRescale (Context.cpp:650-737): the key switch
+  // of rx with P (bx, ax) added, then ModDown or ModDownAndRescale
+  CHD_CHECK(a.has_rx && a.np.aux == 0, kErrShape, "Relinearize: input must have rx and no aux primes");
+  const int level = level_of(*P, a);
+  CHD_CHECK(level >= 0, kErrInvalidLevel, "Relinearize: invalid level");
+  CHD_CHECK(!do_rescale || level >= 1, kErrInvalidLevel, "Not enough q primes to rescale");
+  if (&res == &a) return via_temp(res, [&](Ct64 &t) { return relinearize(t, a, key, do_rescale); });
+  const int n = P->n, tot = a.np.q() + P->alpha;
+  const size_t tw_ = static_cast<size_t>(tot) * n;
+  ArenaScope scope(arena);
+  u64 *acc = static_cast<u64 *>(arena.alloc(2 * tw_ * 8));
+  if (!acc) {
+    set_error("Relinearize: scratch allocation failed");
+    return kErrAlloc;
+  }
+  CHD_TRY(key_mult(level, a.rx, a.bx, a.ax, key, acc, acc + tw_));
+  const double sc = do_rescale ? a.scale / P->rescale_prod[level] : a.scale;
+  const int slots = a.num_slots;
+  CHD_TRY(res.reserve(P->level_np(do_rescale ? level - 1 : level), n));
+  const u64 *srcs[2] = {acc, acc + tw_};
+  u64 *dsts[2] = {res.bx, res.ax};
+  CHD_TRY(moddown(level, do_rescale ? MDType::kModDownRescale : MDType::kModDown, srcs, dsts, 2));
+  res.scale = sc;
+  res.num_slots = slots;
+  return check("relinearize64");
+}
+
+Status Context64::mult_key(Ct64 &res, const Ct64 &a, const Evk64 &key) {
+  // MultKey (Context.cpp:584-607): the key switch of ax, P bx added to the
+  // b accumulator, then ModDown
+  CHD_CHECK(!a.has_rx && a.np.aux == 0, kErrShape, "MultKey: input must be relinearised, without aux primes");
+  const int level = level_of(*P, a);
+  CHD_CHECK(level >= 0, kErrInvalidLevel, "MultKey: invalid level");
+  if (&res == &a) return via_temp(res, [&](Ct64 &t) { return mult_key(t, a, key); });
+  const int n = P->n, tot = a.np.q() + P->alpha;
+  const size_t tw_ = static_cast<size_t>(tot) * n;
+  ArenaScope scope(arena);
+  u64 *acc = static_cast<u64 *>(arena.alloc(2 * tw_ * 8));
+  if (!acc) {
+    set_error("MultKey: scratch allocation failed");
+    return kErrAlloc;
+  }
+  CHD_TRY(key_mult(level, a.ax, a.bx, nullptr, key, acc, acc + tw_));
+  const double sc = a.scale;
+  const int slots = a.num_slots;
+  CHD_TRY(res.reserve(a.np, n));
+  const u64 *srcs[2] = {acc, acc + tw_};
+  u64 *dsts[2] = {res.bx, res.ax};
+  CHD_TRY(moddown(level, MDType::kModDown, srcs, dsts, 2));
+  res.scale = sc;
+  res.num_slots = slots;
+  return check("mult_key64");
+}
+
+Status Context64::permute(Ct64 &res, const Ct64 &a, int rot, bool conjugate) {
+  // Permute / PermuteConjugate (Context.cpp:486-530): the automorphism on
+  // every part
+  CHD_CHECK(a.np.aux == 0, kErrShape, "Permute: no aux primes");
+  u64 galois = 0;
+  if (conjugate) {
+    galois = P->galois_of(-1);
+  } else {
+    const int slots = a.num_slots > 0 ? a.num_slots : P->n / 2;
+    int amount = rot % slots;
+    if (amount < 0) amount += slots;
+    if (amount == 0) return copy(res, a);
+    galois = P->galois_of(amount);
+  }
+  if (&res == &a) return via_temp(res, [&](Ct64 &t) { return permute(t, a, rot, conjugate); });
+  const int n = P->n, nq = a.np.q();
+  const bool rx = a.has_rx;
+  CHD_TRY(res.reserve(a.np, n, rx));
+  std::vector<int> g(nq);
+  P->gidx(a.np, g.data());
+  const u64 *src[3] = {a.bx, a.ax, a.rx};
+  u64 *dst[3] = {res.bx, res.ax, res.rx};
+  Elem64Batch eb{};
+  for (int p = 0; p < (rx ? 3 : 2); p++)
+    for (int r = 0; r < nq; r++) {
+      Elem64Row &e = eb.rows[eb.count++];
+      e = Elem64Row{};
+      e.a1 = src[p] + static_cast<size_t>(r) * n;
+      e.o0 = dst[p] + static_cast<size_t>(r) * n;
+      e.q = P->primes[g[r]];
+      if (eb.count == kMaxElem64Rows) {
+        launch_permute64(eb, galois, stream);
+        eb.count = 0;
+      }
+    }
+  launch_permute64(eb, galois, stream);
+  res.scale = a.scale;
+  res.num_slots = a.num_slots;
+  return check("permute64");
+}
+
+Status Context64::hrot_add(Ct64 &res, const Ct64 &a, const Ct64 &b, const Evk64 &key, int rot) {
+  // HRotAdd (Context.cpp:800-830): HRot(a) + b
+  CHD_CHECK(a.np == b.np, kErrShape, "HRotAdd: level mismatch");
+  Ct64 t;
+  CHD_TRY(hrot(t, a, key, rot));
+  return add(res, t, b);
+}
+
+Status Context64::hconj_add(Ct64 &res, const Ct64 &a, const Ct64 &b, const Evk64 &key) {
+  // HConjAdd (Context.cpp:832-860): HConj(a) + b
+  CHD_CHECK(a.np == b.np, kErrShape, "HConjAdd: level mismatch");
+  Ct64 t;
+  CHD_TRY(hconj(t, a, key));
+  return add(res, t, b);
+}
+
+Status Context64::mult_imag_unit(Ct64 &res, const Ct64 &a) {
+  // ElementWise.cu:625-658: multiply by X^(N/2) = +-psi^(N/2)
+  CHD_CHECK(a.np.aux == 0, kErrShape, "MultImaginaryUnit: no aux primes");
+  const NP np = a.np;
+  std::vector<int> g(np.total());
+  P->gidx(np, g.data());
+  std::vector<u64> k(np.total());
+  for (int r = 0; r < np.total(); r++) k[r] = imag_unit[g[r]];
+  const bool rx = a.has_rx;
+  const u64 *pa[3] = {a.bx, a.ax, a.rx};
+  const double sc = a.scale;
+  const int slots = a.num_slots;
+  CHD_TRY(res.reserve(np, P->n, rx));
+  u64 *pd[3] = {res.bx, res.ax, res.rx};
+  CHD_TRY(elem_parts64(*this, Elem64Op::kMultImagUnit, np, rx ? 3 : 2, pd, pa, nullptr, k.data()));
+  res.scale = sc;
+  res.num_slots = slots;
+  return kOk;
+}
+
+Status Context64::mult_const(Ct64 &res, const Ct64 &a, const u64 *cx, double cscale) {
+  const NP np = a.np;
+  const bool rx = a.has_rx;
+  const u64 *pa[3] = {a.bx, a.ax, a.rx};
+  const double sc = a.scale * cscale;
+  const int slots = a.num_slots;
+  CHD_TRY(res.reserve(np, P->n, rx));
+  u64 *pd[3] = {res.bx, res.ax, res.rx};
+  CHD_TRY(elem_parts64(*this, Elem64Op::kMultConst, np, rx ? 3 : 2, pd, pa, nullptr, cx));
+  res.scale = sc;
+  res.num_slots = slots;
+  return kOk;
+}
+
+Status Context64::add_const(Ct64 &res, const Ct64 &a, const u64 *cx) {
+  // Context.cpp:174-203: the constant is added to bx, ax and rx are copied
+  const NP np = a.np;
+  const bool rx = a.has_rx;
+  if (&res == &a && rx && !res.has_rx) return via_temp(res, [&](Ct64 &t) { return add_const(t, a, cx); });
+  const u64 *keep[2] = {a.ax, a.rx};
+  const u64 *pa[1] = {a.bx};
+  const double sc = a.scale;
+  const int slots = a.num_slots;
+  CHD_TRY(res.reserve(np, P->n, rx));
+  u64 *pd[1] = {res.bx};
+  CHD_TRY(elem_parts64(*this, Elem64Op::kAddConst, np, 1, pd, pa, nullptr, cx));
+  const size_t bytes = static_cast<size_t>(np.total()) * P->n * 8;
+  if (keep[0] != res.ax) cudaMemcpyAsync(res.ax, keep[0], bytes, cudaMemcpyDeviceToDevice, stream);
+  if (rx && keep[1] != res.rx) cudaMemcpyAsync(res.rx, keep[1], bytes, cudaMemcpyDeviceToDevice, stream);
+  res.scale = sc;
+  res.num_slots = slots;
+  return check("add_const64");
+}
+
+Status Context64::level_down(Ct64 &res, const Ct64 &a, int target_level) {
+  // LevelDown (Context.cpp:917-928): per level, times the constant 1 at
+  // that level's scale, then Rescale
+  CHD_CHECK(a.np.aux == 0 && !a.has_rx, kErrShape, "LevelDown: relinearised input without aux primes required");
+  const int level = level_of(*P, a);
+  CHD_CHECK(level >= 0 && target_level >= 0 && level >= target_level, kErrInvalidLevel,
+            "Invalid target level for LevelDown");
+  CHD_CHECK(level <= P->spec.default_encryption_level, kErrInvalidLevel,
+            "LevelDown: input above the default encryption level (no level-down constant there)");
+  if (level == target_level) return copy(res, a);
+  Ct64 cur, tmp;
+  const Ct64 *prev = &a;
+  std::vector<u64> cx;
+  for (int i = level; i > target_level; i--) {
+    encode_const(i, P->scale.at(i), 1.0, 0, &cx);
+    CHD_TRY(mult_const(tmp, *prev, cx.data(), P->scale.at(i)));
+    CHD_TRY(rescale(cur, tmp));
+    prev = &cur;
+  }
+  res.swap(cur);
+  return kOk;
+}
+
 }  // namespace w64
 }  // namespace chd
 
@@ -934,6 +1334,10 @@ namespace {
 int fail64(int code, const std::string &m) {
   set_error(m);
   return code;
+}
+Status missing64(const char *what) {
+  set_error(std::string(what) + ": null argument");
+  return kErrInvalidArg;
 }
 }  // namespace
 
@@ -1180,5 +1584,106 @@ int chd64_rescale(chd64_context *ctx, chd64_ciphertext *res, const chd64_ciphert
 } catch (const std::exception &e) {
   return fail64(CHD_ERR_INTERNAL, e.what());
 }
+
+int chd64_ct_set_rx(chd64_context *ctx, chd64_ciphertext *ct, const uint64_t *rx, int src_on_device) try {
+  CHD64_CTX(ctx);
+  Context64 &C = *ctx->c;
+  if (!ct || !rx) return fail64(CHD_ERR_INVALID_ARG, "chd64_ct_set_rx: null argument");
+  if (!ct->ct.bx) return fail64(CHD_ERR_INVALID_ARG, "chd64_ct_set_rx: import bx and ax first");
+  const NP np = ct->ct.np;
+  // keep bx / ax: reserve grows only the rx buffer here
+  const Status s = ct->ct.reserve(np, C.P->n, true);
+  if (s != kOk) return s;
+  const size_t bytes = static_cast<size_t>(np.total()) * C.P->n * 8;
+  cudaMemcpyAsync(ct->ct.rx, rx, bytes, src_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, C.stream);
+  const cudaError_t e = cudaStreamSynchronize(C.stream);
+  return e == cudaSuccess ? CHD_OK : fail64(CHD_ERR_CUDA, cudaGetErrorString(e));
+} catch (const std::exception &e) {
+  return fail64(CHD_ERR_INTERNAL, e.what());
+}
+
+int chd64_ct_export_rx(chd64_context *ctx, const chd64_ciphertext *ct, uint64_t *rx) try {
+  CHD64_CTX(ctx);
+  Context64 &C = *ctx->c;
+  if (!ct || !rx) return fail64(CHD_ERR_INVALID_ARG, "chd64_ct_export_rx: null argument");
+  if (!ct->ct.has_rx) return fail64(CHD_ERR_INVALID_ARG, "chd64_ct_export_rx: the ciphertext has no rx");
+  const size_t bytes = static_cast<size_t>(ct->ct.np.total()) * C.P->n * 8;
+  cudaMemcpyAsync(rx, ct->ct.rx, bytes, cudaMemcpyDeviceToHost, C.stream);
+  const cudaError_t e = cudaStreamSynchronize(C.stream);
+  return e == cudaSuccess ? CHD_OK : fail64(CHD_ERR_CUDA, cudaGetErrorString(e));
+} catch (const std::exception &e) {
+  return fail64(CHD_ERR_INTERNAL, e.what());
+}
+
+int chd64_ct_has_rx(const chd64_ciphertext *ct) { return ct ? (ct->ct.has_rx ? 1 : 0) : -1; }
+
+double chd64_scale(const chd64_context *ctx, int level) {
+  if (!ctx || level < 0 || level >= static_cast<int>(ctx->c->P->scale.size())) return 0.0;
+  return ctx->c->P->scale[level];
+}
+
+int chd64_encode_const(chd64_context *ctx, int level, double scale, double value, int num_aux, uint64_t *cx) try {
+  CHD64_CTX(ctx);
+  Context64 &C = *ctx->c;
+  if (!cx) return fail64(CHD_ERR_INVALID_ARG, "chd64_encode_const: null output");
+  if (level < -1 || level > C.P->max_level) return fail64(CHD_ERR_INVALID_LEVEL, "chd64_encode_const: invalid level");
+  if (num_aux < 0 || num_aux > C.P->alpha) return fail64(CHD_ERR_INVALID_ARG, "chd64_encode_const: invalid num_aux");
+  std::vector<u64> v;
+  C.encode_const(level, scale, value, num_aux, &v);
+  std::memcpy(cx, v.data(), v.size() * 8);
+  return CHD_OK;
+} catch (const std::exception &e) {
+  return fail64(CHD_ERR_INTERNAL, e.what());
+}
+
+// Context<uint64_t> operations: null checks, then the operation's status
+#define CHD64_OP(name, args, ...)                                         \
+  int name args try {                                                     \
+    CHD64_CTX(ctx);                                                       \
+    if (!res || !a) return fail64(CHD_ERR_INVALID_ARG, #name ": null argument"); \
+    const Status s = __VA_ARGS__;                                         \
+    return s == kOk ? CHD_OK : s;                                         \
+  } catch (const std::exception &e) {                                     \
+    return fail64(CHD_ERR_INTERNAL, e.what());                            \
+  }
+
+CHD64_OP(chd64_copy, (chd64_context * ctx, chd64_ciphertext *res, const chd64_ciphertext *a),
+         ctx->c->copy(res->ct, a->ct))
+CHD64_OP(chd64_neg, (chd64_context * ctx, chd64_ciphertext *res, const chd64_ciphertext *a),
+         ctx->c->neg(res->ct, a->ct))
+CHD64_OP(chd64_mult_imaginary_unit, (chd64_context * ctx, chd64_ciphertext *res, const chd64_ciphertext *a),
+         ctx->c->mult_imag_unit(res->ct, a->ct))
+CHD64_OP(chd64_add, (chd64_context * ctx, chd64_ciphertext *res, const chd64_ciphertext *a, const chd64_ciphertext *b),
+         b ? ctx->c->add(res->ct, a->ct, b->ct) : missing64("chd64_add"))
+CHD64_OP(chd64_sub, (chd64_context * ctx, chd64_ciphertext *res, const chd64_ciphertext *a, const chd64_ciphertext *b),
+         b ? ctx->c->sub(res->ct, a->ct, b->ct) : missing64("chd64_sub"))
+CHD64_OP(chd64_mult, (chd64_context * ctx, chd64_ciphertext *res, const chd64_ciphertext *a, const chd64_ciphertext *b),
+         b ? ctx->c->mult_tensor(res->ct, a->ct, b->ct) : missing64("chd64_mult"))
+CHD64_OP(chd64_relinearize,
+         (chd64_context * ctx, chd64_ciphertext *res, const chd64_ciphertext *a, const chd64_evk *key, int rescale),
+         key ? ctx->c->relinearize(res->ct, a->ct, key->k, rescale != 0) : missing64("chd64_relinearize"))
+CHD64_OP(chd64_mult_key, (chd64_context * ctx, chd64_ciphertext *res, const chd64_ciphertext *a, const chd64_evk *key),
+         key ? ctx->c->mult_key(res->ct, a->ct, key->k) : missing64("chd64_mult_key"))
+CHD64_OP(chd64_permute,
+         (chd64_context * ctx, chd64_ciphertext *res, const chd64_ciphertext *a, int rot, int conjugate),
+         ctx->c->permute(res->ct, a->ct, rot, conjugate != 0))
+CHD64_OP(chd64_hrot_add,
+         (chd64_context * ctx, chd64_ciphertext *res, const chd64_ciphertext *a, const chd64_ciphertext *b,
+          const chd64_evk *key, int rot),
+         b && key ? ctx->c->hrot_add(res->ct, a->ct, b->ct, key->k, rot) : missing64("chd64_hrot_add"))
+CHD64_OP(chd64_hconj_add,
+         (chd64_context * ctx, chd64_ciphertext *res, const chd64_ciphertext *a, const chd64_ciphertext *b,
+          const chd64_evk *key),
+         b && key ? ctx->c->hconj_add(res->ct, a->ct, b->ct, key->k) : missing64("chd64_hconj_add"))
+CHD64_OP(chd64_mult_const,
+         (chd64_context * ctx, chd64_ciphertext *res, const chd64_ciphertext *a, const uint64_t *cx,
+          double const_scale),
+         cx ? ctx->c->mult_const(res->ct, a->ct, cx, const_scale) : missing64("chd64_mult_const"))
+CHD64_OP(chd64_add_const, (chd64_context * ctx, chd64_ciphertext *res, const chd64_ciphertext *a, const uint64_t *cx),
+         cx ? ctx->c->add_const(res->ct, a->ct, cx) : missing64("chd64_add_const"))
+CHD64_OP(chd64_level_down,
+         (chd64_context * ctx, chd64_ciphertext *res, const chd64_ciphertext *a, int target_level),
+         ctx->c->level_down(res->ct, a->ct, target_level))
+#undef CHD64_OP
 
 }  // extern "C"

@@ -48,6 +48,7 @@ class Params64 {
   std::vector<u64> primes;  // ter reversed, main, aux
   std::vector<i64> qinv;
   std::vector<double> rescale_prod;
+  std::vector<double> scale;  // per level up to the default encryption level
   NP level_np(int level, int num_aux = 0) const;
   int np_to_level(const NP &np) const;
   void gidx(const NP &np, int *out) const;
@@ -75,13 +76,17 @@ struct Ct64 {
   NP np;
   double scale = 1.0;
   int num_slots = 0;
-  u64 *bx = nullptr, *ax = nullptr;
-  size_t cap_words = 0;
+  bool has_rx = false;  // the third part of an unrelinearised product
+  u64 *bx = nullptr, *ax = nullptr, *rx = nullptr;
+  size_t cap_words = 0, rx_cap_words = 0;
   Ct64() = default;
   Ct64(const Ct64 &) = delete;
   Ct64 &operator=(const Ct64 &) = delete;
   ~Ct64();
-  Status reserve(const NP &np, int n);
+  // capacity for np (and an rx part when rx); keeps the words already there
+  // only when no buffer grows
+  Status reserve(const NP &np, int n, bool rx = false);
+  void swap(Ct64 &o);
 };
 
 struct Evk64 {
@@ -129,6 +134,27 @@ class Context64 {
   Status hconj(Ct64 &res, const Ct64 &a, const Evk64 &key);
   Status key_switch_permute(Ct64 &res, const Ct64 &a, const Evk64 &key, u64 galois);
   Status rescale(Ct64 &res, const Ct64 &a);
+  // Context<uint64_t> operations (Context.cpp:101-949): element-wise
+  // arithmetic, the three-part tensor, relinearisation, key switching
+  // without the automorphism, automorphisms, level-down
+  Status copy(Ct64 &res, const Ct64 &a);
+  Status add(Ct64 &res, const Ct64 &a, const Ct64 &b);
+  Status sub(Ct64 &res, const Ct64 &a, const Ct64 &b);
+  Status neg(Ct64 &res, const Ct64 &a);
+  Status mult_tensor(Ct64 &res, const Ct64 &a, const Ct64 &b);
+  Status relinearize(Ct64 &res, const Ct64 &a, const Evk64 &key, bool rescale);
+  Status mult_key(Ct64 &res, const Ct64 &a, const Evk64 &key);
+  Status permute(Ct64 &res, const Ct64 &a, int rot, bool conjugate);
+  Status hrot_add(Ct64 &res, const Ct64 &a, const Ct64 &b, const Evk64 &key, int rot);
+  Status hconj_add(Ct64 &res, const Ct64 &a, const Ct64 &b, const Evk64 &key);
+  Status mult_imag_unit(Ct64 &res, const Ct64 &a);
+  // constants: one Montgomery word per prime of the operand's basis
+  Status mult_const(Ct64 &res, const Ct64 &a, const u64 *cx, double cscale);
+  Status add_const(Ct64 &res, const Ct64 &a, const u64 *cx);
+  Status level_down(Ct64 &res, const Ct64 &a, int target_level);
+  // Encoder::EncodeConstant (Encode.cpp:250-275) with 64-bit words
+  void encode_const(int level, double scale, double value, int num_aux, std::vector<u64> *cx) const;
+  std::vector<u64> imag_unit;  // psi^(N/2) per prime, Montgomery
   // key switch of d (q primes, NTT domain) with key, plus P (d0, d1) on the
   // q rows (either may be null): acc (b, a) over Q u P
   Status key_mult(int level, const u64 *d, const u64 *d0, const u64 *d1, const Evk64 &key, u64 *acc_b, u64 *acc_a);
@@ -186,6 +212,7 @@ struct Elem64Row {
   u64 *o0, *o1, *o2;
   u64 q;
   i64 qinv;
+  u64 c;  // per-row constant (Elem64Op)
 };
 constexpr int kMaxElem64Rows = 64;
 struct Elem64Batch {
@@ -196,6 +223,11 @@ struct Elem64Batch {
 void launch_tensor64(const Elem64Batch &b, cudaStream_t s);
 // o0 = a1 + b1 (mod q)
 void launch_add64(const Elem64Batch &b, cudaStream_t s);
+// o0 = op(a1[, b1 | c]) on canonical residues; kMult and kMultConst are
+// Montgomery products, kMultImagUnit multiplies by c in the first half of
+// the evaluation domain and by -c in the second (X^(N/2))
+enum class Elem64Op { kAdd, kSub, kNeg, kMult, kMultConst, kAddConst, kCopy, kMultImagUnit };
+void launch_elem64(Elem64Op op, const Elem64Batch &b, cudaStream_t s);
 // o0[k] = a1[galois(k)] (the automorphism in the bit-reversed domain)
 void launch_permute64(const Elem64Batch &b, u64 galois, cudaStream_t s);
 

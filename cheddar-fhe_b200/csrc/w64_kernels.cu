@@ -286,6 +286,25 @@ __global__ void __launch_bounds__(256) k64_add(const __grid_constant__ Elem64Bat
   e.o0[i] = add_mod(e.a1[i], e.b1[i], e.q);
 }
 
+template <Elem64Op OP>
+__global__ void __launch_bounds__(256) k64_elem(const __grid_constant__ Elem64Batch b) {
+  const Elem64Row &e = b.rows[blockIdx.y];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const u64 q = e.q, x = e.a1[i];
+  u64 o;
+  switch (OP) {
+    case Elem64Op::kAdd: o = add_mod(x, e.b1[i], q); break;
+    case Elem64Op::kSub: o = red2q(x + q - e.b1[i], q); break;
+    case Elem64Op::kNeg: o = x ? q - x : 0; break;
+    case Elem64Op::kMult: o = mont_mul(x, e.b1[i], q, e.qinv); break;
+    case Elem64Op::kMultConst: o = mont_mul(x, e.c, q, e.qinv); break;
+    case Elem64Op::kAddConst: o = add_mod(x, e.c, q); break;
+    case Elem64Op::kCopy: o = x; break;
+    case Elem64Op::kMultImagUnit: o = mont_mul(x, (i & 32768) ? q - e.c : e.c, q, e.qinv); break;
+  }
+  e.o0[i] = o;
+}
+
 __device__ __forceinline__ uint32_t brev17(uint32_t x) { return __brev(x) >> 15; }
 
 __global__ void __launch_bounds__(256) k64_permute(const __grid_constant__ Elem64Batch b, u64 galois) {
@@ -339,6 +358,21 @@ void launch_tensor64(const Elem64Batch &b, cudaStream_t s) {
 void launch_add64(const Elem64Batch &b, cudaStream_t s) {
   if (b.count <= 0) return;
   k64_add<<<dim3(65536 / 256, b.count), 256, 0, s>>>(b);
+}
+
+void launch_elem64(Elem64Op op, const Elem64Batch &b, cudaStream_t s) {
+  if (b.count <= 0) return;
+  const dim3 grid(65536 / 256, b.count);
+  switch (op) {
+    case Elem64Op::kAdd: k64_elem<Elem64Op::kAdd><<<grid, 256, 0, s>>>(b); break;
+    case Elem64Op::kSub: k64_elem<Elem64Op::kSub><<<grid, 256, 0, s>>>(b); break;
+    case Elem64Op::kNeg: k64_elem<Elem64Op::kNeg><<<grid, 256, 0, s>>>(b); break;
+    case Elem64Op::kMult: k64_elem<Elem64Op::kMult><<<grid, 256, 0, s>>>(b); break;
+    case Elem64Op::kMultConst: k64_elem<Elem64Op::kMultConst><<<grid, 256, 0, s>>>(b); break;
+    case Elem64Op::kAddConst: k64_elem<Elem64Op::kAddConst><<<grid, 256, 0, s>>>(b); break;
+    case Elem64Op::kCopy: k64_elem<Elem64Op::kCopy><<<grid, 256, 0, s>>>(b); break;
+    case Elem64Op::kMultImagUnit: k64_elem<Elem64Op::kMultImagUnit><<<grid, 256, 0, s>>>(b); break;
+  }
 }
 
 void launch_permute64(const Elem64Batch &b, u64 galois, cudaStream_t s) {

@@ -572,8 +572,8 @@ int chd_params_level_consts(const char *json_text, int level, int kind, int digi
  * reference's layout ([num_primes][N], Montgomery form x 2^64 mod q,
  * bit-reversed evaluation domain).  N = 2^16; the evaluation core: NTT,
  * ModUp / ModDown / Rescale / ModDownAndRescale, HMult (relinearised,
- * optionally rescaled), HRot.  Same status codes; chd_last_error describes
- * failures. ---- */
+ * optionally rescaled), HRot, HConj and the Context operations below.
+ * Same status codes; chd_last_error describes failures. ---- */
 typedef struct chd64_context chd64_context;
 typedef struct chd64_ciphertext chd64_ciphertext;
 typedef struct chd64_evk chd64_evk;
@@ -621,6 +621,46 @@ int chd64_hrot(chd64_context *ctx, chd64_ciphertext *res, const chd64_ciphertext
 /* Context<uint64_t>::HConj (Context.cpp:793-798) with a conjugation key */
 int chd64_hconj(chd64_context *ctx, chd64_ciphertext *res, const chd64_ciphertext *a, const chd64_evk *key);
 int chd64_rescale(chd64_context *ctx, chd64_ciphertext *res, const chd64_ciphertext *a);
+/* The third part (rx, [num_q][N]) of an unrelinearised ciphertext: set
+ * after chd64_ct_import, read back, and whether a ciphertext has one (1 /
+ * 0, -1 for null) */
+int chd64_ct_set_rx(chd64_context *ctx, chd64_ciphertext *ct, const uint64_t *rx, int src_on_device);
+int chd64_ct_export_rx(chd64_context *ctx, const chd64_ciphertext *ct, uint64_t *rx);
+int chd64_ct_has_rx(const chd64_ciphertext *ct);
+/* Parameter::GetScale (Parameter.cu:145-190) for level 0 .. the default
+ * encryption level, 0 otherwise */
+double chd64_scale(const chd64_context *ctx, int level);
+/* Encoder<uint64_t>::EncodeConstant (Encode.cpp:250-275): value x scale,
+ * rounded toward zero, as one Montgomery word per prime of
+ * level_np(level, num_aux) into cx */
+int chd64_encode_const(chd64_context *ctx, int level, double scale, double value, int num_aux, uint64_t *cx);
+/* Context<uint64_t> operations (Context.h:101-423 with word = uint64_t),
+ * same meaning as their 32-bit chd_* counterparts: Copy, Neg,
+ * MultImaginaryUnit (ElementWise.cu:625-658), Add / Sub (rx kept from the
+ * side that has it; Context.cpp:145-229), Mult (the three-part tensor,
+ * Context.cpp:316-330), Relinearize / RelinearizeRescale (rescale != 0),
+ * MultKey, Permute / PermuteConjugate (conjugate != 0), HRotAdd, HConjAdd,
+ * Mult / Add by a constant (one Montgomery word per prime of a's basis,
+ * host memory; the constant's scale multiplies a's) and LevelDown (to
+ * target_level, inputs up to the default encryption level) */
+int chd64_copy(chd64_context *ctx, chd64_ciphertext *res, const chd64_ciphertext *a);
+int chd64_neg(chd64_context *ctx, chd64_ciphertext *res, const chd64_ciphertext *a);
+int chd64_mult_imaginary_unit(chd64_context *ctx, chd64_ciphertext *res, const chd64_ciphertext *a);
+int chd64_add(chd64_context *ctx, chd64_ciphertext *res, const chd64_ciphertext *a, const chd64_ciphertext *b);
+int chd64_sub(chd64_context *ctx, chd64_ciphertext *res, const chd64_ciphertext *a, const chd64_ciphertext *b);
+int chd64_mult(chd64_context *ctx, chd64_ciphertext *res, const chd64_ciphertext *a, const chd64_ciphertext *b);
+int chd64_relinearize(chd64_context *ctx, chd64_ciphertext *res, const chd64_ciphertext *a, const chd64_evk *key,
+                      int rescale);
+int chd64_mult_key(chd64_context *ctx, chd64_ciphertext *res, const chd64_ciphertext *a, const chd64_evk *key);
+int chd64_permute(chd64_context *ctx, chd64_ciphertext *res, const chd64_ciphertext *a, int rot, int conjugate);
+int chd64_hrot_add(chd64_context *ctx, chd64_ciphertext *res, const chd64_ciphertext *a, const chd64_ciphertext *b,
+                   const chd64_evk *key, int rot);
+int chd64_hconj_add(chd64_context *ctx, chd64_ciphertext *res, const chd64_ciphertext *a, const chd64_ciphertext *b,
+                    const chd64_evk *key);
+int chd64_mult_const(chd64_context *ctx, chd64_ciphertext *res, const chd64_ciphertext *a, const uint64_t *cx,
+                     double const_scale);
+int chd64_add_const(chd64_context *ctx, chd64_ciphertext *res, const chd64_ciphertext *a, const uint64_t *cx);
+int chd64_level_down(chd64_context *ctx, chd64_ciphertext *res, const chd64_ciphertext *a, int target_level);
 
 #ifdef __cplusplus
 }

@@ -785,6 +785,81 @@ int refx64_time_hmult(void *p, int level, const uint64_t *a_bx, const uint64_t *
   return rc;
 }
 
+// Context<uint64_t> operations by name (Context.h:101-423) on imported
+// ciphertexts: a (and b) at `level`, each with rx when its rx pointer is
+// given; an imported key of `beta` digits when beta > 0; arg = rotation or
+// target level; (scale, value) = the constant of MultConst / AddConst,
+// encoded by the reference's Encoder::EncodeConstant at `level`.  The
+// result's parts go to out_bx / out_ax (and out_rx when it has rx); info =
+// {num_main, num_ter, has_rx}.
+int refx64_op(void *p, const char *op, int level, const uint64_t *a_bx, const uint64_t *a_ax, const uint64_t *a_rx,
+              const uint64_t *b_bx, const uint64_t *b_ax, const uint64_t *b_rx, int beta, const uint64_t *k_bx,
+              const uint64_t *k_ax, int arg, double scale, double value, uint64_t *out_bx, uint64_t *out_ax,
+              uint64_t *out_rx, int *info) {
+  auto *R = static_cast<RefCtx64 *>(p);
+  Ciphertext<word64> a, b, res;
+  auto load = [&](Ciphertext<word64> &c, const uint64_t *bx, const uint64_t *ax, const uint64_t *rx) {
+    ct_in64(*R, c, level, bx, ax);
+    if (rx) {
+      c.PrepareRx();
+      copy_in64(c.rx_, rx, poly_words(c.GetNP(), R->degree));
+    }
+  };
+  load(a, a_bx, a_ax, a_rx);
+  if (b_bx) load(b, b_bx, b_ax, b_rx);
+  EvaluationKey<word64> key;
+  if (beta > 0) key_in64(*R, key, beta, k_bx, k_ax);
+  const std::string o(op);
+  auto &C = *R->ctx;
+  if (o == "Copy")
+    C.Copy(res, a);
+  else if (o == "Neg")
+    C.Neg(res, a);
+  else if (o == "MultImaginaryUnit")
+    C.MultImaginaryUnit(res, a);
+  else if (o == "Add")
+    C.Add(res, a, b);
+  else if (o == "Sub")
+    C.Sub(res, a, b);
+  else if (o == "Mult")
+    C.Mult(res, a, b);
+  else if (o == "Relinearize")
+    C.Relinearize(res, a, key);
+  else if (o == "RelinearizeRescale")
+    C.RelinearizeRescale(res, a, key);
+  else if (o == "MultKey")
+    C.MultKey(res, a, key);
+  else if (o == "Permute")
+    C.Permute(res, a, arg);
+  else if (o == "PermuteConjugate")
+    C.PermuteConjugate(res, a);
+  else if (o == "HRotAdd")
+    C.HRotAdd(res, a, b, key, arg);
+  else if (o == "HConjAdd")
+    C.HConjAdd(res, a, b, key);
+  else if (o == "LevelDown")
+    C.LevelDown(res, a, arg);
+  else if (o == "MultConst" || o == "AddConst") {
+    Constant<word64> c;
+    C.encoder_.EncodeConstant(c, level, scale, value);
+    if (o == "MultConst")
+      C.Mult(res, a, c);
+    else
+      C.Add(res, a, c);
+  } else {
+    return -2;
+  }
+  const NPInfo np = res.GetNP();
+  const size_t w = poly_words(np, R->degree);
+  copy_out64(out_bx, res.bx_, w);
+  copy_out64(out_ax, res.ax_, w);
+  if (res.HasRx() && out_rx) copy_out64(out_rx, res.rx_, w);
+  info[0] = np.num_main_;
+  info[1] = np.num_ter_;
+  info[2] = res.HasRx() ? 1 : 0;
+  return last_cuda();
+}
+
 int refx64_hrot(void *p, int level, const uint64_t *a_bx, const uint64_t *a_ax, int beta, const uint64_t *k_bx,
                 const uint64_t *k_ax, int rot, uint64_t *out_bx, uint64_t *out_ax) {
   auto *R = static_cast<RefCtx64 *>(p);

@@ -91,6 +91,8 @@ def lib():
             "refx64_hmult": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, C.c_int, vp, vp, C.c_int, vp, vp]),
             "refx64_hrot": (C.c_int, [vp, C.c_int, vp, vp, C.c_int, vp, vp, C.c_int, vp, vp]),
             "refx64_hconj": (C.c_int, [vp, C.c_int, vp, vp, C.c_int, vp, vp, vp, vp]),
+            "refx64_op": (C.c_int, [vp, C.c_char_p, C.c_int, vp, vp, vp, vp, vp, vp, C.c_int, vp, vp, C.c_int,
+                                    C.c_double, C.c_double, vp, vp, vp, vp]),
             "refx64_time_hmult": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, C.c_int, vp, vp, C.c_int, C.c_int, C.c_int,
                                             C.POINTER(C.c_float)]),
         }
@@ -461,6 +463,26 @@ class RefContext64:
         _chk(lib().refx64_hconj(self.ptr, level, a0.ctypes.data, a1.ctypes.data, kb.shape[0], kb.ctypes.data,
                                 ka.ctypes.data, ob.ctypes.data, oa.ctypes.data), "hconj64")
         return ob, oa
+
+    def op(self, name, level, a, b=None, key=None, arg=0, scale=0.0, value=0.0):
+        """Context<uint64_t>::<name> on imported ciphertexts a (and b), each
+        (bx, ax) or (bx, ax, rx) at `level`, and an imported key (kb, ka);
+        returns the result's parts, rx included when it has one."""
+        a = [_u64(x) for x in a]
+        b = [_u64(x) for x in b] if b is not None else None
+        ptr = lambda parts, i: parts[i].ctypes.data if parts is not None and len(parts) > i else None  # noqa: E731
+        kb, ka = (_u64(key[0]), _u64(key[1])) if key is not None else (None, None)
+        rows = a[0].shape[0]
+        ob = np.zeros((rows, self.n), dtype=np.uint64)
+        oa, orx = np.zeros_like(ob), np.zeros_like(ob)
+        info = np.zeros(3, dtype=np.int32)
+        _chk(lib().refx64_op(self.ptr, name.encode(), level, ptr(a, 0), ptr(a, 1), ptr(a, 2), ptr(b, 0), ptr(b, 1),
+                             ptr(b, 2), kb.shape[0] if kb is not None else 0,
+                             kb.ctypes.data if kb is not None else None, ka.ctypes.data if ka is not None else None,
+                             int(arg), float(scale), float(value), ob.ctypes.data, oa.ctypes.data, orx.ctypes.data,
+                             info.ctypes.data), "op64 " + name)
+        r = int(info[0] + info[1])
+        return (ob[:r], oa[:r], orx[:r]) if info[2] else (ob[:r], oa[:r])
 
     def time_hmult(self, level, a, b, key, rescale=True, warmup=3, iters=20):
         """Device milliseconds per HMult of the reference's 64-bit build."""

@@ -354,6 +354,78 @@ def case_w64():
     return out
 
 
+def case_w64_ops():
+    """The 64-bit word path's Context operations against the reference's
+    own Context<uint64_t> on bootparam_40_64bit.json (Context.h:101-423):
+    Copy, Neg, MultImaginaryUnit, Add / Sub (also with rx on one side),
+    Mult (three-part tensor), Relinearize, RelinearizeRescale, MultKey,
+    Permute, PermuteConjugate, HRotAdd, HConjAdd, MultConst / AddConst
+    (constants from each side's own EncodeConstant) and LevelDown, on
+    uniform ciphertexts and keys at several levels, every word equal."""
+    p = load("bootparam_40_64bit.json")
+    ref = refdrv.RefContext64(p)
+    g = chd.Context64(json.dumps(p))
+    n = g.n
+    primes = g.primes()
+    nt, nm, na = len(p["terminal_primes"]), len(p["main_primes"]), len(p["auxiliary_primes"])
+    L = nt + nm
+    rng = np.random.default_rng(640)
+
+    def rows_of(level, aux=0):
+        m, t = g.level_np(level)
+        return [nt - t + i for i in range(m + t)] + [L + a for a in range(aux)]
+
+    def uniform(rows):
+        return np.stack([rng.integers(0, int(primes[r]), n, dtype=np.uint64) for r in rows])
+
+    beta_max = -(-L // na)
+    kb = np.stack([uniform(rows_of(g.max_level, na)) for _ in range(beta_max)])
+    ka = np.stack([uniform(rows_of(g.max_level, na)) for _ in range(beta_max)])
+    key = chd.EvaluationKey64(g, kb, ka)
+    K = (kb, ka)
+    enc = p["default_encryption_level"]
+    checked = []
+    for lvl in sorted({g.max_level, enc, 9, 2}, reverse=True):
+        scale = g.scale(min(lvl, enc))  # the imported ciphertexts' scale
+        a = tuple(uniform(rows_of(lvl)) for _ in range(2))
+        b = tuple(uniform(rows_of(lvl)) for _ in range(2))
+        r3 = uniform(rows_of(lvl))
+        ga, gb = g.import_ct(lvl, a, scale=scale), g.import_ct(lvl, b, scale=scale)
+        g3 = g.import_ct(lvl, a, scale=scale).set_rx(r3)
+        a3 = a + (r3,)
+        cx = g.encode_const(lvl, scale, 0.6180339887)
+        pairs = [
+            ("Copy", g.Copy(ga), ref.op("Copy", lvl, a)),
+            ("Neg", g.Neg(ga), ref.op("Neg", lvl, a)),
+            ("Neg rx", g.Neg(g3), ref.op("Neg", lvl, a3)),
+            ("MultImaginaryUnit", g.MultImaginaryUnit(ga), ref.op("MultImaginaryUnit", lvl, a)),
+            ("Add", g.Add(ga, gb), ref.op("Add", lvl, a, b)),
+            ("Sub", g.Sub(ga, gb), ref.op("Sub", lvl, a, b)),
+            ("Add rx", g.Add(g3, gb), ref.op("Add", lvl, a3, b)),
+            ("Sub rx", g.Sub(gb, g3), ref.op("Sub", lvl, b, a3)),
+            ("Mult", g.Mult(ga, gb), ref.op("Mult", lvl, a, b)),
+            ("Relinearize", g.Relinearize(g3, key), ref.op("Relinearize", lvl, a3, key=K)),
+            ("MultKey", g.MultKey(ga, key), ref.op("MultKey", lvl, a, key=K)),
+            ("Permute", g.Permute(ga, 5), ref.op("Permute", lvl, a, arg=5)),
+            ("PermuteConjugate", g.PermuteConjugate(ga), ref.op("PermuteConjugate", lvl, a)),
+            ("HRotAdd", g.HRotAdd(ga, gb, key, 3), ref.op("HRotAdd", lvl, a, b, key=K, arg=3)),
+            ("HConjAdd", g.HConjAdd(ga, gb, key), ref.op("HConjAdd", lvl, a, b, key=K)),
+            ("MultConst", g.MultConst(ga, cx, scale), ref.op("MultConst", lvl, a, scale=scale, value=0.6180339887)),
+            ("AddConst", g.AddConst(ga, cx), ref.op("AddConst", lvl, a, scale=scale, value=0.6180339887)),
+        ]
+        if lvl >= 1:
+            pairs.append(("RelinearizeRescale", g.RelinearizeRescale(g3, key),
+                          ref.op("RelinearizeRescale", lvl, a3, key=K)))
+        if 2 <= lvl <= enc:
+            pairs.append(("LevelDown", g.LevelDown(ga, lvl - 2), ref.op("LevelDown", lvl, a, arg=lvl - 2)))
+        for what, ours, theirs in pairs:
+            mine = ours.numpy()
+            assert len(mine) == len(theirs), f"64-bit {what} level {lvl}: parts {len(mine)} vs {len(theirs)}"
+            eq(f"64-bit {what} level {lvl}", list(mine), list(theirs))
+            checked.append(f"{what}@{lvl}")
+    return {"params": "bootparam_40_64bit.json", "checked": len(checked)}
+
+
 def case_hoisted():
     """Hoisted rotations: the reference's HoistHandler::EvaluateBabyStep
     (Hoist.cu:578-691; one ModUp, every rotation's key product and

@@ -36,7 +36,7 @@ pytestmark = pytest.mark.gpu
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
-@pytest.mark.parametrize("case", ["ntt24", "modswitch", "keyswitch", "mixed_batch", "w64", "hoisted", "context_ops", "context_ops40",
+@pytest.mark.parametrize("case", ["ntt24", "modswitch", "keyswitch", "mixed_batch", "w64", "w64_ops", "hoisted", "context_ops", "context_ops40",
                                   "encode", "decode", "boot40", "boot30", "boot35", "boot40_sparse"])
 def test_reference_parity(cuda_ok, case):
     if not refdrv.available():
