@@ -349,6 +349,144 @@ class BootContext {
 
 inline Ciphertext::Ciphertext(Context &ctx) { check(chd_ct_create(ctx.raw(), &ct_)); }
 
+// ---- the 64-bit word path: Context<uint64_t> (Context.cpp:952) ----
+
+class Context64;
+
+// Ciphertext<uint64_t>: uint64 residues [np][N] per part (rx after Mult)
+class Ciphertext64 {
+ public:
+  explicit Ciphertext64(Context64 &ctx);
+  ~Ciphertext64() { chd64_ct_destroy(ct_); }
+  Ciphertext64(const Ciphertext64 &) = delete;
+  Ciphertext64 &operator=(const Ciphertext64 &) = delete;
+  Ciphertext64(Ciphertext64 &&o) noexcept : ct_(o.ct_) { o.ct_ = nullptr; }
+  int NumMain() const { return info().num_main; }
+  int NumTer() const { return info().num_ter; }
+  bool HasRx() const { return chd64_ct_has_rx(ct_) == 1; }
+  double GetScale() const { return info().scale; }
+  int GetNumSlots() const { return info().num_slots; }
+  chd64_ciphertext *raw() const { return ct_; }
+
+ private:
+  struct Info {
+    int num_main, num_ter;
+    double scale;
+    int num_slots;
+  };
+  Info info() const {
+    Info i{};
+    check(chd64_ct_info(ct_, &i.num_main, &i.num_ter, &i.scale, &i.num_slots));
+    return i;
+  }
+  chd64_ciphertext *ct_ = nullptr;
+};
+
+// EvaluationKey<uint64_t>: beta pairs over [L + alpha][N]
+class EvaluationKey64 {
+ public:
+  EvaluationKey64(Context64 &ctx, int beta, const uint64_t *bx, const uint64_t *ax, bool on_device);
+  ~EvaluationKey64() { chd64_evk_destroy(k_); }
+  EvaluationKey64(const EvaluationKey64 &) = delete;
+  EvaluationKey64 &operator=(const EvaluationKey64 &) = delete;
+  chd64_evk *raw() const { return k_; }
+
+ private:
+  chd64_evk *k_ = nullptr;
+};
+
+// Context<uint64_t> (Context.h:17-424 with word = uint64_t)
+class Context64 {
+ public:
+  using Ct = Ciphertext64;
+  using Evk = EvaluationKey64;
+  static std::shared_ptr<Context64> Create(const std::string &param_json, int device = 0) {
+    chd64_context *c = nullptr;
+    check(chd64_context_create_json(param_json.c_str(), device, &c));
+    return std::shared_ptr<Context64>(new Context64(c));
+  }
+  ~Context64() { chd64_context_destroy(c_); }
+  Context64(const Context64 &) = delete;
+  Context64 &operator=(const Context64 &) = delete;
+
+  chd64_context *raw() const { return c_; }
+  int MaxLevel() const { return chd64_max_level(c_); }
+  double GetScale(int level) const { return chd64_scale(c_, level); }
+  void SetStream(void *cuda_stream) { check(chd64_context_set_stream(c_, cuda_stream)); }
+  void Synchronize() { check(chd64_context_synchronize(c_)); }
+
+  void Import(Ct &ct, int level, double scale, int num_slots, const uint64_t *bx, const uint64_t *ax,
+              const uint64_t *rx = nullptr, bool on_device = false) {
+    check(chd64_ct_import(c_, ct.raw(), level, scale, num_slots, bx, ax, on_device ? 1 : 0));
+    if (rx) check(chd64_ct_set_rx(c_, ct.raw(), rx, on_device ? 1 : 0));
+  }
+  void Export(const Ct &ct, uint64_t *bx, uint64_t *ax, uint64_t *rx = nullptr) {
+    check(chd64_ct_export(c_, ct.raw(), bx, ax));
+    if (rx && ct.HasRx()) check(chd64_ct_export_rx(c_, ct.raw(), rx));
+  }
+  // Encoder<uint64_t>::EncodeConstant: one Montgomery word per prime
+  std::vector<uint64_t> EncodeConstant(int level, double scale, double value, int num_aux = 0) {
+    int m = 0, t = 0;
+    check(chd64_level_np(c_, level, &m, &t));
+    std::vector<uint64_t> cx(m + t + num_aux);
+    check(chd64_encode_const(c_, level, scale, value, num_aux, cx.data()));
+    return cx;
+  }
+
+  // ---- evaluator (same signatures as the reference; constants as words) ----
+  void Copy(Ct &res, const Ct &a) const { check(chd64_copy(c_, res.raw(), a.raw())); }
+  void Add(Ct &res, const Ct &a, const Ct &b) const { check(chd64_add(c_, res.raw(), a.raw(), b.raw())); }
+  void Sub(Ct &res, const Ct &a, const Ct &b) const { check(chd64_sub(c_, res.raw(), a.raw(), b.raw())); }
+  void Neg(Ct &res, const Ct &a) const { check(chd64_neg(c_, res.raw(), a.raw())); }
+  void Mult(Ct &res, const Ct &a, const Ct &b) const { check(chd64_mult(c_, res.raw(), a.raw(), b.raw())); }
+  void Mult(Ct &res, const Ct &a, const std::vector<uint64_t> &cx, double const_scale) const {
+    check(chd64_mult_const(c_, res.raw(), a.raw(), cx.data(), const_scale));
+  }
+  void Add(Ct &res, const Ct &a, const std::vector<uint64_t> &cx) const {
+    check(chd64_add_const(c_, res.raw(), a.raw(), cx.data()));
+  }
+  void MultImaginaryUnit(Ct &res, const Ct &a) const { check(chd64_mult_imaginary_unit(c_, res.raw(), a.raw())); }
+  void Rescale(Ct &res, const Ct &a) const { check(chd64_rescale(c_, res.raw(), a.raw())); }
+  void Relinearize(Ct &res, const Ct &a, const Evk &key) const {
+    check(chd64_relinearize(c_, res.raw(), a.raw(), key.raw(), 0));
+  }
+  void RelinearizeRescale(Ct &res, const Ct &a, const Evk &key) const {
+    check(chd64_relinearize(c_, res.raw(), a.raw(), key.raw(), 1));
+  }
+  void MultKey(Ct &res, const Ct &a, const Evk &key) const { check(chd64_mult_key(c_, res.raw(), a.raw(), key.raw())); }
+  void Permute(Ct &res, const Ct &a, int rot_dist) const { check(chd64_permute(c_, res.raw(), a.raw(), rot_dist, 0)); }
+  void PermuteConjugate(Ct &res, const Ct &a) const { check(chd64_permute(c_, res.raw(), a.raw(), 0, 1)); }
+  void HMult(Ct &res, const Ct &a, const Ct &b, const Evk &mult_key, bool rescale = true) const {
+    check(chd64_hmult(c_, res.raw(), a.raw(), b.raw(), mult_key.raw(), rescale ? 1 : 0));
+  }
+  void HRot(Ct &res, const Ct &a, const Evk &rot_key, int rot_dist) const {
+    check(chd64_hrot(c_, res.raw(), a.raw(), rot_key.raw(), rot_dist));
+  }
+  void HConj(Ct &res, const Ct &a, const Evk &conj_key) const {
+    check(chd64_hconj(c_, res.raw(), a.raw(), conj_key.raw()));
+  }
+  void HRotAdd(Ct &res, const Ct &a, const Ct &b, const Evk &rot_key, int rot_dist) const {
+    check(chd64_hrot_add(c_, res.raw(), a.raw(), b.raw(), rot_key.raw(), rot_dist));
+  }
+  void HConjAdd(Ct &res, const Ct &a, const Ct &b, const Evk &conj_key) const {
+    check(chd64_hconj_add(c_, res.raw(), a.raw(), b.raw(), conj_key.raw()));
+  }
+  void LevelDown(Ct &res, const Ct &a, int target_level) const {
+    check(chd64_level_down(c_, res.raw(), a.raw(), target_level));
+  }
+
+ private:
+  explicit Context64(chd64_context *c) : c_(c) {}
+  chd64_context *c_ = nullptr;
+};
+
+inline Ciphertext64::Ciphertext64(Context64 &ctx) { check(chd64_ct_create(ctx.raw(), &ct_)); }
+
+inline EvaluationKey64::EvaluationKey64(Context64 &ctx, int beta, const uint64_t *bx, const uint64_t *ax,
+                                        bool on_device) {
+  check(chd64_evk_create(ctx.raw(), beta, bx, ax, on_device ? 1 : 0, &k_));
+}
+
 inline EvaluationKey::EvaluationKey(Context &ctx, int beta, const uint32_t *bx, const uint32_t *ax,
                                     bool on_device) {
   check(chd_evk_create(ctx.raw(), beta, bx, ax, on_device ? 1 : 0, &k_));
