@@ -1320,7 +1320,7 @@ KERNEL_OF_STAGE = {
 
 # sources a stage's kernel is compiled from (cheddar-fhe_b200/csrc): a
 # committed DRAM-traffic capture counts only while their fingerprint matches
-KERNEL_SOURCES = {"ks_rows": ["keyswitch.cu", "arith.cuh", "ntt_common.cuh", "kernels.h"]}
+KERNEL_SOURCES = {"ks_rows": ["keyswitch.cu", "arith.cuh", "ntt_common.cuh"]}
 
 
 def kernel_fingerprint(stage):

@@ -595,13 +595,14 @@ Status elem_parts(Context &C, ElemOp op, const NP &np, int parts, uint32_t *cons
                   const uint32_t *const *b, const uint32_t *k);
 
 // Splits a long list of rows into RowBatch launches: as few launches as
-// kMaxRows allows, with the rows spread evenly over them (a short last
-// launch would leave most SMs idle).
+// `cap` rows per launch (at most kMaxRows) allow, with the rows spread
+// evenly over them (a short last launch would leave most SMs idle).
 template <typename F>
-void for_row_batches(const std::vector<RowDesc> &rows, F &&launch) {
+void for_row_batches(const std::vector<RowDesc> &rows, F &&launch, int cap = kMaxRows) {
+  cap = cap < 1 || cap > kMaxRows ? kMaxRows : cap;
   const int total = static_cast<int>(rows.size());
-  const int nbat = (total + kMaxRows - 1) / kMaxRows;
-  const int per = nbat > 0 ? (total + nbat - 1) / nbat : kMaxRows;
+  const int nbat = (total + cap - 1) / cap;
+  const int per = nbat > 0 ? (total + nbat - 1) / nbat : cap;
   RowBatch rb;
   rb.count = 0;
   for (const RowDesc &r : rows) {

@@ -36,12 +36,15 @@ enum RowFlags : uint32_t {
   kMulSrc2 = 32u,      // inverse NTT row phase: input is src (.) src2 (Montgomery)
 };
 
-constexpr int kMaxRows = 120;
+// rows per row-phase launch: 256 descriptors of 72 bytes keep the launch
+// parameters under the 32 KiB limit
+constexpr int kMaxRows = 256;
 
 struct RowBatch {
   int count;
   RowDesc rows[kMaxRows];
 };
+static_assert(sizeof(RowBatch) + 16 <= 32764, "row batch beyond the kernel parameter limit");
 
 // Forward negacyclic NTT (bit-reversed output) of `count` limbs.
 // Column phase then row phase for log_n = 16; a single-kernel shared-memory
