@@ -129,3 +129,27 @@ def test_ntt_batches_on_alternating_streams(cuda_ok):
     assert np.array_equal(outs[True], outs[False])
     for i in (0, 13, 31):
         assert np.array_equal(outs[True][i], o.ntt(lvl, x[i], mont=True))
+
+
+def test_failed_half_leaves_context_usable(cuda_ok):
+    # a key with too few digits makes the first half of a split batch fail
+    # after the fork: the call returns the error, the join is still
+    # recorded, and the next batch on the same context is right
+    o, g = pair(KS)
+    (kb, ka), key = mult_key(KS)
+    lvl = 22
+    pairs = [(uniform_parts(KS, lvl, 3800 + i), uniform_parts(KS, lvl, 3850 + i)) for i in range(4)]
+    ga = [g.import_ct(lvl, a) for a, _ in pairs]
+    gb = [g.import_ct(lvl, b) for _, b in pairs]
+    short = chd.EvaluationKey(g, np.ascontiguousarray(kb[:1]), np.ascontiguousarray(ka[:1]))
+    g.stream_split = True
+    with pytest.raises(chd.CheddarError) as err:
+        g.HMultBatch(ga, gb, short, rescale=True)
+    assert "too few digits" in str(err.value)
+    g.synchronize()
+    outs = g.HMultBatch(ga, gb, key, rescale=True)
+    g.synchronize()
+    for r, (a, b) in zip(outs, pairs):
+        ref = o.hmult(lvl, a, b, (kb, ka), rescale=True)
+        p = _parts(r)
+        assert np.array_equal(p[0], ref[0]) and np.array_equal(p[1], ref[1])
