@@ -1028,7 +1028,24 @@ Status Context::modup_many(int level, int count, const uint32_t *const *src, uin
   ArenaScope scope(arena);
   int32_t *xt = static_cast<int32_t *>(arena.alloc(static_cast<size_t>(count) * nq * n * 4));
   CHD_CHECK(xt, kErrAlloc, "modup: scratch allocation failed");
-  if (P->log_n == 16) return modup_fused(level, count, src, dst, reinterpret_cast<uint32_t *>(xt));
+  if (P->log_n == 16) {
+    uint32_t *rows_out = reinterpret_cast<uint32_t *>(xt);
+    // two or more inputs: the halves on two streams (as the fused key
+    // switch), each with its own part of the scratch, unless an output of
+    // one half is an input of the other
+    const int h = (count + 1) / 2;
+    bool split = split_streams && aux_stream != nullptr && count >= 2;
+    for (int c = 0; c < count && split; c++)
+      for (int e = 0; e < count && split; e++)
+        if ((c < h) != (e < h))
+          for (int i = 0; i < m.beta; i++)
+            if (m.dig_e[i] > 0 && dst[c][i] == src[e]) split = false;
+    if (!split) return modup_fused(level, count, src, dst, rows_out);
+    return fork_halves([&](bool second) {
+      return second ? modup_fused(level, count - h, src + h, dst + h, rows_out + static_cast<size_t>(h) * nq * n)
+                    : modup_fused(level, h, src, dst, rows_out);
+    });
+  }
   // 1. INTT * (N q-hat_i)^-1, centred (INTTAndMultConst with normalize)
   std::vector<RowDesc> rows;
   for (int c = 0; c < count; c++)

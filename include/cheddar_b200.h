@@ -458,10 +458,11 @@ int chd_ks_tuned_shapes(int *out, int cap);
 int chd_ks_rows_tuned_shapes(int *out, int cap);
 /* Two-stream key switching (no reference counterpart; on by default, the
  * environment variable CHD_SPLIT_STREAMS=0 turns it off at context
- * creation): a fused key switch of two or more ciphertexts, and a ModDown
- * family call on four or more polynomials, at N = 2^16 (HMult / Relinearize
- * / MultKey / HRot batches, batched ModDown and rescaling, batched
- * bootstrapping) runs its two halves on the context stream and on a second
+ * creation): a fused key switch of two or more ciphertexts, a batched ModUp
+ * of two or more, and a ModDown family call on four or more polynomials, at
+ * N = 2^16 (HMult / Relinearize / MultKey / HRot batches, hoisted rotation
+ * batches, batched ModDown and rescaling, batched bootstrapping) runs its
+ * two halves on the context stream and on a second
  * stream of the context, forked from and joined back into the context
  * stream by events (graph capture included), unless a result of one half is
  * an operand or a result of the other.  Results are identical either way.

@@ -141,7 +141,8 @@ def test_failed_half_leaves_context_usable(cuda_ok):
     pairs = [(uniform_parts(KS, lvl, 3800 + i), uniform_parts(KS, lvl, 3850 + i)) for i in range(4)]
     ga = [g.import_ct(lvl, a) for a, _ in pairs]
     gb = [g.import_ct(lvl, b) for _, b in pairs]
-    short = chd.EvaluationKey(g, np.ascontiguousarray(kb[:1]), np.ascontiguousarray(ka[:1]))
+    _, basis = key.info()  # the key basis, one digit only
+    short = chd.EvaluationKey(g, np.ascontiguousarray(kb[:1]), np.ascontiguousarray(ka[:1]), basis=basis)
     g.stream_split = True
     with pytest.raises(chd.CheddarError) as err:
         g.HMultBatch(ga, gb, short, rescale=True)
