@@ -320,7 +320,8 @@ def main():
         for t in chd.ks_tuned_shapes()]
     # the row pass's choice per shape (ciphertexts, rows, mode) -> variant
     line["config"]["autotuned_row_passes"] = [
-        f"cts{t['cts']} rows{t['rows']} mode{t['mode']}: {'prefetch' if t['prefetch'] else 'in_place_loads'}"
+        f"cts{t['cts']} rows{t['rows']} mode{t['mode']}: "
+        f"{({0: 'in_place_loads', 1: 'prefetch', 2: 'in_place_loads_4ctas'}).get(t['variant'], t['variant'])}"
         for t in chd.ks_rows_tuned_shapes()]
     if rank == 0 and world == 1 and not args.no_reference_gpu and not args.hmult_only:
         ref = reference_gpu_run(args)

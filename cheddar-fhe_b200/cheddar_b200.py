@@ -259,13 +259,14 @@ def ks_tuned_shapes():
 
 def ks_rows_tuned_shapes():
     """The key-switch row pass's autotuned choices in this process: one dict
-    per launch shape with `prefetch` True when the variant that loads ahead
-    won."""
+    per launch shape with its `variant` (0 loads where used at 3 CTAs per
+    SM, 1 loads ahead at 2, 2 loads where used at 4) and `prefetch` True for
+    variant 1."""
     n = lib().chd_ks_rows_tuned_shapes(None, 0)
     out = (C.c_int * (5 * max(1, n)))()
     n = lib().chd_ks_rows_tuned_shapes(out, n)
     return [dict(device=out[5 * i], cts=out[5 * i + 1], rows=out[5 * i + 2], mode=out[5 * i + 3],
-                 prefetch=bool(out[5 * i + 4])) for i in range(n)]
+                 variant=out[5 * i + 4], prefetch=out[5 * i + 4] == 1) for i in range(n)]
 
 
 def load_params(name_or_path):

@@ -29,10 +29,11 @@ namespace {
 
 // PREFETCH: each digit's key words are loaded before its row NTT and the
 // next digit's ModUp row during it (more loads in flight per warp, sized for
-// 2 CTAs per SM); otherwise each load is issued where it is used (3 CTAs per
-// SM).  Both compute the same words; the launcher picks per launch shape.
-template <bool PREFETCH>
-__global__ void __launch_bounds__(256, PREFETCH ? 2 : 3) k_ks_rows(const __grid_constant__ KSRowsDesc d) {
+// 2 CTAs per SM); otherwise each load is issued where it is used, at MINB
+// CTAs per SM (3: 80 registers; 4: 64 registers, a few words spilled).  All
+// compute the same words; the launcher picks per launch shape.
+template <bool PREFETCH, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_ks_rows(const __grid_constant__ KSRowsDesc d) {
   __shared__ uint32_t sm[4][512];
   // grid (count, 32, max_rows): the ciphertexts sharing one key row are
   // neighbours in launch order, so the key row comes from HBM once
@@ -154,25 +155,29 @@ __global__ void __launch_bounds__(256, PREFETCH ? 2 : 3) k_ks_rows(const __grid_
 namespace {
 // Autotuning of the row pass (with the column passes' CHD_BCONV_AUTO): the
 // first launch of a shape (device, ciphertexts, largest row count, mode)
-// outside a stream capture times both variants three times, interleaved,
-// after a warm-up, and caches the faster; every launch writes the same
-// words, so the timing launches leave the right outputs.
+// outside a stream capture times the variants three times, interleaved,
+// after a warm-up, and caches the fastest; every launch writes the same
+// words, so the timing launches leave the right outputs.  Variants: 0 loads
+// where used at 3 CTAs per SM, 1 prefetching at 2, 2 loads where used at 4.
+constexpr int kKsRowsVariants = 3;
 std::mutex g_ksr_mu;
-std::map<std::tuple<int, int, int, int>, bool> g_ksr_cache;
+std::map<std::tuple<int, int, int, int>, int> g_ksr_cache;
 
-void launch_variant(const KSRowsDesc &d, bool prefetch, cudaStream_t s) {
+void launch_variant(const KSRowsDesc &d, int variant, cudaStream_t s) {
   const dim3 grid(d.count, 32, d.max_rows);
-  if (prefetch)
-    k_ks_rows<true><<<grid, 256, 0, s>>>(d);
+  if (variant == 1)
+    k_ks_rows<true, 2><<<grid, 256, 0, s>>>(d);
+  else if (variant == 2)
+    k_ks_rows<false, 4><<<grid, 256, 0, s>>>(d);
   else
-    k_ks_rows<false><<<grid, 256, 0, s>>>(d);
+    k_ks_rows<false, 3><<<grid, 256, 0, s>>>(d);
 }
 }  // namespace
 
 void launch_ks_rows(const KSRowsDesc &d, int log_n, cudaStream_t s, bool tune) {
   if (d.count <= 0 || d.max_rows <= 0 || log_n != 16) return;
   if (!tune) {
-    launch_variant(d, false, s);
+    launch_variant(d, 0, s);
     return;
   }
   int dev = 0;
@@ -188,38 +193,42 @@ void launch_ks_rows(const KSRowsDesc &d, int log_n, cudaStream_t s, bool tune) {
   }
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
-    launch_variant(d, false, s);
+    launch_variant(d, 0, s);
     return;
   }
-  cudaEvent_t ev[7] = {};
+  constexpr int kReps = 3;
+  cudaEvent_t ev[kReps * kKsRowsVariants + 1] = {};
   for (auto &e : ev)
     if (cudaEventCreate(&e) != cudaSuccess) {
       for (auto &f : ev)
         if (f) cudaEventDestroy(f);
-      launch_variant(d, false, s);
+      launch_variant(d, 0, s);
       return;
     }
-  launch_variant(d, false, s);
-  launch_variant(d, true, s);
+  for (int v = 0; v < kKsRowsVariants; v++) launch_variant(d, v, s);
   cudaEventRecord(ev[0], s);
-  for (int r = 0; r < 3; r++) {
-    launch_variant(d, false, s);
-    cudaEventRecord(ev[2 * r + 1], s);
-    launch_variant(d, true, s);
-    cudaEventRecord(ev[2 * r + 2], s);
-  }
-  bool ok = cudaEventSynchronize(ev[6]) == cudaSuccess;
-  float best[2] = {1e30f, 1e30f};
-  for (int r = 0; ok && r < 3; r++)
-    for (int v = 0; ok && v < 2; v++) {
+  for (int r = 0; r < kReps; r++)
+    for (int v = 0; v < kKsRowsVariants; v++) {
+      launch_variant(d, v, s);
+      cudaEventRecord(ev[r * kKsRowsVariants + v + 1], s);
+    }
+  bool ok = cudaEventSynchronize(ev[kReps * kKsRowsVariants]) == cudaSuccess;
+  float best[kKsRowsVariants];
+  for (float &b : best) b = 1e30f;
+  for (int r = 0; ok && r < kReps; r++)
+    for (int v = 0; ok && v < kKsRowsVariants; v++) {
       float t = 0.f;
-      ok = cudaEventElapsedTime(&t, ev[2 * r + v], ev[2 * r + v + 1]) == cudaSuccess;
+      const int i = r * kKsRowsVariants + v;
+      ok = cudaEventElapsedTime(&t, ev[i], ev[i + 1]) == cudaSuccess;
       best[v] = t < best[v] ? t : best[v];
     }
   for (auto &e : ev) cudaEventDestroy(e);
   if (ok) {
+    int pick = 0;
+    for (int v = 1; v < kKsRowsVariants; v++)
+      if (best[v] < best[pick]) pick = v;
     std::lock_guard<std::mutex> lock(g_ksr_mu);
-    g_ksr_cache[key] = best[1] < best[0];
+    g_ksr_cache[key] = pick;
   }
 }
 
@@ -232,7 +241,7 @@ int ks_rows_tuned_shapes(int *out, int cap) {
       out[5 * k + 1] = std::get<1>(e.first);
       out[5 * k + 2] = std::get<2>(e.first);
       out[5 * k + 3] = std::get<3>(e.first);
-      out[5 * k + 4] = e.second ? 1 : 0;
+      out[5 * k + 4] = e.second;
     }
     k++;
   }

@@ -452,9 +452,10 @@ int chd_ks_tuned_shapes(int *out, int cap);
 /* The same for the key-switch row pass (no reference counterpart): with
  * CHD_BCONV_AUTO its first launch of each shape times the variant that
  * loads each digit's key words and the next digit's ModUp row ahead (2 CTAs
- * per SM) against the one that loads where it computes (3 CTAs per SM);
- * five ints per shape (device, ciphertexts, largest row count of the
- * launch, mode, 1 for the prefetching variant); returns the count. */
+ * per SM) against the one that loads where it computes at 3 and at 4 CTAs
+ * per SM; five ints per shape (device, ciphertexts, largest row count of
+ * the launch, mode, variant: 0 loads where used at 3 CTAs per SM, 1 loads
+ * ahead, 2 loads where used at 4); returns the count. */
 int chd_ks_rows_tuned_shapes(int *out, int cap);
 /* Two-stream key switching (no reference counterpart; on by default, the
  * environment variable CHD_SPLIT_STREAMS=0 turns it off at context
