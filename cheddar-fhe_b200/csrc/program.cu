@@ -61,6 +61,34 @@ Status Context::run_program(const Program &prog, std::vector<DeviceCt> &regs, co
   return run_program_batch(prog, 1, &r, keys, lts);
 }
 
+namespace {
+// Per-ciphertext launches of one op on alternating streams: forks the
+// context's second stream from the context stream at construction, selects
+// the stream of ciphertext i, and at destruction (every exit path) restores
+// the context stream and joins the second stream back into it.
+struct Alternation {
+  Context &C;
+  bool on;
+  cudaStream_t main;
+  Alternation(Context &c, bool want) : C(c), on(want), main(c.stream) {
+    if (on)
+      on = cudaEventRecord(C.ev_fork, main) == cudaSuccess && cudaStreamWaitEvent(C.aux_stream, C.ev_fork, 0) == cudaSuccess;
+  }
+  void select(int i) {
+    if (on) C.stream = (i & 1) ? C.aux_stream : main;
+  }
+  void finish() {
+    if (!on) return;
+    on = false;
+    C.stream = main;
+    if (cudaEventRecord(C.ev_join, C.aux_stream) == cudaSuccess) cudaStreamWaitEvent(main, C.ev_join, 0);
+  }
+  ~Alternation() { finish(); }
+  Alternation(const Alternation &) = delete;
+  Alternation &operator=(const Alternation &) = delete;
+};
+}  // namespace
+
 Status Context::run_program_batch(const Program &prog, int count, std::vector<DeviceCt> *const *R,
                                   const ProgKeys &keys, const std::vector<const LTPlan *> *lts) {
   // The program on `count` ciphertexts, each with its own registers R[c]:
@@ -319,9 +347,16 @@ Status Context::run_program_batch(const Program &prog, int count, std::vector<De
       continue;
     }
     // ---- ops that run per ciphertext (constant accumulations of the
-    // batch joined into few launches) ----
+    // batch joined into few launches; the element-wise ops of consecutive
+    // ciphertexts, which take no scratch, alternate between the context
+    // stream and its second stream so that their short launches overlap) ----
     defer = count > 1 && (op.kind == OpKind::kConstMult || op.kind == OpKind::kConstAccum);
+    const bool alt = count > 1 && split_streams && aux_stream != nullptr &&
+                     (op.kind == OpKind::kTensor || op.kind == OpKind::kAdd || op.kind == OpKind::kSub ||
+                      op.kind == OpKind::kAddConst || op.kind == OpKind::kCopy || op.kind == OpKind::kMultImag);
+    Alternation alternation(*this, alt);
     for (int bc = 0; bc < count; bc++) {
+    alternation.select(bc);
     std::vector<DeviceCt> &regs = *R[bc];
     DeviceCt &spare = regs[prog.nregs], &spare2 = regs[prog.nregs + 1];
     DeviceCt &t = spare;
@@ -505,6 +540,7 @@ Status Context::run_program_batch(const Program &prog, int count, std::vector<De
     }
     if (!meta) swap_regs(regs.at(op.dst), t);
     }
+    alternation.finish();
     defer = false;
     flush_accum();
   }
