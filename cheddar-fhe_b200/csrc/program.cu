@@ -296,7 +296,11 @@ Status Context::run_program_batch(const Program &prog, int count, std::vector<De
         }
         CHD_CHECK(conj_key, kErrKey, "program: conjugation key missing");
         CHD_TRY(mult_key_batch(op.a, *conj_key));
-        for (int c = 0; c < count; c++) CHD_TRY(permute(R[c]->at(prog.nregs), R[c]->at(prog.nregs + 1), -1));
+        Alternation alternation(*this, split_streams && aux_stream != nullptr);
+        for (int c = 0; c < count; c++) {
+          alternation.select(c);
+          CHD_TRY(permute(R[c]->at(prog.nregs), R[c]->at(prog.nregs + 1), -1));
+        }
         break;
       }
       case OpKind::kHRotAdd: {
@@ -311,7 +315,9 @@ Status Context::run_program_batch(const Program &prog, int count, std::vector<De
         const DeviceEvk *k = nullptr;
         CHD_TRY(rot_key_of(op.rot, &k));
         CHD_TRY(mult_key_batch(op.a, *k));
+        Alternation alternation(*this, split_streams && aux_stream != nullptr);
         for (int c = 0; c < count; c++) {
+          alternation.select(c);
           // res = Permute(MultKey(a)) + b (Context.cpp:800-830)
           DeviceCt &t = R[c]->at(prog.nregs);
           CHD_TRY(permute(t, R[c]->at(prog.nregs + 1), dist));
