@@ -2323,7 +2323,7 @@ Status Context::hoisted_rotate_batch(int count, const DeviceCt *const *a, int R,
         }
         d.galois_inv[j] = P->galois_of(n / 2 - dd[j0 + j]);
       }
-      launch_hoisted(d, P->log_n, stream);
+      launch_hoisted(d, P->log_n, stream, ks_engine == 2);
     }
   }
   return check_cuda("hoisted rotate");

@@ -2,6 +2,10 @@
 // automorphism kernels.  All are HBM-streaming integer kernels: each thread
 // owns 4 consecutive coefficients (128-bit loads and stores), grid.y walks
 // the limbs (or jobs) of the batch.
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include "arith.cuh"
 #include "kernels.h"
 
@@ -246,10 +250,10 @@ __global__ void __launch_bounds__(256) k_permute(const __grid_constant__ Permute
 // a batch that read the same key tile are neighbours in launch order, so the
 // keys come from HBM once per batch.
 // BMAX: digits held per thread; with at most 4 (every parameter set here at
-// the levels hoisted rotations run at) the kernel fits 3 CTAs per SM instead
-// of 2
-template <int BMAX>
-__global__ void __launch_bounds__(256, BMAX <= 4 ? 3 : 2) k_hoisted(const __grid_constant__ HoistDesc d, int log_n) {
+// the levels hoisted rotations run at) the kernel fits 3 CTAs per SM (MINB)
+// instead of 2, or 4 with a few words spilled
+template <int BMAX, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_hoisted(const __grid_constant__ HoistDesc d, int log_n) {
   const int n = 1 << log_n;
   const int c = blockIdx.x;
   const int r = blockIdx.z;
@@ -372,15 +376,80 @@ void launch_permute(const PermuteBatch &b, int log_n, cudaStream_t s) {
   k_permute<<<dim3((n / 4 + 255) / 256, b.count), 256, 0, s>>>(b, log_n);
 }
 
-void launch_hoisted(const HoistDesc &d, int log_n, cudaStream_t s) {
-  if (d.rows <= 0 || d.R <= 0) return;
+namespace {
+// Autotuning of the baby-step kernel (with CHD_BCONV_AUTO): for up to 4
+// digits, the first launch of a shape (device, ciphertexts, rotations, rows,
+// digits) outside a stream capture times the 3- and 4-CTA forms three times,
+// interleaved, after a warm-up, and caches the faster; every launch writes
+// the same words.
+std::mutex g_hoist_mu;
+std::map<std::tuple<int, int, int, int, int>, int> g_hoist_cache;
+
+void launch_hoisted_variant(const HoistDesc &d, int log_n, int variant, cudaStream_t s) {
   const int n = 1 << log_n;
-  if (d.count <= 0 || d.count > kMaxHoistCts) return;
   const dim3 grid(d.count, (n / 4 + 255) / 256, d.rows);
-  if (d.beta <= 4)
-    k_hoisted<4><<<grid, 256, 0, s>>>(d, log_n);
+  if (d.beta > 4)
+    k_hoisted<8, 2><<<grid, 256, 0, s>>>(d, log_n);
+  else if (variant == 1)
+    k_hoisted<4, 4><<<grid, 256, 0, s>>>(d, log_n);
   else
-    k_hoisted<8><<<grid, 256, 0, s>>>(d, log_n);
+    k_hoisted<4, 3><<<grid, 256, 0, s>>>(d, log_n);
+}
+}  // namespace
+
+void launch_hoisted(const HoistDesc &d, int log_n, cudaStream_t s, bool tune) {
+  if (d.rows <= 0 || d.R <= 0) return;
+  if (d.count <= 0 || d.count > kMaxHoistCts) return;
+  if (!tune || d.beta > 4) {
+    launch_hoisted_variant(d, log_n, 0, s);
+    return;
+  }
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const auto key = std::make_tuple(dev, d.count, d.R, d.rows, d.beta);
+  {
+    std::lock_guard<std::mutex> lock(g_hoist_mu);
+    auto it = g_hoist_cache.find(key);
+    if (it != g_hoist_cache.end()) {
+      launch_hoisted_variant(d, log_n, it->second, s);
+      return;
+    }
+  }
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+    launch_hoisted_variant(d, log_n, 0, s);
+    return;
+  }
+  constexpr int kVariants = 2, kReps = 3;
+  cudaEvent_t ev[kVariants * kReps + 1] = {};
+  for (auto &e : ev)
+    if (cudaEventCreate(&e) != cudaSuccess) {
+      for (auto &f : ev)
+        if (f) cudaEventDestroy(f);
+      launch_hoisted_variant(d, log_n, 0, s);
+      return;
+    }
+  for (int v = 0; v < kVariants; v++) launch_hoisted_variant(d, log_n, v, s);
+  cudaEventRecord(ev[0], s);
+  for (int r = 0; r < kReps; r++)
+    for (int v = 0; v < kVariants; v++) {
+      launch_hoisted_variant(d, log_n, v, s);
+      cudaEventRecord(ev[r * kVariants + v + 1], s);
+    }
+  bool ok = cudaEventSynchronize(ev[kVariants * kReps]) == cudaSuccess;
+  float best[kVariants] = {1e30f, 1e30f};
+  for (int r = 0; ok && r < kReps; r++)
+    for (int v = 0; ok && v < kVariants; v++) {
+      float t = 0.f;
+      const int i = r * kVariants + v;
+      ok = cudaEventElapsedTime(&t, ev[i], ev[i + 1]) == cudaSuccess;
+      best[v] = t < best[v] ? t : best[v];
+    }
+  for (auto &e : ev) cudaEventDestroy(e);
+  if (ok) {
+    std::lock_guard<std::mutex> lock(g_hoist_mu);
+    g_hoist_cache[key] = best[1] < best[0] ? 1 : 0;
+  }
 }
 
 }  // namespace chd

@@ -322,6 +322,8 @@ struct HoistDesc {
   int16_t key_row[64];
   int beta, rows, nq, R, count;
 };
-void launch_hoisted(const HoistDesc &d, int log_n, cudaStream_t s);
+// tune: time the 3- and 4-CTA forms on the first launch of each shape (up
+// to 4 digits) and keep the faster
+void launch_hoisted(const HoistDesc &d, int log_n, cudaStream_t s, bool tune = false);
 
 }  // namespace chd
