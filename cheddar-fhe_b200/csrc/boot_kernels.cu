@@ -11,6 +11,10 @@
 //    ElementWiseHandler::PAccum).
 //  * k_const_accum: sum_i c_i * ct_i with one constant per limb and term
 //    (ElementWiseHandler::CAccum, src/core/ElementWise.cu:1355-1643).
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include "arith.cuh"
 #include "kernels.h"
 
@@ -71,8 +75,8 @@ __device__ __forceinline__ void st_vec(uint32_t *p, const uint32_t (&x)[V]) {
 // steps share one Montgomery reduction (mont_mac2).  Block
 // x = ciphertext + count * column block: the blocks of a batch that read the
 // same plaintext tile run back to back and share it through L2.
-template <int G, int V>
-__global__ void __launch_bounds__(256) k_pt_accum(const __grid_constant__ PtAccumDesc d) {
+template <int G, int V, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_pt_accum(const __grid_constant__ PtAccumDesc d) {
   const int r = blockIdx.y;
   const int c = blockIdx.x % d.count, xb = blockIdx.x / d.count;
   const uint32_t q = d.q[r];
@@ -175,7 +179,61 @@ void launch_modup_to_max(const ModUpToMaxDesc &d, cudaStream_t s) {
   k_modup_to_max<<<dim3(64, d.rows, d.parts), 256, 0, s>>>(d);
 }
 
-void launch_pt_accum(const PtAccumDesc &d, cudaStream_t s) {
+namespace {
+// The faster of two launch variants of a shape: cached per (device, shape);
+// the first launch of a shape outside a stream capture times both three
+// times, interleaved, after a warm-up (every launch writes the same words);
+// returns the variant the caller launches once more.
+std::mutex g_pt_mu;
+std::map<std::tuple<int, int, int, int, int>, int> g_pt_cache;
+
+template <class F>
+int pick_variant(std::tuple<int, int, int, int> shape, F &&launch, cudaStream_t s) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const auto key = std::tuple_cat(std::make_tuple(dev), shape);
+  {
+    std::lock_guard<std::mutex> lock(g_pt_mu);
+    auto it = g_pt_cache.find(key);
+    if (it != g_pt_cache.end()) return it->second;
+  }
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return 0;
+  constexpr int kReps = 3;
+  cudaEvent_t ev[2 * kReps + 1] = {};
+  for (auto &e : ev)
+    if (cudaEventCreate(&e) != cudaSuccess) {
+      for (auto &f : ev)
+        if (f) cudaEventDestroy(f);
+      return 0;
+    }
+  launch(0);
+  launch(1);
+  cudaEventRecord(ev[0], s);
+  for (int r = 0; r < kReps; r++)
+    for (int v = 0; v < 2; v++) {
+      launch(v);
+      cudaEventRecord(ev[2 * r + v + 1], s);
+    }
+  bool ok = cudaEventSynchronize(ev[2 * kReps]) == cudaSuccess;
+  float best[2] = {1e30f, 1e30f};
+  for (int r = 0; ok && r < kReps; r++)
+    for (int v = 0; ok && v < 2; v++) {
+      float t = 0.f;
+      ok = cudaEventElapsedTime(&t, ev[2 * r + v], ev[2 * r + v + 1]) == cudaSuccess;
+      best[v] = t < best[v] ? t : best[v];
+    }
+  for (auto &e : ev) cudaEventDestroy(e);
+  const int pick = ok && best[1] < best[0] ? 1 : 0;
+  if (ok) {
+    std::lock_guard<std::mutex> lock(g_pt_mu);
+    g_pt_cache[key] = pick;
+  }
+  return pick;
+}
+}  // namespace
+
+void launch_pt_accum(const PtAccumDesc &d, cudaStream_t s, bool tune) {
   if (d.rows <= 0 || d.rows > 64 || d.outs <= 0 || d.outs > kMaxPtAccumOuts || d.ins <= 0 ||
       d.ins > kMaxPtAccumIn || d.count <= 0 || d.count > kMaxPtAccumCts)
     return;
@@ -191,14 +249,23 @@ void launch_pt_accum(const PtAccumDesc &d, cudaStream_t s) {
     for (int t = 0; t < d.ins; t++) bits |= reinterpret_cast<uintptr_t>(d.pt[o][t]);
   const bool vec = (bits & 15) == 0;
   auto grid = [&](int v) { return dim3(d.count * ((d.n / v + 255) / 256), d.rows); };
-  if (!vec)
-    k_pt_accum<16, 1><<<grid(1), 256, 0, s>>>(d);
-  else if (d.outs <= 4)
-    k_pt_accum<4, 4><<<grid(4), 256, 0, s>>>(d);
-  else if (d.outs <= 8)
-    k_pt_accum<8, 2><<<grid(2), 256, 0, s>>>(d);
-  else
-    k_pt_accum<16, 1><<<grid(1), 256, 0, s>>>(d);
+  if (!vec) {
+    k_pt_accum<16, 1, 4><<<grid(1), 256, 0, s>>>(d);
+  } else if (d.outs <= 4) {
+    // 3 CTAs per SM (74 registers) or 4 (64, a few words spilled): timed
+    // on the first launch of a shape when tuning
+    auto launch = [&](int variant) {
+      if (variant == 1)
+        k_pt_accum<4, 4, 4><<<grid(4), 256, 0, s>>>(d);
+      else
+        k_pt_accum<4, 4, 3><<<grid(4), 256, 0, s>>>(d);
+    };
+    launch(tune ? pick_variant(std::make_tuple(d.count, d.rows, d.ins, d.outs), launch, s) : 0);
+  } else if (d.outs <= 8) {
+    k_pt_accum<8, 2, 4><<<grid(2), 256, 0, s>>>(d);
+  } else {
+    k_pt_accum<16, 1, 4><<<grid(1), 256, 0, s>>>(d);
+  }
 }
 
 void launch_const_accum(const ConstAccumDesc &d, cudaStream_t s) {

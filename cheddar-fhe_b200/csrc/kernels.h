@@ -130,7 +130,9 @@ struct PtAccumDesc {
   int32_t qinv[64];
   int rows, ins, outs, n, count;
 };
-void launch_pt_accum(const PtAccumDesc &d, cudaStream_t s);
+// tune: time the 3- and 4-CTA forms of the 4-output kernel on the first
+// launch of each shape and keep the faster
+void launch_pt_accum(const PtAccumDesc &d, cudaStream_t s, bool tune = false);
 
 // dst[o][r] = sum_t c[t][r] * src[t][o][src_row0[t] + r] for every output o
 // (a ciphertext part; several ciphertexts sharing the terms' constants fill

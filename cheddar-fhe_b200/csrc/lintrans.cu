@@ -297,7 +297,7 @@ Status Context::lt_evaluate_min_ks_batch(int count, DeviceCt *const *res, const 
       d.rows = nq;
       d.n = n;
       d.outs = 1;
-      launch_pt_accum(d, stream);
+      launch_pt_accum(d, stream, ks_engine == 2);
     }
     for (int c = 0; c < count; c++) {
       if (!first) CHD_TRY(add(acc[c], acc[c], tmp[c]));
@@ -527,7 +527,7 @@ struct HoistOps {
             d.out_a[c][o] = outs[c0 + c][o0 + o].second;
           }
         }
-        launch_pt_accum(d, C.stream);
+        launch_pt_accum(d, C.stream, C.ks_engine == 2);
       }
     }
     return kOk;
