@@ -391,6 +391,17 @@ bool tune_and_launch(const MSColBatch &b, int max_k, int max_m, cudaStream_t s, 
     int bi = 0;
     for (int i = 1; i < nc; i++)
       if (best[i] < best[bi]) bi = i;
+    // timed alone, a CUDA-core candidate can edge out a tensor-core one by
+    // noise; but the CUDA-core pass (168-254 registers per thread) shares an
+    // SM poorly with the kernels of a key switch's other half on the second
+    // stream, so within 3 % of the fastest the fastest tensor-core candidate
+    // is kept
+    if (cand[bi].engine == 0) {
+      int ti = -1;
+      for (int i = 0; i < nc; i++)
+        if (cand[i].engine != 0 && best[i] <= best[bi] * 1.03f && (ti < 0 || best[i] < best[ti])) ti = i;
+      if (ti >= 0) bi = ti;
+    }
     *out = cand[bi];
     std::lock_guard<std::mutex> lock(g_tune_mu);
     g_tune_cache[key] = cand[bi];

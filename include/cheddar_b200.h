@@ -436,7 +436,9 @@ int chd_bconv_batch(chd_context *ctx, int engine, int npoly, const int32_t *xt_d
  * (device, sources, jobs, targets) outside a stream capture times the
  * three with each split of the targets over 1, 2, 4 or the heuristic
  * number of CTAs per column tile (one host synchronisation per shape and
- * process) and keeps the fastest; an untuned shape met during a capture
+ * process) and keeps the fastest (a tensor-core candidate within 3 % of a
+ * faster CUDA-core one, as it shares an SM better with the other stream's
+ * kernels); an untuned shape met during a capture
  * uses the tensor cores with the heuristic split.  No reference counterpart (the reference has one CUDA-core
  * implementation, src/core/ModSwitch.cu:23-171).  chd_get_ks_engine returns
  * the engine, -1 for a null context. */
