@@ -165,7 +165,10 @@ struct MSColJob {
   uint8_t dst_row[64], dst_gidx[64];
   uint32_t c0[16], c0s[16];
 };
-constexpr int kMaxMSColJobs = 24;
+// jobs per column-pass launch: 64 descriptors of 320 bytes keep the launch
+// parameters under the 32 KiB limit (a batched ModDown of 30 ciphertexts'
+// 60 polynomials is one launch per stream half)
+constexpr int kMaxMSColJobs = 64;
 struct MSColBatch {
   int count;
   int engine;             // base conversion on 0: CUDA cores, 1: tensor cores, 3: tensor cores with
@@ -177,6 +180,7 @@ struct MSColBatch {
   const int32_t *qinvs;
   MSColJob jobs[kMaxMSColJobs];
 };
+static_assert(sizeof(MSColBatch) + 16 <= 32764, "column-pass batch beyond the kernel parameter limit");
 void launch_modswitch_cols(const MSColBatch &b, int log_n, cudaStream_t s);
 // the autotuned choices (engine, target split) cached so far: 6 ints per
 // shape (device, largest K, jobs, largest M, engine, split); returns the count
