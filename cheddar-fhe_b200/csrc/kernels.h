@@ -270,11 +270,14 @@ struct ElemRow {
   int32_t qinv;
   uint32_t k;             // per-limb constant
 };
-constexpr int kMaxElemRows = 96;
+// limbs per element-wise launch: every part of a ciphertext of up to 64
+// primes, or of a few of them, in one launch (parameter size checked below)
+constexpr int kMaxElemRows = 256;
 struct ElemBatch {
   int count;
   ElemRow rows[kMaxElemRows];
 };
+static_assert(sizeof(ElemBatch) + 16 <= 32764, "element-wise batch beyond the kernel parameter limit");
 void launch_elementwise(ElemOp op, const ElemBatch &b, int log_n, cudaStream_t s);
 
 // Tensor product of (b1, a1) x (b2, a2) -> (d0, d1, d2) (Karatsuba form)
@@ -300,12 +303,13 @@ struct PermuteRow {
   const uint32_t *add;   // optional addend (PermuteAccum with src0)
   uint32_t q;
 };
-constexpr int kMaxPermuteRows = 128;
+constexpr int kMaxPermuteRows = 256;
 struct PermuteBatch {
   int count;
   uint32_t galois;
   PermuteRow rows[kMaxPermuteRows];
 };
+static_assert(sizeof(PermuteBatch) + 16 <= 32764, "permute batch beyond the kernel parameter limit");
 void launch_permute(const PermuteBatch &b, int log_n, cudaStream_t s);
 
 // Hoisted rotations: one launch for up to kMaxHoist rotations of one ModUp'ed
